@@ -1,0 +1,149 @@
+/*
+ * C-ABI of libsfincs_gpu.so: the B200 SFINCS time-stepping core.
+ *
+ * The first block replaces the reference's BMI/XMI shared-library surface
+ * one for one (source/src/sfincs_bmi.f90, built as sfincs.dll/libsfincs.so and
+ * bound by xmipy or any iso_c_binding caller): same symbol names, argument
+ * passing (by reference unless the Fortran declares `value`), return codes
+ * (0 = success) and 1-based cell indices.  The remaining blocks are additions
+ * with no counterpart in the reference.
+ *
+ * Threading: like the reference (module-level state), the BMI block drives
+ * ONE global model per process; callers serialise calls.  The sfg_model_* and
+ * sfg_ensemble_* handles are independent objects.
+ */
+#ifndef SFINCS_BMI_H
+#define SFINCS_BMI_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define SFG_API __attribute__((visibility("default")))
+#else
+#define SFG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- BMI string-length constants (sfincs_bmi.f90:41-52) ------------------ */
+extern SFG_API int BMI_LENVARADDRESS;    /* 64   */
+extern SFG_API int BMI_LENVARTYPE;       /* 64   */
+extern SFG_API int BMI_LENGRIDTYPE;      /* 64   */
+extern SFG_API int BMI_LENCOMPONENTNAME; /* 64   */
+extern SFG_API int BMI_LENVERSION;       /* 256  */
+extern SFG_API int BMI_LENERRMESSAGE;    /* 1024 */
+
+/* ---- lifecycle ------------------------------------------------------------- */
+/* sfincs_bmi.f90:56-63.  Reads ./sfincs.inp (current working directory), sets
+ * use_qext, builds the device-resident model on the current CUDA device.
+ * Returns 0, or non-zero with get_last_bmi_error() describing the failure
+ * (the reference stops the process on bad input instead). */
+SFG_API int initialize(void);
+/* sfincs_bmi.f90:65-73: exactly one time step (if t < tstop). */
+SFG_API int update(void);
+/* sfincs_bmi.f90:75-85: step while t < t_target (the last step may overshoot). */
+SFG_API int update_until(double t_target);
+/* sfincs_bmi.f90:87-93: releases the model; returns 1 if the run stopped on
+ * the minimum-time-step instability check (sfincs_lib.f90:634-648, 807-815). */
+SFG_API int finalize(void);
+
+/* ---- data exchange ---------------------------------------------------------- */
+/* sfincs_bmi.f90:95-129.  Host pointers owned by the library, valid until
+ * finalize().  Names: "z_xz","z_yz","zb","subgrid_z_zmin","qext" (float[np]),
+ * "zs" (double[np]).  "zs" is refreshed from the device after every
+ * update()/update_until() once its pointer has been taken; "qext" is copied to
+ * the device before every update()/update_until() once its pointer has been
+ * taken.  Unknown or unavailable names: *ptr = NULL, returns -1. */
+SFG_API int get_value_ptr(const char* name, void** ptr);
+/* sfincs_bmi.f90:131-157: shape[0] = np for the names above. */
+SFG_API int get_var_shape(const char* name, int shape[6]);
+/* sfincs_bmi.f90:159-185: "float", "double" or "integer" into type[BMI_LENVARTYPE]. */
+SFG_API int get_var_type(const char* name, char* type);
+/* sfincs_bmi.f90:187-207 */
+SFG_API int get_var_rank(const char* name, int* rank);
+/* sfincs_bmi.f90:209-235: only "qext" (switches the external source term). */
+SFG_API int set_logical(const char* name, const int* value);
+
+/* ---- time (sfincs_bmi.f90:237-275) -------------------------------------------- */
+SFG_API int get_start_time(double* t);
+SFG_API int get_end_time(double* t);
+SFG_API int get_time_step(double* dt);
+SFG_API int get_current_time(double* t);
+
+/* ---- extras -------------------------------------------------------------------- */
+/* sfincs_bmi.f90:277-284: re-derive zbuvmx (and the device bed level) after the
+ * caller edited "zb" through its pointer. */
+SFG_API int update_zbuv(void);
+/* sfincs_bmi.f90:286-297: wave-enhanced roughness is not part of this core
+ * (initialize() rejects inputs that enable it); returns 0 without effect. */
+SFG_API int update_apparent_roughness(void);
+/* sfincs_bmi.f90:299-316: 1-based active-cell index of point (x, y), 0 if outside. */
+SFG_API int get_sfincs_cell_index(const double* x, const double* y, int* index);
+/* sfincs_bmi.f90:318-349: n points, n passed by value. */
+SFG_API int get_sfincs_cell_indices(const double* x, const double* y, int* index, int n);
+/* sfincs_bmi.f90:351-373: area (m2) of 1-based cell index. */
+SFG_API int get_sfincs_cell_area(const int* index, double* area);
+/* sfincs_bmi.f90:378-387: last error message into msg[BMI_LENERRMESSAGE]. */
+SFG_API int get_last_bmi_error(char* msg);
+
+/* ---- additions (no counterpart in the reference) -------------------------------- */
+/* initialize() for a model directory other than the working directory. */
+SFG_API int initialize_config(const char* model_dir);
+/* Copy-based access: "zs" (double[np]), "zsmax","qext" (float[np]),
+ * "z_volume" (double[np], subgrid), "qx","qy","uvx","uvy" (float[np]: flux /
+ * velocity of each cell's right (x) or upper (y) face, 0 where no face).
+ * bytes must equal the array size. */
+SFG_API int get_var(const char* name, void* dst, size_t bytes);
+SFG_API int set_var(const char* name, const void* src, size_t bytes);
+
+/* ---- model handles: independent models (no global state) ------------------------- */
+/* Create a device-resident model from <model_dir>/sfincs.inp.  bmi != 0 turns
+ * the external source term (qext) on, as initialize() does.  NULL on error;
+ * the message is then in err[errlen]. */
+SFG_API void* sfg_model_create(const char* model_dir, int bmi, char* err, int errlen);
+SFG_API void sfg_model_destroy(void* model);
+/* sfincs_update semantics: run while t < t_end, at most max_steps steps when
+ * max_steps >= 0; steps are issued as CUDA graphs of `chunk` steps. */
+SFG_API int sfg_model_run(void* model, double t_end, long long max_steps, int chunk);
+/* Issue nsteps steps on the model's stream without waiting (timing helper). */
+SFG_API int sfg_model_issue(void* model, int nsteps);
+SFG_API int sfg_model_sync(void* model);
+/* [t, dt, min_dt, nt, error, t0, t1, np, npuv, nkcuv2, ngbnd, subgrid,
+ *  bflux_vol, rain_vol, src_vol, dtmax, dtmin, device_bytes, ntiles] */
+SFG_API int sfg_model_scalars(void* model, double out[19]);
+/* Same names as get_var, plus "kfuv" (float[2*np]: u then v face wet flags). */
+SFG_API int sfg_model_get(void* model, const char* name, void* dst, size_t bytes);
+SFG_API int sfg_model_set(void* model, const char* name, const void* src, size_t bytes);
+/* Total water volume (m3, FP64) of the active cells; subgrid: sum of z_volume. */
+SFG_API int sfg_model_volume(void* model, double* volume);
+/* CUDA stream the model's kernels run on (cudaStream_t), for event timing. */
+SFG_API void* sfg_model_stream(void* model);
+
+/* ---- ensembles: many uneven models advanced by the same launches -------------------- */
+SFG_API void* sfg_ensemble_create(const char* const* model_dirs, int n, int bmi, char* err, int errlen);
+SFG_API void sfg_ensemble_destroy(void* ens);
+/* Run every member to its own t_end[i] (per-member dt); steps issued in CUDA
+ * graphs of `chunk` steps, host checks completion once per chunk. */
+SFG_API int sfg_ensemble_run(void* ens, const double* t_end, long long max_steps, int chunk);
+SFG_API int sfg_ensemble_issue(void* ens, int nsteps);
+SFG_API int sfg_ensemble_sync(void* ens);
+SFG_API int sfg_ensemble_scalars(void* ens, int member, double out[19]);
+SFG_API int sfg_ensemble_get(void* ens, int member, const char* name, void* dst, size_t bytes);
+SFG_API void* sfg_ensemble_stream(void* ens);
+
+/* ---- diagnostics: host-side layout of a model, no device work -------------------------- */
+/* Loads <model_dir> on the host only and copies one layout array (compact
+ * reference cell order) into dst: "counts" (double[8]: np, npuv, ngbnd,
+ * nkcuv2, nlevels, nalloc, dtmax, dtmin), "flags" (double[np]), "zs" and
+ * "zvol" (initial state, double[np]), "zbmx","gn2" (double[2*np]: u then v
+ * face of each cell), "gb_cell" (double[ngbnd], compact index), "gb_fac",
+ * "kb_cell","kb_dir","kb_sign" (double[nkcuv2]).  Returns 0 or -1. */
+SFG_API int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SFINCS_BMI_H */

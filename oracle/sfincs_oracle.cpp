@@ -1,0 +1,2074 @@
+// SFINCS time-stepping oracle: a CPU restatement of the reference's hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library links, loads or
+// calls this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
+// baseline leg use it, as the checker.
+//
+// Parity status: UNPINNED against reference outputs.  The reference (Fortran 90
+// + netcdf-fortran) cannot be compiled in this image (no Fortran compiler, no
+// netCDF-C library) and ships no tests or golden vectors; this restatement is
+// pinned by analytic invariants and hand-derived single-step known answers in
+// tests/ instead.
+//
+// The code mirrors the reference routine by routine, with 1-based arrays so the
+// index arithmetic reads like the Fortran.  Every function names the reference
+// lines it restates (paths relative to the SFINCS source tree).
+//
+// Precision is a template parameter: T for the reference's real*4 quantities,
+// TZ for zs (real*8 in the reference), TV for z_volume (real*8).  Three
+// instantiations are exported: "fp64" (everything double), "ref" (the
+// reference's own mixed precision) and "f32" (the CUDA core's precision: zs in
+// float, z_volume in double).  Build with -ffp-contract=off so float
+// expressions round exactly as written.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ncread.h"
+
+namespace orc {
+
+template <class X>
+struct F1 {  // 1-based Fortran-style vector
+  std::vector<X> v;
+  void alloc(long n, X init = X(0)) { v.assign((size_t)n + 1, init); }
+  X& operator()(long i) { return v[(size_t)i]; }
+  const X& operator()(long i) const { return v[(size_t)i]; }
+  long size() const { return v.empty() ? 0 : (long)v.size() - 1; }
+  bool allocated() const { return !v.empty(); }
+  void fill(X x) { std::fill(v.begin() + (v.empty() ? 0 : 1), v.end(), x); }
+};
+
+template <class X>
+struct F2 {  // (n1, n2) column-major, 1-based
+  std::vector<X> v;
+  long n1 = 0, n2 = 0;
+  void alloc(long a, long b, X init = X(0)) { n1 = a; n2 = b; v.assign((size_t)a * b, init); }
+  X& operator()(long i, long j) { return v[(size_t)(j - 1) * n1 + (i - 1)]; }
+};
+
+// ----------------------------------------------------------------- sfincs.inp
+// read_line / read_*_input: sfincs_read.f90:5-249.
+struct InpFile {
+  std::vector<std::pair<std::string, std::string>> kv;
+  explicit InpFile(const std::string& path) {
+    std::ifstream f(path);
+    if (!f) throw std::runtime_error("cannot open " + path);
+    std::string line0;
+    while (std::getline(f, line0)) {
+      // notabs: tab stops every 8 columns (sfincs_read.f90:252-300)
+      std::string line;
+      for (char c : line0) {
+        if (c == '\t') {
+          size_t ip = line.size() + 1;
+          ip = ip + (8 - ((ip - 1) % 8));
+          line.resize(ip - 1, ' ');
+        } else {
+          line.push_back(c);
+        }
+      }
+      size_t jn = line.find('\r');
+      if (jn != std::string::npos) line = line.substr(0, jn);
+      if (line.empty()) continue;
+      if (line[0] == '#' || line[0] == '!' || line[0] == '@') continue;
+      size_t j = line.find('=');
+      if (j == std::string::npos) continue;
+      std::string key = line.substr(0, j);
+      while (!key.empty() && key.back() == ' ') key.pop_back();
+      std::string val = line.substr(j + 1);
+      size_t h = val.find('#');
+      if (h != std::string::npos) val = val.substr(0, h);
+      size_t a = val.find_first_not_of(' ');
+      val = (a == std::string::npos) ? std::string() : val.substr(a);
+      while (!val.empty() && val.back() == ' ') val.pop_back();
+      kv.emplace_back(key, val);
+    }
+  }
+  const std::string* find(const std::string& key) const {
+    for (auto& p : kv)
+      if (p.first == key) return &p.second;
+    return nullptr;
+  }
+  float real(const std::string& k, float def) const {
+    auto s = find(k);
+    return s ? (float)std::strtod(s->c_str(), nullptr) : def;
+  }
+  int integer(const std::string& k, int def) const {
+    auto s = find(k);
+    return s ? (int)std::strtol(s->c_str(), nullptr, 10) : def;
+  }
+  std::string str(const std::string& k, const std::string& def) const {
+    auto s = find(k);
+    return s ? *s : def;
+  }
+  bool logical(const std::string& k, bool def) const {
+    auto s = find(k);
+    if (!s) return def;
+    char c = s->empty() ? ' ' : (*s)[0];
+    return c == '1' || c == 'y' || c == 'Y' || c == 't' || c == 'T';
+  }
+};
+
+// julian_date / time_difference: sfincs_date.f90:183-215
+static long julian_date(long y, long m, long d) {
+  return d - 32075 + 1461 * (y + 4800 + (m - 14) / 12) / 4 + 367 * (m - 2 - ((m - 14) / 12) * 12) / 12 -
+         3 * ((y + 4900 + (m - 14) / 12) / 100) / 4;
+}
+static long time_difference(const std::string& a, const std::string& b) {
+  auto parse = [](const std::string& s, long v[6]) {
+    auto num = [&](size_t p, size_t n) { return std::strtol(s.substr(p, n).c_str(), nullptr, 10); };
+    v[0] = num(0, 4); v[1] = num(4, 2); v[2] = num(6, 2); v[3] = num(9, 2); v[4] = num(11, 2); v[5] = num(13, 2);
+  };
+  long x[6], y[6];
+  parse(a, x);
+  parse(b, y);
+  long j1 = julian_date(x[0], x[1], x[2]), j2 = julian_date(y[0], y[1], y[2]);
+  return (j2 - j1) * 86400 + (y[3] * 3600 + y[4] * 60 + y[5]) - (x[3] * 3600 + x[4] * 60 + x[5]);
+}
+
+static std::vector<std::vector<double>> read_ascii_table(const std::string& path) {
+  std::ifstream f(path);
+  if (!f) throw std::runtime_error("cannot open " + path);
+  std::vector<std::vector<double>> rows;
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream is(line);
+    std::vector<double> r;
+    double x;
+    while (is >> x) r.push_back(x);
+    if (!r.empty()) rows.push_back(r);
+  }
+  return rows;
+}
+
+template <class X>
+static std::vector<X> read_stream(const std::string& path, size_t n, size_t offset_bytes = 0) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw std::runtime_error("cannot open " + path);
+  f.seekg((std::streamoff)offset_bytes);
+  std::vector<X> out(n);
+  f.read(reinterpret_cast<char*>(out.data()), (std::streamsize)(n * sizeof(X)));
+  if (!f) throw std::runtime_error("short read " + path);
+  return out;
+}
+
+// -------------------------------------------------------------------- model
+template <class T, class TZ, class TV>
+struct Model {
+  std::string dir;
+  std::string path(const std::string& f) const { return dir + "/" + f; }
+
+  // --- inputs and switches (sfincs_input.f90:50-343, derived :347-745)
+  int mmax, nmax;
+  float dx, dy, x0, y0, rotation;
+  std::string trefstr, tstartstr, tstopstr;
+  float tspinup, alfa, theta, hmin_cfl, manning, manning_land, manning_sea, rghlevland, zini, qinf, dtmax,
+      huthresh, huvmin, rhoa, rhow, latitude, pavbnd, gapres, advlim, slopelim, qinf_zmin, btfilter, btrelax,
+      nuviscdim, wiggle_factor, wiggle_threshold, uvlim, uvmax, nuviscfac, dtmaxout;
+  int bndtype, iadvection, baro, storevelmax, storefluxmax, storetwet, storetzsmax;
+  std::string inputtype, advstr, qtrfile, depfile, zsinifile, rstfile, mskfile, indexfile, sbgfile, manningfile,
+      bndfile, bzsfile, bcafile, bzifile, srcfile, disfile, wndfile, prcpfile, qinffile, scsfile, sefffile,
+      psifile, f0file, infiltrationfile, inftype;
+  bool coriolis, viscosity, friction2d, advection_mask, wiggle_suppression, h73table, spinup_meteo;
+  float t0, t1, g, pi, fcorio, twet_threshold;
+  bool crsgeo = false, advection, thetasmoothing, subgrid, store_maximum_waterlevel, store_maximum_velocity,
+       store_maximum_flux, store_twet, store_t_zsmax, use_quadtree, wind, precip, patmos, infiltration,
+       use_qext, store_cumulative_precipitation = false;
+  int advection_scheme = 1;
+
+  // --- quadtree (sfincs_quadtree.F90:8-48)
+  long qt_np;
+  int qt_nlev;
+  float qt_x0, qt_y0, qt_dx, qt_dy, qt_rot;
+  int qt_nmax, qt_mmax;
+  F1<int8_t> qt_level, qt_md, qt_mu, qt_nd, qt_nu;
+  F1<int32_t> qt_md1, qt_md2, qt_mu1, qt_mu2, qt_nd1, qt_nd2, qt_nu1, qt_nu2, qt_n, qt_m, qt_nm_indices,
+      qt_first, qt_last;
+  F1<float> qt_dxr, qt_dyr;
+  float qt_cosrot, qt_sinrot;
+
+  // --- mesh (sfincs_data.f90)
+  long np, npuv, ncuv;
+  int nref;
+  F1<int8_t> kcs, kcuv, kfuv, uv_flags_iref, uv_flags_type, uv_flags_dir, z_flags_iref, mask_adv;
+  F1<int32_t> index_sfincs_in_quadtree, index_quadtree_in_sfincs, z_index_z_n, z_index_z_m, z_index_uv_md,
+      z_index_uv_mu, z_index_uv_nd, z_index_uv_nu, z_index_uv_md1, z_index_uv_md2, z_index_uv_mu1, z_index_uv_mu2,
+      z_index_uv_nd1, z_index_uv_nd2, z_index_uv_nu1, z_index_uv_nu2, uv_index_z_nm, uv_index_z_nmu,
+      uv_index_u_nmd, uv_index_u_nmu, uv_index_u_ndm, uv_index_u_num, uv_index_v_ndm, uv_index_v_nm,
+      uv_index_v_ndmu, uv_index_v_nmu, cuv_index_uv, cuv_index_uv1, cuv_index_uv2;
+  F1<float> dxr, dyr, dxyr, z_xz, z_yz, dxrm, dxrinv, dxr2inv, dxrinvc, dyrm, dyrinv, dyr2inv, dyrinvc, cell_area,
+      nuvisc;
+  float dtmin, cosrot, sinrot;
+
+  // --- bathymetry / subgrid
+  F1<float> zb, zbuv, zbuvmx, gn2uv;
+  int subgrid_nlevels = 0;
+  F1<float> sg_z_zmin, sg_z_zmax, sg_z_volmax, sg_uv_zmin, sg_uv_zmax, sg_uv_navg_w, sg_uv_fnfit, sg_uv_havg_zmax,
+      sg_uv_nrep_zmax;
+  F2<float> sg_z_dep, sg_uv_havg, sg_uv_nrep, sg_uv_pwet;
+
+  // --- boundaries
+  long ngbnd = 0, nkcuv2 = 0, nbnd = 0, ntbnd = 0, itbndlast = 1;
+  bool boundaries_in_mask = false, water_level_boundaries_in_mask = false, outflow_boundaries_in_mask = false,
+       downstream_river_boundaries_in_mask = false, neumann_boundaries_in_mask = false;
+  F1<int32_t> nmindbnd, index_kcuv2, nmbkcuv2, nmikcuv2, ibkcuv2, ind1_bnd_gbp, ind2_bnd_gbp, nmi_gbp;
+  F1<int8_t> ibuvdir;
+  F1<float> zsb, zsb0, uvmean, fac_bnd_gbp, x_bnd, y_bnd, t_bnd, zst_bnd;
+  F2<float> zs_bnd;
+
+  // --- meteo, infiltration, sources
+  long ntwnd = 0, itwndlast = 1, ntprcp = 0, itprcplast = 1;
+  F1<float> twnd, wndmag, wnddir, tprcpt, tprcpv, cdval;
+  F1<float> tauwu, tauwv, prcp, netprcp, qext, qinffield, qinfmap, cumprcp, cuminf;
+  long nsrc = 0, ntsrc = 0, itsrclast = 1;
+  F1<int32_t> nmindsrc;
+  F1<float> tsrc, qtsrc;
+  F2<float> qsrc;
+
+  // --- hydro state
+  F1<TZ> zs;
+  F1<TV> z_volume;
+  F1<T> q, q0, uv, uv0, zs0, zsderv, zsmax, vmax, qmax, twet;
+  F1<float> t_zsmax;
+  F1<T> x73;  // unused unless h73table (power7over3, sfincs_momentum.f90:787-820)
+
+  // --- time loop
+  double t;
+  float dt, min_dt, dtavg;
+  long nt = 0;
+  int error = 0;
+
+  // ================================================================ init
+  void read_sfincs_input() {  // sfincs_input.f90:5-747 (hot-path keywords)
+    InpFile in(path("sfincs.inp"));
+    mmax = in.integer("mmax", 0);
+    nmax = in.integer("nmax", 0);
+    dx = in.real("dx", 0.0f);
+    dy = in.real("dy", 0.0f);
+    x0 = in.real("x0", 0.0f);
+    y0 = in.real("y0", 0.0f);
+    rotation = in.real("rotation", 0.0f);
+    trefstr = in.str("tref", "none");
+    tstartstr = in.str("tstart", "20000101 000000");
+    tstopstr = in.str("tstop", "20000101 000000");
+    tspinup = in.real("tspinup", 0.0f);
+    dtmaxout = in.real("dtmaxout", 9999999.0f);
+    alfa = in.real("alpha", 0.50f);
+    theta = in.real("theta", 1.0f);
+    hmin_cfl = in.real("hmin_cfl", 0.1f);
+    manning = in.real("manning", 0.04f);
+    manning_land = in.real("manning_land", -999.0f);
+    manning_sea = in.real("manning_sea", -999.0f);
+    rghlevland = in.real("rgh_lev_land", 0.0f);
+    zini = in.real("zsini", 0.0f);
+    qinf = in.real("qinf", 0.0f);
+    dtmax = in.real("dtmax", 60.0f);
+    huthresh = in.real("huthresh", 0.05f);
+    huvmin = in.real("huvmin", 0.0f);
+    rhoa = in.real("rhoa", 1.25f);
+    rhow = in.real("rhow", 1024.0f);
+    inputtype = in.str("inputformat", "bin");
+    bndtype = in.integer("bndtype", 1);
+    iadvection = in.integer("advection", 1);
+    latitude = in.real("latitude", 0.0f);
+    pavbnd = in.real("pavbnd", 0.0f);
+    gapres = in.real("gapres", 101200.0f);
+    baro = in.integer("baro", 1);
+    advlim = in.real("advlim", 1.0f);
+    slopelim = in.real("slopelim", 9999.9f);
+    qinf_zmin = in.real("qinf_zmin", 0.0f);
+    btfilter = in.real("btfilter", 60.0f);
+    coriolis = in.logical("coriolis", true);
+    nuviscdim = in.real("nuvisc", 0.01f);
+    viscosity = in.logical("viscosity", false);
+    spinup_meteo = in.integer("spinup_meteo", 0) != 0;
+    advstr = in.str("advection_scheme", "upw1");
+    btrelax = in.real("btrelax", 3600.0f);
+    wiggle_suppression = in.logical("wiggle_suppression", true);
+    wiggle_factor = in.real("wiggle_factor", 0.1f);
+    wiggle_threshold = in.real("wiggle_threshold", 0.1f);
+    uvlim = in.real("uvlim", 10.0f);
+    uvmax = in.real("uvmax", 1000.0f);
+    friction2d = in.logical("friction2d", true);
+    advection_mask = in.logical("advection_mask", true);
+    nuviscfac = in.real("nuviscfac", 100.0f);
+    h73table = in.logical("h73table", false);
+    qtrfile = in.str("qtrfile", "none");
+    depfile = in.str("depfile", "none");
+    zsinifile = in.str("inifile", "none");
+    rstfile = in.str("rstfile", "none");
+    mskfile = in.str("mskfile", "none");
+    indexfile = in.str("indexfile", "none");
+    sbgfile = in.str("sbgfile", "none");
+    manningfile = in.str("manningfile", "none");
+    bndfile = in.str("bndfile", "none");
+    bzsfile = in.str("bzsfile", "none");
+    bcafile = in.str("bcafile", "none");
+    bzifile = in.str("bzifile", "none");
+    srcfile = in.str("srcfile", "none");
+    disfile = in.str("disfile", "none");
+    wndfile = in.str("wndfile", "none");
+    prcpfile = in.str("prcfile", "none");
+    if (prcpfile.substr(0, 4) == "none") prcpfile = in.str("precipfile", "none");
+    qinffile = in.str("qinffile", "none");
+    scsfile = in.str("scsfile", "none");
+    sefffile = in.str("sefffile", "none");
+    psifile = in.str("psifile", "none");
+    f0file = in.str("f0file", "none");
+    infiltrationfile = in.str("infiltration_file", "none");
+    inftype = in.str("infiltration_type", "none");
+    storevelmax = in.integer("storevelmax", 0);
+    storefluxmax = in.integer("storefluxmax", 0);
+    storetwet = in.integer("storetwet", 0);
+    storetzsmax = in.integer("storetzsmax", 0);
+    twet_threshold = in.real("twet_threshold", 0.01f);
+    int igeo = in.integer("crsgeo", 0);
+    if (trefstr.substr(0, 4) == "none") trefstr = tstartstr;
+    t0 = (float)(time_difference(trefstr, tstartstr) * 1.0);
+    t1 = (float)(time_difference(trefstr, tstopstr) * 1.0);
+    tspinup = t0 + tspinup;
+    g = 9.81f;
+    pi = 3.14159f;
+    qinf = qinf / (float)(3600 * 1000);
+    rotation = rotation * pi / 180.0f;
+    cosrot = std::cos(rotation);
+    sinrot = std::sin(rotation);
+    fcorio = 0.0f;
+    if (igeo != 0) throw std::runtime_error("oracle: geographic grids are not part of this path");
+    crsgeo = false;
+    fcorio = 2.0f * 7.2921e-05f * std::sin(latitude * pi / 180.0f);
+    if (latitude < 0.01f && latitude > -0.01f) coriolis = false;
+    store_maximum_waterlevel = dtmaxout > 0.0f;
+    store_maximum_velocity = storevelmax == 1 && dtmaxout > 0.0f;
+    store_maximum_flux = storefluxmax == 1 && dtmaxout > 0.0f;
+    store_twet = storetwet == 1;
+    store_t_zsmax = storetzsmax == 1;
+    subgrid = sbgfile.substr(0, 4) != "none";
+    advection = iadvection > 0;
+    thetasmoothing = theta < 0.9999f;
+    if (advection) {
+      advection_scheme = 1;
+      if (advstr == "original") advection_scheme = 0;
+    }
+  }
+
+  // initialize_processes: sfincs_domain.f90:59-140 (time-series meteo only)
+  void initialize_processes() {
+    use_quadtree = qtrfile.substr(0, 4) != "none";
+    wind = wndfile.substr(0, 4) != "none";
+    precip = prcpfile.substr(0, 4) != "none";
+    patmos = false;
+  }
+
+  // make_quadtree_from_indices: sfincs_quadtree.F90:445-669
+  void make_quadtree_from_indices(long n_act, const std::vector<int32_t>& indices) {
+    std::vector<int32_t> vm(n_act + 1), vn(n_act + 1), vnmu(n_act + 1, 0), vnmd(n_act + 1, 0), vnum(n_act + 1, 0),
+        vndm(n_act + 1, 0);
+    std::vector<int32_t> g((size_t)nmax * mmax, 0);
+    auto G = [&](long n, long m) -> int32_t& { return g[(size_t)(m - 1) * nmax + (n - 1)]; };
+    for (long nm = 1; nm <= n_act; nm++) {
+      long m = (indices[nm - 1] - 1) / nmax + 1;
+      long n = indices[nm - 1] - (m - 1) * nmax;
+      vm[nm] = (int32_t)m;
+      vn[nm] = (int32_t)n;
+      G(n, m) = (int32_t)nm;
+    }
+    for (long nm = 1; nm <= n_act; nm++) {
+      long m = vm[nm], n = vn[nm];
+      if (m < mmax) vnmu[nm] = G(n, m + 1);
+      if (m > 1) vnmd[nm] = G(n, m - 1);
+      if (n < nmax) vnum[nm] = G(n + 1, m);
+      if (n > 1) vndm[nm] = G(n - 1, m);
+    }
+    qt_np = n_act;
+    qt_nlev = 1;
+    qt_nmax = nmax;
+    qt_mmax = mmax;
+    qt_x0 = x0;
+    qt_y0 = y0;
+    qt_dx = dx;
+    qt_dy = dy;
+    qt_rot = rotation;
+    qt_cosrot = std::cos(qt_rot);
+    qt_sinrot = std::sin(qt_rot);
+    qt_dxr.alloc(1);
+    qt_dyr.alloc(1);
+    qt_dxr(1) = dx;
+    qt_dyr(1) = dy;
+    qt_level.alloc(n_act, 1);
+    qt_md.alloc(n_act); qt_mu.alloc(n_act); qt_nd.alloc(n_act); qt_nu.alloc(n_act);
+    qt_md1.alloc(n_act); qt_md2.alloc(n_act); qt_mu1.alloc(n_act); qt_mu2.alloc(n_act);
+    qt_nd1.alloc(n_act); qt_nd2.alloc(n_act); qt_nu1.alloc(n_act); qt_nu2.alloc(n_act);
+    qt_n.alloc(n_act); qt_m.alloc(n_act);
+    for (long ip = 1; ip <= n_act; ip++) {
+      qt_md1(ip) = vnmd[ip];
+      qt_mu1(ip) = vnmu[ip];
+      qt_nd1(ip) = vndm[ip];
+      qt_nu1(ip) = vnum[ip];
+      qt_n(ip) = vn[ip];
+      qt_m(ip) = vm[ip];
+    }
+    build_qt_search();
+  }
+
+  void build_qt_search() {  // sfincs_quadtree.F90:154-186, 637-667
+    qt_nm_indices.alloc(qt_np);
+    qt_first.alloc(qt_nlev);
+    qt_last.alloc(qt_nlev);
+    int ireflast = 0;
+    for (long ip = 1; ip <= qt_np; ip++) {
+      int iref = qt_level(ip);
+      long nmx = (long)qt_nmax << (iref - 1);
+      qt_nm_indices(ip) = (int32_t)((qt_m(ip) - 1) * nmx + qt_n(ip));
+      if (iref > ireflast) {
+        qt_first(iref) = (int32_t)ip;
+        ireflast = iref;
+      }
+      qt_last(iref) = (int32_t)ip;
+    }
+  }
+
+  // initialize_mesh: sfincs_domain.f90:143-1586
+  void initialize_mesh() {
+    std::vector<int8_t> mskq;
+    if (use_quadtree) throw std::runtime_error("oracle: quadtree files are read in a later build step");
+    if (inputtype != "bin") throw std::runtime_error("oracle: only inputformat=bin is restated");
+    {
+      auto head = read_stream<int32_t>(path(indexfile), 1);
+      long n_act = head[0];
+      auto idx = read_stream<int32_t>(path(indexfile), (size_t)n_act, 4);
+      make_quadtree_from_indices(n_act, idx);
+      mskq = read_stream<int8_t>(path(mskfile), (size_t)n_act);
+    }
+    rotation = qt_rot;
+    nref = qt_nlev;
+    // count and remap active points (:327-482)
+    index_sfincs_in_quadtree.alloc(qt_np);
+    np = 0;
+    for (long ip = 1; ip <= qt_np; ip++)
+      if (mskq[ip - 1] > 0) np++;
+    kcs.alloc(np);
+    index_quadtree_in_sfincs.alloc(np);
+    z_flags_iref.alloc(np);
+    F1<int8_t> z_flags_md, z_flags_mu, z_flags_nd, z_flags_nu;
+    F1<int32_t> z_index_z_md1, z_index_z_md2, z_index_z_mu1, z_index_z_mu2, z_index_z_nd1, z_index_z_nd2,
+        z_index_z_nu1, z_index_z_nu2, z_index_cuv_md, z_index_cuv_mu, z_index_cuv_nd, z_index_cuv_nu;
+    z_flags_md.alloc(np); z_flags_mu.alloc(np); z_flags_nd.alloc(np); z_flags_nu.alloc(np);
+    z_index_z_md1.alloc(np); z_index_z_md2.alloc(np); z_index_z_mu1.alloc(np); z_index_z_mu2.alloc(np);
+    z_index_z_nd1.alloc(np); z_index_z_nd2.alloc(np); z_index_z_nu1.alloc(np); z_index_z_nu2.alloc(np);
+    z_index_z_n.alloc(np); z_index_z_m.alloc(np);
+    z_index_uv_md1.alloc(np); z_index_uv_md2.alloc(np); z_index_uv_mu1.alloc(np); z_index_uv_mu2.alloc(np);
+    z_index_uv_nd1.alloc(np); z_index_uv_nd2.alloc(np); z_index_uv_nu1.alloc(np); z_index_uv_nu2.alloc(np);
+    z_index_uv_md.alloc(np); z_index_uv_mu.alloc(np); z_index_uv_nd.alloc(np); z_index_uv_nu.alloc(np);
+    z_index_cuv_md.alloc(np); z_index_cuv_mu.alloc(np); z_index_cuv_nd.alloc(np); z_index_cuv_nu.alloc(np);
+    np = 0;
+    for (long ip = 1; ip <= qt_np; ip++) {
+      if (mskq[ip - 1] > 0) {
+        np++;
+        index_sfincs_in_quadtree(ip) = (int32_t)np;
+        index_quadtree_in_sfincs(np) = (int32_t)ip;
+      }
+    }
+    for (long ip = 1; ip <= np; ip++) {
+      long iq = index_quadtree_in_sfincs(ip);
+      kcs(ip) = mskq[iq - 1];
+      z_flags_iref(ip) = qt_level(iq);
+      z_index_z_n(ip) = qt_n(iq);
+      z_index_z_m(ip) = qt_m(iq);
+      z_flags_nu(ip) = qt_nu(iq);
+      z_flags_nd(ip) = qt_nd(iq);
+      z_flags_mu(ip) = qt_mu(iq);
+      z_flags_md(ip) = qt_md(iq);
+      if (qt_nu1(iq) > 0) z_index_z_nu1(ip) = index_sfincs_in_quadtree(qt_nu1(iq));
+      if (qt_nu2(iq) > 0) z_index_z_nu2(ip) = index_sfincs_in_quadtree(qt_nu2(iq));
+      if (qt_nd1(iq) > 0) z_index_z_nd1(ip) = index_sfincs_in_quadtree(qt_nd1(iq));
+      if (qt_nd2(iq) > 0) z_index_z_nd2(ip) = index_sfincs_in_quadtree(qt_nd2(iq));
+      if (qt_mu1(iq) > 0) z_index_z_mu1(ip) = index_sfincs_in_quadtree(qt_mu1(iq));
+      if (qt_mu2(iq) > 0) z_index_z_mu2(ip) = index_sfincs_in_quadtree(qt_mu2(iq));
+      if (qt_md1(iq) > 0) z_index_z_md1(ip) = index_sfincs_in_quadtree(qt_md1(iq));
+      if (qt_md2(iq) > 0) z_index_z_md2(ip) = index_sfincs_in_quadtree(qt_md2(iq));
+    }
+    // count u and v points (:486-533)
+    long npu = 0, npv = 0;
+    for (long nm = 1; nm <= np; nm++) {
+      if (z_flags_mu(nm) < 1) {
+        if (z_index_z_mu1(nm) > 0) npu++;
+      } else {
+        if (z_index_z_mu1(nm) > 0) npu++;
+        if (z_index_z_mu2(nm) > 0) npu++;
+      }
+      if (z_flags_nu(nm) < 1) {
+        if (z_index_z_nu1(nm) > 0) npv++;
+      } else {
+        if (z_index_z_nu1(nm) > 0) npv++;
+        if (z_index_z_nu2(nm) > 0) npv++;
+      }
+    }
+    npuv = npu + npv;
+    ncuv = 0;
+    if (qt_nlev > 1) {  // :537-596
+      for (long nm = 1; nm <= np; nm++) {
+        if (z_flags_md(nm) == 1 && (z_index_z_md1(nm) > 0 || z_index_z_md2(nm) > 0)) ncuv++;
+        if (z_flags_mu(nm) == 1 && (z_index_z_mu1(nm) > 0 || z_index_z_mu2(nm) > 0)) ncuv++;
+        if (z_flags_nd(nm) == 1 && (z_index_z_nd1(nm) > 0 || z_index_z_nd2(nm) > 0)) ncuv++;
+        if (z_flags_nu(nm) == 1 && (z_index_z_nu1(nm) > 0 || z_index_z_nu2(nm) > 0)) ncuv++;
+      }
+    }
+    long npuvtotal = npuv + ncuv;
+    z_index_uv_md.fill((int32_t)(npuvtotal + 1));
+    z_index_uv_mu.fill((int32_t)(npuvtotal + 1));
+    z_index_uv_nd.fill((int32_t)(npuvtotal + 1));
+    z_index_uv_nu.fill((int32_t)(npuvtotal + 1));
+    cuv_index_uv.alloc(ncuv);
+    cuv_index_uv1.alloc(ncuv, (int32_t)(npuvtotal + 1));
+    cuv_index_uv2.alloc(ncuv, (int32_t)(npuvtotal + 1));
+    long irefuv = 0;  // :618-678
+    for (long nm = 1; nm <= np; nm++) {
+      if (z_flags_md(nm) == 1 && (z_index_z_md1(nm) > 0 || z_index_z_md2(nm) > 0)) {
+        irefuv++;
+        cuv_index_uv(irefuv) = (int32_t)(npuv + irefuv);
+        z_index_cuv_md(nm) = (int32_t)irefuv;
+      }
+      if (z_flags_mu(nm) == 1 && (z_index_z_mu1(nm) > 0 || z_index_z_mu2(nm) > 0)) {
+        irefuv++;
+        cuv_index_uv(irefuv) = (int32_t)(npuv + irefuv);
+        z_index_cuv_mu(nm) = (int32_t)irefuv;
+      }
+      if (z_flags_nd(nm) == 1 && (z_index_z_nd1(nm) > 0 || z_index_z_nd2(nm) > 0)) {
+        irefuv++;
+        cuv_index_uv(irefuv) = (int32_t)(npuv + irefuv);
+        z_index_cuv_nd(nm) = (int32_t)irefuv;
+      }
+      if (z_flags_nu(nm) == 1 && (z_index_z_nu1(nm) > 0 || z_index_z_nu2(nm) > 0)) {
+        irefuv++;
+        cuv_index_uv(irefuv) = (int32_t)(npuv + irefuv);
+        z_index_cuv_nu(nm) = (int32_t)irefuv;
+      }
+    }
+    kcuv.alloc(npuv + ncuv + 1);
+    uv_index_z_nm.alloc(npuv);
+    uv_index_z_nmu.alloc(npuv);
+    uv_flags_iref.alloc(npuv);
+    uv_flags_dir.alloc(npuv);
+    uv_flags_type.alloc(npuv);
+    bool need8 = advection || coriolis || viscosity || thetasmoothing || friction2d;
+    if (need8) {
+      uv_index_u_nmd.alloc(npuv); uv_index_u_nmu.alloc(npuv); uv_index_u_num.alloc(npuv);
+      uv_index_u_ndm.alloc(npuv); uv_index_v_ndm.alloc(npuv); uv_index_v_nm.alloc(npuv);
+      uv_index_v_ndmu.alloc(npuv); uv_index_v_nmu.alloc(npuv);
+    }
+    long ip = 0;  // uv enumeration :721-1003
+    for (long nm = 1; nm <= np; nm++) {
+      long nmu, num, icuv;
+      if (z_flags_mu(nm) == 0) {
+        if (z_index_z_mu1(nm) > 0) {
+          ip++;
+          nmu = z_index_z_mu1(nm);
+          uv_index_z_nm(ip) = (int32_t)nm;
+          uv_index_z_nmu(ip) = (int32_t)nmu;
+          z_index_uv_mu(nm) = (int32_t)ip;
+          z_index_uv_md(nmu) = (int32_t)ip;
+          z_index_uv_mu1(nm) = (int32_t)ip;
+          z_index_uv_md1(nmu) = (int32_t)ip;
+          uv_flags_iref(ip) = z_flags_iref(nm);
+          uv_flags_dir(ip) = 0;
+          uv_flags_type(ip) = 0;
+        }
+      } else if (z_flags_mu(nm) == -1) {
+        if (z_index_z_mu1(nm) > 0) {
+          ip++;
+          nmu = z_index_z_mu1(nm);
+          uv_index_z_nm(ip) = (int32_t)nm;
+          uv_index_z_nmu(ip) = (int32_t)nmu;
+          z_index_uv_mu(nm) = (int32_t)ip;
+          z_index_uv_mu1(nm) = (int32_t)ip;
+          icuv = z_index_cuv_md(nmu);
+          if (z_index_z_md1(z_index_z_mu1(nm)) == nm) {
+            cuv_index_uv1(icuv) = (int32_t)ip;
+            z_index_uv_md1(nmu) = (int32_t)ip;
+          } else {
+            cuv_index_uv2(icuv) = (int32_t)ip;
+            z_index_uv_md2(nmu) = (int32_t)ip;
+          }
+          z_index_uv_md(nmu) = cuv_index_uv(icuv);
+          uv_flags_iref(ip) = z_flags_iref(nm);
+          uv_flags_dir(ip) = 0;
+          uv_flags_type(ip) = -1;
+        }
+      } else {
+        if (z_index_z_mu1(nm) > 0) {
+          ip++;
+          nmu = z_index_z_mu1(nm);
+          uv_index_z_nm(ip) = (int32_t)nm;
+          uv_index_z_nmu(ip) = (int32_t)nmu;
+          z_index_uv_mu1(nm) = (int32_t)ip;
+          z_index_uv_md(nmu) = (int32_t)ip;
+          z_index_uv_md1(nmu) = (int32_t)ip;
+          icuv = z_index_cuv_mu(nm);
+          z_index_uv_mu(nm) = cuv_index_uv(icuv);
+          cuv_index_uv1(icuv) = (int32_t)ip;
+          uv_flags_iref(ip) = (int8_t)(z_flags_iref(nm) + 1);
+          uv_flags_dir(ip) = 0;
+          uv_flags_type(ip) = 1;
+        }
+        if (z_index_z_mu2(nm) > 0) {
+          ip++;
+          nmu = z_index_z_mu2(nm);
+          uv_index_z_nm(ip) = (int32_t)nm;
+          uv_index_z_nmu(ip) = (int32_t)nmu;
+          z_index_uv_mu2(nm) = (int32_t)ip;
+          z_index_uv_md(nmu) = (int32_t)ip;
+          z_index_uv_md1(nmu) = (int32_t)ip;
+          icuv = z_index_cuv_mu(nm);
+          z_index_uv_mu(nm) = cuv_index_uv(icuv);
+          cuv_index_uv2(icuv) = (int32_t)ip;
+          uv_flags_iref(ip) = (int8_t)(z_flags_iref(nm) + 1);
+          uv_flags_dir(ip) = 0;
+          uv_flags_type(ip) = 1;
+        }
+      }
+      if (z_flags_nu(nm) == 0) {
+        if (z_index_z_nu1(nm) > 0) {
+          ip++;
+          num = z_index_z_nu1(nm);
+          uv_index_z_nm(ip) = (int32_t)nm;
+          uv_index_z_nmu(ip) = (int32_t)num;
+          z_index_uv_nu(nm) = (int32_t)ip;
+          z_index_uv_nd(num) = (int32_t)ip;
+          z_index_uv_nu1(nm) = (int32_t)ip;
+          z_index_uv_nd1(num) = (int32_t)ip;
+          uv_flags_iref(ip) = z_flags_iref(nm);
+          uv_flags_dir(ip) = 1;
+          uv_flags_type(ip) = 0;
+        }
+      } else if (z_flags_nu(nm) == -1) {
+        if (z_index_z_nu1(nm) > 0) {
+          ip++;
+          num = z_index_z_nu1(nm);
+          uv_index_z_nm(ip) = (int32_t)nm;
+          uv_index_z_nmu(ip) = (int32_t)num;
+          z_index_uv_nu(nm) = (int32_t)ip;
+          z_index_uv_nu1(nm) = (int32_t)ip;
+          icuv = z_index_cuv_nd(num);
+          if (z_index_z_nd1(z_index_z_nu1(nm)) == nm) {
+            cuv_index_uv1(icuv) = (int32_t)ip;
+            z_index_uv_nd1(num) = (int32_t)ip;
+          } else {
+            cuv_index_uv2(icuv) = (int32_t)ip;
+            z_index_uv_nd2(num) = (int32_t)ip;
+          }
+          z_index_uv_nd(num) = cuv_index_uv(icuv);
+          uv_flags_iref(ip) = z_flags_iref(nm);
+          uv_flags_dir(ip) = 1;
+          uv_flags_type(ip) = -1;
+        }
+      } else {
+        if (z_index_z_nu1(nm) > 0) {
+          ip++;
+          num = z_index_z_nu1(nm);
+          uv_index_z_nm(ip) = (int32_t)nm;
+          uv_index_z_nmu(ip) = (int32_t)num;
+          z_index_uv_nd(num) = (int32_t)ip;
+          z_index_uv_nu1(nm) = (int32_t)ip;
+          z_index_uv_nd1(num) = (int32_t)ip;
+          icuv = z_index_cuv_nu(nm);
+          z_index_uv_nu(nm) = cuv_index_uv(icuv);
+          cuv_index_uv1(icuv) = (int32_t)ip;
+          uv_flags_iref(ip) = (int8_t)(z_flags_iref(nm) + 1);
+          uv_flags_dir(ip) = 1;
+          uv_flags_type(ip) = 1;
+        }
+        if (z_index_z_nu2(nm) > 0) {
+          ip++;
+          num = z_index_z_nu2(nm);
+          uv_index_z_nm(ip) = (int32_t)nm;
+          uv_index_z_nmu(ip) = (int32_t)num;
+          z_index_uv_nd(num) = (int32_t)ip;
+          z_index_uv_nu2(nm) = (int32_t)ip;
+          z_index_uv_nd1(num) = (int32_t)ip;
+          icuv = z_index_cuv_nu(nm);
+          z_index_uv_nu(nm) = cuv_index_uv(icuv);
+          cuv_index_uv2(icuv) = (int32_t)ip;
+          uv_flags_iref(ip) = (int8_t)(z_flags_iref(nm) + 1);
+          uv_flags_dir(ip) = 1;
+          uv_flags_type(ip) = 1;
+        }
+      }
+    }
+    if (need8) {  // 8 uv neighbours :1007-1261
+      for (long ip2 = 1; ip2 <= npuv; ip2++) {
+        long nm = uv_index_z_nm(ip2);
+        if (uv_flags_dir(ip2) == 0) {
+          long nmu = uv_index_z_nmu(ip2);
+          uv_index_u_nmd(ip2) = z_index_uv_md(nm);
+          uv_index_u_nmu(ip2) = z_index_uv_mu(nmu);
+          if (z_flags_nd(nm) > -1) {
+            long ndm = z_index_z_nd1(nm);
+            if (ndm > 0) uv_index_u_ndm(ip2) = z_index_uv_mu(ndm);
+          } else {
+            long ndm = z_index_z_nd2(nm);
+            if (ndm > 0) {
+              if (z_flags_mu(ndm) == 0) {
+                uv_index_u_ndm(ip2) = z_index_uv_mu(ndm);
+              } else {
+                long ndmu = z_index_z_mu1(ndm);
+                if (ndmu > 0) uv_index_u_ndm(ip2) = z_index_uv_md(ndmu);
+              }
+            }
+          }
+          if (z_flags_nu(nm) > -1) {
+            long num = z_index_z_nu1(nm);
+            if (num > 0) uv_index_u_num(ip2) = z_index_uv_mu(num);
+          } else {
+            long num = z_index_z_nu2(nm);
+            if (num > 0) {
+              if (z_flags_mu(num) == 0) {
+                uv_index_u_num(ip2) = z_index_uv_mu(num);
+              } else {
+                long numu = z_index_z_mu1(num);
+                if (numu > 0) uv_index_u_num(ip2) = z_index_uv_md(numu);
+              }
+            }
+          }
+          uv_index_v_nm(ip2) = z_index_uv_nu(nm);
+          uv_index_v_ndm(ip2) = z_index_uv_nd(nm);
+          uv_index_v_nmu(ip2) = z_index_uv_nu(nmu);
+          uv_index_v_ndmu(ip2) = z_index_uv_nd(nmu);
+        } else {
+          long num = uv_index_z_nmu(ip2);
+          uv_index_u_nmd(ip2) = z_index_uv_nd(nm);
+          uv_index_u_nmu(ip2) = z_index_uv_nu(num);
+          if (z_flags_md(nm) > -1) {
+            long nmd = z_index_z_md1(nm);
+            if (nmd > 0) uv_index_u_ndm(ip2) = z_index_uv_nu(nmd);
+          } else {
+            long nmd = z_index_z_md2(nm);
+            if (nmd > 0) {
+              if (z_flags_nu(nmd) == 0) {
+                uv_index_u_ndm(ip2) = z_index_uv_nu(nmd);
+              } else {
+                long nmdu = z_index_z_nu1(nmd);
+                if (nmdu > 0) uv_index_u_ndm(ip2) = z_index_uv_nd(nmdu);
+              }
+            }
+          }
+          if (z_flags_mu(nm) > -1) {
+            long nmu = z_index_z_mu1(nm);
+            if (nmu > 0) uv_index_u_num(ip2) = z_index_uv_nu(nmu);
+          } else {
+            long nmu = z_index_z_mu2(nm);
+            if (nmu > 0) {
+              if (z_flags_nu(nmu) == 0) {
+                uv_index_u_num(ip2) = z_index_uv_nu(nmu);
+              } else {
+                long numu = z_index_z_nu1(nmu);
+                if (numu > 0) uv_index_u_num(ip2) = z_index_uv_nd(numu);
+              }
+            }
+          }
+          uv_index_v_nm(ip2) = z_index_uv_mu(nm);
+          uv_index_v_ndm(ip2) = z_index_uv_md(nm);
+          uv_index_v_nmu(ip2) = z_index_uv_mu(num);
+          uv_index_v_ndmu(ip2) = z_index_uv_md(num);
+        }
+        if (uv_index_u_nmd(ip2) == 0) uv_index_u_nmd(ip2) = (int32_t)ip2;
+        if (uv_index_u_nmu(ip2) == 0) uv_index_u_nmu(ip2) = (int32_t)ip2;
+        if (uv_index_u_ndm(ip2) == 0) uv_index_u_ndm(ip2) = (int32_t)ip2;
+        if (uv_index_u_num(ip2) == 0) uv_index_u_num(ip2) = (int32_t)ip2;
+        if (uv_index_v_ndm(ip2) == 0) uv_index_v_ndm(ip2) = (int32_t)(npuvtotal + 1);
+        if (uv_index_v_ndmu(ip2) == 0) uv_index_v_ndmu(ip2) = (int32_t)(npuvtotal + 1);
+        if (uv_index_v_nm(ip2) == 0) uv_index_v_nm(ip2) = (int32_t)(npuvtotal + 1);
+        if (uv_index_v_nmu(ip2) == 0) uv_index_v_nmu(ip2) = (int32_t)(npuvtotal + 1);
+      }
+    }
+    // geometry :1369-1541 (projected)
+    dxr.alloc(nref); dyr.alloc(nref); dxyr.alloc(nref);
+    for (int iref = 1; iref <= nref; iref++) {
+      dxr(iref) = dx / (float)(1 << (iref - 1));
+      dyr(iref) = dy / (float)(1 << (iref - 1));
+      dxyr(iref) = std::min(dxr(iref), dyr(iref));
+    }
+    z_xz.alloc(np);
+    z_yz.alloc(np);
+    for (long nm = 1; nm <= np; nm++) {
+      float n = (float)z_index_z_n(nm), m = (float)z_index_z_m(nm);
+      int iref = z_flags_iref(nm);
+      z_xz(nm) = x0 + cosrot * (1.0f * (m - 0.5f)) * dxr(iref) - sinrot * (1.0f * (n - 0.5f)) * dyr(iref);
+      z_yz(nm) = y0 + sinrot * (1.0f * (m - 0.5f)) * dxr(iref) + cosrot * (1.0f * (n - 0.5f)) * dyr(iref);
+    }
+    float dxymin = 1.0e6f;
+    dxrm.alloc(nref); dxrinv.alloc(nref); dxr2inv.alloc(nref); dxrinvc.alloc(nref);
+    dyrm.alloc(nref); dyrinv.alloc(nref); dyr2inv.alloc(nref); dyrinvc.alloc(nref);
+    cell_area.alloc(nref);
+    for (int iref = 1; iref <= nref; iref++) {
+      dxrm(iref) = dxr(iref);
+      dxrinv(iref) = 1.0f / dxrm(iref);
+      dxr2inv(iref) = dxrinv(iref) * dxrinv(iref);
+      dyrm(iref) = dyr(iref);
+      dyrinv(iref) = 1.0f / dyrm(iref);
+      dyr2inv(iref) = dyrinv(iref) * dyrinv(iref);
+      cell_area(iref) = dxrm(iref) * dyrm(iref);
+      if (iref > 1) {
+        dxrinvc(iref) = 1.0f / (3.0f * dxrm(iref) / 2.0f);
+        dyrinvc(iref) = 1.0f / (3.0f * dyrm(iref) / 2.0f);
+      }
+      dxymin = std::min(dxymin, dxr(iref));
+      dxymin = std::min(dxymin, dyr(iref));
+    }
+    dtmax = std::min(dtmax, alfa * dxymin / (std::sqrt(9.81f * hmin_cfl)));
+    dtmin = alfa * dxymin / (1.25f * std::fabs(uvmax));
+    nuvisc.alloc(nref);
+    if (viscosity)
+      for (int iref = 1; iref <= nref; iref++) nuvisc(iref) = std::max(nuviscdim * dxyr(iref), 0.0f);
+  }
+
+  // initialize_bathymetry: sfincs_domain.f90:1588-1744
+  void initialize_bathymetry() {
+    if (!subgrid) {
+      zb.alloc(np);
+      zbuv.alloc(npuv);
+      zbuvmx.alloc(npuv);
+      auto d = read_stream<float>(path(depfile), (size_t)np);
+      for (long i = 1; i <= np; i++) zb(i) = d[i - 1];
+      for (long ip = 1; ip <= npuv; ip++) {
+        long nm = uv_index_z_nm(ip), nmu = uv_index_z_nmu(ip);
+        if (uv_flags_type(ip) == 0)
+          zbuv(ip) = 0.5f * (zb(nm) + zb(nmu));
+        else if (uv_flags_type(ip) == -1)
+          zbuv(ip) = 0.3333f * zb(nm) + 0.6667f * zb(nmu);
+        else
+          zbuv(ip) = 0.6667f * zb(nm) + 0.3333f * zb(nmu);
+        zbuvmx(ip) = std::max(zb(nm), zb(nmu)) + huthresh;
+      }
+    } else {
+      read_subgrid_file_netcdf();
+    }
+  }
+
+  // read_subgrid_file / read_subgrid_file_netcdf: sfincs_subgrid.F90:20-455
+  void read_subgrid_file_netcdf() {
+    huthresh = 0.0f;  // :40
+    nc3::File nc(path(sbgfile));
+    subgrid_nlevels = (int)nc.dim("levels");
+    long L = subgrid_nlevels;
+    // regular grid: identity remapping (:246-270)
+    auto zmin = nc.read_float("z_zmin"), zmax = nc.read_float("z_zmax"), volmax = nc.read_float("z_volmax"),
+         zlev = nc.read_float("z_level"), uzmin = nc.read_float("uv_zmin"), uzmax = nc.read_float("uv_zmax"),
+         uffit = nc.read_float("uv_ffit"), unavg = nc.read_float("uv_navg"), uhavg = nc.read_float("uv_havg"),
+         unrep = nc.read_float("uv_nrep"), upwet = nc.read_float("uv_pwet");
+    if ((long)zmin.size() != np || (long)uzmin.size() != npuv)
+      throw std::runtime_error("oracle: subgrid file does not match the mesh");
+    sg_z_zmin.alloc(np); sg_z_zmax.alloc(np); sg_z_volmax.alloc(np); sg_z_dep.alloc(L, np);
+    sg_uv_zmin.alloc(npuv); sg_uv_zmax.alloc(npuv); sg_uv_navg_w.alloc(npuv); sg_uv_fnfit.alloc(npuv);
+    sg_uv_havg.alloc(L, npuv); sg_uv_nrep.alloc(L, npuv); sg_uv_pwet.alloc(L, npuv);
+    sg_uv_havg_zmax.alloc(npuv); sg_uv_nrep_zmax.alloc(npuv);
+    for (long ip = 1; ip <= np; ip++) {
+      sg_z_zmin(ip) = zmin[ip - 1];
+      sg_z_zmax(ip) = zmax[ip - 1];
+      sg_z_volmax(ip) = volmax[ip - 1];
+      for (long k = 1; k <= L; k++) sg_z_dep(k, ip) = zlev[(ip - 1) * L + (k - 1)];
+    }
+    for (long ip = 1; ip <= npuv; ip++) {
+      sg_uv_zmin(ip) = uzmin[ip - 1];
+      sg_uv_zmax(ip) = uzmax[ip - 1];
+      sg_uv_zmax(ip) = std::max(sg_uv_zmax(ip), sg_uv_zmin(ip) + 0.01f);
+      sg_uv_fnfit(ip) = uffit[ip - 1];
+      float nv = std::max(unavg[ip - 1], 0.0001f);
+      sg_uv_navg_w(ip) = g * (nv * nv);
+      for (long k = 1; k <= L; k++) {
+        sg_uv_havg(k, ip) = uhavg[(ip - 1) * L + (k - 1)];
+        float nr = std::max(unrep[(ip - 1) * L + (k - 1)], 0.0001f);
+        sg_uv_nrep(k, ip) = g * (nr * nr);
+        sg_uv_pwet(k, ip) = upwet[(ip - 1) * L + (k - 1)];
+      }
+    }
+    for (long ip = 1; ip <= npuv; ip++) {  // :364-388
+      long nm = uv_index_z_nm(ip), nmu = uv_index_z_nmu(ip);
+      if (sg_z_zmin(nm) > sg_uv_zmin(ip)) {
+        sg_uv_zmin(ip) = std::max(sg_uv_zmin(ip), sg_z_zmin(nm));
+        sg_uv_zmax(ip) = std::max(sg_uv_zmax(ip), sg_uv_zmin(ip) + 0.01f);
+      }
+      if (sg_z_zmin(nmu) > sg_uv_zmin(ip)) {
+        sg_uv_zmin(ip) = std::max(sg_uv_zmin(ip), sg_z_zmin(nmu));
+        sg_uv_zmax(ip) = std::max(sg_uv_zmax(ip), sg_uv_zmin(ip) + 0.01f);
+      }
+    }
+    for (long nm = 1; nm <= np; nm++)  // :400-411
+      if (sg_z_zmax(nm) - sg_z_zmin(nm) <= 0.0f) sg_z_zmax(nm) = sg_z_zmax(nm) + 0.01f;
+    for (long ip = 1; ip <= npuv; ip++)  // :421-433
+      if (sg_uv_zmax(ip) - sg_uv_zmin(ip) < 1.0e-7f) sg_uv_zmax(ip) = sg_uv_zmax(ip) + 0.01f;
+    for (long ip = 1; ip <= npuv; ip++) {  // :443-446
+      sg_uv_havg_zmax(ip) = sg_uv_havg(L, ip) - sg_uv_zmax(ip);
+      sg_uv_nrep_zmax(ip) = sg_uv_nrep(L, ip);
+    }
+  }
+
+  // initialize_boundaries: sfincs_domain.f90:1765-1958
+  void initialize_boundaries() {
+    ngbnd = 0;
+    for (long nm = 1; nm <= np; nm++) {
+      int k = kcs(nm);
+      if (k == 2 || k == 3 || k == 5 || k == 6) {
+        boundaries_in_mask = true;
+        ngbnd++;
+        if (k == 2) water_level_boundaries_in_mask = true;
+        if (k == 3) outflow_boundaries_in_mask = true;
+        if (k == 5) downstream_river_boundaries_in_mask = true;
+        if (k == 6) neumann_boundaries_in_mask = true;
+      }
+    }
+    nmindbnd.alloc(ngbnd);
+    zsb.alloc(ngbnd);
+    zsb0.alloc(ngbnd);
+    ngbnd = 0;
+    for (long nm = 1; nm <= np; nm++) {
+      int k = kcs(nm);
+      if (k == 2 || k == 3 || k == 5 || k == 6) nmindbnd(++ngbnd) = (int32_t)nm;
+    }
+    nkcuv2 = 0;
+    kcuv.fill(0);
+    for (long ip = 1; ip <= npuv; ip++) {
+      int a = kcs(uv_index_z_nm(ip)), b = kcs(uv_index_z_nmu(ip));
+      if (a > 1 && b > 1)
+        kcuv(ip) = 0;
+      else if (a * b == 0)
+        kcuv(ip) = 0;
+      else if ((a == 1 && b == 2) || (a == 2 && b == 1)) {
+        kcuv(ip) = 2;
+        nkcuv2++;
+      } else if ((a == 1 && b == 3) || (a == 3 && b == 1)) {
+        kcuv(ip) = 2;
+        nkcuv2++;
+      } else if ((a == 1 && b == 5) || (a == 5 && b == 1)) {
+        kcuv(ip) = 2;
+        nkcuv2++;
+      } else if ((a == 1 && b == 6) || (a == 6 && b == 1)) {
+        kcuv(ip) = 6;
+        nkcuv2++;
+      } else
+        kcuv(ip) = 1;
+    }
+    index_kcuv2.alloc(nkcuv2); nmbkcuv2.alloc(nkcuv2); nmikcuv2.alloc(nkcuv2);
+    ibuvdir.alloc(nkcuv2); uvmean.alloc(nkcuv2); ibkcuv2.alloc(nkcuv2);
+    long ik = 0;
+    for (long ip = 1; ip <= npuv; ip++) {
+      if (kcuv(ip) == 2 || kcuv(ip) == 6) {
+        ik++;
+        index_kcuv2(ik) = (int32_t)ip;
+        long nm = uv_index_z_nm(ip), nmu = uv_index_z_nmu(ip);
+        if (kcs(nm) == 1) {
+          nmbkcuv2(ik) = (int32_t)nmu;
+          nmikcuv2(ik) = (int32_t)nm;
+          ibuvdir(ik) = -1;
+        } else {
+          nmbkcuv2(ik) = (int32_t)nm;
+          nmikcuv2(ik) = (int32_t)nmu;
+          ibuvdir(ik) = 1;
+        }
+        for (long ib = 1; ib <= ngbnd; ib++) {
+          if (nmindbnd(ib) == nmbkcuv2(ik)) {
+            ibkcuv2(ik) = (int32_t)ib;
+            if (kcs(nmindbnd(ib)) == 3) {
+              zsb0(ib) = subgrid ? sg_z_zmin(nmindbnd(ib)) : zb(nmindbnd(ib));
+              zsb(ib) = zsb0(ib);
+            }
+            break;
+          }
+        }
+      }
+    }
+  }
+
+  // initialize_roughness: sfincs_domain.f90:1960-2061
+  void initialize_roughness() {
+    if (subgrid) return;
+    gn2uv.alloc(npuv, 9.81f * 0.02f * 0.02f);
+    if (manningfile.substr(0, 4) != "none") {
+      auto r = read_stream<float>(path(manningfile), (size_t)np);
+      for (long ip = 1; ip <= npuv; ip++) {
+        long nm = uv_index_z_nm(ip), nmu = uv_index_z_nmu(ip);
+        if (kcuv(ip) > 0) {
+          float a = 0.5f * (r[nm - 1] + r[nmu - 1]);
+          gn2uv(ip) = 9.81f * (a * a);
+        }
+      }
+    } else {
+      float gn2land = manning_land < 0.0f ? 9.81f * (manning * manning) : 9.81f * (manning_land * manning_land);
+      float gn2sea = manning_sea < 0.0f ? 9.81f * (manning * manning) : 9.81f * (manning_sea * manning_sea);
+      for (long ip = 1; ip <= npuv; ip++)
+        if (kcuv(ip) > 0) gn2uv(ip) = zbuv(ip) > rghlevland ? gn2land : gn2sea;
+    }
+  }
+
+  // initialize_infiltration: sfincs_infiltration.f90:8-606 (con and c2d)
+  void initialize_infiltration() {
+    infiltration = false;
+    if (!precip) return;
+    if (qinf > 0.0f) {
+      inftype = "con";
+      infiltration = true;
+    } else if (qinffile.substr(0, 4) != "none") {
+      inftype = "c2d";
+      infiltration = true;
+    } else if (scsfile != "none" || sefffile != "none" || psifile != "none" || f0file != "none" ||
+               infiltrationfile != "none") {
+      throw std::runtime_error("oracle: only con/c2d infiltration types are restated");
+    }
+    cumprcp.alloc(np);
+    cuminf.alloc(np);
+    if (!infiltration) return;
+    qinffield.alloc(np);
+    if (inftype == "con") {
+      for (long nm = 1; nm <= np; nm++) {
+        float zz = subgrid ? sg_z_zmin(nm) : zb(nm);
+        qinffield(nm) = zz > qinf_zmin ? qinf : 0.0f;
+      }
+    } else {
+      auto r = read_stream<float>(path(qinffile), (size_t)np);
+      for (long nm = 1; nm <= np; nm++) qinffield(nm) = r[nm - 1] / 3600.0f / 1000.0f;
+    }
+    qinfmap.alloc(np);
+  }
+
+  // initialize_hydro + set_initial_conditions + compute_initial_subgrid_volumes:
+  // sfincs_domain.f90:2183-2410, sfincs_initial_conditions.F90:14-180, sfincs_subgrid.F90:907-962
+  void initialize_hydro() {
+    zs.alloc(np);
+    q.alloc(npuv + ncuv + 1);
+    q0.alloc(npuv + ncuv + 1);
+    uv.alloc(npuv + ncuv + 1);
+    uv0.alloc(npuv + ncuv + 1);
+    kfuv.alloc(npuv);
+    if (wiggle_suppression) {
+      zs0.alloc(np);
+      zsderv.alloc(np);
+    }
+    if (store_maximum_waterlevel) zsmax.alloc(np);
+    if (store_maximum_velocity) vmax.alloc(np);
+    if (store_maximum_flux) qmax.alloc(np);
+    if (store_twet) twet.alloc(np);
+    if (store_t_zsmax) t_zsmax.alloc(np);
+    if (rstfile.substr(0, 4) != "none" || zsinifile.substr(0, 4) != "none")
+      throw std::runtime_error("oracle: restart/ini files are not part of this path");
+    for (long nm = 1; nm <= np; nm++) {
+      double inizs = (double)zini;
+      if (subgrid)
+        zs(nm) = (TZ)std::max((double)sg_z_zmin(nm), inizs);
+      else
+        zs(nm) = (TZ)std::max((double)zb(nm), inizs);
+    }
+    if (wiggle_suppression)
+      for (long nm = 1; nm <= np; nm++) zs0(nm) = (T)zs(nm);
+    for (long ic = 1; ic <= ncuv; ic++) {
+      q(cuv_index_uv(ic)) = (T)0.5f * (q(cuv_index_uv1(ic)) + q(cuv_index_uv2(ic)));
+      uv(cuv_index_uv(ic)) = (T)0.5f * (uv(cuv_index_uv1(ic)) + uv(cuv_index_uv2(ic)));
+    }
+    if (store_maximum_waterlevel) zsmax.fill((T)-999.0f);
+    if (store_maximum_velocity) vmax.fill((T)-999.0f);
+    if (store_twet) twet.fill((T)0.0f);
+    if (store_t_zsmax) t_zsmax.fill(-999.0f);
+    uv.fill((T)0);
+    if (wind) {
+      tauwu.alloc(np);
+      tauwv.alloc(np);
+    }
+    if (precip) {
+      prcp.alloc(np);
+      netprcp.alloc(np);
+    }
+    if (use_qext) qext.alloc(np);
+    if (subgrid) {
+      z_volume.alloc(np);
+      long L = subgrid_nlevels;
+      for (long nm = 1; nm <= np; nm++) {
+        if (zs(nm) >= sg_z_zmax(nm)) {
+          z_volume(nm) = (TV)((double)sg_z_volmax(nm) + (double)cell_area(z_flags_iref(nm)) *
+                                                         ((double)zs(nm) - (double)std::max(sg_z_zmax(nm), -20.0f)));
+        } else {
+          long ivol = 1;
+          for (long il = 2; il <= L; il++) {
+            if (sg_z_dep(il, nm) > zs(nm)) {
+              ivol = il - 1;
+              break;
+            }
+          }
+          float dzvol = sg_z_volmax(nm) / (float)(L - 1);
+          float facint = (float)(((double)zs(nm) - (double)sg_z_dep(ivol, nm)) /
+                                 (double)std::max(sg_z_dep(ivol + 1, nm) - sg_z_dep(ivol, nm), 0.001f));
+          z_volume(nm) = (TV)((float)(ivol - 1) * dzvol + facint * dzvol);
+        }
+      }
+    }
+  }
+
+  // set_advection_mask: sfincs_domain.f90:2114-2180
+  void set_advection_mask() {
+    for (long ic = 1; ic <= ncuv; ic++) {
+      int a = kcuv(cuv_index_uv1(ic)), b = kcuv(cuv_index_uv2(ic));
+      int8_t& k = kcuv(cuv_index_uv(ic));
+      if (a == 0 || b == 0)
+        k = 0;
+      else if (a == 2 || b == 2)
+        k = 2;
+      else if (a == 4 || b == 4)
+        k = 4;
+      else
+        k = 1;
+    }
+    if (advection) {
+      mask_adv.alloc(npuv, 1);
+      if (advection_mask && (use_quadtree || nmax > 1)) {
+        for (long ip = 1; ip <= npuv; ip++) {
+          if (kcuv(uv_index_u_nmu(ip)) != 1 || kcuv(uv_index_u_nmd(ip)) != 1 || kcuv(uv_index_v_nm(ip)) != 1 ||
+              kcuv(uv_index_v_nmu(ip)) != 1 || kcuv(uv_index_v_ndm(ip)) != 1 || kcuv(uv_index_v_ndmu(ip)) != 1 ||
+              kcuv(uv_index_u_ndm(ip)) != 1 || kcuv(uv_index_u_num(ip)) != 1)
+            mask_adv(ip) = 0;
+        }
+      }
+    }
+  }
+
+  // read_boundary_data (bnd/bzs branch) + find_boundary_indices: sfincs_boundaries.f90:8-213, 455-679
+  void read_boundary_data() {
+    nbnd = 0;
+    ntbnd = 0;
+    itbndlast = 1;
+    if (bndfile.substr(0, 4) != "none") {
+      auto xy = read_ascii_table(path(bndfile));
+      nbnd = (long)xy.size();
+      x_bnd.alloc(nbnd);
+      y_bnd.alloc(nbnd);
+      for (long n = 1; n <= nbnd; n++) {
+        x_bnd(n) = (float)xy[n - 1][0];
+        y_bnd(n) = (float)xy[n - 1][1];
+      }
+      if (bzsfile.substr(0, 4) != "none") {
+        auto tb = read_ascii_table(path(bzsfile));
+        ntbnd = (long)tb.size();
+        t_bnd.alloc(ntbnd);
+        zs_bnd.alloc(nbnd, ntbnd);
+        zst_bnd.alloc(nbnd);
+        for (long it = 1; it <= ntbnd; it++) {
+          t_bnd(it) = (float)tb[it - 1][0];
+          for (long ib = 1; ib <= nbnd; ib++) zs_bnd(ib, it) = (float)tb[it - 1][ib];
+        }
+      } else {
+        ntbnd = 2;
+        t_bnd.alloc(2);
+        zs_bnd.alloc(nbnd, 2);
+        zst_bnd.alloc(nbnd);
+        t_bnd(1) = t0;
+        t_bnd(2) = t1;
+      }
+      if (t_bnd(1) > (t0 + 1.0f) || t_bnd(ntbnd) < (t1 - 1.0f)) {
+        if (t_bnd(1) > (t0 + 1.0f))
+          t_bnd(1) = t0 - 1.0f;
+        else
+          t_bnd(ntbnd) = t1 + 1.0f;
+      }
+    } else if (water_level_boundaries_in_mask) {
+      nbnd = 1;
+      x_bnd.alloc(1);
+      y_bnd.alloc(1);
+      ntbnd = 2;
+      t_bnd.alloc(2);
+      zs_bnd.alloc(1, 2);
+      zst_bnd.alloc(1);
+      t_bnd(1) = t0;
+      t_bnd(2) = t1;
+    }
+    if (downstream_river_boundaries_in_mask)
+      throw std::runtime_error("oracle: downstream river boundaries are not restated");
+  }
+
+  void find_boundary_indices() {
+    if (ngbnd == 0) return;
+    if (nbnd == 0) return;
+    ind1_bnd_gbp.alloc(ngbnd);
+    ind2_bnd_gbp.alloc(ngbnd);
+    fac_bnd_gbp.alloc(ngbnd);
+    if (neumann_boundaries_in_mask) nmi_gbp.alloc(ngbnd);
+    for (long ib = 1; ib <= ngbnd; ib++) {
+      long nm = nmindbnd(ib);
+      float x = z_xz(nm), y = z_yz(nm);
+      if (kcs(nm) == 2) {
+        if (nbnd > 1) {
+          float dst1 = 1.0e10f, dst2 = 1.0e10f;
+          long ib1 = 0, ib2 = 0;
+          for (long ibnd = 1; ibnd <= nbnd; ibnd++) {
+            float ddx = x_bnd(ibnd) - x, ddy = y_bnd(ibnd) - y;
+            float dst = std::sqrt(ddx * ddx + ddy * ddy);
+            if (dst < dst1) {
+              dst2 = dst1;
+              ib2 = ib1;
+              dst1 = dst;
+              ib1 = ibnd;
+            } else if (dst < dst2) {
+              dst2 = dst;
+              ib2 = ibnd;
+            }
+          }
+          ind1_bnd_gbp(ib) = (int32_t)ib1;
+          ind2_bnd_gbp(ib) = (int32_t)ib2;
+          fac_bnd_gbp(ib) = dst2 / std::max(dst1 + dst2, 1.0e-9f);
+        } else {
+          ind1_bnd_gbp(ib) = 1;
+          ind2_bnd_gbp(ib) = 1;
+          fac_bnd_gbp(ib) = 1.0f;
+        }
+      } else if (kcs(nm) == 6) {
+        // regular grid: find_sfincs_cell(n, m+-1 / n+-1, iref) through the quadtree search arrays
+        long n = z_index_z_n(nm), m = z_index_z_m(nm);
+        auto find = [&](long nn, long mm) -> long {
+          long nmq = find_qt_by_index(nn, mm, z_flags_iref(nm));
+          return nmq > 0 ? index_sfincs_in_quadtree(nmq) : 0;
+        };
+        long cand[4][2] = {{n, m + 1}, {n + 1, m}, {n, m - 1}, {n - 1, m}};
+        for (auto& c : cand) {
+          long nmi = find(c[0], c[1]);
+          if (nmi > 0 && kcs(nmi) == 1) nmi_gbp(ib) = (int32_t)nmi;
+        }
+        if (nmi_gbp(ib) == 0) kcs(nm) = 0;
+      }
+    }
+  }
+
+  // find_quadtree_cell_by_index + binary_search: sfincs_quadtree.F90:822-850
+  long find_qt_by_index(long n, long m, int iref) {
+    long nmx = (long)qt_nmax << (iref - 1);
+    long nm = (m - 1) * nmx + n;
+    long i1 = qt_first(iref), i2 = qt_last(iref);
+    if (nm <= 0 || n < 1 || m < 1) return 0;
+    long lo = i1, hi = i2;
+    while (lo <= hi) {
+      long mid = (lo + hi) / 2;
+      long v = qt_nm_indices(mid);
+      if (v == nm) return mid;
+      if (v < nm)
+        lo = mid + 1;
+      else
+        hi = mid - 1;
+    }
+    return 0;
+  }
+
+  // read_meteo_data (time-series part) + Cd table: sfincs_meteo.f90:247-327
+  void read_meteo_data() {
+    if (wndfile.substr(0, 4) != "none") {
+      auto tb = read_ascii_table(path(wndfile));
+      ntwnd = (long)tb.size();
+      itwndlast = 1;
+      twnd.alloc(ntwnd);
+      wndmag.alloc(ntwnd);
+      wnddir.alloc(ntwnd);
+      for (long it = 1; it <= ntwnd; it++) {
+        twnd(it) = (float)tb[it - 1][0];
+        wndmag(it) = (float)tb[it - 1][1];
+        wnddir(it) = (float)tb[it - 1][2];
+        wnddir(it) = pi * (270.0f - wnddir(it)) / 180.0f - rotation;
+      }
+    }
+    if (prcpfile.substr(0, 4) != "none") {
+      auto tb = read_ascii_table(path(prcpfile));
+      ntprcp = (long)tb.size();
+      itprcplast = 1;
+      tprcpt.alloc(ntprcp);
+      tprcpv.alloc(ntprcp);
+      for (long it = 1; it <= ntprcp; it++) {
+        tprcpt(it) = (float)tb[it - 1][0];
+        tprcpv(it) = (float)tb[it - 1][1];
+      }
+    }
+    float cd_wnd[3] = {0.0f, 28.0f, 50.0f}, cd_val[3] = {0.0010f, 0.0025f, 0.0015f};
+    int cd_nr = 3;
+    cdval.alloc(1000);
+    for (int iw = 1; iw <= 1000; iw++) {
+      float wnd = (float)iw * 0.1f;
+      for (int icd = 1; icd <= cd_nr - 1; icd++) {
+        cdval(iw) = cd_val[icd - 1];
+        if (wnd >= cd_wnd[icd - 1] && wnd < cd_wnd[icd]) {
+          cdval(iw) = cd_val[icd - 1] +
+                      (wnd - cd_wnd[icd - 1]) * (cd_val[icd] - cd_val[icd - 1]) / (cd_wnd[icd] - cd_wnd[icd - 1]);
+          break;
+        } else if (wnd >= cd_wnd[cd_nr - 1]) {
+          cdval(iw) = cd_val[cd_nr - 1];
+          break;
+        }
+      }
+    }
+  }
+
+  // read_discharges (src/dis branch): sfincs_discharges.f90:8-324
+  void read_discharges() {
+    nsrc = 0;
+    ntsrc = 0;
+    itsrclast = 1;
+    if (srcfile.substr(0, 4) == "none") return;
+    auto xy = read_ascii_table(path(srcfile));
+    nsrc = (long)xy.size();
+    auto tb = read_ascii_table(path(disfile));
+    ntsrc = (long)tb.size();
+    nmindsrc.alloc(nsrc);
+    qtsrc.alloc(nsrc);
+    tsrc.alloc(ntsrc);
+    qsrc.alloc(nsrc, ntsrc);
+    for (long it = 1; it <= ntsrc; it++) {
+      tsrc(it) = (float)tb[it - 1][0];
+      for (long is = 1; is <= nsrc; is++) qsrc(is, it) = (float)tb[it - 1][is];
+    }
+    for (long is = 1; is <= nsrc; is++) {
+      long nmq = find_quadtree_cell((float)xy[is - 1][0], (float)xy[is - 1][1]);
+      nmindsrc(is) = nmq > 0 ? index_sfincs_in_quadtree(nmq) : 0;
+      if (nmindsrc(is) == 0) throw std::runtime_error("oracle: source point outside the active mesh");
+    }
+  }
+
+  // find_quadtree_cell: sfincs_quadtree.F90:764-820
+  long find_quadtree_cell(float x, float y) {
+    float xt = qt_cosrot * (x - qt_x0) + qt_sinrot * (y - qt_y0);
+    float yt = -qt_sinrot * (x - qt_x0) + qt_cosrot * (y - qt_y0);
+    for (int iref = qt_nlev; iref >= 1; iref--) {
+      long n = (long)(yt / qt_dyr(iref)) + 1;
+      long m = (long)(xt / qt_dxr(iref)) + 1;
+      long idx = find_qt_by_index(n, m, iref);
+      if (idx > 0 && qt_level(idx) == iref) return idx;
+    }
+    return 0;
+  }
+
+  void initialize(const std::string& d, bool bmi) {
+    dir = d;
+    read_sfincs_input();
+    use_qext = bmi;
+    read_meteo_data();
+    initialize_processes();
+    initialize_mesh();
+    initialize_bathymetry();
+    initialize_boundaries();
+    initialize_roughness();
+    initialize_infiltration();
+    initialize_hydro();
+    if (qt_nlev == 1) use_quadtree = false;  // sfincs_domain.f90:42-50
+    set_advection_mask();
+    read_boundary_data();
+    find_boundary_indices();
+    read_discharges();
+    t = t0;  // sfincs_lib.f90:279-292
+    dt = 1.0e-6f;
+    min_dt = 1.0e-6f;
+    dtavg = 0.0f;
+    nt = 0;
+  }
+
+  // ============================================================ time step
+  // update_meteo_forcing (time-series part): sfincs_meteo.f90:1246-1558
+  void update_meteo_forcing(double tt, float dtt) {
+    if (wind) {  // update_wind_forcing_from_timeseries :1445-1508
+      for (long itw = itwndlast; itw <= ntwnd; itw++) {
+        if ((double)twnd(itw) > tt) {
+          long i0 = std::max(itw - 1, 1L);  // out-of-range guard: series must cover t
+          float twfac = (float)((tt - (double)twnd(i0)) / (double)(twnd(itw) - twnd(i0)));
+          float vmag = wndmag(i0) * (1.0f - twfac) + wndmag(itw) * twfac;
+          float twopi = 2.0f * pi;
+          float dr0 = std::fmod(wnddir(i0), twopi);
+          if (dr0 < 0) dr0 += twopi;
+          float dr1 = std::fmod(wnddir(itw), twopi);
+          if (dr1 < 0) dr1 += twopi;
+          if (dr1 > dr0 + pi)
+            dr0 = dr0 + 2.0f * pi;
+          else if (dr0 > dr1 + pi)
+            dr1 = dr1 + 2.0f * pi;
+          float vdir = dr0 * (1.0f - twfac) + dr1 * twfac;
+          float cd = cdval((long)(vmag * 10.0f) + 1);
+          double twu = (double)(vmag * vmag * std::cos(vdir) * rhoa * cd / rhow);
+          double twv = (double)(vmag * vmag * std::sin(vdir) * rhoa * cd / rhow);
+          for (long nm = 1; nm <= np; nm++) {
+            tauwu(nm) = (float)twu;
+            tauwv(nm) = (float)twv;
+          }
+          itwndlast = itw - 1 >= 1 ? itw - 1 : 1;
+          break;
+        }
+      }
+    }
+    if (precip) {  // update_precipitation_from_timeseries :1510-1558
+      long itp;
+      for (itp = itprcplast; itp <= ntprcp; itp++)
+        if ((double)tprcpt(itp) > tt) break;
+      itp = std::max(std::min(itp, ntprcp), 1L);
+      long i0 = std::max(itp - 1, 1L);  // out-of-range guard: series must cover t
+      float twfac = (float)((tt - (double)tprcpt(i0)) / (double)(tprcpt(itp) - tprcpt(i0)));
+      if (i0 == itp) twfac = 0.0f;
+      float ptmp = (tprcpv(i0) * (1.0f - twfac) + tprcpv(itp) * twfac) / (float)(1000 * 3600);
+      for (long nm = 1; nm <= np; nm++) {
+        prcp(nm) = ptmp;
+        netprcp(nm) = ptmp;
+        if (store_cumulative_precipitation) cumprcp(nm) = cumprcp(nm) + ptmp * dtt;
+      }
+      itprcplast = itp - 1 >= 1 ? itp - 1 : 1;
+    }
+  }
+
+  // update_infiltration_map (con/c2d): sfincs_infiltration.f90:609-676
+  void update_infiltration_map(float dtt) {
+    for (long nm = 1; nm <= np; nm++) {
+      qinfmap(nm) = qinffield(nm);
+      if (subgrid) {
+        if (z_volume(nm) <= 0.0) qinfmap(nm) = 0.0f;
+      } else {
+        if (zs(nm) <= zb(nm)) qinfmap(nm) = 0.0f;
+      }
+      netprcp(nm) = netprcp(nm) - qinfmap(nm);
+      if (store_cumulative_precipitation) cuminf(nm) = cuminf(nm) + qinfmap(nm) * dtt;
+    }
+  }
+
+  // update_boundary_points: sfincs_boundaries.f90:682-758
+  void update_boundary_points(double tt) {
+    if (nbnd == 0) return;
+    long itb0 = 1, itb1 = 1;
+    float tb = 0.0f;
+    if ((double)t_bnd(1) > (tt - 1.0e-3)) {
+      itb0 = 1;
+      itb1 = 1;
+      tb = t_bnd(itb0);
+    } else if ((double)t_bnd(ntbnd) < (tt + 1.0e-3)) {
+      itb0 = ntbnd;
+      itb1 = ntbnd;
+      tb = t_bnd(itb0);
+    } else {
+      for (long itb = itbndlast; itb <= ntbnd; itb++) {
+        if ((double)t_bnd(itb) > (tt + 1.0e-6)) {
+          itb0 = itb - 1;
+          itb1 = itb;
+          tb = (float)tt;
+          itbndlast = itb - 1;
+          break;
+        }
+      }
+    }
+    float tbfac = (tb - t_bnd(itb0)) / std::max(t_bnd(itb1) - t_bnd(itb0), 1.0e-6f);
+    for (long ib = 1; ib <= nbnd; ib++)
+      zst_bnd(ib) = zs_bnd(ib, itb0) + (zs_bnd(ib, itb1) - zs_bnd(ib, itb0)) * tbfac;
+  }
+
+  // update_boundary_conditions: sfincs_boundaries.f90:761-921
+  void update_boundary_conditions(double tt) {
+    for (long ib = 1; ib <= ngbnd; ib++) {
+      long nmb = nmindbnd(ib);
+      if (kcs(nmb) == 2) {
+        double zst;
+        if (nbnd > 1)
+          zst = (double)(zst_bnd(ind1_bnd_gbp(ib)) * fac_bnd_gbp(ib) +
+                         zst_bnd(ind2_bnd_gbp(ib)) * (1.0f - fac_bnd_gbp(ib)));
+        else
+          zst = (double)zst_bnd(1);
+        float zsetup = 0.0f, zig = 0.0f;
+        if (tt < (double)(tspinup - 1.0e-3f)) {
+          float smfac = (float)(1.0 - (tt - (double)t0) / (double)(tspinup - t0));
+          float zs0act = (float)(zst + (double)zsetup);
+          zsb0(ib) = zini * smfac + zs0act * (1.0f - smfac);
+          zs0act = (float)(zst + (double)zsetup + (double)zig);
+          zsb(ib) = zini * smfac + zs0act * (1.0f - smfac);
+        } else {
+          zsb0(ib) = (float)(zst + (double)zsetup);
+          zsb(ib) = (float)(zst + (double)zsetup + (double)zig);
+        }
+        if (subgrid) {
+          zsb0(ib) = std::max(zsb0(ib), sg_z_zmin(nmb));
+          zsb(ib) = std::max(zsb(ib), sg_z_zmin(nmb));
+        } else {
+          zsb0(ib) = std::max(zsb0(ib), zb(nmb));
+          zsb(ib) = std::max(zsb(ib), zb(nmb));
+        }
+      } else if (kcs(nmb) == 6) {
+        zs(nmb) = zs(nmi_gbp(ib));
+      }
+    }
+  }
+
+  // update_boundary_fluxes: sfincs_boundaries.f90:924-1122
+  void update_boundary_fluxes(float dtt, double tt) {
+    float factime = std::min(dtt / btfilter, 1.0f);
+    float one_minus_factime = 1.0f - factime;
+    float facrel = 1.0f - std::min(dtt / btrelax, 1.0f);
+    long L = subgrid_nlevels;
+    for (long ib = 1; ib <= nkcuv2; ib++) {
+      long indb = ibkcuv2(ib);
+      long nmb = nmbkcuv2(ib);
+      if (kcs(nmb) == 6) continue;
+      long nmi = nmikcuv2(ib);
+      long ip = index_kcuv2(ib);
+      float zsnmi = (float)zs(nmi);
+      float zsnmb = zsb(indb);
+      float zs0nmb = zsb0(indb);
+      float hnmb;
+      if (bndtype == 1) {
+        if (subgrid) {
+          float zsuv = std::max(zsnmb, zsnmi);
+          float depthuv;
+          if (zsuv >= sg_uv_zmax(ip) - 1.0e-4f) {
+            depthuv = sg_uv_havg_zmax(ip) + zsuv;
+          } else if (zsuv > sg_uv_zmin(ip)) {
+            float dzuv = (sg_uv_zmax(ip) - sg_uv_zmin(ip)) / (float)(L - 1);
+            long iuv = (long)((zsuv - sg_uv_zmin(ip)) / dzuv) + 1;
+            float facint = (zsuv - (sg_uv_zmin(ip) + (float)(iuv - 1) * dzuv)) / dzuv;
+            depthuv = sg_uv_havg(iuv, ip) + (sg_uv_havg(iuv + 1, ip) - sg_uv_havg(iuv, ip)) * facint;
+          } else {
+            depthuv = 0.0f;
+          }
+          hnmb = std::max(depthuv, huthresh);
+          zsnmb = std::max(zsnmb, sg_z_zmin(nmb));
+          zs0nmb = std::max(zs0nmb, sg_z_zmin(nmb));
+        } else {
+          hnmb = std::max(0.5f * (zsnmb + zsnmi) - zbuv(ip), huthresh);
+          zsnmb = std::max(zsnmb, zb(nmb));
+          zs0nmb = std::max(zs0nmb, zb(nmb));
+        }
+        if (hnmb < huthresh + 1.0e-6f || kcuv(ip) == 3) {
+          q(ip) = (T)0;
+          uv(ip) = (T)0;
+          uvmean(ib) = 0.0f;
+        } else {
+          float sq = std::sqrt(g / hnmb);
+          float ui = sq * (zsnmb - zs0nmb);
+          float ub = (float)ibuvdir(ib) * (2.0f * ui - sq * (zsnmi - zs0nmb));
+          float qq = ub * hnmb + uvmean(ib);
+          if (subgrid) {
+            if (z_volume(nmi) <= 0.0) qq = ibuvdir(ib) == 1 ? std::max(qq, 0.0f) : std::min(qq, 0.0f);
+            if (zsnmb - sg_z_zmin(nmb) < huthresh) qq = ibuvdir(ib) == 1 ? std::min(qq, 0.0f) : std::max(qq, 0.0f);
+          } else {
+            if (zsnmi - zb(nmi) <= huthresh) qq = ibuvdir(ib) == 1 ? std::max(qq, 0.0f) : std::min(qq, 0.0f);
+            if (zsnmb - zb(nmb) < huthresh) qq = ibuvdir(ib) == 1 ? std::min(qq, 0.0f) : std::max(qq, 0.0f);
+          }
+          q(ip) = (T)qq;
+          uv(ip) = (T)std::max(std::min(qq / hnmb, 4.0f), -4.0f);
+        }
+        if (btfilter >= -1.0e-6f)
+          uvmean(ib) = factime * (float)q(ip) + facrel * one_minus_factime * uvmean(ib);
+        else
+          uvmean(ib) = 0.0f;
+        zs(nmb) = (TZ)zsb(indb);
+        if (store_maximum_waterlevel) {
+          if (store_t_zsmax && zs(nmb) > zsmax(nmb)) t_zsmax(nmb) = (float)tt;
+          zsmax(nmb) = (T)std::max((double)zsmax(nmb), (double)zs(nmb));
+        }
+      }
+    }
+  }
+
+  // update_discharges (point sources): sfincs_discharges.f90:325-368
+  void update_discharges(double tt) {
+    if (nsrc <= 0) return;
+    for (long its = itsrclast; its <= ntsrc; its++) {
+      if ((double)tsrc(its) > tt) {
+        long i0 = std::max(its - 1, 1L);
+        for (long is = 1; is <= nsrc; is++)
+          qtsrc(is) = (float)((double)qsrc(is, i0) +
+                              (double)(qsrc(is, its) - qsrc(is, i0)) * (tt - (double)tsrc(i0)) /
+                                  (double)(tsrc(its) - tsrc(i0)));
+        itsrclast = its - 1 >= 1 ? its - 1 : 1;
+        break;
+      }
+    }
+  }
+
+  // compute_fluxes: sfincs_momentum.f90:9-784 (projected grids)
+  void compute_fluxes(float dtt) {
+    min_dt = dtmax;
+    for (long ip = 1; ip <= npuv + ncuv; ip++) {
+      q0(ip) = q(ip);
+      uv0(ip) = uv(ip);
+    }
+    const T expo = (T)(1.0f / 3.0f);
+    const long L = subgrid_nlevels;
+    float mdt = min_dt;
+#pragma omp parallel for schedule(dynamic, 256) reduction(min : mdt)
+    for (long ip = 1; ip <= npuv; ip++) {
+      if (!(kcuv(ip) == 1 || kcuv(ip) == 6)) continue;
+      long nm = uv_index_z_nm(ip), nmu = uv_index_z_nmu(ip);
+      bool iok = false;
+      T zsu = (T)std::max(zs(nm), zs(nmu));
+      T zmin = 0, zmax = 0;
+      if (subgrid) {
+        zmin = sg_uv_zmin(ip);
+        zmax = sg_uv_zmax(ip);
+        if (zsu > zmin + (T)huthresh) iok = true;
+      } else {
+        if (zsu > (T)zbuvmx(ip)) iok = true;
+      }
+      if (iok) {
+        int iref = 1, itype = 0;
+        if (use_quadtree) {
+          iref = uv_flags_iref(ip);
+          itype = uv_flags_type(ip);
+        }
+        int idir = uv_flags_dir(ip);
+        T dxuvinv, dyuvinv, dxuv2inv, dyuv2inv;
+        if (itype == 0) {
+          if (idir == 0) {
+            dxuvinv = dxrinv(iref); dyuvinv = dyrinv(iref); dxuv2inv = dxr2inv(iref); dyuv2inv = dyr2inv(iref);
+          } else {
+            dxuvinv = dyrinv(iref); dyuvinv = dxrinv(iref); dxuv2inv = dyr2inv(iref); dyuv2inv = dxr2inv(iref);
+          }
+        } else {
+          if (idir == 0) {
+            dxuvinv = dxrinvc(iref); dyuvinv = dyrinv(iref); dxuv2inv = 0; dyuv2inv = dyr2inv(iref);
+          } else {
+            dxuvinv = dyrinvc(iref); dyuvinv = dxrinv(iref); dxuv2inv = 0; dyuv2inv = dxr2inv(iref);
+          }
+        }
+        T fcoriouv = (T)fcorio;
+        T qx_nm = q0(ip);
+        T qx_nmd = 0, qx_nmu = 0, qy_nm = 0, qy_nmu = 0, qy_ndm = 0, qy_ndmu = 0;
+        T uu_nm = 0, uu_nmd = 0, uu_nmu = 0, uu_ndm = 0, uu_num = 0, vu = 0;
+        if (advection || coriolis || viscosity || friction2d || thetasmoothing) {
+          qx_nmd = q0(uv_index_u_nmd(ip));
+          qx_nmu = q0(uv_index_u_nmu(ip));
+          qy_nm = q0(uv_index_v_nm(ip));
+          qy_nmu = q0(uv_index_v_nmu(ip));
+          qy_ndm = q0(uv_index_v_ndm(ip));
+          qy_ndmu = q0(uv_index_v_ndmu(ip));
+          uu_nm = uv0(ip);
+          uu_nmd = uv0(uv_index_u_nmd(ip));
+          uu_nmu = uv0(uv_index_u_nmu(ip));
+          uu_ndm = uv0(uv_index_u_ndm(ip));
+          uu_num = uv0(uv_index_u_num(ip));
+          vu = (uv0(uv_index_v_ndm(ip)) + uv0(uv_index_v_ndmu(ip)) + uv0(uv_index_v_nm(ip)) + uv0(uv_index_v_nmu(ip))) /
+               (T)4;
+        }
+        T phi = 1;
+        T hu, gnavg2;
+        if (subgrid) {
+          if (zsu > zmax) {
+            hu = sg_uv_havg_zmax(ip) + zsu;
+            gnavg2 = sg_uv_navg_w(ip) -
+                     (sg_uv_navg_w(ip) - sg_uv_nrep_zmax(ip)) / (sg_uv_fnfit(ip) * (zsu - zmax) + (T)1);
+          } else {
+            T dzuv = (zmax - zmin) / (T)(L - 1);
+            long iuv = std::min((long)((zsu - zmin) / dzuv) + 1, L - 1);
+            T facint = (zsu - (zmin + (T)(iuv - 1) * dzuv)) / dzuv;
+            hu = sg_uv_havg(iuv, ip) + (sg_uv_havg(iuv + 1, ip) - sg_uv_havg(iuv, ip)) * facint;
+            gnavg2 = sg_uv_nrep(iuv, ip) + (sg_uv_nrep(iuv + 1, ip) - sg_uv_nrep(iuv, ip)) * facint;
+            phi = sg_uv_pwet(iuv, ip) + (sg_uv_pwet(iuv + 1, ip) - sg_uv_pwet(iuv, ip)) * facint;
+          }
+        } else {
+          hu = std::max(zsu - (T)zbuvmx(ip), (T)huthresh);
+          gnavg2 = gn2uv(ip);
+        }
+        T hwet = hu / phi;
+        T dzdx;
+        if (slopelim < 9999.0f)
+          dzdx = (T)std::min(std::max((T)((zs(nmu) - zs(nm)) * dxuvinv), (T)-slopelim), (T)slopelim);
+        else
+          dzdx = (T)((zs(nmu) - zs(nm)) * dxuvinv);
+        T frc = -(T)g * hu * dzdx;
+        if (advection) {
+          if (mask_adv(ip) == 1) {
+            T dqxudx = 0, dqyudy = 0;
+            if (advection_scheme == 0) {
+              if (qx_nm > (T)1.0e-6f)
+                dqxudx = (qx_nm * uu_nm - qx_nmd * uu_nmd) * dxuvinv;
+              else if (qx_nm < (T)-1.0e-6f)
+                dqxudx = (qx_nmu * uu_nmu - qx_nm * uu_nm) * dxuvinv;
+              T qy = qy_ndm + qy_ndmu + qy_nm + qy_nmu;
+              if (qy > (T)1.0e-6f)
+                dqyudy = (qy_ndm + qy_ndmu) * (uu_nm - uu_ndm) * dyuvinv / (T)2;
+              else if (qy < (T)-1.0e-6f)
+                dqyudy = (qy_nm + qy_nmu) * (uu_num - uu_nm) * dyuvinv / (T)2;
+            } else {
+              T qd = (qx_nmd + qx_nm) / (T)2;
+              T qu = (qx_nm + qx_nmu) / (T)2;
+              if (qd > (T)1.0e-6f) {
+                T ud = (uu_nmd + uu_nm) / (T)2;
+                dqxudx = (qd * (uu_nm - uu_nmd) + ud * (qx_nm - qx_nmd)) * dxuvinv;
+              }
+              if (qu < (T)-1.0e-6f) {
+                T uu = (uu_nm + uu_nmu) / (T)2;
+                dqxudx = dqxudx + (qu * (uu_nmu - uu_nm) + uu * (qx_nmu - qx_nm)) * dxuvinv;
+              }
+              qu = (qy_nm + qy_nmu) / (T)2;
+              qd = (qy_ndm + qy_ndmu) / (T)2;
+              if (qd > (T)1.0e-6f) dqyudy = qd * (uu_nm - uu_ndm) * dyuvinv;
+              if (qu < (T)-1.0e-6f) dqyudy = dqyudy + qu * (uu_num - uu_nm) * dyuvinv;
+              T ud = (uu_nmd + uu_nm) / (T)2;
+              T uu = (uu_nm + uu_nmu) / (T)2;
+              if (ud > (T)1.0e-6f) dqyudy = dqyudy + ud * (qy_nm - qy_ndm) * dyuvinv;
+              if (uu < (T)-1.0e-6f) dqyudy = dqyudy + uu * (qy_nmu - qy_ndmu) * dyuvinv;
+            }
+            T adv = -phi * (dqxudx + dqyudy);
+            adv = std::min(std::max(adv, -(T)advlim * hu), (T)advlim * hu);
+            frc = frc + adv;
+          }
+        }
+        if (viscosity) {
+          T lap = (uu_nmu - (T)2 * uu_nm + uu_nmd) * dxuv2inv + (uu_num - (T)2 * uu_nm + uu_ndm) * dyuv2inv;
+          if (itype == 0)
+            frc = frc + (T)nuvisc(iref) * hu * lap;
+          else
+            frc = frc + (T)nuviscfac * (T)nuvisc(iref) * hu * lap;
+        }
+        if (coriolis) {
+          if (idir == 0)
+            frc = frc + fcoriouv * hu * vu;
+          else
+            frc = frc - fcoriouv * hu * vu;
+        }
+        if (wind) {
+          T tw = idir == 0 ? (T)tauwu(nm) : (T)tauwv(nm);
+          if (hwet > (T)0.25f)
+            frc = frc + phi * tw;
+          else
+            frc = frc + tw * hu * (T)4;
+        }
+        T qfr;
+        if (kfuv(ip) == 0) {
+          qfr = std::sqrt(std::fabs(dzdx) / (std::max(gnavg2, (T)1.0e-5f) / (T)10)) * std::pow(hu, (T)(5.0f / 3.0f));
+        } else {
+          if (friction2d)
+            qfr = std::sqrt(qx_nm * qx_nm + (hu * vu) * (hu * vu));
+          else
+            qfr = std::fabs(qx_nm);
+        }
+        T qsm = qx_nm;
+        if (thetasmoothing) {
+          if (kcuv(uv_index_u_nmd(ip)) == 1 && kcuv(uv_index_u_nmu(ip)) == 1) {
+            if (std::fabs(qx_nmd) > (T)1.0e-6f && std::fabs(qx_nmu) > (T)1.0e-6f)
+              qsm = (T)theta * qx_nm + (T)0.5f * ((T)1 - (T)theta) * (qx_nmu + qx_nmd);
+          }
+        }
+        if (h73table) throw std::runtime_error("oracle: h73table is off by default and not restated");
+        T hu73 = hu * hu * std::pow(hu, expo);
+        T qn = (qsm + frc * (T)dtt) / ((T)1 + gnavg2 * (T)dtt * qfr / hu73);
+        if (subgrid && wiggle_suppression) {
+          T mdrv = std::fabs(zsderv(nm) - zsderv(nmu)) - (T)wiggle_threshold;
+          if (mdrv > (T)0) qn = qn * (T)wiggle_threshold / ((T)wiggle_factor * mdrv + (T)wiggle_threshold);
+        }
+        if (subgrid) {
+          if (z_volume(nm) < 0.0) qn = std::min(qn, (T)0);
+          if (z_volume(nmu) < 0.0) qn = std::max(qn, (T)0);
+        } else {
+          if ((double)zs(nm) < (double)zb(nm)) qn = std::min(qn, (T)0);
+          if ((double)zs(nmu) < (double)zb(nmu)) qn = std::max(qn, (T)0);
+        }
+        qn = std::min(std::max(qn, -hu * (T)uvlim), hu * (T)uvlim);
+        q(ip) = qn;
+        uv(ip) = qn / std::max(hu, (T)huvmin);
+        kfuv(ip) = 1;
+        T min_dt_ip = (T)1 / (std::max(std::sqrt((T)g * hu), std::fabs(uv(ip))) * dxuvinv);
+        mdt = std::min(mdt, (float)min_dt_ip);
+      } else {
+        q(ip) = (T)0;
+        uv(ip) = (T)0;
+        kfuv(ip) = 0;
+      }
+    }
+    min_dt = mdt;
+    for (long ic = 1; ic <= ncuv; ic++) {
+      q(cuv_index_uv(ic)) = (q(cuv_index_uv1(ic)) + q(cuv_index_uv2(ic))) / (T)2;
+      uv(cuv_index_uv(ic)) = (uv(cuv_index_uv1(ic)) + uv(cuv_index_uv2(ic))) / (T)2;
+    }
+  }
+
+  // compute_water_levels_regular: sfincs_continuity.f90:46-262
+  void compute_water_levels_regular(float dtt, double tt) {
+    for (long is = 1; is <= nsrc; is++) {
+      long nm = nmindsrc(is);
+      zs(nm) = (TZ)std::max((double)(zs(nm) + (TZ)(qtsrc(is) * dtt / cell_area(z_flags_iref(nm)))), (double)zb(nm));
+    }
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long nm = 1; nm <= np; nm++) {
+      if (kcs(nm) == 1) {
+        if (precip) zs(nm) = zs(nm) + (TZ)((T)netprcp(nm) * (T)dtt);
+        if (use_qext) zs(nm) = zs(nm) + (TZ)((T)qext(nm) * (T)dtt);
+        long nmd = z_index_uv_md(nm), nmu = z_index_uv_mu(nm), ndm = z_index_uv_nd(nm), num = z_index_uv_nu(nm);
+        int ir = z_flags_iref(nm);
+        T dz = ((q(nmd) - q(nmu)) * (T)dxrinv(ir) + (q(ndm) - q(num)) * (T)dyrinv(ir)) * (T)dtt;
+        zs(nm) = zs(nm) + (TZ)dz;
+      }
+      if (store_maximum_waterlevel) {
+        if (store_t_zsmax && zs(nm) > zsmax(nm) && (zs(nm) - zb(nm)) > huthresh) t_zsmax(nm) = (float)tt;
+        zsmax(nm) = (T)std::max((double)zsmax(nm), (double)zs(nm));
+      }
+    }
+  }
+
+  // compute_water_levels_subgrid: sfincs_continuity.f90:265-624
+  void compute_water_levels_subgrid(float dtt, double tt) {
+    for (long is = 1; is <= nsrc; is++) {
+      long nm = nmindsrc(is);
+      if (z_volume(nm) >= 0.0 || (qtsrc(is) < 0.0f && z_volume(nm) >= 0.0))
+        z_volume(nm) = z_volume(nm) + (TV)(qtsrc(is) * dtt);
+    }
+    const long L = subgrid_nlevels;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long nm = 1; nm <= np; nm++) {
+      T dvol = 0;
+      if (kcs(nm) == 1) {
+        long nmd = z_index_uv_md(nm), nmu = z_index_uv_mu(nm), ndm = z_index_uv_nd(nm), num = z_index_uv_nu(nm);
+        if (use_quadtree) {
+          int ir = z_flags_iref(nm);
+          dvol = dvol + ((q(nmd) - q(nmu)) * (T)dyrm(ir) + (q(ndm) - q(num)) * (T)dxrm(ir)) * (T)dtt;
+        } else {
+          dvol = dvol + ((q(nmd) - q(nmu)) * (T)dy + (q(ndm) - q(num)) * (T)dx) * (T)dtt;
+        }
+      }
+      if (kcs(nm) == 1 || kcs(nm) == 4) {
+        T a = cell_area(z_flags_iref(nm));
+        if (precip || use_qext) {
+          T dzsdt = 0;
+          if (precip) dzsdt = dzsdt + (T)netprcp(nm);
+          if (use_qext) dzsdt = dzsdt + (T)qext(nm);
+          dvol = dvol + dzsdt * a * (T)dtt;
+        }
+        z_volume(nm) = z_volume(nm) + (TV)dvol;
+        T zs00 = 0, zs11 = 0;
+        if (wiggle_suppression) {
+          zs00 = zs0(nm);
+          zs11 = (T)zs(nm);
+          zs0(nm) = zs11;
+        }
+        if (z_volume(nm) >= (TV)(sg_z_volmax(nm) * 0.999f)) {
+          zs(nm) = (TZ)((TV)std::max(sg_z_zmax(nm), -20.0f) + (z_volume(nm) - (TV)sg_z_volmax(nm)) / (TV)a);
+        } else if (z_volume(nm) <= (TV)1.0e-6f) {
+          zs(nm) = (TZ)std::max(sg_z_zmin(nm), -20.0f);
+        } else {
+          T dzvol = (T)sg_z_volmax(nm) / (T)(L - 1);
+          long iuv = (long)(z_volume(nm) / (TV)dzvol) + 1;
+          T facint = (T)((z_volume(nm) - (TV)((T)(iuv - 1) * dzvol)) / (TV)dzvol);
+          zs(nm) = (TZ)((T)sg_z_dep(iuv, nm) + ((T)sg_z_dep(iuv + 1, nm) - (T)sg_z_dep(iuv, nm)) * facint);
+        }
+        // zs is real*8 in the reference: zs - 2*zs11 + zs00 is evaluated in TZ precision
+        if (wiggle_suppression) zsderv(nm) = (T)(zs(nm) - (TZ)((T)2 * zs11) + (TZ)zs00);
+      }
+      if (store_maximum_waterlevel) {
+        if (store_t_zsmax && zs(nm) > zsmax(nm) && (zs(nm) - sg_z_zmin(nm)) > huthresh) t_zsmax(nm) = (float)tt;
+        zsmax(nm) = (T)std::max((double)zsmax(nm), (double)zs(nm));
+      }
+    }
+  }
+
+  // compute_store_variables: sfincs_continuity.f90:626-720
+  void compute_store_variables(float dtt) {
+    for (long nm = 1; nm <= np; nm++) {
+      T qz = 0, uvz = 0;
+      if (kcs(nm) == 1 || kcs(nm) == 4) {
+        long nmd = z_index_uv_md(nm), nmu = z_index_uv_mu(nm), ndm = z_index_uv_nd(nm), num = z_index_uv_nu(nm);
+        if (store_maximum_velocity) {
+          T quz = (uv(nmd) + uv(nmu)) / (T)2, qvz = (uv(ndm) + uv(num)) / (T)2;
+          uvz = std::sqrt(quz * quz + qvz * qvz);
+          vmax(nm) = std::max(vmax(nm), uvz);
+        }
+        if (store_maximum_flux) {
+          T quz = (q(nmd) + q(nmu)) / (T)2, qvz = (q(ndm) + q(num)) / (T)2;
+          qz = std::sqrt(quz * quz + qvz * qvz);
+          qmax(nm) = std::max(qmax(nm), qz);
+        }
+        if (store_twet) {
+          double base = subgrid ? (double)sg_z_zmin(nm) : (double)zb(nm);
+          if ((double)zs(nm) - base > (double)twet_threshold) twet(nm) = twet(nm) + (T)dtt;
+        }
+      }
+    }
+  }
+
+  // sfincs_update: sfincs_lib.f90:337-683 (output and optional processes elided)
+  int update(double dtrange, long max_steps = -1) {
+    double tend;
+    bool single = false;
+    if (dtrange < -999.0)
+      tend = t1;
+    else if (dtrange <= 0.0) {
+      tend = t1;
+      single = true;
+    } else
+      tend = t + dtrange;
+    long done = 0;
+    while (t < tend) {
+      if (max_steps >= 0 && done >= max_steps) break;
+      nt++;
+      dt = alfa * min_dt;
+      float dtchk = alfa * min_dt;
+      t = t + (double)dt;
+      dtavg = dtavg + dt;
+      if (wind || patmos || precip) {
+        update_meteo_forcing(t, dt);
+        if (infiltration) update_infiltration_map(dt);
+      }
+      if (boundaries_in_mask) {
+        if (nbnd > 0) update_boundary_points(t);
+        update_boundary_conditions(t);
+        update_boundary_fluxes(dt, t);
+      }
+      update_discharges(t);
+      compute_fluxes(dt);
+      if (subgrid)
+        compute_water_levels_subgrid(dt, t);
+      else
+        compute_water_levels_regular(dt, t);
+      if (store_maximum_velocity || store_maximum_flux || store_twet) compute_store_variables(dt);
+      if (dtchk < dtmin && nt > 1) {
+        error = 1;
+        t = (double)t1 + 1.0;
+      }
+      done++;
+      if (single) tend = t0;
+    }
+    return 0;
+  }
+};
+
+struct Handle {
+  std::string precision;
+  void* m = nullptr;
+  std::string err;
+};
+
+}  // namespace orc
+
+using namespace orc;
+using M64 = Model<double, double, double>;
+using MRef = Model<float, double, double>;
+using M32 = Model<float, float, double>;
+
+template <class Fn>
+static auto dispatch(Handle* h, Fn fn) {
+  if (h->precision == "fp64") return fn(*static_cast<M64*>(h->m));
+  if (h->precision == "ref") return fn(*static_cast<MRef*>(h->m));
+  return fn(*static_cast<M32*>(h->m));
+}
+
+template <class A, class X>
+static void copy_out(const F1<A>& a, X* out, long n) {
+  for (long i = 0; i < n; i++) out[i] = (X)a((long)i + 1);
+}
+
+static thread_local std::string g_last_error;
+
+extern "C" {
+
+// Create and initialise a model from <dir>/sfincs.inp.  precision: "fp64", "ref", "f32".
+// bmi != 0 mirrors the BMI initialize() (use_qext on).  Returns NULL on error.
+void* oracle_create(const char* dir, const char* precision, int bmi) {
+  auto* h = new Handle();
+  h->precision = precision;
+  try {
+    if (h->precision == "fp64") {
+      auto* m = new M64();
+      h->m = m;
+      m->initialize(dir, bmi != 0);
+    } else if (h->precision == "ref") {
+      auto* m = new MRef();
+      h->m = m;
+      m->initialize(dir, bmi != 0);
+    } else if (h->precision == "f32") {
+      auto* m = new M32();
+      h->m = m;
+      m->initialize(dir, bmi != 0);
+    } else {
+      throw std::runtime_error("unknown precision");
+    }
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return nullptr;
+  }
+  return h;
+}
+
+const char* oracle_last_error() { return g_last_error.c_str(); }
+
+void oracle_destroy(void* hv) {
+  auto* h = static_cast<Handle*>(hv);
+  if (!h) return;
+  dispatch(h, [&](auto& m) {
+    delete &m;
+    return 0;
+  });
+  delete h;
+}
+
+// sfincs_update(dtrange) semantics; max_steps < 0 means unbounded.  Returns steps taken.
+long oracle_update(void* hv, double dtrange, long max_steps) {
+  auto* h = static_cast<Handle*>(hv);
+  return dispatch(h, [&](auto& m) {
+    long n0 = m.nt;
+    m.update(dtrange, max_steps);
+    return m.nt - n0;
+  });
+}
+
+// Scalars: [t, dt, min_dt, t0, t1, nt, error, dtmax, dtmin, np, npuv, nkcuv2, ngbnd, subgrid, nlevels]
+void oracle_scalars(void* hv, double* out) {
+  auto* h = static_cast<Handle*>(hv);
+  dispatch(h, [&](auto& m) {
+    double v[] = {m.t, m.dt, m.min_dt, m.t0, m.t1, (double)m.nt, (double)m.error, m.dtmax, m.dtmin,
+                  (double)m.np, (double)m.npuv, (double)m.nkcuv2, (double)m.ngbnd, (double)m.subgrid,
+                  (double)m.subgrid_nlevels};
+    std::memcpy(out, v, sizeof(v));
+    return 0;
+  });
+}
+
+// Copy a named array to a double buffer of length n (cells: np, faces: npuv).
+// Names: zs zsmax z_volume zs0 zsderv zb kcs nm_n nm_m q uv kfuv kcuv uv_nm uv_nmu uv_dir netprcp qext
+int oracle_get(void* hv, const char* name, double* out, long n) {
+  auto* h = static_cast<Handle*>(hv);
+  std::string s(name);
+  return dispatch(h, [&](auto& m) -> int {
+    if (s == "zs") copy_out(m.zs, out, n);
+    else if (s == "zsmax" && m.zsmax.allocated()) copy_out(m.zsmax, out, n);
+    else if (s == "z_volume" && m.z_volume.allocated()) copy_out(m.z_volume, out, n);
+    else if (s == "zs0" && m.zs0.allocated()) copy_out(m.zs0, out, n);
+    else if (s == "zsderv" && m.zsderv.allocated()) copy_out(m.zsderv, out, n);
+    else if (s == "zb" && m.zb.allocated()) copy_out(m.zb, out, n);
+    else if (s == "kcs") copy_out(m.kcs, out, n);
+    else if (s == "nm_n") copy_out(m.z_index_z_n, out, n);
+    else if (s == "nm_m") copy_out(m.z_index_z_m, out, n);
+    else if (s == "q") copy_out(m.q, out, n);
+    else if (s == "uv") copy_out(m.uv, out, n);
+    else if (s == "kfuv") copy_out(m.kfuv, out, n);
+    else if (s == "kcuv") copy_out(m.kcuv, out, n);
+    else if (s == "mask_adv" && m.mask_adv.allocated()) copy_out(m.mask_adv, out, n);
+    else if (s == "uv_nm") copy_out(m.uv_index_z_nm, out, n);
+    else if (s == "uv_nmu") copy_out(m.uv_index_z_nmu, out, n);
+    else if (s == "uv_dir") copy_out(m.uv_flags_dir, out, n);
+    else if (s == "netprcp" && m.netprcp.allocated()) copy_out(m.netprcp, out, n);
+    else if (s == "qext" && m.qext.allocated()) copy_out(m.qext, out, n);
+    else if (s == "uvmean") copy_out(m.uvmean, out, n);
+    else return -1;
+    return 0;
+  });
+}
+
+// Overwrite a named state array from a double buffer (zs, q, uv, qext, zsmax, z_volume).
+int oracle_set(void* hv, const char* name, const double* in, long n) {
+  auto* h = static_cast<Handle*>(hv);
+  std::string s(name);
+  return dispatch(h, [&](auto& m) -> int {
+    using MT = std::remove_reference_t<decltype(m)>;
+    auto put = [&](auto& arr) {
+      using X = std::remove_reference_t<decltype(arr(1))>;
+      for (long i = 0; i < n; i++) arr((long)i + 1) = (X)in[i];
+    };
+    (void)sizeof(MT);
+    if (s == "zs") put(m.zs);
+    else if (s == "q") put(m.q);
+    else if (s == "uv") put(m.uv);
+    else if (s == "qext" && m.qext.allocated()) put(m.qext);
+    else if (s == "z_volume" && m.z_volume.allocated()) put(m.z_volume);
+    else return -1;
+    return 0;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,716 @@
+// C-ABI of libsfincs_gpu.so: the reference's BMI surface (sfincs_bmi.f90)
+// re-implemented over the B200 core, plus model and ensemble handles.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../../include/sfincs_bmi.h"
+#include "model.h"
+
+namespace sfg {
+void launch_gather_f32_f64(const float* src, const int32_t* cmp, double* out, long long n, cudaStream_t s);
+void launch_gather_f32(const float* src, const int32_t* cmp, float* out, long long n, cudaStream_t s);
+void launch_gather_f64(const double* src, const int32_t* cmp, double* out, long long n, cudaStream_t s);
+void launch_gather_u8(const uint8_t* src, const int32_t* cmp, float* out, long long n, cudaStream_t s);
+void launch_scatter_f32(const float* in, const int32_t* cmp, float* dst, long long n, cudaStream_t s);
+void launch_scatter_f64_f32(const double* in, const int32_t* cmp, float* dst, long long n, cudaStream_t s);
+int volume_parts(long long n);
+void launch_volume(const ScnDev* d_scn, const int32_t* cmp, long long n, double* part, double* out, cudaStream_t s);
+
+namespace {
+
+thread_local std::string g_err = "no error";
+
+// One model with its runner and data-interface staging buffers.
+struct ModelHandle {
+  std::unique_ptr<HostModel> host;
+  std::unique_ptr<DeviceModel> dev;
+  std::unique_ptr<Runner> runner;
+  void* d_stage = nullptr;  // 8*np bytes
+  double* d_part = nullptr;
+  double* d_vol = nullptr;
+  // BMI host mirrors (pinned)
+  double* h_zs = nullptr;
+  float* h_qext = nullptr;
+  bool zs_exported = false, qext_exported = false;
+
+  ModelHandle(const std::string& dir, bool bmi) {
+    host = load_model(dir, bmi);
+    dev = std::make_unique<DeviceModel>(*host);
+    runner = std::make_unique<Runner>(std::vector<DeviceModel*>{dev.get()});
+    const size_t np = (size_t)std::max<long long>(host->np, 1);
+    check_cuda(cudaMalloc(&d_stage, np * 8 * 2), "stage");
+    check_cuda(cudaMalloc(&d_part, (size_t)volume_parts((long long)np) * sizeof(double)), "parts");
+    check_cuda(cudaMalloc(&d_vol, sizeof(double)), "vol");
+    check_cuda(cudaMallocHost(&h_zs, np * sizeof(double)), "pinned zs");
+    check_cuda(cudaMallocHost(&h_qext, np * sizeof(float)), "pinned qext");
+    std::memset(h_qext, 0, np * sizeof(float));
+    refresh_zs();
+  }
+  ~ModelHandle() {
+    runner.reset();
+    dev.reset();
+    if (d_stage) cudaFree(d_stage);
+    if (d_part) cudaFree(d_part);
+    if (d_vol) cudaFree(d_vol);
+    if (h_zs) cudaFreeHost(h_zs);
+    if (h_qext) cudaFreeHost(h_qext);
+  }
+  long long np() const { return host->np; }
+  cudaStream_t s() const { return runner->stream(); }
+  int latest(const StepState& st) const { return st.run ? (st.parity ^ 1) : st.parity; }
+
+  void refresh_zs() {
+    launch_gather_f32_f64(dev->dev().zs, dev->d_cmp_off(), (double*)d_stage, np(), s());
+    check_cuda(cudaMemcpyAsync(h_zs, d_stage, (size_t)np() * 8, cudaMemcpyDeviceToHost, s()), "zs to host");
+    runner->sync();
+  }
+  void push_qext() {
+    if (!dev->dev().qext) return;
+    check_cuda(cudaMemcpyAsync(d_stage, h_qext, (size_t)np() * 4, cudaMemcpyHostToDevice, s()), "qext to device");
+    launch_scatter_f32((const float*)d_stage, dev->d_cmp_off(), const_cast<float*>(dev->dev().qext), np(), s());
+  }
+  void before_update() {
+    if (qext_exported) push_qext();
+  }
+  void after_update() {
+    if (zs_exported) refresh_zs();
+  }
+  void run(double tend, long long max_steps, int chunk) { runner->run({tend}, max_steps, chunk); }
+
+  void scalars(double* out) {
+    StepState st = runner->read_state(0);
+    const HostModel& h = *host;
+    double t = st.t;
+    if (st.stop_pending) t = h.t1 + 1.0;  // sfincs_lib.f90:646 takes effect at the end of the step
+    double v[19] = {t,
+                    st.dt,
+                    st.min_dt,
+                    (double)st.nt,
+                    (double)st.error,
+                    h.t0,
+                    h.t1,
+                    (double)h.np,
+                    (double)h.npuv,
+                    (double)h.p.nkcuv2,
+                    (double)h.p.ngbnd,
+                    (double)h.p.subgrid,
+                    st.bflux_vol,
+                    st.rain_vol * (double)h.n_kcs1,
+                    st.src_vol,
+                    h.p.dtmax,
+                    h.p.dtmin,
+                    (double)dev->bytes(),
+                    (double)runner->ntiles()};
+    std::memcpy(out, v, sizeof(v));
+  }
+
+  double volume() {
+    launch_volume(runner->d_scns(), dev->d_cmp_off(), np(), d_part, d_vol, s());
+    double v = 0.0;
+    check_cuda(cudaMemcpyAsync(&v, d_vol, sizeof(double), cudaMemcpyDeviceToHost, s()), "volume");
+    runner->sync();
+    return v;
+  }
+
+  void get(const std::string& name, void* dst, size_t bytes) {
+    const long long n = np();
+    ScnDev& D = dev->dev();
+    StepState st = runner->read_state(0);
+    const int p = latest(st);
+    auto need = [&](size_t b) {
+      if (bytes != b) throw std::runtime_error("get_var('" + name + "'): expected " + std::to_string(b) + " bytes");
+    };
+    auto f32 = [&](const float* src) {
+      need((size_t)n * 4);
+      launch_gather_f32(src, dev->d_cmp_off(), (float*)d_stage, n, s());
+      check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 4, cudaMemcpyDeviceToHost, s()), "get");
+    };
+    if (name == "zs") {
+      need((size_t)n * 8);
+      launch_gather_f32_f64(D.zs, dev->d_cmp_off(), (double*)d_stage, n, s());
+      check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 8, cudaMemcpyDeviceToHost, s()), "get");
+    } else if (name == "zsmax") {
+      f32(D.zsmax);
+    } else if (name == "qext") {
+      if (!D.qext) throw std::runtime_error("qext is not enabled for this model");
+      f32(D.qext);
+    } else if (name == "z_volume") {
+      if (!D.zvol) throw std::runtime_error("z_volume exists only for subgrid models");
+      need((size_t)n * 8);
+      launch_gather_f64(D.zvol, dev->d_cmp_off(), (double*)d_stage, n, s());
+      check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 8, cudaMemcpyDeviceToHost, s()), "get");
+    } else if (name == "qx") {
+      f32(D.qu[p]);
+    } else if (name == "qy") {
+      f32(D.qv[p]);
+    } else if (name == "uvx") {
+      f32(D.uu[p]);
+    } else if (name == "uvy") {
+      f32(D.vv[p]);
+    } else if (name == "zs0" && D.zs0) {
+      f32(D.zs0);
+    } else if (name == "zsderv" && D.zsderv) {
+      f32(D.zsderv);
+    } else if (name == "kfuv") {
+      need((size_t)n * 8);
+      launch_gather_u8(D.kfuv, dev->d_cmp_off(), (float*)d_stage, n, s());
+      check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 8, cudaMemcpyDeviceToHost, s()), "get");
+    } else {
+      throw std::runtime_error("unknown variable '" + name + "'");
+    }
+    runner->sync();
+  }
+
+  void set(const std::string& name, const void* src, size_t bytes) {
+    const long long n = np();
+    ScnDev& D = dev->dev();
+    StepState st = runner->read_state(0);
+    const int p = latest(st);
+    auto put32 = [&](float* dstp) {
+      if (bytes != (size_t)n * 4) throw std::runtime_error("set_var('" + name + "'): wrong size");
+      check_cuda(cudaMemcpyAsync(d_stage, src, bytes, cudaMemcpyHostToDevice, s()), "set");
+      launch_scatter_f32((const float*)d_stage, dev->d_cmp_off(), dstp, n, s());
+    };
+    if (name == "zs") {
+      if (bytes != (size_t)n * 8) throw std::runtime_error("set_var('zs'): wrong size");
+      check_cuda(cudaMemcpyAsync(d_stage, src, bytes, cudaMemcpyHostToDevice, s()), "set");
+      launch_scatter_f64_f32((const double*)d_stage, dev->d_cmp_off(), D.zs, n, s());
+    } else if (name == "qext") {
+      if (!D.qext) throw std::runtime_error("qext is not enabled for this model");
+      put32(const_cast<float*>(D.qext));
+      std::memcpy(h_qext, src, bytes);
+    } else if (name == "qx") {
+      put32(D.qu[p]);
+    } else if (name == "qy") {
+      put32(D.qv[p]);
+    } else if (name == "uvx") {
+      put32(D.uu[p]);
+    } else if (name == "uvy") {
+      put32(D.vv[p]);
+    } else {
+      throw std::runtime_error("variable '" + name + "' cannot be set");
+    }
+    runner->sync();
+    if (zs_exported && name == "zs") refresh_zs();
+  }
+
+  // find_quadtree_cell on a single-level grid (sfincs_quadtree.F90:764-820)
+  int cell_index(double xd, double yd) const {
+    const HostModel& h = *host;
+    const float x = (float)xd, y = (float)yd;
+    const float xt = h.cosrot * (x - h.x0) + h.sinrot * (y - h.y0);
+    const float yt = -h.sinrot * (x - h.x0) + h.cosrot * (y - h.y0);
+    const int n = (int)(yt / h.p.dy) + 1, m = (int)(xt / h.p.dx) + 1;
+    if (n < 1 || n > h.p.nmax || m < 1 || m > h.p.mmax) return 0;
+    const int32_t ic = h.dense2cmp[(size_t)m * h.p.ld + kGhostPad + n];
+    return ic < 0 ? 0 : ic + 1;
+  }
+
+  void update_zbuv() {
+    HostModel& h = *host;
+    if (h.p.subgrid) return;  // zbuvmx exists only for regular bathymetry
+    for (long long i = 0; i < h.np; i++) h.zb[h.cmp_off[i]] = h.zb_cmp[i];
+    const int ld = h.p.ld;
+    for (int m = 1; m <= h.p.mmax; m++)
+      for (int n = 1; n <= h.p.nmax; n++) {
+        const size_t c = (size_t)m * ld + kGhostPad + n;
+        if (!(h.flags[c] & F_ACT)) continue;
+        if (m < h.p.mmax && (h.flags[c + ld] & F_ACT)) h.zbmx_u[c] = std::max(h.zb[c], h.zb[c + ld]) + h.p.huthresh;
+        if (n < h.p.nmax && (h.flags[c + 1] & F_ACT)) h.zbmx_v[c] = std::max(h.zb[c], h.zb[c + 1]) + h.p.huthresh;
+      }
+    const size_t NA = (size_t)h.p.nalloc;
+    check_cuda(cudaMemcpy((void*)dev->dev().zb, h.zb.data(), NA * 4, cudaMemcpyHostToDevice), "zb");
+    check_cuda(cudaMemcpy((void*)dev->dev().zbmx_u, h.zbmx_u.data(), NA * 4, cudaMemcpyHostToDevice), "zbmx_u");
+    check_cuda(cudaMemcpy((void*)dev->dev().zbmx_v, h.zbmx_v.data(), NA * 4, cudaMemcpyHostToDevice), "zbmx_v");
+  }
+};
+
+struct EnsembleHandle {
+  std::vector<std::unique_ptr<HostModel>> hosts;
+  std::vector<std::unique_ptr<DeviceModel>> devs;
+  std::unique_ptr<Runner> runner;
+  void* d_stage = nullptr;
+  size_t stage_bytes = 0;
+};
+
+ModelHandle* g_bmi = nullptr;
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+void copy_err(char* err, int errlen, const std::string& msg) {
+  if (err && errlen > 0) {
+    std::strncpy(err, msg.c_str(), (size_t)errlen - 1);
+    err[errlen - 1] = 0;
+  }
+}
+
+int require_bmi() {
+  if (!g_bmi) throw std::runtime_error("model not initialized (call initialize first)");
+  return 0;
+}
+
+}  // namespace
+}  // namespace sfg
+
+using sfg::g_bmi;
+using sfg::g_err;
+using sfg::guarded;
+
+extern "C" {
+
+int BMI_LENVARADDRESS = 64;
+int BMI_LENVARTYPE = 64;
+int BMI_LENGRIDTYPE = 64;
+int BMI_LENCOMPONENTNAME = 64;
+int BMI_LENVERSION = 256;
+int BMI_LENERRMESSAGE = 1024;
+
+int initialize_config(const char* model_dir) {
+  return guarded([&] {
+    if (g_bmi) throw std::runtime_error("model already initialized (call finalize first)");
+    g_bmi = new sfg::ModelHandle(model_dir ? model_dir : ".", true);
+    return 0;
+  });
+}
+
+int initialize(void) { return initialize_config("."); }
+
+int update(void) {
+  return guarded([&] {
+    sfg::require_bmi();
+    g_bmi->before_update();
+    g_bmi->runner->step_once();
+    g_bmi->after_update();
+    return 0;
+  });
+}
+
+int update_until(double t_target) {
+  return guarded([&] {
+    sfg::require_bmi();
+    g_bmi->before_update();
+    g_bmi->run(t_target, -1, 32);
+    g_bmi->after_update();
+    return 0;
+  });
+}
+
+int finalize(void) {
+  int err = 0;
+  int rc = guarded([&] {
+    if (!g_bmi) return 0;
+    double s[19];
+    g_bmi->scalars(s);
+    err = (int)s[4];
+    delete g_bmi;
+    g_bmi = nullptr;
+    return 0;
+  });
+  return rc != 0 ? rc : err;
+}
+
+int get_value_ptr(const char* name, void** ptr) {
+  *ptr = nullptr;
+  return guarded([&]() -> int {
+    sfg::require_bmi();
+    std::string n(name);
+    sfg::HostModel& h = *g_bmi->host;
+    if (n == "z_xz")
+      *ptr = h.z_xz.data();
+    else if (n == "z_yz")
+      *ptr = h.z_yz.data();
+    else if (n == "zs") {
+      g_bmi->zs_exported = true;
+      g_bmi->refresh_zs();
+      *ptr = g_bmi->h_zs;
+    } else if (n == "zb" && !h.p.subgrid)
+      *ptr = h.zb_cmp.data();
+    else if (n == "subgrid_z_zmin" && h.p.subgrid)
+      *ptr = h.zmin_cmp.data();
+    else if (n == "qext" && h.p.use_qext) {
+      g_bmi->qext_exported = true;
+      *ptr = g_bmi->h_qext;
+    } else
+      return -1;
+    return 0;
+  });
+}
+
+int get_var_shape(const char* name, int shape[6]) {
+  for (int i = 0; i < 6; i++) shape[i] = 0;
+  return guarded([&]() -> int {
+    sfg::require_bmi();
+    std::string n(name);
+    if (n == "z_xz" || n == "z_yz" || n == "zs" || n == "zb" || n == "uorb" || n == "subgrid_z_zmin" || n == "qext" ||
+        n == "z_index_z_n" || n == "z_index_z_m") {
+      shape[0] = (int)g_bmi->np();
+      return 0;
+    }
+    return -1;
+  });
+}
+
+int get_var_type(const char* name, char* type) {
+  std::string n(name), t;
+  if (n == "z_xz" || n == "z_yz" || n == "zb" || n == "subgrid_z_zmin" || n == "qext" || n == "uorb")
+    t = "float";
+  else if (n == "zs")
+    t = "double";
+  else if (n == "z_index_z_n" || n == "z_index_z_m")
+    t = "integer";
+  else {
+    if (type) type[0] = 0;
+    return -1;
+  }
+  std::strcpy(type, t.c_str());
+  return 0;
+}
+
+int get_var_rank(const char* name, int* rank) {
+  std::string n(name);
+  if (n == "z_xz" || n == "z_yz" || n == "zs" || n == "zb" || n == "subgrid_z_zmin" || n == "qext" || n == "uorb") {
+    *rank = 1;
+    return 0;
+  }
+  return -1;
+}
+
+int set_logical(const char* name, const int* value) {
+  return guarded([&]() -> int {
+    sfg::require_bmi();
+    if (std::string(name) != "qext") return -1;
+    const bool on = value[0] != 0;
+    sfg::ScnDev& D = g_bmi->dev->dev();
+    if (on && !D.qext) throw std::runtime_error("qext array was not allocated for this model");
+    D.use_qext = on ? 1 : 0;
+    g_bmi->runner->refresh_params();
+    return 0;
+  });
+}
+
+int get_start_time(double* t) {
+  return guarded([&] {
+    sfg::require_bmi();
+    *t = g_bmi->host->t0;
+    return 0;
+  });
+}
+int get_end_time(double* t) {
+  return guarded([&] {
+    sfg::require_bmi();
+    *t = g_bmi->host->t1;
+    return 0;
+  });
+}
+int get_time_step(double* dt) {
+  return guarded([&] {
+    sfg::require_bmi();
+    double s[19];
+    g_bmi->scalars(s);
+    *dt = s[1];
+    return 0;
+  });
+}
+int get_current_time(double* t) {
+  return guarded([&] {
+    sfg::require_bmi();
+    double s[19];
+    g_bmi->scalars(s);
+    *t = s[0];
+    return 0;
+  });
+}
+
+int update_zbuv(void) {
+  return guarded([&] {
+    sfg::require_bmi();
+    g_bmi->update_zbuv();
+    return 0;
+  });
+}
+
+int update_apparent_roughness(void) { return 0; }
+
+int get_sfincs_cell_index(const double* x, const double* y, int* index) {
+  return guarded([&] {
+    sfg::require_bmi();
+    *index = g_bmi->cell_index(*x, *y);
+    return 0;
+  });
+}
+
+int get_sfincs_cell_indices(const double* x, const double* y, int* index, int n) {
+  return guarded([&] {
+    sfg::require_bmi();
+    for (int i = 0; i < n; i++) index[i] = g_bmi->cell_index(x[i], y[i]);
+    return 0;
+  });
+}
+
+int get_sfincs_cell_area(const int* index, double* area) {
+  return guarded([&] {
+    sfg::require_bmi();
+    if (*index < 1 || *index > g_bmi->np()) throw std::runtime_error("cell index out of range");
+    *area = (double)g_bmi->host->p.area;
+    return 0;
+  });
+}
+
+int get_last_bmi_error(char* msg) {
+  sfg::copy_err(msg, BMI_LENERRMESSAGE, g_err);
+  return 0;
+}
+
+int get_var(const char* name, void* dst, size_t bytes) {
+  return guarded([&] {
+    sfg::require_bmi();
+    g_bmi->get(name, dst, bytes);
+    return 0;
+  });
+}
+
+int set_var(const char* name, const void* src, size_t bytes) {
+  return guarded([&] {
+    sfg::require_bmi();
+    g_bmi->set(name, src, bytes);
+    return 0;
+  });
+}
+
+// ---------------------------------------------------------------- model handles
+void* sfg_model_create(const char* model_dir, int bmi, char* err, int errlen) {
+  try {
+    return new sfg::ModelHandle(model_dir, bmi != 0);
+  } catch (std::exception& e) {
+    sfg::copy_err(err, errlen, e.what());
+    g_err = e.what();
+    return nullptr;
+  }
+}
+void sfg_model_destroy(void* m) { delete static_cast<sfg::ModelHandle*>(m); }
+int sfg_model_run(void* m, double t_end, long long max_steps, int chunk) {
+  return guarded([&] {
+    auto* h = static_cast<sfg::ModelHandle*>(m);
+    h->run(t_end, max_steps, chunk > 0 ? chunk : 32);
+    return 0;
+  });
+}
+int sfg_model_issue(void* m, int nsteps) {
+  return guarded([&] {
+    auto* h = static_cast<sfg::ModelHandle*>(m);
+    // unbounded target so that issued steps always execute
+    const double big = 1.0e300;
+    const int left = -1;
+    sfg::check_cuda(cudaMemcpyAsync(&h->dev->state()->tend, &big, 8, cudaMemcpyHostToDevice, h->s()), "tend");
+    sfg::check_cuda(cudaMemcpyAsync(&h->dev->state()->steps_left, &left, 4, cudaMemcpyHostToDevice, h->s()), "left");
+    h->runner->issue(nsteps);
+    sfg::check_cuda(cudaGetLastError(), "issue");
+    return 0;
+  });
+}
+int sfg_model_sync(void* m) {
+  return guarded([&] {
+    static_cast<sfg::ModelHandle*>(m)->runner->sync();
+    return 0;
+  });
+}
+int sfg_model_scalars(void* m, double out[19]) {
+  return guarded([&] {
+    static_cast<sfg::ModelHandle*>(m)->scalars(out);
+    return 0;
+  });
+}
+int sfg_model_get(void* m, const char* name, void* dst, size_t bytes) {
+  return guarded([&] {
+    static_cast<sfg::ModelHandle*>(m)->get(name, dst, bytes);
+    return 0;
+  });
+}
+int sfg_model_set(void* m, const char* name, const void* src, size_t bytes) {
+  return guarded([&] {
+    static_cast<sfg::ModelHandle*>(m)->set(name, src, bytes);
+    return 0;
+  });
+}
+int sfg_model_volume(void* m, double* v) {
+  return guarded([&] {
+    *v = static_cast<sfg::ModelHandle*>(m)->volume();
+    return 0;
+  });
+}
+void* sfg_model_stream(void* m) { return (void*)static_cast<sfg::ModelHandle*>(m)->s(); }
+
+// ---------------------------------------------------------------- ensembles
+void* sfg_ensemble_create(const char* const* dirs, int n, int bmi, char* err, int errlen) {
+  auto* e = new sfg::EnsembleHandle();
+  try {
+    std::vector<sfg::DeviceModel*> ptrs;
+    size_t maxnp = 1;
+    for (int i = 0; i < n; i++) {
+      e->hosts.push_back(sfg::load_model(dirs[i], bmi != 0));
+      e->devs.push_back(std::make_unique<sfg::DeviceModel>(*e->hosts.back()));
+      ptrs.push_back(e->devs.back().get());
+      maxnp = std::max(maxnp, (size_t)e->hosts.back()->np);
+    }
+    e->runner = std::make_unique<sfg::Runner>(ptrs);
+    e->stage_bytes = maxnp * 8 * 2;
+    sfg::check_cuda(cudaMalloc(&e->d_stage, e->stage_bytes), "stage");
+    return e;
+  } catch (std::exception& ex) {
+    sfg::copy_err(err, errlen, ex.what());
+    g_err = ex.what();
+    e->runner.reset();
+    e->devs.clear();
+    delete e;
+    return nullptr;
+  }
+}
+void sfg_ensemble_destroy(void* ev) {
+  auto* e = static_cast<sfg::EnsembleHandle*>(ev);
+  if (!e) return;
+  e->runner.reset();
+  e->devs.clear();
+  if (e->d_stage) cudaFree(e->d_stage);
+  delete e;
+}
+int sfg_ensemble_run(void* ev, const double* t_end, long long max_steps, int chunk) {
+  return guarded([&] {
+    auto* e = static_cast<sfg::EnsembleHandle*>(ev);
+    std::vector<double> te(t_end, t_end + e->devs.size());
+    e->runner->run(te, max_steps, chunk > 0 ? chunk : 32);
+    return 0;
+  });
+}
+int sfg_ensemble_issue(void* ev, int nsteps) {
+  return guarded([&] {
+    auto* e = static_cast<sfg::EnsembleHandle*>(ev);
+    const double big = 1.0e300;
+    const int left = -1;
+    for (auto& d : e->devs) {
+      sfg::check_cuda(cudaMemcpyAsync(&d->state()->tend, &big, 8, cudaMemcpyHostToDevice, e->runner->stream()), "tend");
+      sfg::check_cuda(cudaMemcpyAsync(&d->state()->steps_left, &left, 4, cudaMemcpyHostToDevice, e->runner->stream()),
+                      "left");
+    }
+    e->runner->issue(nsteps);
+    sfg::check_cuda(cudaGetLastError(), "issue");
+    return 0;
+  });
+}
+int sfg_ensemble_sync(void* ev) {
+  return guarded([&] {
+    static_cast<sfg::EnsembleHandle*>(ev)->runner->sync();
+    return 0;
+  });
+}
+int sfg_ensemble_scalars(void* ev, int i, double out[19]) {
+  return guarded([&] {
+    auto* e = static_cast<sfg::EnsembleHandle*>(ev);
+    if (i < 0 || i >= (int)e->devs.size()) throw std::runtime_error("member index out of range");
+    sfg::StepState st = e->runner->read_state(i);
+    const sfg::HostModel& h = *e->hosts[i];
+    double t = st.stop_pending ? h.t1 + 1.0 : st.t;
+    double v[19] = {t, st.dt, st.min_dt, (double)st.nt, (double)st.error, h.t0, h.t1, (double)h.np, (double)h.npuv,
+                    (double)h.p.nkcuv2, (double)h.p.ngbnd, (double)h.p.subgrid, st.bflux_vol,
+                    st.rain_vol * (double)h.n_kcs1, st.src_vol, h.p.dtmax, h.p.dtmin, (double)e->devs[i]->bytes(),
+                    (double)e->runner->ntiles()};
+    std::memcpy(out, v, sizeof(v));
+    return 0;
+  });
+}
+int sfg_ensemble_get(void* ev, int i, const char* name, void* dst, size_t bytes) {
+  return guarded([&] {
+    auto* e = static_cast<sfg::EnsembleHandle*>(ev);
+    if (i < 0 || i >= (int)e->devs.size()) throw std::runtime_error("member index out of range");
+    sfg::DeviceModel& d = *e->devs[i];
+    const long long n = e->hosts[i]->np;
+    sfg::StepState st = e->runner->read_state(i);
+    const int p = st.run ? (st.parity ^ 1) : st.parity;
+    std::string nm(name);
+    cudaStream_t s = e->runner->stream();
+    if (nm == "zs") {
+      if (bytes != (size_t)n * 8) throw std::runtime_error("wrong size for zs");
+      sfg::launch_gather_f32_f64(d.dev().zs, d.d_cmp_off(), (double*)e->d_stage, n, s);
+    } else {
+      const float* src = nullptr;
+      if (nm == "zsmax") src = d.dev().zsmax;
+      else if (nm == "qx") src = d.dev().qu[p];
+      else if (nm == "qy") src = d.dev().qv[p];
+      else if (nm == "uvx") src = d.dev().uu[p];
+      else if (nm == "uvy") src = d.dev().vv[p];
+      else throw std::runtime_error("unknown ensemble variable " + nm);
+      if (bytes != (size_t)n * 4) throw std::runtime_error("wrong size for " + nm);
+      sfg::launch_gather_f32(src, d.d_cmp_off(), (float*)e->d_stage, n, s);
+    }
+    sfg::check_cuda(cudaMemcpyAsync(dst, e->d_stage, bytes, cudaMemcpyDeviceToHost, s), "get");
+    e->runner->sync();
+    return 0;
+  });
+}
+void* sfg_ensemble_stream(void* ev) { return (void*)static_cast<sfg::EnsembleHandle*>(ev)->runner->stream(); }
+
+int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst, size_t n) {
+  return guarded([&]() -> int {
+    auto H = sfg::load_model(model_dir, bmi != 0);
+    const sfg::HostModel& h = *H;
+    const std::string nm(name);
+    std::vector<double> out;
+    const size_t NA = (size_t)h.p.nalloc;
+    auto per_cell = [&](auto get) {
+      out.resize((size_t)h.np);
+      for (long long i = 0; i < h.np; i++) out[i] = (double)get((size_t)h.cmp_off[i]);
+    };
+    if (nm == "counts") {
+      out = {(double)h.np, (double)h.npuv, (double)h.p.ngbnd, (double)h.p.nkcuv2, (double)h.p.nlev, (double)NA,
+             (double)h.p.dtmax, (double)h.p.dtmin};
+    } else if (nm == "flags") {
+      per_cell([&](size_t c) { return h.flags[c]; });
+    } else if (nm == "zs") {
+      per_cell([&](size_t c) { return h.zs[c]; });
+    } else if (nm == "zvol") {
+      if (h.zvol.empty()) return -1;
+      per_cell([&](size_t c) { return h.zvol[c]; });
+    } else if (nm == "zbmx" || nm == "gn2") {
+      const auto& u = nm == "zbmx" ? h.zbmx_u : h.gn2_u;
+      const auto& v = nm == "zbmx" ? h.zbmx_v : h.gn2_v;
+      if (u.empty()) return -1;
+      out.resize((size_t)h.np * 2);
+      for (long long i = 0; i < h.np; i++) {
+        out[i] = u[h.cmp_off[i]];
+        out[h.np + i] = v[h.cmp_off[i]];
+      }
+    } else if (nm == "gb_cell") {
+      for (auto c : h.gb_cell) out.push_back((double)h.dense2cmp[c]);
+    } else if (nm == "gb_fac") {
+      for (auto f : h.gb_fac) out.push_back(f);
+    } else if (nm == "kb_cell") {
+      for (auto c : h.kb_face) out.push_back((double)h.dense2cmp[c]);
+    } else if (nm == "kb_dir") {
+      for (auto d : h.kb_dir) out.push_back(d);
+    } else if (nm == "kb_sign") {
+      for (auto d : h.kb_sign) out.push_back(d);
+    } else {
+      return -1;
+    }
+    if (out.size() != n) throw std::runtime_error("sfg_layout_get(" + nm + "): size is " + std::to_string(out.size()));
+    std::memcpy(dst, out.data(), n * sizeof(double));
+    return 0;
+  });
+}
+
+}  // extern "C"

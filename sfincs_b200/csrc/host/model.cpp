@@ -1,0 +1,898 @@
+// Model loading (reference input files -> dense B200 layout), device
+// residency and the CUDA-graph step runner.
+#include "model.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+
+#include "inputs.h"
+
+namespace sfg {
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static bool is_none(const std::string& s) { return s.size() >= 4 && s.compare(0, 4, "none") == 0; }
+
+// ============================================================================
+// load_model
+// ============================================================================
+std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
+  auto H = std::make_unique<HostModel>();
+  HostModel& h = *H;
+  ScnDev& P = h.p;
+  h.dir = dir;
+  auto path = [&](const std::string& f) { return dir + "/" + f; };
+  InpFile in(path("sfincs.inp"));
+
+  // ---- keywords and defaults (sfincs_input.f90:50-343) ----------------------
+  const int mmax = in.integer("mmax", 0), nmax = in.integer("nmax", 0);
+  const float dx = in.real("dx", 0.0f), dy = in.real("dy", 0.0f);
+  const float x0 = in.real("x0", 0.0f), y0 = in.real("y0", 0.0f);
+  float rotation = in.real("rotation", 0.0f);
+  std::string tref = in.str("tref", "none"), tstart = in.str("tstart", "20000101 000000"),
+              tstop = in.str("tstop", "20000101 000000");
+  float tspinup = in.real("tspinup", 0.0f);
+  const float dtmaxout = in.real("dtmaxout", 9999999.0f);
+  P.alfa = in.real("alpha", 0.50f);
+  P.theta = in.real("theta", 1.0f);
+  const float hmin_cfl = in.real("hmin_cfl", 0.1f);
+  const float manning = in.real("manning", 0.04f), manning_land = in.real("manning_land", -999.0f),
+              manning_sea = in.real("manning_sea", -999.0f), rghlevland = in.real("rgh_lev_land", 0.0f);
+  P.zini = in.real("zsini", 0.0f);
+  float qinf = in.real("qinf", 0.0f);
+  float dtmax = in.real("dtmax", 60.0f);
+  P.huthresh = in.real("huthresh", 0.05f);
+  P.huvmin = in.real("huvmin", 0.0f);
+  P.rhoa = in.real("rhoa", 1.25f);
+  P.rhow = in.real("rhow", 1024.0f);
+  const std::string inputtype = in.str("inputformat", "bin");
+  const int bndtype = in.integer("bndtype", 1);
+  const int iadvection = in.integer("advection", 1);
+  const float latitude = in.real("latitude", 0.0f);
+  P.advlim = in.real("advlim", 1.0f);
+  P.slopelim = in.real("slopelim", 9999.9f);
+  const float qinf_zmin = in.real("qinf_zmin", 0.0f);
+  P.btfilter = in.real("btfilter", 60.0f);
+  const int igeo = in.integer("crsgeo", 0);
+  bool coriolis = in.logical("coriolis", true);
+  const float nuviscdim = in.real("nuvisc", 0.01f);
+  const bool viscosity = in.logical("viscosity", false);
+  const std::string advstr = in.str("advection_scheme", "upw1");
+  P.btrelax = in.real("btrelax", 3600.0f);
+  const bool wiggle = in.logical("wiggle_suppression", true);
+  P.wiggle_factor = in.real("wiggle_factor", 0.1f);
+  P.wiggle_threshold = in.real("wiggle_threshold", 0.1f);
+  P.uvlim = in.real("uvlim", 10.0f);
+  const float uvmax = in.real("uvmax", 1000.0f);
+  const bool friction2d = in.logical("friction2d", true);
+  const bool advection_mask = in.logical("advection_mask", true);
+  P.nuviscfac = in.real("nuviscfac", 100.0f);
+  if (in.logical("h73table", false)) throw std::runtime_error("h73table is not supported by this core");
+  const std::string qtrfile = in.str("qtrfile", "none"), depfile = in.str("depfile", "none"),
+                    inifile = in.str("inifile", "none"), rstfile = in.str("rstfile", "none"),
+                    mskfile = in.str("mskfile", "none"), indexfile = in.str("indexfile", "none"),
+                    sbgfile = in.str("sbgfile", "none"), manningfile = in.str("manningfile", "none"),
+                    bndfile = in.str("bndfile", "none"), bzsfile = in.str("bzsfile", "none"),
+                    srcfile = in.str("srcfile", "none"), disfile = in.str("disfile", "none"),
+                    wndfile = in.str("wndfile", "none"), qinffile = in.str("qinffile", "none");
+  std::string prcpfile = in.str("prcfile", "none");
+  if (is_none(prcpfile)) prcpfile = in.str("precipfile", "none");
+  // Inputs outside this core's path: refuse loudly instead of silently ignoring physics.
+  for (const char* k : {"bcafile", "bzifile", "bdrfile", "thdfile", "weirfile", "drnfile", "volfile", "spwfile",
+                        "amufile", "amvfile", "ampfile", "amprfile", "netbndbzsbzifile", "netsrcdisfile",
+                        "netamuamvfile", "netamprfile", "netampfile", "netspwfile", "infiltration_file",
+                        "scsfile", "sefffile", "psifile", "f0file", "wavemaker_wvmfile", "wvmfile"}) {
+    if (!is_none(in.str(k, "none"))) throw std::runtime_error(std::string("input '") + k + "' is not supported by this core");
+  }
+  for (const char* k : {"snapwave", "nonh", "bathtub", "vegetation"})
+    if (in.logical(k, false) || in.integer(k, 0) != 0)
+      throw std::runtime_error(std::string("process '") + k + "' is not supported by this core");
+  if (!is_none(qtrfile)) throw std::runtime_error("quadtree meshes (qtrfile) are not supported by this core yet");
+  if (!is_none(inifile) || !is_none(rstfile)) throw std::runtime_error("inifile/rstfile are not supported by this core yet");
+  if (igeo != 0) throw std::runtime_error("geographic grids (crsgeo=1) are not supported by this core");
+  if (inputtype != "bin") throw std::runtime_error("only inputformat = bin is supported");
+  if (bndtype != 1) throw std::runtime_error("only bndtype = 1 is supported");
+  if (nmax <= 0 || mmax <= 0) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
+
+  // ---- derived (sfincs_input.f90:347-745) ------------------------------------
+  if (is_none(tref)) tref = tstart;
+  const float t0 = (float)(seconds_between(tref, tstart) * 1.0);
+  const float t1 = (float)(seconds_between(tref, tstop) * 1.0);
+  tspinup = t0 + tspinup;
+  P.g = 9.81f;
+  P.pi = 3.14159f;
+  qinf = qinf / (float)(3600 * 1000);
+  rotation = rotation * P.pi / 180.0f;
+  const float cosrot = std::cos(rotation), sinrot = std::sin(rotation);
+  P.fcorio = 2.0f * 7.2921e-05f * std::sin(latitude * P.pi / 180.0f);
+  if (latitude < 0.01f && latitude > -0.01f) coriolis = false;
+  P.coriolis = coriolis;
+  P.store_zsmax = dtmaxout > 0.0f;
+  h.store_vmax = in.integer("storevelmax", 0) == 1 && dtmaxout > 0.0f;
+  h.store_qmax = in.integer("storefluxmax", 0) == 1 && dtmaxout > 0.0f;
+  h.store_twet = in.integer("storetwet", 0) == 1;
+  P.subgrid = !is_none(sbgfile);
+  P.advection = iadvection > 0;
+  P.adv_scheme = 1;
+  if (P.advection && advstr == "original") P.adv_scheme = 0;
+  P.thetasmooth = P.theta < 0.9999f;
+  P.viscosity = viscosity;
+  P.friction2d = friction2d;
+  P.wiggle = wiggle;
+  P.wind = !is_none(wndfile);
+  P.precip = !is_none(prcpfile);
+  P.use_qext = bmi;
+  P.t0 = t0;
+  P.t1 = t1;
+  P.tspinup = tspinup;
+  h.t0 = t0;
+  h.t1 = t1;
+  if (P.subgrid) P.huthresh = 0.0f;  // sfincs_subgrid.F90:40 (netCDF tables)
+
+  // ---- mesh: index + mask files (sfincs_domain.f90:250-482) -------------------
+  const long long n_idx = read_binary<int32_t>(path(indexfile), 1)[0];
+  auto idx = read_binary<int32_t>(path(indexfile), (size_t)n_idx, 4);
+  auto msk_idx = read_binary<int8_t>(path(mskfile), (size_t)n_idx);
+  P.nmax = nmax;
+  P.mmax = mmax;
+  const int ld = ((nmax + 1 + kGhostPad + 1) + 31) / 32 * 32;
+  P.ld = ld;
+  P.nalloc = (int64_t)(mmax + 2) * ld;
+  P.dx = dx;
+  P.dy = dy;
+  const size_t NA = (size_t)P.nalloc;
+  auto OFF = [&](int n, int m) -> int64_t { return (int64_t)m * ld + kGhostPad + n; };
+  std::vector<int8_t> kcs(NA, 0);
+  std::vector<int32_t> cmp_of(NA, -1);  // dense -> compact index (0-based)
+  for (long long i = 0; i < n_idx; i++) {
+    if (msk_idx[i] <= 0) continue;
+    const int m = (idx[i] - 1) / nmax + 1;
+    const int n = idx[i] - (m - 1) * nmax;
+    if (m < 1 || m > mmax || n < 1 || n > nmax) throw std::runtime_error("index file entry outside the grid");
+    const int64_t c = OFF(n, m);
+    kcs[c] = msk_idx[i];
+    cmp_of[c] = (int32_t)h.cmp_off.size();
+    h.cmp_off.push_back((int32_t)c);
+    h.z_n.push_back(n);
+    h.z_m.push_back(m);
+  }
+  h.np = (long long)h.cmp_off.size();
+  for (int8_t k : kcs)
+    if (k == 4 || k == 5) throw std::runtime_error("msk values 4/5 (wave makers, downstream river) are not supported");
+  auto act = [&](int n, int m) { return n >= 1 && n <= nmax && m >= 1 && m <= mmax && kcs[OFF(n, m)] > 0; };
+
+  // ---- geometry (sfincs_domain.f90:1369-1541, projected, one level) -----------
+  P.dxinv = 1.0f / dx;
+  P.dyinv = 1.0f / dy;
+  P.dx2inv = P.dxinv * P.dxinv;
+  P.dy2inv = P.dyinv * P.dyinv;
+  P.area = dx * dy;
+  P.nref = 1;
+  float dxymin = 1.0e6f;
+  dxymin = std::min(dxymin, dx);
+  dxymin = std::min(dxymin, dy);
+  P.dtmax = std::min(dtmax, P.alfa * dxymin / (std::sqrt(9.81f * hmin_cfl)));
+  P.dtmin = P.alfa * dxymin / (1.25f * std::fabs(uvmax));
+  P.nuvisc = viscosity ? std::max(nuviscdim * std::min(dx, dy), 0.0f) : 0.0f;
+  h.z_xz.resize(h.np);
+  h.z_yz.resize(h.np);
+  for (long long i = 0; i < h.np; i++) {
+    const float n = (float)h.z_n[i], m = (float)h.z_m[i];
+    h.z_xz[i] = x0 + cosrot * (1.0f * (m - 0.5f)) * dx - sinrot * (1.0f * (n - 0.5f)) * dy;
+    h.z_yz[i] = y0 + sinrot * (1.0f * (m - 0.5f)) * dx + cosrot * (1.0f * (n - 0.5f)) * dy;
+  }
+
+  // ---- faces and their reference order (sfincs_domain.f90:727-1003) ----------
+  // kcu/kcv: kcuv of the u/v face owned by each dense cell (0 where no face).
+  std::vector<int8_t> kcu(NA, 0), kcv(NA, 0);
+  std::vector<int64_t> face_off;  // compact face ip-1 -> dense offset
+  std::vector<int8_t> face_dir;
+  auto kcuv_of = [&](int a, int b) -> int8_t {  // sfincs_domain.f90:1833-1884
+    if (a > 1 && b > 1) return 0;
+    if (a * b == 0) return 0;
+    if ((a == 1 && b == 2) || (a == 2 && b == 1)) return 2;
+    if ((a == 1 && b == 3) || (a == 3 && b == 1)) return 2;
+    if ((a == 1 && b == 5) || (a == 5 && b == 1)) return 2;
+    if ((a == 1 && b == 6) || (a == 6 && b == 1)) return 6;
+    return 1;
+  };
+  for (long long i = 0; i < h.np; i++) {
+    const int n = h.z_n[i], m = h.z_m[i];
+    const int64_t c = OFF(n, m);
+    if (act(n, m + 1)) {
+      face_off.push_back(c);
+      face_dir.push_back(0);
+      kcu[c] = kcuv_of(kcs[c], kcs[OFF(n, m + 1)]);
+    }
+    if (act(n + 1, m)) {
+      face_off.push_back(c);
+      face_dir.push_back(1);
+      kcv[c] = kcuv_of(kcs[c], kcs[OFF(n + 1, m)]);
+    }
+  }
+  h.npuv = (long long)face_off.size();
+
+  // ---- bathymetry (regular) or subgrid tables -----------------------------------
+  std::vector<float> sg_level_raw;  // z_level as read, [np][levels]
+  h.zb_cmp.assign(h.np, 0.0f);
+  h.zmin_cmp.assign(h.np, 0.0f);
+  if (!P.subgrid) {
+    auto zbc = read_binary<float>(path(depfile), (size_t)h.np);
+    h.zb.assign(NA, 0.0f);
+    for (long long i = 0; i < h.np; i++) {
+      h.zb[h.cmp_off[i]] = zbc[i];
+      h.zb_cmp[i] = zbc[i];
+    }
+    h.zbmx_u.assign(NA, 0.0f);
+    h.zbmx_v.assign(NA, 0.0f);
+    for (size_t f = 0; f < face_off.size(); f++) {
+      const int64_t c = face_off[f];
+      const int64_t cu = face_dir[f] == 0 ? c + ld : c + 1;
+      (face_dir[f] == 0 ? h.zbmx_u : h.zbmx_v)[c] = std::max(h.zb[c], h.zb[cu]) + P.huthresh;
+    }
+  } else {
+    NcFile nc(path(sbgfile));
+    const int L = (int)nc.dim("levels");
+    if (L < 2) throw std::runtime_error("subgrid tables need at least two levels");
+    P.nlev = L;
+    auto zmin = nc.floats("z_zmin"), zmax = nc.floats("z_zmax"), volmax = nc.floats("z_volmax"),
+         zlev = nc.floats("z_level"), uzmin = nc.floats("uv_zmin"), uzmax = nc.floats("uv_zmax"),
+         uffit = nc.floats("uv_ffit"), unavg = nc.floats("uv_navg"), uhavg = nc.floats("uv_havg"),
+         unrep = nc.floats("uv_nrep"), upwet = nc.floats("uv_pwet");
+    if ((long long)zmin.size() != h.np || (long long)uzmin.size() != h.npuv)
+      throw std::runtime_error("subgrid file dimensions do not match the mesh (np/npuv)");
+    sg_level_raw = zlev;
+    // sfincs_subgrid.F90:276-446: read, convert n -> g n^2, and condition the tables
+    for (long long f = 0; f < h.npuv; f++) uzmax[f] = std::max(uzmax[f], uzmin[f] + 0.01f);
+    for (long long f = 0; f < h.npuv; f++) {
+      const int64_t c = face_off[f];
+      const int64_t cu = face_dir[f] == 0 ? c + ld : c + 1;
+      const float zn = zmin[cmp_of[c]], znu = zmin[cmp_of[cu]];
+      if (zn > uzmin[f]) {
+        uzmin[f] = std::max(uzmin[f], zn);
+        uzmax[f] = std::max(uzmax[f], uzmin[f] + 0.01f);
+      }
+      if (znu > uzmin[f]) {
+        uzmin[f] = std::max(uzmin[f], znu);
+        uzmax[f] = std::max(uzmax[f], uzmin[f] + 0.01f);
+      }
+    }
+    for (long long i = 0; i < h.np; i++)
+      if (zmax[i] - zmin[i] <= 0.0f) zmax[i] = zmax[i] + 0.01f;
+    for (long long f = 0; f < h.npuv; f++)
+      if (uzmax[f] - uzmin[f] < 1.0e-7f) uzmax[f] = uzmax[f] + 0.01f;
+    h.zz_min.assign(NA, 0.0f);
+    h.zz_max.assign(NA, 0.0f);
+    h.zz_volmax.assign(NA, 0.0f);
+    h.zlev.assign((size_t)(L - 1) * NA, make_float2(0.0f, 0.0f));
+    for (long long i = 0; i < h.np; i++) {
+      const int64_t c = h.cmp_off[i];
+      h.zz_min[c] = zmin[i];
+      h.zz_max[c] = zmax[i];
+      h.zz_volmax[c] = volmax[i];
+      h.zmin_cmp[i] = zmin[i];
+      for (int k = 0; k < L - 1; k++) {
+        const float a = zlev[(size_t)i * L + k], b = zlev[(size_t)i * L + k + 1];
+        h.zlev[(size_t)k * NA + c] = make_float2(a, b - a);
+      }
+    }
+    h.sgz_u.assign(NA, make_float2(0, 0));
+    h.sgz_v.assign(NA, make_float2(0, 0));
+    h.sgw_u.assign(NA, make_float4(0, 0, 0, 0));
+    h.sgw_v.assign(NA, make_float4(0, 0, 0, 0));
+    h.rec_u.assign((size_t)(L - 1) * NA, UvRec{});
+    h.rec_v.assign((size_t)(L - 1) * NA, UvRec{});
+    std::vector<float> hv(L), nv(L), pv(L);
+    for (long long f = 0; f < h.npuv; f++) {
+      const int64_t c = face_off[f];
+      const bool isu = face_dir[f] == 0;
+      for (int k = 0; k < L; k++) {
+        hv[k] = uhavg[(size_t)f * L + k];
+        const float nr = std::max(unrep[(size_t)f * L + k], 0.0001f);
+        nv[k] = P.g * (nr * nr);
+        pv[k] = upwet[(size_t)f * L + k];
+      }
+      const float na = std::max(unavg[f], 0.0001f);
+      const float navg_w = P.g * (na * na);
+      (isu ? h.sgz_u : h.sgz_v)[c] = make_float2(uzmin[f], uzmax[f]);
+      (isu ? h.sgw_u : h.sgw_v)[c] = make_float4(hv[L - 1] - uzmax[f], nv[L - 1], navg_w, uffit[f]);
+      auto& rec = isu ? h.rec_u : h.rec_v;
+      for (int k = 0; k < L - 1; k++) {
+        UvRec r{};
+        r.havg = hv[k];
+        r.dhavg = hv[k + 1] - hv[k];
+        r.nrep = nv[k];
+        r.dnrep = nv[k + 1] - nv[k];
+        r.pwet = pv[k];
+        r.dpwet = pv[k + 1] - pv[k];
+        rec[(size_t)k * NA + c] = r;
+      }
+    }
+  }
+
+  // ---- boundaries (sfincs_domain.f90:1765-1958) -----------------------------------
+  std::vector<int32_t> gb_index(NA, -1);
+  bool water_level_bnd = false, neumann_bnd = false;
+  for (long long i = 0; i < h.np; i++) {
+    const int64_t c = h.cmp_off[i];
+    const int k = kcs[c];
+    if (k == 2 || k == 3 || k == 5 || k == 6) {
+      gb_index[c] = (int32_t)h.gb_cell.size();
+      h.gb_cell.push_back((int32_t)c);
+      h.gb_kcs.push_back((int8_t)k);
+      if (k == 2) water_level_bnd = true;
+      if (k == 6) neumann_bnd = true;
+    }
+  }
+  const size_t ngb = h.gb_cell.size();
+  h.zsb.assign(ngb, 0.0f);
+  h.zsb0.assign(ngb, 0.0f);
+  h.gb_i1.assign(ngb, 0);
+  h.gb_i2.assign(ngb, 0);
+  h.gb_fac.assign(ngb, 0.0f);
+  h.gb_nmi.assign(ngb, 0);
+  // kcuv==2/6 faces in reference ip order; outflow (kcs==3) levels fixed here
+  struct KB {
+    int64_t face, nmb, nmi;
+    int8_t dir, sign;
+  };
+  std::vector<KB> kb_all;
+  for (size_t f = 0; f < face_off.size(); f++) {
+    const int64_t c = face_off[f];
+    const int8_t kc = face_dir[f] == 0 ? kcu[c] : kcv[c];
+    if (kc != 2 && kc != 6) continue;
+    const int64_t cu = face_dir[f] == 0 ? c + ld : c + 1;
+    KB e;
+    e.face = c;
+    e.dir = face_dir[f];
+    if (kcs[c] == 1) {
+      e.nmb = cu;
+      e.nmi = c;
+      e.sign = -1;
+    } else {
+      e.nmb = c;
+      e.nmi = cu;
+      e.sign = 1;
+    }
+    const int ib = gb_index[e.nmb];
+    if (kcs[e.nmb] == 3) {
+      h.zsb0[ib] = P.subgrid ? h.zz_min[e.nmb] : h.zb[e.nmb];
+      h.zsb[ib] = h.zsb0[ib];
+    }
+    kb_all.push_back(e);
+  }
+
+  // ---- boundary conditions files (sfincs_boundaries.f90:8-213) ----------------------
+  int nbnd = 0, ntbnd = 0;
+  std::vector<float> xb, yb;
+  if (!is_none(bndfile)) {
+    auto xy = read_table(path(bndfile));
+    nbnd = (int)xy.size();
+    for (auto& r : xy) {
+      xb.push_back((float)r.at(0));
+      yb.push_back((float)r.at(1));
+    }
+    if (!is_none(bzsfile)) {
+      auto tb = read_table(path(bzsfile));
+      ntbnd = (int)tb.size();
+      h.zs_bnd.assign((size_t)ntbnd * nbnd, 0.0f);
+      for (int it = 0; it < ntbnd; it++) {
+        if ((int)tb[it].size() < nbnd + 1) throw std::runtime_error("bzs file has fewer columns than bnd points");
+        h.t_bnd.push_back((float)tb[it][0]);
+        for (int ib = 0; ib < nbnd; ib++) h.zs_bnd[(size_t)it * nbnd + ib] = (float)tb[it][ib + 1];
+      }
+    } else {
+      ntbnd = 2;
+      h.t_bnd = {t0, t1};
+      h.zs_bnd.assign((size_t)2 * nbnd, 0.0f);
+    }
+    if (ntbnd < 1) throw std::runtime_error("empty boundary time series");
+    if (h.t_bnd[0] > (t0 + 1.0f) || h.t_bnd[ntbnd - 1] < (t1 - 1.0f)) {
+      if (h.t_bnd[0] > (t0 + 1.0f))
+        h.t_bnd[0] = t0 - 1.0f;
+      else
+        h.t_bnd[ntbnd - 1] = t1 + 1.0f;
+    }
+  } else if (water_level_bnd) {
+    nbnd = 1;
+    xb = {0.0f};
+    yb = {0.0f};
+    ntbnd = 2;
+    h.t_bnd = {t0, t1};
+    h.zs_bnd = {0.0f, 0.0f};
+  }
+  P.nbnd = nbnd;
+  P.ntbnd = ntbnd;
+
+  // ---- find_boundary_indices (sfincs_boundaries.f90:455-679) -------------------------
+  if (ngb > 0 && nbnd > 0) {
+    for (size_t ib = 0; ib < ngb; ib++) {
+      const int64_t c = h.gb_cell[ib];
+      const long long ic = cmp_of[c];
+      const float x = h.z_xz[ic], y = h.z_yz[ic];
+      if (kcs[c] == 2) {
+        if (nbnd > 1) {
+          float dst1 = 1.0e10f, dst2 = 1.0e10f;
+          int ib1 = 0, ib2 = 0;
+          for (int j = 0; j < nbnd; j++) {
+            const float ddx = xb[j] - x, ddy = yb[j] - y;
+            const float dst = std::sqrt(ddx * ddx + ddy * ddy);
+            if (dst < dst1) {
+              dst2 = dst1;
+              ib2 = ib1;
+              dst1 = dst;
+              ib1 = j + 1;
+            } else if (dst < dst2) {
+              dst2 = dst;
+              ib2 = j + 1;
+            }
+          }
+          if (ib2 == 0) ib2 = ib1;
+          h.gb_i1[ib] = ib1 - 1;
+          h.gb_i2[ib] = ib2 - 1;
+          h.gb_fac[ib] = dst2 / std::max(dst1 + dst2, 1.0e-9f);
+        } else {
+          h.gb_i1[ib] = 0;
+          h.gb_i2[ib] = 0;
+          h.gb_fac[ib] = 1.0f;
+        }
+      } else if (kcs[c] == 6) {
+        const int n = h.z_n[ic], m = h.z_m[ic];
+        const int cand[4][2] = {{n, m + 1}, {n + 1, m}, {n, m - 1}, {n - 1, m}};
+        int32_t nmi = -1;
+        for (auto& q : cand)
+          if (act(q[0], q[1]) && kcs[OFF(q[0], q[1])] == 1) nmi = (int32_t)OFF(q[0], q[1]);
+        if (nmi < 0) {
+          kcs[c] = 0;  // isolated Neumann cell reset to inactive (sfincs_boundaries.f90:661-672)
+          h.gb_kcs[ib] = 0;
+        } else {
+          h.gb_nmi[ib] = nmi;
+        }
+      }
+    }
+  }
+  (void)neumann_bnd;
+  for (auto& e : kb_all) {
+    if (kcs[e.nmb] == 6) continue;  // lateral Neumann faces are updated by the momentum kernel
+    h.kb_face.push_back((int32_t)e.face);
+    h.kb_dir.push_back(e.dir);
+    h.kb_gb.push_back(gb_index[e.nmb]);
+    h.kb_nmi.push_back((int32_t)e.nmi);
+    h.kb_sign.push_back(e.sign);
+    h.kb_zbuv.push_back(P.subgrid ? 0.0f
+                                  : 0.5f * (h.zb[e.face] + h.zb[e.dir == 0 ? e.face + ld : e.face + 1]));
+  }
+  h.dense2cmp = cmp_of;
+  h.x0 = x0;
+  h.y0 = y0;
+  h.cosrot = cosrot;
+  h.sinrot = sinrot;
+  P.ngbnd = (int)ngb;
+  P.nkcuv2 = (int)h.kb_face.size();
+
+  // ---- roughness (sfincs_domain.f90:1960-2061) -------------------------------------------
+  if (!P.subgrid) {
+    h.gn2_u.assign(NA, 9.81f * 0.02f * 0.02f);
+    h.gn2_v.assign(NA, 9.81f * 0.02f * 0.02f);
+    std::vector<float> rgh;
+    if (!is_none(manningfile)) rgh = read_binary<float>(path(manningfile), (size_t)h.np);
+    const float gn2land = manning_land < 0.0f ? 9.81f * (manning * manning) : 9.81f * (manning_land * manning_land);
+    const float gn2sea = manning_sea < 0.0f ? 9.81f * (manning * manning) : 9.81f * (manning_sea * manning_sea);
+    for (size_t f = 0; f < face_off.size(); f++) {
+      const int64_t c = face_off[f];
+      const bool isu = face_dir[f] == 0;
+      const int64_t cu = isu ? c + ld : c + 1;
+      if ((isu ? kcu[c] : kcv[c]) <= 0) continue;
+      float val;
+      if (!rgh.empty()) {
+        const float a = 0.5f * (rgh[cmp_of[c]] + rgh[cmp_of[cu]]);
+        val = 9.81f * (a * a);
+      } else {
+        const float zbuv = 0.5f * (h.zb[c] + h.zb[cu]);
+        val = zbuv > rghlevland ? gn2land : gn2sea;
+      }
+      (isu ? h.gn2_u : h.gn2_v)[c] = val;
+    }
+  }
+
+  // ---- infiltration con/c2d (sfincs_infiltration.f90:8-606) ---------------------------------
+  P.infiltration = 0;
+  if (P.precip) {
+    if (qinf > 0.0f) {
+      P.infiltration = 1;
+      h.qinf.assign(NA, 0.0f);
+      for (long long i = 0; i < h.np; i++) {
+        const int64_t c = h.cmp_off[i];
+        const float zz = P.subgrid ? h.zz_min[c] : h.zb[c];
+        h.qinf[c] = zz > qinf_zmin ? qinf : 0.0f;
+      }
+    } else if (!is_none(qinffile)) {
+      P.infiltration = 1;
+      h.qinf.assign(NA, 0.0f);
+      auto r = read_binary<float>(path(qinffile), (size_t)h.np);
+      for (long long i = 0; i < h.np; i++) h.qinf[h.cmp_off[i]] = r[i] / 3600.0f / 1000.0f;
+    }
+  }
+
+  // ---- flags, advection mask, theta smoothing -----------------------------------------------
+  h.flags.assign(NA, 0);
+  auto KU = [&](int n, int m) -> int { return (n >= 1 && n <= nmax && m >= 1 && m <= mmax) ? kcu[OFF(n, m)] : 0; };
+  auto KV = [&](int n, int m) -> int { return (n >= 1 && n <= nmax && m >= 1 && m <= mmax) ? kcv[OFF(n, m)] : 0; };
+  const bool do_mask = P.advection && advection_mask && nmax > 1;
+  for (long long i = 0; i < h.np; i++) {
+    const int n = h.z_n[i], m = h.z_m[i];
+    const int64_t c = OFF(n, m);
+    uint16_t f = F_ACT;
+    if (kcs[c] == 1) f |= F_KCS1;
+    const int ku = kcu[c], kv = kcv[c];
+    if (ku == 1 || ku == 6) f |= F_UACT;
+    if (kv == 1 || kv == 6) f |= F_VACT;
+    const bool cdn = act(n - 1, m), cup = act(n + 1, m), clf = act(n, m - 1), crt = act(n, m + 1);
+    if (cdn) f |= F_CDN;
+    if (cup) f |= F_CUP;
+    if (clf) f |= F_CLF;
+    if (crt) f |= F_CRT;
+    if (P.advection) {  // sfincs_domain.f90:2147-2178
+      bool madv_u = true, madv_v = true;
+      if (do_mask) {
+        const int u_ndm = cdn ? KU(n - 1, m) : ku, u_num = cup ? KU(n + 1, m) : ku;
+        madv_u = KU(n, m + 1) == 1 && KU(n, m - 1) == 1 && KV(n, m) == 1 && KV(n, m + 1) == 1 && KV(n - 1, m) == 1 &&
+                 KV(n - 1, m + 1) == 1 && u_ndm == 1 && u_num == 1;
+        const int v_ndm = clf ? KV(n, m - 1) : kv, v_num = crt ? KV(n, m + 1) : kv;
+        madv_v = KV(n + 1, m) == 1 && KV(n - 1, m) == 1 && KU(n, m) == 1 && KU(n + 1, m) == 1 && KU(n, m - 1) == 1 &&
+                 KU(n + 1, m - 1) == 1 && v_ndm == 1 && v_num == 1;
+      }
+      if (madv_u) f |= F_UADV;
+      if (madv_v) f |= F_VADV;
+    }
+    if (KU(n, m - 1) == 1 && KU(n, m + 1) == 1) f |= F_UTH;  // kcuv(u_nmd)==1 and kcuv(u_nmu)==1
+    if (KV(n - 1, m) == 1 && KV(n + 1, m) == 1) f |= F_VTH;
+    h.flags[c] = f;
+  }
+  h.kcs_cmp.resize(h.np);
+  for (long long i = 0; i < h.np; i++) {
+    h.kcs_cmp[i] = kcs[h.cmp_off[i]];
+    if (kcs[h.cmp_off[i]] == 1) {
+      h.n_kcs1++;
+      h.area_total_kcs1 += (double)P.area;
+    }
+  }
+
+  // ---- initial conditions (sfincs_initial_conditions.F90:98-106, sfincs_subgrid.F90:907-962) --
+  h.zs.assign(NA, 0.0f);
+  for (long long i = 0; i < h.np; i++) {
+    const int64_t c = h.cmp_off[i];
+    const float base = P.subgrid ? h.zz_min[c] : h.zb[c];
+    h.zs[c] = (float)std::max((double)base, (double)P.zini);
+  }
+  h.zsmax.assign(NA, -999.0f);
+  if (P.wiggle) h.zs0 = h.zs;
+  if (P.subgrid) {
+    const int L = P.nlev;
+    h.zvol.assign(NA, 0.0);
+    h.vneg.assign(NA, 0);
+    for (long long i = 0; i < h.np; i++) {
+      const int64_t c = h.cmp_off[i];
+      const double zs = h.zs[c];
+      if (zs >= (double)h.zz_max[c]) {
+        h.zvol[c] = (double)h.zz_volmax[c] + (double)P.area * (zs - (double)std::max(h.zz_max[c], -20.0f));
+      } else {
+        const float* dep = &sg_level_raw[(size_t)i * L];  // z_level of this cell, levels 1..L
+        int ivol = 1;
+        for (int il = 2; il <= L; il++) {
+          if ((double)dep[il - 1] > zs) {
+            ivol = il - 1;
+            break;
+          }
+        }
+        const float dzvol = h.zz_volmax[c] / (float)(L - 1);
+        const float facint =
+            (float)((zs - (double)dep[ivol - 1]) / (double)std::max(dep[ivol] - dep[ivol - 1], 0.001f));
+        h.zvol[c] = (double)((float)(ivol - 1) * dzvol + facint * dzvol);
+      }
+      h.vneg[c] = h.zvol[c] < 0.0 ? 1 : 0;
+    }
+  }
+
+  // ---- meteo time series and Cd table (sfincs_meteo.f90:247-327) ------------------------------
+  if (P.wind) {
+    auto tb = read_table(path(wndfile));
+    for (auto& r : tb) {
+      h.twnd.push_back((float)r.at(0));
+      h.wmag.push_back((float)r.at(1));
+      h.wdir.push_back(P.pi * (270.0f - (float)r.at(2)) / 180.0f - rotation);
+    }
+    P.ntwnd = (int)h.twnd.size();
+    if (P.ntwnd < 2) throw std::runtime_error("wind time series needs at least two records");
+  }
+  if (P.precip) {
+    auto tb = read_table(path(prcpfile));
+    for (auto& r : tb) {
+      h.tprcp.push_back((float)r.at(0));
+      h.vprcp.push_back((float)r.at(1));
+    }
+    P.ntprcp = (int)h.tprcp.size();
+    if (P.ntprcp < 1) throw std::runtime_error("empty precipitation time series");
+  }
+  {
+    const float cd_wnd[3] = {0.0f, 28.0f, 50.0f}, cd_val[3] = {0.0010f, 0.0025f, 0.0015f};
+    h.cdval.assign(1000, 0.0f);
+    for (int iw = 1; iw <= 1000; iw++) {
+      const float wnd = (float)iw * 0.1f;
+      for (int icd = 1; icd <= 2; icd++) {
+        h.cdval[iw - 1] = cd_val[icd - 1];
+        if (wnd >= cd_wnd[icd - 1] && wnd < cd_wnd[icd]) {
+          h.cdval[iw - 1] = cd_val[icd - 1] + (wnd - cd_wnd[icd - 1]) * (cd_val[icd] - cd_val[icd - 1]) /
+                                                  (cd_wnd[icd] - cd_wnd[icd - 1]);
+          break;
+        } else if (wnd >= cd_wnd[2]) {
+          h.cdval[iw - 1] = cd_val[2];
+          break;
+        }
+      }
+    }
+  }
+
+  // ---- point sources (sfincs_discharges.f90:8-324) ------------------------------------------------
+  if (!is_none(srcfile)) {
+    auto xy = read_table(path(srcfile));
+    auto tb = read_table(path(disfile));
+    const int nsrc = (int)xy.size();
+    for (auto& r : xy) {
+      const float x = (float)r.at(0), y = (float)r.at(1);
+      const float xt = cosrot * (x - x0) + sinrot * (y - y0);
+      const float yt = -sinrot * (x - x0) + cosrot * (y - y0);
+      const int n = (int)(yt / dy) + 1, m = (int)(xt / dx) + 1;  // sfincs_quadtree.F90:788-790
+      if (!act(n, m)) throw std::runtime_error("point source outside the active mesh");
+      h.src_cell.push_back((int32_t)OFF(n, m));
+    }
+    for (auto& r : tb) {
+      if ((int)r.size() < nsrc + 1) throw std::runtime_error("dis file has fewer columns than src points");
+      h.tsrc.push_back((float)r[0]);
+      for (int is = 0; is < nsrc; is++) h.qsrc.push_back((float)r[is + 1]);
+    }
+    P.nsrc = nsrc;
+    P.ntsrc = (int)h.tsrc.size();
+  }
+  return H;
+}
+
+// ============================================================================
+// DeviceModel
+// ============================================================================
+template <class X>
+X* DeviceModel::alloc(size_t n) {
+  if (n == 0) return nullptr;
+  void* p = nullptr;
+  check_cuda(cudaMalloc(&p, n * sizeof(X)), "cudaMalloc");
+  check_cuda(cudaMemset(p, 0, n * sizeof(X)), "cudaMemset");
+  allocs_.push_back(p);
+  bytes_ += n * sizeof(X);
+  return static_cast<X*>(p);
+}
+
+template <class X>
+X* DeviceModel::upload(const std::vector<X>& v) {
+  if (v.empty()) return nullptr;
+  X* p = alloc<X>(v.size());
+  check_cuda(cudaMemcpy(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice), "upload");
+  return p;
+}
+
+DeviceModel::DeviceModel(const HostModel& h) : h_(&h) {
+  d_ = h.p;
+  const size_t NA = (size_t)h.p.nalloc;
+  try {
+    d_.zs = upload(h.zs);
+    d_.zsmax = upload(h.zsmax);
+    d_.zvol = upload(h.zvol);
+    d_.zs0 = h.p.wiggle ? upload(h.zs0) : nullptr;
+    d_.zsderv = h.p.wiggle ? alloc<float>(NA) : nullptr;
+    d_.kfuv = alloc<uint8_t>(NA);
+    d_.vneg = h.p.subgrid ? upload(h.vneg) : nullptr;
+    for (int b = 0; b < 2; b++) {
+      d_.qu[b] = alloc<float>(NA);
+      d_.qv[b] = alloc<float>(NA);
+      d_.uu[b] = alloc<float>(NA);
+      d_.vv[b] = alloc<float>(NA);
+    }
+    d_.flags = upload(h.flags);
+    d_.zb = upload(h.zb);
+    d_.zbmx_u = upload(h.zbmx_u);
+    d_.zbmx_v = upload(h.zbmx_v);
+    d_.gn2_u = upload(h.gn2_u);
+    d_.gn2_v = upload(h.gn2_v);
+    d_.sgz_u = upload(h.sgz_u);
+    d_.sgz_v = upload(h.sgz_v);
+    d_.sgw_u = upload(h.sgw_u);
+    d_.sgw_v = upload(h.sgw_v);
+    d_.rec_u = upload(h.rec_u);
+    d_.rec_v = upload(h.rec_v);
+    d_.zz_min = upload(h.zz_min);
+    d_.zz_max = upload(h.zz_max);
+    d_.zz_volmax = upload(h.zz_volmax);
+    d_.zlev = upload(h.zlev);
+    d_.qext = h.p.use_qext ? alloc<float>(NA) : nullptr;
+    d_.qinf = upload(h.qinf);
+    d_.t_bnd = upload(h.t_bnd);
+    d_.zs_bnd = upload(h.zs_bnd);
+    d_.zst_bnd = alloc<float>((size_t)std::max(h.p.nbnd, 1));
+    d_.gb_cell = upload(h.gb_cell);
+    d_.gb_kcs = upload(h.gb_kcs);
+    d_.gb_i1 = upload(h.gb_i1);
+    d_.gb_i2 = upload(h.gb_i2);
+    d_.gb_fac = upload(h.gb_fac);
+    d_.gb_nmi = upload(h.gb_nmi);
+    d_.zsb = upload(h.zsb);
+    d_.zsb0 = upload(h.zsb0);
+    d_.kb_face = upload(h.kb_face);
+    d_.kb_dir = upload(h.kb_dir);
+    d_.kb_gb = upload(h.kb_gb);
+    d_.kb_nmi = upload(h.kb_nmi);
+    d_.kb_sign = upload(h.kb_sign);
+    d_.kb_zbuv = upload(h.kb_zbuv);
+    d_.uvmean = alloc<float>((size_t)std::max(h.p.nkcuv2, 1));
+    d_.tprcp = upload(h.tprcp);
+    d_.vprcp = upload(h.vprcp);
+    d_.twnd = upload(h.twnd);
+    d_.wmag = upload(h.wmag);
+    d_.wdir = upload(h.wdir);
+    d_.cdval = upload(h.cdval);
+    d_.tsrc = upload(h.tsrc);
+    d_.qsrc = upload(h.qsrc);
+    d_.qtsrc = alloc<float>((size_t)std::max(h.p.nsrc, 1));
+    d_.src_cell = upload(h.src_cell);
+    d_cmp_ = upload(h.cmp_off);
+    d_.st = alloc<StepState>(1);
+    StepState s{};
+    s.t = h.t0;  // sfincs_lib.f90:279-282: t = t0, first min_dt = 1e-6
+    s.tend = h.t0;
+    s.min_dt = 1.0e-6f;
+    s.dt = 1.0e-6f;
+    s.itbndlast = s.itprcplast = s.itwndlast = s.itsrclast = 1;
+    s.steps_left = 0;
+    float one_e_minus6 = 1.0e-6f;
+    std::memcpy(&s.min_dt_bits, &one_e_minus6, 4);
+    check_cuda(cudaMemcpy(d_.st, &s, sizeof(s), cudaMemcpyHostToDevice), "init step state");
+  } catch (...) {
+    for (void* p : allocs_) cudaFree(p);
+    allocs_.clear();
+    throw;
+  }
+}
+
+DeviceModel::~DeviceModel() {
+  for (void* p : allocs_) cudaFree(p);
+}
+
+// ============================================================================
+// Runner
+// ============================================================================
+Runner::Runner(std::vector<DeviceModel*> models, int tile_m) : models_(std::move(models)) {
+  if (models_.empty()) throw std::runtime_error("Runner needs at least one model");
+  if (tile_m != 8) throw std::runtime_error("only 32x8 cell tiles are built into this library");
+  subgrid_ = models_[0]->host().p.subgrid;
+  std::vector<ScnDev> scns;
+  std::vector<Tile> tiles;
+  for (size_t i = 0; i < models_.size(); i++) {
+    const HostModel& h = models_[i]->host();
+    if (h.p.subgrid != subgrid_) throw std::runtime_error("an ensemble must be all-subgrid or all-regular");
+    if (h.p.nsrc > 0) any_src_ = 1;
+    scns.push_back(models_[i]->dev());
+    const int nmax = h.p.nmax, mmax = h.p.mmax;
+    for (int m0 = 1; m0 <= mmax; m0 += tile_m) {
+      for (int n0 = 1; n0 <= nmax; n0 += 32) {
+        // skip tiles without any active cell
+        bool any = false;
+        for (int m = m0; m < m0 + tile_m && m <= mmax && !any; m++)
+          for (int n = n0; n < n0 + 32 && n <= nmax; n++)
+            if (h.flags[(size_t)m * h.p.ld + kGhostPad + n] & F_ACT) {
+              any = true;
+              break;
+            }
+        if (any) tiles.push_back(Tile{(int)i, n0, m0, 0});
+      }
+    }
+  }
+  ntiles_ = (int)tiles.size();
+  check_cuda(cudaMalloc(&d_scns_, scns.size() * sizeof(ScnDev)), "cudaMalloc scns");
+  check_cuda(cudaMemcpy(d_scns_, scns.data(), scns.size() * sizeof(ScnDev), cudaMemcpyHostToDevice), "scns");
+  if (ntiles_ > 0) {
+    check_cuda(cudaMalloc(&d_tiles_, tiles.size() * sizeof(Tile)), "cudaMalloc tiles");
+    check_cuda(cudaMemcpy(d_tiles_, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice), "tiles");
+  }
+  check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  check_cuda(cudaMallocHost(&h_states_, models_.size() * sizeof(StepState)), "pinned states");
+}
+
+Runner::~Runner() {
+  if (graph_) cudaGraphExecDestroy(graph_);
+  if (stream_) cudaStreamDestroy(stream_);
+  if (d_scns_) cudaFree(d_scns_);
+  if (d_tiles_) cudaFree(d_tiles_);
+  if (h_states_) cudaFreeHost(h_states_);
+}
+
+void Runner::build_graph(int chunk) {
+  if (graph_ && graph_chunk_ == chunk) return;
+  if (graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  cudaGraph_t g;
+  check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+  for (int i = 0; i < chunk; i++) launch_step(d_scns_, nscn(), d_tiles_, ntiles_, subgrid_, any_src_, stream_);
+  check_cuda(cudaStreamEndCapture(stream_, &g), "end capture");
+  check_cuda(cudaGraphInstantiate(&graph_, g, 0), "graph instantiate");
+  cudaGraphDestroy(g);
+  graph_chunk_ = chunk;
+}
+
+void Runner::refresh_params() {
+  std::vector<ScnDev> scns;
+  for (auto* m : models_) scns.push_back(m->dev());
+  check_cuda(cudaMemcpyAsync(d_scns_, scns.data(), scns.size() * sizeof(ScnDev), cudaMemcpyHostToDevice, stream_),
+             "refresh params");
+  sync();
+}
+
+void Runner::issue(int nsteps) {
+  for (int i = 0; i < nsteps; i++) launch_step(d_scns_, nscn(), d_tiles_, ntiles_, subgrid_, any_src_, stream_);
+}
+
+void Runner::sync() { check_cuda(cudaStreamSynchronize(stream_), "stream sync"); }
+
+StepState Runner::read_state(int i) {
+  check_cuda(cudaMemcpyAsync(&h_states_[i], models_[i]->state(), sizeof(StepState), cudaMemcpyDeviceToHost, stream_),
+             "read state");
+  sync();
+  return h_states_[i];
+}
+
+void Runner::step_once() {
+  for (auto* m : models_) {
+    const double tend = m->host().t1;
+    const int one = 1;
+    check_cuda(cudaMemcpyAsync(&m->state()->tend, &tend, sizeof(double), cudaMemcpyHostToDevice, stream_), "tend");
+    check_cuda(cudaMemcpyAsync(&m->state()->steps_left, &one, sizeof(int), cudaMemcpyHostToDevice, stream_), "steps");
+  }
+  issue(1);
+  check_cuda(cudaGetLastError(), "step launch");
+  sync();
+}
+
+void Runner::run(const std::vector<double>& tend, long long max_steps, int chunk) {
+  if (tend.size() != models_.size()) throw std::runtime_error("one target time per model is required");
+  std::vector<double> tend_h = tend;
+  std::vector<int> left((size_t)nscn(), max_steps >= 0 ? (int)std::min<long long>(max_steps, 0x7fffffff) : -1);
+  for (int i = 0; i < nscn(); i++) {
+    check_cuda(cudaMemcpyAsync(&models_[i]->state()->tend, &tend_h[i], sizeof(double), cudaMemcpyHostToDevice, stream_),
+               "tend");
+    check_cuda(cudaMemcpyAsync(&models_[i]->state()->steps_left, &left[i], sizeof(int), cudaMemcpyHostToDevice,
+                               stream_),
+               "steps");
+  }
+  build_graph(chunk);
+  for (;;) {
+    check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+    for (int i = 0; i < nscn(); i++)
+      check_cuda(cudaMemcpyAsync(&h_states_[i], models_[i]->state(), sizeof(StepState), cudaMemcpyDeviceToHost,
+                                 stream_),
+                 "read state");
+    sync();
+    bool all_done = true;
+    for (int i = 0; i < nscn(); i++) {
+      const StepState& s = h_states_[i];
+      const bool done = s.stop_pending || !(s.t < s.tend) || s.steps_left == 0;
+      if (!done) all_done = false;
+    }
+    if (all_done) break;
+  }
+}
+
+}  // namespace sfg

@@ -1,0 +1,133 @@
+// Host side of the B200 SFINCS core: model loading (reference input files ->
+// dense device layout), device residency, and the step runner (single model or
+// an ensemble of uneven models advanced by the same launches).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../sfg_device.h"
+
+namespace sfg {
+
+// Everything read from a model directory and laid out densely on the host.
+struct HostModel {
+  std::string dir;
+  ScnDev p{};  // scalar parameters (pointer fields unused on the host copy)
+  // switches and inputs that stay on the host
+  bool store_vmax = false, store_qmax = false, store_twet = false;
+  double t0 = 0, t1 = 0;
+  long long np = 0, npuv = 0;
+  // dense static arrays
+  std::vector<uint16_t> flags;
+  std::vector<float> zb, zbmx_u, zbmx_v, gn2_u, gn2_v;
+  std::vector<float2> sgz_u, sgz_v;
+  std::vector<float4> sgw_u, sgw_v;
+  std::vector<UvRec> rec_u, rec_v;
+  std::vector<float> zz_min, zz_max, zz_volmax;
+  std::vector<float2> zlev;
+  std::vector<float> qinf;
+  // dense initial state
+  std::vector<float> zs, zsmax, zs0;
+  std::vector<double> zvol;
+  std::vector<uint8_t> vneg;
+  // compact (reference nm order) <-> dense
+  std::vector<int32_t> cmp_off;           // [np] dense offset of compact cell nm-1
+  std::vector<int32_t> dense2cmp;         // [nalloc] compact index (0-based) or -1
+  float x0 = 0, y0 = 0, cosrot = 1, sinrot = 0;
+  std::vector<float> z_xz, z_yz, zb_cmp, zmin_cmp;  // compact, for the BMI data interface
+  std::vector<int8_t> kcs_cmp;
+  std::vector<int32_t> z_n, z_m;
+  // boundary lists
+  std::vector<int32_t> gb_cell, gb_i1, gb_i2, gb_nmi;
+  std::vector<int8_t> gb_kcs;
+  std::vector<float> gb_fac, zsb, zsb0;
+  std::vector<int32_t> kb_face, kb_gb, kb_nmi;
+  std::vector<int8_t> kb_dir, kb_sign;
+  std::vector<float> kb_zbuv;
+  // forcing series
+  std::vector<float> t_bnd, zs_bnd;  // zs_bnd [ntbnd][nbnd]
+  std::vector<float> tprcp, vprcp, twnd, wmag, wdir, cdval;
+  std::vector<float> tsrc, qsrc;     // qsrc [ntsrc][nsrc]
+  std::vector<int32_t> src_cell;
+  long long n_kcs1 = 0;
+  double area_total_kcs1 = 0;
+};
+
+// Reads <dir>/sfincs.inp and the files it names.  bmi mirrors the reference's
+// BMI initialize() (use_qext on).  Throws std::runtime_error on bad input.
+std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi);
+
+// Device residency of one model: all arrays allocated once, state updated in place.
+class DeviceModel {
+ public:
+  explicit DeviceModel(const HostModel& h);
+  ~DeviceModel();
+  DeviceModel(const DeviceModel&) = delete;
+  DeviceModel& operator=(const DeviceModel&) = delete;
+  const HostModel& host() const { return *h_; }
+  ScnDev& dev() { return d_; }
+  StepState* state() { return d_.st; }
+  size_t bytes() const { return bytes_; }
+  // compact (nm order) views
+  int32_t* d_cmp_off() { return d_cmp_; }
+
+ private:
+  template <class X>
+  X* upload(const std::vector<X>& v);
+  template <class X>
+  X* alloc(size_t n);
+  const HostModel* h_;
+  ScnDev d_{};
+  std::vector<void*> allocs_;
+  int32_t* d_cmp_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+// Advances one or more device models together.  Every launch covers all
+// models; models whose time has reached their own target are skipped on the
+// device (no host round trip per step).
+class Runner {
+ public:
+  Runner(std::vector<DeviceModel*> models, int tile_m = 8);
+  ~Runner();
+  // Run until every model reached its target time; at most max_steps steps
+  // per model when max_steps >= 0.  Steps are issued in CUDA-graph chunks of
+  // `chunk` steps; the host checks completion once per chunk.
+  void run(const std::vector<double>& tend, long long max_steps, int chunk = 32);
+  // One step exactly (reference update()).
+  void step_once();
+  void sync();
+  cudaStream_t stream() const { return stream_; }
+  StepState read_state(int i);
+  // re-upload the scalar parameters of every model (after a host-side change)
+  void refresh_params();
+  const ScnDev* d_scns() const { return d_scns_; }
+  int ntiles() const { return ntiles_; }
+  int nscn() const { return (int)models_.size(); }
+  // issue `nsteps` steps on the stream (no host sync); used for timing
+  void issue(int nsteps);
+
+ private:
+  void build_graph(int chunk);
+  std::vector<DeviceModel*> models_;
+  ScnDev* d_scns_ = nullptr;
+  Tile* d_tiles_ = nullptr;
+  int ntiles_ = 0;
+  int subgrid_ = 0;
+  int any_src_ = 0;
+  cudaStream_t stream_ = nullptr;
+  cudaGraphExec_t graph_ = nullptr;
+  int graph_chunk_ = 0;
+  StepState* h_states_ = nullptr;  // pinned mirror of the step states
+};
+
+void launch_step(const ScnDev* d_scns, int nscn, const Tile* d_tiles, int ntiles, int subgrid, int any_src,
+                 cudaStream_t s);
+
+void check_cuda(cudaError_t e, const char* what);
+
+}  // namespace sfg

@@ -1,0 +1,155 @@
+// Device-side data layout of the B200 SFINCS core.
+//
+// Regular (and regular-subgrid) meshes are stored DENSE: every array is a
+// padded (mmax+2) x ld column-major grid with n (y) fastest, so that the
+// reference's twelve explicit uv neighbour index arrays
+// (sfincs_domain.f90:1007-1261) become implicit +-1 / +-ld offsets and every
+// warp reads 32 consecutive cells.  Cell (n, m), 1-based as in the reference,
+// sits at   off(n, m) = m*ld + 31 + n   (n = 0 and n = nmax+1, m = 0 and
+// m = mmax+1 are inactive ghost cells; n = 1 lands on a 128-byte boundary).
+// The u face at off(n,m) joins (n,m)-(n,m+1); the v face joins (n,m)-(n+1,m).
+// Faces that do not exist in the reference keep q = uv = 0 forever, which is
+// exactly the reference's "dummy" uv point npuv+ncuv+1.
+//
+// All kernels are written against a table of scenarios, so one launch can
+// advance a single model (the BMI drop-in) or many uneven models (ensembles).
+#pragma once
+#include <cstdint>
+
+namespace sfg {
+
+constexpr int kGhostPad = 31;  // low padding so that n = 1 is 128-byte aligned
+
+// Static per-cell flag bits (uint16_t).
+enum : uint16_t {
+  F_ACT = 1u << 0,     // cell exists (msk > 0)
+  F_KCS1 = 1u << 1,    // kcs == 1: continuity update
+  F_UACT = 1u << 2,    // u face exists and kcuv in {1,6}: momentum update
+  F_VACT = 1u << 3,    // v face exists and kcuv in {1,6}
+  F_UADV = 1u << 4,    // u face mask_adv == 1
+  F_VADV = 1u << 5,    // v face mask_adv == 1
+  F_CDN = 1u << 6,     // cell (n-1,m) exists  (u face u_ndm neighbour; else self)
+  F_CUP = 1u << 7,     // cell (n+1,m) exists  (u face u_num neighbour; else self)
+  F_CLF = 1u << 8,     // cell (n,m-1) exists  (v face u_ndm neighbour; else self)
+  F_CRT = 1u << 9,     // cell (n,m+1) exists  (v face u_num neighbour; else self)
+  F_UTH = 1u << 10,    // u face: kcuv(u_nmd)==1 and kcuv(u_nmu)==1 (theta smoothing)
+  F_VTH = 1u << 11,    // v face: same
+};
+
+// kfuv bits (uint8_t per cell, mutable)
+enum : uint8_t { K_U = 1u, K_V = 2u };
+
+// One subgrid uv lookup record: values at level k and the increment to k+1
+// (computed with the same float subtraction the reference performs inline at
+// sfincs_momentum.f90:376-378), so one 32-byte sector serves one lookup.
+struct alignas(32) UvRec {
+  float havg, dhavg, nrep, dnrep, pwet, dpwet, pad0, pad1;
+};
+
+// Per-scenario mutable step state (device memory).  Time is FP64.
+struct alignas(16) StepState {
+  double t;            // model time (s), reference sfincs_lib.f90:57 real*8
+  double tend;         // end of the current update interval
+  double bflux_vol;    // FP64 accumulated boundary inflow volume (m3)
+  double rain_vol;     // FP64 accumulated rain volume over kcs==1 cells (m3)
+  double src_vol;      // FP64 accumulated point-source volume (m3)
+  unsigned int min_dt_bits;  // float bits; atomicMin target of the flux kernel
+  float dt;            // current step (real*4)
+  float min_dt;        // min_dt used for the current dt
+  float ptmp;          // uniform rain for this step (m/s)
+  float twu, twv;      // uniform wind stress for this step
+  int nt;              // steps taken
+  int run;             // 1 if the current step executes
+  int parity;          // which q/uv buffer holds the latest values
+  int error;           // 1 = instability stop (sfincs_lib.f90:634-648)
+  int stop_pending;    // instability detected: t := t1 + 1 at the next step
+  int single;          // update(): at most one step
+  int steps_left;      // for single / bounded calls
+  int itbndlast, itprcplast, itwndlast, itsrclast;
+  int pad_[2];
+};
+
+struct ScnDev {
+  // ---- grid
+  int nmax, mmax, ld, subgrid;
+  int64_t nalloc;
+  float dx, dy, dxinv, dyinv, dx2inv, dy2inv, area;
+  // ---- physics switches and parameters (sfincs_input.f90 defaults)
+  float g, huthresh, huvmin, alfa, uvlim, advlim, slopelim, wiggle_threshold, wiggle_factor, theta;
+  float nuvisc, nuviscfac, fcorio, dtmax, dtmin, rhoa, rhow, btfilter, btrelax, zini, tspinup, t0, t1;
+  int advection, adv_scheme, viscosity, coriolis, friction2d, thetasmooth, wiggle, wind, precip, use_qext;
+  int store_zsmax, infiltration, nlev, nref;
+  // ---- state
+  float* zs;
+  float* zsmax;
+  double* zvol;
+  float* zs0;
+  float* zsderv;
+  uint8_t* kfuv;
+  uint8_t* vneg;       // subgrid: z_volume < 0 (written by continuity)
+  float* qu[2];
+  float* qv[2];
+  float* uu[2];
+  float* vv[2];
+  const uint16_t* flags;
+  // ---- regular bathymetry
+  const float* zb;
+  const float* zbmx_u;   // zbuvmx of the u face
+  const float* zbmx_v;
+  const float* gn2_u;
+  const float* gn2_v;
+  // ---- subgrid tables
+  const float2* sgz_u;   // (zmin, zmax) of the u face
+  const float2* sgz_v;
+  const float4* sgw_u;   // (havg_zmax, nrep_zmax, navg_w, fnfit)
+  const float4* sgw_v;
+  const UvRec* rec_u;    // [level k = 0..nlev-2][cell offset]
+  const UvRec* rec_v;
+  const float* zz_min;
+  const float* zz_max;
+  const float* zz_volmax;
+  const float2* zlev;    // [level][cell]: (dep_k, dep_k+1 - dep_k)
+  // ---- per-cell forcing
+  const float* qext;
+  const float* qinf;     // infiltration field (m/s), con/c2d
+  // ---- boundary forcing
+  int nbnd, ntbnd, ngbnd, nkcuv2;
+  const float* t_bnd;    // [ntbnd]
+  const float* zs_bnd;   // [ntbnd][nbnd]
+  float* zst_bnd;        // [nbnd]
+  const int* gb_cell;    // [ngbnd] boundary cell offset
+  const int8_t* gb_kcs;  // [ngbnd] kcs of the boundary cell (2,3,6)
+  const int* gb_i1;      // [ngbnd] nearest bnd points (0-based) and weight
+  const int* gb_i2;
+  const float* gb_fac;
+  const int* gb_nmi;     // [ngbnd] Neumann interior cell offset
+  float* zsb;            // [ngbnd]
+  float* zsb0;           // [ngbnd]
+  const int* kb_face;    // [nkcuv2] face offset
+  const int8_t* kb_dir;  // [nkcuv2] 0 = u face, 1 = v face
+  const int* kb_gb;      // [nkcuv2] index into the boundary-cell arrays
+  const int* kb_nmi;     // [nkcuv2] interior cell offset
+  const int8_t* kb_sign; // [nkcuv2] ibuvdir
+  const float* kb_zbuv;  // [nkcuv2] zbuv of the face at initialisation (regular grids)
+  float* uvmean;         // [nkcuv2]
+  // ---- time series (uniform meteo, point sources)
+  int ntprcp, ntwnd, nsrc, ntsrc;
+  const float* tprcp;
+  const float* vprcp;
+  const float* twnd;
+  const float* wmag;
+  const float* wdir;
+  const float* cdval;    // [1000]
+  const float* tsrc;
+  const float* qsrc;     // [ntsrc][nsrc]
+  float* qtsrc;          // [nsrc]
+  const int* src_cell;   // [nsrc]
+  float pi;
+  StepState* st;
+};
+
+struct Tile {  // one CTA of the cell kernels
+  int scn, n0, m0, pad;
+};
+
+}  // namespace sfg
