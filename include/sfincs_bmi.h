@@ -120,6 +120,11 @@ SFG_API int sfg_model_set(void* model, const char* name, const void* src, size_t
 SFG_API int sfg_model_volume(void* model, double* volume);
 /* CUDA stream the model's kernels run on (cudaStream_t), for event timing. */
 SFG_API void* sfg_model_stream(void* model);
+/* Run nsteps steps with CUDA events between the individual launches (on the
+ * model's stream) and return the mean duration in ms of the
+ * [step+boundary, momentum, point sources, continuity] launches in ms_out[4];
+ * launches_per_step receives how many kernels one step launches. */
+SFG_API int sfg_model_kernel_times(void* model, int nsteps, double ms_out[4], int* launches_per_step);
 
 /* ---- ensembles: many uneven models advanced by the same launches -------------------- */
 SFG_API void* sfg_ensemble_create(const char* const* model_dirs, int n, int bmi, char* err, int errlen);
@@ -132,14 +137,16 @@ SFG_API int sfg_ensemble_sync(void* ens);
 SFG_API int sfg_ensemble_scalars(void* ens, int member, double out[19]);
 SFG_API int sfg_ensemble_get(void* ens, int member, const char* name, void* dst, size_t bytes);
 SFG_API void* sfg_ensemble_stream(void* ens);
+SFG_API int sfg_ensemble_kernel_times(void* ens, int nsteps, double ms_out[4], int* launches_per_step);
 
 /* ---- diagnostics: host-side layout of a model, no device work -------------------------- */
 /* Loads <model_dir> on the host only and copies one layout array (compact
- * reference cell order) into dst: "counts" (double[8]: np, npuv, ngbnd,
- * nkcuv2, nlevels, nalloc, dtmax, dtmin), "flags" (double[np]), "zs" and
+ * reference cell order) into dst: "counts" (double[10]: np, npuv, ngbnd,
+ * nkcuv2, nlevels, nalloc, dtmax, dtmin, t0, t1), "flags" (double[np]), "zs" and
  * "zvol" (initial state, double[np]), "zbmx","gn2" (double[2*np]: u then v
- * face of each cell), "gb_cell" (double[ngbnd], compact index), "gb_fac",
- * "kb_cell","kb_dir","kb_sign" (double[nkcuv2]).  Returns 0 or -1. */
+ * face of each cell), "gb_cell" (double[ngbnd], compact index), "kb_cell",
+ * "kb_dir","kb_sign","kb_fac" (double[nkcuv2], water-level boundary faces in
+ * reference order).  Returns 0 or -1. */
 SFG_API int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst, size_t n);
 
 #ifdef __cplusplus

@@ -89,11 +89,17 @@ class Oracle:
     def update_until(self, t_target: float) -> int:
         return self.update(float(t_target) - self.scalars()["t"])
 
-    def get(self, name: str) -> np.ndarray:
-        s = self.scalars()
-        n = int(s["npuv"]) if name in ("q", "uv", "kfuv", "kcuv", "mask_adv", "uv_nm", "uv_nmu", "uv_dir") else int(s["np"])
-        if name == "uvmean":
-            n = int(s["nkcuv2"])
+    def get(self, name: str, n: int | None = None) -> np.ndarray:
+        """Copy a named array; n defaults to npuv for face arrays, nkcuv2 for
+        uvmean and np otherwise (pass n for the boundary-face lists kb_*)."""
+        if n is None:
+            s = self.scalars()
+            if name in ("q", "uv", "kfuv", "kcuv", "mask_adv", "uv_nm", "uv_nmu", "uv_dir"):
+                n = int(s["npuv"])
+            elif name == "uvmean":
+                n = int(s["nkcuv2"])
+            else:
+                n = int(s["np"])
         out = np.zeros(n, np.float64)
         rc = lib().oracle_get(self._h, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n)
         if rc != 0:

@@ -2045,6 +2045,20 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "netprcp" && m.netprcp.allocated()) copy_out(m.netprcp, out, n);
     else if (s == "qext" && m.qext.allocated()) copy_out(m.qext, out, n);
     else if (s == "uvmean") copy_out(m.uvmean, out, n);
+    else if (s == "kb_cell" || s == "kb_dir" || s == "kb_sign") {
+      // water-level boundary faces (kcuv==2/6 list without lateral Neumann faces), reference order
+      long k = 0;
+      for (long ib = 1; ib <= m.nkcuv2; ib++) {
+        if (m.kcs(m.nmbkcuv2(ib)) == 6) continue;
+        if (k >= n) return -1;
+        long ip = m.index_kcuv2(ib);
+        if (s == "kb_cell") out[k] = (double)(m.uv_index_z_nm(ip) - 1);
+        else if (s == "kb_dir") out[k] = (double)m.uv_flags_dir(ip);
+        else out[k] = (double)m.ibuvdir(ib);
+        k++;
+      }
+      if (k != n) return -1;
+    }
     else return -1;
     return 0;
   });

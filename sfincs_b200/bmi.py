@@ -86,6 +86,8 @@ def lib(build_if_missing: bool = True):
     L.sfg_ensemble_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]
     L.sfg_ensemble_stream.restype = ctypes.c_void_p
     L.sfg_ensemble_stream.argtypes = [ctypes.c_void_p]
+    L.sfg_model_kernel_times.argtypes = [ctypes.c_void_p, ctypes.c_int, c_dp, c_ip]
+    L.sfg_ensemble_kernel_times.argtypes = [ctypes.c_void_p, ctypes.c_int, c_dp, c_ip]
     L.sfg_layout_get.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, c_dp, ctypes.c_size_t]
     _lib = L
     return L
@@ -281,6 +283,13 @@ class Model:
     def stream(self) -> int:
         return int(self.L.sfg_model_stream(self._h) or 0)
 
+    def kernel_times(self, nsteps: int):
+        """Mean ms per launch of [step+boundary, momentum, sources, continuity] and launches per step."""
+        out = (ctypes.c_double * 4)()
+        lps = ctypes.c_int()
+        _check(self.L.sfg_model_kernel_times(self._h, int(nsteps), out, ctypes.byref(lps)), "kernel_times")
+        return list(out), lps.value
+
 
 class Ensemble:
     """Many uneven models advanced together by the same launches (per-member dt)."""
@@ -330,3 +339,9 @@ class Ensemble:
     @property
     def stream(self) -> int:
         return int(self.L.sfg_ensemble_stream(self._h) or 0)
+
+    def kernel_times(self, nsteps: int):
+        out = (ctypes.c_double * 4)()
+        lps = ctypes.c_int()
+        _check(self.L.sfg_ensemble_kernel_times(self._h, int(nsteps), out, ctypes.byref(lps)), "kernel_times")
+        return list(out), lps.value

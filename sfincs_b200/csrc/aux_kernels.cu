@@ -23,13 +23,17 @@ __global__ void k_gather_f64(const double* __restrict__ src, const int32_t* __re
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     out[i] = src[cmp[i]];
 }
-__global__ void k_gather_u8(const uint8_t* __restrict__ src, const int32_t* __restrict__ cmp, float* __restrict__ out,
-                            long long n) {
+// Wet flags (bit 0) of the u and v face of every cell: out[0:n] = u, out[n:2n] = v.
+__global__ void k_gather_u8(const uint8_t* __restrict__ ku, const uint8_t* __restrict__ kv,
+                            const int32_t* __restrict__ cmp, float* __restrict__ out, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const uint8_t k = src[cmp[i]];
-    out[i] = (float)(k & 1);
-    out[n + i] = (float)((k >> 1) & 1);
+    out[i] = (float)(ku[cmp[i]] & 1);
+    out[n + i] = (float)(kv[cmp[i]] & 1);
   }
+}
+__global__ void k_or_u8(uint8_t* __restrict__ a, uint8_t mask, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    a[i] |= mask;
 }
 __global__ void k_scatter_f32(const float* __restrict__ in, const int32_t* __restrict__ cmp, float* __restrict__ dst,
                               long long n) {
@@ -86,8 +90,12 @@ void launch_gather_f32(const float* src, const int32_t* cmp, float* out, long lo
 void launch_gather_f64(const double* src, const int32_t* cmp, double* out, long long n, cudaStream_t s) {
   if (n > 0) k_gather_f64<<<grid_for(n), 256, 0, s>>>(src, cmp, out, n);
 }
-void launch_gather_u8(const uint8_t* src, const int32_t* cmp, float* out, long long n, cudaStream_t s) {
-  if (n > 0) k_gather_u8<<<grid_for(n), 256, 0, s>>>(src, cmp, out, n);
+void launch_gather_u8(const uint8_t* ku, const uint8_t* kv, const int32_t* cmp, float* out, long long n,
+                      cudaStream_t s) {
+  if (n > 0) k_gather_u8<<<grid_for(n), 256, 0, s>>>(ku, kv, cmp, out, n);
+}
+void launch_or_u8(uint8_t* a, uint8_t mask, long long n, cudaStream_t s) {
+  if (n > 0) k_or_u8<<<grid_for(n), 256, 0, s>>>(a, mask, n);
 }
 void launch_scatter_f32(const float* in, const int32_t* cmp, float* dst, long long n, cudaStream_t s) {
   if (n > 0) k_scatter_f32<<<grid_for(n), 256, 0, s>>>(in, cmp, dst, n);

@@ -18,7 +18,9 @@ namespace sfg {
 void launch_gather_f32_f64(const float* src, const int32_t* cmp, double* out, long long n, cudaStream_t s);
 void launch_gather_f32(const float* src, const int32_t* cmp, float* out, long long n, cudaStream_t s);
 void launch_gather_f64(const double* src, const int32_t* cmp, double* out, long long n, cudaStream_t s);
-void launch_gather_u8(const uint8_t* src, const int32_t* cmp, float* out, long long n, cudaStream_t s);
+void launch_gather_u8(const uint8_t* ku, const uint8_t* kv, const int32_t* cmp, float* out, long long n,
+                      cudaStream_t s);
+void launch_or_u8(uint8_t* a, uint8_t mask, long long n, cudaStream_t s);
 void launch_scatter_f32(const float* in, const int32_t* cmp, float* dst, long long n, cudaStream_t s);
 void launch_scatter_f64_f32(const double* in, const int32_t* cmp, float* dst, long long n, cudaStream_t s);
 int volume_parts(long long n);
@@ -161,7 +163,7 @@ struct ModelHandle {
       f32(D.zsderv);
     } else if (name == "kfuv") {
       need((size_t)n * 8);
-      launch_gather_u8(D.kfuv, dev->d_cmp_off(), (float*)d_stage, n, s());
+      launch_gather_u8(D.kf[0], D.kf[1], dev->d_cmp_off(), (float*)d_stage, n, s());
       check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 8, cudaMemcpyDeviceToHost, s()), "get");
     } else {
       throw std::runtime_error("unknown variable '" + name + "'");
@@ -197,6 +199,11 @@ struct ModelHandle {
       put32(D.vv[p]);
     } else {
       throw std::runtime_error("variable '" + name + "' cannot be set");
+    }
+    if (name == "qx" || name == "qy" || name == "uvx" || name == "uvy") {
+      // host-written fluxes: make every face write its buffers on the next two steps
+      launch_or_u8(D.kf[0], KF_WET2, (long long)D.nalloc, s());
+      launch_or_u8(D.kf[1], KF_WET2, (long long)D.nalloc, s());
     }
     runner->sync();
     if (zs_exported && name == "zs") refresh_zs();
@@ -555,6 +562,19 @@ int sfg_model_volume(void* m, double* v) {
   });
 }
 void* sfg_model_stream(void* m) { return (void*)static_cast<sfg::ModelHandle*>(m)->s(); }
+int sfg_model_kernel_times(void* m, int nsteps, double ms_out[4], int* launches_per_step) {
+  return guarded([&] {
+    auto* h = static_cast<sfg::ModelHandle*>(m);
+    const double big = 1.0e300;
+    const int left = -1;
+    sfg::check_cuda(cudaMemcpyAsync(&h->dev->state()->tend, &big, 8, cudaMemcpyHostToDevice, h->s()), "tend");
+    sfg::check_cuda(cudaMemcpyAsync(&h->dev->state()->steps_left, &left, 4, cudaMemcpyHostToDevice, h->s()), "left");
+    auto t = h->runner->time_kernels(nsteps);
+    for (int k = 0; k < 4; k++) ms_out[k] = t[k];
+    if (launches_per_step) *launches_per_step = h->runner->launches_per_step();
+    return 0;
+  });
+}
 
 // ---------------------------------------------------------------- ensembles
 void* sfg_ensemble_create(const char* const* dirs, int n, int bmi, char* err, int errlen) {
@@ -663,6 +683,22 @@ int sfg_ensemble_get(void* ev, int i, const char* name, void* dst, size_t bytes)
   });
 }
 void* sfg_ensemble_stream(void* ev) { return (void*)static_cast<sfg::EnsembleHandle*>(ev)->runner->stream(); }
+int sfg_ensemble_kernel_times(void* ev, int nsteps, double ms_out[4], int* launches_per_step) {
+  return guarded([&] {
+    auto* e = static_cast<sfg::EnsembleHandle*>(ev);
+    const double big = 1.0e300;
+    const int left = -1;
+    for (auto& d : e->devs) {
+      sfg::check_cuda(cudaMemcpyAsync(&d->state()->tend, &big, 8, cudaMemcpyHostToDevice, e->runner->stream()), "tend");
+      sfg::check_cuda(cudaMemcpyAsync(&d->state()->steps_left, &left, 4, cudaMemcpyHostToDevice, e->runner->stream()),
+                      "left");
+    }
+    auto t = e->runner->time_kernels(nsteps);
+    for (int k = 0; k < 4; k++) ms_out[k] = t[k];
+    if (launches_per_step) *launches_per_step = e->runner->launches_per_step();
+    return 0;
+  });
+}
 
 int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst, size_t n) {
   return guarded([&]() -> int {
@@ -676,8 +712,8 @@ int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst
       for (long long i = 0; i < h.np; i++) out[i] = (double)get((size_t)h.cmp_off[i]);
     };
     if (nm == "counts") {
-      out = {(double)h.np, (double)h.npuv, (double)h.p.ngbnd, (double)h.p.nkcuv2, (double)h.p.nlev, (double)NA,
-             (double)h.p.dtmax, (double)h.p.dtmin};
+      out = {(double)h.np,    (double)h.npuv,  (double)h.p.ngbnd, (double)h.p.nkcuv2, (double)h.p.nlev,
+             (double)NA,      (double)h.p.dtmax, (double)h.p.dtmin, h.t0, h.t1};
     } else if (nm == "flags") {
       per_cell([&](size_t c) { return h.flags[c]; });
     } else if (nm == "zs") {
@@ -695,15 +731,15 @@ int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst
         out[h.np + i] = v[h.cmp_off[i]];
       }
     } else if (nm == "gb_cell") {
-      for (auto c : h.gb_cell) out.push_back((double)h.dense2cmp[c]);
-    } else if (nm == "gb_fac") {
-      for (auto f : h.gb_fac) out.push_back(f);
+      for (auto c : h.gb_cmp) out.push_back((double)c);
     } else if (nm == "kb_cell") {
-      for (auto c : h.kb_face) out.push_back((double)h.dense2cmp[c]);
+      for (auto& b : h.bfaces) out.push_back((double)h.dense2cmp[b.face]);
     } else if (nm == "kb_dir") {
-      for (auto d : h.kb_dir) out.push_back(d);
+      for (auto& b : h.bfaces) out.push_back((double)(b.info & 1));
     } else if (nm == "kb_sign") {
-      for (auto d : h.kb_sign) out.push_back(d);
+      for (auto& b : h.bfaces) out.push_back((b.info & 2) ? 1.0 : -1.0);
+    } else if (nm == "kb_fac") {
+      for (auto& b : h.bfaces) out.push_back((double)b.fac);
     } else {
       return -1;
     }

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 
@@ -317,26 +318,22 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
 
   // ---- boundaries (sfincs_domain.f90:1765-1958) -----------------------------------
   std::vector<int32_t> gb_index(NA, -1);
-  bool water_level_bnd = false, neumann_bnd = false;
+  std::vector<int32_t> gb_cell;
+  bool water_level_bnd = false;
   for (long long i = 0; i < h.np; i++) {
     const int64_t c = h.cmp_off[i];
     const int k = kcs[c];
     if (k == 2 || k == 3 || k == 5 || k == 6) {
-      gb_index[c] = (int32_t)h.gb_cell.size();
-      h.gb_cell.push_back((int32_t)c);
-      h.gb_kcs.push_back((int8_t)k);
+      gb_index[c] = (int32_t)gb_cell.size();
+      gb_cell.push_back((int32_t)c);
+      h.gb_cmp.push_back((int32_t)i);
       if (k == 2) water_level_bnd = true;
-      if (k == 6) neumann_bnd = true;
     }
   }
-  const size_t ngb = h.gb_cell.size();
-  h.zsb.assign(ngb, 0.0f);
-  h.zsb0.assign(ngb, 0.0f);
-  h.gb_i1.assign(ngb, 0);
-  h.gb_i2.assign(ngb, 0);
-  h.gb_fac.assign(ngb, 0.0f);
-  h.gb_nmi.assign(ngb, 0);
-  // kcuv==2/6 faces in reference ip order; outflow (kcs==3) levels fixed here
+  const size_t ngb = gb_cell.size();
+  std::vector<int> gb_i1(ngb, 0), gb_i2(ngb, 0), gb_nmi(ngb, -1);
+  std::vector<float> gb_fac(ngb, 0.0f), gb_zfix(ngb, 0.0f);
+  // kcuv==2/6 faces in reference ip order; outflow (kcs==3) levels are fixed here
   struct KB {
     int64_t face, nmb, nmi;
     int8_t dir, sign;
@@ -359,11 +356,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
       e.nmi = cu;
       e.sign = 1;
     }
-    const int ib = gb_index[e.nmb];
-    if (kcs[e.nmb] == 3) {
-      h.zsb0[ib] = P.subgrid ? h.zz_min[e.nmb] : h.zb[e.nmb];
-      h.zsb[ib] = h.zsb0[ib];
-    }
+    if (kcs[e.nmb] == 3) gb_zfix[gb_index[e.nmb]] = P.subgrid ? h.zz_min[e.nmb] : h.zb[e.nmb];
     kb_all.push_back(e);
   }
 
@@ -412,7 +405,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   // ---- find_boundary_indices (sfincs_boundaries.f90:455-679) -------------------------
   if (ngb > 0 && nbnd > 0) {
     for (size_t ib = 0; ib < ngb; ib++) {
-      const int64_t c = h.gb_cell[ib];
+      const int64_t c = gb_cell[ib];
       const long long ic = cmp_of[c];
       const float x = h.z_xz[ic], y = h.z_yz[ic];
       if (kcs[c] == 2) {
@@ -433,13 +426,11 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
             }
           }
           if (ib2 == 0) ib2 = ib1;
-          h.gb_i1[ib] = ib1 - 1;
-          h.gb_i2[ib] = ib2 - 1;
-          h.gb_fac[ib] = dst2 / std::max(dst1 + dst2, 1.0e-9f);
+          gb_i1[ib] = ib1 - 1;
+          gb_i2[ib] = ib2 - 1;
+          gb_fac[ib] = dst2 / std::max(dst1 + dst2, 1.0e-9f);
         } else {
-          h.gb_i1[ib] = 0;
-          h.gb_i2[ib] = 0;
-          h.gb_fac[ib] = 1.0f;
+          gb_fac[ib] = 1.0f;
         }
       } else if (kcs[c] == 6) {
         const int n = h.z_n[ic], m = h.z_m[ic];
@@ -447,25 +438,31 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
         int32_t nmi = -1;
         for (auto& q : cand)
           if (act(q[0], q[1]) && kcs[OFF(q[0], q[1])] == 1) nmi = (int32_t)OFF(q[0], q[1]);
-        if (nmi < 0) {
+        if (nmi < 0)
           kcs[c] = 0;  // isolated Neumann cell reset to inactive (sfincs_boundaries.f90:661-672)
-          h.gb_kcs[ib] = 0;
-        } else {
-          h.gb_nmi[ib] = nmi;
-        }
+        else
+          gb_nmi[ib] = nmi;
       }
     }
   }
-  (void)neumann_bnd;
+  for (size_t ib = 0; ib < ngb; ib++)
+    if (kcs[gb_cell[ib]] == 6 && gb_nmi[ib] >= 0) h.neu.push_back(make_int2(gb_cell[ib], gb_nmi[ib]));
   for (auto& e : kb_all) {
     if (kcs[e.nmb] == 6) continue;  // lateral Neumann faces are updated by the momentum kernel
-    h.kb_face.push_back((int32_t)e.face);
-    h.kb_dir.push_back(e.dir);
-    h.kb_gb.push_back(gb_index[e.nmb]);
-    h.kb_nmi.push_back((int32_t)e.nmi);
-    h.kb_sign.push_back(e.sign);
-    h.kb_zbuv.push_back(P.subgrid ? 0.0f
-                                  : 0.5f * (h.zb[e.face] + h.zb[e.dir == 0 ? e.face + ld : e.face + 1]));
+    const int ib = gb_index[e.nmb];
+    BndFace b{};
+    b.face = (int)e.face;
+    b.nmb = (int)e.nmb;
+    b.nmi = (int)e.nmi;
+    b.info = (e.dir == 1 ? 1 : 0) | (e.sign > 0 ? 2 : 0) | (kcs[e.nmb] == 3 ? 4 : 0) | (nbnd > 1 ? 8 : 0);
+    b.i1 = gb_i1[ib];
+    b.i2 = gb_i2[ib];
+    b.fac = gb_fac[ib];
+    b.zbuv = P.subgrid ? 0.0f : 0.5f * (h.zb[e.face] + h.zb[e.dir == 0 ? e.face + ld : e.face + 1]);
+    b.floor = P.subgrid ? h.zz_min[e.nmb] : h.zb[e.nmb];
+    b.zfix = gb_zfix[ib];
+    if (kcs[e.nmb] == 2 && nbnd == 0) b.info |= 4, b.zfix = 0.0f;  // no boundary data: zsb stays 0
+    h.bfaces.push_back(b);
   }
   h.dense2cmp = cmp_of;
   h.x0 = x0;
@@ -473,7 +470,8 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   h.cosrot = cosrot;
   h.sinrot = sinrot;
   P.ngbnd = (int)ngb;
-  P.nkcuv2 = (int)h.kb_face.size();
+  P.nkcuv2 = (int)h.bfaces.size();
+  P.nneu = (int)h.neu.size();
 
   // ---- roughness (sfincs_domain.f90:1960-2061) -------------------------------------------
   if (!P.subgrid) {
@@ -693,7 +691,8 @@ DeviceModel::DeviceModel(const HostModel& h) : h_(&h) {
     d_.zvol = upload(h.zvol);
     d_.zs0 = h.p.wiggle ? upload(h.zs0) : nullptr;
     d_.zsderv = h.p.wiggle ? alloc<float>(NA) : nullptr;
-    d_.kfuv = alloc<uint8_t>(NA);
+    d_.kf[0] = alloc<uint8_t>(NA);
+    d_.kf[1] = alloc<uint8_t>(NA);
     d_.vneg = h.p.subgrid ? upload(h.vneg) : nullptr;
     for (int b = 0; b < 2; b++) {
       d_.qu[b] = alloc<float>(NA);
@@ -722,21 +721,9 @@ DeviceModel::DeviceModel(const HostModel& h) : h_(&h) {
     d_.t_bnd = upload(h.t_bnd);
     d_.zs_bnd = upload(h.zs_bnd);
     d_.zst_bnd = alloc<float>((size_t)std::max(h.p.nbnd, 1));
-    d_.gb_cell = upload(h.gb_cell);
-    d_.gb_kcs = upload(h.gb_kcs);
-    d_.gb_i1 = upload(h.gb_i1);
-    d_.gb_i2 = upload(h.gb_i2);
-    d_.gb_fac = upload(h.gb_fac);
-    d_.gb_nmi = upload(h.gb_nmi);
-    d_.zsb = upload(h.zsb);
-    d_.zsb0 = upload(h.zsb0);
-    d_.kb_face = upload(h.kb_face);
-    d_.kb_dir = upload(h.kb_dir);
-    d_.kb_gb = upload(h.kb_gb);
-    d_.kb_nmi = upload(h.kb_nmi);
-    d_.kb_sign = upload(h.kb_sign);
-    d_.kb_zbuv = upload(h.kb_zbuv);
+    d_.bfaces = upload(h.bfaces);
     d_.uvmean = alloc<float>((size_t)std::max(h.p.nkcuv2, 1));
+    d_.neu = upload(h.neu);
     d_.tprcp = upload(h.tprcp);
     d_.vprcp = upload(h.vprcp);
     d_.twnd = upload(h.twnd);
@@ -783,6 +770,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m) : models_(std::move
     const HostModel& h = models_[i]->host();
     if (h.p.subgrid != subgrid_) throw std::runtime_error("an ensemble must be all-subgrid or all-regular");
     if (h.p.nsrc > 0) any_src_ = 1;
+    bnd_blocks_ = std::max(bnd_blocks_, (h.p.nkcuv2 + h.p.nneu + 127) / 128);
     scns.push_back(models_[i]->dev());
     const int nmax = h.p.nmax, mmax = h.p.mmax;
     for (int m0 = 1; m0 <= mmax; m0 += tile_m) {
@@ -807,6 +795,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m) : models_(std::move
     check_cuda(cudaMemcpy(d_tiles_, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice), "tiles");
   }
   check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  if (const char* v = std::getenv("SFG_MOMENTUM_VARIANT")) variant_ = std::atoi(v) == 3 ? 3 : 2;
   check_cuda(cudaMallocHost(&h_states_, models_.size() * sizeof(StepState)), "pinned states");
 }
 
@@ -826,7 +815,7 @@ void Runner::build_graph(int chunk) {
   }
   cudaGraph_t g;
   check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-  for (int i = 0; i < chunk; i++) launch_step(d_scns_, nscn(), d_tiles_, ntiles_, subgrid_, any_src_, stream_);
+  for (int i = 0; i < chunk; i++) launch_step(d_scns_, nscn(), bnd_blocks_, d_tiles_, ntiles_, subgrid_, any_src_, variant_, stream_);
   check_cuda(cudaStreamEndCapture(stream_, &g), "end capture");
   check_cuda(cudaGraphInstantiate(&graph_, g, 0), "graph instantiate");
   cudaGraphDestroy(g);
@@ -842,7 +831,39 @@ void Runner::refresh_params() {
 }
 
 void Runner::issue(int nsteps) {
-  for (int i = 0; i < nsteps; i++) launch_step(d_scns_, nscn(), d_tiles_, ntiles_, subgrid_, any_src_, stream_);
+  // whole chunks as CUDA-graph replays, the remainder as direct launches
+  const int chunk = 32;
+  if (nsteps >= chunk) {
+    build_graph(chunk);
+    for (int i = 0; i < nsteps / chunk; i++) check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+  }
+  for (int i = 0; i < nsteps % chunk; i++) launch_step(d_scns_, nscn(), bnd_blocks_, d_tiles_, ntiles_, subgrid_, any_src_, variant_, stream_);
+}
+
+std::vector<double> Runner::time_kernels(int nsteps) {
+  std::vector<cudaEvent_t> ev(5);
+  for (auto& e : ev) check_cuda(cudaEventCreate(&e), "event");
+  std::vector<double> acc(4, 0.0);
+  for (int i = 0; i < nsteps; i++) {
+    check_cuda(cudaEventRecord(ev[0], stream_), "record");
+    launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
+    check_cuda(cudaEventRecord(ev[1], stream_), "record");
+    launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
+    check_cuda(cudaEventRecord(ev[2], stream_), "record");
+    if (any_src_) launch_sources(d_scns_, nscn(), stream_);
+    check_cuda(cudaEventRecord(ev[3], stream_), "record");
+    launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
+    check_cuda(cudaEventRecord(ev[4], stream_), "record");
+    check_cuda(cudaEventSynchronize(ev[4]), "event sync");
+    for (int k = 0; k < 4; k++) {
+      float ms = 0.0f;
+      check_cuda(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]), "elapsed");
+      acc[k] += ms;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (auto& a : acc) a /= std::max(nsteps, 1);
+  return acc;
 }
 
 void Runner::sync() { check_cuda(cudaStreamSynchronize(stream_), "stream sync"); }

@@ -41,13 +41,10 @@ struct HostModel {
   std::vector<float> z_xz, z_yz, zb_cmp, zmin_cmp;  // compact, for the BMI data interface
   std::vector<int8_t> kcs_cmp;
   std::vector<int32_t> z_n, z_m;
-  // boundary lists
-  std::vector<int32_t> gb_cell, gb_i1, gb_i2, gb_nmi;
-  std::vector<int8_t> gb_kcs;
-  std::vector<float> gb_fac, zsb, zsb0;
-  std::vector<int32_t> kb_face, kb_gb, kb_nmi;
-  std::vector<int8_t> kb_dir, kb_sign;
-  std::vector<float> kb_zbuv;
+  // boundary lists (reference order of the kcuv==2 faces)
+  std::vector<BndFace> bfaces;
+  std::vector<int2> neu;               // Neumann cell, interior cell
+  std::vector<int32_t> gb_cmp;         // compact index of every boundary cell (diagnostics)
   // forcing series
   std::vector<float> t_bnd, zs_bnd;  // zs_bnd [ntbnd][nbnd]
   std::vector<float> tprcp, vprcp, twnd, wmag, wdir, cdval;
@@ -107,9 +104,23 @@ class Runner {
   void refresh_params();
   const ScnDev* d_scns() const { return d_scns_; }
   int ntiles() const { return ntiles_; }
+  int bnd_blocks() const { return bnd_blocks_; }
+  // kernel variant (momentum occupancy target); SFG_MOMENTUM_VARIANT overrides the default
+  void set_variant(int v) {
+    variant_ = v;
+    if (graph_) {
+      cudaGraphExecDestroy(graph_);
+      graph_ = nullptr;
+    }
+  }
+  int variant() const { return variant_; }
   int nscn() const { return (int)models_.size(); }
   // issue `nsteps` steps on the stream (no host sync); used for timing
   void issue(int nsteps);
+  // Issue nsteps steps with CUDA events between the launches; returns the mean
+  // duration (ms) of [step+boundary, momentum, sources, continuity] launches.
+  std::vector<double> time_kernels(int nsteps);
+  int launches_per_step() const { return 3 + any_src_; }
 
  private:
   void build_graph(int chunk);
@@ -117,6 +128,8 @@ class Runner {
   ScnDev* d_scns_ = nullptr;
   Tile* d_tiles_ = nullptr;
   int ntiles_ = 0;
+  int bnd_blocks_ = 0;
+  int variant_ = 2;
   int subgrid_ = 0;
   int any_src_ = 0;
   cudaStream_t stream_ = nullptr;
@@ -125,8 +138,13 @@ class Runner {
   StepState* h_states_ = nullptr;  // pinned mirror of the step states
 };
 
-void launch_step(const ScnDev* d_scns, int nscn, const Tile* d_tiles, int ntiles, int subgrid, int any_src,
-                 cudaStream_t s);
+void launch_step(const ScnDev* d_scns, int nscn, int bnd_blocks, const Tile* d_tiles, int ntiles, int subgrid,
+                 int any_src, int variant, cudaStream_t s);
+void launch_step_bnd(const ScnDev* d_scns, int nscn, int bnd_blocks, cudaStream_t s);
+void launch_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, int variant,
+                     cudaStream_t s);
+void launch_sources(const ScnDev* d_scns, int nscn, cudaStream_t s);
+void launch_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s);
 
 void check_cuda(cudaError_t e, const char* what);
 

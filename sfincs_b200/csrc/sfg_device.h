@@ -36,8 +36,27 @@ enum : uint16_t {
   F_VTH = 1u << 11,    // v face: same
 };
 
-// kfuv bits (uint8_t per cell, mutable)
-enum : uint8_t { K_U = 1u, K_V = 2u };
+// Per-face wet history (uint8_t, one array per face direction, mutable):
+// bit 0 = wet after the previous step (the reference's kfuv), bit 1 = wet the
+// step before.  A face dry for two consecutive steps holds q = uv = 0 in both
+// ping-pong buffers, so its (zero) writes are skipped.
+enum : uint8_t { KF_WET = 1u, KF_WET2 = 2u };
+
+// One water-level boundary face (kcuv == 2), packed so one thread reads it in
+// three 16-byte loads.  The boundary cell's level is recomputed per face from
+// the two nearest boundary points (sfincs_boundaries.f90:806-876).
+struct alignas(16) BndFace {
+  int face;      // dense offset of the face
+  int nmb;       // dense offset of the boundary cell
+  int nmi;       // dense offset of the interior cell
+  int info;      // bit0: v face; bit1: ibuvdir = +1 (else -1); bit2: outflow cell (kcs 3); bit3: multiple bnd points
+  int i1, i2;    // nearest boundary points (0-based)
+  float fac;     // weight of i1
+  float zbuv;    // zbuv of the face (regular grids; sfincs_domain.f90:1692)
+  float floor;   // zb or subgrid z_zmin of the boundary cell
+  float zfix;    // fixed level of an outflow (kcs 3) cell (sfincs_domain.f90:1937-1948)
+  int pad0, pad1;
+};
 
 // One subgrid uv lookup record: values at level k and the increment to k+1
 // (computed with the same float subtraction the reference performs inline at
@@ -63,10 +82,10 @@ struct alignas(16) StepState {
   int parity;          // which q/uv buffer holds the latest values
   int error;           // 1 = instability stop (sfincs_lib.f90:634-648)
   int stop_pending;    // instability detected: t := t1 + 1 at the next step
-  int single;          // update(): at most one step
+  float tbfac;         // boundary time-interpolation factor of the current step
+  int itb0, itb1;      // boundary time records of the current step (1-based)
   int steps_left;      // for single / bounded calls
   int itbndlast, itprcplast, itwndlast, itsrclast;
-  int pad_[2];
 };
 
 struct ScnDev {
@@ -85,7 +104,7 @@ struct ScnDev {
   double* zvol;
   float* zs0;
   float* zsderv;
-  uint8_t* kfuv;
+  uint8_t* kf[2];      // wet history of the u / v face owned by each cell
   uint8_t* vneg;       // subgrid: z_volume < 0 (written by continuity)
   float* qu[2];
   float* qv[2];
@@ -113,25 +132,13 @@ struct ScnDev {
   const float* qext;
   const float* qinf;     // infiltration field (m/s), con/c2d
   // ---- boundary forcing
-  int nbnd, ntbnd, ngbnd, nkcuv2;
+  int nbnd, ntbnd, nkcuv2, nneu, ngbnd;
   const float* t_bnd;    // [ntbnd]
   const float* zs_bnd;   // [ntbnd][nbnd]
-  float* zst_bnd;        // [nbnd]
-  const int* gb_cell;    // [ngbnd] boundary cell offset
-  const int8_t* gb_kcs;  // [ngbnd] kcs of the boundary cell (2,3,6)
-  const int* gb_i1;      // [ngbnd] nearest bnd points (0-based) and weight
-  const int* gb_i2;
-  const float* gb_fac;
-  const int* gb_nmi;     // [ngbnd] Neumann interior cell offset
-  float* zsb;            // [ngbnd]
-  float* zsb0;           // [ngbnd]
-  const int* kb_face;    // [nkcuv2] face offset
-  const int8_t* kb_dir;  // [nkcuv2] 0 = u face, 1 = v face
-  const int* kb_gb;      // [nkcuv2] index into the boundary-cell arrays
-  const int* kb_nmi;     // [nkcuv2] interior cell offset
-  const int8_t* kb_sign; // [nkcuv2] ibuvdir
-  const float* kb_zbuv;  // [nkcuv2] zbuv of the face at initialisation (regular grids)
+  float* zst_bnd;        // [nbnd] levels at the boundary points for the current step
+  const BndFace* bfaces; // [nkcuv2]
   float* uvmean;         // [nkcuv2]
+  const int2* neu;       // [nneu] Neumann (kcs 6) cell and its interior cell (dense offsets)
   // ---- time series (uniform meteo, point sources)
   int ntprcp, ntwnd, nsrc, ntsrc;
   const float* tprcp;

@@ -1,0 +1,116 @@
+"""Host-side layout of the B200 core against the oracle's literal index arrays.
+
+The core replaces the reference's explicit uv index arrays
+(sfincs_domain.f90:727-1261) by a dense grid with implicit neighbours and
+per-cell flag bits.  These CPU tests check, cell by cell, that the flags encode
+exactly the reference's face activity (kcuv), advection mask (mask_adv),
+regular-cell mask (kcs), initial state and boundary-face lists.
+"""
+import numpy as np
+import pytest
+
+from sfincs_b200 import bmi as B
+from sfincs_b200 import synth
+
+F_ACT, F_KCS1, F_UACT, F_VACT, F_UADV, F_VADV = 1, 2, 4, 8, 16, 32
+F_CDN, F_CUP, F_CLF, F_CRT = 64, 128, 256, 512
+
+
+def _oracle(d, prec="fp64"):
+    from oracle.oracle import Oracle
+
+    return Oracle(d, prec)
+
+
+def _masks():
+    def plain(**p):
+        m = synth.plain_regular(nmax=14, mmax=17, dx=300.0, tstop=600.0, nbumps=5)
+        m.params.update(p)
+        return m
+
+    out = {}
+    out["plain"] = plain()
+    m = plain(advection=1)
+    m.msk[5:8, 6:9] = 0            # hole
+    m.msk[0, 3:7] = 6              # lateral Neumann edge
+    m.msk[-1, 9:12] = 3            # outflow cells
+    m.msk[4, 0] = 0                # gap in the water-level boundary
+    out["holes_neumann_outflow_adv"] = m
+    m = plain(advection=1, advection_mask=0, theta=0.9)
+    m.msk[2:4, 2:4] = 0
+    out["adv_nomask_theta"] = m
+    m = plain()
+    m.bnd = np.array([[0.0, 500.0], [0.0, 3500.0], [0.0, 2000.0]])
+    tb = m.bzs[:, 0]
+    m.bzs = np.stack([tb, np.sin(tb / 3000.0), 0.5 * np.cos(tb / 2000.0), 0.2 + 0 * tb], axis=1)
+    out["three_bnd_points"] = m
+    return out
+
+
+MASKS = _masks()
+
+
+@pytest.mark.parametrize("name", sorted(MASKS))
+def test_flags_match_oracle_index_arrays(tmp_path, name):
+    d = MASKS[name].write(str(tmp_path))
+    o = _oracle(d)
+    s = o.scalars()
+    n = int(s["np"])
+    cnt = B.layout(d, "counts", 10)
+    assert int(cnt[0]) == n and int(cnt[1]) == int(s["npuv"])
+    assert cnt[6] == pytest.approx(s["dtmax"], rel=0, abs=0)
+    assert cnt[7] == pytest.approx(s["dtmin"], rel=0, abs=0)
+    assert cnt[8] == s["t0"] and cnt[9] == s["t1"]
+    flags = B.layout(d, "flags", n).astype(np.int64)
+    assert np.all(flags & F_ACT)
+    assert np.array_equal((flags & F_KCS1) > 0, o.get("kcs") == 1)
+    kcuv = o.get("kcuv")
+    cell = o.get("uv_nm").astype(np.int64) - 1
+    dirn = o.get("uv_dir").astype(np.int64)
+    act = np.isin(kcuv, (1, 6))
+    bit = np.where(dirn == 0, F_UACT, F_VACT)
+    assert np.array_equal((flags[cell] & bit) > 0, act)
+    if MASKS[name].params.get("advection", 0):
+        madv = o.get("mask_adv")
+        abit = np.where(dirn == 0, F_UADV, F_VADV)
+        assert np.array_equal((flags[cell] & abit) > 0, madv == 1)
+    # faces that do not exist in the reference are never active in the layout
+    nfaces = ((flags & F_UACT) > 0).sum() + ((flags & F_VACT) > 0).sum()
+    assert nfaces == act.sum()
+
+
+@pytest.mark.parametrize("name", sorted(MASKS))
+def test_boundary_faces_and_initial_state(tmp_path, name):
+    d = MASKS[name].write(str(tmp_path))
+    o = _oracle(d, "f32")
+    s = o.scalars()
+    cnt = B.layout(d, "counts", 10)
+    nkb = int(cnt[3])
+    kb_cell = B.layout(d, "kb_cell", nkb)
+    kb_dir = B.layout(d, "kb_dir", nkb)
+    kb_sign = B.layout(d, "kb_sign", nkb)
+    assert np.array_equal(kb_cell, o.get("kb_cell", nkb))
+    assert np.array_equal(kb_dir, o.get("kb_dir", nkb))
+    assert np.array_equal(kb_sign, o.get("kb_sign", nkb))
+    assert int(cnt[2]) == int(s["ngbnd"])
+    zs = B.layout(d, "zs", int(s["np"]))
+    assert np.array_equal(zs, o.get("zs"))
+
+
+def test_subgrid_tables_and_volumes(tmp_path):
+    m = synth.subgrid_regular(nmax=12, mmax=16, dx=400.0, P=6, tstop=1800.0, coast_x=2000.0)
+    d = m.write(str(tmp_path))
+    o = _oracle(d, "f32")
+    n = int(o.scalars()["np"])
+    cnt = B.layout(d, "counts", 10)
+    assert int(cnt[4]) == 10
+    assert np.array_equal(B.layout(d, "zs", n), o.get("zs"))
+    assert np.array_equal(B.layout(d, "zvol", n), o.get("z_volume"))
+
+
+def test_unsupported_inputs_are_refused(tmp_path):
+    m = synth.plain_regular(nmax=6, mmax=7, dx=300.0, tstop=600.0, nbumps=1)
+    m.params["thdfile"] = "sfincs.thd"
+    d = m.write(str(tmp_path))
+    with pytest.raises(RuntimeError, match="thdfile"):
+        B.layout(d, "counts", 10)

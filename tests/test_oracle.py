@@ -1,0 +1,150 @@
+"""Pins of the CPU oracle (the checker).
+
+The reference ships no tests or golden vectors and cannot be compiled here, so
+the oracle is pinned by (1) an independent pure-Python restatement of the plain
+step (tests/golden/pyref.py), (2) committed golden fixtures that freeze its
+output on small seeded cases, and (3) analytic invariants of the scheme.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+from sfincs_b200 import synth  # noqa: E402
+
+
+def _oracle(d, prec="fp64"):
+    from oracle.oracle import Oracle
+
+    return Oracle(d, prec)
+
+
+def test_oracle_matches_pure_python_restatement(tmp_path):
+    from pyref import PyRef
+
+    m = synth.plain_regular(nmax=6, mmax=8, dx=250.0, tstop=900.0, seed=11, nbumps=3)
+    m.msk[3, 4] = 0
+    d = m.write(str(tmp_path))
+    o = _oracle(d, "fp64")
+    bzs = np.loadtxt(os.path.join(d, "sfincs.bzs"))  # the values as written to the model file
+    f = np.float32
+    r = PyRef(m.msk, m.zb.astype(np.float64), 250.0, 250.0, zini=0.0, huthresh=0.01, alpha=0.5,
+              gn2_sea=float(f(9.81) * (f(0.02) * f(0.02))), gn2_land=float(f(9.81) * (f(0.04) * f(0.04))),
+              rgh_lev=0.0, t_bnd=bzs[:, 0].astype(np.float32).astype(np.float64),
+              zs_bnd=bzs[:, 1].astype(np.float32).astype(np.float64))
+    n_ = o.get("nm_n").astype(int) - 1
+    m_ = o.get("nm_m").astype(int) - 1
+    cell = o.get("uv_nm").astype(int) - 1
+    dirn = o.get("uv_dir").astype(int)
+    for step in range(40):
+        o.update(-1.0)
+        r.step()
+        zs_r = np.array([r.zs[a][b] for a, b in zip(n_, m_)])
+        q_r = np.array([(r.qu if d_ == 0 else r.qv)[(n_[c], m_[c])] for c, d_ in zip(cell, dirn)])
+        s = o.scalars()
+        assert s["t"] == pytest.approx(r.t, rel=1e-12)
+        np.testing.assert_allclose(o.get("zs"), zs_r, rtol=0, atol=1e-9, err_msg=f"zs step {step}")
+        np.testing.assert_allclose(o.get("q"), q_r, rtol=0, atol=1e-9, err_msg=f"q step {step}")
+
+
+@pytest.mark.parametrize("name", ["plain_6x8", "subgrid_8x10"])
+def test_golden_fixture(tmp_path, name):
+    import make_golden
+
+    case = {n: (m, k) for n, m, k in make_golden.cases()}[name]
+    m, nsteps = case
+    d = m.write(str(tmp_path))
+    o = _oracle(d, "fp64")
+    o.update(-1000.0, nsteps)
+    g = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    s = o.scalars()
+    assert s["nt"] == g["nt"] and s["t"] == pytest.approx(float(g["t"]), rel=1e-13)
+    np.testing.assert_allclose(o.get("zs"), g["zs"], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(o.get("q"), g["q"], rtol=0, atol=1e-11)
+    if "z_volume" in g:
+        np.testing.assert_allclose(o.get("z_volume"), g["z_volume"], rtol=1e-12, atol=1e-8)
+
+
+def _closed(m):
+    m.msk[:, :] = np.where(m.msk > 0, 1, 0)
+    m.bnd = None
+    m.bzs = None
+    return m
+
+
+@pytest.mark.parametrize("prec", ["fp64", "ref", "f32"])
+def test_lake_at_rest(tmp_path, prec):
+    m = _closed(synth.plain_regular(nmax=10, mmax=12, dx=300.0, tstop=1200.0, nbumps=4))
+    m.zb = np.minimum(m.zb, -1.0).astype(np.float32)
+    m.params["zsini"] = 0.25
+    d = m.write(str(tmp_path))
+    o = _oracle(d, prec)
+    z0 = o.get("zs")
+    o.update(-1000.0, 100)
+    assert np.array_equal(o.get("zs"), z0)
+    assert np.all(o.get("q") == 0.0)
+
+
+def test_dry_bed_stays_dry(tmp_path):
+    m = _closed(synth.plain_regular(nmax=8, mmax=9, dx=300.0, tstop=1200.0, nbumps=2))
+    m.zb = (m.zb + 20.0).astype(np.float32)  # everything above zsini
+    d = m.write(str(tmp_path))
+    o = _oracle(d)
+    z0 = o.get("zs")
+    o.update(-1000.0, 50)
+    assert np.array_equal(o.get("zs"), z0)
+
+
+def test_closed_basin_conserves_volume_regular(tmp_path):
+    m = _closed(synth.plain_regular(nmax=12, mmax=14, dx=200.0, tstop=3600.0, nbumps=5))
+    m.zb = np.minimum(m.zb, -0.5).astype(np.float32)
+    m.params["advection"] = 1
+    d = m.write(str(tmp_path))
+    o = _oracle(d)
+    zs = o.get("zs")
+    zs = zs + 0.5 * np.exp(-np.arange(zs.size) / 40.0)  # a mound of water
+    o.set("zs", zs)
+    zb = o.get("zb")
+    v0 = np.sum(o.get("zs") - zb)
+    o.update(-1000.0, 300)
+    v1 = np.sum(o.get("zs") - zb)
+    assert abs(v1 - v0) <= 1e-10 * abs(v0)
+    assert np.abs(o.get("q")).max() > 0  # water moved
+
+
+def test_rain_on_flat_closed_basin(tmp_path):
+    m = _closed(synth.plain_regular(nmax=6, mmax=7, dx=200.0, tstop=3600.0, nbumps=0))
+    m.zb = np.full_like(m.zb, -2.0)
+    m.prcp = np.array([[0.0, 36.0], [7200.0, 36.0]])  # 36 mm/h = 1e-5 m/s
+    d = m.write(str(tmp_path))
+    o = _oracle(d)
+    o.update(-1000.0, 60)
+    s = o.scalars()
+    zs = o.get("zs")
+    # every cell gained P * (t - t0); the rain rate is the real*4 value of 36 mm/h in m/s
+    p = float(np.float32(36.0) / np.float32(1000 * 3600))
+    assert np.ptp(zs) <= 1e-12
+    # (the time interpolation of the rain series is done in real*4: ~1e-7 relative wobble)
+    assert zs[0] - 0.0 == pytest.approx(p * (s["t"] - s["t0"]), rel=2e-7)
+
+
+def test_symmetric_dam_break(tmp_path):
+    m = _closed(synth.plain_regular(nmax=9, mmax=16, dx=100.0, tstop=3600.0, nbumps=0))
+    m.zb = np.full_like(m.zb, -1.0)
+    d = m.write(str(tmp_path))
+    o = _oracle(d)
+    n = o.get("nm_n").astype(int)
+    mm = o.get("nm_m").astype(int)
+    zs = np.where(mm <= 8, 1.0, 0.0)
+    o.set("zs", zs)
+    o.update(-1000.0, 80)
+    z = o.get("zs")
+    grid = np.zeros((9, 16))
+    grid[n - 1, mm - 1] = z
+    # mirror symmetry across the channel axis (n -> 10 - n)
+    np.testing.assert_allclose(grid, grid[::-1, :], rtol=0, atol=1e-12)
+    assert grid[:, 12].max() > 0.0  # the front travelled east
