@@ -795,16 +795,48 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m) : models_(std::move
     check_cuda(cudaMemcpy(d_tiles_, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice), "tiles");
   }
   check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
-  if (const char* v = std::getenv("SFG_MOMENTUM_VARIANT")) variant_ = std::atoi(v) == 3 ? 3 : 2;
+  if (const char* v = std::getenv("SFG_MOMENTUM_VARIANT")) {
+    const int x = std::atoi(v);
+    variant_ = (x == 2 || x == 3 || x == 4) ? x : 4;
+  }
+  // TMA tensor maps (one set per model) and persistent grid sizes
+  std::vector<MapSet> maps;
+  for (auto* m : models_) maps.push_back(build_map_set(m->dev()));
+  check_cuda(cudaMalloc(&d_maps_, maps.size() * sizeof(MapSet)), "cudaMalloc maps");
+  check_cuda(cudaMemcpy(d_maps_, maps.data(), maps.size() * sizeof(MapSet), cudaMemcpyHostToDevice), "maps");
+  int dev = 0, nsm = 0, nb_m = 0, nb_c = 0;
+  check_cuda(cudaGetDevice(&dev), "device");
+  check_cuda(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "sm count");
+  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_m, momentum_tma_fn(subgrid_), 256, momentum_tma_smem()),
+             "occupancy");
+  check_cuda(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_c, continuity_tma_fn(subgrid_), 256, continuity_tma_smem()),
+      "occupancy");
+  mom_grid_ = std::max(1, std::min(ntiles_, std::max(nb_m, 1) * nsm));
+  con_grid_ = std::max(1, std::min(ntiles_, std::max(nb_c, 1) * nsm));
   check_cuda(cudaMallocHost(&h_states_, models_.size() * sizeof(StepState)), "pinned states");
 }
 
 Runner::~Runner() {
   if (graph_) cudaGraphExecDestroy(graph_);
+  if (d_maps_) cudaFree(d_maps_);
   if (stream_) cudaStreamDestroy(stream_);
   if (d_scns_) cudaFree(d_scns_);
   if (d_tiles_) cudaFree(d_tiles_);
   if (h_states_) cudaFreeHost(h_states_);
+}
+
+void Runner::launch_one() {
+  launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
+  if (variant_ == 4)
+    launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, mom_grid_, stream_);
+  else
+    launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
+  if (any_src_) launch_sources(d_scns_, nscn(), stream_);
+  if (variant_ == 4)
+    launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_);
+  else
+    launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
 }
 
 void Runner::build_graph(int chunk) {
@@ -815,7 +847,7 @@ void Runner::build_graph(int chunk) {
   }
   cudaGraph_t g;
   check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-  for (int i = 0; i < chunk; i++) launch_step(d_scns_, nscn(), bnd_blocks_, d_tiles_, ntiles_, subgrid_, any_src_, variant_, stream_);
+  for (int i = 0; i < chunk; i++) launch_one();
   check_cuda(cudaStreamEndCapture(stream_, &g), "end capture");
   check_cuda(cudaGraphInstantiate(&graph_, g, 0), "graph instantiate");
   cudaGraphDestroy(g);
@@ -837,7 +869,7 @@ void Runner::issue(int nsteps) {
     build_graph(chunk);
     for (int i = 0; i < nsteps / chunk; i++) check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
   }
-  for (int i = 0; i < nsteps % chunk; i++) launch_step(d_scns_, nscn(), bnd_blocks_, d_tiles_, ntiles_, subgrid_, any_src_, variant_, stream_);
+  for (int i = 0; i < nsteps % chunk; i++) launch_one();
 }
 
 std::vector<double> Runner::time_kernels(int nsteps) {
@@ -848,11 +880,17 @@ std::vector<double> Runner::time_kernels(int nsteps) {
     check_cuda(cudaEventRecord(ev[0], stream_), "record");
     launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
     check_cuda(cudaEventRecord(ev[1], stream_), "record");
-    launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
+    if (variant_ == 4)
+      launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, mom_grid_, stream_);
+    else
+      launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
     check_cuda(cudaEventRecord(ev[2], stream_), "record");
     if (any_src_) launch_sources(d_scns_, nscn(), stream_);
     check_cuda(cudaEventRecord(ev[3], stream_), "record");
-    launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
+    if (variant_ == 4)
+      launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_);
+    else
+      launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
     check_cuda(cudaEventRecord(ev[4], stream_), "record");
     check_cuda(cudaEventSynchronize(ev[4]), "event sync");
     for (int k = 0; k < 4; k++) {

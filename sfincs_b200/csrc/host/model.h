@@ -114,6 +114,8 @@ class Runner {
     }
   }
   int variant() const { return variant_; }
+  // launch one step (all kernels) on the runner's stream
+  void launch_one();
   int nscn() const { return (int)models_.size(); }
   // issue `nsteps` steps on the stream (no host sync); used for timing
   void issue(int nsteps);
@@ -129,7 +131,9 @@ class Runner {
   Tile* d_tiles_ = nullptr;
   int ntiles_ = 0;
   int bnd_blocks_ = 0;
-  int variant_ = 2;
+  int variant_ = 4;
+  MapSet* d_maps_ = nullptr;  // TMA tensor maps, one set per model
+  int mom_grid_ = 0, con_grid_ = 0;
   int subgrid_ = 0;
   int any_src_ = 0;
   cudaStream_t stream_ = nullptr;
@@ -147,5 +151,15 @@ void launch_sources(const ScnDev* d_scns, int nscn, cudaStream_t s);
 void launch_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s);
 
 void check_cuda(cudaError_t e, const char* what);
+
+MapSet build_map_set(const ScnDev& d);
+int momentum_tma_smem();
+int continuity_tma_smem();
+const void* momentum_tma_fn(int subgrid);
+const void* continuity_tma_fn(int subgrid);
+void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
+                         int grid, cudaStream_t s);
+void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
+                           int grid, cudaStream_t s);
 
 }  // namespace sfg

@@ -1,0 +1,647 @@
+// TMA-staged momentum and continuity kernels (sm_100a).
+//
+// Same arithmetic as kernels.cu (sfincs_momentum.f90:157-752,
+// sfincs_continuity.f90:46-624), different memory pipeline: persistent CTAs of
+// 256 threads walk the tile table with a stride of gridDim.x; for every 32 x 8
+// cell tile one elected thread issues one 2-D cp.async.bulk.tensor load per
+// state array (the tile plus the one-cell halo the stencil reads) into a shared
+// memory stage, completing on an mbarrier.  Two stages: the next tile streams in
+// while the current one is computed.  Only the data-dependent subgrid table
+// records are still read with per-thread loads.
+//
+// All TMA coordinates keep the innermost coordinate a multiple of 16 bytes
+// (tile origins are 128-byte aligned, halos are rounded down to 4 floats / 8
+// half-words / 16 bytes), loads only (no TMA stores, no cluster multicast).
+// Every mbarrier wait is bounded: on timeout the CTA records a fault in the
+// scenario's step state, skips the tile and later drains its copies (bounded).
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "sfg_device.h"
+
+namespace sfg {
+
+// --------------------------------------------------------------------------
+// PTX helpers
+// --------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: ~2^22 try_wait rounds (each already suspends for a while) before giving up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ float warp_min_t(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// --------------------------------------------------------------------------
+// Shared-memory stage layouts (byte offsets; every box starts 128-byte aligned)
+// --------------------------------------------------------------------------
+namespace mom {
+// box widths / heights and the tile origin inside each box
+// zs/zsderv/zb: 36 x 9 (n0..n0+35, m0..m0+8); qu: 36 x 10 (m0-1..m0+8);
+// qv: 40 x 9 (n0-4..n0+35); uu, vv: 40 x 10 (n0-4.., m0-1..)
+constexpr int W_ZS = 36, W_QU = 36, W_QV = 40, W_UV = 40;
+constexpr int O_ZS = 0, O_QU = 1408, O_QV = 2944, O_UU = 4480, O_VV = 6144, O_FLAGS = 7808, O_KFU = 8320,
+              O_KFV = 8576;
+constexpr int O_VNEG = 8832, O_ZSD = 9344, O_SGZU = 10752, O_SGZV = 12800;       // subgrid
+constexpr int O_ZB = 8832, O_ZBMXU = 10240, O_ZBMXV = 11264, O_GN2U = 12288, O_GN2V = 13312;  // regular
+constexpr int STAGE = 14848;
+constexpr uint32_t B_COMMON = 36 * 9 * 4 + 36 * 10 * 4 + 40 * 9 * 4 + 2 * 40 * 10 * 4 + 32 * 8 * 2 + 2 * 32 * 8;
+}  // namespace mom
+
+namespace con {
+constexpr int O_QU = 0, O_QV = 1152, O_ZS = 2304, O_ZSMAX = 3328, O_FLAGS = 4352, O_ZVOL = 4864, O_VOLMAX = 6912,
+              O_VNEG = 7936, O_ZS0 = 8192, O_QEXT = 9216, O_QINF = 10240, O_ZB = 11264;
+constexpr int STAGE = 12288;
+}  // namespace con
+
+__device__ __forceinline__ const void* map_of(const MapSet* maps, int scn, int id) { return maps[scn].m[id]; }
+
+// --------------------------------------------------------------------------
+// Momentum
+// --------------------------------------------------------------------------
+template <bool SG>
+__device__ __forceinline__ bool issue_momentum(const ScnDev* scns, const MapSet* maps, const Tile& tl,
+                                               unsigned char* st, uint64_t* bar) {
+  const ScnDev& S = scns[tl.scn];
+  const StepState& ss = *S.st;
+  if (!ss.run) return false;
+  const int p = ss.parity;
+  const int x = kGhostPad + tl.n0;  // multiple of 32
+  const int y = tl.m0;
+  uint32_t bytes = mom::B_COMMON;
+  if (SG) bytes += 48 * 9 + 2 * 64 * 8 * 4 + (S.wiggle ? 36 * 9 * 4 : 0);
+  else bytes += 36 * 9 * 4 + 4 * 32 * 8 * 4;
+  mbar_expect_tx(bar, bytes);
+  tma_load_2d(st + mom::O_ZS, map_of(maps, tl.scn, MM_ZS), x, y, bar);
+  tma_load_2d(st + mom::O_QU, map_of(maps, tl.scn, MM_QU0 + p), x, y - 1, bar);
+  tma_load_2d(st + mom::O_QV, map_of(maps, tl.scn, MM_QV0 + p), x - 4, y, bar);
+  tma_load_2d(st + mom::O_UU, map_of(maps, tl.scn, MM_UU0 + p), x - 4, y - 1, bar);
+  tma_load_2d(st + mom::O_VV, map_of(maps, tl.scn, MM_VV0 + p), x - 4, y - 1, bar);
+  tma_load_2d(st + mom::O_FLAGS, map_of(maps, tl.scn, MM_FLAGS), x, y, bar);
+  tma_load_2d(st + mom::O_KFU, map_of(maps, tl.scn, MM_KFU), x, y, bar);
+  tma_load_2d(st + mom::O_KFV, map_of(maps, tl.scn, MM_KFV), x, y, bar);
+  if (SG) {
+    tma_load_2d(st + mom::O_VNEG, map_of(maps, tl.scn, MM_VNEG), x, y, bar);
+    if (S.wiggle) tma_load_2d(st + mom::O_ZSD, map_of(maps, tl.scn, MM_ZSD), x, y, bar);
+    tma_load_2d(st + mom::O_SGZU, map_of(maps, tl.scn, MM_SGZU), 2 * x, y, bar);
+    tma_load_2d(st + mom::O_SGZV, map_of(maps, tl.scn, MM_SGZV), 2 * x, y, bar);
+  } else {
+    tma_load_2d(st + mom::O_ZB, map_of(maps, tl.scn, MM_ZB), x, y, bar);
+    tma_load_2d(st + mom::O_ZBMXU, map_of(maps, tl.scn, MM_ZBMXU), x, y, bar);
+    tma_load_2d(st + mom::O_ZBMXV, map_of(maps, tl.scn, MM_ZBMXV), x, y, bar);
+    tma_load_2d(st + mom::O_GN2U, map_of(maps, tl.scn, MM_GN2U), x, y, bar);
+    tma_load_2d(st + mom::O_GN2V, map_of(maps, tl.scn, MM_GN2V), x, y, bar);
+  }
+  return true;
+}
+
+// Gathered inputs of one face (sfincs_momentum.f90:317-335 naming).
+struct FaceV {
+  float qx_nm, qx_nmd, qx_nmu, qy_nm, qy_nmu, qy_ndm, qy_ndmu;
+  float uu_nm, uu_nmd, uu_nmu, uu_ndm, uu_num, vu;
+};
+
+// Flux update of one wet face from gathered inputs (sfincs_momentum.f90:389-733).
+// Returns min_dt_ip; writes q, uv.
+template <bool SG, int DIR>
+__device__ __forceinline__ float face_flux(const ScnDev& S, const StepState& st, uint16_t f, uint8_t kf, float zs_nm,
+                                           float zs_nmu, float hu, float gnavg2, float phi, const FaceV& a,
+                                           bool dry_nm, bool dry_nmu, float zd_nm, float zd_nmu, float& q_out,
+                                           float& uv_out) {
+  constexpr uint16_t ADV = DIR == 0 ? F_UADV : F_VADV;
+  constexpr uint16_t TH = DIR == 0 ? F_UTH : F_VTH;
+  const float dxuvinv = DIR == 0 ? S.dxinv : S.dyinv;
+  const float dyuvinv = DIR == 0 ? S.dyinv : S.dxinv;
+  const float dxuv2inv = DIR == 0 ? S.dx2inv : S.dy2inv;
+  const float dyuv2inv = DIR == 0 ? S.dy2inv : S.dx2inv;
+  const float hwet = hu / phi;
+  float dzdx;
+  if (S.slopelim < 9999.0f)
+    dzdx = fminf(fmaxf((zs_nmu - zs_nm) * dxuvinv, -S.slopelim), S.slopelim);
+  else
+    dzdx = (zs_nmu - zs_nm) * dxuvinv;
+  float frc = -S.g * hu * dzdx;
+  if (S.advection && (f & ADV)) {
+    float dqxudx = 0.0f, dqyudy = 0.0f;
+    if (S.adv_scheme == 0) {
+      if (a.qx_nm > 1.0e-6f)
+        dqxudx = (a.qx_nm * a.uu_nm - a.qx_nmd * a.uu_nmd) * dxuvinv;
+      else if (a.qx_nm < -1.0e-6f)
+        dqxudx = (a.qx_nmu * a.uu_nmu - a.qx_nm * a.uu_nm) * dxuvinv;
+      const float qy = a.qy_ndm + a.qy_ndmu + a.qy_nm + a.qy_nmu;
+      if (qy > 1.0e-6f)
+        dqyudy = (a.qy_ndm + a.qy_ndmu) * (a.uu_nm - a.uu_ndm) * dyuvinv / 2.0f;
+      else if (qy < -1.0e-6f)
+        dqyudy = (a.qy_nm + a.qy_nmu) * (a.uu_num - a.uu_nm) * dyuvinv / 2.0f;
+    } else {
+      float qd = (a.qx_nmd + a.qx_nm) / 2.0f;
+      float qu = (a.qx_nm + a.qx_nmu) / 2.0f;
+      if (qd > 1.0e-6f) {
+        const float ud = (a.uu_nmd + a.uu_nm) / 2.0f;
+        dqxudx = (qd * (a.uu_nm - a.uu_nmd) + ud * (a.qx_nm - a.qx_nmd)) * dxuvinv;
+      }
+      if (qu < -1.0e-6f) {
+        const float uu = (a.uu_nm + a.uu_nmu) / 2.0f;
+        dqxudx = dqxudx + (qu * (a.uu_nmu - a.uu_nm) + uu * (a.qx_nmu - a.qx_nm)) * dxuvinv;
+      }
+      qu = (a.qy_nm + a.qy_nmu) / 2.0f;
+      qd = (a.qy_ndm + a.qy_ndmu) / 2.0f;
+      if (qd > 1.0e-6f) dqyudy = qd * (a.uu_nm - a.uu_ndm) * dyuvinv;
+      if (qu < -1.0e-6f) dqyudy = dqyudy + qu * (a.uu_num - a.uu_nm) * dyuvinv;
+      const float ud = (a.uu_nmd + a.uu_nm) / 2.0f;
+      const float uu = (a.uu_nm + a.uu_nmu) / 2.0f;
+      if (ud > 1.0e-6f) dqyudy = dqyudy + ud * (a.qy_nm - a.qy_ndm) * dyuvinv;
+      if (uu < -1.0e-6f) dqyudy = dqyudy + uu * (a.qy_nmu - a.qy_ndmu) * dyuvinv;
+    }
+    float adv = -phi * (dqxudx + dqyudy);
+    adv = fminf(fmaxf(adv, -S.advlim * hu), S.advlim * hu);
+    frc = frc + adv;
+  }
+  if (S.viscosity) {
+    frc = frc + S.nuvisc * hu *
+                    ((a.uu_nmu - 2.0f * a.uu_nm + a.uu_nmd) * dxuv2inv +
+                     (a.uu_num - 2.0f * a.uu_nm + a.uu_ndm) * dyuv2inv);
+  }
+  if (S.coriolis) {
+    if (DIR == 0)
+      frc = frc + S.fcorio * hu * a.vu;
+    else
+      frc = frc - S.fcorio * hu * a.vu;
+  }
+  if (S.wind) {
+    const float tauw = DIR == 0 ? st.twu : st.twv;
+    if (hwet > 0.25f)
+      frc = frc + phi * tauw;
+    else
+      frc = frc + tauw * hu * 4.0f;
+  }
+  float qfr;
+  if (!(kf & KF_WET)) {
+    qfr = sqrtf(fabsf(dzdx) / (fmaxf(gnavg2, 1.0e-5f) / 10.0f)) * powf(hu, 5.0f / 3.0f);
+  } else if (S.friction2d) {
+    qfr = sqrtf(a.qx_nm * a.qx_nm + (hu * a.vu) * (hu * a.vu));
+  } else {
+    qfr = fabsf(a.qx_nm);
+  }
+  float qsm = a.qx_nm;
+  if (S.thetasmooth && (f & TH) && fabsf(a.qx_nmd) > 1.0e-6f && fabsf(a.qx_nmu) > 1.0e-6f)
+    qsm = S.theta * a.qx_nm + 0.5f * (1.0f - S.theta) * (a.qx_nmu + a.qx_nmd);
+  const float dt = st.dt;
+  const float hu73 = hu * hu * powf(hu, 1.0f / 3.0f);
+  float q = (qsm + frc * dt) / (1.0f + gnavg2 * dt * qfr / hu73);
+  if (SG && S.wiggle) {
+    const float mdrv = fabsf(zd_nm - zd_nmu) - S.wiggle_threshold;
+    if (mdrv > 0.0f) q = q * S.wiggle_threshold / (S.wiggle_factor * mdrv + S.wiggle_threshold);
+  }
+  if (dry_nm) q = fminf(q, 0.0f);
+  if (dry_nmu) q = fmaxf(q, 0.0f);
+  q = fminf(fmaxf(q, -hu * S.uvlim), hu * S.uvlim);
+  const float uv = q / fmaxf(hu, S.huvmin);
+  q_out = q;
+  uv_out = uv;
+  return 1.0f / (fmaxf(sqrtf(S.g * hu), fabsf(uv)) * dxuvinv);
+}
+
+// Subgrid depth / roughness / wet fraction at the face level zsu (sfincs_momentum.f90:345-380).
+struct SgLook {
+  bool full;
+  float facint;
+  float4 w;   // full branch
+  UvRec r;    // interpolation branch
+};
+
+template <bool SG>
+__global__ void __launch_bounds__(256) k_momentum_tma(const ScnDev* __restrict__ scns, const MapSet* __restrict__ maps,
+                                                      const Tile* __restrict__ tiles, int ntiles) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int s_issued[2];
+  __shared__ float s_min[8];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + 32 * ty;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint32_t phase[2] = {0u, 0u};
+  int tile = blockIdx.x;
+  if (tid == 0) s_issued[0] = tile < ntiles ? issue_momentum<SG>(scns, maps, tiles[tile], smem, &bar[0]) : 0;
+  for (int it = 0; tile < ntiles; it++) {
+    const int s = it & 1;
+    const int next = tile + gridDim.x;
+    __syncthreads();  // s_issued[s] visible; stage s^1 no longer read
+    if (tid == 0) {
+      fence_proxy_async();
+      s_issued[s ^ 1] =
+          next < ntiles ? issue_momentum<SG>(scns, maps, tiles[next], smem + (s ^ 1) * mom::STAGE, &bar[s ^ 1]) : 0;
+    }
+    if (s_issued[s]) {
+      const Tile tl = tiles[tile];
+      const ScnDev& S = scns[tl.scn];
+      StepState& st = *S.st;
+      const bool ok = mbar_wait_bounded(&bar[s], phase[s]);
+      phase[s] ^= 1u;
+      float mdt = FLT_MAX;
+      const int n = tl.n0 + tx, m = tl.m0 + ty;
+      if (!ok) {
+        st.fault = 1;
+      } else if (n <= S.nmax && m <= S.mmax) {
+        const unsigned char* sm = smem + s * mom::STAGE;
+        const float* zs = (const float*)(sm + mom::O_ZS);
+        const float* qu = (const float*)(sm + mom::O_QU);
+        const float* qv = (const float*)(sm + mom::O_QV);
+        const float* uu = (const float*)(sm + mom::O_UU);
+        const float* vv = (const float*)(sm + mom::O_VV);
+        auto ZS = [&](int dm, int dn) { return zs[(ty + dm) * mom::W_ZS + tx + dn]; };
+        auto QU = [&](int dm, int dn) { return qu[(ty + 1 + dm) * mom::W_QU + tx + dn]; };
+        auto QV = [&](int dm, int dn) { return qv[(ty + dm) * mom::W_QV + tx + 4 + dn]; };
+        auto UU = [&](int dm, int dn) { return uu[(ty + 1 + dm) * mom::W_UV + tx + 4 + dn]; };
+        auto VV = [&](int dm, int dn) { return vv[(ty + 1 + dm) * mom::W_UV + tx + 4 + dn]; };
+        const uint16_t f = ((const uint16_t*)(sm + mom::O_FLAGS))[ty * 32 + tx];
+        const uint8_t kfu = (sm + mom::O_KFU)[ty * 32 + tx];
+        const uint8_t kfv = (sm + mom::O_KFV)[ty * 32 + tx];
+        const int64_t c = (int64_t)m * S.ld + kGhostPad + n;
+        const int p = st.parity;
+        const float zs_c = ZS(0, 0), zs_u = ZS(1, 0), zs_v = ZS(0, 1);
+        const float zsu_u = fmaxf(zs_c, zs_u), zsu_v = fmaxf(zs_c, zs_v);
+        float zmin_u, zmax_u = 0.0f, zmin_v, zmax_v = 0.0f;
+        if (SG) {
+          const float* gu = (const float*)(sm + mom::O_SGZU);
+          const float* gv = (const float*)(sm + mom::O_SGZV);
+          zmin_u = gu[ty * 64 + 2 * tx];
+          zmax_u = gu[ty * 64 + 2 * tx + 1];
+          zmin_v = gv[ty * 64 + 2 * tx];
+          zmax_v = gv[ty * 64 + 2 * tx + 1];
+        } else {
+          zmin_u = ((const float*)(sm + mom::O_ZBMXU))[ty * 32 + tx];
+          zmin_v = ((const float*)(sm + mom::O_ZBMXV))[ty * 32 + tx];
+        }
+        const bool act_u = f & F_UACT, act_v = f & F_VACT;
+        const bool wet_u = act_u && (SG ? zsu_u > zmin_u + S.huthresh : zsu_u > zmin_u);
+        const bool wet_v = act_v && (SG ? zsu_v > zmin_v + S.huthresh : zsu_v > zmin_v);
+        // ---- issue the data-dependent table loads of both faces first
+        SgLook lu{}, lv{};
+        if (SG) {
+          auto look = [&](bool wet, float zsu, float zmin, float zmax, const float4* W, const UvRec* R, SgLook& L) {
+            if (!wet) return;
+            if (zsu > zmax) {
+              L.full = true;
+              L.w = W[c];
+            } else {
+              L.full = false;
+              const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
+              int iuv = (int)((zsu - zmin) / dzuv) + 1;
+              iuv = min(iuv, S.nlev - 1);
+              L.facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
+              L.r = R[(int64_t)(iuv - 1) * S.nalloc + c];
+            }
+          };
+          look(wet_u, zsu_u, zmin_u, zmax_u, S.sgw_u, S.rec_u, lu);
+          look(wet_v, zsu_v, zmin_v, zmax_v, S.sgw_v, S.rec_v, lv);
+        }
+        // ---- u face
+        if (act_u) {
+          float qn = 0.0f, un = 0.0f;
+          if (wet_u) {
+            FaceV a;
+            a.qx_nm = QU(0, 0);
+            a.qx_nmd = QU(-1, 0);
+            a.qx_nmu = QU(1, 0);
+            a.qy_nm = QV(0, 0);
+            a.qy_nmu = QV(1, 0);
+            a.qy_ndm = QV(0, -1);
+            a.qy_ndmu = QV(1, -1);
+            a.uu_nm = UU(0, 0);
+            a.uu_nmd = UU(-1, 0);
+            a.uu_nmu = UU(1, 0);
+            a.uu_ndm = (f & F_CDN) ? UU(0, -1) : a.uu_nm;
+            a.uu_num = (f & F_CUP) ? UU(0, 1) : a.uu_nm;
+            a.vu = (VV(0, -1) + VV(1, -1) + VV(0, 0) + VV(1, 0)) / 4.0f;
+            float hu, gnavg2, phi = 1.0f, zd0 = 0.0f, zd1 = 0.0f;
+            bool dry0, dry1;
+            if (SG) {
+              const uint8_t* vn = sm + mom::O_VNEG;
+              dry0 = vn[ty * 48 + tx] != 0;
+              dry1 = vn[(ty + 1) * 48 + tx] != 0;
+              if (S.wiggle) {
+                const float* zd = (const float*)(sm + mom::O_ZSD);
+                zd0 = zd[ty * mom::W_ZS + tx];
+                zd1 = zd[(ty + 1) * mom::W_ZS + tx];
+              }
+              if (lu.full) {
+                hu = lu.w.x + zsu_u;
+                gnavg2 = lu.w.z - (lu.w.z - lu.w.y) / (lu.w.w * (zsu_u - zmax_u) + 1.0f);
+              } else {
+                hu = lu.r.havg + lu.r.dhavg * lu.facint;
+                gnavg2 = lu.r.nrep + lu.r.dnrep * lu.facint;
+                phi = lu.r.pwet + lu.r.dpwet * lu.facint;
+              }
+            } else {
+              const float* zb = (const float*)(sm + mom::O_ZB);
+              dry0 = zs_c < zb[ty * mom::W_ZS + tx];
+              dry1 = zs_u < zb[(ty + 1) * mom::W_ZS + tx];
+              hu = fmaxf(zsu_u - zmin_u, S.huthresh);
+              gnavg2 = ((const float*)(sm + mom::O_GN2U))[ty * 32 + tx];
+            }
+            mdt = fminf(mdt, face_flux<SG, 0>(S, st, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1,
+                                              qn, un));
+            S.qu[p ^ 1][c] = qn;
+            S.uu[p ^ 1][c] = un;
+          } else if (kfu & KF_WET2) {
+            S.qu[p ^ 1][c] = 0.0f;
+            S.uu[p ^ 1][c] = 0.0f;
+          }
+          const uint8_t kn = wet_u ? (uint8_t)(KF_WET | ((kfu & KF_WET) ? KF_WET2 : 0))
+                                   : (uint8_t)((kfu & KF_WET) ? KF_WET2 : 0);
+          if (kn != kfu) S.kf[0][c] = kn;
+        }
+        // ---- v face
+        if (act_v) {
+          float qn = 0.0f, un = 0.0f;
+          if (wet_v) {
+            FaceV a;
+            a.qx_nm = QV(0, 0);
+            a.qx_nmd = QV(0, -1);
+            a.qx_nmu = QV(0, 1);
+            a.qy_nm = QU(0, 0);
+            a.qy_nmu = QU(0, 1);
+            a.qy_ndm = QU(-1, 0);
+            a.qy_ndmu = QU(-1, 1);
+            a.uu_nm = VV(0, 0);
+            a.uu_nmd = VV(0, -1);
+            a.uu_nmu = VV(0, 1);
+            a.uu_ndm = (f & F_CLF) ? VV(-1, 0) : a.uu_nm;
+            a.uu_num = (f & F_CRT) ? VV(1, 0) : a.uu_nm;
+            a.vu = (UU(-1, 0) + UU(-1, 1) + UU(0, 0) + UU(0, 1)) / 4.0f;
+            float hu, gnavg2, phi = 1.0f, zd0 = 0.0f, zd1 = 0.0f;
+            bool dry0, dry1;
+            if (SG) {
+              const uint8_t* vn = sm + mom::O_VNEG;
+              dry0 = vn[ty * 48 + tx] != 0;
+              dry1 = vn[ty * 48 + tx + 1] != 0;
+              if (S.wiggle) {
+                const float* zd = (const float*)(sm + mom::O_ZSD);
+                zd0 = zd[ty * mom::W_ZS + tx];
+                zd1 = zd[ty * mom::W_ZS + tx + 1];
+              }
+              if (lv.full) {
+                hu = lv.w.x + zsu_v;
+                gnavg2 = lv.w.z - (lv.w.z - lv.w.y) / (lv.w.w * (zsu_v - zmax_v) + 1.0f);
+              } else {
+                hu = lv.r.havg + lv.r.dhavg * lv.facint;
+                gnavg2 = lv.r.nrep + lv.r.dnrep * lv.facint;
+                phi = lv.r.pwet + lv.r.dpwet * lv.facint;
+              }
+            } else {
+              const float* zb = (const float*)(sm + mom::O_ZB);
+              dry0 = zs_c < zb[ty * mom::W_ZS + tx];
+              dry1 = zs_v < zb[ty * mom::W_ZS + tx + 1];
+              hu = fmaxf(zsu_v - zmin_v, S.huthresh);
+              gnavg2 = ((const float*)(sm + mom::O_GN2V))[ty * 32 + tx];
+            }
+            mdt = fminf(mdt, face_flux<SG, 1>(S, st, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1,
+                                              qn, un));
+            S.qv[p ^ 1][c] = qn;
+            S.vv[p ^ 1][c] = un;
+          } else if (kfv & KF_WET2) {
+            S.qv[p ^ 1][c] = 0.0f;
+            S.vv[p ^ 1][c] = 0.0f;
+          }
+          const uint8_t kn = wet_v ? (uint8_t)(KF_WET | ((kfv & KF_WET) ? KF_WET2 : 0))
+                                   : (uint8_t)((kfv & KF_WET) ? KF_WET2 : 0);
+          if (kn != kfv) S.kf[1][c] = kn;
+        }
+      }
+      // CTA min of the CFL step, one atomicMin per tile
+      mdt = warp_min_t(mdt);
+      if (tx == 0) s_min[ty] = mdt;
+      __syncthreads();
+      if (ty == 0) {
+        float v = tx < 8 ? s_min[tx] : FLT_MAX;
+        v = warp_min_t(v);
+        if (tx == 0 && v < FLT_MAX) atomicMin(&st.min_dt_bits, __float_as_uint(v));
+      }
+    }
+    tile = next;
+  }
+  // drain: every issued stage has been waited for in the loop; nothing in flight here
+}
+
+// --------------------------------------------------------------------------
+// Continuity
+// --------------------------------------------------------------------------
+template <bool SG>
+__device__ __forceinline__ bool issue_continuity(const ScnDev* scns, const MapSet* maps, const Tile& tl,
+                                                 unsigned char* st, uint64_t* bar) {
+  const ScnDev& S = scns[tl.scn];
+  const StepState& ss = *S.st;
+  if (!ss.run) return false;
+  const int p1 = ss.parity ^ 1;
+  const int x = kGhostPad + tl.n0;
+  const int y = tl.m0;
+  uint32_t bytes = 32 * 9 * 4 + 36 * 8 * 4 + 32 * 8 * 4 * 2 + 32 * 8 * 2;
+  if (SG) bytes += 32 * 8 * 8 + 32 * 8 * 4 + 32 * 8 + (S.wiggle ? 32 * 8 * 4 : 0);
+  if (S.use_qext) bytes += 32 * 8 * 4;
+  if (S.infiltration) bytes += 32 * 8 * 4 + (SG ? 0 : 32 * 8 * 4);
+  mbar_expect_tx(bar, bytes);
+  tma_load_2d(st + con::O_QU, map_of(maps, tl.scn, MC_QU0 + p1), x, y - 1, bar);
+  tma_load_2d(st + con::O_QV, map_of(maps, tl.scn, MC_QV0 + p1), x - 4, y, bar);
+  tma_load_2d(st + con::O_ZS, map_of(maps, tl.scn, MC_ZS), x, y, bar);
+  tma_load_2d(st + con::O_ZSMAX, map_of(maps, tl.scn, MC_ZSMAX), x, y, bar);
+  tma_load_2d(st + con::O_FLAGS, map_of(maps, tl.scn, MC_FLAGS), x, y, bar);
+  if (SG) {
+    tma_load_2d(st + con::O_ZVOL, map_of(maps, tl.scn, MC_ZVOL), x, y, bar);
+    tma_load_2d(st + con::O_VOLMAX, map_of(maps, tl.scn, MC_VOLMAX), x, y, bar);
+    tma_load_2d(st + con::O_VNEG, map_of(maps, tl.scn, MC_VNEG), x, y, bar);
+    if (S.wiggle) tma_load_2d(st + con::O_ZS0, map_of(maps, tl.scn, MC_ZS0), x, y, bar);
+  }
+  if (S.use_qext) tma_load_2d(st + con::O_QEXT, map_of(maps, tl.scn, MC_QEXT), x, y, bar);
+  if (S.infiltration) {
+    tma_load_2d(st + con::O_QINF, map_of(maps, tl.scn, MC_QINF), x, y, bar);
+    if (!SG) tma_load_2d(st + con::O_ZB, map_of(maps, tl.scn, MC_ZB), x, y, bar);
+  }
+  return true;
+}
+
+template <bool SG>
+__global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict__ scns, const MapSet* __restrict__ maps,
+                                                        const Tile* __restrict__ tiles, int ntiles) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int s_issued[2];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + 32 * ty;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint32_t phase[2] = {0u, 0u};
+  int tile = blockIdx.x;
+  if (tid == 0) s_issued[0] = tile < ntiles ? issue_continuity<SG>(scns, maps, tiles[tile], smem, &bar[0]) : 0;
+  for (int it = 0; tile < ntiles; it++) {
+    const int s = it & 1;
+    const int next = tile + gridDim.x;
+    __syncthreads();
+    if (tid == 0) {
+      fence_proxy_async();
+      s_issued[s ^ 1] =
+          next < ntiles ? issue_continuity<SG>(scns, maps, tiles[next], smem + (s ^ 1) * con::STAGE, &bar[s ^ 1])
+                        : 0;
+    }
+    if (s_issued[s]) {
+      const Tile tl = tiles[tile];
+      const ScnDev& S = scns[tl.scn];
+      StepState& st = *S.st;
+      const bool ok = mbar_wait_bounded(&bar[s], phase[s]);
+      phase[s] ^= 1u;
+      const int n = tl.n0 + tx, m = tl.m0 + ty;
+      if (!ok) {
+        st.fault = 1;
+      } else if (n <= S.nmax && m <= S.mmax) {
+        const unsigned char* sm = smem + s * con::STAGE;
+        const int k = ty * 32 + tx;
+        const uint16_t f = ((const uint16_t*)(sm + con::O_FLAGS))[k];
+        if (f & F_ACT) {
+          const int64_t c = (int64_t)m * S.ld + kGhostPad + n;
+          const float* qu = (const float*)(sm + con::O_QU);
+          const float* qv = (const float*)(sm + con::O_QV);
+          const float q_md = qu[ty * 32 + tx], q_mu = qu[(ty + 1) * 32 + tx];
+          const float q_nd = qv[ty * 36 + tx + 3], q_nu = qv[ty * 36 + tx + 4];
+          const float zs_old = ((const float*)(sm + con::O_ZS))[k];
+          const float zm = ((const float*)(sm + con::O_ZSMAX))[k];
+          const float dt = st.dt;
+          float zsn = zs_old;
+          if (f & F_KCS1) {
+            const float qx = S.use_qext ? ((const float*)(sm + con::O_QEXT))[k] : 0.0f;
+            const float qi = S.infiltration ? ((const float*)(sm + con::O_QINF))[k] : 0.0f;
+            if (SG) {
+              const double v_old = ((const double*)(sm + con::O_ZVOL))[k];
+              const float volmax = ((const float*)(sm + con::O_VOLMAX))[k];
+              const uint8_t vn_old = (sm + con::O_VNEG)[k];
+              const float zs00 = S.wiggle ? ((const float*)(sm + con::O_ZS0))[k] : 0.0f;
+              float dvol = ((q_md - q_mu) * S.dy + (q_nd - q_nu) * S.dx) * dt;
+              if (S.precip || S.use_qext) {
+                float dzsdt = 0.0f;
+                if (S.precip) {
+                  const float qinfmap = (S.infiltration && v_old > 0.0) ? qi : 0.0f;
+                  dzsdt = dzsdt + (st.ptmp - qinfmap);
+                }
+                if (S.use_qext) dzsdt = dzsdt + qx;
+                dvol = dvol + dzsdt * S.area * dt;
+              }
+              const double v = v_old + (double)dvol;
+              if (v != v_old) S.zvol[c] = v;
+              const float zs11 = zs_old;
+              if (v >= (double)(volmax * 0.999f)) {
+                zsn = (float)((double)fmaxf(S.zz_max[c], -20.0f) + (v - (double)volmax) / (double)S.area);
+              } else if (v <= (double)1.0e-6f) {
+                zsn = fmaxf(S.zz_min[c], -20.0f);
+              } else {
+                const float dzvol = volmax / (float)(S.nlev - 1);
+                const int iuv = (int)(v / (double)dzvol) + 1;
+                const float facint = (float)((v - (double)((float)(iuv - 1) * dzvol)) / (double)dzvol);
+                const float2 dep = S.zlev[(int64_t)(iuv - 1) * S.nalloc + c];
+                zsn = dep.x + dep.y * facint;
+              }
+              if (zsn != zs_old) S.zs[c] = zsn;
+              if (S.wiggle) {
+                if (zs11 != zs00) S.zs0[c] = zs11;
+                S.zsderv[c] = zsn - 2.0f * zs11 + zs00;
+              }
+              const uint8_t vn = v < 0.0 ? 1 : 0;
+              if (vn != vn_old) S.vneg[c] = vn;
+            } else {
+              float z = zs_old;
+              if (S.precip) {
+                const float zbc = S.infiltration ? ((const float*)(sm + con::O_ZB))[k] : 0.0f;
+                const float qinfmap = (S.infiltration && !(z <= zbc)) ? qi : 0.0f;
+                z = z + (st.ptmp - qinfmap) * dt;
+              }
+              if (S.use_qext) z = z + qx * dt;
+              z = z + ((q_md - q_mu) * S.dxinv + (q_nd - q_nu) * S.dyinv) * dt;
+              if (z != zs_old) S.zs[c] = z;
+              zsn = z;
+            }
+          }
+          if (S.store_zsmax && zsn > zm) S.zsmax[c] = zsn;
+        }
+      }
+    }
+    tile = next;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Launchers
+// --------------------------------------------------------------------------
+int momentum_tma_smem() { return 2 * mom::STAGE; }
+int continuity_tma_smem() { return 2 * con::STAGE; }
+
+const void* momentum_tma_fn(int subgrid) {
+  return subgrid ? (const void*)k_momentum_tma<true> : (const void*)k_momentum_tma<false>;
+}
+const void* continuity_tma_fn(int subgrid) {
+  return subgrid ? (const void*)k_continuity_tma<true> : (const void*)k_continuity_tma<false>;
+}
+
+void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
+                         int grid, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  const dim3 blk(32, 8);
+  if (subgrid)
+    k_momentum_tma<true><<<grid, blk, 2 * mom::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles);
+  else
+    k_momentum_tma<false><<<grid, blk, 2 * mom::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles);
+}
+
+void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
+                           int grid, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  const dim3 blk(32, 8);
+  if (subgrid)
+    k_continuity_tma<true><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles);
+  else
+    k_continuity_tma<false><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles);
+}
+
+}  // namespace sfg

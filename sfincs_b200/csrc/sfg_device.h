@@ -86,6 +86,7 @@ struct alignas(16) StepState {
   int itb0, itb1;      // boundary time records of the current step (1-based)
   int steps_left;      // for single / bounded calls
   int itbndlast, itprcplast, itwndlast, itsrclast;
+  int fault;           // nonzero: a bounded wait in a staged kernel gave up (its tile was skipped)
 };
 
 struct ScnDev {
@@ -157,6 +158,22 @@ struct ScnDev {
 
 struct Tile {  // one CTA of the cell kernels
   int scn, n0, m0, pad;
+};
+
+// TMA tensor maps of one scenario (2-D views of the dense arrays, boxes sized
+// for 32 x 8 cell tiles plus the halo each kernel needs).  The maps live in
+// device memory, 64-byte aligned, one MapSet per scenario.
+enum MapId : int {
+  // momentum
+  MM_ZS, MM_QU0, MM_QU1, MM_QV0, MM_QV1, MM_UU0, MM_UU1, MM_VV0, MM_VV1, MM_FLAGS, MM_KFU, MM_KFV,
+  MM_VNEG, MM_ZSD, MM_SGZU, MM_SGZV, MM_ZB, MM_ZBMXU, MM_ZBMXV, MM_GN2U, MM_GN2V,
+  // continuity
+  MC_QU0, MC_QU1, MC_QV0, MC_QV1, MC_ZS, MC_ZSMAX, MC_ZVOL, MC_ZS0, MC_VOLMAX, MC_VNEG, MC_FLAGS, MC_QEXT,
+  MC_QINF, MC_ZB,
+  NUM_MAPS
+};
+struct alignas(64) MapSet {
+  unsigned char m[NUM_MAPS][128];  // CUtensorMap objects (opaque, 128 bytes each)
 };
 
 }  // namespace sfg

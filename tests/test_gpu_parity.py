@@ -18,10 +18,23 @@ from conftest import oracle_faces_to_cells, small_plain, small_subgrid
 pytestmark = pytest.mark.gpu
 
 
-def _model(d):
+def _model(d, variant=None):
+    """variant: kernel path (2, 3: per-thread loads; 4: TMA-staged tiles); None = library default."""
+    import os
+
     from sfincs_b200.bmi import Model
 
-    return Model(d)
+    old = os.environ.get("SFG_MOMENTUM_VARIANT")
+    if variant is not None:
+        os.environ["SFG_MOMENTUM_VARIANT"] = str(variant)
+    try:
+        return Model(d)
+    finally:
+        if variant is not None:
+            if old is None:
+                del os.environ["SFG_MOMENTUM_VARIANT"]
+            else:
+                os.environ["SFG_MOMENTUM_VARIANT"] = old
 
 
 def _oracle(d, prec):
@@ -48,11 +61,12 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("variant", [2, 4])
 @pytest.mark.parametrize("kind", sorted(CASES))
-def test_stepwise_matches_f32_oracle(tmp_path, kind):
+def test_stepwise_matches_f32_oracle(tmp_path, kind, variant):
     d, _ = CASES[kind](tmp_path)
     o = _oracle(d, "f32")
-    g = _model(d)
+    g = _model(d, variant)
     steps_done = 0
     for n in (1, 1, 2, 6, 30, 60):
         o.update(-1000.0, n)
@@ -114,14 +128,15 @@ def test_full_run_against_fp64_oracle(tmp_path, kind):
 
 
 @pytest.mark.parametrize("kind", ["plain", "subgrid"])
-def test_deterministic(tmp_path, kind):
+def test_deterministic_and_paths_agree(tmp_path, kind):
+    """Bitwise reproducible; the per-thread-load and TMA-staged paths compute identical states."""
     d, _ = CASES[kind](tmp_path)
-    a, b = _model(d), _model(d)
-    a.step(200)
-    b.step(200)
-    assert np.array_equal(a.get("zs"), b.get("zs"))
-    assert np.array_equal(a.get("qx"), b.get("qx"))
-    assert np.array_equal(a.get("qy"), b.get("qy"))
+    a, b, c = _model(d, 4), _model(d, 4), _model(d, 2)
+    for g in (a, b, c):
+        g.step(200)
+    for name in ("zs", "qx", "qy", "uvx", "uvy"):
+        assert np.array_equal(a.get(name), b.get(name)), name
+        assert np.array_equal(a.get(name), c.get(name)), name
 
 
 def test_lake_at_rest(tmp_path):
