@@ -118,6 +118,14 @@ SFG_API int sfg_model_get(void* model, const char* name, void* dst, size_t bytes
 SFG_API int sfg_model_set(void* model, const char* name, const void* src, size_t bytes);
 /* Total water volume (m3, FP64) of the active cells; subgrid: sum of z_volume. */
 SFG_API int sfg_model_volume(void* model, double* volume);
+/* The same sum (bit for bit) for callers that must not allocate device memory
+ * when they ask for it; no counterpart in the reference.  Its scratch (4096
+ * FP64 partial sums and the total) is a fixed array inside the library, one
+ * per device and shared by every model on it, so calls that overlap in time
+ * race and must be serialised.  The first call on a device looks the array
+ * up; make it before any stream capture begins.  Synchronises the model's
+ * stream.  Returns 0, or 1 with the reason in get_last_bmi_error(). */
+SFG_API int sfg_model_volume_noalloc(void* model, double* volume);
 /* CUDA stream the model's kernels run on (cudaStream_t), for event timing. */
 SFG_API void* sfg_model_stream(void* model);
 /* Run nsteps steps with CUDA events between the individual launches (on the

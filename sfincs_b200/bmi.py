@@ -73,6 +73,7 @@ def lib(build_if_missing: bool = True):
     L.sfg_model_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]
     L.sfg_model_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]
     L.sfg_model_volume.argtypes = [ctypes.c_void_p, c_dp]
+    L.sfg_model_volume_noalloc.argtypes = [ctypes.c_void_p, c_dp]
     L.sfg_model_stream.restype = ctypes.c_void_p
     L.sfg_model_stream.argtypes = [ctypes.c_void_p]
     L.sfg_ensemble_create.restype = ctypes.c_void_p
@@ -277,6 +278,13 @@ class Model:
     def volume(self) -> float:
         v = ctypes.c_double()
         _check(self.L.sfg_model_volume(self._h, ctypes.byref(v)), "sfg_model_volume")
+        return v.value
+
+    def volume_noalloc(self) -> float:
+        """volume() through the entry point that allocates nothing (fixed
+        scratch array in the library, shared per device: do not overlap calls)."""
+        v = ctypes.c_double()
+        _check(self.L.sfg_model_volume_noalloc(self._h, ctypes.byref(v)), "sfg_model_volume_noalloc")
         return v.value
 
     @property

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "sfg_device.h"
 
@@ -108,6 +109,87 @@ void launch_volume(const ScnDev* d_scn, const int32_t* cmp, long long n, double*
   const int g = grid_for(n);
   k_volume_partial<<<g, 256, 0, s>>>(d_scn, cmp, n, part);
   k_volume_final<<<1, 32, 0, s>>>(part, g, out);
+}
+
+// ---- volume sum that allocates nothing ---------------------------------------
+// launch_volume() above sums into buffers the model allocated when it was
+// created.  Some callers want the volume at a moment when they must not
+// allocate device memory at all: a server that reserved its whole HBM budget
+// for resident models up front and admits work against that budget, or a
+// host loop that cannot let a cudaMalloc/cudaFree synchronise the device while
+// other models' steps are still running on other streams.  This variant keeps
+// its scratch (one FP64 partial sum per CTA, then the total) in a fixed array
+// compiled into the library, so a call performs no allocation of any kind.
+//
+// Limits: the array holds kNoAllocMaxParts partials.  The sum uses a
+// grid-stride loop over at most that many CTAs, so every model size fits; a
+// launch shape needing more partials is rejected with an error.  Nothing in
+// the array has to start at zero: each CTA overwrites its own partial and the
+// final pass overwrites the total before the host reads it.  There is one
+// array per device, shared by every model on that device, so calls that
+// overlap in time (two host threads, or two streams in flight) race on it and
+// must be serialised by the caller.
+constexpr int kNoAllocMaxParts = 4096;
+static __device__ __align__(256) double g_volume_scratch[kNoAllocMaxParts + 1];  // partials, then the total
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double* g_scratch_ptr[kMaxDevices] = {};  // device address of g_volume_scratch, per device ordinal
+
+// The first call on a device looks the array's address up with
+// cudaGetSymbolAddress (with that device current); later calls reuse it.  Make
+// the first call for each device before any stream capture begins.
+int volume_scratch(double** out, const char** why) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    *why = "no usable current CUDA device for the volume scratch array";
+    return 1;
+  }
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_volume_scratch);
+    if (e != cudaSuccess || !p) {
+      *why = "cudaGetSymbolAddress failed for the volume scratch array";
+      return 1;
+    }
+    g_scratch_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_scratch_ptr[dev];
+  return 0;
+}
+}  // namespace
+
+// Same sum as launch_volume (same kernels, same launch shape, so the same
+// bits), with the partials and the total in g_volume_scratch; the total is
+// copied to *host_out and the stream is synchronised before returning.
+int volume_noalloc(const ScnDev* d_scn, const int32_t* cmp, long long n, cudaStream_t s, double* host_out,
+                   const char** why) {
+  if (n < 0) {
+    *why = "negative cell count";
+    return 1;
+  }
+  const int g = grid_for(n);
+  if (g > kNoAllocMaxParts) {
+    *why = "volume sum needs more partial sums than the fixed scratch array holds (4096)";
+    return 1;
+  }
+  double* scratch = nullptr;
+  if (volume_scratch(&scratch, why)) return 1;
+  k_volume_partial<<<g, 256, 0, s>>>(d_scn, cmp, n, scratch);
+  k_volume_final<<<1, 32, 0, s>>>(scratch, g, scratch + kNoAllocMaxParts);
+  if (cudaGetLastError() != cudaSuccess) {
+    *why = "volume kernel launch failed";
+    return 1;
+  }
+  if (cudaMemcpyAsync(host_out, scratch + kNoAllocMaxParts, sizeof(double), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    *why = "copy of the volume to the host failed";
+    return 1;
+  }
+  return 0;
 }
 
 }  // namespace sfg

@@ -25,6 +25,8 @@ void launch_scatter_f32(const float* in, const int32_t* cmp, float* dst, long lo
 void launch_scatter_f64_f32(const double* in, const int32_t* cmp, float* dst, long long n, cudaStream_t s);
 int volume_parts(long long n);
 void launch_volume(const ScnDev* d_scn, const int32_t* cmp, long long n, double* part, double* out, cudaStream_t s);
+int volume_noalloc(const ScnDev* d_scn, const int32_t* cmp, long long n, cudaStream_t s, double* host_out,
+                   const char** why);
 
 namespace {
 
@@ -560,6 +562,21 @@ int sfg_model_volume(void* m, double* v) {
     *v = static_cast<sfg::ModelHandle*>(m)->volume();
     return 0;
   });
+}
+// No try/catch wrapper and no std::string on the success path: this entry
+// point allocates nothing (see volume_noalloc in aux_kernels.cu).
+int sfg_model_volume_noalloc(void* m, double* v) {
+  if (!m || !v) {
+    sfg::g_err = "sfg_model_volume_noalloc: null model or output pointer";
+    return 1;
+  }
+  auto* h = static_cast<sfg::ModelHandle*>(m);
+  const char* why = nullptr;
+  if (sfg::volume_noalloc(h->runner->d_scns(), h->dev->d_cmp_off(), h->np(), h->s(), v, &why)) {
+    sfg::g_err = std::string("sfg_model_volume_noalloc: ") + (why ? why : "failed");
+    return 1;
+  }
+  return 0;
 }
 void* sfg_model_stream(void* m) { return (void*)static_cast<sfg::ModelHandle*>(m)->s(); }
 int sfg_model_kernel_times(void* m, int nsteps, double ms_out[4], int* launches_per_step) {
