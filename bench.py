@@ -207,8 +207,49 @@ def cpu_reference(d: str, steps: int, warmup: int, budget_s: float = 20.0):
             "seconds": el}
 
 
+def reference_scenarios(args):
+    """Reference arm for the ensemble workload: the oracle (reference
+    precision, all host cores) timed on a bounded sample of one mid-size
+    member, extrapolated to every member's cell count and step count."""
+    from oracle.oracle import Oracle
+    from sfincs_b200 import ensemble
+
+    specs = ensemble.member_specs(n=args.members)
+    cells = np.array([s["nmax"] * s["mmax"] for s in specs], dtype=np.float64)
+    mid = int(np.argsort(cells)[len(specs) // 2])
+    d = ensemble.generate([specs[mid]], log=log)[0]
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    o = Oracle(d, "ref")
+    npc = o.scalars()["np"]
+    o.update(-1000.0, 5)
+    t0 = time.perf_counter()
+    done = 0
+    while time.perf_counter() - t0 < args.cpu_budget:
+        done += o.update(-1000.0, 5)
+    el = time.perf_counter() - t0
+    dt = o.scalars()["dt"]
+    o.close()
+    rate = npc * done / el
+    tsim = specs[mid]["tstop"]
+    total_s = float(np.sum(cells * (tsim / dt))) / rate
+    value = len(specs) / total_s * 3600.0
+    return {"impl": "reference", "metric": "scenarios/h", "value": value, "unit": "scenarios/h",
+            "n_gpus": args.gpus, "steps": done, "warmup": 5, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64 (reference precision)", "data": "synthetic",
+            "config": {"workload": f"uneven ensemble of {len(specs)} members (as --workload ensemble)",
+                       "parallelism": "host OpenMP"},
+            "cpu_baseline": {"value": value, "unit": "scenarios/h", "cores": int(os.environ["OMP_NUM_THREADS"]),
+                             "kind": "port",
+                             "sample": f"{done} steps of a {int(npc)}-cell member in {el:.1f}s "
+                                       f"({rate:.3e} cell-updates/s), extrapolated to all members at dt={dt:.3f}s"},
+            "e2e": {"value": value, "unit": "scenarios/h", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
+        return
+    if args.workload in ("ensemble", "serve"):
+        print(json.dumps(reference_scenarios(args)), flush=True)
         return
     d = workload_dir(args.workload, rank)
     cb = cpu_reference(d, args.steps, args.warmup, budget_s=args.cpu_budget)
@@ -273,10 +314,11 @@ def run_ours(args, rank: int, world: int, local: int):
     tfile = os.path.join(ROOT, "profiles", f"traffic_{wl}.json")
     if os.path.exists(tfile):
         try:
-            traffic = json.load(open(tfile)).get("momentum_bytes_per_launch_scaled")
+            traffic = json.load(open(tfile)).get("momentum_bytes_per_launch")
         except Exception:
             traffic = None
     s1 = g.scalars()
+    mom_kernel = "k_momentum" if os.environ.get("SFG_MOMENTUM_VARIANT", "5") in ("2", "3") else "k_momentum_tma"
     # ---- full simulated run (12 h for the subgrid workload), device-resident
     full = None
     if args.full_run and rank == 0:
@@ -329,7 +371,7 @@ def run_ours(args, rank: int, world: int, local: int):
                    "timed_from_t_s": s0["t"], "sim_time_after_timing_s": s1["t"]},
         "gpu_launches": lps * args.steps,
         "kernel_ms": {"step_bnd": ktimes[0], "momentum": ktimes[1], "sources": ktimes[2], "continuity": ktimes[3]},
-        "roofline": {"bound": "hbm", "kernel": "k_momentum", "achieved": ach_mom, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": mom_kernel, "achieved": ach_mom, "peak": peak, "unit": "GB/s",
                      "frac": ach_mom / peak, "traffic": traffic, "peak_source": peak_src,
                      "bytes_per_cell": BYTES[wl], "step_achieved_gbs": step_bytes, "step_frac": step_bytes / peak},
         "clocks": clocks,
@@ -341,13 +383,161 @@ def run_ours(args, rank: int, world: int, local: int):
         print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args, rank: int, world: int, local: int):
+    """Uneven ensemble: 64 subgrid members (sides log-uniform 200..1500 cells),
+    each simulating 6 h.  Batched (one launch sequence advances every member,
+    per-member dt, CUDA graphs, autotuned kernel variant) against the plain
+    path (the same members solved one after another, each with its own model).
+    Members are split across ranks (replicas)."""
+    import torch
+
+    from sfincs_b200 import ensemble
+    from sfincs_b200.bmi import Ensemble, Model
+
+    torch.cuda.set_device(local)
+    specs = ensemble.member_specs(n=args.members)
+    mine = specs[rank::world]
+    dirs = ensemble.generate(mine, log=log)
+    barrier(world)
+    ncell = [s["nmax"] * s["mmax"] for s in mine]
+    # ---- batched
+    E = Ensemble(dirs)
+    E.set_autotune(True)
+    t1 = [E.scalars(i)["t1"] for i in range(len(dirs))]
+    st = torch.cuda.ExternalStream(E.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0.record(st)
+    E.run(t1)
+    e1.record(st)
+    e1.synchronize()
+    ms_b = max_over_ranks(e0.elapsed_time(e1), world)
+    steps_b = [int(E.scalars(i)["nt"]) for i in range(len(dirs))]
+    variant = E.variant
+    zs_b = [E.get(i, "zs") for i in range(len(dirs))]
+    E.close()
+    torch.cuda.empty_cache()
+    # ---- plain: one model at a time
+    ms_p = 0.0
+    same = True
+    for i, d in enumerate(dirs):
+        g = Model(d)
+        sp = torch.cuda.ExternalStream(g.stream)
+        torch.cuda.synchronize()
+        e0.record(sp)
+        g.run(g.scalars()["t1"])
+        e1.record(sp)
+        e1.synchronize()
+        ms_p += e0.elapsed_time(e1)
+        same = same and np.array_equal(g.get("zs"), zs_b[i])
+        g.close()
+    ms_p = max_over_ranks(ms_p, world)
+    n_all = len(specs)
+    value = n_all / (ms_b / 1e3) * 3600.0
+    plain = n_all / (ms_p / 1e3) * 3600.0
+    cell_updates = sum(c * s for c, s in zip(ncell, steps_b))
+    line = {
+        "metric": "scenarios/h", "value": value, "unit": "scenarios/h", "n_gpus": world, "steps": max(steps_b),
+        "warmup": 0, "ms_per_step": ms_b / max(steps_b), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (f64 time and volume)", "data": "synthetic",
+        "config": {"workload": f"uneven ensemble: {n_all} subgrid members, sides log-uniform 200..1500 cells at "
+                               "100 m (P=10 subgrid pixels), surge U(1,4) m, rain U(0,80) mm/h, 6 h simulated each",
+                   "members": n_all, "members_per_rank": len(dirs), "cells_total_rank0": int(sum(ncell)),
+                   "parallelism": f"replicas x{world} (members split across ranks)",
+                   "l2": "device-resident state far larger than L2"},
+        "gpu_launches": None,
+        "batched": {"seconds": ms_b / 1e3, "scenarios_per_h": value, "autotuned_variant": variant,
+                    "cell_updates_per_s": cell_updates / (ms_b / 1e3)},
+        "plain": {"seconds": ms_p / 1e3, "scenarios_per_h": plain},
+        "batched_over_plain": value / plain,
+        "alone_equals_mix_bitwise": bool(same),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_serve(args, rank: int, world: int, local: int):
+    """Served forecast stream: requests (subgrid regular grids, lognormal sizes
+    clipped to 0.1M..10M cells, seeded fractal DEMs, random surge and rain,
+    24 h simulated each) arrive as a Poisson process whose rate loads the GPU
+    to about 80 %; the continuous-batching server admits them by HBM budget
+    and reports scenarios/h with p50/p99 latency.  Each rank serves its own
+    stream (replicas)."""
+    import torch
+
+    from sfincs_b200 import ensemble
+    from sfincs_b200.bmi import Model
+    from sfincs_b200.serve import Request, Server
+
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(11 + rank)
+    specs = []
+    for i in range(args.requests):
+        cells = float(np.clip(rng.lognormal(np.log(0.5e6), 1.0), 0.1e6, 10e6))
+        side = int(round(np.sqrt(cells)))
+        specs.append(dict(nmax=side, mmax=side, dx=100.0, P=8, seed=5000 + 100 * rank + i, tstop=86400.0,
+                          surge_peak=float(rng.uniform(1.0, 4.0)), rain_mmh=float(rng.uniform(0.0, 80.0)),
+                          rain_hours=3.0, coast_x=0.15 * side * 100.0, t_peak=43200.0, width_h=6.0))
+    dirs = ensemble.generate(specs, log=log)
+    # calibration: device throughput on a mid-size request -> service-time estimate
+    mid = int(np.argsort([s["nmax"] ** 2 for s in specs])[len(specs) // 2])
+    g = Model(dirs[mid])
+    g.step(64)
+    st = torch.cuda.ExternalStream(g.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    g.issue(128)
+    e1.record(st)
+    e1.synchronize()
+    rate = g.scalars()["np"] * 128 / (e0.elapsed_time(e1) / 1e3)
+    dt_est = g.scalars()["dt"]
+    g.close()
+    service = np.array([s["nmax"] * s["mmax"] * (86400.0 / dt_est) / rate for s in specs])
+    lam = 0.8 / service.mean()
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(specs)))
+    arrivals -= arrivals[0]
+    reqs = [Request(arrival_s=float(a), model_dir=d, rid=i) for i, (a, d) in enumerate(zip(arrivals, dirs))]
+    torch.cuda.empty_cache()
+    srv = Server(max_slots=32, chunk=32, prep_threads=4)
+    barrier(world)
+    out = srv.serve(reqs, fetch=("zsmax",))
+    srv.close()
+    makespan = max_over_ranks(out["makespan_s"], world)
+    value = world * len(reqs) / makespan * 3600.0
+    cells = [r.cells for r in out["results"]]
+    cu = sum(r.cells * r.steps for r in out["results"])
+    line = {
+        "metric": "scenarios/h", "value": value, "unit": "scenarios/h", "n_gpus": world,
+        "steps": int(sum(r.steps for r in out["results"])), "warmup": 0, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 time and volume)",
+        "data": "synthetic",
+        "config": {"workload": "served forecast stream: subgrid regular grids, lognormal sizes (median 0.5M, "
+                               "clipped 0.1M..10M cells) at 100 m, P=8, surge U(1,4) m, rain U(0,80) mm/h 3 h, "
+                               "24 h simulated each; Poisson arrivals at ~80 % estimated load",
+                   "requests_per_rank": len(reqs), "cells_min": int(min(cells)), "cells_max": int(max(cells)),
+                   "arrival_rate_per_s": lam, "service_estimate_s": float(service.mean()),
+                   "parallelism": f"replicas x{world} (one request stream per rank)",
+                   "quadtree_requests": "not served: quadtree meshes are not built in this core"},
+        "gpu_launches": None,
+        "latency_p50_s": out["latency_p50_s"], "latency_p99_s": out["latency_p99_s"],
+        "latency_max_s": out["latency_max_s"], "makespan_s": makespan, "mean_running": out["mean_running"],
+        "cell_updates_per_s": cu / out["makespan_s"],
+        "errors": int(sum(1 for r in out["results"] if r.error)),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="subgrid", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="subgrid", choices=sorted(WORKLOADS) + ["ensemble", "serve"])
+    ap.add_argument("--requests", type=int, default=24, help="requests per rank (--workload serve)")
+    ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--full-run", type=int, default=1, help="also time the whole simulated period (rank 0)")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work")
@@ -356,6 +546,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, rank, world)
+        elif args.workload == "ensemble":
+            run_ensemble(args, rank, world, local)
+        elif args.workload == "serve":
+            run_serve(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -109,6 +109,13 @@ SFG_API void sfg_model_destroy(void* model);
 SFG_API int sfg_model_run(void* model, double t_end, long long max_steps, int chunk);
 /* Issue nsteps steps on the model's stream without waiting (timing helper). */
 SFG_API int sfg_model_issue(void* model, int nsteps);
+/* Kernel variant: 5 (default) and 4 are the TMA-staged tile kernels compiled
+ * for 4 and 3 CTAs per SM, 2 and 3 the per-thread-load kernels.  All compute
+ * bitwise identical states.  With autotune on, the next run() times one
+ * chunk of real steps with each of 5, 4 and 2 and keeps the fastest. */
+SFG_API int sfg_model_set_autotune(void* model, int on);
+SFG_API int sfg_model_variant(void* model);
+SFG_API int sfg_model_set_variant(void* model, int variant);
 SFG_API int sfg_model_sync(void* model);
 /* [t, dt, min_dt, nt, error, t0, t1, np, npuv, nkcuv2, ngbnd, subgrid,
  *  bflux_vol, rain_vol, src_vol, dtmax, dtmin, device_bytes, ntiles] */
@@ -141,11 +148,46 @@ SFG_API void sfg_ensemble_destroy(void* ens);
  * graphs of `chunk` steps, host checks completion once per chunk. */
 SFG_API int sfg_ensemble_run(void* ens, const double* t_end, long long max_steps, int chunk);
 SFG_API int sfg_ensemble_issue(void* ens, int nsteps);
+SFG_API int sfg_ensemble_set_autotune(void* ens, int on);
+SFG_API int sfg_ensemble_variant(void* ens);
+SFG_API int sfg_ensemble_set_variant(void* ens, int variant);
 SFG_API int sfg_ensemble_sync(void* ens);
 SFG_API int sfg_ensemble_scalars(void* ens, int member, double out[19]);
 SFG_API int sfg_ensemble_get(void* ens, int member, const char* name, void* dst, size_t bytes);
 SFG_API void* sfg_ensemble_stream(void* ens);
 SFG_API int sfg_ensemble_kernel_times(void* ens, int nsteps, double ms_out[4], int* launches_per_step);
+
+/* ---- serving pool: continuous batching of independent requests ------------------------ */
+/* A pool of at most max_slots resident models whose device memory together
+ * stays within hbm_budget_bytes.  Resident models advance together in the same
+ * launches (per-model dt); models join and leave between chunks of steps. */
+SFG_API void* sfg_pool_create(int max_slots, double hbm_budget_bytes, char* err, int errlen);
+SFG_API void sfg_pool_destroy(void* pool);
+/* Host-only preparation of a model (reads the inputs, builds the layout); no
+ * device work, callable from any host thread while the pool is stepping. */
+SFG_API void* sfg_prepare(const char* model_dir, int bmi, char* err, int errlen);
+/* Exact device bytes the prepared model needs once admitted. */
+SFG_API double sfg_prepared_bytes(void* prepared);
+SFG_API double sfg_prepared_cells(void* prepared);
+SFG_API void sfg_prepared_destroy(void* prepared);
+/* Admit a prepared model to run until t_end (negative: the model's own tstop):
+ * returns its slot (the pool then
+ * owns the prepared model), -1 if no slot is free or the budget would be
+ * exceeded (the prepared model stays the caller's), -2 on error. */
+SFG_API int sfg_pool_admit(void* pool, void* prepared, double t_end);
+/* Advance every running model by up to nsteps steps (CUDA graph chunks) and
+ * return how many are still running (-2 on error). */
+SFG_API int sfg_pool_advance(void* pool, int nsteps);
+/* Slots whose model has finished (reached t_end or stopped), up to cap. */
+SFG_API int sfg_pool_finished(void* pool, int* slots, int cap);
+SFG_API int sfg_pool_scalars(void* pool, int slot, double out[19]);
+/* "zs","z_volume" (double[np]); "zsmax","qx","qy","uvx","uvy" (float[np]). */
+SFG_API int sfg_pool_get(void* pool, int slot, const char* name, void* dst, size_t bytes);
+/* Free the slot and its device memory. */
+SFG_API int sfg_pool_release(void* pool, int slot);
+SFG_API double sfg_pool_used_bytes(void* pool);
+SFG_API int sfg_pool_resident(void* pool);
+SFG_API void* sfg_pool_stream(void* pool);
 
 /* ---- diagnostics: host-side layout of a model, no device work -------------------------- */
 /* Loads <model_dir> on the host only and copies one layout array (compact

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <type_traits>
 #include <memory>
 #include <sstream>
 #include <stdexcept>
@@ -1748,7 +1749,10 @@ struct Model {
           }
         }
         if (h73table) throw std::runtime_error("oracle: h73table is off by default and not restated");
-        T hu73 = hu * hu * std::pow(hu, expo);
+        // The CUDA core evaluates hu**(1.0/3.0) as a cube root (under one ulp from
+        // hu**0.333333343 for 1e-3 <= hu <= 1e3); the "f32" (core precision)
+        // instantiation does the same, "ref" and "fp64" keep the reference's pow.
+        T hu73 = hu * hu * (std::is_same<TZ, float>::value ? std::cbrt(hu) : std::pow(hu, expo));
         T qn = (qsm + frc * (T)dtt) / ((T)1 + gnavg2 * (T)dtt * qfr / hu73);
         if (subgrid && wiggle_suppression) {
           T mdrv = std::fabs(zsderv(nm) - zsderv(nmu)) - (T)wiggle_threshold;

@@ -73,6 +73,11 @@ def lib(build_if_missing: bool = True):
     L.sfg_model_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]
     L.sfg_model_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]
     L.sfg_model_volume.argtypes = [ctypes.c_void_p, c_dp]
+    for f in ("sfg_model_set_autotune", "sfg_model_set_variant", "sfg_ensemble_set_autotune",
+              "sfg_ensemble_set_variant"):
+        getattr(L, f).argtypes = [ctypes.c_void_p, ctypes.c_int]
+    for f in ("sfg_model_variant", "sfg_ensemble_variant"):
+        getattr(L, f).argtypes = [ctypes.c_void_p]
     L.sfg_model_volume_noalloc.argtypes = [ctypes.c_void_p, c_dp]
     L.sfg_model_stream.restype = ctypes.c_void_p
     L.sfg_model_stream.argtypes = [ctypes.c_void_p]
@@ -280,6 +285,16 @@ class Model:
         _check(self.L.sfg_model_volume(self._h, ctypes.byref(v)), "sfg_model_volume")
         return v.value
 
+    @property
+    def variant(self) -> int:
+        return int(self.L.sfg_model_variant(self._h))
+
+    def set_variant(self, v: int) -> None:
+        _check(self.L.sfg_model_set_variant(self._h, int(v)), "sfg_model_set_variant")
+
+    def set_autotune(self, on: bool = True) -> None:
+        _check(self.L.sfg_model_set_autotune(self._h, int(bool(on))), "sfg_model_set_autotune")
+
     def volume_noalloc(self) -> float:
         """volume() through the entry point that allocates nothing (fixed
         scratch array in the library, shared per device: do not overlap calls)."""
@@ -330,6 +345,16 @@ class Ensemble:
 
     def issue(self, nsteps: int) -> None:
         _check(self.L.sfg_ensemble_issue(self._h, int(nsteps)), "sfg_ensemble_issue")
+
+    @property
+    def variant(self) -> int:
+        return int(self.L.sfg_ensemble_variant(self._h))
+
+    def set_variant(self, v: int) -> None:
+        _check(self.L.sfg_ensemble_set_variant(self._h, int(v)), "sfg_ensemble_set_variant")
+
+    def set_autotune(self, on: bool = True) -> None:
+        _check(self.L.sfg_ensemble_set_autotune(self._h, int(bool(on))), "sfg_ensemble_set_autotune")
 
     def sync(self) -> None:
         _check(self.L.sfg_ensemble_sync(self._h), "sfg_ensemble_sync")

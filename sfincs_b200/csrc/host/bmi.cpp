@@ -275,6 +275,9 @@ int require_bmi() {
 }
 
 }  // namespace
+
+void set_last_error(const std::string& msg) { g_err = msg; }
+
 }  // namespace sfg
 
 using sfg::g_bmi;
@@ -520,6 +523,20 @@ int sfg_model_run(void* m, double t_end, long long max_steps, int chunk) {
     return 0;
   });
 }
+int sfg_model_set_autotune(void* m, int on) {
+  return guarded([&] {
+    static_cast<sfg::ModelHandle*>(m)->runner->set_autotune(on != 0);
+    return 0;
+  });
+}
+int sfg_model_variant(void* m) { return static_cast<sfg::ModelHandle*>(m)->runner->variant(); }
+int sfg_model_set_variant(void* m, int variant) {
+  return guarded([&] {
+    if (variant < 2 || variant > 5) throw std::runtime_error("kernel variant must be 2, 3, 4 or 5");
+    static_cast<sfg::ModelHandle*>(m)->runner->set_variant(variant);
+    return 0;
+  });
+}
 int sfg_model_issue(void* m, int nsteps) {
   return guarded([&] {
     auto* h = static_cast<sfg::ModelHandle*>(m);
@@ -634,6 +651,20 @@ int sfg_ensemble_run(void* ev, const double* t_end, long long max_steps, int chu
     return 0;
   });
 }
+int sfg_ensemble_set_autotune(void* ev, int on) {
+  return guarded([&] {
+    static_cast<sfg::EnsembleHandle*>(ev)->runner->set_autotune(on != 0);
+    return 0;
+  });
+}
+int sfg_ensemble_variant(void* ev) { return static_cast<sfg::EnsembleHandle*>(ev)->runner->variant(); }
+int sfg_ensemble_set_variant(void* ev, int variant) {
+  return guarded([&] {
+    if (variant < 2 || variant > 5) throw std::runtime_error("kernel variant must be 2, 3, 4 or 5");
+    static_cast<sfg::EnsembleHandle*>(ev)->runner->set_variant(variant);
+    return 0;
+  });
+}
 int sfg_ensemble_issue(void* ev, int nsteps) {
   return guarded([&] {
     auto* e = static_cast<sfg::EnsembleHandle*>(ev);
@@ -683,6 +714,10 @@ int sfg_ensemble_get(void* ev, int i, const char* name, void* dst, size_t bytes)
     if (nm == "zs") {
       if (bytes != (size_t)n * 8) throw std::runtime_error("wrong size for zs");
       sfg::launch_gather_f32_f64(d.dev().zs, d.d_cmp_off(), (double*)e->d_stage, n, s);
+    } else if (nm == "z_volume") {
+      if (!d.dev().zvol) throw std::runtime_error("z_volume exists only for subgrid models");
+      if (bytes != (size_t)n * 8) throw std::runtime_error("wrong size for z_volume");
+      sfg::launch_gather_f64(d.dev().zvol, d.d_cmp_off(), (double*)e->d_stage, n, s);
     } else {
       const float* src = nullptr;
       if (nm == "zsmax") src = d.dev().zsmax;

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <stdexcept>
 
 #include "inputs.h"
@@ -657,85 +658,139 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     P.nsrc = nsrc;
     P.ntsrc = (int)h.tsrc.size();
   }
+  // 32 x 8 cell tiles that hold at least one active cell (the work list of the
+  // cell kernels; a runner concatenates the lists of its models)
+  for (int m0 = 1; m0 <= P.mmax; m0 += 8)
+    for (int n0 = 1; n0 <= P.nmax; n0 += 32) {
+      bool any = false;
+      for (int m = m0; m < m0 + 8 && m <= P.mmax && !any; m++)
+        for (int n = n0; n < n0 + 32 && n <= P.nmax; n++)
+          if (h.flags[(size_t)m * P.ld + kGhostPad + n] & F_ACT) {
+            any = true;
+            break;
+          }
+      if (any) h.tiles.push_back(int2{n0, m0});
+    }
   return H;
 }
 
 // ============================================================================
 // DeviceModel
 // ============================================================================
-template <class X>
-X* DeviceModel::alloc(size_t n) {
-  if (n == 0) return nullptr;
-  void* p = nullptr;
-  check_cuda(cudaMalloc(&p, n * sizeof(X)), "cudaMalloc");
-  check_cuda(cudaMemset(p, 0, n * sizeof(X)), "cudaMemset");
-  allocs_.push_back(p);
-  bytes_ += n * sizeof(X);
-  return static_cast<X*>(p);
+// Device residency in ONE allocation: the layout pass below runs twice, first
+// to size every array (256-byte aligned sub-allocations), then to place and
+// upload them.  device_bytes_needed() runs only the first pass, so admission
+// control knows a model's footprint before anything is allocated.
+namespace {
+struct Placer {
+  char* base = nullptr;  // null: sizing pass
+  size_t off = 0;
+  template <class X>
+  X* take(size_t n) {
+    if (n == 0) return nullptr;
+    off = (off + 255) & ~(size_t)255;
+    X* p = base ? reinterpret_cast<X*>(base + off) : nullptr;
+    off += n * sizeof(X);
+    return p;
+  }
+};
+}  // namespace
+
+template <class F>
+static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, Placer& pl, F&& fill) {
+  const size_t NA = (size_t)h.p.nalloc;
+  auto up = [&](auto& dst, const auto& v) {
+    using X = typename std::decay_t<decltype(v)>::value_type;
+    X* q = pl.template take<X>(v.size());
+    if (q) fill(q, v.data(), v.size() * sizeof(X));
+    dst = q;
+  };
+  auto zero = [&](auto& dst, size_t n) {
+    using X = std::remove_const_t<std::remove_pointer_t<std::decay_t<decltype(dst)>>>;
+    X* q = pl.template take<X>(n);
+    if (q) fill(q, nullptr, n * sizeof(X));
+    dst = q;
+  };
+  up(d.zs, h.zs);
+  up(d.zsmax, h.zsmax);
+  up(d.zvol, h.zvol);
+  if (h.p.wiggle) {
+    up(d.zs0, h.zs0);
+    zero(d.zsderv, NA);
+  } else {
+    d.zs0 = nullptr;
+    d.zsderv = nullptr;
+  }
+  zero(d.kf[0], NA);
+  zero(d.kf[1], NA);
+  if (h.p.subgrid) up(d.vneg, h.vneg);
+  else d.vneg = nullptr;
+  for (int b = 0; b < 2; b++) {
+    zero(d.qu[b], NA);
+    zero(d.qv[b], NA);
+    zero(d.uu[b], NA);
+    zero(d.vv[b], NA);
+  }
+  up(d.flags, h.flags);
+  up(d.zb, h.zb);
+  up(d.zbmx_u, h.zbmx_u);
+  up(d.zbmx_v, h.zbmx_v);
+  up(d.gn2_u, h.gn2_u);
+  up(d.gn2_v, h.gn2_v);
+  up(d.sgz_u, h.sgz_u);
+  up(d.sgz_v, h.sgz_v);
+  up(d.sgw_u, h.sgw_u);
+  up(d.sgw_v, h.sgw_v);
+  up(d.rec_u, h.rec_u);
+  up(d.rec_v, h.rec_v);
+  up(d.zz_min, h.zz_min);
+  up(d.zz_max, h.zz_max);
+  up(d.zz_volmax, h.zz_volmax);
+  up(d.zlev, h.zlev);
+  if (h.p.use_qext) zero(d.qext, NA);
+  else d.qext = nullptr;
+  up(d.qinf, h.qinf);
+  up(d.t_bnd, h.t_bnd);
+  up(d.zs_bnd, h.zs_bnd);
+  zero(d.zst_bnd, (size_t)std::max(h.p.nbnd, 1));
+  up(d.bfaces, h.bfaces);
+  zero(d.uvmean, (size_t)std::max(h.p.nkcuv2, 1));
+  up(d.neu, h.neu);
+  up(d.tprcp, h.tprcp);
+  up(d.vprcp, h.vprcp);
+  up(d.twnd, h.twnd);
+  up(d.wmag, h.wmag);
+  up(d.wdir, h.wdir);
+  up(d.cdval, h.cdval);
+  up(d.tsrc, h.tsrc);
+  up(d.qsrc, h.qsrc);
+  zero(d.qtsrc, (size_t)std::max(h.p.nsrc, 1));
+  up(d.src_cell, h.src_cell);
+  up(cmp, h.cmp_off);
+  zero(d.st, 1);
 }
 
-template <class X>
-X* DeviceModel::upload(const std::vector<X>& v) {
-  if (v.empty()) return nullptr;
-  X* p = alloc<X>(v.size());
-  check_cuda(cudaMemcpy(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice), "upload");
-  return p;
+size_t device_bytes_needed(const HostModel& h) {
+  ScnDev d = h.p;
+  int32_t* cmp = nullptr;
+  Placer pl;
+  place_model(h, d, cmp, pl, [](void*, const void*, size_t) {});
+  return (pl.off + 255) & ~(size_t)255;
 }
 
 DeviceModel::DeviceModel(const HostModel& h) : h_(&h) {
   d_ = h.p;
-  const size_t NA = (size_t)h.p.nalloc;
+  bytes_ = device_bytes_needed(h);
+  check_cuda(cudaMalloc(&block_, bytes_), "cudaMalloc model");
   try {
-    d_.zs = upload(h.zs);
-    d_.zsmax = upload(h.zsmax);
-    d_.zvol = upload(h.zvol);
-    d_.zs0 = h.p.wiggle ? upload(h.zs0) : nullptr;
-    d_.zsderv = h.p.wiggle ? alloc<float>(NA) : nullptr;
-    d_.kf[0] = alloc<uint8_t>(NA);
-    d_.kf[1] = alloc<uint8_t>(NA);
-    d_.vneg = h.p.subgrid ? upload(h.vneg) : nullptr;
-    for (int b = 0; b < 2; b++) {
-      d_.qu[b] = alloc<float>(NA);
-      d_.qv[b] = alloc<float>(NA);
-      d_.uu[b] = alloc<float>(NA);
-      d_.vv[b] = alloc<float>(NA);
-    }
-    d_.flags = upload(h.flags);
-    d_.zb = upload(h.zb);
-    d_.zbmx_u = upload(h.zbmx_u);
-    d_.zbmx_v = upload(h.zbmx_v);
-    d_.gn2_u = upload(h.gn2_u);
-    d_.gn2_v = upload(h.gn2_v);
-    d_.sgz_u = upload(h.sgz_u);
-    d_.sgz_v = upload(h.sgz_v);
-    d_.sgw_u = upload(h.sgw_u);
-    d_.sgw_v = upload(h.sgw_v);
-    d_.rec_u = upload(h.rec_u);
-    d_.rec_v = upload(h.rec_v);
-    d_.zz_min = upload(h.zz_min);
-    d_.zz_max = upload(h.zz_max);
-    d_.zz_volmax = upload(h.zz_volmax);
-    d_.zlev = upload(h.zlev);
-    d_.qext = h.p.use_qext ? alloc<float>(NA) : nullptr;
-    d_.qinf = upload(h.qinf);
-    d_.t_bnd = upload(h.t_bnd);
-    d_.zs_bnd = upload(h.zs_bnd);
-    d_.zst_bnd = alloc<float>((size_t)std::max(h.p.nbnd, 1));
-    d_.bfaces = upload(h.bfaces);
-    d_.uvmean = alloc<float>((size_t)std::max(h.p.nkcuv2, 1));
-    d_.neu = upload(h.neu);
-    d_.tprcp = upload(h.tprcp);
-    d_.vprcp = upload(h.vprcp);
-    d_.twnd = upload(h.twnd);
-    d_.wmag = upload(h.wmag);
-    d_.wdir = upload(h.wdir);
-    d_.cdval = upload(h.cdval);
-    d_.tsrc = upload(h.tsrc);
-    d_.qsrc = upload(h.qsrc);
-    d_.qtsrc = alloc<float>((size_t)std::max(h.p.nsrc, 1));
-    d_.src_cell = upload(h.src_cell);
-    d_cmp_ = upload(h.cmp_off);
-    d_.st = alloc<StepState>(1);
+    Placer pl;
+    pl.base = static_cast<char*>(block_);
+    place_model(h, d_, d_cmp_, pl, [](void* dst, const void* src, size_t n) {
+      if (src)
+        check_cuda(cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice), "upload");
+      else
+        check_cuda(cudaMemset(dst, 0, n), "cudaMemset");
+    });
     StepState s{};
     s.t = h.t0;  // sfincs_lib.f90:279-282: t = t0, first min_dt = 1e-6
     s.tend = h.t0;
@@ -747,20 +802,21 @@ DeviceModel::DeviceModel(const HostModel& h) : h_(&h) {
     std::memcpy(&s.min_dt_bits, &one_e_minus6, 4);
     check_cuda(cudaMemcpy(d_.st, &s, sizeof(s), cudaMemcpyHostToDevice), "init step state");
   } catch (...) {
-    for (void* p : allocs_) cudaFree(p);
-    allocs_.clear();
+    cudaFree(block_);
+    block_ = nullptr;
     throw;
   }
 }
 
 DeviceModel::~DeviceModel() {
-  for (void* p : allocs_) cudaFree(p);
+  if (block_) cudaFree(block_);
 }
 
 // ============================================================================
 // Runner
 // ============================================================================
-Runner::Runner(std::vector<DeviceModel*> models, int tile_m) : models_(std::move(models)) {
+Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream)
+    : models_(std::move(models)), stream_(stream), own_stream_(stream == nullptr) {
   if (models_.empty()) throw std::runtime_error("Runner needs at least one model");
   if (tile_m != 8) throw std::runtime_error("only 32x8 cell tiles are built into this library");
   subgrid_ = models_[0]->host().p.subgrid;
@@ -772,20 +828,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m) : models_(std::move
     if (h.p.nsrc > 0) any_src_ = 1;
     bnd_blocks_ = std::max(bnd_blocks_, (h.p.nkcuv2 + h.p.nneu + 127) / 128);
     scns.push_back(models_[i]->dev());
-    const int nmax = h.p.nmax, mmax = h.p.mmax;
-    for (int m0 = 1; m0 <= mmax; m0 += tile_m) {
-      for (int n0 = 1; n0 <= nmax; n0 += 32) {
-        // skip tiles without any active cell
-        bool any = false;
-        for (int m = m0; m < m0 + tile_m && m <= mmax && !any; m++)
-          for (int n = n0; n < n0 + 32 && n <= nmax; n++)
-            if (h.flags[(size_t)m * h.p.ld + kGhostPad + n] & F_ACT) {
-              any = true;
-              break;
-            }
-        if (any) tiles.push_back(Tile{(int)i, n0, m0, 0});
-      }
-    }
+    for (const int2& t : h.tiles) tiles.push_back(Tile{(int)i, t.x, t.y, 0});
   }
   ntiles_ = (int)tiles.size();
   check_cuda(cudaMalloc(&d_scns_, scns.size() * sizeof(ScnDev)), "cudaMalloc scns");
@@ -794,33 +837,40 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m) : models_(std::move
     check_cuda(cudaMalloc(&d_tiles_, tiles.size() * sizeof(Tile)), "cudaMalloc tiles");
     check_cuda(cudaMemcpy(d_tiles_, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice), "tiles");
   }
-  check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  if (own_stream_) check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
   if (const char* v = std::getenv("SFG_MOMENTUM_VARIANT")) {
     const int x = std::atoi(v);
-    variant_ = (x == 2 || x == 3 || x == 4) ? x : 4;
+    variant_ = (x >= 2 && x <= 5) ? x : 5;
   }
   // TMA tensor maps (one set per model) and persistent grid sizes
   std::vector<MapSet> maps;
   for (auto* m : models_) maps.push_back(build_map_set(m->dev()));
   check_cuda(cudaMalloc(&d_maps_, maps.size() * sizeof(MapSet)), "cudaMalloc maps");
   check_cuda(cudaMemcpy(d_maps_, maps.data(), maps.size() * sizeof(MapSet), cudaMemcpyHostToDevice), "maps");
+  configure_grids();
+  check_cuda(cudaMallocHost(&h_states_, models_.size() * sizeof(StepState)), "pinned states");
+}
+
+// Persistent grids of the TMA kernels: resident CTAs per SM x SM count, capped
+// by the number of tiles.
+void Runner::configure_grids() {
   int dev = 0, nsm = 0, nb_m = 0, nb_c = 0;
   check_cuda(cudaGetDevice(&dev), "device");
   check_cuda(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "sm count");
-  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_m, momentum_tma_fn(subgrid_), 256, momentum_tma_smem()),
+  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_m, momentum_tma_fn(subgrid_, tma_minb(), one() != nullptr), 256,
+                                                           momentum_tma_smem()),
              "occupancy");
   check_cuda(
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_c, continuity_tma_fn(subgrid_), 256, continuity_tma_smem()),
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_c, continuity_tma_fn(subgrid_, one() != nullptr), 256, continuity_tma_smem()),
       "occupancy");
   mom_grid_ = std::max(1, std::min(ntiles_, std::max(nb_m, 1) * nsm));
   con_grid_ = std::max(1, std::min(ntiles_, std::max(nb_c, 1) * nsm));
-  check_cuda(cudaMallocHost(&h_states_, models_.size() * sizeof(StepState)), "pinned states");
 }
 
 Runner::~Runner() {
   if (graph_) cudaGraphExecDestroy(graph_);
   if (d_maps_) cudaFree(d_maps_);
-  if (stream_) cudaStreamDestroy(stream_);
+  if (stream_ && own_stream_) cudaStreamDestroy(stream_);
   if (d_scns_) cudaFree(d_scns_);
   if (d_tiles_) cudaFree(d_tiles_);
   if (h_states_) cudaFreeHost(h_states_);
@@ -828,13 +878,13 @@ Runner::~Runner() {
 
 void Runner::launch_one() {
   launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
-  if (variant_ == 4)
-    launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, mom_grid_, stream_);
+  if (tma())
+    launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, tma_minb(), mom_grid_, stream_, one());
   else
     launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
   if (any_src_) launch_sources(d_scns_, nscn(), stream_);
-  if (variant_ == 4)
-    launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_);
+  if (tma())
+    launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_, one());
   else
     launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
 }
@@ -855,6 +905,11 @@ void Runner::build_graph(int chunk) {
 }
 
 void Runner::refresh_params() {
+  // single-model launches carry the parameters by value: re-capture the graph
+  if (graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
   std::vector<ScnDev> scns;
   for (auto* m : models_) scns.push_back(m->dev());
   check_cuda(cudaMemcpyAsync(d_scns_, scns.data(), scns.size() * sizeof(ScnDev), cudaMemcpyHostToDevice, stream_),
@@ -880,15 +935,15 @@ std::vector<double> Runner::time_kernels(int nsteps) {
     check_cuda(cudaEventRecord(ev[0], stream_), "record");
     launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
     check_cuda(cudaEventRecord(ev[1], stream_), "record");
-    if (variant_ == 4)
-      launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, mom_grid_, stream_);
+    if (tma())
+      launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, tma_minb(), mom_grid_, stream_, one());
     else
       launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
     check_cuda(cudaEventRecord(ev[2], stream_), "record");
     if (any_src_) launch_sources(d_scns_, nscn(), stream_);
     check_cuda(cudaEventRecord(ev[3], stream_), "record");
-    if (variant_ == 4)
-      launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_);
+    if (tma())
+      launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_, one());
     else
       launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
     check_cuda(cudaEventRecord(ev[4], stream_), "record");
@@ -925,6 +980,41 @@ void Runner::step_once() {
   sync();
 }
 
+// Autotuner: times one chunk of real steps with each kernel variant on this
+// runner's own models and keeps the fastest.  Every variant computes bitwise
+// the same states (the GPU tests check it), so the choice never changes a
+// result, and the tuning steps are part of the run.  Only meaningful while
+// the models still have steps to take; returns the chosen variant.
+int Runner::autotune(int chunk) {
+  static const int kCandidates[] = {5, 4, 2};
+  cudaEvent_t e0, e1;
+  check_cuda(cudaEventCreate(&e0), "event");
+  check_cuda(cudaEventCreate(&e1), "event");
+  int best = variant_;
+  float best_ms = 0.0f;
+  tune_ms_.clear();
+  for (int v : kCandidates) {
+    set_variant(v);
+    build_graph(chunk);
+    check_cuda(cudaEventRecord(e0, stream_), "record");
+    check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+    check_cuda(cudaEventRecord(e1, stream_), "record");
+    check_cuda(cudaEventSynchronize(e1), "event sync");
+    float ms = 0.0f;
+    check_cuda(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+    tune_ms_.push_back({v, ms});
+    if (best_ms == 0.0f || ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  set_variant(best);
+  tuned_ = true;
+  return best;
+}
+
 void Runner::run(const std::vector<double>& tend, long long max_steps, int chunk) {
   if (tend.size() != models_.size()) throw std::runtime_error("one target time per model is required");
   std::vector<double> tend_h = tend;
@@ -936,22 +1026,41 @@ void Runner::run(const std::vector<double>& tend, long long max_steps, int chunk
                                stream_),
                "steps");
   }
-  build_graph(chunk);
-  for (;;) {
-    check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+  auto all_done = [&]() {
+    for (int i = 0; i < nscn(); i++) {
+      const StepState& s = h_states_[i];
+      if (!(s.stop_pending || !(s.t < s.tend) || s.steps_left == 0)) return false;
+    }
+    return true;
+  };
+  auto read_states = [&]() {
     for (int i = 0; i < nscn(); i++)
       check_cuda(cudaMemcpyAsync(&h_states_[i], models_[i]->state(), sizeof(StepState), cudaMemcpyDeviceToHost,
                                  stream_),
                  "read state");
+  };
+  if (autotune_ && !tuned_) {
+    autotune(chunk);
+    read_states();
     sync();
-    bool all_done = true;
-    for (int i = 0; i < nscn(); i++) {
-      const StepState& s = h_states_[i];
-      const bool done = s.stop_pending || !(s.t < s.tend) || s.steps_left == 0;
-      if (!done) all_done = false;
-    }
-    if (all_done) break;
+    if (all_done()) return;
   }
+  build_graph(chunk);
+  // Two chunks in flight: chunk k+1 is queued before the host looks at the
+  // states copied after chunk k, so the GPU never waits for the host.  Steps
+  // queued past a model's end are no-ops on the device (k_step stops it).
+  cudaEvent_t ready;
+  check_cuda(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
+  check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+  for (;;) {
+    read_states();
+    check_cuda(cudaEventRecord(ready, stream_), "record");
+    check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+    check_cuda(cudaEventSynchronize(ready), "event sync");
+    if (all_done()) break;
+  }
+  cudaEventDestroy(ready);
+  sync();
 }
 
 }  // namespace sfg

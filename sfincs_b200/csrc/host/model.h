@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../sfg_device.h"
@@ -52,6 +53,7 @@ struct HostModel {
   std::vector<int32_t> src_cell;
   long long n_kcs1 = 0;
   double area_total_kcs1 = 0;
+  std::vector<int2> tiles;  // (n0, m0) of every 32 x 8 tile holding an active cell
 };
 
 // Reads <dir>/sfincs.inp and the files it names.  bmi mirrors the reference's
@@ -73,28 +75,32 @@ class DeviceModel {
   int32_t* d_cmp_off() { return d_cmp_; }
 
  private:
-  template <class X>
-  X* upload(const std::vector<X>& v);
-  template <class X>
-  X* alloc(size_t n);
   const HostModel* h_;
   ScnDev d_{};
-  std::vector<void*> allocs_;
+  void* block_ = nullptr;  // every device array of the model, one allocation
   int32_t* d_cmp_ = nullptr;
   size_t bytes_ = 0;
 };
+
+// Device bytes a DeviceModel of h will allocate (exact; no allocation made).
+size_t device_bytes_needed(const HostModel& h);
 
 // Advances one or more device models together.  Every launch covers all
 // models; models whose time has reached their own target are skipped on the
 // device (no host round trip per step).
 class Runner {
  public:
-  Runner(std::vector<DeviceModel*> models, int tile_m = 8);
+  // stream: run on this stream (not owned); null: the runner creates its own.
+  Runner(std::vector<DeviceModel*> models, int tile_m = 8, cudaStream_t stream = nullptr);
   ~Runner();
   // Run until every model reached its target time; at most max_steps steps
   // per model when max_steps >= 0.  Steps are issued in CUDA-graph chunks of
   // `chunk` steps; the host checks completion once per chunk.
   void run(const std::vector<double>& tend, long long max_steps, int chunk = 32);
+  // Autotune the kernel variant on the next chunk of steps (see model.cpp).
+  int autotune(int chunk = 32);
+  void set_autotune(bool on) { autotune_ = on; }
+  const std::vector<std::pair<int, float>>& tune_ms() const { return tune_ms_; }
   // One step exactly (reference update()).
   void step_once();
   void sync();
@@ -112,8 +118,16 @@ class Runner {
       cudaGraphExecDestroy(graph_);
       graph_ = nullptr;
     }
+    configure_grids();
   }
   int variant() const { return variant_; }
+  // variants 4 and 5: TMA-staged kernels (5: momentum compiled for 4 CTAs/SM);
+  // 2 and 3: per-thread-load kernels
+  bool tma() const { return variant_ >= 4; }
+  // the one model of a single-model runner (its parameters travel by value in
+  // the launches), null for an ensemble
+  const ScnDev* one() const { return models_.size() == 1 ? &models_[0]->dev() : nullptr; }
+  int tma_minb() const { return variant_ == 5 ? 4 : 3; }
   // launch one step (all kernels) on the runner's stream
   void launch_one();
   int nscn() const { return (int)models_.size(); }
@@ -126,20 +140,24 @@ class Runner {
 
  private:
   void build_graph(int chunk);
+  void configure_grids();
   std::vector<DeviceModel*> models_;
   ScnDev* d_scns_ = nullptr;
   Tile* d_tiles_ = nullptr;
   int ntiles_ = 0;
   int bnd_blocks_ = 0;
-  int variant_ = 4;
+  int variant_ = 5;
   MapSet* d_maps_ = nullptr;  // TMA tensor maps, one set per model
   int mom_grid_ = 0, con_grid_ = 0;
   int subgrid_ = 0;
   int any_src_ = 0;
   cudaStream_t stream_ = nullptr;
+  bool own_stream_ = true;
   cudaGraphExec_t graph_ = nullptr;
   int graph_chunk_ = 0;
   StepState* h_states_ = nullptr;  // pinned mirror of the step states
+  bool autotune_ = false, tuned_ = false;
+  std::vector<std::pair<int, float>> tune_ms_;  // (variant, ms per chunk) of the last autotune
 };
 
 void launch_step(const ScnDev* d_scns, int nscn, int bnd_blocks, const Tile* d_tiles, int ntiles, int subgrid,
@@ -155,11 +173,11 @@ void check_cuda(cudaError_t e, const char* what);
 MapSet build_map_set(const ScnDev& d);
 int momentum_tma_smem();
 int continuity_tma_smem();
-const void* momentum_tma_fn(int subgrid);
-const void* continuity_tma_fn(int subgrid);
+const void* momentum_tma_fn(int subgrid, int minb, bool one);
+const void* continuity_tma_fn(int subgrid, bool one);
 void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
-                         int grid, cudaStream_t s);
+                         int minb, int grid, cudaStream_t s, const ScnDev* one);
 void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
-                           int grid, cudaStream_t s);
+                           int grid, cudaStream_t s, const ScnDev* one);
 
 }  // namespace sfg

@@ -451,7 +451,7 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepState&
   if (S.thetasmooth && (f & TH) && fabsf(qx_nmd) > 1.0e-6f && fabsf(qx_nmu) > 1.0e-6f)
     qsm = S.theta * qx_nm + 0.5f * (1.0f - S.theta) * (qx_nmu + qx_nmd);
   const float dt = st.dt;
-  const float hu73 = hu * hu * powf(hu, 1.0f / 3.0f);
+  const float hu73 = hu * hu * cbrtf(hu);  // as in kernels_tma.cu: cube root for hu**(1.0/3.0)
   float q = (qsm + frc * dt) / (1.0f + gnavg2 * dt * qfr / hu73);
   if (SG && S.wiggle) {
     const float mdrv = fabsf(zd_nm - zd_nmu) - S.wiggle_threshold;

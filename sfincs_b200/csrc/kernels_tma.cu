@@ -63,9 +63,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, i
       : "memory");
 }
 
-__device__ __forceinline__ float warp_min_t(float v) {
-  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+__device__ __forceinline__ float warp_max_t(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
+}
+// Fold a warp's largest CFL denominator into the scenario's min_dt: one
+// division and one atomicMin per warp (positive floats order like their bits).
+__device__ __forceinline__ void flush_cfl(StepState* st, float den, int lane) {
+  den = warp_max_t(den);
+  if (lane == 0 && st && den > 0.0f) atomicMin(&st->min_dt_bits, __float_as_uint(1.0f / den));
 }
 
 // --------------------------------------------------------------------------
@@ -92,13 +98,23 @@ constexpr int STAGE = 12288;
 
 __device__ __forceinline__ const void* map_of(const MapSet* maps, int scn, int id) { return maps[scn].m[id]; }
 
+// Where a tile's scenario parameters come from.  ONE: the launch advances a
+// single model whose ScnDev is passed by value as a __grid_constant__ kernel
+// parameter, so every field is a constant-bank operand (no load instruction,
+// no address arithmetic, no aliasing with the stores of the step).  Otherwise
+// the device table of an ensemble, indexed by the tile's scenario.
+template <bool ONE>
+__device__ __forceinline__ const ScnDev& scn_of(const ScnDev* __restrict__ scns, const ScnDev& one, int i) {
+  if (ONE) return one;
+  return scns[i];
+}
+
 // --------------------------------------------------------------------------
 // Momentum
 // --------------------------------------------------------------------------
 template <bool SG>
-__device__ __forceinline__ bool issue_momentum(const ScnDev* scns, const MapSet* maps, const Tile& tl,
+__device__ __forceinline__ bool issue_momentum(const ScnDev& S, const MapSet* maps, const Tile& tl,
                                                unsigned char* st, uint64_t* bar) {
-  const ScnDev& S = scns[tl.scn];
   const StepState& ss = *S.st;
   if (!ss.run) return false;
   const int p = ss.parity;
@@ -138,7 +154,11 @@ struct FaceV {
 };
 
 // Flux update of one wet face from gathered inputs (sfincs_momentum.f90:389-733).
-// Returns min_dt_ip; writes q, uv.
+// Writes q, uv and returns the face's CFL denominator
+// den = max(sqrt(g*hu), |uv|) * dxuvinv.  The reference takes the minimum of
+// 1/den over faces (:731-733); correctly rounded division is monotone, so that
+// minimum equals 1/max(den) bit for bit and one division per CTA replaces one
+// per face.
 template <bool SG, int DIR>
 __device__ __forceinline__ float face_flux(const ScnDev& S, const StepState& st, uint16_t f, uint8_t kf, float zs_nm,
                                            float zs_nmu, float hu, float gnavg2, float phi, const FaceV& a,
@@ -150,7 +170,6 @@ __device__ __forceinline__ float face_flux(const ScnDev& S, const StepState& st,
   const float dyuvinv = DIR == 0 ? S.dyinv : S.dxinv;
   const float dxuv2inv = DIR == 0 ? S.dx2inv : S.dy2inv;
   const float dyuv2inv = DIR == 0 ? S.dy2inv : S.dx2inv;
-  const float hwet = hu / phi;
   float dzdx;
   if (S.slopelim < 9999.0f)
     dzdx = fminf(fmaxf((zs_nmu - zs_nm) * dxuvinv, -S.slopelim), S.slopelim);
@@ -206,6 +225,7 @@ __device__ __forceinline__ float face_flux(const ScnDev& S, const StepState& st,
   }
   if (S.wind) {
     const float tauw = DIR == 0 ? st.twu : st.twv;
+    const float hwet = hu / phi;
     if (hwet > 0.25f)
       frc = frc + phi * tauw;
     else
@@ -223,7 +243,10 @@ __device__ __forceinline__ float face_flux(const ScnDev& S, const StepState& st,
   if (S.thetasmooth && (f & TH) && fabsf(a.qx_nmd) > 1.0e-6f && fabsf(a.qx_nmu) > 1.0e-6f)
     qsm = S.theta * a.qx_nm + 0.5f * (1.0f - S.theta) * (a.qx_nmu + a.qx_nmd);
   const float dt = st.dt;
-  const float hu73 = hu * hu * powf(hu, 1.0f / 3.0f);
+  // hu**2 * hu**(1.0/3.0) (:673).  The real*4 exponent 1.0/3.0 is 0.333333343,
+  // so hu**expo and cbrt(hu) differ by a factor hu**(1e-8): under one ulp for
+  // 1e-3 <= hu <= 1e3.  cbrtf is the cheaper of the two on the device.
+  const float hu73 = hu * hu * cbrtf(hu);
   float q = (qsm + frc * dt) / (1.0f + gnavg2 * dt * qfr / hu73);
   if (SG && S.wiggle) {
     const float mdrv = fabsf(zd_nm - zd_nmu) - S.wiggle_threshold;
@@ -235,7 +258,7 @@ __device__ __forceinline__ float face_flux(const ScnDev& S, const StepState& st,
   const float uv = q / fmaxf(hu, S.huvmin);
   q_out = q;
   uv_out = uv;
-  return 1.0f / (fmaxf(sqrtf(S.g * hu), fabsf(uv)) * dxuvinv);
+  return fmaxf(sqrtf(S.g * hu), fabsf(uv)) * dxuvinv;
 }
 
 // Subgrid depth / roughness / wet fraction at the face level zsu (sfincs_momentum.f90:345-380).
@@ -246,13 +269,14 @@ struct SgLook {
   UvRec r;    // interpolation branch
 };
 
-template <bool SG>
-__global__ void __launch_bounds__(256) k_momentum_tma(const ScnDev* __restrict__ scns, const MapSet* __restrict__ maps,
-                                                      const Tile* __restrict__ tiles, int ntiles) {
+template <bool SG, int MINB, bool ONE>
+__global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __restrict__ scns,
+                                                            const MapSet* __restrict__ maps,
+                                                            const Tile* __restrict__ tiles, int ntiles,
+                                                            const __grid_constant__ ScnDev one) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_issued[2];
-  __shared__ float s_min[8];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + 32 * ty;
   if (tid == 0) {
@@ -263,23 +287,34 @@ __global__ void __launch_bounds__(256) k_momentum_tma(const ScnDev* __restrict__
   __syncthreads();
   uint32_t phase[2] = {0u, 0u};
   int tile = blockIdx.x;
-  if (tid == 0) s_issued[0] = tile < ntiles ? issue_momentum<SG>(scns, maps, tiles[tile], smem, &bar[0]) : 0;
+  // running CFL denominator of this thread's faces, for scenario cfl_st
+  StepState* cfl_st = nullptr;
+  float cfl_den = 0.0f;
+  if (tid == 0)
+    s_issued[0] = tile < ntiles ? issue_momentum<SG>(scn_of<ONE>(scns, one, tiles[tile].scn), maps, tiles[tile],
+                                                     smem, &bar[0])
+                                : 0;
   for (int it = 0; tile < ntiles; it++) {
     const int s = it & 1;
     const int next = tile + gridDim.x;
     __syncthreads();  // s_issued[s] visible; stage s^1 no longer read
     if (tid == 0) {
       fence_proxy_async();
-      s_issued[s ^ 1] =
-          next < ntiles ? issue_momentum<SG>(scns, maps, tiles[next], smem + (s ^ 1) * mom::STAGE, &bar[s ^ 1]) : 0;
+      s_issued[s ^ 1] = next < ntiles ? issue_momentum<SG>(scn_of<ONE>(scns, one, tiles[next].scn), maps,
+                                                           tiles[next], smem + (s ^ 1) * mom::STAGE, &bar[s ^ 1])
+                                      : 0;
     }
     if (s_issued[s]) {
       const Tile tl = tiles[tile];
-      const ScnDev& S = scns[tl.scn];
+      const ScnDev& S = scn_of<ONE>(scns, one, tl.scn);
       StepState& st = *S.st;
+      if (&st != cfl_st) {  // the tile's scenario changed (CTA-uniform)
+        flush_cfl(cfl_st, cfl_den, tx);
+        cfl_st = &st;
+        cfl_den = 0.0f;
+      }
       const bool ok = mbar_wait_bounded(&bar[s], phase[s]);
       phase[s] ^= 1u;
-      float mdt = FLT_MAX;
       const int n = tl.n0 + tx, m = tl.m0 + ty;
       if (!ok) {
         st.fault = 1;
@@ -381,8 +416,8 @@ __global__ void __launch_bounds__(256) k_momentum_tma(const ScnDev* __restrict__
               hu = fmaxf(zsu_u - zmin_u, S.huthresh);
               gnavg2 = ((const float*)(sm + mom::O_GN2U))[ty * 32 + tx];
             }
-            mdt = fminf(mdt, face_flux<SG, 0>(S, st, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1,
-                                              qn, un));
+            cfl_den = fmaxf(cfl_den, face_flux<SG, 0>(S, st, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1,
+                                                      zd0, zd1, qn, un));
             S.qu[p ^ 1][c] = qn;
             S.uu[p ^ 1][c] = un;
           } else if (kfu & KF_WET2) {
@@ -437,8 +472,8 @@ __global__ void __launch_bounds__(256) k_momentum_tma(const ScnDev* __restrict__
               hu = fmaxf(zsu_v - zmin_v, S.huthresh);
               gnavg2 = ((const float*)(sm + mom::O_GN2V))[ty * 32 + tx];
             }
-            mdt = fminf(mdt, face_flux<SG, 1>(S, st, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1,
-                                              qn, un));
+            cfl_den = fmaxf(cfl_den, face_flux<SG, 1>(S, st, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1,
+                                                      zd0, zd1, qn, un));
             S.qv[p ^ 1][c] = qn;
             S.vv[p ^ 1][c] = un;
           } else if (kfv & KF_WET2) {
@@ -450,18 +485,10 @@ __global__ void __launch_bounds__(256) k_momentum_tma(const ScnDev* __restrict__
           if (kn != kfv) S.kf[1][c] = kn;
         }
       }
-      // CTA min of the CFL step, one atomicMin per tile
-      mdt = warp_min_t(mdt);
-      if (tx == 0) s_min[ty] = mdt;
-      __syncthreads();
-      if (ty == 0) {
-        float v = tx < 8 ? s_min[tx] : FLT_MAX;
-        v = warp_min_t(v);
-        if (tx == 0 && v < FLT_MAX) atomicMin(&st.min_dt_bits, __float_as_uint(v));
-      }
     }
     tile = next;
   }
+  flush_cfl(cfl_st, cfl_den, tx);
   // drain: every issued stage has been waited for in the loop; nothing in flight here
 }
 
@@ -469,9 +496,8 @@ __global__ void __launch_bounds__(256) k_momentum_tma(const ScnDev* __restrict__
 // Continuity
 // --------------------------------------------------------------------------
 template <bool SG>
-__device__ __forceinline__ bool issue_continuity(const ScnDev* scns, const MapSet* maps, const Tile& tl,
+__device__ __forceinline__ bool issue_continuity(const ScnDev& S, const MapSet* maps, const Tile& tl,
                                                  unsigned char* st, uint64_t* bar) {
-  const ScnDev& S = scns[tl.scn];
   const StepState& ss = *S.st;
   if (!ss.run) return false;
   const int p1 = ss.parity ^ 1;
@@ -501,9 +527,10 @@ __device__ __forceinline__ bool issue_continuity(const ScnDev* scns, const MapSe
   return true;
 }
 
-template <bool SG>
+template <bool SG, bool ONE>
 __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict__ scns, const MapSet* __restrict__ maps,
-                                                        const Tile* __restrict__ tiles, int ntiles) {
+                                                        const Tile* __restrict__ tiles, int ntiles,
+                                                        const __grid_constant__ ScnDev one) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_issued[2];
@@ -517,20 +544,23 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
   __syncthreads();
   uint32_t phase[2] = {0u, 0u};
   int tile = blockIdx.x;
-  if (tid == 0) s_issued[0] = tile < ntiles ? issue_continuity<SG>(scns, maps, tiles[tile], smem, &bar[0]) : 0;
+  if (tid == 0)
+    s_issued[0] = tile < ntiles ? issue_continuity<SG>(scn_of<ONE>(scns, one, tiles[tile].scn), maps, tiles[tile],
+                                                       smem, &bar[0])
+                                : 0;
   for (int it = 0; tile < ntiles; it++) {
     const int s = it & 1;
     const int next = tile + gridDim.x;
     __syncthreads();
     if (tid == 0) {
       fence_proxy_async();
-      s_issued[s ^ 1] =
-          next < ntiles ? issue_continuity<SG>(scns, maps, tiles[next], smem + (s ^ 1) * con::STAGE, &bar[s ^ 1])
-                        : 0;
+      s_issued[s ^ 1] = next < ntiles ? issue_continuity<SG>(scn_of<ONE>(scns, one, tiles[next].scn), maps,
+                                                             tiles[next], smem + (s ^ 1) * con::STAGE, &bar[s ^ 1])
+                                      : 0;
     }
     if (s_issued[s]) {
       const Tile tl = tiles[tile];
-      const ScnDev& S = scns[tl.scn];
+      const ScnDev& S = scn_of<ONE>(scns, one, tl.scn);
       StepState& st = *S.st;
       const bool ok = mbar_wait_bounded(&bar[s], phase[s]);
       phase[s] ^= 1u;
@@ -617,31 +647,68 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
 int momentum_tma_smem() { return 2 * mom::STAGE; }
 int continuity_tma_smem() { return 2 * con::STAGE; }
 
-const void* momentum_tma_fn(int subgrid) {
-  return subgrid ? (const void*)k_momentum_tma<true> : (const void*)k_momentum_tma<false>;
+// minb: CTAs per SM the momentum kernel is compiled for (3: up to 80
+// registers per thread; 4: at most 64), an autotuned choice.  one: the single
+// scenario of the launch (passed by value), or null for an ensemble table.
+template <bool SG, bool ONE>
+static const void* momentum_fn(int minb) {
+  return minb >= 4 ? (const void*)k_momentum_tma<SG, 4, ONE> : (const void*)k_momentum_tma<SG, 3, ONE>;
 }
-const void* continuity_tma_fn(int subgrid) {
-  return subgrid ? (const void*)k_continuity_tma<true> : (const void*)k_continuity_tma<false>;
+const void* momentum_tma_fn(int subgrid, int minb, bool one) {
+  if (one) return subgrid ? momentum_fn<true, true>(minb) : momentum_fn<false, true>(minb);
+  return subgrid ? momentum_fn<true, false>(minb) : momentum_fn<false, false>(minb);
+}
+const void* continuity_tma_fn(int subgrid, bool one) {
+  if (one) return subgrid ? (const void*)k_continuity_tma<true, true> : (const void*)k_continuity_tma<false, true>;
+  return subgrid ? (const void*)k_continuity_tma<true, false> : (const void*)k_continuity_tma<false, false>;
+}
+
+template <bool SG, int MINB, bool ONE>
+static void mom_launch(int grid, cudaStream_t s, const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles,
+                       int ntiles, const ScnDev& one) {
+  k_momentum_tma<SG, MINB, ONE><<<grid, dim3(32, 8), 2 * mom::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, one);
 }
 
 void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
-                         int grid, cudaStream_t s) {
+                         int minb, int grid, cudaStream_t s, const ScnDev* one) {
   if (ntiles <= 0) return;
-  const dim3 blk(32, 8);
-  if (subgrid)
-    k_momentum_tma<true><<<grid, blk, 2 * mom::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles);
-  else
-    k_momentum_tma<false><<<grid, blk, 2 * mom::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles);
+  static const ScnDev none{};
+  const ScnDev& o = one ? *one : none;
+  const bool b4 = minb >= 4;
+  if (one) {
+    if (subgrid)
+      b4 ? mom_launch<true, 4, true>(grid, s, d_scns, d_maps, d_tiles, ntiles, o)
+         : mom_launch<true, 3, true>(grid, s, d_scns, d_maps, d_tiles, ntiles, o);
+    else
+      b4 ? mom_launch<false, 4, true>(grid, s, d_scns, d_maps, d_tiles, ntiles, o)
+         : mom_launch<false, 3, true>(grid, s, d_scns, d_maps, d_tiles, ntiles, o);
+  } else {
+    if (subgrid)
+      b4 ? mom_launch<true, 4, false>(grid, s, d_scns, d_maps, d_tiles, ntiles, o)
+         : mom_launch<true, 3, false>(grid, s, d_scns, d_maps, d_tiles, ntiles, o);
+    else
+      b4 ? mom_launch<false, 4, false>(grid, s, d_scns, d_maps, d_tiles, ntiles, o)
+         : mom_launch<false, 3, false>(grid, s, d_scns, d_maps, d_tiles, ntiles, o);
+  }
 }
 
 void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
-                           int grid, cudaStream_t s) {
+                           int grid, cudaStream_t s, const ScnDev* one) {
   if (ntiles <= 0) return;
+  static const ScnDev none{};
+  const ScnDev& o = one ? *one : none;
   const dim3 blk(32, 8);
-  if (subgrid)
-    k_continuity_tma<true><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles);
-  else
-    k_continuity_tma<false><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles);
+  if (one) {
+    if (subgrid)
+      k_continuity_tma<true, true><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, o);
+    else
+      k_continuity_tma<false, true><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, o);
+  } else {
+    if (subgrid)
+      k_continuity_tma<true, false><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, o);
+    else
+      k_continuity_tma<false, false><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, o);
+  }
 }
 
 }  // namespace sfg

@@ -19,7 +19,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _model(d, variant=None):
-    """variant: kernel path (2, 3: per-thread loads; 4: TMA-staged tiles); None = library default."""
+    """variant: kernel path (2, 3: per-thread loads; 4, 5: TMA-staged tiles, 5 compiled for 4 CTAs/SM);
+    None = library default."""
     import os
 
     from sfincs_b200.bmi import Model
@@ -61,7 +62,7 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("variant", [2, 4])
+@pytest.mark.parametrize("variant", [2, 4, 5])
 @pytest.mark.parametrize("kind", sorted(CASES))
 def test_stepwise_matches_f32_oracle(tmp_path, kind, variant):
     d, _ = CASES[kind](tmp_path)
@@ -131,12 +132,12 @@ def test_full_run_against_fp64_oracle(tmp_path, kind):
 def test_deterministic_and_paths_agree(tmp_path, kind):
     """Bitwise reproducible; the per-thread-load and TMA-staged paths compute identical states."""
     d, _ = CASES[kind](tmp_path)
-    a, b, c = _model(d, 4), _model(d, 4), _model(d, 2)
-    for g in (a, b, c):
+    runs = [_model(d, v) for v in (5, 5, 4, 2)]
+    for g in runs:
         g.step(200)
     for name in ("zs", "qx", "qy", "uvx", "uvy"):
-        assert np.array_equal(a.get(name), b.get(name)), name
-        assert np.array_equal(a.get(name), c.get(name)), name
+        for g in runs[1:]:
+            assert np.array_equal(runs[0].get(name), g.get(name)), name
 
 
 def test_lake_at_rest(tmp_path):
