@@ -36,7 +36,7 @@ class File {
       dims_.push_back((uint64_t)u32());
       dimnames_[nm] = (int)dims_.size() - 1;
     }
-    skip_attrs();
+    read_attrs(&gatts_);
     tag = u32();
     n = u32();
     for (uint32_t i = 0; i < (tag ? n : 0); i++) {
@@ -60,7 +60,17 @@ class File {
     return dims_[it->second];
   }
   bool has(const std::string& n) const { return vars_.count(n) != 0; }
+  // numeric global attribute (first value), as double
+  double att(const std::string& n) const {
+    auto it = gatts_.find(n);
+    if (it == gatts_.end()) throw std::runtime_error("missing global attribute " + n + " in " + path_);
+    return it->second;
+  }
   std::vector<float> read_float(const std::string& n) const {
+    auto d = read_double(n);
+    return std::vector<float>(d.begin(), d.end());
+  }
+  std::vector<double> read_double(const std::string& n) const {
     auto it = vars_.find(n);
     if (it == vars_.end()) throw std::runtime_error("missing variable " + n + " in " + path_);
     const Var& v = it->second;
@@ -70,22 +80,22 @@ class File {
     f.seekg((std::streamoff)v.begin);
     f.read(reinterpret_cast<char*>(raw.data()), (std::streamsize)raw.size());
     if (!f) throw std::runtime_error("short read of " + n);
-    std::vector<float> out((size_t)v.count);
-    for (size_t i = 0; i < out.size(); i++) {
-      const uint8_t* p = raw.data() + i * sz[v.type];
-      switch (v.type) {
-        case 1: out[i] = (float)(int8_t)p[0]; break;
-        case 3: out[i] = (float)(int16_t)((p[0] << 8) | p[1]); break;
-        case 4: out[i] = (float)(int32_t)be32(p); break;
-        case 5: { uint32_t b = be32(p); float x; std::memcpy(&x, &b, 4); out[i] = x; break; }
-        case 6: { uint64_t b = ((uint64_t)be32(p) << 32) | be32(p + 4); double x; std::memcpy(&x, &b, 8); out[i] = (float)x; break; }
-        default: throw std::runtime_error("unsupported netCDF type");
-      }
-    }
+    std::vector<double> out((size_t)v.count);
+    for (size_t i = 0; i < out.size(); i++) out[i] = value(v.type, raw.data() + i * sz[v.type]);
     return out;
   }
 
  private:
+  static double value(int type, const uint8_t* p) {
+    switch (type) {
+      case 1: return (double)(int8_t)p[0];
+      case 3: return (double)(int16_t)((p[0] << 8) | p[1]);
+      case 4: return (double)(int32_t)be32(p);
+      case 5: { uint32_t b = be32(p); float x; std::memcpy(&x, &b, 4); return (double)x; }
+      case 6: { uint64_t b = ((uint64_t)be32(p) << 32) | be32(p + 4); double x; std::memcpy(&x, &b, 8); return x; }
+      default: throw std::runtime_error("unsupported netCDF type");
+    }
+  }
   static uint32_t be32(const uint8_t* p) { return ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3]; }
   uint32_t u32() {
     if (pos_ + 4 > hdr_.size()) throw std::runtime_error("truncated netCDF header");
@@ -99,6 +109,16 @@ class File {
     std::string s(reinterpret_cast<const char*>(&hdr_[pos_]), n);
     pos_ += (n + 3) & ~3u;
     return s;
+  }
+  void read_attrs(std::map<std::string, double>* into) {
+    static const int sz[] = {0, 1, 1, 2, 4, 4, 8};
+    uint32_t tag = u32(), n = u32();
+    for (uint32_t i = 0; i < (tag ? n : 0); i++) {
+      std::string nm = name();
+      uint32_t t = u32(), cnt = u32();
+      if (t != 2 && cnt > 0 && t <= 6) (*into)[nm] = value((int)t, &hdr_[pos_]);
+      pos_ += ((size_t)cnt * sz[t] + 3) & ~(size_t)3;
+    }
   }
   void skip_attrs() {
     static const int sz[] = {0, 1, 1, 2, 4, 4, 8};
@@ -116,6 +136,7 @@ class File {
   std::vector<uint64_t> dims_;
   std::map<std::string, int> dimnames_;
   std::map<std::string, Var> vars_;
+  std::map<std::string, double> gatts_;
 };
 
 }  // namespace nc3

@@ -195,7 +195,7 @@ struct Model {
   F1<int8_t> qt_level, qt_md, qt_mu, qt_nd, qt_nu;
   F1<int32_t> qt_md1, qt_md2, qt_mu1, qt_mu2, qt_nd1, qt_nd2, qt_nu1, qt_nu2, qt_n, qt_m, qt_nm_indices,
       qt_first, qt_last;
-  F1<float> qt_dxr, qt_dyr;
+  F1<float> qt_dxr, qt_dyr, qt_zz;
   float qt_cosrot, qt_sinrot;
 
   // --- mesh (sfincs_data.f90)
@@ -439,12 +439,79 @@ struct Model {
     }
   }
 
+  // quadtree_read_file + quadtree_read_file_netcdf: sfincs_quadtree.F90:64-160, 295-440
+  std::vector<int8_t> read_quadtree_netcdf() {
+    if (qtrfile.find(".nc") == std::string::npos)
+      throw std::runtime_error("oracle: only netCDF quadtree files are restated");
+    nc3::File nc(path(qtrfile));
+    qt_np = (long)nc.dim("mesh2d_nFaces");
+    auto i32 = [&](const char* v, F1<int32_t>& a) {
+      auto d = nc.read_double(v);
+      a.alloc(qt_np);
+      for (long i = 1; i <= qt_np; i++) a(i) = (int32_t)d[i - 1];
+    };
+    auto i8 = [&](const char* v, F1<int8_t>& a) {
+      auto d = nc.read_double(v);
+      a.alloc(qt_np);
+      for (long i = 1; i <= qt_np; i++) a(i) = (int8_t)d[i - 1];
+    };
+    i32("n", qt_n);
+    i32("m", qt_m);
+    i8("level", qt_level);
+    i8("md", qt_md); i32("md1", qt_md1); i32("md2", qt_md2);
+    i8("mu", qt_mu); i32("mu1", qt_mu1); i32("mu2", qt_mu2);
+    i8("nd", qt_nd); i32("nd1", qt_nd1); i32("nd2", qt_nd2);
+    i8("nu", qt_nu); i32("nu1", qt_nu1); i32("nu2", qt_nu2);
+    {
+      auto z = nc.read_double("z");
+      qt_zz.alloc(qt_np);
+      for (long i = 1; i <= qt_np; i++) qt_zz(i) = (float)z[i - 1];
+    }
+    std::vector<int8_t> mskq((size_t)qt_np);
+    {
+      auto mk = nc.read_double("mask");
+      for (long i = 0; i < qt_np; i++) mskq[(size_t)i] = (int8_t)mk[(size_t)i];
+    }
+    qt_x0 = (float)nc.att("x0");
+    qt_y0 = (float)nc.att("y0");
+    qt_dx = (float)nc.att("dx");
+    qt_dy = (float)nc.att("dy");
+    qt_rot = (float)nc.att("rotation");
+    qt_nmax = (int)nc.att("nmax");
+    qt_mmax = (int)nc.att("mmax");
+    qt_nlev = (int)nc.att("nr_levels");
+    const float pi = 3.141592653589793f;
+    qt_rot = qt_rot * pi / 180.0f;
+    qt_cosrot = std::cos(qt_rot);
+    qt_sinrot = std::sin(qt_rot);
+    qt_dxr.alloc(qt_nlev);
+    qt_dyr.alloc(qt_nlev);
+    for (int iref = 1; iref <= qt_nlev; iref++) {
+      qt_dxr(iref) = qt_dx / (float)(1 << (iref - 1));
+      qt_dyr(iref) = qt_dy / (float)(1 << (iref - 1));
+    }
+    for (long nm = 1; nm <= qt_np; nm++) {  // :118-126
+      int iref = qt_level(nm);
+      qt_nmax = std::max(qt_nmax, (int)((1.0f * (qt_n(nm) - 1) + 0.01f) / (float)(1 << (iref - 1))) + 1);
+      qt_mmax = std::max(qt_mmax, (int)((1.0f * (qt_m(nm) - 1) + 0.01f) / (float)(1 << (iref - 1))) + 1);
+    }
+    build_qt_search();
+    return mskq;
+  }
+
   // initialize_mesh: sfincs_domain.f90:143-1586
   void initialize_mesh() {
     std::vector<int8_t> mskq;
-    if (use_quadtree) throw std::runtime_error("oracle: quadtree files are read in a later build step");
     if (inputtype != "bin") throw std::runtime_error("oracle: only inputformat=bin is restated");
-    {
+    if (use_quadtree) {
+      mskq = read_quadtree_netcdf();  // :193-215 (netCDF quadtree: the mask comes with the file, :302-305)
+      x0 = qt_x0;
+      y0 = qt_y0;
+      nmax = qt_nmax;
+      mmax = qt_mmax;
+      dx = qt_dx;
+      dy = qt_dy;
+    } else {
       auto head = read_stream<int32_t>(path(indexfile), 1);
       long n_act = head[0];
       auto idx = read_stream<int32_t>(path(indexfile), (size_t)n_act, 4);
@@ -839,8 +906,12 @@ struct Model {
       zb.alloc(np);
       zbuv.alloc(npuv);
       zbuvmx.alloc(npuv);
-      auto d = read_stream<float>(path(depfile), (size_t)np);
-      for (long i = 1; i <= np; i++) zb(i) = d[i - 1];
+      if (use_quadtree && depfile.substr(0, 4) == "none") {  // :1618-1638
+        for (long i = 1; i <= np; i++) zb(i) = qt_zz(index_quadtree_in_sfincs(i));
+      } else {
+        auto d = read_stream<float>(path(depfile), (size_t)np);
+        for (long i = 1; i <= np; i++) zb(i) = d[i - 1];
+      }
       for (long ip = 1; ip <= npuv; ip++) {
         long nm = uv_index_z_nm(ip), nmu = uv_index_z_nmu(ip);
         if (uv_flags_type(ip) == 0)
@@ -862,35 +933,73 @@ struct Model {
     nc3::File nc(path(sbgfile));
     subgrid_nlevels = (int)nc.dim("levels");
     long L = subgrid_nlevels;
-    // regular grid: identity remapping (:246-270)
     auto zmin = nc.read_float("z_zmin"), zmax = nc.read_float("z_zmax"), volmax = nc.read_float("z_volmax"),
          zlev = nc.read_float("z_level"), uzmin = nc.read_float("uv_zmin"), uzmax = nc.read_float("uv_zmax"),
          uffit = nc.read_float("uv_ffit"), unavg = nc.read_float("uv_navg"), uhavg = nc.read_float("uv_havg"),
          unrep = nc.read_float("uv_nrep"), upwet = nc.read_float("uv_pwet");
-    if ((long)zmin.size() != np || (long)uzmin.size() != npuv)
-      throw std::runtime_error("oracle: subgrid file does not match the mesh");
+    // file index (0-based) of every active cell and uv point: identity on a
+    // regular grid (:246-270); on a quadtree the file covers every quadtree
+    // point and its right/upper faces (:166-245)
+    std::vector<long> zi((size_t)np), ui((size_t)npuv);
+    if (use_quadtree) {
+      long npuvq = 0, npuvs = 0;
+      for (long ip = 1; ip <= qt_np; ip++) {
+        long nm = index_sfincs_in_quadtree(ip);
+        if (nm > 0) zi[(size_t)nm - 1] = ip - 1;
+        auto face = [&](int32_t nb, const F1<int32_t>& zuv) {
+          if (nb > 0) {
+            npuvq++;
+            if (nm > 0 && zuv(nm) > 0) {
+              if (npuvs >= npuv) throw std::runtime_error("oracle: subgrid file faces do not match the mesh");
+              ui[(size_t)npuvs++] = npuvq - 1;
+            }
+          }
+        };
+        if (qt_mu(ip) < 1) {
+          face(qt_mu1(ip), z_index_uv_mu1);
+        } else {
+          face(qt_mu1(ip), z_index_uv_mu1);
+          face(qt_mu2(ip), z_index_uv_mu2);
+        }
+        if (qt_nu(ip) < 1) {
+          face(qt_nu1(ip), z_index_uv_nu1);
+        } else {
+          face(qt_nu1(ip), z_index_uv_nu1);
+          face(qt_nu2(ip), z_index_uv_nu2);
+        }
+      }
+      if ((long)zmin.size() != qt_np || (long)uzmin.size() != npuvq || npuvs != npuv)
+        throw std::runtime_error("oracle: subgrid file does not match the quadtree mesh");
+    } else {
+      if ((long)zmin.size() != np || (long)uzmin.size() != npuv)
+        throw std::runtime_error("oracle: subgrid file does not match the mesh");
+      for (long i = 0; i < np; i++) zi[(size_t)i] = i;
+      for (long i = 0; i < npuv; i++) ui[(size_t)i] = i;
+    }
     sg_z_zmin.alloc(np); sg_z_zmax.alloc(np); sg_z_volmax.alloc(np); sg_z_dep.alloc(L, np);
     sg_uv_zmin.alloc(npuv); sg_uv_zmax.alloc(npuv); sg_uv_navg_w.alloc(npuv); sg_uv_fnfit.alloc(npuv);
     sg_uv_havg.alloc(L, npuv); sg_uv_nrep.alloc(L, npuv); sg_uv_pwet.alloc(L, npuv);
     sg_uv_havg_zmax.alloc(npuv); sg_uv_nrep_zmax.alloc(npuv);
     for (long ip = 1; ip <= np; ip++) {
-      sg_z_zmin(ip) = zmin[ip - 1];
-      sg_z_zmax(ip) = zmax[ip - 1];
-      sg_z_volmax(ip) = volmax[ip - 1];
-      for (long k = 1; k <= L; k++) sg_z_dep(k, ip) = zlev[(ip - 1) * L + (k - 1)];
+      const long f = zi[(size_t)ip - 1];
+      sg_z_zmin(ip) = zmin[f];
+      sg_z_zmax(ip) = zmax[f];
+      sg_z_volmax(ip) = volmax[f];
+      for (long k = 1; k <= L; k++) sg_z_dep(k, ip) = zlev[f * L + (k - 1)];
     }
     for (long ip = 1; ip <= npuv; ip++) {
-      sg_uv_zmin(ip) = uzmin[ip - 1];
-      sg_uv_zmax(ip) = uzmax[ip - 1];
+      const long f = ui[(size_t)ip - 1];
+      sg_uv_zmin(ip) = uzmin[f];
+      sg_uv_zmax(ip) = uzmax[f];
       sg_uv_zmax(ip) = std::max(sg_uv_zmax(ip), sg_uv_zmin(ip) + 0.01f);
-      sg_uv_fnfit(ip) = uffit[ip - 1];
-      float nv = std::max(unavg[ip - 1], 0.0001f);
+      sg_uv_fnfit(ip) = uffit[f];
+      float nv = std::max(unavg[f], 0.0001f);
       sg_uv_navg_w(ip) = g * (nv * nv);
       for (long k = 1; k <= L; k++) {
-        sg_uv_havg(k, ip) = uhavg[(ip - 1) * L + (k - 1)];
-        float nr = std::max(unrep[(ip - 1) * L + (k - 1)], 0.0001f);
+        sg_uv_havg(k, ip) = uhavg[f * L + (k - 1)];
+        float nr = std::max(unrep[f * L + (k - 1)], 0.0001f);
         sg_uv_nrep(k, ip) = g * (nr * nr);
-        sg_uv_pwet(k, ip) = upwet[(ip - 1) * L + (k - 1)];
+        sg_uv_pwet(k, ip) = upwet[f * L + (k - 1)];
       }
     }
     for (long ip = 1; ip <= npuv; ip++) {  // :364-388
