@@ -2155,6 +2155,24 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "uv_nm") copy_out(m.uv_index_z_nm, out, n);
     else if (s == "uv_nmu") copy_out(m.uv_index_z_nmu, out, n);
     else if (s == "uv_dir") copy_out(m.uv_flags_dir, out, n);
+    else if (s == "uv_iref" && m.uv_flags_iref.allocated()) copy_out(m.uv_flags_iref, out, n);
+    else if (s == "uv_type" && m.uv_flags_type.allocated()) copy_out(m.uv_flags_type, out, n);
+    else if (s == "uv_u_nmd" && m.uv_index_u_nmd.allocated()) copy_out(m.uv_index_u_nmd, out, n);
+    else if (s == "uv_u_nmu" && m.uv_index_u_nmu.allocated()) copy_out(m.uv_index_u_nmu, out, n);
+    else if (s == "uv_u_ndm" && m.uv_index_u_ndm.allocated()) copy_out(m.uv_index_u_ndm, out, n);
+    else if (s == "uv_u_num" && m.uv_index_u_num.allocated()) copy_out(m.uv_index_u_num, out, n);
+    else if (s == "uv_v_ndm" && m.uv_index_v_ndm.allocated()) copy_out(m.uv_index_v_ndm, out, n);
+    else if (s == "uv_v_nm" && m.uv_index_v_nm.allocated()) copy_out(m.uv_index_v_nm, out, n);
+    else if (s == "uv_v_ndmu" && m.uv_index_v_ndmu.allocated()) copy_out(m.uv_index_v_ndmu, out, n);
+    else if (s == "uv_v_nmu" && m.uv_index_v_nmu.allocated()) copy_out(m.uv_index_v_nmu, out, n);
+    else if (s == "z_uv_md") copy_out(m.z_index_uv_md, out, n);
+    else if (s == "z_uv_mu") copy_out(m.z_index_uv_mu, out, n);
+    else if (s == "z_uv_nd") copy_out(m.z_index_uv_nd, out, n);
+    else if (s == "z_uv_nu") copy_out(m.z_index_uv_nu, out, n);
+    else if (s == "cuv_uv1" && m.ncuv > 0) copy_out(m.cuv_index_uv1, out, n);
+    else if (s == "cuv_uv2" && m.ncuv > 0) copy_out(m.cuv_index_uv2, out, n);
+    else if (s == "zbuvmx" && m.zbuvmx.allocated()) copy_out(m.zbuvmx, out, n);
+    else if (s == "gn2uv" && m.gn2uv.allocated()) copy_out(m.gn2uv, out, n);
     else if (s == "netprcp" && m.netprcp.allocated()) copy_out(m.netprcp, out, n);
     else if (s == "qext" && m.qext.allocated()) copy_out(m.qext, out, n);
     else if (s == "uvmean") copy_out(m.uvmean, out, n);

@@ -47,7 +47,7 @@ __global__ void k_scatter_f64_f32(const double* __restrict__ in, const int32_t* 
     dst[cmp[i]] = (float)in[i];
 }
 
-// Volume of kcs==1 cells: subgrid sum(z_volume), regular sum((zs - zb) * area).
+// Volume of kcs==1 cells: subgrid sum(z_volume), regular sum((zs - zb) * cell area).
 // Pass 1 writes one FP64 partial per CTA; pass 2 sums the partials in index
 // order, so the result does not depend on scheduling.
 __global__ void k_volume_partial(const ScnDev* __restrict__ scn, const int32_t* __restrict__ cmp, long long n,
@@ -57,7 +57,8 @@ __global__ void k_volume_partial(const ScnDev* __restrict__ scn, const int32_t* 
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int32_t c = cmp[i];
     if (!(S.flags[c] & F_KCS1)) continue;
-    acc += S.subgrid ? S.zvol[c] : ((double)S.zs[c] - (double)S.zb[c]) * (double)S.area;
+    const float area = S.quadtree ? S.lv_area[S.qlev[c]] : S.area;
+    acc += S.subgrid ? S.zvol[c] : ((double)S.zs[c] - (double)S.zb[c]) * (double)area;
   }
   __shared__ double s[32];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);

@@ -107,7 +107,7 @@ struct ModelHandle {
                     (double)h.p.ngbnd,
                     (double)h.p.subgrid,
                     st.bflux_vol,
-                    st.rain_vol * (double)h.n_kcs1,
+                    st.rain_vol * h.area_total_kcs1,
                     st.src_vol,
                     h.p.dtmax,
                     h.p.dtmin,
@@ -132,9 +132,9 @@ struct ModelHandle {
     auto need = [&](size_t b) {
       if (bytes != b) throw std::runtime_error("get_var('" + name + "'): expected " + std::to_string(b) + " bytes");
     };
-    auto f32 = [&](const float* src) {
+    auto f32 = [&](const float* src, const int32_t* map = nullptr) {
       need((size_t)n * 4);
-      launch_gather_f32(src, dev->d_cmp_off(), (float*)d_stage, n, s());
+      launch_gather_f32(src, map ? map : dev->d_cmp_off(), (float*)d_stage, n, s());
       check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 4, cudaMemcpyDeviceToHost, s()), "get");
     };
     if (name == "zs") {
@@ -152,18 +152,19 @@ struct ModelHandle {
       launch_gather_f64(D.zvol, dev->d_cmp_off(), (double*)d_stage, n, s());
       check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 8, cudaMemcpyDeviceToHost, s()), "get");
     } else if (name == "qx") {
-      f32(D.qu[p]);
+      f32(D.qu[p], dev->face_map(0));
     } else if (name == "qy") {
-      f32(D.qv[p]);
+      f32(D.qv[p], dev->face_map(1));
     } else if (name == "uvx") {
-      f32(D.uu[p]);
+      f32(D.uu[p], dev->face_map(0));
     } else if (name == "uvy") {
-      f32(D.vv[p]);
+      f32(D.vv[p], dev->face_map(1));
     } else if (name == "zs0" && D.zs0) {
       f32(D.zs0);
     } else if (name == "zsderv" && D.zsderv) {
       f32(D.zsderv);
     } else if (name == "kfuv") {
+      if (D.quadtree) throw std::runtime_error("kfuv is not available per cell on quadtree meshes");
       need((size_t)n * 8);
       launch_gather_u8(D.kf[0], D.kf[1], dev->d_cmp_off(), (float*)d_stage, n, s());
       check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 8, cudaMemcpyDeviceToHost, s()), "get");
@@ -178,6 +179,8 @@ struct ModelHandle {
     ScnDev& D = dev->dev();
     StepState st = runner->read_state(0);
     const int p = latest(st);
+    if (D.quadtree && name != "zs" && name != "qext")
+      throw std::runtime_error("set_var('" + name + "') is not available on quadtree meshes");
     auto put32 = [&](float* dstp) {
       if (bytes != (size_t)n * 4) throw std::runtime_error("set_var('" + name + "'): wrong size");
       check_cuda(cudaMemcpyAsync(d_stage, src, bytes, cudaMemcpyHostToDevice, s()), "set");
@@ -214,6 +217,7 @@ struct ModelHandle {
   // find_quadtree_cell on a single-level grid (sfincs_quadtree.F90:764-820)
   int cell_index(double xd, double yd) const {
     const HostModel& h = *host;
+    if (h.p.quadtree) return quadtree_cell_index(h, xd, yd);
     const float x = (float)xd, y = (float)yd;
     const float xt = h.cosrot * (x - h.x0) + h.sinrot * (y - h.y0);
     const float yt = -h.sinrot * (x - h.x0) + h.cosrot * (y - h.y0);
@@ -226,6 +230,7 @@ struct ModelHandle {
   void update_zbuv() {
     HostModel& h = *host;
     if (h.p.subgrid) return;  // zbuvmx exists only for regular bathymetry
+    if (h.p.quadtree) throw std::runtime_error("update_zbuv is not available on quadtree meshes");
     for (long long i = 0; i < h.np; i++) h.zb[h.cmp_off[i]] = h.zb_cmp[i];
     const int ld = h.p.ld;
     for (int m = 1; m <= h.p.mmax; m++)
@@ -695,7 +700,7 @@ int sfg_ensemble_scalars(void* ev, int i, double out[19]) {
     double t = st.stop_pending ? h.t1 + 1.0 : st.t;
     double v[19] = {t, st.dt, st.min_dt, (double)st.nt, (double)st.error, h.t0, h.t1, (double)h.np, (double)h.npuv,
                     (double)h.p.nkcuv2, (double)h.p.ngbnd, (double)h.p.subgrid, st.bflux_vol,
-                    st.rain_vol * (double)h.n_kcs1, st.src_vol, h.p.dtmax, h.p.dtmin, (double)e->devs[i]->bytes(),
+                    st.rain_vol * h.area_total_kcs1, st.src_vol, h.p.dtmax, h.p.dtmin, (double)e->devs[i]->bytes(),
                     (double)e->runner->ntiles()};
     std::memcpy(out, v, sizeof(v));
     return 0;
@@ -720,14 +725,15 @@ int sfg_ensemble_get(void* ev, int i, const char* name, void* dst, size_t bytes)
       sfg::launch_gather_f64(d.dev().zvol, d.d_cmp_off(), (double*)e->d_stage, n, s);
     } else {
       const float* src = nullptr;
+      const int32_t* map = d.d_cmp_off();
       if (nm == "zsmax") src = d.dev().zsmax;
-      else if (nm == "qx") src = d.dev().qu[p];
-      else if (nm == "qy") src = d.dev().qv[p];
-      else if (nm == "uvx") src = d.dev().uu[p];
-      else if (nm == "uvy") src = d.dev().vv[p];
+      else if (nm == "qx") src = d.dev().qu[p], map = d.face_map(0);
+      else if (nm == "qy") src = d.dev().qv[p], map = d.face_map(1);
+      else if (nm == "uvx") src = d.dev().uu[p], map = d.face_map(0);
+      else if (nm == "uvy") src = d.dev().vv[p], map = d.face_map(1);
       else throw std::runtime_error("unknown ensemble variable " + nm);
       if (bytes != (size_t)n * 4) throw std::runtime_error("wrong size for " + nm);
-      sfg::launch_gather_f32(src, d.d_cmp_off(), (float*)e->d_stage, n, s);
+      sfg::launch_gather_f32(src, map, (float*)e->d_stage, n, s);
     }
     sfg::check_cuda(cudaMemcpyAsync(dst, e->d_stage, bytes, cudaMemcpyDeviceToHost, s), "get");
     e->runner->sync();
@@ -785,7 +791,47 @@ int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst
     } else if (nm == "gb_cell") {
       for (auto c : h.gb_cmp) out.push_back((double)c);
     } else if (nm == "kb_cell") {
-      for (auto& b : h.bfaces) out.push_back((double)h.dense2cmp[b.face]);
+      for (auto& b : h.bfaces)
+        out.push_back(h.p.quadtree ? (double)h.qface[b.face].nm : (double)h.dense2cmp[b.face]);
+    } else if (h.p.quadtree && nm == "qt_counts") {
+      out = {(double)h.np, (double)h.npuv, (double)h.p.ncuv, (double)h.p.nref};
+    } else if (h.p.quadtree && nm.compare(0, 3, "uv_") == 0) {
+      // uv-point arrays, 1-based indices as in the reference
+      for (auto& f : h.qface) {
+        double v;
+        if (nm == "uv_nm") v = f.nm + 1;
+        else if (nm == "uv_nmu") v = f.nmu + 1;
+        else if (nm == "uv_dir") v = (f.info & sfg::QF_DIR) ? 1 : 0;
+        else if (nm == "uv_iref") v = (double)(((f.info >> 8) & 15u) + 1);
+        else if (nm == "uv_trans") v = (f.info & sfg::QF_TRANS) ? 1 : 0;
+        else if (nm == "uv_act") v = (f.info & sfg::QF_ACT) ? 1 : 0;
+        else if (nm == "uv_adv") v = (f.info & sfg::QF_ADV) ? 1 : 0;
+        else if (nm == "uv_th") v = (f.info & sfg::QF_TH) ? 1 : 0;
+        else if (nm == "uv_u_nmd") v = f.u_nmd + 1;
+        else if (nm == "uv_u_nmu") v = f.u_nmu + 1;
+        else if (nm == "uv_u_ndm") v = f.u_ndm + 1;
+        else if (nm == "uv_u_num") v = f.u_num + 1;
+        else if (nm == "uv_v_ndm") v = f.v_ndm + 1;
+        else if (nm == "uv_v_nm") v = f.v_nm + 1;
+        else if (nm == "uv_v_ndmu") v = f.v_ndmu + 1;
+        else if (nm == "uv_v_nmu") v = f.v_nmu + 1;
+        else return -1;
+        out.push_back(v);
+      }
+    } else if (h.p.quadtree && nm.compare(0, 5, "z_uv_") == 0) {
+      for (auto& c : h.qcell) {
+        if (nm == "z_uv_md") out.push_back(c.x + 1);
+        else if (nm == "z_uv_mu") out.push_back(c.y + 1);
+        else if (nm == "z_uv_nd") out.push_back(c.z + 1);
+        else if (nm == "z_uv_nu") out.push_back(c.w + 1);
+        else return -1;
+      }
+    } else if (h.p.quadtree && (nm == "cuv_uv1" || nm == "cuv_uv2")) {
+      for (auto& c : h.qcuv) out.push_back((nm == "cuv_uv1" ? c.x : c.y) + 1);
+    } else if (h.p.quadtree && (nm == "zbuvmx" || nm == "gn2uv")) {
+      const auto& v = nm == "zbuvmx" ? h.zbmx_q : h.gn2_q;
+      if (v.empty()) return -1;
+      out.assign(v.begin(), v.end());
     } else if (nm == "kb_dir") {
       for (auto& b : h.bfaces) out.push_back((double)(b.info & 1));
     } else if (nm == "kb_sign") {

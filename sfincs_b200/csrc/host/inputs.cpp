@@ -144,15 +144,17 @@ NcFile::NcFile(const std::string& path) : path_(path) {
     dimlen.push_back(c.u32());
     dims_[n] = dimlen.back();
   }
-  auto skip_attrs = [&]() {
+  auto skip_attrs = [&](std::map<std::string, double>* keep) {
     uint32_t t = c.u32(), k = c.u32();
     for (uint32_t i = 0; i < (t ? k : 0); i++) {
-      c.name();
+      std::string an = c.name();
       uint32_t ty = c.u32(), ne = c.u32();
+      if (ty < 1 || ty > 6) throw std::runtime_error("bad netCDF attribute type in " + path_);
+      if (keep && ty != 2 && ne > 0) (*keep)[an] = value_of((int)ty, &c.b[c.p]);
       c.p += ((size_t)ne * kTypeSize[ty] + 3) & ~(size_t)3;
     }
   };
-  skip_attrs();
+  skip_attrs(&gatts_);
   tag = c.u32();
   cnt = c.u32();
   for (uint32_t i = 0; i < (tag ? cnt : 0); i++) {
@@ -160,7 +162,7 @@ NcFile::NcFile(const std::string& path) : path_(path) {
     uint32_t nd = c.u32();
     uint64_t count = 1;
     for (uint32_t d = 0; d < nd; d++) count *= (uint64_t)dimlen.at(c.u32());
-    skip_attrs();
+    skip_attrs(nullptr);
     Var v;
     v.type = (int)c.u32();
     c.u32();
@@ -176,7 +178,18 @@ long long NcFile::dim(const std::string& n) const {
   return it->second;
 }
 
+double NcFile::att(const std::string& n) const {
+  auto it = gatts_.find(n);
+  if (it == gatts_.end()) throw std::runtime_error("netCDF global attribute '" + n + "' missing in " + path_);
+  return it->second;
+}
+
 std::vector<float> NcFile::floats(const std::string& n) const {
+  auto d = doubles(n);
+  return std::vector<float>(d.begin(), d.end());
+}
+
+std::vector<double> NcFile::doubles(const std::string& n) const {
   auto it = vars_.find(n);
   if (it == vars_.end()) throw std::runtime_error("netCDF variable '" + n + "' missing in " + path_);
   const Var& v = it->second;
@@ -187,20 +200,24 @@ std::vector<float> NcFile::floats(const std::string& n) const {
   f.seekg((std::streamoff)v.begin);
   f.read(reinterpret_cast<char*>(raw.data()), (std::streamsize)raw.size());
   if ((size_t)f.gcount() != raw.size()) throw std::runtime_error("short read of netCDF variable " + n);
-  std::vector<float> out((size_t)v.count);
-  for (size_t i = 0; i < out.size(); i++) {
-    const uint8_t* p = &raw[i * sz];
-    uint64_t be = 0;
-    for (int k = 0; k < sz; k++) be = be << 8 | p[k];
-    switch (v.type) {
-      case 1: out[i] = (float)(int8_t)be; break;
-      case 3: out[i] = (float)(int16_t)be; break;
-      case 4: out[i] = (float)(int32_t)be; break;
-      case 5: { uint32_t u = (uint32_t)be; float x; std::memcpy(&x, &u, 4); out[i] = x; break; }
-      case 6: { double x; std::memcpy(&x, &be, 8); out[i] = (float)x; break; }
-    }
-  }
+  std::vector<double> out((size_t)v.count);
+  for (size_t i = 0; i < out.size(); i++) out[i] = value_of(v.type, &raw[i * sz]);
   return out;
+}
+
+// One big-endian value of netCDF type t (byte, short, int, float, double).
+double NcFile::value_of(int t, const uint8_t* p) {
+  const int sz = kTypeSize[t];
+  uint64_t be = 0;
+  for (int k = 0; k < sz; k++) be = be << 8 | p[k];
+  switch (t) {
+    case 1: return (double)(int8_t)be;
+    case 3: return (double)(int16_t)be;
+    case 4: return (double)(int32_t)be;
+    case 5: { uint32_t u = (uint32_t)be; float x; std::memcpy(&x, &u, 4); return (double)x; }
+    case 6: { double x; std::memcpy(&x, &be, 8); return x; }
+  }
+  throw std::runtime_error("unsupported netCDF type");
 }
 
 }  // namespace sfg

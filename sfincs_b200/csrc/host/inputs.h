@@ -38,7 +38,10 @@ class NcFile {
  public:
   explicit NcFile(const std::string& path);
   long long dim(const std::string& name) const;
+  bool has(const std::string& name) const { return vars_.count(name) != 0; }
   std::vector<float> floats(const std::string& name) const;
+  std::vector<double> doubles(const std::string& name) const;
+  double att(const std::string& name) const;  // numeric global attribute (first value)
 
  private:
   struct Var {
@@ -48,6 +51,8 @@ class NcFile {
   std::string path_;
   std::map<std::string, long long> dims_;
   std::map<std::string, Var> vars_;
+  std::map<std::string, double> gatts_;
+  static double value_of(int type, const uint8_t* p);
 };
 
 }  // namespace sfg

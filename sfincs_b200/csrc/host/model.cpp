@@ -23,13 +23,100 @@ static bool is_none(const std::string& s) { return s.size() >= 4 && s.compare(0,
 // ============================================================================
 // load_model
 // ============================================================================
-std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
-  auto H = std::make_unique<HostModel>();
-  HostModel& h = *H;
+// Water-level boundary points and their time series (sfincs_boundaries.f90:8-213).
+void read_boundary_series(HostModel& h, const Keys& k, bool water_level_bnd, std::vector<float>& xb,
+                          std::vector<float>& yb, int& nbnd) {
   ScnDev& P = h.p;
-  h.dir = dir;
-  auto path = [&](const std::string& f) { return dir + "/" + f; };
-  InpFile in(path("sfincs.inp"));
+  auto path = [&](const std::string& f) { return h.dir + "/" + f; };
+  int ntbnd = 0;
+  nbnd = 0;
+  if (!is_none(k.bndfile)) {
+    auto xy = read_table(path(k.bndfile));
+    nbnd = (int)xy.size();
+    for (auto& r : xy) {
+      xb.push_back((float)r.at(0));
+      yb.push_back((float)r.at(1));
+    }
+    if (!is_none(k.bzsfile)) {
+      auto tb = read_table(path(k.bzsfile));
+      ntbnd = (int)tb.size();
+      h.zs_bnd.assign((size_t)ntbnd * nbnd, 0.0f);
+      for (int it = 0; it < ntbnd; it++) {
+        if ((int)tb[it].size() < nbnd + 1) throw std::runtime_error("bzs file has fewer columns than bnd points");
+        h.t_bnd.push_back((float)tb[it][0]);
+        for (int ib = 0; ib < nbnd; ib++) h.zs_bnd[(size_t)it * nbnd + ib] = (float)tb[it][ib + 1];
+      }
+    } else {
+      ntbnd = 2;
+      h.t_bnd = {k.t0, k.t1};
+      h.zs_bnd.assign((size_t)2 * nbnd, 0.0f);
+    }
+    if (ntbnd < 1) throw std::runtime_error("empty boundary time series");
+    if (h.t_bnd[0] > (k.t0 + 1.0f) || h.t_bnd[ntbnd - 1] < (k.t1 - 1.0f)) {
+      if (h.t_bnd[0] > (k.t0 + 1.0f))
+        h.t_bnd[0] = k.t0 - 1.0f;
+      else
+        h.t_bnd[ntbnd - 1] = k.t1 + 1.0f;
+    }
+  } else if (water_level_bnd) {
+    nbnd = 1;
+    xb = {0.0f};
+    yb = {0.0f};
+    ntbnd = 2;
+    h.t_bnd = {k.t0, k.t1};
+    h.zs_bnd = {0.0f, 0.0f};
+  }
+  P.nbnd = nbnd;
+  P.ntbnd = ntbnd;
+}
+
+// Uniform wind and rain time series and the wind drag table (sfincs_meteo.f90:247-327).
+void read_meteo_series(HostModel& h, const Keys& k, float rotation) {
+  ScnDev& P = h.p;
+  auto path = [&](const std::string& f) { return h.dir + "/" + f; };
+  if (P.wind) {
+    auto tb = read_table(path(k.wndfile));
+    for (auto& r : tb) {
+      h.twnd.push_back((float)r.at(0));
+      h.wmag.push_back((float)r.at(1));
+      h.wdir.push_back(P.pi * (270.0f - (float)r.at(2)) / 180.0f - rotation);
+    }
+    P.ntwnd = (int)h.twnd.size();
+    if (P.ntwnd < 2) throw std::runtime_error("wind time series needs at least two records");
+  }
+  if (P.precip) {
+    auto tb = read_table(path(k.prcpfile));
+    for (auto& r : tb) {
+      h.tprcp.push_back((float)r.at(0));
+      h.vprcp.push_back((float)r.at(1));
+    }
+    P.ntprcp = (int)h.tprcp.size();
+    if (P.ntprcp < 1) throw std::runtime_error("empty precipitation time series");
+  }
+  {
+    const float cd_wnd[3] = {0.0f, 28.0f, 50.0f}, cd_val[3] = {0.0010f, 0.0025f, 0.0015f};
+    h.cdval.assign(1000, 0.0f);
+    for (int iw = 1; iw <= 1000; iw++) {
+      const float wnd = (float)iw * 0.1f;
+      for (int icd = 1; icd <= 2; icd++) {
+        h.cdval[iw - 1] = cd_val[icd - 1];
+        if (wnd >= cd_wnd[icd - 1] && wnd < cd_wnd[icd]) {
+          h.cdval[iw - 1] = cd_val[icd - 1] + (wnd - cd_wnd[icd - 1]) * (cd_val[icd] - cd_val[icd - 1]) /
+                                                  (cd_wnd[icd] - cd_wnd[icd - 1]);
+          break;
+        } else if (wnd >= cd_wnd[2]) {
+          h.cdval[iw - 1] = cd_val[2];
+          break;
+        }
+      }
+    }
+  }
+}
+
+// Keywords of sfincs.inp with the reference's defaults and the values derived
+// from them (sfincs_input.f90:50-745); scalar switches go straight into h.p.
+Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
+  ScnDev& P = h.p;
 
   // ---- keywords and defaults (sfincs_input.f90:50-343) ----------------------
   const int mmax = in.integer("mmax", 0), nmax = in.integer("nmax", 0);
@@ -94,12 +181,12 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   for (const char* k : {"snapwave", "nonh", "bathtub", "vegetation"})
     if (in.logical(k, false) || in.integer(k, 0) != 0)
       throw std::runtime_error(std::string("process '") + k + "' is not supported by this core");
-  if (!is_none(qtrfile)) throw std::runtime_error("quadtree meshes (qtrfile) are not supported by this core yet");
   if (!is_none(inifile) || !is_none(rstfile)) throw std::runtime_error("inifile/rstfile are not supported by this core yet");
   if (igeo != 0) throw std::runtime_error("geographic grids (crsgeo=1) are not supported by this core");
   if (inputtype != "bin") throw std::runtime_error("only inputformat = bin is supported");
   if (bndtype != 1) throw std::runtime_error("only bndtype = 1 is supported");
-  if (nmax <= 0 || mmax <= 0) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
+  const bool quadtree = !is_none(qtrfile);
+  if (!quadtree && (nmax <= 0 || mmax <= 0)) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
 
   // ---- derived (sfincs_input.f90:347-745) ------------------------------------
   if (is_none(tref)) tref = tstart;
@@ -135,6 +222,40 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   h.t0 = t0;
   h.t1 = t1;
   if (P.subgrid) P.huthresh = 0.0f;  // sfincs_subgrid.F90:40 (netCDF tables)
+  Keys k;
+  k.mmax = mmax; k.nmax = nmax; k.dx = dx; k.dy = dy; k.x0 = x0; k.y0 = y0; k.rotation = rotation;
+  k.cosrot = cosrot; k.sinrot = sinrot; k.t0 = t0; k.t1 = t1; k.hmin_cfl = hmin_cfl; k.dtmax = dtmax;
+  k.uvmax = uvmax; k.nuviscdim = nuviscdim; k.viscosity = viscosity; k.manning = manning;
+  k.manning_land = manning_land; k.manning_sea = manning_sea; k.rghlevland = rghlevland; k.qinf = qinf;
+  k.qinf_zmin = qinf_zmin; k.advection_mask = advection_mask; k.qtrfile = qtrfile; k.depfile = depfile;
+  k.mskfile = mskfile; k.indexfile = indexfile; k.sbgfile = sbgfile; k.manningfile = manningfile;
+  k.bndfile = bndfile; k.bzsfile = bzsfile; k.srcfile = srcfile; k.disfile = disfile; k.wndfile = wndfile;
+  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree;
+  return k;
+}
+
+std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
+  auto H = std::make_unique<HostModel>();
+  HostModel& h = *H;
+  ScnDev& P = h.p;
+  h.dir = dir;
+  auto path = [&](const std::string& f) { return dir + "/" + f; };
+  InpFile in(path("sfincs.inp"));
+  const Keys K = parse_keys(in, h, bmi);
+  if (K.quadtree) {
+    load_quadtree(h, K);
+    return H;
+  }
+  const int mmax = K.mmax, nmax = K.nmax;
+  const float dx = K.dx, dy = K.dy, x0 = K.x0, y0 = K.y0, rotation = K.rotation, cosrot = K.cosrot,
+              sinrot = K.sinrot, t0 = K.t0, t1 = K.t1, hmin_cfl = K.hmin_cfl, dtmax = K.dtmax, uvmax = K.uvmax,
+              nuviscdim = K.nuviscdim, manning = K.manning, manning_land = K.manning_land,
+              manning_sea = K.manning_sea, rghlevland = K.rghlevland, qinf = K.qinf, qinf_zmin = K.qinf_zmin;
+  const bool viscosity = K.viscosity, advection_mask = K.advection_mask;
+  const std::string &depfile = K.depfile, &mskfile = K.mskfile, &indexfile = K.indexfile, &sbgfile = K.sbgfile,
+                    &manningfile = K.manningfile, &bndfile = K.bndfile, &bzsfile = K.bzsfile,
+                    &srcfile = K.srcfile, &disfile = K.disfile, &wndfile = K.wndfile, &qinffile = K.qinffile,
+                    &prcpfile = K.prcpfile;
 
   // ---- mesh: index + mask files (sfincs_domain.f90:250-482) -------------------
   const long long n_idx = read_binary<int32_t>(path(indexfile), 1)[0];
@@ -362,46 +483,9 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   }
 
   // ---- boundary conditions files (sfincs_boundaries.f90:8-213) ----------------------
-  int nbnd = 0, ntbnd = 0;
+  int nbnd = 0;
   std::vector<float> xb, yb;
-  if (!is_none(bndfile)) {
-    auto xy = read_table(path(bndfile));
-    nbnd = (int)xy.size();
-    for (auto& r : xy) {
-      xb.push_back((float)r.at(0));
-      yb.push_back((float)r.at(1));
-    }
-    if (!is_none(bzsfile)) {
-      auto tb = read_table(path(bzsfile));
-      ntbnd = (int)tb.size();
-      h.zs_bnd.assign((size_t)ntbnd * nbnd, 0.0f);
-      for (int it = 0; it < ntbnd; it++) {
-        if ((int)tb[it].size() < nbnd + 1) throw std::runtime_error("bzs file has fewer columns than bnd points");
-        h.t_bnd.push_back((float)tb[it][0]);
-        for (int ib = 0; ib < nbnd; ib++) h.zs_bnd[(size_t)it * nbnd + ib] = (float)tb[it][ib + 1];
-      }
-    } else {
-      ntbnd = 2;
-      h.t_bnd = {t0, t1};
-      h.zs_bnd.assign((size_t)2 * nbnd, 0.0f);
-    }
-    if (ntbnd < 1) throw std::runtime_error("empty boundary time series");
-    if (h.t_bnd[0] > (t0 + 1.0f) || h.t_bnd[ntbnd - 1] < (t1 - 1.0f)) {
-      if (h.t_bnd[0] > (t0 + 1.0f))
-        h.t_bnd[0] = t0 - 1.0f;
-      else
-        h.t_bnd[ntbnd - 1] = t1 + 1.0f;
-    }
-  } else if (water_level_bnd) {
-    nbnd = 1;
-    xb = {0.0f};
-    yb = {0.0f};
-    ntbnd = 2;
-    h.t_bnd = {t0, t1};
-    h.zs_bnd = {0.0f, 0.0f};
-  }
-  P.nbnd = nbnd;
-  P.ntbnd = ntbnd;
+  read_boundary_series(h, K, water_level_bnd, xb, yb, nbnd);
 
   // ---- find_boundary_indices (sfincs_boundaries.f90:455-679) -------------------------
   if (ngb > 0 && nbnd > 0) {
@@ -462,6 +546,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     b.zbuv = P.subgrid ? 0.0f : 0.5f * (h.zb[e.face] + h.zb[e.dir == 0 ? e.face + ld : e.face + 1]);
     b.floor = P.subgrid ? h.zz_min[e.nmb] : h.zb[e.nmb];
     b.zfix = gb_zfix[ib];
+    b.len = e.dir == 1 ? dx : dy;
     if (kcs[e.nmb] == 2 && nbnd == 0) b.info |= 4, b.zfix = 0.0f;  // no boundary data: zsb stays 0
     h.bfaces.push_back(b);
   }
@@ -599,43 +684,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   }
 
   // ---- meteo time series and Cd table (sfincs_meteo.f90:247-327) ------------------------------
-  if (P.wind) {
-    auto tb = read_table(path(wndfile));
-    for (auto& r : tb) {
-      h.twnd.push_back((float)r.at(0));
-      h.wmag.push_back((float)r.at(1));
-      h.wdir.push_back(P.pi * (270.0f - (float)r.at(2)) / 180.0f - rotation);
-    }
-    P.ntwnd = (int)h.twnd.size();
-    if (P.ntwnd < 2) throw std::runtime_error("wind time series needs at least two records");
-  }
-  if (P.precip) {
-    auto tb = read_table(path(prcpfile));
-    for (auto& r : tb) {
-      h.tprcp.push_back((float)r.at(0));
-      h.vprcp.push_back((float)r.at(1));
-    }
-    P.ntprcp = (int)h.tprcp.size();
-    if (P.ntprcp < 1) throw std::runtime_error("empty precipitation time series");
-  }
-  {
-    const float cd_wnd[3] = {0.0f, 28.0f, 50.0f}, cd_val[3] = {0.0010f, 0.0025f, 0.0015f};
-    h.cdval.assign(1000, 0.0f);
-    for (int iw = 1; iw <= 1000; iw++) {
-      const float wnd = (float)iw * 0.1f;
-      for (int icd = 1; icd <= 2; icd++) {
-        h.cdval[iw - 1] = cd_val[icd - 1];
-        if (wnd >= cd_wnd[icd - 1] && wnd < cd_wnd[icd]) {
-          h.cdval[iw - 1] = cd_val[icd - 1] + (wnd - cd_wnd[icd - 1]) * (cd_val[icd] - cd_val[icd - 1]) /
-                                                  (cd_wnd[icd] - cd_wnd[icd - 1]);
-          break;
-        } else if (wnd >= cd_wnd[2]) {
-          h.cdval[iw - 1] = cd_val[2];
-          break;
-        }
-      }
-    }
-  }
+  read_meteo_series(h, K, rotation);
 
   // ---- point sources (sfincs_discharges.f90:8-324) ------------------------------------------------
   if (!is_none(srcfile)) {
@@ -697,7 +746,8 @@ struct Placer {
 }  // namespace
 
 template <class F>
-static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, Placer& pl, F&& fill) {
+static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& qmu, int32_t*& qmv, Placer& pl,
+                        F&& fill) {
   const size_t NA = (size_t)h.p.nalloc;
   auto up = [&](auto& dst, const auto& v) {
     using X = typename std::decay_t<decltype(v)>::value_type;
@@ -711,6 +761,60 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, Placer& pl
     if (q) fill(q, nullptr, n * sizeof(X));
     dst = q;
   };
+  if (h.p.quadtree) {
+    // compact cells (npc), uv points (npuv) and q/uv arrays (npuv + ncuv + dummy)
+    const size_t NC = (size_t)h.np, NF = (size_t)h.npuv, NQ = (size_t)(h.npuv + h.p.ncuv + 1);
+    up(d.zs, h.zs);
+    up(d.zsmax, h.zsmax);
+    up(d.zvol, h.zvol);
+    if (h.p.wiggle) {
+      up(d.zs0, h.zs0);
+      zero(d.zsderv, NC);
+    } else {
+      d.zs0 = nullptr;
+      d.zsderv = nullptr;
+    }
+    zero(d.kf[0], NF);
+    d.kf[1] = d.kf[0];
+    if (h.p.subgrid) up(d.vneg, h.vneg);
+    else d.vneg = nullptr;
+    for (int b = 0; b < 2; b++) {
+      zero(d.qu[b], NQ);
+      zero(d.uu[b], NQ);
+      d.qv[b] = d.qu[b];
+      d.vv[b] = d.uu[b];
+    }
+    up(d.flags, h.flags);
+    up(d.zb, h.zb);
+    d.zbmx_u = d.zbmx_v = d.gn2_u = d.gn2_v = nullptr;
+    up(d.zbmx, h.zbmx_q);
+    up(d.gn2, h.gn2_q);
+    up(d.sgz_u, h.sgz_u);
+    d.sgz_v = d.sgz_u;
+    up(d.sgw_u, h.sgw_u);
+    d.sgw_v = d.sgw_u;
+    up(d.rec_u, h.rec_u);
+    d.rec_v = d.rec_u;
+    up(d.zz_min, h.zz_min);
+    up(d.zz_max, h.zz_max);
+    up(d.zz_volmax, h.zz_volmax);
+    up(d.zlev, h.zlev);
+    if (h.p.use_qext) zero(d.qext, NC);
+    else d.qext = nullptr;
+    up(d.qinf, h.qinf);
+    up(d.qface, h.qface);
+    up(d.qcell, h.qcell);
+    up(d.qcuv, h.qcuv);
+    up(d.qlev, h.qlev);
+    up(qmu, h.qmap_u);
+    up(qmv, h.qmap_v);
+  } else {
+    d.qface = nullptr;
+    d.qcell = nullptr;
+    d.qcuv = nullptr;
+    d.qlev = nullptr;
+    d.zbmx = d.gn2 = nullptr;
+    qmu = qmv = nullptr;
   up(d.zs, h.zs);
   up(d.zsmax, h.zsmax);
   up(d.zvol, h.zvol);
@@ -750,6 +854,7 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, Placer& pl
   if (h.p.use_qext) zero(d.qext, NA);
   else d.qext = nullptr;
   up(d.qinf, h.qinf);
+  }
   up(d.t_bnd, h.t_bnd);
   up(d.zs_bnd, h.zs_bnd);
   zero(d.zst_bnd, (size_t)std::max(h.p.nbnd, 1));
@@ -772,9 +877,9 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, Placer& pl
 
 size_t device_bytes_needed(const HostModel& h) {
   ScnDev d = h.p;
-  int32_t* cmp = nullptr;
+  int32_t *cmp = nullptr, *qmu = nullptr, *qmv = nullptr;
   Placer pl;
-  place_model(h, d, cmp, pl, [](void*, const void*, size_t) {});
+  place_model(h, d, cmp, qmu, qmv, pl, [](void*, const void*, size_t) {});
   return (pl.off + 255) & ~(size_t)255;
 }
 
@@ -785,7 +890,7 @@ DeviceModel::DeviceModel(const HostModel& h) : h_(&h) {
   try {
     Placer pl;
     pl.base = static_cast<char*>(block_);
-    place_model(h, d_, d_cmp_, pl, [](void* dst, const void* src, size_t n) {
+    place_model(h, d_, d_cmp_, d_qmap_u_, d_qmap_v_, pl, [](void* dst, const void* src, size_t n) {
       if (src)
         check_cuda(cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice), "upload");
       else
@@ -820,15 +925,33 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
   if (models_.empty()) throw std::runtime_error("Runner needs at least one model");
   if (tile_m != 8) throw std::runtime_error("only 32x8 cell tiles are built into this library");
   subgrid_ = models_[0]->host().p.subgrid;
+  qt_ = models_[0]->host().p.quadtree;
   std::vector<ScnDev> scns;
   std::vector<Tile> tiles;
   for (size_t i = 0; i < models_.size(); i++) {
     const HostModel& h = models_[i]->host();
     if (h.p.subgrid != subgrid_) throw std::runtime_error("an ensemble must be all-subgrid or all-regular");
+    if (h.p.quadtree != qt_) throw std::runtime_error("an ensemble must be all-quadtree or all-regular-grid");
     if (h.p.nsrc > 0) any_src_ = 1;
     bnd_blocks_ = std::max(bnd_blocks_, (h.p.nkcuv2 + h.p.nneu + 127) / 128);
     scns.push_back(models_[i]->dev());
-    for (const int2& t : h.tiles) tiles.push_back(Tile{(int)i, t.x, t.y, 0});
+    if (!qt_)
+      for (const int2& t : h.tiles) tiles.push_back(Tile{(int)i, t.x, t.y, 0});
+  }
+  if (qt_) {
+    // quadtree work lists: 256-wide chunks of uv points, combined points and cells
+    auto chunks = [&](auto count_of) {
+      int n = 0;
+      for (size_t i = 0; i < models_.size(); i++) {
+        const long long cnt = count_of(models_[i]->host());
+        for (long long f0 = 0; f0 < cnt; f0 += 256, n++)
+          tiles.push_back(Tile{(int)i, (int)f0, (int)std::min<long long>(256, cnt - f0), 0});
+      }
+      return n;
+    };
+    nqf_ = chunks([](const HostModel& h) { return h.npuv; });
+    nqcuv_ = chunks([](const HostModel& h) { return (long long)h.p.ncuv; });
+    nqc_ = chunks([](const HostModel& h) { return h.np; });
   }
   ntiles_ = (int)tiles.size();
   check_cuda(cudaMalloc(&d_scns_, scns.size() * sizeof(ScnDev)), "cudaMalloc scns");
@@ -842,18 +965,21 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
     const int x = std::atoi(v);
     variant_ = (x >= 2 && x <= 5) ? x : 5;
   }
-  // TMA tensor maps (one set per model) and persistent grid sizes
-  std::vector<MapSet> maps;
-  for (auto* m : models_) maps.push_back(build_map_set(m->dev()));
-  check_cuda(cudaMalloc(&d_maps_, maps.size() * sizeof(MapSet)), "cudaMalloc maps");
-  check_cuda(cudaMemcpy(d_maps_, maps.data(), maps.size() * sizeof(MapSet), cudaMemcpyHostToDevice), "maps");
-  configure_grids();
+  if (!qt_) {
+    // TMA tensor maps (one set per model) and persistent grid sizes
+    std::vector<MapSet> maps;
+    for (auto* m : models_) maps.push_back(build_map_set(m->dev()));
+    check_cuda(cudaMalloc(&d_maps_, maps.size() * sizeof(MapSet)), "cudaMalloc maps");
+    check_cuda(cudaMemcpy(d_maps_, maps.data(), maps.size() * sizeof(MapSet), cudaMemcpyHostToDevice), "maps");
+    configure_grids();
+  }
   check_cuda(cudaMallocHost(&h_states_, models_.size() * sizeof(StepState)), "pinned states");
 }
 
 // Persistent grids of the TMA kernels: resident CTAs per SM x SM count, capped
 // by the number of tiles.
 void Runner::configure_grids() {
+  if (qt_) return;  // quadtree kernels launch one CTA per work chunk
   int dev = 0, nsm = 0, nb_m = 0, nb_c = 0;
   check_cuda(cudaGetDevice(&dev), "device");
   check_cuda(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "sm count");
@@ -876,17 +1002,31 @@ Runner::~Runner() {
   if (h_states_) cudaFreeHost(h_states_);
 }
 
-void Runner::launch_one() {
-  launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
-  if (tma())
+void Runner::launch_momentum_any() {
+  if (qt_) {
+    launch_qt_momentum(d_scns_, d_tiles_, nqf_, subgrid_, stream_);
+    launch_qt_cuv(d_scns_, d_tiles_ + nqf_, nqcuv_, stream_);
+  } else if (tma()) {
     launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, tma_minb(), mom_grid_, stream_, one());
-  else
+  } else {
     launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
-  if (any_src_) launch_sources(d_scns_, nscn(), stream_);
-  if (tma())
+  }
+}
+
+void Runner::launch_continuity_any() {
+  if (qt_)
+    launch_qt_continuity(d_scns_, d_tiles_ + nqf_ + nqcuv_, nqc_, subgrid_, stream_);
+  else if (tma())
     launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_, one());
   else
     launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
+}
+
+void Runner::launch_one() {
+  launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
+  launch_momentum_any();
+  if (any_src_) launch_sources(d_scns_, nscn(), stream_);
+  launch_continuity_any();
 }
 
 void Runner::build_graph(int chunk) {
@@ -935,17 +1075,11 @@ std::vector<double> Runner::time_kernels(int nsteps) {
     check_cuda(cudaEventRecord(ev[0], stream_), "record");
     launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
     check_cuda(cudaEventRecord(ev[1], stream_), "record");
-    if (tma())
-      launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, tma_minb(), mom_grid_, stream_, one());
-    else
-      launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
+    launch_momentum_any();
     check_cuda(cudaEventRecord(ev[2], stream_), "record");
     if (any_src_) launch_sources(d_scns_, nscn(), stream_);
     check_cuda(cudaEventRecord(ev[3], stream_), "record");
-    if (tma())
-      launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_, one());
-    else
-      launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
+    launch_continuity_any();
     check_cuda(cudaEventRecord(ev[4], stream_), "record");
     check_cuda(cudaEventSynchronize(ev[4]), "event sync");
     for (int k = 0; k < 4; k++) {
@@ -986,6 +1120,7 @@ void Runner::step_once() {
 // result, and the tuning steps are part of the run.  Only meaningful while
 // the models still have steps to take; returns the chosen variant.
 int Runner::autotune(int chunk) {
+  if (qt_) return variant_;  // one quadtree kernel path
   static const int kCandidates[] = {5, 4, 2};
   cudaEvent_t e0, e1;
   check_cuda(cudaEventCreate(&e0), "event");

@@ -54,7 +54,38 @@ struct HostModel {
   long long n_kcs1 = 0;
   double area_total_kcs1 = 0;
   std::vector<int2> tiles;  // (n0, m0) of every 32 x 8 tile holding an active cell
+  // ---- quadtree meshes (p.quadtree != 0): compact cells and uv points
+  std::vector<FaceQ> qface;
+  std::vector<int4> qcell;
+  std::vector<int2> qcuv;
+  std::vector<uint8_t> qlev;
+  std::vector<float> zbmx_q, gn2_q;
+  std::vector<int32_t> qmap_u, qmap_v;  // q index of each cell's right / upper uv point (BMI qx, qy)
+  std::vector<float> cell_area;         // [np] m2
+  std::vector<int64_t> qt_key;          // sorted keys (level, m, n) of the active cells, for point lookup
+  std::vector<int32_t> qt_key_cell;     // compact cell of each key
 };
+
+class InpFile;
+
+// Keywords of sfincs.inp needed after parsing (file names, grid, derived values).
+struct Keys {
+  int mmax = 0, nmax = 0;
+  float dx = 0, dy = 0, x0 = 0, y0 = 0, rotation = 0, cosrot = 1, sinrot = 0, t0 = 0, t1 = 0;
+  float hmin_cfl = 0, dtmax = 0, uvmax = 0, nuviscdim = 0, manning = 0, manning_land = 0, manning_sea = 0,
+        rghlevland = 0, qinf = 0, qinf_zmin = 0;
+  bool viscosity = false, advection_mask = true, quadtree = false;
+  std::string qtrfile, depfile, mskfile, indexfile, sbgfile, manningfile, bndfile, bzsfile, srcfile, disfile,
+      wndfile, qinffile, prcpfile;
+};
+Keys parse_keys(const InpFile& in, HostModel& h, bool bmi);
+void read_boundary_series(HostModel& h, const Keys& k, bool water_level_bnd, std::vector<float>& xb,
+                          std::vector<float>& yb, int& nbnd);
+void read_meteo_series(HostModel& h, const Keys& k, float rotation);
+// Quadtree mesh (qtrfile): compact cells and uv points (host/qtmodel.cpp).
+void load_quadtree(HostModel& h, const Keys& k);
+// 1-based active cell of a quadtree mesh at point (x, y), 0 outside.
+int quadtree_cell_index(const HostModel& h, double x, double y);
 
 // Reads <dir>/sfincs.inp and the files it names.  bmi mirrors the reference's
 // BMI initialize() (use_qext on).  Throws std::runtime_error on bad input.
@@ -73,12 +104,21 @@ class DeviceModel {
   size_t bytes() const { return bytes_; }
   // compact (nm order) views
   int32_t* d_cmp_off() { return d_cmp_; }
+  // q index of each cell's right / upper uv point (quadtree meshes; null otherwise)
+  const int32_t* d_qmap_u() const { return d_qmap_u_; }
+  // gather map of a per-cell face array: dir 0 = right (x) face, 1 = upper (y) face
+  const int32_t* face_map(int dir) const {
+    if (d_qmap_u_) return dir == 0 ? d_qmap_u_ : d_qmap_v_;
+    return d_cmp_;
+  }
+  const int32_t* d_qmap_v() const { return d_qmap_v_; }
 
  private:
   const HostModel* h_;
   ScnDev d_{};
   void* block_ = nullptr;  // every device array of the model, one allocation
   int32_t* d_cmp_ = nullptr;
+  int32_t *d_qmap_u_ = nullptr, *d_qmap_v_ = nullptr;
   size_t bytes_ = 0;
 };
 
@@ -136,11 +176,13 @@ class Runner {
   // Issue nsteps steps with CUDA events between the launches; returns the mean
   // duration (ms) of [step+boundary, momentum, sources, continuity] launches.
   std::vector<double> time_kernels(int nsteps);
-  int launches_per_step() const { return 3 + any_src_; }
+  int launches_per_step() const { return 3 + any_src_ + (qt_ && nqcuv_ > 0 ? 1 : 0); }
 
  private:
   void build_graph(int chunk);
   void configure_grids();
+  void launch_momentum_any();
+  void launch_continuity_any();
   std::vector<DeviceModel*> models_;
   ScnDev* d_scns_ = nullptr;
   Tile* d_tiles_ = nullptr;
@@ -150,6 +192,8 @@ class Runner {
   MapSet* d_maps_ = nullptr;  // TMA tensor maps, one set per model
   int mom_grid_ = 0, con_grid_ = 0;
   int subgrid_ = 0;
+  int qt_ = 0;                       // quadtree models: face / combined-point / cell work lists in d_tiles_
+  int nqf_ = 0, nqcuv_ = 0, nqc_ = 0;
   int any_src_ = 0;
   cudaStream_t stream_ = nullptr;
   bool own_stream_ = true;
@@ -179,5 +223,8 @@ void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile*
                          int minb, int grid, cudaStream_t s, const ScnDev* one);
 void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
                            int grid, cudaStream_t s, const ScnDev* one);
+void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s);
+void launch_qt_cuv(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, cudaStream_t s);
+void launch_qt_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s);
 
 }  // namespace sfg

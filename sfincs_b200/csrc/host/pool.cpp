@@ -170,9 +170,9 @@ struct Pool {
     auto need = [&](size_t b) {
       if (bytes != b) throw std::runtime_error("pool get('" + name + "'): expected " + std::to_string(b) + " bytes");
     };
-    auto f32 = [&](const float* src) {
+    auto f32 = [&](const float* src, const int32_t* map = nullptr) {
       need((size_t)n * 4);
-      launch_gather_f32(src, s.dev->d_cmp_off(), (float*)d_stage, n, stream);
+      launch_gather_f32(src, map ? map : s.dev->d_cmp_off(), (float*)d_stage, n, stream);
     };
     if (name == "zs") {
       need(need8);
@@ -183,13 +183,13 @@ struct Pool {
     } else if (name == "zsmax") {
       f32(D.zsmax);
     } else if (name == "qx") {
-      f32(D.qu[p]);
+      f32(D.qu[p], s.dev->face_map(0));
     } else if (name == "qy") {
-      f32(D.qv[p]);
+      f32(D.qv[p], s.dev->face_map(1));
     } else if (name == "uvx") {
-      f32(D.uu[p]);
+      f32(D.uu[p], s.dev->face_map(0));
     } else if (name == "uvy") {
-      f32(D.vv[p]);
+      f32(D.vv[p], s.dev->face_map(1));
     } else {
       throw std::runtime_error("pool get: unknown variable '" + name + "'");
     }
@@ -207,8 +207,8 @@ struct Pool {
     if (st.stop_pending) t = h.t1 + 1.0;
     double v[19] = {t, st.dt, st.min_dt, (double)st.nt, (double)st.error, h.t0, h.t1, (double)h.np, (double)h.npuv,
                     (double)h.p.nkcuv2, (double)h.p.ngbnd, (double)h.p.subgrid, st.bflux_vol,
-                    st.rain_vol * (double)h.n_kcs1, st.src_vol, h.p.dtmax, h.p.dtmin, (double)s.dev->bytes(),
-                    (double)h.tiles.size()};
+                    st.rain_vol * h.area_total_kcs1, st.src_vol, h.p.dtmax, h.p.dtmin, (double)s.dev->bytes(),
+                    (double)(h.p.quadtree ? h.np : (long long)h.tiles.size())};
     std::memcpy(out, v, sizeof(v));
   }
 };

@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(32) k_step(const ScnDev* __restrict__ scns) {
                         : (float)((t - (double)S.tprcp[i0 - 1]) / (double)(S.tprcp[itp - 1] - S.tprcp[i0 - 1]));
         st.ptmp = (S.vprcp[i0 - 1] * (1.0f - twfac) + S.vprcp[itp - 1] * twfac) / (float)(1000 * 3600);
         st.itprcplast = itp - 1 >= 1 ? itp - 1 : 1;
-        st.rain_vol += (double)st.ptmp * (double)S.area * (double)dt;
+        st.rain_vol += (double)st.ptmp * (double)dt;  // depth; the host multiplies by the kcs==1 area
       }
       // ---- boundary time interpolation (sfincs_boundaries.f90:696-726)
       if (S.nbnd > 0) {
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(128) k_bnd(const ScnDev* __restrict__ scns) {
     }
     S.zs[b.nmb] = zsb_v;
     if (S.store_zsmax) S.zsmax[b.nmb] = fmaxf(S.zsmax[b.nmb], zsb_v);
-    inflow = (double)sgn * (double)qq * (double)(isv ? S.dx : S.dy) * (double)dt;
+    inflow = (double)sgn * (double)qq * (double)b.len * (double)dt;
   } else if (i < S.nkcuv2 + S.nneu) {
     const int2 nn = S.neu[i - S.nkcuv2];  // Neumann: zs(nmb) = zs(nmi) (sfincs_boundaries.f90:903-914)
     S.zs[nn.x] = S.zs[nn.y];

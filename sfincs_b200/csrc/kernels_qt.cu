@@ -1,0 +1,245 @@
+// Quadtree kernels (sm_100a): one thread per uv point (momentum), per
+// combined uv point, and per cell (continuity), over compact arrays in the
+// reference's order.  Work items are 256-wide chunks of one model's points
+// (Tile{scenario, first, count}), so one launch advances every model of an
+// ensemble.  The face arithmetic is face_flux_geo (face_math.h), shared with
+// the regular-grid tile kernels; only the spacing changes per refinement
+// level and at level transitions (sfincs_momentum.f90:205-313).
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "face_math.h"
+#include "sfg_device.h"
+
+namespace sfg {
+
+namespace {
+
+__device__ __forceinline__ float qt_warp_max(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+}  // namespace
+
+// Momentum of one uv point per thread (sfincs_momentum.f90:157-752, quadtree
+// branches).  Dry points get q = uv = 0; points that are not momentum points
+// (kcuv 0, boundary faces) are left alone.
+template <bool SG>
+__global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
+  const Tile tl = tiles[blockIdx.x];
+  const ScnDev& S = scns[tl.scn];
+  StepState& st = *S.st;
+  if (!st.run) return;
+  const int p = st.parity;
+  const float* __restrict__ q0 = S.qu[p];
+  const float* __restrict__ uv0 = S.uu[p];
+  float* q1 = S.qu[p ^ 1];
+  float* uv1 = S.uu[p ^ 1];
+  float den = 0.0f;
+  const int i = tl.n0 + (int)threadIdx.x;
+  if ((int)threadIdx.x < tl.m0) {
+    const FaceQ f = S.qface[i];
+    if (f.info & QF_ACT) {
+      const float zs_nm = S.zs[f.nm], zs_nmu = S.zs[f.nmu];
+      const float zsu = fmaxf(zs_nm, zs_nmu);
+      float zmin = 0.0f, zmax = 0.0f;
+      bool wet;
+      if (SG) {
+        const float2 z = S.sgz_u[i];
+        zmin = z.x;
+        zmax = z.y;
+        wet = zsu > zmin + S.huthresh;
+      } else {
+        wet = zsu > S.zbmx[i];
+      }
+      uint8_t* kfuv = S.kf[0];
+      if (wet) {
+        const int L = (int)((f.info >> 8) & 15u);
+        const int dir = (f.info & QF_DIR) ? 1 : 0;
+        FaceGeo geo;
+        if (!(f.info & QF_TRANS)) {
+          geo.dxuvinv = dir == 0 ? S.lv_dxrinv[L] : S.lv_dyrinv[L];
+          geo.dyuvinv = dir == 0 ? S.lv_dyrinv[L] : S.lv_dxrinv[L];
+          geo.dxuv2inv = dir == 0 ? S.lv_dxr2inv[L] : S.lv_dyr2inv[L];
+          geo.dyuv2inv = dir == 0 ? S.lv_dyr2inv[L] : S.lv_dxr2inv[L];
+          geo.nuvisc = S.lv_nuvisc[L];
+        } else {  // refinement transition: 1.5 cell spacing, no viscosity across (dxuv2inv = 0)
+          geo.dxuvinv = dir == 0 ? S.lv_dxrinvc[L] : S.lv_dyrinvc[L];
+          geo.dyuvinv = dir == 0 ? S.lv_dyrinv[L] : S.lv_dxrinv[L];
+          geo.dxuv2inv = 0.0f;
+          geo.dyuv2inv = dir == 0 ? S.lv_dyr2inv[L] : S.lv_dxr2inv[L];
+          geo.nuvisc = S.lv_nuvisc_t[L];
+        }
+        FaceV a{};
+        a.qx_nm = q0[i];
+        if (S.advection || S.coriolis || S.viscosity || S.friction2d || S.thetasmooth) {
+          a.qx_nmd = q0[f.u_nmd];
+          a.qx_nmu = q0[f.u_nmu];
+          a.qy_nm = q0[f.v_nm];
+          a.qy_nmu = q0[f.v_nmu];
+          a.qy_ndm = q0[f.v_ndm];
+          a.qy_ndmu = q0[f.v_ndmu];
+          a.uu_nm = uv0[i];
+          a.uu_nmd = uv0[f.u_nmd];
+          a.uu_nmu = uv0[f.u_nmu];
+          a.uu_ndm = uv0[f.u_ndm];
+          a.uu_num = uv0[f.u_num];
+          a.vu = (uv0[f.v_ndm] + uv0[f.v_ndmu] + uv0[f.v_nm] + uv0[f.v_nmu]) / 4.0f;
+        }
+        float hu, gnavg2, phi = 1.0f, zd0 = 0.0f, zd1 = 0.0f;
+        bool dry0, dry1;
+        if (SG) {
+          if (zsu > zmax) {
+            const float4 w = S.sgw_u[i];
+            hu = w.x + zsu;
+            gnavg2 = w.z - (w.z - w.y) / (w.w * (zsu - zmax) + 1.0f);
+          } else {
+            const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
+            int iuv = (int)((zsu - zmin) / dzuv) + 1;
+            iuv = min(iuv, S.nlev - 1);
+            const float facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
+            const UvRec r = S.rec_u[(int64_t)(iuv - 1) * S.nalloc + i];
+            hu = r.havg + r.dhavg * facint;
+            gnavg2 = r.nrep + r.dnrep * facint;
+            phi = r.pwet + r.dpwet * facint;
+          }
+          dry0 = S.vneg[f.nm] != 0;
+          dry1 = S.vneg[f.nmu] != 0;
+          if (S.wiggle) {
+            zd0 = S.zsderv[f.nm];
+            zd1 = S.zsderv[f.nmu];
+          }
+        } else {
+          hu = fmaxf(zsu - S.zbmx[i], S.huthresh);
+          gnavg2 = S.gn2[i];
+          dry0 = zs_nm < S.zb[f.nm];
+          dry1 = zs_nmu < S.zb[f.nmu];
+        }
+        float qn, un;
+        den = face_flux_geo<SG>(S, st, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kfuv[i], zs_nm,
+                                zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, qn, un);
+        q1[i] = qn;
+        uv1[i] = un;
+        kfuv[i] = KF_WET;
+      } else {
+        q1[i] = 0.0f;
+        uv1[i] = 0.0f;
+        kfuv[i] = 0;
+      }
+    }
+  }
+  // CFL: largest denominator of the warp, one division and one atomicMin per warp
+  den = qt_warp_max(den);
+  if ((threadIdx.x & 31) == 0 && den > 0.0f) atomicMin(&st.min_dt_bits, __float_as_uint(1.0f / den));
+}
+
+// Combined uv points: mean of the two fine faces (sfincs_momentum.f90:757-779).
+__global__ void __launch_bounds__(256) k_qt_cuv(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
+  const Tile tl = tiles[blockIdx.x];
+  const ScnDev& S = scns[tl.scn];
+  const StepState& st = *S.st;
+  if (!st.run || (int)threadIdx.x >= tl.m0) return;
+  const int ic = tl.n0 + (int)threadIdx.x;
+  const int p1 = st.parity ^ 1;
+  float* q1 = S.qu[p1];
+  float* uv1 = S.uu[p1];
+  const int2 c = S.qcuv[ic];
+  q1[S.npuv + ic] = (q1[c.x] + q1[c.y]) / 2.0f;
+  uv1[S.npuv + ic] = (uv1[c.x] + uv1[c.y]) / 2.0f;
+}
+
+// Continuity of one cell per thread (sfincs_continuity.f90:46-262 and
+// 265-624, quadtree spacing per refinement level).
+template <bool SG>
+__global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict__ scns,
+                                                        const Tile* __restrict__ tiles) {
+  const Tile tl = tiles[blockIdx.x];
+  const ScnDev& S = scns[tl.scn];
+  const StepState& st = *S.st;
+  if (!st.run || (int)threadIdx.x >= tl.m0) return;
+  const int c = tl.n0 + (int)threadIdx.x;
+  const uint16_t fl = S.flags[c];
+  if (!(fl & F_ACT)) return;
+  const float* q = S.qu[st.parity ^ 1];
+  const float zs_old = S.zs[c];
+  const float dt = st.dt;
+  float zsn = zs_old;
+  if (fl & F_KCS1) {
+    const int4 fc = S.qcell[c];
+    const float q_md = q[fc.x], q_mu = q[fc.y], q_nd = q[fc.z], q_nu = q[fc.w];
+    const int L = S.qlev[c];
+    const float qx = S.use_qext ? S.qext[c] : 0.0f;
+    const float qi = S.infiltration ? S.qinf[c] : 0.0f;
+    if (SG) {
+      const double v_old = S.zvol[c];
+      const float volmax = S.zz_volmax[c];
+      const float area = S.lv_area[L];
+      const float zs00 = S.wiggle ? S.zs0[c] : 0.0f;
+      float dvol = ((q_md - q_mu) * S.lv_dyrm[L] + (q_nd - q_nu) * S.lv_dxrm[L]) * dt;
+      if (S.precip || S.use_qext) {
+        float dzsdt = 0.0f;
+        if (S.precip) {
+          const float qinfmap = (S.infiltration && v_old > 0.0) ? qi : 0.0f;
+          dzsdt = dzsdt + (st.ptmp - qinfmap);
+        }
+        if (S.use_qext) dzsdt = dzsdt + qx;
+        dvol = dvol + dzsdt * area * dt;
+      }
+      const double v = v_old + (double)dvol;
+      if (v != v_old) S.zvol[c] = v;
+      const float zs11 = zs_old;
+      if (v >= (double)(volmax * 0.999f)) {
+        zsn = (float)((double)fmaxf(S.zz_max[c], -20.0f) + (v - (double)volmax) / (double)area);
+      } else if (v <= (double)1.0e-6f) {
+        zsn = fmaxf(S.zz_min[c], -20.0f);
+      } else {
+        const float dzvol = volmax / (float)(S.nlev - 1);
+        const int iuv = (int)(v / (double)dzvol) + 1;
+        const float facint = (float)((v - (double)((float)(iuv - 1) * dzvol)) / (double)dzvol);
+        const float2 dep = S.zlev[(int64_t)(iuv - 1) * S.npc + c];
+        zsn = dep.x + dep.y * facint;
+      }
+      if (zsn != zs_old) S.zs[c] = zsn;
+      if (S.wiggle) {
+        if (zs11 != zs00) S.zs0[c] = zs11;
+        S.zsderv[c] = zsn - 2.0f * zs11 + zs00;
+      }
+      S.vneg[c] = v < 0.0 ? 1 : 0;
+    } else {
+      float z = zs_old;
+      if (S.precip) {
+        const float zbc = S.infiltration ? S.zb[c] : 0.0f;
+        const float qinfmap = (S.infiltration && !(z <= zbc)) ? qi : 0.0f;
+        z = z + (st.ptmp - qinfmap) * dt;
+      }
+      if (S.use_qext) z = z + qx * dt;
+      z = z + ((q_md - q_mu) * S.lv_dxrinv[L] + (q_nd - q_nu) * S.lv_dyrinv[L]) * dt;
+      if (z != zs_old) S.zs[c] = z;
+      zsn = z;
+    }
+  }
+  if (S.store_zsmax && zsn > S.zsmax[c]) S.zsmax[c] = zsn;
+}
+
+void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  if (subgrid)
+    k_qt_momentum<true><<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+  else
+    k_qt_momentum<false><<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+}
+void launch_qt_cuv(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, cudaStream_t s) {
+  if (ntiles > 0) k_qt_cuv<<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+}
+void launch_qt_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  if (subgrid)
+    k_qt_continuity<true><<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+  else
+    k_qt_continuity<false><<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+}
+
+}  // namespace sfg

@@ -55,7 +55,29 @@ struct alignas(16) BndFace {
   float zbuv;    // zbuv of the face (regular grids; sfincs_domain.f90:1692)
   float floor;   // zb or subgrid z_zmin of the boundary cell
   float zfix;    // fixed level of an outflow (kcs 3) cell (sfincs_domain.f90:1937-1948)
-  int pad0, pad1;
+  float len;     // face length (m): dy for u faces, dx for v faces (per refinement level on a quadtree)
+  int pad1;
+};
+
+// ---- quadtree layout ---------------------------------------------------------
+// Cells and uv points are compact, in the reference's order (sfincs order:
+// by level, then n fastest).  q/uv arrays hold npuv faces, then ncuv combined
+// points (mean of the two fine faces at a refinement transition,
+// sfincs_momentum.f90:757-779), then one dummy entry that stays 0.
+constexpr int kMaxQtLevels = 8;
+enum : uint32_t {
+  QF_DIR = 1u,     // v face
+  QF_ACT = 2u,     // kcuv 1 or 6: the momentum kernel updates the face
+  QF_ADV = 4u,     // advection mask (sfincs_domain.f90:2147-2178)
+  QF_TH = 8u,      // theta smoothing allowed: kcuv(u_nmd) == kcuv(u_nmu) == 1
+  QF_TRANS = 16u,  // refinement transition face (uv_flags_type != 0)
+};
+struct alignas(16) FaceQ {
+  int nm, nmu;                       // cells on either side (0-based)
+  int u_nmd, u_nmu, u_ndm, u_num;    // uv neighbours (sfincs_domain.f90:1007-1261), 0-based q indices
+  int v_ndm, v_nm, v_ndmu, v_nmu;
+  uint32_t info;                     // QF_* bits; bits 8..11: refinement level - 1
+  int pad;
 };
 
 // One subgrid uv lookup record: values at level k and the increment to k+1
@@ -70,7 +92,7 @@ struct alignas(16) StepState {
   double t;            // model time (s), reference sfincs_lib.f90:57 real*8
   double tend;         // end of the current update interval
   double bflux_vol;    // FP64 accumulated boundary inflow volume (m3)
-  double rain_vol;     // FP64 accumulated rain volume over kcs==1 cells (m3)
+  double rain_vol;     // FP64 accumulated rain depth (m); times the kcs==1 area gives the volume
   double src_vol;      // FP64 accumulated point-source volume (m3)
   unsigned int min_dt_bits;  // float bits; atomicMin target of the flux kernel
   float dt;            // current step (real*4)
@@ -154,6 +176,20 @@ struct ScnDev {
   const int* src_cell;   // [nsrc]
   float pi;
   StepState* st;
+  // ---- quadtree (quadtree != 0; the regular-grid fields above that index
+  // cells or faces then hold compact arrays: zs.. over npc cells, qu/qv and
+  // uu/vv both point at the one q / uv array, kf[0] = kfuv, sgz_u/v, sgw_u/v
+  // and rec_u/v at the face tables with nalloc = npuv as the level stride)
+  int quadtree, npc, npuv, ncuv;
+  const FaceQ* qface;   // [npuv]
+  const int4* qcell;    // [npc] q index of the md, mu, nd, nu uv point of each cell
+  const int2* qcuv;     // [ncuv] q indices of the two fine faces of combined point npuv + i
+  const uint8_t* qlev;  // [npc] refinement level - 1
+  const float* zbmx;    // [npuv] regular bed: zbuvmx
+  const float* gn2;     // [npuv] regular bed: g n^2
+  float lv_dxrinv[kMaxQtLevels], lv_dyrinv[kMaxQtLevels], lv_dxr2inv[kMaxQtLevels], lv_dyr2inv[kMaxQtLevels];
+  float lv_dxrinvc[kMaxQtLevels], lv_dyrinvc[kMaxQtLevels], lv_dxrm[kMaxQtLevels], lv_dyrm[kMaxQtLevels];
+  float lv_area[kMaxQtLevels], lv_nuvisc[kMaxQtLevels], lv_nuvisc_t[kMaxQtLevels];
 };
 
 struct Tile {  // one CTA of the cell kernels

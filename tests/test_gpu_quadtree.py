@@ -1,0 +1,100 @@
+"""GPU parity of the quadtree path: the face/cell kernels on multi-level
+meshes against the oracle in the core's precision, step by step, plus lake at
+rest, volume balance across refinement levels, and ensemble members alone vs
+in the mix."""
+import numpy as np
+import pytest
+
+from sfincs_b200 import qtsynth
+from sfincs_b200.bmi import Ensemble, Model
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle(d, prec):
+    from oracle.oracle import Oracle
+
+    return Oracle(d, prec)
+
+
+def _write(tmp_path, subgrid, seed=21, wind=30.0, tstop=1800.0, name="m"):
+    m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=3, bands=(1000.0, 500.0), P=4, seed=seed,
+                                 tstop=tstop, subgrid=subgrid, wind_speed=wind, tide_period=1800.0)
+    d = tmp_path / name
+    d.mkdir()
+    return m.write(str(d)), m
+
+
+def _cell_q(o, n_cells, npq):
+    """Oracle q of each cell's right / upper uv point (combined points and the dummy included)."""
+    q = o.get("q", npq)
+    qx = q[o.get("z_uv_mu", n_cells).astype(int) - 1]
+    qy = q[o.get("z_uv_nu", n_cells).astype(int) - 1]
+    return qx, qy
+
+
+@pytest.mark.parametrize("subgrid", [False, True])
+def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid):
+    from sfincs_b200 import bmi as B
+
+    d, _ = _write(tmp_path, subgrid)
+    qc = B.layout(d, "qt_counts", 4)
+    npc, npuv, ncuv = int(qc[0]), int(qc[1]), int(qc[2])
+    o = _oracle(d, "f32")
+    g = Model(d)
+    done = 0
+    for n in (1, 1, 2, 6, 30, 60):
+        o.update(-1000.0, n)
+        g.step(n)
+        done += n
+        so, sg = o.scalars(), g.scalars()
+        assert sg["nt"] == so["nt"]
+        dzs = float(np.abs(g.get("zs") - o.get("zs")).max())
+        qx, qy = _cell_q(o, npc, npuv + ncuv + 1)
+        dq = max(float(np.abs(g.get("qx") - qx).max()), float(np.abs(g.get("qy") - qy).max()))
+        print(f"quadtree subgrid={subgrid} step {done}: dt {so['dt']:.6g}/{sg['dt']:.6g} |dzs| {dzs:.3g} |dq| {dq:.3g}")
+        assert dzs <= 2e-5 and dq <= 2e-5, (done, dzs, dq)
+        assert abs(sg["t"] - so["t"]) <= 1e-6 * max(1.0, abs(so["t"]))
+
+
+def test_quadtree_lake_at_rest(tmp_path):
+    m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=3, bands=(1000.0, 500.0), P=4, seed=21,
+                                 tstop=1800.0, subgrid=False, wind_speed=0.0)
+    m.mask[:] = 1
+    m.bnd = m.bzs = m.wnd = None
+    m.z = np.minimum(m.z, -1.0).astype(np.float32)
+    m.params["zsini"] = 0.5
+    d = m.write(str(tmp_path))
+    g = Model(d)
+    z0 = g.get("zs")
+    g.step(100)
+    assert np.array_equal(g.get("zs"), z0)
+    assert np.all(g.get("qx") == 0) and np.all(g.get("qy") == 0)
+
+
+def test_quadtree_volume_balance(tmp_path):
+    m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=3, bands=(1000.0, 500.0), P=4, seed=22,
+                                 tstop=1800.0, subgrid=True, wind_speed=10.0, tide_period=1800.0)
+    m.prcp = np.array([[0.0, 60.0], [7200.0, 60.0]])
+    d = m.write(str(tmp_path))
+    g = Model(d)
+    v0 = g.volume()
+    g.step(200)
+    s = g.scalars()
+    v1 = g.volume()
+    src = s["bflux_vol"] + s["rain_vol"] + s["src_vol"]
+    assert abs((v1 - v0) - src) / max(abs(v1), 1.0) <= 1e-6, (v1 - v0, src)
+
+
+def test_quadtree_members_alone_equal_in_mix(tmp_path):
+    dirs = [_write(tmp_path, True, seed=30 + i, tstop=900.0 + 300.0 * i, name=f"m{i}")[0] for i in range(3)]
+    e = Ensemble(dirs)
+    e.run([e.scalars(i)["t1"] for i in range(len(dirs))])
+    for i, d in enumerate(dirs):
+        g = Model(d)
+        g.run(g.scalars()["t1"])
+        assert e.scalars(i)["nt"] == g.scalars()["nt"]
+        for name in ("zs", "qx", "qy", "zsmax"):
+            assert np.array_equal(e.get(i, name), g.get(name)), (i, name)
+        g.close()
+    e.close()
