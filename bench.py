@@ -46,6 +46,12 @@ WORKLOADS = {
                 "3 m surge + 40 mm/h rain 3 h, 12 h simulated"),
     "plain": (dict(kind="plain", nmax=400, mmax=500, dx=50.0, seed=1, tstop=3600.0),
               "plain regular grid 500x400 @50 m (200k cells), 1:100 beach + 20 bumps, 1 m tide, 1 h simulated"),
+    "quadtree": (dict(kind="quadtree", nmax1=800, mmax1=800, dx1=400.0, nlev=4, bands=(6000.0, 4000.0, 2000.0), P=4,
+                      seed=3, tstop=21600.0, subgrid=True, walk_km=9000.0, tide_amp=1.5, tide_period=44712.0,
+                      wind_speed=30.0, advection=1, viscosity=1),
+                 "quadtree 4 levels 400 m -> 50 m (~8.1M cells) refined within 2/4/6 km of a seeded 9000 km "
+                 "random-walk polyline in a 320 km box, 10-level subgrid tables (12.5 m DEM), advection + viscosity, "
+                 "30 m/s onshore wind, 1.5 m 12.42 h tide, 6 h simulated"),
 }
 
 # Algorithmic bytes per cell-update of this layout (each element read or written
@@ -54,6 +60,7 @@ WORKLOADS = {
 BYTES = {
     "subgrid": {"momentum": 125, "continuity": 67},
     "plain": {"momentum": 60, "continuity": 26},
+    "quadtree": {"momentum": 219, "continuity": 83},
 }
 
 
@@ -83,11 +90,16 @@ def workload_dir(name: str, rank: int) -> str:
     shutil.rmtree(tmp, ignore_errors=True)
     kw = dict(kw)
     kind = kw.pop("kind")
-    if kind == "subgrid":
+    if kind in ("subgrid", "quadtree"):
         import torch
 
         dev = "cuda" if torch.cuda.is_available() else "cpu"
-        m = synth.subgrid_regular(device=dev, **kw)
+        if kind == "subgrid":
+            m = synth.subgrid_regular(device=dev, **kw)
+        else:
+            from sfincs_b200 import qtsynth
+
+            m = qtsynth.quadtree_coastal(device=dev, **kw)
         if dev == "cuda":
             torch.cuda.empty_cache()
     else:
@@ -275,8 +287,11 @@ def run_ours(args, rank: int, world: int, local: int):
     s0 = g.scalars()
     npc = int(s0["np"])
     stream = torch.cuda.ExternalStream(g.stream)
-    # warm-up steps (untimed); graphs get instantiated here
+    # warm-up steps (untimed): W direct steps, then one 32-step CUDA-graph chunk so
+    # that the graph is captured and instantiated before the timed region
+    warm = max(args.warmup, 3) + 32
     g.issue(max(args.warmup, 3))
+    g.issue(32)
     g.sync()
     # ---- timed region: K steps, inputs resident in HBM (> L2: 3+ GB resident state)
     sampler = ClockSampler(local)
@@ -319,6 +334,8 @@ def run_ours(args, rank: int, world: int, local: int):
             traffic = None
     s1 = g.scalars()
     mom_kernel = "k_momentum" if os.environ.get("SFG_MOMENTUM_VARIANT", "5") in ("2", "3") else "k_momentum_tma"
+    if wl == "quadtree":
+        mom_kernel = "k_qt_momentum"
     # ---- full simulated run (12 h for the subgrid workload), device-resident
     full = None
     if args.full_run and rank == 0:
@@ -364,7 +381,7 @@ def run_ours(args, rank: int, world: int, local: int):
     _, desc = WORKLOADS[wl]
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
-        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
+        "steps": args.steps, "warmup": warm, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 time and volume)", "data": "synthetic",
         "config": {"workload": desc, "cells": npc, "global_cells": npc * world, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (device-resident state %.1f GB)" % (s0["device_bytes"] / 1e9),

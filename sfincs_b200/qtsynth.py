@@ -41,15 +41,55 @@ def coastline_x(ny_px: int, pixel: float, seed: int, x_mean: float, amplitude: f
     return (x_mean + np.interp(y, yn, walk)).astype(np.float64)
 
 
-def leaf_levels(nmax1: int, mmax1: int, dx1: float, nlev: int, xc_rows: np.ndarray, bands) -> np.ndarray:
-    """Leaf level of every finest-resolution pixel, refined by horizontal
-    distance to the coastline (``bands[k]``: distance within which cells are
-    refined beyond level k+1) and then 2:1 balanced."""
+def random_walk_polyline(seed: int, start, length: float, step: float, box) -> np.ndarray:
+    """Seeded correlated 2-D random walk of total ``length`` m with segments of
+    ``step`` m, reflected at the edges of ``box = (xmax, ymax)``."""
+    rng = np.random.default_rng(seed)
+    n = max(2, int(length / step))
+    pts = np.empty((n + 1, 2))
+    pts[0] = start
+    ang = rng.uniform(0, 2 * np.pi)
+    for i in range(n):
+        ang += rng.normal(0.0, 0.35)
+        p = pts[i] + step * np.array([np.cos(ang), np.sin(ang)])
+        for k in (0, 1):
+            if p[k] < 0 or p[k] > box[k]:
+                p[k] = min(max(p[k], 0.0), box[k])
+                ang = np.pi - ang if k == 0 else -ang
+        pts[i + 1] = p
+    return pts
+
+
+def polyline_distance(pts: np.ndarray, ny: int, nx: int, px: float) -> np.ndarray:
+    """Distance (m) from every pixel centre of an (ny, nx) raster of pixel size
+    px to the polyline (rasterised at px/2 spacing, exact Euclidean transform)."""
+    from scipy import ndimage
+
+    seg = np.diff(pts, axis=0)
+    lens = np.hypot(seg[:, 0], seg[:, 1])
+    k = np.maximum(2, (lens / (0.5 * px)).astype(np.int64) + 1)
+    sid = np.repeat(np.arange(seg.shape[0]), k)
+    t = (np.arange(int(k.sum())) - np.repeat(np.cumsum(k) - k, k)) / np.repeat(k - 1, k)
+    xs = ((pts[sid, 0] + t * seg[sid, 0]) / px).astype(np.int64)
+    ys = ((pts[sid, 1] + t * seg[sid, 1]) / px).astype(np.int64)
+    ok = (xs >= 0) & (xs < nx) & (ys >= 0) & (ys < ny)
+    on = np.ones((ny, nx), bool)
+    on[ys[ok], xs[ok]] = False
+    return ndimage.distance_transform_edt(on) * px
+
+
+def leaf_levels(nmax1: int, mmax1: int, dx1: float, nlev: int, xc_rows: np.ndarray, bands,
+                dist: Optional[np.ndarray] = None) -> np.ndarray:
+    """Leaf level of every finest-resolution pixel, refined by distance
+    (``bands[k]``: distance within which cells are refined beyond level k+1)
+    and then 2:1 balanced.  The distance is horizontal distance to the
+    coastline x(row), or the given raster."""
     R = 1 << (nlev - 1)
     ny, nx = nmax1 * R, mmax1 * R
     px = dx1 / R
-    x = (np.arange(nx) + 0.5) * px
-    dist = np.abs(x[None, :] - xc_rows[:, None])
+    if dist is None:
+        x = (np.arange(nx) + 0.5) * px
+        dist = np.abs(x[None, :] - xc_rows[:, None])
     target = np.ones((ny, nx), np.int8)
     for k, b in enumerate(bands[: nlev - 1]):
         target[dist < b] = k + 2
@@ -352,12 +392,15 @@ class QuadtreeModel:
 def quadtree_coastal(nmax1=40, mmax1=60, dx1=400.0, nlev=4, bands=(2000.0, 1000.0, 500.0), P=4, seed=3,
                      tstop=21600.0, subgrid=True, tide_amp=1.5, tide_period=44712.0, wind_speed=30.0,
                      coast_frac=0.4, coast_wander=0.1, device="cpu", nlev_tab=10,
-                     advection=1, viscosity=1) -> QuadtreeModel:
+                     advection=1, viscosity=1, walk_km: float = 0.0) -> QuadtreeModel:
     """Quadtree coastal model: ``nlev`` levels from ``dx1`` down, refined within
     ``bands`` of a random-walk coastline (sea to the west), a fractal DEM at
     ``P`` pixels per finest cell (relief -15..+25 m), a water-level boundary
     on the west edge with a sinusoidal tide, and a uniform onshore wind
-    (from the west) of ``wind_speed`` m/s."""
+    (from the west) of ``wind_speed`` m/s.  With ``walk_km`` > 0 the
+    refinement follows a seeded 2-D random-walk polyline of that length
+    starting on the coast (distance-banded as for the coastline) instead of
+    the coastline itself."""
     import torch
 
     R = 1 << (nlev - 1)
@@ -368,7 +411,14 @@ def quadtree_coastal(nmax1=40, mmax1=60, dx1=400.0, nlev=4, bands=(2000.0, 1000.
     xc = coastline_x(ny_px, pixel, seed, coast_frac * xw, coast_wander * xw)
     # leaf levels from the coastline at the finest cell rows
     xc_rows = xc.reshape(nmax1 * R, P).mean(axis=1)
-    lev = leaf_levels(nmax1, mmax1, dx1, nlev, xc_rows, bands)
+    dist = None
+    if walk_km > 0:
+        ny_c, nx_c = nmax1 * R, mmax1 * R
+        pts = random_walk_polyline(seed + 1, (float(xc_rows[ny_c // 2]), ny_c * dx1 / R / 2), walk_km * 1000.0,
+                                   200.0, (nx_c * dx1 / R, ny_c * dx1 / R))
+        dist = polyline_distance(pts, ny_c, nx_c, dx1 / R)
+    lev = leaf_levels(nmax1, mmax1, dx1, nlev, xc_rows, bands, dist)
+    del dist
     mesh = build_mesh(lev, nmax1, mmax1, dx1, nlev)
     # DEM: trend relative to the local coastline plus a fractal
     from .synth import fractal_surface

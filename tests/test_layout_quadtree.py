@@ -14,22 +14,22 @@ def _oracle(d, prec="f32"):
     return Oracle(d, prec)
 
 
-def _model(tmp_path, subgrid, seed=21, nlev=3, advection=1, viscosity=1):
+def _model(tmp_path, subgrid, seed=21, nlev=3, advection=1, viscosity=1, walk_km=0.0):
     m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=nlev, bands=(1000.0, 500.0, 250.0)[: nlev - 1],
                                  P=4, seed=seed, tstop=1800.0, subgrid=subgrid, advection=advection,
-                                 viscosity=viscosity)
+                                 viscosity=viscosity, walk_km=walk_km)
     return m.write(str(tmp_path)), m
 
 
-@pytest.mark.parametrize("subgrid", [False, True])
-def test_quadtree_mesh_matches_oracle(tmp_path, subgrid):
-    d, m = _model(tmp_path, subgrid)
+@pytest.mark.parametrize("subgrid,nlev,walk_km", [(False, 3, 0.0), (True, 3, 0.0), (True, 4, 12.0)])
+def test_quadtree_mesh_matches_oracle(tmp_path, subgrid, nlev, walk_km):
+    d, m = _model(tmp_path, subgrid, nlev=nlev, walk_km=walk_km)
     o = _oracle(d)
     s = o.scalars()
     qc = B.layout(d, "qt_counts", 4)
     npc, npuv, ncuv = int(qc[0]), int(qc[1]), int(qc[2])
     assert npc == int(s["np"]) and npuv == int(s["npuv"])
-    assert ncuv > 0 and int(qc[3]) == 3
+    assert ncuv > 0 and int(qc[3]) == nlev
     for name in ("uv_nm", "uv_nmu", "uv_dir", "uv_iref", "uv_u_nmd", "uv_u_nmu", "uv_u_ndm", "uv_u_num",
                  "uv_v_ndm", "uv_v_nm", "uv_v_ndmu", "uv_v_nmu"):
         assert np.array_equal(B.layout(d, name, npuv), o.get(name, npuv)), name
