@@ -19,8 +19,9 @@ if ROOT not in sys.path:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="subgrid", choices=["subgrid", "plain"])
-    ap.add_argument("--n", type=int, default=1000, help="cells per side (subgrid) or nmax (plain)")
+    ap.add_argument("--workload", default="subgrid", choices=["subgrid", "plain", "quadtree"])
+    ap.add_argument("--n", type=int, default=1000,
+                    help="cells per side (subgrid), nmax (plain) or level-1 cells per side (quadtree)")
     ap.add_argument("--P", type=int, default=20, help="subgrid pixels per cell side")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--steps", type=int, default=3)
@@ -35,6 +36,13 @@ def main():
         if args.workload == "subgrid":
             m = synth.subgrid_regular(nmax=args.n, mmax=args.n, dx=100.0, P=args.P, seed=2, tstop=43200.0,
                                       device="cuda")
+        elif args.workload == "quadtree":
+            from sfincs_b200 import qtsynth
+
+            # the bench's quadtree workload scaled to n level-1 cells per side (800 in the bench)
+            m = qtsynth.quadtree_coastal(nmax1=args.n, mmax1=args.n, dx1=400.0, nlev=4,
+                                         bands=(6000.0, 4000.0, 2000.0), P=4, seed=3, tstop=21600.0, subgrid=True,
+                                         walk_km=9000.0 * (args.n / 800.0) ** 2, device="cuda")
         else:
             m = synth.plain_regular(nmax=args.n, mmax=int(args.n * 1.25), dx=50.0)
         m.write(d)
