@@ -1,16 +1,16 @@
 // B200 kernels of the SFINCS time-stepping core (sm_100a).
 //
-// One model time step is four launches (five with point sources), all driven
+// One model time step is three launches (four with point sources), all driven
 // by a device-resident table of scenarios so that one launch advances one model
 // (BMI drop-in) or an uneven ensemble with per-scenario dt:
 //
-//   k_step          one warp per scenario: dt = alfa*min_dt, t += dt (FP64),
-//                   uniform meteo, boundary time interpolation, CFL reset,
-//                   instability check.  sfincs_lib.f90:379-548,
-//                   sfincs_meteo.f90:1445-1558, sfincs_boundaries.f90:682-758.
-//   k_bnd           one thread per water-level boundary face / Neumann cell:
-//                   boundary levels and weakly reflective boundary fluxes.
-//                   sfincs_boundaries.f90:761-1122.
+//   k_step_bnd      one CTA per scenario: step control (dt = alfa*min_dt,
+//                   t += dt in FP64, uniform meteo, boundary time
+//                   interpolation, CFL reset, instability check;
+//                   sfincs_lib.f90:379-548, sfincs_meteo.f90:1445-1558,
+//                   sfincs_boundaries.f90:682-758), then one thread per
+//                   water-level boundary face / Neumann cell: boundary levels
+//                   and weakly reflective fluxes (sfincs_boundaries.f90:761-1122).
 //   k_momentum<SG>  one thread per uv face (blockDim.z selects u or v, warp
 //                   uniform): local-inertia flux, subgrid uv lookup, advection,
 //                   viscosity, Coriolis, wind, friction, limiters, and the CFL
@@ -35,6 +35,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "pdl.h"
 #include "sfg_device.h"
 
 namespace sfg {
@@ -53,140 +54,137 @@ __device__ __forceinline__ int64_t off(const ScnDev& S, int n, int m) {
 }
 
 // --------------------------------------------------------------------------
-// k_step: step control, one warp per scenario.
+// Step control (run by thread 0 of the step kernel).
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(32) k_step(const ScnDev* __restrict__ scns) {
-  const ScnDev& S = scns[blockIdx.x];
-  StepState& st = *S.st;
-  __shared__ int s_go;
-  if (threadIdx.x == 0) {
-    if (st.run) {  // previous step executed: its outputs are in the other buffer
-      st.parity ^= 1;
-      st.run = 0;
-    }
-    if (st.stop_pending) {  // sfincs_lib.f90:646
-      st.t = (double)S.t1 + 1.0;
-      st.stop_pending = 0;
-    }
-    const int go = (st.t < st.tend) && (st.steps_left != 0);
-    if (go) {
-      st.nt += 1;
-      const float mdt = __uint_as_float(st.min_dt_bits);
-      const float dt = S.alfa * mdt;  // sfincs_lib.f90:391-392
-      const float dtchk = S.alfa * mdt;
-      st.min_dt = mdt;
-      st.dt = dt;
-      const double t = st.t + (double)dt;
-      st.t = t;
-      // ---- uniform wind from time series (sfincs_meteo.f90:1445-1508)
-      if (S.wind) {
-        for (int itw = st.itwndlast; itw <= S.ntwnd; itw++) {
-          if ((double)S.twnd[itw - 1] > t) {
-            const int i0 = itw - 1 >= 1 ? itw - 1 : 1;
-            const float twfac =
-                (float)((t - (double)S.twnd[i0 - 1]) / (double)(S.twnd[itw - 1] - S.twnd[i0 - 1]));
-            const float vmag = S.wmag[i0 - 1] * (1.0f - twfac) + S.wmag[itw - 1] * twfac;
-            const float twopi = 2.0f * S.pi;
-            float dr0 = fmodf(S.wdir[i0 - 1], twopi);
-            if (dr0 < 0.0f) dr0 += twopi;
-            float dr1 = fmodf(S.wdir[itw - 1], twopi);
-            if (dr1 < 0.0f) dr1 += twopi;
-            if (dr1 > dr0 + S.pi)
-              dr0 = dr0 + 2.0f * S.pi;
-            else if (dr0 > dr1 + S.pi)
-              dr1 = dr1 + 2.0f * S.pi;
-            const float vdir = dr0 * (1.0f - twfac) + dr1 * twfac;
-            int icd = (int)(vmag * 10.0f) + 1;
-            icd = icd < 1 ? 1 : (icd > 1000 ? 1000 : icd);
-            const float cd = S.cdval[icd - 1];
-            st.twu = vmag * vmag * cosf(vdir) * S.rhoa * cd / S.rhow;
-            st.twv = vmag * vmag * sinf(vdir) * S.rhoa * cd / S.rhow;
-            st.itwndlast = itw - 1 >= 1 ? itw - 1 : 1;
-            break;
-          }
-        }
-      }
-      // ---- uniform rain from time series (sfincs_meteo.f90:1510-1558)
-      if (S.precip) {
-        int itp;
-        for (itp = st.itprcplast; itp <= S.ntprcp; itp++)
-          if ((double)S.tprcp[itp - 1] > t) break;
-        itp = max(min(itp, S.ntprcp), 1);
-        const int i0 = itp - 1 >= 1 ? itp - 1 : 1;
-        const float twfac =
-            (i0 == itp) ? 0.0f
-                        : (float)((t - (double)S.tprcp[i0 - 1]) / (double)(S.tprcp[itp - 1] - S.tprcp[i0 - 1]));
-        st.ptmp = (S.vprcp[i0 - 1] * (1.0f - twfac) + S.vprcp[itp - 1] * twfac) / (float)(1000 * 3600);
-        st.itprcplast = itp - 1 >= 1 ? itp - 1 : 1;
-        st.rain_vol += (double)st.ptmp * (double)dt;  // depth; the host multiplies by the kcs==1 area
-      }
-      // ---- boundary time interpolation (sfincs_boundaries.f90:696-726)
-      if (S.nbnd > 0) {
-        int itb0 = 1, itb1 = 1;
-        float tb = 0.0f;
-        if ((double)S.t_bnd[0] > (t - 1.0e-3)) {
-          itb0 = itb1 = 1;
-          tb = S.t_bnd[0];
-        } else if ((double)S.t_bnd[S.ntbnd - 1] < (t + 1.0e-3)) {
-          itb0 = itb1 = S.ntbnd;
-          tb = S.t_bnd[S.ntbnd - 1];
-        } else {
-          for (int itb = st.itbndlast; itb <= S.ntbnd; itb++) {
-            if ((double)S.t_bnd[itb - 1] > (t + 1.0e-6)) {
-              itb0 = itb - 1;
-              itb1 = itb;
-              tb = (float)t;
-              st.itbndlast = itb - 1;
-              break;
-            }
-          }
-        }
-        st.itb0 = itb0;
-        st.itb1 = itb1;
-        st.tbfac = (tb - S.t_bnd[itb0 - 1]) / fmaxf(S.t_bnd[itb1 - 1] - S.t_bnd[itb0 - 1], 1.0e-6f);
-      }
-      // ---- point-source discharges (sfincs_discharges.f90:341-359)
-      if (S.nsrc > 0) {
-        for (int its = st.itsrclast; its <= S.ntsrc; its++) {
-          if ((double)S.tsrc[its - 1] > t) {
-            const int i0 = its - 1 >= 1 ? its - 1 : 1;
-            const float* a = S.qsrc + (size_t)(i0 - 1) * S.nsrc;
-            const float* b = S.qsrc + (size_t)(its - 1) * S.nsrc;
-            for (int is = 0; is < S.nsrc; is++)
-              S.qtsrc[is] = (float)((double)a[is] + (double)(b[is] - a[is]) * (t - (double)S.tsrc[i0 - 1]) /
-                                                        (double)(S.tsrc[its - 1] - S.tsrc[i0 - 1]));
-            st.itsrclast = its - 1 >= 1 ? its - 1 : 1;
-            break;
-          }
-        }
-      }
-      st.min_dt_bits = __float_as_uint(S.dtmax);  // sfincs_momentum.f90:99
-      if (dtchk < S.dtmin && st.nt > 1) {         // sfincs_lib.f90:634-648
-        st.error = 1;
-        st.stop_pending = 1;
-      }
-      st.run = 1;
-      if (st.steps_left > 0) st.steps_left -= 1;
-    }
-    s_go = go;
+// Step control of one scenario (thread 0): returns whether the scenario takes
+// this step.
+__device__ __forceinline__ int step_control(const ScnDev& S, StepState& st) {
+  if (st.run) {  // previous step executed: its outputs are in the other buffer
+    st.parity ^= 1;
+    st.run = 0;
   }
-  __syncthreads();
-  if (!s_go || S.nbnd <= 0) return;
-  // ---- levels at the boundary points (sfincs_boundaries.f90:728-756)
+  if (st.stop_pending) {  // sfincs_lib.f90:646
+    st.t = (double)S.t1 + 1.0;
+    st.stop_pending = 0;
+  }
+  const int go = (st.t < st.tend) && (st.steps_left != 0);
+  if (go) {
+    st.nt += 1;
+    const float mdt = __uint_as_float(st.min_dt_bits);
+    const float dt = S.alfa * mdt;  // sfincs_lib.f90:391-392
+    const float dtchk = S.alfa * mdt;
+    st.min_dt = mdt;
+    st.dt = dt;
+    const double t = st.t + (double)dt;
+    st.t = t;
+    // ---- uniform wind from time series (sfincs_meteo.f90:1445-1508)
+    if (S.wind) {
+      for (int itw = st.itwndlast; itw <= S.ntwnd; itw++) {
+        if ((double)S.twnd[itw - 1] > t) {
+          const int i0 = itw - 1 >= 1 ? itw - 1 : 1;
+          const float twfac =
+              (float)((t - (double)S.twnd[i0 - 1]) / (double)(S.twnd[itw - 1] - S.twnd[i0 - 1]));
+          const float vmag = S.wmag[i0 - 1] * (1.0f - twfac) + S.wmag[itw - 1] * twfac;
+          const float twopi = 2.0f * S.pi;
+          float dr0 = fmodf(S.wdir[i0 - 1], twopi);
+          if (dr0 < 0.0f) dr0 += twopi;
+          float dr1 = fmodf(S.wdir[itw - 1], twopi);
+          if (dr1 < 0.0f) dr1 += twopi;
+          if (dr1 > dr0 + S.pi)
+            dr0 = dr0 + 2.0f * S.pi;
+          else if (dr0 > dr1 + S.pi)
+            dr1 = dr1 + 2.0f * S.pi;
+          const float vdir = dr0 * (1.0f - twfac) + dr1 * twfac;
+          int icd = (int)(vmag * 10.0f) + 1;
+          icd = icd < 1 ? 1 : (icd > 1000 ? 1000 : icd);
+          const float cd = S.cdval[icd - 1];
+          st.twu = vmag * vmag * cosf(vdir) * S.rhoa * cd / S.rhow;
+          st.twv = vmag * vmag * sinf(vdir) * S.rhoa * cd / S.rhow;
+          st.itwndlast = itw - 1 >= 1 ? itw - 1 : 1;
+          break;
+        }
+      }
+    }
+    // ---- uniform rain from time series (sfincs_meteo.f90:1510-1558)
+    if (S.precip) {
+      int itp;
+      for (itp = st.itprcplast; itp <= S.ntprcp; itp++)
+        if ((double)S.tprcp[itp - 1] > t) break;
+      itp = max(min(itp, S.ntprcp), 1);
+      const int i0 = itp - 1 >= 1 ? itp - 1 : 1;
+      const float twfac =
+          (i0 == itp) ? 0.0f
+                      : (float)((t - (double)S.tprcp[i0 - 1]) / (double)(S.tprcp[itp - 1] - S.tprcp[i0 - 1]));
+      st.ptmp = (S.vprcp[i0 - 1] * (1.0f - twfac) + S.vprcp[itp - 1] * twfac) / (float)(1000 * 3600);
+      st.itprcplast = itp - 1 >= 1 ? itp - 1 : 1;
+      st.rain_vol += (double)st.ptmp * (double)dt;  // depth; the host multiplies by the kcs==1 area
+    }
+    // ---- boundary time interpolation (sfincs_boundaries.f90:696-726)
+    if (S.nbnd > 0) {
+      int itb0 = 1, itb1 = 1;
+      float tb = 0.0f;
+      if ((double)S.t_bnd[0] > (t - 1.0e-3)) {
+        itb0 = itb1 = 1;
+        tb = S.t_bnd[0];
+      } else if ((double)S.t_bnd[S.ntbnd - 1] < (t + 1.0e-3)) {
+        itb0 = itb1 = S.ntbnd;
+        tb = S.t_bnd[S.ntbnd - 1];
+      } else {
+        for (int itb = st.itbndlast; itb <= S.ntbnd; itb++) {
+          if ((double)S.t_bnd[itb - 1] > (t + 1.0e-6)) {
+            itb0 = itb - 1;
+            itb1 = itb;
+            tb = (float)t;
+            st.itbndlast = itb - 1;
+            break;
+          }
+        }
+      }
+      st.itb0 = itb0;
+      st.itb1 = itb1;
+      st.tbfac = (tb - S.t_bnd[itb0 - 1]) / fmaxf(S.t_bnd[itb1 - 1] - S.t_bnd[itb0 - 1], 1.0e-6f);
+    }
+    // ---- point-source discharges (sfincs_discharges.f90:341-359)
+    if (S.nsrc > 0) {
+      for (int its = st.itsrclast; its <= S.ntsrc; its++) {
+        if ((double)S.tsrc[its - 1] > t) {
+          const int i0 = its - 1 >= 1 ? its - 1 : 1;
+          const float* a = S.qsrc + (size_t)(i0 - 1) * S.nsrc;
+          const float* b = S.qsrc + (size_t)(its - 1) * S.nsrc;
+          for (int is = 0; is < S.nsrc; is++)
+            S.qtsrc[is] = (float)((double)a[is] + (double)(b[is] - a[is]) * (t - (double)S.tsrc[i0 - 1]) /
+                                                      (double)(S.tsrc[its - 1] - S.tsrc[i0 - 1]));
+          st.itsrclast = its - 1 >= 1 ? its - 1 : 1;
+          break;
+        }
+      }
+    }
+    st.min_dt_bits = __float_as_uint(S.dtmax);  // sfincs_momentum.f90:99
+    if (dtchk < S.dtmin && st.nt > 1) {         // sfincs_lib.f90:634-648
+      st.error = 1;
+      st.stop_pending = 1;
+    }
+    st.run = 1;
+    if (st.steps_left > 0) st.steps_left -= 1;
+  }
+  return go;
+}
+
+// Levels at the boundary points for this step (sfincs_boundaries.f90:728-756).
+__device__ __forceinline__ void boundary_levels(const ScnDev& S, const StepState& st, int tid, int nthreads) {
   const float* z0 = S.zs_bnd + (size_t)(st.itb0 - 1) * S.nbnd;
   const float* z1 = S.zs_bnd + (size_t)(st.itb1 - 1) * S.nbnd;
   const float tbfac = st.tbfac;
-  for (int ib = threadIdx.x; ib < S.nbnd; ib += blockDim.x) S.zst_bnd[ib] = z0[ib] + (z1[ib] - z0[ib]) * tbfac;
+  for (int ib = tid; ib < S.nbnd; ib += nthreads) S.zst_bnd[ib] = z0[ib] + (z1[ib] - z0[ib]) * tbfac;
 }
 
+
 // --------------------------------------------------------------------------
-// k_bnd: boundary faces and Neumann cells; grid (items, scenarios).
+// Boundary faces and Neumann cells.
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_bnd(const ScnDev* __restrict__ scns) {
-  const ScnDev& S = scns[blockIdx.y];
-  StepState& st = *S.st;
-  if (!st.run) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One water-level boundary face (i < nkcuv2) or Neumann cell: returns its FP64
+// inflow volume this step.
+__device__ __forceinline__ double boundary_item(const ScnDev& S, StepState& st, int i) {
   double inflow = 0.0;
   if (i < S.nkcuv2) {
     const BndFace b = S.bfaces[i];
@@ -278,15 +276,41 @@ __global__ void __launch_bounds__(128) k_bnd(const ScnDev* __restrict__ scns) {
     const int2 nn = S.neu[i - S.nkcuv2];  // Neumann: zs(nmb) = zs(nmi) (sfincs_boundaries.f90:903-914)
     S.zs[nn.x] = S.zs[nn.y];
   }
-  // FP64 volume-balance accumulator of the boundary inflow
-  __shared__ double s_red[4];
+  return inflow;
+}
+
+__device__ __forceinline__ void add_inflow(StepState& st, double inflow) {
+  // FP64 volume-balance accumulator of the boundary inflow: block sum, one atomic
+  __shared__ double s_red[32];
   inflow = warp_sum(inflow);
   if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = inflow;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const double tot = s_red[0] + s_red[1] + s_red[2] + s_red[3];
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += s_red[w];
     if (tot != 0.0) atomicAdd(&st.bflux_vol, tot);
   }
+}
+
+
+// Step control, boundary point levels and all boundary faces of one scenario
+// in one CTA (one launch per step instead of two; ONE: the single scenario's
+// parameters by value).
+template <bool ONE>
+__global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ scns, const __grid_constant__ ScnDev one) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
+  const ScnDev& S = ONE ? one : scns[blockIdx.x];
+  StepState& st = *S.st;
+  __shared__ int s_go;
+  if (threadIdx.x == 0) s_go = step_control(S, st);
+  __syncthreads();
+  if (!s_go) return;
+  if (S.nbnd > 0) boundary_levels(S, st, threadIdx.x, blockDim.x);
+  __syncthreads();  // zst_bnd written by this CTA
+  double inflow = 0.0;
+  for (int i = threadIdx.x; i < S.nkcuv2 + S.nneu; i += blockDim.x) inflow += boundary_item(S, st, i);
+  add_inflow(st, inflow);
 }
 
 // --------------------------------------------------------------------------
@@ -470,6 +494,8 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepState&
 
 template <bool SG, int MINB>
 __global__ void __launch_bounds__(512, MINB) k_momentum(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
   const StepState& st = *S.st;
@@ -500,6 +526,8 @@ __global__ void __launch_bounds__(512, MINB) k_momentum(const ScnDev* __restrict
 // Point sources, applied in the reference's sequential order before the cell loop.
 // --------------------------------------------------------------------------
 __global__ void k_sources(const ScnDev* __restrict__ scns) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   const ScnDev& S = scns[blockIdx.x];
   StepState& st = *S.st;
   if (!st.run || S.nsrc == 0 || threadIdx.x != 0) return;
@@ -527,6 +555,8 @@ __global__ void k_sources(const ScnDev* __restrict__ scns) {
 // --------------------------------------------------------------------------
 template <bool SG>
 __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
   const StepState& st = *S.st;
@@ -612,9 +642,15 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
 // --------------------------------------------------------------------------
 // Host-callable launchers.
 // --------------------------------------------------------------------------
-void launch_step_bnd(const ScnDev* d_scns, int nscn, int bnd_blocks, cudaStream_t s) {
-  k_step<<<nscn, 32, 0, s>>>(d_scns);
-  if (bnd_blocks > 0) k_bnd<<<dim3(bnd_blocks, nscn), 128, 0, s>>>(d_scns);
+// One CTA per scenario: 1024 threads for the boundary faces when there are
+// many (large grids), one warp otherwise.
+void launch_step_bnd(const ScnDev* d_scns, int nscn, int bnd_blocks, cudaStream_t s, const ScnDev* one) {
+  const int threads = bnd_blocks > 1 ? 1024 : (bnd_blocks == 1 ? 128 : 32);
+  static const ScnDev none{};
+  if (one)
+    launch_pdl(k_step_bnd<true>, dim3(1), dim3(threads), 0, s, d_scns, *one);
+  else
+    launch_pdl(k_step_bnd<false>, dim3(nscn), dim3(threads), 0, s, d_scns, none);
 }
 
 // variant: CTAs per SM the register allocation is sized for (2: no spills, 3: 40 registers)
@@ -624,31 +660,33 @@ void launch_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int 
   const dim3 blk(32, 8, 2);
   if (subgrid) {
     if (variant == 3)
-      k_momentum<true, 3><<<ntiles, blk, 0, s>>>(d_scns, d_tiles);
+      launch_pdl(k_momentum<true, 3>, dim3(ntiles), dim3(blk), 0, s, d_scns, d_tiles);
     else
-      k_momentum<true, 2><<<ntiles, blk, 0, s>>>(d_scns, d_tiles);
+      launch_pdl(k_momentum<true, 2>, dim3(ntiles), dim3(blk), 0, s, d_scns, d_tiles);
   } else {
     if (variant == 3)
-      k_momentum<false, 3><<<ntiles, blk, 0, s>>>(d_scns, d_tiles);
+      launch_pdl(k_momentum<false, 3>, dim3(ntiles), dim3(blk), 0, s, d_scns, d_tiles);
     else
-      k_momentum<false, 2><<<ntiles, blk, 0, s>>>(d_scns, d_tiles);
+      launch_pdl(k_momentum<false, 2>, dim3(ntiles), dim3(blk), 0, s, d_scns, d_tiles);
   }
 }
 
-void launch_sources(const ScnDev* d_scns, int nscn, cudaStream_t s) { k_sources<<<nscn, 32, 0, s>>>(d_scns); }
+void launch_sources(const ScnDev* d_scns, int nscn, cudaStream_t s) {
+  launch_pdl(k_sources, dim3(nscn), dim3(32), 0, s, d_scns);
+}
 
 void launch_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {
   if (ntiles <= 0) return;
   const dim3 blk(32, 8);
   if (subgrid)
-    k_continuity<true><<<ntiles, blk, 0, s>>>(d_scns, d_tiles);
+    launch_pdl(k_continuity<true>, dim3(ntiles), dim3(blk), 0, s, d_scns, d_tiles);
   else
-    k_continuity<false><<<ntiles, blk, 0, s>>>(d_scns, d_tiles);
+    launch_pdl(k_continuity<false>, dim3(ntiles), dim3(blk), 0, s, d_scns, d_tiles);
 }
 
 void launch_step(const ScnDev* d_scns, int nscn, int bnd_blocks, const Tile* d_tiles, int ntiles, int subgrid,
                  int any_src, int variant, cudaStream_t s) {
-  launch_step_bnd(d_scns, nscn, bnd_blocks, s);
+  launch_step_bnd(d_scns, nscn, bnd_blocks, s, nullptr);
   launch_momentum(d_scns, d_tiles, ntiles, subgrid, variant, s);
   if (any_src) launch_sources(d_scns, nscn, s);
   launch_continuity(d_scns, d_tiles, ntiles, subgrid, s);

@@ -11,6 +11,7 @@
 #include <cstdint>
 
 #include "face_math.h"
+#include "pdl.h"
 #include "sfg_device.h"
 
 namespace sfg {
@@ -29,6 +30,8 @@ __device__ __forceinline__ float qt_warp_max(float v) {
 // (kcuv 0, boundary faces) are left alone.
 template <bool SG>
 __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
   StepState& st = *S.st;
@@ -138,6 +141,8 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
 
 // Combined uv points: mean of the two fine faces (sfincs_momentum.f90:757-779).
 __global__ void __launch_bounds__(256) k_qt_cuv(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
   const StepState& st = *S.st;
@@ -156,6 +161,8 @@ __global__ void __launch_bounds__(256) k_qt_cuv(const ScnDev* __restrict__ scns,
 template <bool SG>
 __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict__ scns,
                                                         const Tile* __restrict__ tiles) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
   const StepState& st = *S.st;
@@ -227,19 +234,19 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
 void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {
   if (ntiles <= 0) return;
   if (subgrid)
-    k_qt_momentum<true><<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+    launch_pdl(k_qt_momentum<true>, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
   else
-    k_qt_momentum<false><<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+    launch_pdl(k_qt_momentum<false>, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
 }
 void launch_qt_cuv(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, cudaStream_t s) {
-  if (ntiles > 0) k_qt_cuv<<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+  if (ntiles > 0) launch_pdl(k_qt_cuv, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
 }
 void launch_qt_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {
   if (ntiles <= 0) return;
   if (subgrid)
-    k_qt_continuity<true><<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+    launch_pdl(k_qt_continuity<true>, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
   else
-    k_qt_continuity<false><<<ntiles, 256, 0, s>>>(d_scns, d_tiles);
+    launch_pdl(k_qt_continuity<false>, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
 }
 
 }  // namespace sfg

@@ -20,6 +20,7 @@
 #include <cstdint>
 
 #include "face_math.h"
+#include "pdl.h"
 #include "sfg_device.h"
 
 namespace sfg {
@@ -180,6 +181,8 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
                                                             const MapSet* __restrict__ maps,
                                                             const Tile* __restrict__ tiles, int ntiles,
                                                             const __grid_constant__ ScnDev one) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_issued[2];
@@ -437,6 +440,8 @@ template <bool SG, bool ONE>
 __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict__ scns, const MapSet* __restrict__ maps,
                                                         const Tile* __restrict__ tiles, int ntiles,
                                                         const __grid_constant__ ScnDev one) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_issued[2];
@@ -572,7 +577,8 @@ const void* continuity_tma_fn(int subgrid, bool one) {
 template <bool SG, int MINB, bool ONE>
 static void mom_launch(int grid, cudaStream_t s, const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles,
                        int ntiles, const ScnDev& one) {
-  k_momentum_tma<SG, MINB, ONE><<<grid, dim3(32, 8), 2 * mom::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, one);
+  launch_pdl(k_momentum_tma<SG, MINB, ONE>, dim3(grid), dim3(32, 8), 2 * mom::STAGE, s, d_scns, d_maps, d_tiles, ntiles,
+             one);
 }
 
 void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
@@ -606,14 +612,14 @@ void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Til
   const dim3 blk(32, 8);
   if (one) {
     if (subgrid)
-      k_continuity_tma<true, true><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, o);
+      launch_pdl(k_continuity_tma<true, true>, dim3(grid), dim3(blk), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, o);
     else
-      k_continuity_tma<false, true><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, o);
+      launch_pdl(k_continuity_tma<false, true>, dim3(grid), dim3(blk), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, o);
   } else {
     if (subgrid)
-      k_continuity_tma<true, false><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, o);
+      launch_pdl(k_continuity_tma<true, false>, dim3(grid), dim3(blk), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, o);
     else
-      k_continuity_tma<false, false><<<grid, blk, 2 * con::STAGE, s>>>(d_scns, d_maps, d_tiles, ntiles, o);
+      launch_pdl(k_continuity_tma<false, false>, dim3(grid), dim3(blk), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, o);
   }
 }
 
