@@ -314,6 +314,7 @@ int update(void) {
     g_bmi->before_update();
     g_bmi->runner->step_once();
     g_bmi->after_update();
+    g_bmi->runner->sync();  // the step is complete when update() returns, as in the reference
     return 0;
   });
 }

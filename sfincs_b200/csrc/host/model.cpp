@@ -974,6 +974,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
     configure_grids();
   }
   check_cuda(cudaMallocHost(&h_states_, models_.size() * sizeof(StepState)), "pinned states");
+  check_cuda(cudaMallocHost(&h_ctl_, models_.size() * sizeof(RunCtl)), "pinned run targets");
 }
 
 // Persistent grids of the TMA kernels: resident CTAs per SM x SM count, capped
@@ -1000,6 +1001,7 @@ Runner::~Runner() {
   if (d_scns_) cudaFree(d_scns_);
   if (d_tiles_) cudaFree(d_tiles_);
   if (h_states_) cudaFreeHost(h_states_);
+  if (h_ctl_) cudaFreeHost(h_ctl_);
 }
 
 void Runner::launch_momentum_any() {
@@ -1023,7 +1025,7 @@ void Runner::launch_continuity_any() {
 }
 
 void Runner::launch_one() {
-  launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
+  launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_, one());
   launch_momentum_any();
   if (any_src_) launch_sources(d_scns_, nscn(), stream_);
   launch_continuity_any();
@@ -1073,7 +1075,7 @@ std::vector<double> Runner::time_kernels(int nsteps) {
   std::vector<double> acc(4, 0.0);
   for (int i = 0; i < nsteps; i++) {
     check_cuda(cudaEventRecord(ev[0], stream_), "record");
-    launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_);
+    launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_, one());
     check_cuda(cudaEventRecord(ev[1], stream_), "record");
     launch_momentum_any();
     check_cuda(cudaEventRecord(ev[2], stream_), "record");
@@ -1103,15 +1105,20 @@ StepState Runner::read_state(int i) {
 }
 
 void Runner::step_once() {
-  for (auto* m : models_) {
-    const double tend = m->host().t1;
-    const int one = 1;
-    check_cuda(cudaMemcpyAsync(&m->state()->tend, &tend, sizeof(double), cudaMemcpyHostToDevice, stream_), "tend");
-    check_cuda(cudaMemcpyAsync(&m->state()->steps_left, &one, sizeof(int), cudaMemcpyHostToDevice, stream_), "steps");
+  // run targets from pinned memory (no pageable round trip); the step is then
+  // stream-ordered before whatever the caller queues next (e.g. the zs refresh)
+  for (size_t i = 0; i < models_.size(); i++) {
+    h_ctl_[i].tend = models_[i]->host().t1;
+    h_ctl_[i].steps_left = 1;
+    check_cuda(cudaMemcpyAsync(&models_[i]->state()->tend, &h_ctl_[i].tend, sizeof(double), cudaMemcpyHostToDevice,
+                               stream_),
+               "tend");
+    check_cuda(cudaMemcpyAsync(&models_[i]->state()->steps_left, &h_ctl_[i].steps_left, sizeof(int),
+                               cudaMemcpyHostToDevice, stream_),
+               "steps");
   }
   issue(1);
   check_cuda(cudaGetLastError(), "step launch");
-  sync();
 }
 
 // Autotuner: times one chunk of real steps with each kernel variant on this

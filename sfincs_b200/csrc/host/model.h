@@ -141,7 +141,7 @@ class Runner {
   int autotune(int chunk = 32);
   void set_autotune(bool on) { autotune_ = on; }
   const std::vector<std::pair<int, float>>& tune_ms() const { return tune_ms_; }
-  // One step exactly (reference update()).
+  // One step exactly (reference update()); queued on the stream, not waited for.
   void step_once();
   void sync();
   cudaStream_t stream() const { return stream_; }
@@ -200,13 +200,18 @@ class Runner {
   cudaGraphExec_t graph_ = nullptr;
   int graph_chunk_ = 0;
   StepState* h_states_ = nullptr;  // pinned mirror of the step states
+  struct RunCtl {
+    double tend;
+    int steps_left;
+  };
+  RunCtl* h_ctl_ = nullptr;  // pinned run targets of step_once()
   bool autotune_ = false, tuned_ = false;
   std::vector<std::pair<int, float>> tune_ms_;  // (variant, ms per chunk) of the last autotune
 };
 
 void launch_step(const ScnDev* d_scns, int nscn, int bnd_blocks, const Tile* d_tiles, int ntiles, int subgrid,
                  int any_src, int variant, cudaStream_t s);
-void launch_step_bnd(const ScnDev* d_scns, int nscn, int bnd_blocks, cudaStream_t s);
+void launch_step_bnd(const ScnDev* d_scns, int nscn, int bnd_blocks, cudaStream_t s, const ScnDev* one);
 void launch_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, int variant,
                      cudaStream_t s);
 void launch_sources(const ScnDev* d_scns, int nscn, cudaStream_t s);
