@@ -224,7 +224,7 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, StepState& st, 
         depthuv = (isv ? S.sgw_v[b.face] : S.sgw_u[b.face]).x + zsuv;
       } else if (zsuv > zr.x) {
         const float dzuv = (zr.y - zr.x) / (float)(S.nlev - 1);
-        const int iuv = (int)((zsuv - zr.x) / dzuv) + 1;
+        const int iuv = lev_index((zsuv - zr.x) / dzuv, S.nlev);
         const float facint = (zsuv - (zr.x + (float)(iuv - 1) * dzuv)) / dzuv;
         const UvRec r = (isv ? S.rec_v : S.rec_u)[(int64_t)(iuv - 1) * S.nalloc + b.face];
         depthuv = r.havg + r.dhavg * facint;
@@ -382,8 +382,7 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepState&
       gnavg2 = w.z - (w.z - w.y) / (w.w * (zsu - zmax) + 1.0f);
     } else {  // sfincs_momentum.f90:372-378
       const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
-      int iuv = (int)((zsu - zmin) / dzuv) + 1;
-      iuv = min(iuv, S.nlev - 1);
+      const int iuv = lev_index((zsu - zmin) / dzuv, S.nlev);
       const float facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
       const UvRec r = (DIR == 0 ? S.rec_u : S.rec_v)[(int64_t)(iuv - 1) * S.nalloc + c];
       hu = r.havg + r.dhavg * facint;
@@ -612,7 +611,7 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
         zsn = fmaxf(S.zz_min[c], -20.0f);
       } else {
         const float dzvol = volmax / (float)(S.nlev - 1);
-        const int iuv = (int)(v / (double)dzvol) + 1;
+        const int iuv = lev_index(v / (double)dzvol, S.nlev);
         const float facint = (float)((v - (double)((float)(iuv - 1) * dzvol)) / (double)dzvol);
         const float2 dep = S.zlev[(int64_t)(iuv - 1) * S.nalloc + c];
         zsn = dep.x + dep.y * facint;

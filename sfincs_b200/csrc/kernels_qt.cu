@@ -101,8 +101,7 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
             gnavg2 = w.z - (w.z - w.y) / (w.w * (zsu - zmax) + 1.0f);
           } else {
             const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
-            int iuv = (int)((zsu - zmin) / dzuv) + 1;
-            iuv = min(iuv, S.nlev - 1);
+            const int iuv = lev_index((zsu - zmin) / dzuv, S.nlev);
             const float facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
             const UvRec r = S.rec_u[(int64_t)(iuv - 1) * S.nalloc + i];
             hu = r.havg + r.dhavg * facint;
@@ -204,7 +203,7 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
         zsn = fmaxf(S.zz_min[c], -20.0f);
       } else {
         const float dzvol = volmax / (float)(S.nlev - 1);
-        const int iuv = (int)(v / (double)dzvol) + 1;
+        const int iuv = lev_index(v / (double)dzvol, S.nlev);
         const float facint = (float)((v - (double)((float)(iuv - 1) * dzvol)) / (double)dzvol);
         const float2 dep = S.zlev[(int64_t)(iuv - 1) * S.npc + c];
         zsn = dep.x + dep.y * facint;

@@ -272,8 +272,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
             } else {
               L.full = false;
               const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
-              int iuv = (int)((zsu - zmin) / dzuv) + 1;
-              iuv = min(iuv, S.nlev - 1);
+              const int iuv = lev_index((zsu - zmin) / dzuv, S.nlev);
               L.facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
               L.r = R[(int64_t)(iuv - 1) * S.nalloc + c];
             }
@@ -519,7 +518,7 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
                 zsn = fmaxf(S.zz_min[c], -20.0f);
               } else {
                 const float dzvol = volmax / (float)(S.nlev - 1);
-                const int iuv = (int)(v / (double)dzvol) + 1;
+                const int iuv = lev_index(v / (double)dzvol, S.nlev);
                 const float facint = (float)((v - (double)((float)(iuv - 1) * dzvol)) / (double)dzvol);
                 const float2 dep = S.zlev[(int64_t)(iuv - 1) * S.nalloc + c];
                 zsn = dep.x + dep.y * facint;

@@ -212,4 +212,16 @@ struct alignas(64) MapSet {
   unsigned char m[NUM_MAPS][128];  // CUtensorMap objects (opaque, 128 bytes each)
 };
 
+#ifdef __CUDACC__
+// 1-based table interval int(x) + 1 of a subgrid lookup (sfincs_momentum.f90:
+// 372-378, sfincs_continuity.f90:566), clamped to [1, nlev - 1].  For every
+// finite x that the callers' guards let through the interval is already in
+// that range, so the clamp changes no result.  It matters for non-finite state
+// after a model has gone unstable: the guards pass NaN to the interval branch,
+// and an f64 NaN converts to INT_MIN (an f32 NaN to 0), which would otherwise
+// index far outside the table.
+__device__ __forceinline__ int lev_index(float x, int nlev) { return min(max((int)x + 1, 1), nlev - 1); }
+__device__ __forceinline__ int lev_index(double x, int nlev) { return min(max((int)x + 1, 1), nlev - 1); }
+#endif
+
 }  // namespace sfg
