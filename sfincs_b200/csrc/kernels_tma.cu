@@ -169,11 +169,13 @@ __device__ __forceinline__ float face_flux(const ScnDev& S, const StepState& st,
 }
 
 // Subgrid depth / roughness / wet fraction at the face level zsu (sfincs_momentum.f90:345-380).
+// full (zsu above the table): v = (havg_zmax, nrep_zmax, navg_w, fnfit) of the face;
+// otherwise v = (havg, dhavg, nrep, dnrep) and v2 = (pwet, dpwet) of level interval iuv.
 struct SgLook {
-  bool full;
+  float4 v;
+  float2 v2;
   float facint;
-  float4 w;   // full branch
-  UvRec r;    // interpolation branch
+  bool full;
 };
 
 template <bool SG, int MINB, bool ONE>
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
     fence_barrier_init();
   }
   __syncthreads();
-  uint32_t phase[2] = {0u, 0u};
+  uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
   int tile = blockIdx.x;
   // running CFL denominator of this thread's faces, for scenario cfl_st
   StepState* cfl_st = nullptr;
@@ -222,8 +224,8 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
         cfl_st = &st;
         cfl_den = 0.0f;
       }
-      const bool ok = mbar_wait_bounded(&bar[s], phase[s]);
-      phase[s] ^= 1u;
+      const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u);
+      phase ^= 1u << s;
       const int n = tl.n0 + tx, m = tl.m0 + ty;
       if (!ok) {
         st.fault = 1;
@@ -266,16 +268,17 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
         if (SG) {
           auto look = [&](bool wet, float zsu, float zmin, float zmax, const float4* W, const UvRec* R, SgLook& L) {
             if (!wet) return;
-            if (zsu > zmax) {
-              L.full = true;
-              L.w = W[c];
-            } else {
-              L.full = false;
+            L.full = zsu > zmax;
+            const float4* src = W + c;
+            if (!L.full) {
               const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
               const int iuv = lev_index((zsu - zmin) / dzuv, S.nlev);
               L.facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
-              L.r = R[(int64_t)(iuv - 1) * S.nalloc + c];
+              const UvRec* r = R + (int64_t)(iuv - 1) * S.nalloc + c;
+              src = reinterpret_cast<const float4*>(r);
+              L.v2 = *reinterpret_cast<const float2*>(&r->pwet);
             }
+            L.v = *src;
           };
           look(wet_u, zsu_u, zmin_u, zmax_u, S.sgw_u, S.rec_u, lu);
           look(wet_v, zsu_v, zmin_v, zmax_v, S.sgw_v, S.rec_v, lv);
@@ -310,12 +313,12 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
                 zd1 = zd[(ty + 1) * mom::W_ZS + tx];
               }
               if (lu.full) {
-                hu = lu.w.x + zsu_u;
-                gnavg2 = lu.w.z - (lu.w.z - lu.w.y) / (lu.w.w * (zsu_u - zmax_u) + 1.0f);
+                hu = lu.v.x + zsu_u;
+                gnavg2 = lu.v.z - (lu.v.z - lu.v.y) / (lu.v.w * (zsu_u - zmax_u) + 1.0f);
               } else {
-                hu = lu.r.havg + lu.r.dhavg * lu.facint;
-                gnavg2 = lu.r.nrep + lu.r.dnrep * lu.facint;
-                phi = lu.r.pwet + lu.r.dpwet * lu.facint;
+                hu = lu.v.x + lu.v.y * lu.facint;
+                gnavg2 = lu.v.z + lu.v.w * lu.facint;
+                phi = lu.v2.x + lu.v2.y * lu.facint;
               }
             } else {
               const float* zb = (const float*)(sm + mom::O_ZB);
@@ -366,12 +369,12 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
                 zd1 = zd[ty * mom::W_ZS + tx + 1];
               }
               if (lv.full) {
-                hu = lv.w.x + zsu_v;
-                gnavg2 = lv.w.z - (lv.w.z - lv.w.y) / (lv.w.w * (zsu_v - zmax_v) + 1.0f);
+                hu = lv.v.x + zsu_v;
+                gnavg2 = lv.v.z - (lv.v.z - lv.v.y) / (lv.v.w * (zsu_v - zmax_v) + 1.0f);
               } else {
-                hu = lv.r.havg + lv.r.dhavg * lv.facint;
-                gnavg2 = lv.r.nrep + lv.r.dnrep * lv.facint;
-                phi = lv.r.pwet + lv.r.dpwet * lv.facint;
+                hu = lv.v.x + lv.v.y * lv.facint;
+                gnavg2 = lv.v.z + lv.v.w * lv.facint;
+                phi = lv.v2.x + lv.v2.y * lv.facint;
               }
             } else {
               const float* zb = (const float*)(sm + mom::O_ZB);
@@ -452,7 +455,7 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
     fence_barrier_init();
   }
   __syncthreads();
-  uint32_t phase[2] = {0u, 0u};
+  uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
   int tile = blockIdx.x;
   if (tid == 0)
     s_issued[0] = tile < ntiles ? issue_continuity<SG>(scn_of<ONE>(scns, one, tiles[tile].scn), maps, tiles[tile],
@@ -472,8 +475,8 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
       const Tile tl = tiles[tile];
       const ScnDev& S = scn_of<ONE>(scns, one, tl.scn);
       StepState& st = *S.st;
-      const bool ok = mbar_wait_bounded(&bar[s], phase[s]);
-      phase[s] ^= 1u;
+      const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u);
+      phase ^= 1u << s;
       const int n = tl.n0 + tx, m = tl.m0 + ty;
       if (!ok) {
         st.fault = 1;
