@@ -28,7 +28,7 @@ struct FaceV {
 // minimum equals 1/max(den) bit for bit and one division per CTA replaces one
 // per face.
 template <bool SG>
-__device__ __forceinline__ float face_flux_geo(const ScnDev& S, const StepState& st, int dir, bool adv_on,
+__device__ __forceinline__ float face_flux_geo(const ScnDev& S, const StepVals& st, int dir, bool adv_on,
                                                bool theta_on, const FaceGeo& geo, uint8_t kf, float zs_nm,
                                                float zs_nmu, float hu, float gnavg2, float phi, const FaceV& a,
                                                bool dry_nm, bool dry_nmu, float zd_nm, float zd_nmu, float& q_out,

@@ -35,6 +35,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "face_math.h"
 #include "pdl.h"
 #include "sfg_device.h"
 
@@ -317,7 +318,8 @@ __global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ sc
 // k_momentum: one thread per uv face.
 // --------------------------------------------------------------------------
 template <bool SG, int DIR>
-__device__ __forceinline__ float momentum_face(const ScnDev& S, const StepState& st, int p, int64_t c) {
+__device__ __forceinline__ float momentum_face(const ScnDev& S, const StepVals& sv, int64_t c) {
+  const int p = sv.parity;
   const int64_t ld = S.ld;
   const int64_t du = DIR == 0 ? ld : 1;  // to the cell across the face (nmu)
   const int64_t dq = DIR == 0 ? 1 : ld;  // transverse direction
@@ -395,100 +397,34 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepState&
     hu = fmaxf(zsu - zmin, S.huthresh);
     gnavg2 = (DIR == 0 ? S.gn2_u : S.gn2_v)[c];
   }
-  const float dxuvinv = DIR == 0 ? S.dxinv : S.dyinv;
-  const float dyuvinv = DIR == 0 ? S.dyinv : S.dxinv;
-  const float dxuv2inv = DIR == 0 ? S.dx2inv : S.dy2inv;
-  const float dyuv2inv = DIR == 0 ? S.dy2inv : S.dx2inv;
-  const float vu = (v0 + v1 + v2 + v3) / 4.0f;
-  const float hwet = hu / phi;
-  // ---- forcing terms (sfincs_momentum.f90:399-608)
-  float dzdx;
-  if (S.slopelim < 9999.0f)
-    dzdx = fminf(fmaxf((zs_nmu - zs_nm) * dxuvinv, -S.slopelim), S.slopelim);
-  else
-    dzdx = (zs_nmu - zs_nm) * dxuvinv;
-  float frc = -S.g * hu * dzdx;
-  if (S.advection && (f & ADV)) {
-    float dqxudx = 0.0f, dqyudy = 0.0f;
-    if (S.adv_scheme == 0) {
-      if (qx_nm > 1.0e-6f)
-        dqxudx = (qx_nm * uu_nm - qx_nmd * uu_nmd) * dxuvinv;
-      else if (qx_nm < -1.0e-6f)
-        dqxudx = (qx_nmu * uu_nmu - qx_nm * uu_nm) * dxuvinv;
-      const float qy = qy_ndm + qy_ndmu + qy_nm + qy_nmu;
-      if (qy > 1.0e-6f)
-        dqyudy = (qy_ndm + qy_ndmu) * (uu_nm - uu_ndm) * dyuvinv / 2.0f;
-      else if (qy < -1.0e-6f)
-        dqyudy = (qy_nm + qy_nmu) * (uu_num - uu_nm) * dyuvinv / 2.0f;
-    } else {
-      float qd = (qx_nmd + qx_nm) / 2.0f;
-      float qu = (qx_nm + qx_nmu) / 2.0f;
-      if (qd > 1.0e-6f) {
-        const float ud = (uu_nmd + uu_nm) / 2.0f;
-        dqxudx = (qd * (uu_nm - uu_nmd) + ud * (qx_nm - qx_nmd)) * dxuvinv;
-      }
-      if (qu < -1.0e-6f) {
-        const float uu = (uu_nm + uu_nmu) / 2.0f;
-        dqxudx = dqxudx + (qu * (uu_nmu - uu_nm) + uu * (qx_nmu - qx_nm)) * dxuvinv;
-      }
-      qu = (qy_nm + qy_nmu) / 2.0f;
-      qd = (qy_ndm + qy_ndmu) / 2.0f;
-      if (qd > 1.0e-6f) dqyudy = qd * (uu_nm - uu_ndm) * dyuvinv;
-      if (qu < -1.0e-6f) dqyudy = dqyudy + qu * (uu_num - uu_nm) * dyuvinv;
-      const float ud = (uu_nmd + uu_nm) / 2.0f;
-      const float uu = (uu_nm + uu_nmu) / 2.0f;
-      if (ud > 1.0e-6f) dqyudy = dqyudy + ud * (qy_nm - qy_ndm) * dyuvinv;
-      if (uu < -1.0e-6f) dqyudy = dqyudy + uu * (qy_nmu - qy_ndmu) * dyuvinv;
-    }
-    float adv = -phi * (dqxudx + dqyudy);
-    adv = fminf(fmaxf(adv, -S.advlim * hu), S.advlim * hu);
-    frc = frc + adv;
-  }
-  if (S.viscosity) {
-    frc = frc + S.nuvisc * hu *
-                    ((uu_nmu - 2.0f * uu_nm + uu_nmd) * dxuv2inv + (uu_num - 2.0f * uu_nm + uu_ndm) * dyuv2inv);
-  }
-  if (S.coriolis) {  // sfincs_momentum.f90:533-545
-    if (DIR == 0)
-      frc = frc + S.fcorio * hu * vu;
-    else
-      frc = frc - S.fcorio * hu * vu;
-  }
-  if (S.wind) {
-    const float tauw = DIR == 0 ? st.twu : st.twv;
-    if (hwet > 0.25f)
-      frc = frc + phi * tauw;
-    else
-      frc = frc + tauw * hu * 4.0f;
-  }
-  // ---- friction and the new flux (sfincs_momentum.f90:612-724)
-  float qfr;
-  if (!(kf & KF_WET)) {
-    qfr = sqrtf(fabsf(dzdx) / (fmaxf(gnavg2, 1.0e-5f) / 10.0f)) * powf(hu, 5.0f / 3.0f);
-  } else if (S.friction2d) {
-    qfr = sqrtf(qx_nm * qx_nm + (hu * vu) * (hu * vu));
-  } else {
-    qfr = fabsf(qx_nm);
-  }
-  float qsm = qx_nm;
-  if (S.thetasmooth && (f & TH) && fabsf(qx_nmd) > 1.0e-6f && fabsf(qx_nmu) > 1.0e-6f)
-    qsm = S.theta * qx_nm + 0.5f * (1.0f - S.theta) * (qx_nmu + qx_nmd);
-  const float dt = st.dt;
-  const float hu73 = hu * hu * cbrtf(hu);  // as in kernels_tma.cu: cube root for hu**(1.0/3.0)
-  float q = (qsm + frc * dt) / (1.0f + gnavg2 * dt * qfr / hu73);
-  if (SG && S.wiggle) {
-    const float mdrv = fabsf(zd_nm - zd_nmu) - S.wiggle_threshold;
-    if (mdrv > 0.0f) q = q * S.wiggle_threshold / (S.wiggle_factor * mdrv + S.wiggle_threshold);
-  }
-  if (dry_nm) q = fminf(q, 0.0f);
-  if (dry_nmu) q = fmaxf(q, 0.0f);
-  q = fminf(fmaxf(q, -hu * S.uvlim), hu * S.uvlim);
-  const float uv = q / fmaxf(hu, S.huvmin);
+  FaceGeo geo;
+  geo.dxuvinv = DIR == 0 ? S.dxinv : S.dyinv;
+  geo.dyuvinv = DIR == 0 ? S.dyinv : S.dxinv;
+  geo.dxuv2inv = DIR == 0 ? S.dx2inv : S.dy2inv;
+  geo.dyuv2inv = DIR == 0 ? S.dy2inv : S.dx2inv;
+  geo.nuvisc = S.nuvisc;
+  FaceV a;
+  a.qx_nm = qx_nm;
+  a.qx_nmd = qx_nmd;
+  a.qx_nmu = qx_nmu;
+  a.qy_nm = qy_nm;
+  a.qy_nmu = qy_nmu;
+  a.qy_ndm = qy_ndm;
+  a.qy_ndmu = qy_ndmu;
+  a.uu_nm = uu_nm;
+  a.uu_nmd = uu_nmd;
+  a.uu_nmu = uu_nmu;
+  a.uu_ndm = uu_ndm;
+  a.uu_num = uu_num;
+  a.vu = (v0 + v1 + v2 + v3) / 4.0f;
+  float q, uv;
+  const float den = face_flux_geo<SG>(S, sv, DIR, (f & ADV) != 0, (f & TH) != 0, geo, kf, zs_nm, zs_nmu, hu, gnavg2,
+                                      phi, a, dry_nm, dry_nmu, zd_nm, zd_nmu, q, uv);
   Qn[c] = q;
   Un[c] = uv;
   const uint8_t kfn = (uint8_t)(KF_WET | ((kf & KF_WET) ? KF_WET2 : 0));
   if (kfn != kf) kfp[c] = kfn;
-  return 1.0f / (fmaxf(sqrtf(S.g * hu), fabsf(uv)) * dxuvinv);  // sfincs_momentum.f90:731
+  return 1.0f / den;  // sfincs_momentum.f90:731
 }
 
 template <bool SG, int MINB>
@@ -499,13 +435,13 @@ __global__ void __launch_bounds__(512, MINB) k_momentum(const ScnDev* __restrict
   const ScnDev& S = scns[tl.scn];
   const StepState& st = *S.st;
   if (!st.run) return;
-  const int p = st.parity;
+  const StepVals sv = step_vals(st);
   const int n = tl.n0 + threadIdx.x;
   const int m = tl.m0 + threadIdx.y;
   float mdt = FLT_MAX;
   if (n <= S.nmax && m <= S.mmax) {
     const int64_t c = off(S, n, m);
-    mdt = threadIdx.z == 0 ? momentum_face<SG, 0>(S, st, p, c) : momentum_face<SG, 1>(S, st, p, c);
+    mdt = threadIdx.z == 0 ? momentum_face<SG, 0>(S, sv, c) : momentum_face<SG, 1>(S, sv, c);
   }
   // CTA min of the CFL time step, then one atomicMin per CTA (float bits of a positive value)
   __shared__ float s_min[16];

@@ -36,7 +36,8 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
   const ScnDev& S = scns[tl.scn];
   StepState& st = *S.st;
   if (!st.run) return;
-  const int p = st.parity;
+  const StepVals sv = step_vals(st);
+  const int p = sv.parity;
   const float* __restrict__ q0 = S.qu[p];
   const float* __restrict__ uv0 = S.uu[p];
   float* q1 = S.qu[p ^ 1];
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
           dry1 = zs_nmu < S.zb[f.nmu];
         }
         float qn, un;
-        den = face_flux_geo<SG>(S, st, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kfuv[i], zs_nm,
+        den = face_flux_geo<SG>(S, sv, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kfuv[i], zs_nm,
                                 zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, qn, un);
         q1[i] = qn;
         uv1[i] = un;

@@ -152,7 +152,7 @@ __device__ __forceinline__ bool issue_momentum(const ScnDev& S, const MapSet* ma
 // Regular-grid face of direction DIR: spacing and switches from the scenario
 // and the cell's flag bits.
 template <bool SG, int DIR>
-__device__ __forceinline__ float face_flux(const ScnDev& S, const StepState& st, uint16_t f, uint8_t kf, float zs_nm,
+__device__ __forceinline__ float face_flux(const ScnDev& S, const StepVals& st, uint16_t f, uint8_t kf, float zs_nm,
                                            float zs_nmu, float hu, float gnavg2, float phi, const FaceV& a,
                                            bool dry_nm, bool dry_nmu, float zd_nm, float zd_nmu, float& q_out,
                                            float& uv_out) {
@@ -178,6 +178,8 @@ struct SgLook {
   bool full;
 };
 
+// Thread 0 reads each tile's header when it issues the tile's loads and passes
+// it on through shared memory; the step scalars are read once per scenario.
 template <bool SG, int MINB, bool ONE>
 __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __restrict__ scns,
                                                             const MapSet* __restrict__ maps,
@@ -188,41 +190,48 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_issued[2];
+  __shared__ Tile s_tile[2];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + 32 * ty;
+  int tile = blockIdx.x;
+  // thread 0: load tile t into stage k
+  auto issue = [&](int t, int k) {
+    if (t < ntiles) {
+      const Tile tn = tiles[t];
+      s_tile[k] = tn;
+      s_issued[k] = issue_momentum<SG>(scn_of<ONE>(scns, one, tn.scn), maps, tn, smem + k * mom::STAGE, &bar[k]);
+    } else {
+      s_issued[k] = 0;
+    }
+  };
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     fence_barrier_init();
+    issue(tile, 0);
   }
-  __syncthreads();
   uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
-  int tile = blockIdx.x;
-  // running CFL denominator of this thread's faces, for scenario cfl_st
+  // running CFL denominator of this thread's faces and the step scalars, for scenario cfl_st
   StepState* cfl_st = nullptr;
+  StepVals sv{};
   float cfl_den = 0.0f;
-  if (tid == 0)
-    s_issued[0] = tile < ntiles ? issue_momentum<SG>(scn_of<ONE>(scns, one, tiles[tile].scn), maps, tiles[tile],
-                                                     smem, &bar[0])
-                                : 0;
   for (int it = 0; tile < ntiles; it++) {
     const int s = it & 1;
     const int next = tile + gridDim.x;
-    __syncthreads();  // s_issued[s] visible; stage s^1 no longer read
+    __syncthreads();  // s_issued[s] and s_tile[s] visible; stage s^1 no longer read
     if (tid == 0) {
       fence_proxy_async();
-      s_issued[s ^ 1] = next < ntiles ? issue_momentum<SG>(scn_of<ONE>(scns, one, tiles[next].scn), maps,
-                                                           tiles[next], smem + (s ^ 1) * mom::STAGE, &bar[s ^ 1])
-                                      : 0;
+      issue(next, s ^ 1);
     }
     if (s_issued[s]) {
-      const Tile tl = tiles[tile];
+      const Tile tl = s_tile[s];
       const ScnDev& S = scn_of<ONE>(scns, one, tl.scn);
       StepState& st = *S.st;
       if (&st != cfl_st) {  // the tile's scenario changed (CTA-uniform)
         flush_cfl(cfl_st, cfl_den, tx);
         cfl_st = &st;
         cfl_den = 0.0f;
+        sv = step_vals(st);
       }
       const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u);
       phase ^= 1u << s;
@@ -245,7 +254,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
         const uint8_t kfu = (sm + mom::O_KFU)[ty * 32 + tx];
         const uint8_t kfv = (sm + mom::O_KFV)[ty * 32 + tx];
         const int64_t c = (int64_t)m * S.ld + kGhostPad + n;
-        const int p = st.parity;
+        const int p = sv.parity;
         const float zs_c = ZS(0, 0), zs_u = ZS(1, 0), zs_v = ZS(0, 1);
         const float zsu_u = fmaxf(zs_c, zs_u), zsu_v = fmaxf(zs_c, zs_v);
         float zmin_u, zmax_u = 0.0f, zmin_v, zmax_v = 0.0f;
@@ -327,7 +336,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               hu = fmaxf(zsu_u - zmin_u, S.huthresh);
               gnavg2 = ((const float*)(sm + mom::O_GN2U))[ty * 32 + tx];
             }
-            cfl_den = fmaxf(cfl_den, face_flux<SG, 0>(S, st, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1,
+            cfl_den = fmaxf(cfl_den, face_flux<SG, 0>(S, sv, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1,
                                                       zd0, zd1, qn, un));
             S.qu[p ^ 1][c] = qn;
             S.uu[p ^ 1][c] = un;
@@ -383,7 +392,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               hu = fmaxf(zsu_v - zmin_v, S.huthresh);
               gnavg2 = ((const float*)(sm + mom::O_GN2V))[ty * 32 + tx];
             }
-            cfl_den = fmaxf(cfl_den, face_flux<SG, 1>(S, st, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1,
+            cfl_den = fmaxf(cfl_den, face_flux<SG, 1>(S, sv, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1,
                                                       zd0, zd1, qn, un));
             S.qv[p ^ 1][c] = qn;
             S.vv[p ^ 1][c] = un;
@@ -447,34 +456,45 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_issued[2];
+  __shared__ Tile s_tile[2];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + 32 * ty;
+  int tile = blockIdx.x;
+  // thread 0: load tile t into stage k (the header travels to the other threads through shared memory)
+  auto issue = [&](int t, int k) {
+    if (t < ntiles) {
+      const Tile tn = tiles[t];
+      s_tile[k] = tn;
+      s_issued[k] = issue_continuity<SG>(scn_of<ONE>(scns, one, tn.scn), maps, tn, smem + k * con::STAGE, &bar[k]);
+    } else {
+      s_issued[k] = 0;
+    }
+  };
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     fence_barrier_init();
+    issue(tile, 0);
   }
-  __syncthreads();
   uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
-  int tile = blockIdx.x;
-  if (tid == 0)
-    s_issued[0] = tile < ntiles ? issue_continuity<SG>(scn_of<ONE>(scns, one, tiles[tile].scn), maps, tiles[tile],
-                                                       smem, &bar[0])
-                                : 0;
+  const StepState* sv_st = nullptr;  // scenario whose step scalars sv holds
+  StepVals sv{};
   for (int it = 0; tile < ntiles; it++) {
     const int s = it & 1;
     const int next = tile + gridDim.x;
-    __syncthreads();
+    __syncthreads();  // s_issued[s] and s_tile[s] visible; stage s^1 no longer read
     if (tid == 0) {
       fence_proxy_async();
-      s_issued[s ^ 1] = next < ntiles ? issue_continuity<SG>(scn_of<ONE>(scns, one, tiles[next].scn), maps,
-                                                             tiles[next], smem + (s ^ 1) * con::STAGE, &bar[s ^ 1])
-                                      : 0;
+      issue(next, s ^ 1);
     }
     if (s_issued[s]) {
-      const Tile tl = tiles[tile];
+      const Tile tl = s_tile[s];
       const ScnDev& S = scn_of<ONE>(scns, one, tl.scn);
       StepState& st = *S.st;
+      if (&st != sv_st) {
+        sv_st = &st;
+        sv = step_vals(st);
+      }
       const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u);
       phase ^= 1u << s;
       const int n = tl.n0 + tx, m = tl.m0 + ty;
@@ -492,7 +512,7 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
           const float q_nd = qv[ty * 36 + tx + 3], q_nu = qv[ty * 36 + tx + 4];
           const float zs_old = ((const float*)(sm + con::O_ZS))[k];
           const float zm = ((const float*)(sm + con::O_ZSMAX))[k];
-          const float dt = st.dt;
+          const float dt = sv.dt;
           float zsn = zs_old;
           if (f & F_KCS1) {
             const float qx = S.use_qext ? ((const float*)(sm + con::O_QEXT))[k] : 0.0f;
@@ -507,7 +527,7 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
                 float dzsdt = 0.0f;
                 if (S.precip) {
                   const float qinfmap = (S.infiltration && v_old > 0.0) ? qi : 0.0f;
-                  dzsdt = dzsdt + (st.ptmp - qinfmap);
+                  dzsdt = dzsdt + (sv.ptmp - qinfmap);
                 }
                 if (S.use_qext) dzsdt = dzsdt + qx;
                 dvol = dvol + dzsdt * S.area * dt;
@@ -538,7 +558,7 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
               if (S.precip) {
                 const float zbc = S.infiltration ? ((const float*)(sm + con::O_ZB))[k] : 0.0f;
                 const float qinfmap = (S.infiltration && !(z <= zbc)) ? qi : 0.0f;
-                z = z + (st.ptmp - qinfmap) * dt;
+                z = z + (sv.ptmp - qinfmap) * dt;
               }
               if (S.use_qext) z = z + qx * dt;
               z = z + ((q_md - q_mu) * S.dxinv + (q_nd - q_nu) * S.dyinv) * dt;

@@ -213,6 +213,16 @@ struct alignas(64) MapSet {
 };
 
 #ifdef __CUDACC__
+// The step scalars a cell or face update reads, copied into registers once per
+// scenario instead of being re-read from the step state for every cell.
+struct StepVals {
+  float dt, ptmp, twu, twv;
+  int parity;
+};
+__device__ __forceinline__ StepVals step_vals(const StepState& st) {
+  return StepVals{st.dt, st.ptmp, st.twu, st.twv, st.parity};
+}
+
 // 1-based table interval int(x) + 1 of a subgrid lookup (sfincs_momentum.f90:
 // 372-378, sfincs_continuity.f90:566), clamped to [1, nlev - 1].  For every
 // finite x that the callers' guards let through the interval is already in
