@@ -984,9 +984,10 @@ void Runner::configure_grids() {
   int dev = 0, nsm = 0, nb_m = 0, nb_c = 0;
   check_cuda(cudaGetDevice(&dev), "device");
   check_cuda(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "sm count");
-  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_m, momentum_tma_fn(subgrid_, tma_minb(), one() != nullptr), 256,
-                                                           momentum_tma_smem()),
-             "occupancy");
+  const void* mfn = momentum_tma_fn(subgrid_, variant_, one() != nullptr);
+  check_cuda(cudaFuncSetAttribute(mfn, cudaFuncAttributeMaxDynamicSharedMemorySize, momentum_tma_smem(variant_)),
+             "momentum shared memory");
+  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_m, mfn, 256, momentum_tma_smem(variant_)), "occupancy");
   check_cuda(
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_c, continuity_tma_fn(subgrid_, one() != nullptr), 256, continuity_tma_smem()),
       "occupancy");
@@ -1009,7 +1010,7 @@ void Runner::launch_momentum_any() {
     launch_qt_momentum(d_scns_, d_tiles_, nqf_, subgrid_, stream_);
     launch_qt_cuv(d_scns_, d_tiles_ + nqf_, nqcuv_, stream_);
   } else if (tma()) {
-    launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, tma_minb(), mom_grid_, stream_, one());
+    launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, variant_, mom_grid_, stream_, one());
   } else {
     launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
   }

@@ -161,13 +161,12 @@ class Runner {
     configure_grids();
   }
   int variant() const { return variant_; }
-  // variants 4 and 5: TMA-staged kernels (5: momentum compiled for 4 CTAs/SM);
+  // variants 4 and 5: TMA-staged kernels (momentum compiled for 3 / 4 CTAs/SM);
   // 2 and 3: per-thread-load kernels
   bool tma() const { return variant_ >= 4; }
   // the one model of a single-model runner (its parameters travel by value in
   // the launches), null for an ensemble
   const ScnDev* one() const { return models_.size() == 1 ? &models_[0]->dev() : nullptr; }
-  int tma_minb() const { return variant_ == 5 ? 4 : 3; }
   // launch one step (all kernels) on the runner's stream
   void launch_one();
   int nscn() const { return (int)models_.size(); }
@@ -220,12 +219,12 @@ void launch_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, in
 void check_cuda(cudaError_t e, const char* what);
 
 MapSet build_map_set(const ScnDev& d);
-int momentum_tma_smem();
+int momentum_tma_smem(int form);
 int continuity_tma_smem();
-const void* momentum_tma_fn(int subgrid, int minb, bool one);
+const void* momentum_tma_fn(int subgrid, int form, bool one);
 const void* continuity_tma_fn(int subgrid, bool one);
 void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
-                         int minb, int grid, cudaStream_t s, const ScnDev* one);
+                         int form, int grid, cudaStream_t s, const ScnDev* one);
 void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
                            int grid, cudaStream_t s, const ScnDev* one);
 void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s);

@@ -180,7 +180,9 @@ struct SgLook {
 
 // Thread 0 reads each tile's header when it issues the tile's loads and passes
 // it on through shared memory; the step scalars are read once per scenario.
-template <bool SG, int MINB, bool ONE>
+// NST stages: the loads of a tile are issued NST - 1 tiles before its update
+// (one CTA barrier per tile orders the reuse of a stage).
+template <bool SG, int MINB, bool ONE, int NST>
 __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __restrict__ scns,
                                                             const MapSet* __restrict__ maps,
                                                             const Tile* __restrict__ tiles, int ntiles,
@@ -188,11 +190,12 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
   pdl_wait();  // the previous kernel of the step has completed
   pdl_trigger();
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar[2];
-  __shared__ int s_issued[2];
-  __shared__ Tile s_tile[2];
+  __shared__ __align__(8) uint64_t bar[NST];
+  __shared__ int s_issued[NST];
+  __shared__ Tile s_tile[NST];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + 32 * ty;
+  const int G = gridDim.x;
   int tile = blockIdx.x;
   // thread 0: load tile t into stage k
   auto issue = [&](int t, int k) {
@@ -205,23 +208,22 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
     }
   };
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int k = 0; k < NST; k++) mbar_init(&bar[k], 1);
     fence_barrier_init();
-    issue(tile, 0);
+    for (int k = 0; k < NST - 1; k++) issue(tile + k * G, k);
   }
   uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
   // running CFL denominator of this thread's faces and the step scalars, for scenario cfl_st
   StepState* cfl_st = nullptr;
   StepVals sv{};
   float cfl_den = 0.0f;
-  for (int it = 0; tile < ntiles; it++) {
-    const int s = it & 1;
-    const int next = tile + gridDim.x;
-    __syncthreads();  // s_issued[s] and s_tile[s] visible; stage s^1 no longer read
+  int s = 0;  // stage of the current tile
+  for (; tile < ntiles; tile += G) {
+    const int sl = s == 0 ? NST - 1 : s - 1;  // stage of the previous tile, refilled now
+    __syncthreads();  // s_issued[s] and s_tile[s] visible; stage sl no longer read
     if (tid == 0) {
       fence_proxy_async();
-      issue(next, s ^ 1);
+      issue(tile + (NST - 1) * G, sl);
     }
     if (s_issued[s]) {
       const Tile tl = s_tile[s];
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
         }
       }
     }
-    tile = next;
+    s = s + 1 == NST ? 0 : s + 1;
   }
   flush_cfl(cfl_st, cfl_den, tx);
   // drain: every issued stage has been waited for in the loop; nothing in flight here
@@ -577,53 +579,37 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
 // --------------------------------------------------------------------------
 // Launchers
 // --------------------------------------------------------------------------
-int momentum_tma_smem() { return 2 * mom::STAGE; }
 int continuity_tma_smem() { return 2 * con::STAGE; }
 
-// minb: CTAs per SM the momentum kernel is compiled for (3: up to 80
-// registers per thread; 4: at most 64), an autotuned choice.  one: the single
-// scenario of the launch (passed by value), or null for an ensemble table.
+// form: the momentum kernel variant, an autotuned choice: 4 / 5 compiled for
+// 3 / 4 CTAs per SM (up to 80 / 64 registers per thread).  Both use two
+// stages; three (loads issued two tiles ahead) measured slower on the 4M-cell
+// subgrid workload.  one: the single scenario of the launch (passed by value),
+// or null for an ensemble table.
+int momentum_tma_smem(int form) { return 2 * mom::STAGE; }
+
 template <bool SG, bool ONE>
-static const void* momentum_fn(int minb) {
-  return minb >= 4 ? (const void*)k_momentum_tma<SG, 4, ONE> : (const void*)k_momentum_tma<SG, 3, ONE>;
+static const void* momentum_fn(int form) {
+  return form == 5 ? (const void*)k_momentum_tma<SG, 4, ONE, 2> : (const void*)k_momentum_tma<SG, 3, ONE, 2>;
 }
-const void* momentum_tma_fn(int subgrid, int minb, bool one) {
-  if (one) return subgrid ? momentum_fn<true, true>(minb) : momentum_fn<false, true>(minb);
-  return subgrid ? momentum_fn<true, false>(minb) : momentum_fn<false, false>(minb);
+const void* momentum_tma_fn(int subgrid, int form, bool one) {
+  if (one) return subgrid ? momentum_fn<true, true>(form) : momentum_fn<false, true>(form);
+  return subgrid ? momentum_fn<true, false>(form) : momentum_fn<false, false>(form);
 }
 const void* continuity_tma_fn(int subgrid, bool one) {
   if (one) return subgrid ? (const void*)k_continuity_tma<true, true> : (const void*)k_continuity_tma<false, true>;
   return subgrid ? (const void*)k_continuity_tma<true, false> : (const void*)k_continuity_tma<false, false>;
 }
 
-template <bool SG, int MINB, bool ONE>
-static void mom_launch(int grid, cudaStream_t s, const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles,
-                       int ntiles, const ScnDev& one) {
-  launch_pdl(k_momentum_tma<SG, MINB, ONE>, dim3(grid), dim3(32, 8), 2 * mom::STAGE, s, d_scns, d_maps, d_tiles, ntiles,
-             one);
-}
-
 void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
-                         int minb, int grid, cudaStream_t s, const ScnDev* one) {
+                         int form, int grid, cudaStream_t s, const ScnDev* one) {
   if (ntiles <= 0) return;
   static const ScnDev none{};
-  const ScnDev& o = one ? *one : none;
-  const bool b4 = minb >= 4;
-  if (one) {
-    if (subgrid)
-      b4 ? mom_launch<true, 4, true>(grid, s, d_scns, d_maps, d_tiles, ntiles, o)
-         : mom_launch<true, 3, true>(grid, s, d_scns, d_maps, d_tiles, ntiles, o);
-    else
-      b4 ? mom_launch<false, 4, true>(grid, s, d_scns, d_maps, d_tiles, ntiles, o)
-         : mom_launch<false, 3, true>(grid, s, d_scns, d_maps, d_tiles, ntiles, o);
-  } else {
-    if (subgrid)
-      b4 ? mom_launch<true, 4, false>(grid, s, d_scns, d_maps, d_tiles, ntiles, o)
-         : mom_launch<true, 3, false>(grid, s, d_scns, d_maps, d_tiles, ntiles, o);
-    else
-      b4 ? mom_launch<false, 4, false>(grid, s, d_scns, d_maps, d_tiles, ntiles, o)
-         : mom_launch<false, 3, false>(grid, s, d_scns, d_maps, d_tiles, ntiles, o);
-  }
+  // every form has this signature (ScnDev by value)
+  using Kernel = void (*)(const ScnDev*, const MapSet*, const Tile*, int, ScnDev);
+  const Kernel k = reinterpret_cast<Kernel>(const_cast<void*>(momentum_tma_fn(subgrid, form, one != nullptr)));
+  launch_pdl(k, dim3(grid), dim3(32, 8), momentum_tma_smem(form), s, d_scns, d_maps, d_tiles, ntiles,
+             one ? *one : none);
 }
 
 void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
