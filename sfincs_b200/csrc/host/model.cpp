@@ -362,6 +362,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     NcFile nc(path(sbgfile));
     const int L = (int)nc.dim("levels");
     if (L < 2) throw std::runtime_error("subgrid tables need at least two levels");
+    if (L > kMaxSubgridLevels) throw std::runtime_error("subgrid tables with more than 254 levels are not supported");
     P.nlev = L;
     auto zmin = nc.floats("z_zmin"), zmax = nc.floats("z_zmax"), volmax = nc.floats("z_volmax"),
          zlev = nc.floats("z_level"), uzmin = nc.floats("uv_zmin"), uzmax = nc.floats("uv_zmax"),
@@ -808,6 +809,8 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     up(d.qlev, h.qlev);
     up(qmu, h.qmap_u);
     up(qmv, h.qmap_v);
+    d.rc_u = d.rc_v = nullptr;
+    d.rl_u = d.rl_v = nullptr;
   } else {
     d.qface = nullptr;
     d.qcell = nullptr;
@@ -815,6 +818,8 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     d.qlev = nullptr;
     d.zbmx = d.gn2 = nullptr;
     qmu = qmv = nullptr;
+    d.rc_u = d.rc_v = nullptr;  // set below for subgrid models
+    d.rl_u = d.rl_v = nullptr;
   up(d.zs, h.zs);
   up(d.zsmax, h.zsmax);
   up(d.zvol, h.zvol);
@@ -851,6 +856,15 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.zz_max, h.zz_max);
   up(d.zz_volmax, h.zz_volmax);
   up(d.zlev, h.zlev);
+  if (h.p.subgrid) {  // record cache, empty (all codes 0)
+    zero(d.rc_u, NA * 6);
+    zero(d.rc_v, NA * 6);
+    zero(d.rl_u, NA);
+    zero(d.rl_v, NA);
+  } else {
+    d.rc_u = d.rc_v = nullptr;
+    d.rl_u = d.rl_v = nullptr;
+  }
   if (h.p.use_qext) zero(d.qext, NA);
   else d.qext = nullptr;
   up(d.qinf, h.qinf);
@@ -985,9 +999,9 @@ void Runner::configure_grids() {
   check_cuda(cudaGetDevice(&dev), "device");
   check_cuda(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "sm count");
   const void* mfn = momentum_tma_fn(subgrid_, variant_, one() != nullptr);
-  check_cuda(cudaFuncSetAttribute(mfn, cudaFuncAttributeMaxDynamicSharedMemorySize, momentum_tma_smem(variant_)),
+  check_cuda(cudaFuncSetAttribute(mfn, cudaFuncAttributeMaxDynamicSharedMemorySize, momentum_tma_smem(variant_, subgrid_)),
              "momentum shared memory");
-  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_m, mfn, 256, momentum_tma_smem(variant_)), "occupancy");
+  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_m, mfn, 256, momentum_tma_smem(variant_, subgrid_)), "occupancy");
   check_cuda(
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_c, continuity_tma_fn(subgrid_, one() != nullptr), 256, continuity_tma_smem()),
       "occupancy");

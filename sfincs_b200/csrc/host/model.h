@@ -219,7 +219,7 @@ void launch_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, in
 void check_cuda(cudaError_t e, const char* what);
 
 MapSet build_map_set(const ScnDev& d);
-int momentum_tma_smem(int form);
+int momentum_tma_smem(int form, int subgrid);
 int continuity_tma_smem();
 const void* momentum_tma_fn(int subgrid, int form, bool one);
 const void* continuity_tma_fn(int subgrid, bool one);

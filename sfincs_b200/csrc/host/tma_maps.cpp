@@ -65,6 +65,9 @@ MapSet build_map_set(const ScnDev& d) {
     if (d.wiggle) f32(MM_ZSD, d.zsderv, 36, 9, "zsderv");
     encode(ms.m[MM_SGZU], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, d.sgz_u, 2 * W, R, 2 * W * 4, 64, 8, "sgz_u");
     encode(ms.m[MM_SGZV], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, d.sgz_v, 2 * W, R, 2 * W * 4, 64, 8, "sgz_v");
+    // record-cache codes (one byte per face)
+    encode(ms.m[MM_RLU], CU_TENSOR_MAP_DATA_TYPE_UINT8, d.rl_u, W, R, W, 32, 8, "record codes u");
+    encode(ms.m[MM_RLV], CU_TENSOR_MAP_DATA_TYPE_UINT8, d.rl_v, W, R, W, 32, 8, "record codes v");
   } else {
     f32(MM_ZB, d.zb, 36, 9, "zb");
     f32(MM_ZBMXU, d.zbmx_u, 32, 8, "zbmx_u");

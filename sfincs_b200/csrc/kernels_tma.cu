@@ -87,8 +87,12 @@ constexpr int W_ZS = 36, W_QU = 36, W_QV = 40, W_UV = 40;
 constexpr int O_ZS = 0, O_QU = 1408, O_QV = 2944, O_UU = 4480, O_VV = 6144, O_FLAGS = 7808, O_KFU = 8320,
               O_KFV = 8576;
 constexpr int O_VNEG = 8832, O_ZSD = 9344, O_SGZU = 10752, O_SGZV = 12800;       // subgrid
+// subgrid record-cache codes: one byte per face (the 24-byte entries are read per thread)
+constexpr int O_RLU = 14848, O_RLV = 15104;
 constexpr int O_ZB = 8832, O_ZBMXU = 10240, O_ZBMXV = 11264, O_GN2U = 12288, O_GN2V = 13312;  // regular
-constexpr int STAGE = 14848;
+constexpr int STAGE = 14848, STAGE_SG = 15360;
+template <bool SG>
+__host__ __device__ constexpr int stage_bytes() { return SG ? STAGE_SG : STAGE; }
 constexpr uint32_t B_COMMON = 36 * 9 * 4 + 36 * 10 * 4 + 40 * 9 * 4 + 2 * 40 * 10 * 4 + 32 * 8 * 2 + 2 * 32 * 8;
 }  // namespace mom
 
@@ -123,7 +127,7 @@ __device__ __forceinline__ bool issue_momentum(const ScnDev& S, const MapSet* ma
   const int x = kGhostPad + tl.n0;  // multiple of 32
   const int y = tl.m0;
   uint32_t bytes = mom::B_COMMON;
-  if (SG) bytes += 48 * 9 + 2 * 64 * 8 * 4 + (S.wiggle ? 36 * 9 * 4 : 0);
+  if (SG) bytes += 48 * 9 + 2 * 64 * 8 * 4 + 2 * 32 * 8 + (S.wiggle ? 36 * 9 * 4 : 0);
   else bytes += 36 * 9 * 4 + 4 * 32 * 8 * 4;
   mbar_expect_tx(bar, bytes);
   tma_load_2d(st + mom::O_ZS, map_of(maps, tl.scn, MM_ZS), x, y, bar);
@@ -139,6 +143,8 @@ __device__ __forceinline__ bool issue_momentum(const ScnDev& S, const MapSet* ma
     if (S.wiggle) tma_load_2d(st + mom::O_ZSD, map_of(maps, tl.scn, MM_ZSD), x, y, bar);
     tma_load_2d(st + mom::O_SGZU, map_of(maps, tl.scn, MM_SGZU), 2 * x, y, bar);
     tma_load_2d(st + mom::O_SGZV, map_of(maps, tl.scn, MM_SGZV), 2 * x, y, bar);
+    tma_load_2d(st + mom::O_RLU, map_of(maps, tl.scn, MM_RLU), x, y, bar);
+    tma_load_2d(st + mom::O_RLV, map_of(maps, tl.scn, MM_RLV), x, y, bar);
   } else {
     tma_load_2d(st + mom::O_ZB, map_of(maps, tl.scn, MM_ZB), x, y, bar);
     tma_load_2d(st + mom::O_ZBMXU, map_of(maps, tl.scn, MM_ZBMXU), x, y, bar);
@@ -202,7 +208,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
     if (t < ntiles) {
       const Tile tn = tiles[t];
       s_tile[k] = tn;
-      s_issued[k] = issue_momentum<SG>(scn_of<ONE>(scns, one, tn.scn), maps, tn, smem + k * mom::STAGE, &bar[k]);
+      s_issued[k] = issue_momentum<SG>(scn_of<ONE>(scns, one, tn.scn), maps, tn, smem + k * mom::stage_bytes<SG>(), &bar[k]);
     } else {
       s_issued[k] = 0;
     }
@@ -241,7 +247,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
       if (!ok) {
         st.fault = 1;
       } else if (n <= S.nmax && m <= S.mmax) {
-        const unsigned char* sm = smem + s * mom::STAGE;
+        const unsigned char* sm = smem + s * mom::stage_bytes<SG>();
         const float* zs = (const float*)(sm + mom::O_ZS);
         const float* qu = (const float*)(sm + mom::O_QU);
         const float* qv = (const float*)(sm + mom::O_QV);
@@ -277,22 +283,50 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
         // ---- issue the data-dependent table loads of both faces first
         SgLook lu{}, lv{};
         if (SG) {
-          auto look = [&](bool wet, float zsu, float zmin, float zmax, const float4* W, const UvRec* R, SgLook& L) {
+          // A scattered read of one table record costs a whole 128-byte line of
+          // DRAM traffic.  Each face keeps a cache entry: the 6 values it used
+          // last step, contiguous per face, so a warp reads whole lines.  The
+          // entry is requested first, its level code arrived with the tile, and
+          // when the face still needs that level (water levels move slowly
+          // against the table spacing) the entry is used; otherwise the tables
+          // are read and the entry is refreshed.  Either way the values are the
+          // table's, bit for bit.
+          const int kc = ty * 32 + tx;
+          auto look = [&](bool wet, float zsu, float zmin, float zmax, const float4* W, const UvRec* R, int o_rl,
+                          float* rc, uint8_t* rl, SgLook& L) {
             if (!wet) return;
+            const float2* eg = reinterpret_cast<const float2*>(rc + 6 * c);
+            const float2 a = eg[0], b = eg[1], d = eg[2];
             L.full = zsu > zmax;
-            const float4* src = W + c;
+            int code = kRecFull;
+            const UvRec* r = nullptr;
             if (!L.full) {
               const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
               const int iuv = lev_index((zsu - zmin) / dzuv, S.nlev);
               L.facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
-              const UvRec* r = R + (int64_t)(iuv - 1) * S.nalloc + c;
-              src = reinterpret_cast<const float4*>(r);
-              L.v2 = *reinterpret_cast<const float2*>(&r->pwet);
+              r = R + (int64_t)(iuv - 1) * S.nalloc + c;
+              code = iuv;
             }
-            L.v = *src;
+            if (code == (int)(sm + o_rl)[kc]) {
+              L.v = make_float4(a.x, a.y, b.x, b.y);
+              L.v2 = d;
+            } else {
+              if (L.full) {
+                L.v = W[c];
+                L.v2 = make_float2(0.0f, 0.0f);
+              } else {
+                L.v = *reinterpret_cast<const float4*>(r);
+                L.v2 = *reinterpret_cast<const float2*>(&r->pwet);
+              }
+              float2* e = reinterpret_cast<float2*>(rc + 6 * c);
+              e[0] = make_float2(L.v.x, L.v.y);
+              e[1] = make_float2(L.v.z, L.v.w);
+              e[2] = L.v2;
+              rl[c] = (uint8_t)code;
+            }
           };
-          look(wet_u, zsu_u, zmin_u, zmax_u, S.sgw_u, S.rec_u, lu);
-          look(wet_v, zsu_v, zmin_v, zmax_v, S.sgw_v, S.rec_v, lv);
+          look(wet_u, zsu_u, zmin_u, zmax_u, S.sgw_u, S.rec_u, mom::O_RLU, S.rc_u, S.rl_u, lu);
+          look(wet_v, zsu_v, zmin_v, zmax_v, S.sgw_v, S.rec_v, mom::O_RLV, S.rc_v, S.rl_v, lv);
         }
         // ---- u face
         if (act_u) {
@@ -586,7 +620,7 @@ int continuity_tma_smem() { return 2 * con::STAGE; }
 // stages; three (loads issued two tiles ahead) measured slower on the 4M-cell
 // subgrid workload.  one: the single scenario of the launch (passed by value),
 // or null for an ensemble table.
-int momentum_tma_smem(int form) { return 2 * mom::STAGE; }
+int momentum_tma_smem(int form, int subgrid) { return 2 * (subgrid ? mom::STAGE_SG : mom::STAGE); }
 
 template <bool SG, bool ONE>
 static const void* momentum_fn(int form) {
@@ -608,7 +642,7 @@ void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile*
   // every form has this signature (ScnDev by value)
   using Kernel = void (*)(const ScnDev*, const MapSet*, const Tile*, int, ScnDev);
   const Kernel k = reinterpret_cast<Kernel>(const_cast<void*>(momentum_tma_fn(subgrid, form, one != nullptr)));
-  launch_pdl(k, dim3(grid), dim3(32, 8), momentum_tma_smem(form), s, d_scns, d_maps, d_tiles, ntiles,
+  launch_pdl(k, dim3(grid), dim3(32, 8), momentum_tma_smem(form, subgrid), s, d_scns, d_maps, d_tiles, ntiles,
              one ? *one : none);
 }
 

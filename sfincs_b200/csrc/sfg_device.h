@@ -19,6 +19,8 @@
 namespace sfg {
 
 constexpr int kGhostPad = 31;  // low padding so that n = 1 is 128-byte aligned
+constexpr int kRecFull = 255;  // record-cache code of the full branch (zsu above the table)
+constexpr int kMaxSubgridLevels = 254;  // level codes 1..nlev-1 stay below kRecFull
 
 // Static per-cell flag bits (uint16_t).
 enum : uint16_t {
@@ -151,6 +153,15 @@ struct ScnDev {
   const float* zz_max;
   const float* zz_volmax;
   const float2* zlev;    // [level][cell]: (dep_k, dep_k+1 - dep_k)
+  // Per-face record cache (regular subgrid grids, TMA kernels).  rc: 6 floats
+  // per face, the table values the face used last step (UvRec fields havg ..
+  // dpwet for level k, or the full-branch coefficients sgw); rl: what rc
+  // holds, 0 = nothing, k + 1 = level k, kRecFull = the full branch.  Both
+  // depend on (face, level) only, so an entry never goes stale.
+  float* rc_u;
+  float* rc_v;
+  uint8_t* rl_u;
+  uint8_t* rl_v;
   // ---- per-cell forcing
   const float* qext;
   const float* qinf;     // infiltration field (m/s), con/c2d
@@ -202,7 +213,7 @@ struct Tile {  // one CTA of the cell kernels
 enum MapId : int {
   // momentum
   MM_ZS, MM_QU0, MM_QU1, MM_QV0, MM_QV1, MM_UU0, MM_UU1, MM_VV0, MM_VV1, MM_FLAGS, MM_KFU, MM_KFV,
-  MM_VNEG, MM_ZSD, MM_SGZU, MM_SGZV, MM_ZB, MM_ZBMXU, MM_ZBMXV, MM_GN2U, MM_GN2V,
+  MM_VNEG, MM_ZSD, MM_SGZU, MM_SGZV, MM_ZB, MM_ZBMXU, MM_ZBMXV, MM_GN2U, MM_GN2V, MM_RLU, MM_RLV,
   // continuity
   MC_QU0, MC_QU1, MC_QV0, MC_QV1, MC_ZS, MC_ZSMAX, MC_ZVOL, MC_ZS0, MC_VOLMAX, MC_VNEG, MC_FLAGS, MC_QEXT,
   MC_QINF, MC_ZB,
