@@ -811,6 +811,8 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     up(qmv, h.qmap_v);
     d.rc_u = d.rc_v = nullptr;
     d.rl_u = d.rl_v = nullptr;
+    d.zc = nullptr;
+    d.zl = nullptr;
   } else {
     d.qface = nullptr;
     d.qcell = nullptr;
@@ -820,6 +822,8 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     qmu = qmv = nullptr;
     d.rc_u = d.rc_v = nullptr;  // set below for subgrid models
     d.rl_u = d.rl_v = nullptr;
+    d.zc = nullptr;
+    d.zl = nullptr;
   up(d.zs, h.zs);
   up(d.zsmax, h.zsmax);
   up(d.zvol, h.zvol);
@@ -861,9 +865,13 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     zero(d.rc_v, NA * 6);
     zero(d.rl_u, NA);
     zero(d.rl_v, NA);
+    zero(d.zc, NA);
+    zero(d.zl, NA);
   } else {
     d.rc_u = d.rc_v = nullptr;
     d.rl_u = d.rl_v = nullptr;
+    d.zc = nullptr;
+    d.zl = nullptr;
   }
   if (h.p.use_qext) zero(d.qext, NA);
   else d.qext = nullptr;

@@ -88,6 +88,7 @@ MapSet build_map_set(const ScnDev& d) {
     f32(MC_VOLMAX, d.zz_volmax, 32, 8, "z_volmax");
     encode(ms.m[MC_VNEG], CU_TENSOR_MAP_DATA_TYPE_UINT8, d.vneg, W, R, W, 32, 8, "vneg (continuity)");
     if (d.wiggle) f32(MC_ZS0, d.zs0, 32, 8, "zs0");
+    encode(ms.m[MC_ZL], CU_TENSOR_MAP_DATA_TYPE_UINT8, d.zl, W, R, W, 32, 8, "z_level cache codes");
   }
   if (d.use_qext) f32(MC_QEXT, d.qext, 32, 8, "qext");
   if (d.infiltration) {

@@ -98,8 +98,8 @@ constexpr uint32_t B_COMMON = 36 * 9 * 4 + 36 * 10 * 4 + 40 * 9 * 4 + 2 * 40 * 1
 
 namespace con {
 constexpr int O_QU = 0, O_QV = 1152, O_ZS = 2304, O_ZSMAX = 3328, O_FLAGS = 4352, O_ZVOL = 4864, O_VOLMAX = 6912,
-              O_VNEG = 7936, O_ZS0 = 8192, O_QEXT = 9216, O_QINF = 10240, O_ZB = 11264;
-constexpr int STAGE = 12288;
+              O_VNEG = 7936, O_ZS0 = 8192, O_QEXT = 9216, O_QINF = 10240, O_ZB = 11264, O_ZL = 12288;
+constexpr int STAGE = 12544;
 }  // namespace con
 
 __device__ __forceinline__ const void* map_of(const MapSet* maps, int scn, int id) { return maps[scn].m[id]; }
@@ -460,7 +460,7 @@ __device__ __forceinline__ bool issue_continuity(const ScnDev& S, const MapSet* 
   const int x = kGhostPad + tl.n0;
   const int y = tl.m0;
   uint32_t bytes = 32 * 9 * 4 + 36 * 8 * 4 + 32 * 8 * 4 * 2 + 32 * 8 * 2;
-  if (SG) bytes += 32 * 8 * 8 + 32 * 8 * 4 + 32 * 8 + (S.wiggle ? 32 * 8 * 4 : 0);
+  if (SG) bytes += 32 * 8 * 8 + 32 * 8 * 4 + 32 * 8 + 32 * 8 + (S.wiggle ? 32 * 8 * 4 : 0);
   if (S.use_qext) bytes += 32 * 8 * 4;
   if (S.infiltration) bytes += 32 * 8 * 4 + (SG ? 0 : 32 * 8 * 4);
   mbar_expect_tx(bar, bytes);
@@ -474,6 +474,7 @@ __device__ __forceinline__ bool issue_continuity(const ScnDev& S, const MapSet* 
     tma_load_2d(st + con::O_VOLMAX, map_of(maps, tl.scn, MC_VOLMAX), x, y, bar);
     tma_load_2d(st + con::O_VNEG, map_of(maps, tl.scn, MC_VNEG), x, y, bar);
     if (S.wiggle) tma_load_2d(st + con::O_ZS0, map_of(maps, tl.scn, MC_ZS0), x, y, bar);
+    tma_load_2d(st + con::O_ZL, map_of(maps, tl.scn, MC_ZL), x, y, bar);
   }
   if (S.use_qext) tma_load_2d(st + con::O_QEXT, map_of(maps, tl.scn, MC_QEXT), x, y, bar);
   if (S.infiltration) {
@@ -484,7 +485,7 @@ __device__ __forceinline__ bool issue_continuity(const ScnDev& S, const MapSet* 
 }
 
 template <bool SG, bool ONE>
-__global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict__ scns, const MapSet* __restrict__ maps,
+__global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restrict__ scns, const MapSet* __restrict__ maps,
                                                         const Tile* __restrict__ tiles, int ntiles,
                                                         const __grid_constant__ ScnDev one) {
   pdl_wait();  // the previous kernel of the step has completed
@@ -579,7 +580,16 @@ __global__ void __launch_bounds__(256) k_continuity_tma(const ScnDev* __restrict
                 const float dzvol = volmax / (float)(S.nlev - 1);
                 const int iuv = lev_index(v / (double)dzvol, S.nlev);
                 const float facint = (float)((v - (double)((float)(iuv - 1) * dzvol)) / (double)dzvol);
-                const float2 dep = S.zlev[(int64_t)(iuv - 1) * S.nalloc + c];
+                // the cell's cached pair when it is still in interval iuv (a scattered
+                // z_level read costs a whole 128-byte line), else the table's pair
+                float2 dep;
+                if (iuv == (int)(sm + con::O_ZL)[k]) {
+                  dep = S.zc[c];
+                } else {
+                  dep = S.zlev[(int64_t)(iuv - 1) * S.nalloc + c];
+                  S.zc[c] = dep;
+                  S.zl[c] = (uint8_t)iuv;
+                }
                 zsn = dep.x + dep.y * facint;
               }
               if (zsn != zs_old) S.zs[c] = zsn;

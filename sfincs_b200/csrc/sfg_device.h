@@ -162,6 +162,10 @@ struct ScnDev {
   float* rc_v;
   uint8_t* rl_u;
   uint8_t* rl_v;
+  // The same for the volume-to-level inversion: zc holds the z_level pair of
+  // interval zl - 1 (zl = 0: nothing cached).
+  float2* zc;
+  uint8_t* zl;
   // ---- per-cell forcing
   const float* qext;
   const float* qinf;     // infiltration field (m/s), con/c2d
@@ -216,7 +220,7 @@ enum MapId : int {
   MM_VNEG, MM_ZSD, MM_SGZU, MM_SGZV, MM_ZB, MM_ZBMXU, MM_ZBMXV, MM_GN2U, MM_GN2V, MM_RLU, MM_RLV,
   // continuity
   MC_QU0, MC_QU1, MC_QV0, MC_QV1, MC_ZS, MC_ZSMAX, MC_ZVOL, MC_ZS0, MC_VOLMAX, MC_VNEG, MC_FLAGS, MC_QEXT,
-  MC_QINF, MC_ZB,
+  MC_QINF, MC_ZB, MC_ZL,
   NUM_MAPS
 };
 struct alignas(64) MapSet {
