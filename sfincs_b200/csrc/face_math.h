@@ -22,11 +22,13 @@ struct FaceV {
 };
 
 // Flux update of one wet face from gathered inputs (sfincs_momentum.f90:389-733).
-// Writes q, uv and returns the face's CFL denominator
-// den = max(sqrt(g*hu), |uv|) * dxuvinv.  The reference takes the minimum of
-// 1/den over faces (:731-733); correctly rounded division is monotone, so that
-// minimum equals 1/max(den) bit for bit and one division per CTA replaces one
-// per face.
+// Writes q, uv and returns g*hu.  The face's CFL denominator is
+// den = max(sqrt(g*hu), |uv|) * dxuvinv and the reference takes the minimum of
+// 1/den over faces (:731-733).  Correctly rounded division, square root and
+// multiplication by a positive constant are monotone, so that minimum equals
+// 1 / (max(sqrt(max g*hu), max |uv|) * dxuvinv) over faces of equal spacing,
+// bit for bit: callers fold g*hu and |uv| and take one square root and one
+// division per reduction instead of per face.
 template <bool SG>
 __device__ __forceinline__ float face_flux_geo(const ScnDev& S, const StepVals& st, int dir, bool adv_on,
                                                bool theta_on, const FaceGeo& geo, uint8_t kf, float zs_nm,
@@ -122,7 +124,7 @@ __device__ __forceinline__ float face_flux_geo(const ScnDev& S, const StepVals& 
   const float uv = q / fmaxf(hu, S.huvmin);
   q_out = q;
   uv_out = uv;
-  return fmaxf(sqrtf(S.g * hu), fabsf(uv)) * dxuvinv;
+  return S.g * hu;
 }
 
 }  // namespace sfg

@@ -418,8 +418,9 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepVals& 
   a.uu_num = uu_num;
   a.vu = (v0 + v1 + v2 + v3) / 4.0f;
   float q, uv;
-  const float den = face_flux_geo<SG>(S, sv, DIR, (f & ADV) != 0, (f & TH) != 0, geo, kf, zs_nm, zs_nmu, hu, gnavg2,
+  const float ghu = face_flux_geo<SG>(S, sv, DIR, (f & ADV) != 0, (f & TH) != 0, geo, kf, zs_nm, zs_nmu, hu, gnavg2,
                                       phi, a, dry_nm, dry_nmu, zd_nm, zd_nmu, q, uv);
+  const float den = fmaxf(sqrtf(ghu), fabsf(uv)) * geo.dxuvinv;
   Qn[c] = q;
   Un[c] = uv;
   const uint8_t kfn = (uint8_t)(KF_WET | ((kf & KF_WET) ? KF_WET2 : 0));

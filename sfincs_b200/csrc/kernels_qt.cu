@@ -122,8 +122,9 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
           dry1 = zs_nmu < S.zb[f.nmu];
         }
         float qn, un;
-        den = face_flux_geo<SG>(S, sv, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kfuv[i], zs_nm,
-                                zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, qn, un);
+        const float ghu = face_flux_geo<SG>(S, sv, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kfuv[i],
+                                            zs_nm, zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, qn, un);
+        den = fmaxf(sqrtf(ghu), fabsf(un)) * geo.dxuvinv;  // the face's own spacing (refinement level)
         q1[i] = qn;
         uv1[i] = un;
         kfuv[i] = KF_WET;

@@ -69,10 +69,18 @@ __device__ __forceinline__ float warp_max_t(float v) {
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
-// Fold a warp's largest CFL denominator into the scenario's min_dt: one
-// division and one atomicMin per warp (positive floats order like their bits).
-__device__ __forceinline__ void flush_cfl(StepState* st, float den, int lane) {
-  den = warp_max_t(den);
+// Running CFL terms of a thread's faces: the largest g*hu and |uv| of its u
+// faces and of its v faces (see face_flux_geo: max over faces commutes with the
+// monotone sqrt and the multiplication by the spacing).  A flush folds a warp's
+// terms into the scenario's min_dt: one division and one atomicMin per warp
+// (positive floats order like their bits).
+struct CflTerms {
+  float ghu_u = 0.0f, uv_u = 0.0f, ghu_v = 0.0f, uv_v = 0.0f;
+};
+__device__ __forceinline__ void flush_cfl(StepState* st, const CflTerms& t, float dxinv, float dyinv, int lane) {
+  const float den_u = fmaxf(sqrtf(warp_max_t(t.ghu_u)), warp_max_t(t.uv_u)) * dxinv;
+  const float den_v = fmaxf(sqrtf(warp_max_t(t.ghu_v)), warp_max_t(t.uv_v)) * dyinv;
+  const float den = fmaxf(den_u, den_v);
   if (lane == 0 && st && den > 0.0f) atomicMin(&st->min_dt_bits, __float_as_uint(1.0f / den));
 }
 
@@ -222,7 +230,8 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
   // running CFL denominator of this thread's faces and the step scalars, for scenario cfl_st
   StepState* cfl_st = nullptr;
   StepVals sv{};
-  float cfl_den = 0.0f;
+  CflTerms cfl;
+  float cfl_dxinv = 0.0f, cfl_dyinv = 0.0f;
   int s = 0;  // stage of the current tile
   for (; tile < ntiles; tile += G) {
     const int sl = s == 0 ? NST - 1 : s - 1;  // stage of the previous tile, refilled now
@@ -236,9 +245,11 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
       const ScnDev& S = scn_of<ONE>(scns, one, tl.scn);
       StepState& st = *S.st;
       if (&st != cfl_st) {  // the tile's scenario changed (CTA-uniform)
-        flush_cfl(cfl_st, cfl_den, tx);
+        flush_cfl(cfl_st, cfl, cfl_dxinv, cfl_dyinv, tx);
         cfl_st = &st;
-        cfl_den = 0.0f;
+        cfl = CflTerms{};
+        cfl_dxinv = S.dxinv;
+        cfl_dyinv = S.dyinv;
         sv = step_vals(st);
       }
       const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u);
@@ -372,8 +383,9 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               hu = fmaxf(zsu_u - zmin_u, S.huthresh);
               gnavg2 = ((const float*)(sm + mom::O_GN2U))[ty * 32 + tx];
             }
-            cfl_den = fmaxf(cfl_den, face_flux<SG, 0>(S, sv, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1,
-                                                      zd0, zd1, qn, un));
+            cfl.ghu_u = fmaxf(cfl.ghu_u, face_flux<SG, 0>(S, sv, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1,
+                                                          zd0, zd1, qn, un));
+            cfl.uv_u = fmaxf(cfl.uv_u, fabsf(un));
             S.qu[p ^ 1][c] = qn;
             S.uu[p ^ 1][c] = un;
           } else if (kfu & KF_WET2) {
@@ -428,8 +440,9 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               hu = fmaxf(zsu_v - zmin_v, S.huthresh);
               gnavg2 = ((const float*)(sm + mom::O_GN2V))[ty * 32 + tx];
             }
-            cfl_den = fmaxf(cfl_den, face_flux<SG, 1>(S, sv, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1,
-                                                      zd0, zd1, qn, un));
+            cfl.ghu_v = fmaxf(cfl.ghu_v, face_flux<SG, 1>(S, sv, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1,
+                                                          zd0, zd1, qn, un));
+            cfl.uv_v = fmaxf(cfl.uv_v, fabsf(un));
             S.qv[p ^ 1][c] = qn;
             S.vv[p ^ 1][c] = un;
           } else if (kfv & KF_WET2) {
@@ -444,7 +457,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
     }
     s = s + 1 == NST ? 0 : s + 1;
   }
-  flush_cfl(cfl_st, cfl_den, tx);
+  flush_cfl(cfl_st, cfl, cfl_dxinv, cfl_dyinv, tx);
   // drain: every issued stage has been waited for in the loop; nothing in flight here
 }
 
