@@ -55,10 +55,12 @@ WORKLOADS = {
 }
 
 # Algorithmic bytes per cell-update of this layout (each element read or written
-# once per kernel; stencil neighbours served from cache), wet faces in the table
-# interpolation branch.  Derivation in DESIGN.md.
+# once per kernel; stencil neighbours served from cache), every face wet: the
+# subgrid table values reach a face through its 24-byte record-cache entry, so
+# a level change adds one table record read and one entry write.  Derivation
+# in DESIGN.md.
 BYTES = {
-    "subgrid": {"momentum": 125, "continuity": 67},
+    "subgrid": {"momentum": 111, "continuity": 68},
     "plain": {"momentum": 60, "continuity": 26},
     "quadtree": {"momentum": 219, "continuity": 83},
 }
