@@ -89,6 +89,9 @@ MapSet build_map_set(const ScnDev& d) {
     encode(ms.m[MC_VNEG], CU_TENSOR_MAP_DATA_TYPE_UINT8, d.vneg, W, R, W, 32, 8, "vneg (continuity)");
     if (d.wiggle) f32(MC_ZS0, d.zs0, 32, 8, "zs0");
     encode(ms.m[MC_ZL], CU_TENSOR_MAP_DATA_TYPE_UINT8, d.zl, W, R, W, 32, 8, "z_level cache codes");
+    f32(MC_ZZMIN, d.zz_min, 32, 8, "z_zmin");
+    f32(MC_ZZMAX, d.zz_max, 32, 8, "z_zmax");
+    encode(ms.m[MC_ZC], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, d.zc, 2 * W, R, 2 * W * 4, 64, 8, "z_level cache");
   }
   if (d.use_qext) f32(MC_QEXT, d.qext, 32, 8, "qext");
   if (d.infiltration) {

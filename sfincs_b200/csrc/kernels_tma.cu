@@ -106,8 +106,9 @@ constexpr uint32_t B_COMMON = 36 * 9 * 4 + 36 * 10 * 4 + 40 * 9 * 4 + 2 * 40 * 1
 
 namespace con {
 constexpr int O_QU = 0, O_QV = 1152, O_ZS = 2304, O_ZSMAX = 3328, O_FLAGS = 4352, O_ZVOL = 4864, O_VOLMAX = 6912,
-              O_VNEG = 7936, O_ZS0 = 8192, O_QEXT = 9216, O_QINF = 10240, O_ZB = 11264, O_ZL = 12288;
-constexpr int STAGE = 12544;
+              O_VNEG = 7936, O_ZS0 = 8192, O_QEXT = 9216, O_QINF = 10240, O_ZB = 11264, O_ZL = 12288,
+              O_ZZMIN = 12544, O_ZZMAX = 13568, O_ZC = 14592;  // subgrid: z_zmin, z_zmax, z_level cache
+constexpr int STAGE = 16640;
 }  // namespace con
 
 __device__ __forceinline__ const void* map_of(const MapSet* maps, int scn, int id) { return maps[scn].m[id]; }
@@ -473,7 +474,7 @@ __device__ __forceinline__ bool issue_continuity(const ScnDev& S, const MapSet* 
   const int x = kGhostPad + tl.n0;
   const int y = tl.m0;
   uint32_t bytes = 32 * 9 * 4 + 36 * 8 * 4 + 32 * 8 * 4 * 2 + 32 * 8 * 2;
-  if (SG) bytes += 32 * 8 * 8 + 32 * 8 * 4 + 32 * 8 + 32 * 8 + (S.wiggle ? 32 * 8 * 4 : 0);
+  if (SG) bytes += 32 * 8 * 8 + 32 * 8 * 4 + 32 * 8 + 32 * 8 + 2 * 32 * 8 * 4 + 32 * 8 * 8 + (S.wiggle ? 32 * 8 * 4 : 0);
   if (S.use_qext) bytes += 32 * 8 * 4;
   if (S.infiltration) bytes += 32 * 8 * 4 + (SG ? 0 : 32 * 8 * 4);
   mbar_expect_tx(bar, bytes);
@@ -488,6 +489,9 @@ __device__ __forceinline__ bool issue_continuity(const ScnDev& S, const MapSet* 
     tma_load_2d(st + con::O_VNEG, map_of(maps, tl.scn, MC_VNEG), x, y, bar);
     if (S.wiggle) tma_load_2d(st + con::O_ZS0, map_of(maps, tl.scn, MC_ZS0), x, y, bar);
     tma_load_2d(st + con::O_ZL, map_of(maps, tl.scn, MC_ZL), x, y, bar);
+    tma_load_2d(st + con::O_ZZMIN, map_of(maps, tl.scn, MC_ZZMIN), x, y, bar);
+    tma_load_2d(st + con::O_ZZMAX, map_of(maps, tl.scn, MC_ZZMAX), x, y, bar);
+    tma_load_2d(st + con::O_ZC, map_of(maps, tl.scn, MC_ZC), 2 * x, y, bar);
   }
   if (S.use_qext) tma_load_2d(st + con::O_QEXT, map_of(maps, tl.scn, MC_QEXT), x, y, bar);
   if (S.infiltration) {
@@ -586,9 +590,10 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
               if (v != v_old) S.zvol[c] = v;
               const float zs11 = zs_old;
               if (v >= (double)(volmax * 0.999f)) {
-                zsn = (float)((double)fmaxf(S.zz_max[c], -20.0f) + (v - (double)volmax) / (double)S.area);
+                zsn = (float)((double)fmaxf(((const float*)(sm + con::O_ZZMAX))[k], -20.0f) +
+                              (v - (double)volmax) / (double)S.area);
               } else if (v <= (double)1.0e-6f) {
-                zsn = fmaxf(S.zz_min[c], -20.0f);
+                zsn = fmaxf(((const float*)(sm + con::O_ZZMIN))[k], -20.0f);
               } else {
                 const float dzvol = volmax / (float)(S.nlev - 1);
                 const int iuv = lev_index(v / (double)dzvol, S.nlev);
@@ -597,7 +602,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
                 // z_level read costs a whole 128-byte line), else the table's pair
                 float2 dep;
                 if (iuv == (int)(sm + con::O_ZL)[k]) {
-                  dep = S.zc[c];
+                  dep = ((const float2*)(sm + con::O_ZC))[k];  // staged with the tile
                 } else {
                   dep = S.zlev[(int64_t)(iuv - 1) * S.nalloc + c];
                   S.zc[c] = dep;

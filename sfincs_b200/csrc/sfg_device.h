@@ -220,7 +220,7 @@ enum MapId : int {
   MM_VNEG, MM_ZSD, MM_SGZU, MM_SGZV, MM_ZB, MM_ZBMXU, MM_ZBMXV, MM_GN2U, MM_GN2V, MM_RLU, MM_RLV,
   // continuity
   MC_QU0, MC_QU1, MC_QV0, MC_QV1, MC_ZS, MC_ZSMAX, MC_ZVOL, MC_ZS0, MC_VOLMAX, MC_VNEG, MC_FLAGS, MC_QEXT,
-  MC_QINF, MC_ZB, MC_ZL,
+  MC_QINF, MC_ZB, MC_ZL, MC_ZZMIN, MC_ZZMAX, MC_ZC,
   NUM_MAPS
 };
 struct alignas(64) MapSet {
