@@ -55,156 +55,237 @@ __device__ __forceinline__ int64_t off(const ScnDev& S, int n, int m) {
 }
 
 // --------------------------------------------------------------------------
-// Step control (run by thread 0 of the step kernel).
+// Step control.
 // --------------------------------------------------------------------------
-// Step control of one scenario (thread 0): returns whether the scenario takes
-// this step.
-__device__ __forceinline__ int step_control(const ScnDev& S, StepState& st) {
-  if (st.run) {  // previous step executed: its outputs are in the other buffer
-    st.parity ^= 1;
+// What this step does, from the scenario's step state as the previous step left
+// it.  Every thread of the step kernel computes it from the same loads, so the
+// boundary work needs neither a barrier nor a round trip through memory after
+// thread 0 decides the step; thread 0 then commits it (commit_step).
+struct StepPlan {
+  int go;          // the scenario takes this step
+  int parity;      // buffer holding the latest q / uv after the step's turnover
+  float mdt, dt;   // CFL time step of the previous step, this step's dt
+  double t;        // model time after this step (the current time if !go)
+  int itb0, itb1;  // boundary time records (1-based)
+  int itbndlast;   // cached boundary time record for the next search
+  float tbfac;     // boundary time-interpolation factor
+};
+
+__device__ __forceinline__ StepPlan plan_step(const ScnDev& S, const StepState& st) {
+  StepPlan P;
+  P.parity = st.run ? (st.parity ^ 1) : st.parity;  // previous step executed: its outputs are in the other buffer
+  const double t_now = st.stop_pending ? (double)S.t1 + 1.0 : st.t;  // sfincs_lib.f90:646
+  P.go = (t_now < st.tend) && (st.steps_left != 0);
+  P.mdt = __uint_as_float(st.min_dt_bits);
+  P.dt = S.alfa * P.mdt;  // sfincs_lib.f90:391-392
+  P.t = P.go ? t_now + (double)P.dt : t_now;
+  P.itbndlast = st.itbndlast;
+  P.itb0 = st.itb0;
+  P.itb1 = st.itb1;
+  P.tbfac = st.tbfac;
+  // ---- boundary time interpolation (sfincs_boundaries.f90:696-726)
+  if (P.go && S.nbnd > 0) {
+    const double t = P.t;
+    int itb0 = 1, itb1 = 1;
+    float tb = 0.0f;
+    if ((double)S.t_bnd[0] > (t - 1.0e-3)) {
+      itb0 = itb1 = 1;
+      tb = S.t_bnd[0];
+    } else if ((double)S.t_bnd[S.ntbnd - 1] < (t + 1.0e-3)) {
+      itb0 = itb1 = S.ntbnd;
+      tb = S.t_bnd[S.ntbnd - 1];
+    } else {
+      for (int itb = st.itbndlast; itb <= S.ntbnd; itb++) {
+        if ((double)S.t_bnd[itb - 1] > (t + 1.0e-6)) {
+          itb0 = itb - 1;
+          itb1 = itb;
+          tb = (float)t;
+          P.itbndlast = itb - 1;
+          break;
+        }
+      }
+    }
+    P.itb0 = itb0;
+    P.itb1 = itb1;
+    P.tbfac = (tb - S.t_bnd[itb0 - 1]) / fmaxf(S.t_bnd[itb1 - 1] - S.t_bnd[itb0 - 1], 1.0e-6f);
+  }
+  return P;
+}
+
+// Thread 0 writes the step's decisions and the rest of the step control:
+// uniform meteo, point-source discharges, CFL reset, instability check.
+__device__ __forceinline__ void commit_step(const ScnDev& S, StepState& st, const StepPlan& P) {
+  if (st.run) {
+    st.parity = P.parity;
     st.run = 0;
   }
   if (st.stop_pending) {  // sfincs_lib.f90:646
     st.t = (double)S.t1 + 1.0;
     st.stop_pending = 0;
   }
-  const int go = (st.t < st.tend) && (st.steps_left != 0);
-  if (go) {
-    st.nt += 1;
-    const float mdt = __uint_as_float(st.min_dt_bits);
-    const float dt = S.alfa * mdt;  // sfincs_lib.f90:391-392
-    const float dtchk = S.alfa * mdt;
-    st.min_dt = mdt;
-    st.dt = dt;
-    const double t = st.t + (double)dt;
-    st.t = t;
-    // ---- uniform wind from time series (sfincs_meteo.f90:1445-1508)
-    if (S.wind) {
-      for (int itw = st.itwndlast; itw <= S.ntwnd; itw++) {
-        if ((double)S.twnd[itw - 1] > t) {
-          const int i0 = itw - 1 >= 1 ? itw - 1 : 1;
-          const float twfac =
-              (float)((t - (double)S.twnd[i0 - 1]) / (double)(S.twnd[itw - 1] - S.twnd[i0 - 1]));
-          const float vmag = S.wmag[i0 - 1] * (1.0f - twfac) + S.wmag[itw - 1] * twfac;
-          const float twopi = 2.0f * S.pi;
-          float dr0 = fmodf(S.wdir[i0 - 1], twopi);
-          if (dr0 < 0.0f) dr0 += twopi;
-          float dr1 = fmodf(S.wdir[itw - 1], twopi);
-          if (dr1 < 0.0f) dr1 += twopi;
-          if (dr1 > dr0 + S.pi)
-            dr0 = dr0 + 2.0f * S.pi;
-          else if (dr0 > dr1 + S.pi)
-            dr1 = dr1 + 2.0f * S.pi;
-          const float vdir = dr0 * (1.0f - twfac) + dr1 * twfac;
-          int icd = (int)(vmag * 10.0f) + 1;
-          icd = icd < 1 ? 1 : (icd > 1000 ? 1000 : icd);
-          const float cd = S.cdval[icd - 1];
-          st.twu = vmag * vmag * cosf(vdir) * S.rhoa * cd / S.rhow;
-          st.twv = vmag * vmag * sinf(vdir) * S.rhoa * cd / S.rhow;
-          st.itwndlast = itw - 1 >= 1 ? itw - 1 : 1;
-          break;
-        }
+  if (!P.go) return;
+  st.nt += 1;
+  const float dt = P.dt;
+  const float dtchk = S.alfa * P.mdt;
+  st.min_dt = P.mdt;
+  st.dt = dt;
+  const double t = P.t;
+  st.t = t;
+  // ---- uniform wind from time series (sfincs_meteo.f90:1445-1508)
+  if (S.wind) {
+    for (int itw = st.itwndlast; itw <= S.ntwnd; itw++) {
+      if ((double)S.twnd[itw - 1] > t) {
+        const int i0 = itw - 1 >= 1 ? itw - 1 : 1;
+        const float twfac = (float)((t - (double)S.twnd[i0 - 1]) / (double)(S.twnd[itw - 1] - S.twnd[i0 - 1]));
+        const float vmag = S.wmag[i0 - 1] * (1.0f - twfac) + S.wmag[itw - 1] * twfac;
+        const float twopi = 2.0f * S.pi;
+        float dr0 = fmodf(S.wdir[i0 - 1], twopi);
+        if (dr0 < 0.0f) dr0 += twopi;
+        float dr1 = fmodf(S.wdir[itw - 1], twopi);
+        if (dr1 < 0.0f) dr1 += twopi;
+        if (dr1 > dr0 + S.pi)
+          dr0 = dr0 + 2.0f * S.pi;
+        else if (dr0 > dr1 + S.pi)
+          dr1 = dr1 + 2.0f * S.pi;
+        const float vdir = dr0 * (1.0f - twfac) + dr1 * twfac;
+        int icd = (int)(vmag * 10.0f) + 1;
+        icd = icd < 1 ? 1 : (icd > 1000 ? 1000 : icd);
+        const float cd = S.cdval[icd - 1];
+        st.twu = vmag * vmag * cosf(vdir) * S.rhoa * cd / S.rhow;
+        st.twv = vmag * vmag * sinf(vdir) * S.rhoa * cd / S.rhow;
+        st.itwndlast = itw - 1 >= 1 ? itw - 1 : 1;
+        break;
       }
     }
-    // ---- uniform rain from time series (sfincs_meteo.f90:1510-1558)
-    if (S.precip) {
-      int itp;
-      for (itp = st.itprcplast; itp <= S.ntprcp; itp++)
-        if ((double)S.tprcp[itp - 1] > t) break;
-      itp = max(min(itp, S.ntprcp), 1);
-      const int i0 = itp - 1 >= 1 ? itp - 1 : 1;
-      const float twfac =
-          (i0 == itp) ? 0.0f
-                      : (float)((t - (double)S.tprcp[i0 - 1]) / (double)(S.tprcp[itp - 1] - S.tprcp[i0 - 1]));
-      st.ptmp = (S.vprcp[i0 - 1] * (1.0f - twfac) + S.vprcp[itp - 1] * twfac) / (float)(1000 * 3600);
-      st.itprcplast = itp - 1 >= 1 ? itp - 1 : 1;
-      st.rain_vol += (double)st.ptmp * (double)dt;  // depth; the host multiplies by the kcs==1 area
-    }
-    // ---- boundary time interpolation (sfincs_boundaries.f90:696-726)
-    if (S.nbnd > 0) {
-      int itb0 = 1, itb1 = 1;
-      float tb = 0.0f;
-      if ((double)S.t_bnd[0] > (t - 1.0e-3)) {
-        itb0 = itb1 = 1;
-        tb = S.t_bnd[0];
-      } else if ((double)S.t_bnd[S.ntbnd - 1] < (t + 1.0e-3)) {
-        itb0 = itb1 = S.ntbnd;
-        tb = S.t_bnd[S.ntbnd - 1];
-      } else {
-        for (int itb = st.itbndlast; itb <= S.ntbnd; itb++) {
-          if ((double)S.t_bnd[itb - 1] > (t + 1.0e-6)) {
-            itb0 = itb - 1;
-            itb1 = itb;
-            tb = (float)t;
-            st.itbndlast = itb - 1;
-            break;
-          }
-        }
-      }
-      st.itb0 = itb0;
-      st.itb1 = itb1;
-      st.tbfac = (tb - S.t_bnd[itb0 - 1]) / fmaxf(S.t_bnd[itb1 - 1] - S.t_bnd[itb0 - 1], 1.0e-6f);
-    }
-    // ---- point-source discharges (sfincs_discharges.f90:341-359)
-    if (S.nsrc > 0) {
-      for (int its = st.itsrclast; its <= S.ntsrc; its++) {
-        if ((double)S.tsrc[its - 1] > t) {
-          const int i0 = its - 1 >= 1 ? its - 1 : 1;
-          const float* a = S.qsrc + (size_t)(i0 - 1) * S.nsrc;
-          const float* b = S.qsrc + (size_t)(its - 1) * S.nsrc;
-          for (int is = 0; is < S.nsrc; is++)
-            S.qtsrc[is] = (float)((double)a[is] + (double)(b[is] - a[is]) * (t - (double)S.tsrc[i0 - 1]) /
-                                                      (double)(S.tsrc[its - 1] - S.tsrc[i0 - 1]));
-          st.itsrclast = its - 1 >= 1 ? its - 1 : 1;
-          break;
-        }
-      }
-    }
-    st.min_dt_bits = __float_as_uint(S.dtmax);  // sfincs_momentum.f90:99
-    if (dtchk < S.dtmin && st.nt > 1) {         // sfincs_lib.f90:634-648
-      st.error = 1;
-      st.stop_pending = 1;
-    }
-    st.run = 1;
-    if (st.steps_left > 0) st.steps_left -= 1;
   }
-  return go;
+  // ---- uniform rain from time series (sfincs_meteo.f90:1510-1558)
+  if (S.precip) {
+    int itp;
+    for (itp = st.itprcplast; itp <= S.ntprcp; itp++)
+      if ((double)S.tprcp[itp - 1] > t) break;
+    itp = max(min(itp, S.ntprcp), 1);
+    const int i0 = itp - 1 >= 1 ? itp - 1 : 1;
+    const float twfac =
+        (i0 == itp) ? 0.0f
+                    : (float)((t - (double)S.tprcp[i0 - 1]) / (double)(S.tprcp[itp - 1] - S.tprcp[i0 - 1]));
+    st.ptmp = (S.vprcp[i0 - 1] * (1.0f - twfac) + S.vprcp[itp - 1] * twfac) / (float)(1000 * 3600);
+    st.itprcplast = itp - 1 >= 1 ? itp - 1 : 1;
+    st.rain_vol += (double)st.ptmp * (double)dt;  // depth; the host multiplies by the kcs==1 area
+  }
+  if (S.nbnd > 0) {
+    st.itb0 = P.itb0;
+    st.itb1 = P.itb1;
+    st.tbfac = P.tbfac;
+    st.itbndlast = P.itbndlast;
+  }
+  // ---- point-source discharges (sfincs_discharges.f90:341-359)
+  if (S.nsrc > 0) {
+    for (int its = st.itsrclast; its <= S.ntsrc; its++) {
+      if ((double)S.tsrc[its - 1] > t) {
+        const int i0 = its - 1 >= 1 ? its - 1 : 1;
+        const float* a = S.qsrc + (size_t)(i0 - 1) * S.nsrc;
+        const float* b = S.qsrc + (size_t)(its - 1) * S.nsrc;
+        for (int is = 0; is < S.nsrc; is++)
+          S.qtsrc[is] = (float)((double)a[is] + (double)(b[is] - a[is]) * (t - (double)S.tsrc[i0 - 1]) /
+                                                    (double)(S.tsrc[its - 1] - S.tsrc[i0 - 1]));
+        st.itsrclast = its - 1 >= 1 ? its - 1 : 1;
+        break;
+      }
+    }
+  }
+  st.min_dt_bits = __float_as_uint(S.dtmax);  // sfincs_momentum.f90:99
+  if (dtchk < S.dtmin && st.nt > 1) {         // sfincs_lib.f90:634-648
+    st.error = 1;
+    st.stop_pending = 1;
+  }
+  st.run = 1;
+  if (st.steps_left > 0) st.steps_left -= 1;
 }
-
-// Levels at the boundary points for this step (sfincs_boundaries.f90:728-756).
-__device__ __forceinline__ void boundary_levels(const ScnDev& S, const StepState& st, int tid, int nthreads) {
-  const float* z0 = S.zs_bnd + (size_t)(st.itb0 - 1) * S.nbnd;
-  const float* z1 = S.zs_bnd + (size_t)(st.itb1 - 1) * S.nbnd;
-  const float tbfac = st.tbfac;
-  for (int ib = tid; ib < S.nbnd; ib += nthreads) S.zst_bnd[ib] = z0[ib] + (z1[ib] - z0[ib]) * tbfac;
-}
-
 
 // --------------------------------------------------------------------------
 // Boundary faces and Neumann cells.
 // --------------------------------------------------------------------------
+// Inputs of one boundary item that the kernel the step kernel waits for
+// (continuity) does not write, read before the wait: the face record and the
+// static tables, the running mean flux (written only by the step kernel), and
+// the boundary-point levels of the time records the previous step used, which
+// are the ones this step needs unless it crosses a record of the series.
+struct BndPre {
+  BndFace b;
+  int2 nn;        // Neumann cell pair
+  float2 zr;      // subgrid: z_zmin, z_zmax of the face
+  float wx;       // subgrid: havg at z_zmax minus z_zmax, of the face
+  float zbi;      // regular grids: bed level of the interior cell
+  float um;       // running mean flux
+  int itb0, itb1; // time records the point levels below belong to (0: none read)
+  float z01[4];   // z0[i1], z1[i1], z0[i2], z1[i2]
+};
+
+__device__ __forceinline__ BndPre bnd_pre(const ScnDev& S, const StepState& st, int i) {
+  BndPre r{};
+  if (i < S.nkcuv2) {
+    r.b = S.bfaces[i];
+    const bool isv = r.b.info & 1;
+    if (S.subgrid) {
+      r.zr = isv ? S.sgz_v[r.b.face] : S.sgz_u[r.b.face];
+      r.wx = (isv ? S.sgw_v[r.b.face] : S.sgw_u[r.b.face]).x;
+    } else {
+      r.zbi = S.zb[r.b.nmi];
+    }
+    r.um = S.uvmean[i];
+    const int itb0 = st.itb0, itb1 = st.itb1;  // 0 before the first step
+    if (!(r.b.info & 4) && S.nbnd > 0 && itb0 >= 1 && itb0 <= S.ntbnd && itb1 >= 1 && itb1 <= S.ntbnd) {
+      r.itb0 = itb0;
+      r.itb1 = itb1;
+      const int j1 = (r.b.info & 8) ? r.b.i1 : 0, j2 = (r.b.info & 8) ? r.b.i2 : 0;
+      const float* z0 = S.zs_bnd + (size_t)(r.itb0 - 1) * S.nbnd;
+      const float* z1 = S.zs_bnd + (size_t)(r.itb1 - 1) * S.nbnd;
+      r.z01[0] = z0[j1];
+      r.z01[1] = z1[j1];
+      r.z01[2] = z0[j2];
+      r.z01[3] = z1[j2];
+    }
+  } else if (i < S.nkcuv2 + S.nneu) {
+    r.nn = S.neu[i - S.nkcuv2];
+  }
+  return r;
+}
+
 // One water-level boundary face (i < nkcuv2) or Neumann cell: returns its FP64
 // inflow volume this step.
-__device__ __forceinline__ double boundary_item(const ScnDev& S, StepState& st, int i) {
+__device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan& P, int i, BndPre pre) {
   double inflow = 0.0;
   if (i < S.nkcuv2) {
-    const BndFace b = S.bfaces[i];
+    const BndFace& b = pre.b;
     const bool isv = b.info & 1;
     const float sgn = (b.info & 2) ? 1.0f : -1.0f;
-    const int p = st.parity;
-    const float dt = st.dt;
-    const double t = st.t;
+    const int p = P.parity;
+    const float dt = P.dt;
+    const double t = P.t;
     const float zsnmi = S.zs[b.nmi];
-    // level of the boundary cell (sfincs_boundaries.f90:800-876)
+    const bool vol_dry = S.subgrid && S.zvol[b.nmi] <= 0.0;
+    // level of the boundary cell (sfincs_boundaries.f90:728-756, 800-876)
     float zsnmb, zs0nmb;
     if (b.info & 4) {
       zsnmb = zs0nmb = b.zfix;
     } else {
+      if (S.nbnd > 0 && (pre.itb0 != P.itb0 || pre.itb1 != P.itb1)) {  // not read ahead, or another time record
+        const int j1 = (b.info & 8) ? b.i1 : 0, j2 = (b.info & 8) ? b.i2 : 0;
+        const float* z0 = S.zs_bnd + (size_t)(P.itb0 - 1) * S.nbnd;
+        const float* z1 = S.zs_bnd + (size_t)(P.itb1 - 1) * S.nbnd;
+        pre.z01[0] = z0[j1];
+        pre.z01[1] = z1[j1];
+        pre.z01[2] = z0[j2];
+        pre.z01[3] = z1[j2];
+      }
+      // levels at the two boundary points (:728-756), then the face's weighted level
+      const float zp1 = pre.z01[0] + (pre.z01[1] - pre.z01[0]) * P.tbfac;
+      const float zp2 = pre.z01[2] + (pre.z01[3] - pre.z01[2]) * P.tbfac;
       double zst;
       if (b.info & 8)
-        zst = (double)(S.zst_bnd[b.i1] * b.fac + S.zst_bnd[b.i2] * (1.0f - b.fac));
+        zst = (double)(zp1 * b.fac + zp2 * (1.0f - b.fac));
       else
-        zst = (double)S.zst_bnd[0];
+        zst = (double)zp1;
       float zb0;
       if (t < (double)(S.tspinup - 1.0e-3f)) {
         const float smfac = (float)(1.0 - (t - (double)S.t0) / (double)(S.tspinup - S.t0));
@@ -218,11 +299,11 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, StepState& st, 
     // weakly reflective flux (sfincs_boundaries.f90:968-1093)
     float hnmb;
     if (S.subgrid) {
-      const float2 zr = isv ? S.sgz_v[b.face] : S.sgz_u[b.face];
+      const float2 zr = pre.zr;
       const float zsuv = fmaxf(zsnmb, zsnmi);
       float depthuv;
       if (zsuv >= zr.y - 1.0e-4f) {
-        depthuv = (isv ? S.sgw_v[b.face] : S.sgw_u[b.face]).x + zsuv;
+        depthuv = pre.wx + zsuv;
       } else if (zsuv > zr.x) {
         const float dzuv = (zr.y - zr.x) / (float)(S.nlev - 1);
         const int iuv = lev_index((zsuv - zr.x) / dzuv, S.nlev);
@@ -239,7 +320,7 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, StepState& st, 
     zsnmb = fmaxf(zsnmb, b.floor);
     zs0nmb = fmaxf(zs0nmb, b.floor);
     float qq = 0.0f, uu = 0.0f;
-    float um = S.uvmean[i];
+    float um = pre.um;
     if (hnmb < S.huthresh + 1.0e-6f) {
       um = 0.0f;
     } else {
@@ -248,10 +329,10 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, StepState& st, 
       const float ubv = sgn * (2.0f * ui - sq * (zsnmi - zs0nmb));
       qq = ubv * hnmb + um;
       if (S.subgrid) {
-        if (S.zvol[b.nmi] <= 0.0) qq = sgn > 0.0f ? fmaxf(qq, 0.0f) : fminf(qq, 0.0f);
+        if (vol_dry) qq = sgn > 0.0f ? fmaxf(qq, 0.0f) : fminf(qq, 0.0f);
         if (zsnmb - b.floor < S.huthresh) qq = sgn > 0.0f ? fminf(qq, 0.0f) : fmaxf(qq, 0.0f);
       } else {
-        if (zsnmi - S.zb[b.nmi] <= S.huthresh) qq = sgn > 0.0f ? fmaxf(qq, 0.0f) : fminf(qq, 0.0f);
+        if (zsnmi - pre.zbi <= S.huthresh) qq = sgn > 0.0f ? fmaxf(qq, 0.0f) : fminf(qq, 0.0f);
         if (zsnmb - b.floor < S.huthresh) qq = sgn > 0.0f ? fminf(qq, 0.0f) : fmaxf(qq, 0.0f);
       }
       uu = fmaxf(fminf(qq / hnmb, 4.0f), -4.0f);
@@ -274,14 +355,14 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, StepState& st, 
     if (S.store_zsmax) S.zsmax[b.nmb] = fmaxf(S.zsmax[b.nmb], zsb_v);
     inflow = (double)sgn * (double)qq * (double)b.len * (double)dt;
   } else if (i < S.nkcuv2 + S.nneu) {
-    const int2 nn = S.neu[i - S.nkcuv2];  // Neumann: zs(nmb) = zs(nmi) (sfincs_boundaries.f90:903-914)
-    S.zs[nn.x] = S.zs[nn.y];
+    S.zs[pre.nn.x] = S.zs[pre.nn.y];  // Neumann: zs(nmb) = zs(nmi) (sfincs_boundaries.f90:903-914)
   }
   return inflow;
 }
 
+// FP64 volume-balance accumulator of the boundary inflow: block sum, one
+// atomic.  Every thread of the block passes its barrier.
 __device__ __forceinline__ void add_inflow(StepState& st, double inflow) {
-  // FP64 volume-balance accumulator of the boundary inflow: block sum, one atomic
   __shared__ double s_red[32];
   inflow = warp_sum(inflow);
   if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = inflow;
@@ -293,25 +374,32 @@ __device__ __forceinline__ void add_inflow(StepState& st, double inflow) {
   }
 }
 
-
-// Step control, boundary point levels and all boundary faces of one scenario
-// in one CTA (one launch per step instead of two; ONE: the single scenario's
-// parameters by value).
+// Step control and all boundary faces of one scenario in one CTA (ONE: the
+// single scenario's parameters by value).  This kernel's time is its chain of
+// dependent memory accesses, so the chain is kept short: the inputs of each
+// thread's first two boundary items that the previous kernel does not write
+// are read before the kernel waits for it; every thread derives the step plan
+// from the same loads of the step state; thread 0 commits the plan after the
+// barrier of the inflow sum, when no thread reads the step state any more.
 template <bool ONE>
 __global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ scns, const __grid_constant__ ScnDev one) {
-  pdl_wait();  // the previous kernel of the step has completed
-  pdl_trigger();
   const ScnDev& S = ONE ? one : scns[blockIdx.x];
   StepState& st = *S.st;
-  __shared__ int s_go;
-  if (threadIdx.x == 0) s_go = step_control(S, st);
-  __syncthreads();
-  if (!s_go) return;
-  if (S.nbnd > 0) boundary_levels(S, st, threadIdx.x, blockDim.x);
-  __syncthreads();  // zst_bnd written by this CTA
+  const int nitems = S.nkcuv2 + S.nneu;
+  const int i0 = threadIdx.x, i1 = threadIdx.x + blockDim.x;
+  const BndPre pre0 = bnd_pre(S, st, i0);
+  const BndPre pre1 = bnd_pre(S, st, i1);
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
+  const StepPlan P = plan_step(S, st);
   double inflow = 0.0;
-  for (int i = threadIdx.x; i < S.nkcuv2 + S.nneu; i += blockDim.x) inflow += boundary_item(S, st, i);
+  if (P.go) {
+    if (i0 < nitems) inflow += boundary_item(S, P, i0, pre0);
+    if (i1 < nitems) inflow += boundary_item(S, P, i1, pre1);
+    for (int i = i1 + (int)blockDim.x; i < nitems; i += blockDim.x) inflow += boundary_item(S, P, i, bnd_pre(S, st, i));
+  }
   add_inflow(st, inflow);
+  if (threadIdx.x == 0) commit_step(S, st, P);
 }
 
 // --------------------------------------------------------------------------

@@ -8,7 +8,8 @@ infiltration, point sources, and Neumann and outflow boundary cells. For each
 case the CUDA core is compared with the oracle in the core's own precision
 after 1, 2, 4, 10, 40 and 100 steps, on the default kernel path and on the
 per-thread-load path. The bars are those of the main stepwise test: time
-within 1e-6 relative, zs and q within 2e-5.
+within 1e-6 relative, zs and q within 2e-5.  Every kernel path must also store
+the same bits as every other on each case.
 """
 import numpy as np
 import pytest
@@ -123,3 +124,18 @@ def test_physics_stepwise_matches_f32_oracle(tmp_path, kind, variant):
         assert dzs <= 2e-5, f"{kind}: zs differs by {dzs} after {done} steps"
         assert dq <= 2e-5, f"{kind}: q differs by {dq} after {done} steps"
     g.close()
+
+
+@pytest.mark.parametrize("kind", sorted(CASES))
+def test_physics_paths_agree_bitwise(tmp_path, kind):
+    """The TMA-staged tile kernels (5, 4) and the per-thread kernel (2) store
+    the same bits with every optional term switched on."""
+    d = CASES[kind](tmp_path).write(str(tmp_path / kind))
+    runs = [_model(d, v) for v in (5, 4, 2)]
+    for g in runs:
+        g.step(100)
+    for name in ("zs", "qx", "qy", "uvx", "uvy"):
+        for v, g in zip((4, 2), runs[1:]):
+            assert np.array_equal(runs[0].get(name), g.get(name)), f"{name}: variant {v} differs from 5"
+    for g in runs:
+        g.close()
