@@ -112,25 +112,12 @@ __device__ __forceinline__ StepPlan plan_step(const ScnDev& S, const StepState& 
   return P;
 }
 
-// Thread 0 writes the step's decisions and the rest of the step control:
-// uniform meteo, point-source discharges, CFL reset, instability check.
-__device__ __forceinline__ void commit_step(const ScnDev& S, StepState& st, const StepPlan& P) {
-  if (st.run) {
-    st.parity = P.parity;
-    st.run = 0;
-  }
-  if (st.stop_pending) {  // sfincs_lib.f90:646
-    st.t = (double)S.t1 + 1.0;
-    st.stop_pending = 0;
-  }
-  if (!P.go) return;
-  st.nt += 1;
+// Forcing of a step that goes: uniform wind and rain, point-source discharges.
+// It writes only step-state fields that plan_step does not read, so one thread
+// runs it while the others still derive the plan.
+__device__ __forceinline__ void step_forcing(const ScnDev& S, StepState& st, const StepPlan& P) {
   const float dt = P.dt;
-  const float dtchk = S.alfa * P.mdt;
-  st.min_dt = P.mdt;
-  st.dt = dt;
   const double t = P.t;
-  st.t = t;
   // ---- uniform wind from time series (sfincs_meteo.f90:1445-1508)
   if (S.wind) {
     for (int itw = st.itwndlast; itw <= S.ntwnd; itw++) {
@@ -172,12 +159,6 @@ __device__ __forceinline__ void commit_step(const ScnDev& S, StepState& st, cons
     st.itprcplast = itp - 1 >= 1 ? itp - 1 : 1;
     st.rain_vol += (double)st.ptmp * (double)dt;  // depth; the host multiplies by the kcs==1 area
   }
-  if (S.nbnd > 0) {
-    st.itb0 = P.itb0;
-    st.itb1 = P.itb1;
-    st.tbfac = P.tbfac;
-    st.itbndlast = P.itbndlast;
-  }
   // ---- point-source discharges (sfincs_discharges.f90:341-359)
   if (S.nsrc > 0) {
     for (int its = st.itsrclast; its <= S.ntsrc; its++) {
@@ -192,6 +173,31 @@ __device__ __forceinline__ void commit_step(const ScnDev& S, StepState& st, cons
         break;
       }
     }
+  }
+}
+
+// Thread 0 writes the step's decisions and the rest of the step control (CFL
+// reset, instability check) once no thread reads the step state any more.
+__device__ __forceinline__ void commit_step(const ScnDev& S, StepState& st, const StepPlan& P) {
+  if (st.run) {
+    st.parity = P.parity;
+    st.run = 0;
+  }
+  if (st.stop_pending) {  // sfincs_lib.f90:646
+    st.t = (double)S.t1 + 1.0;
+    st.stop_pending = 0;
+  }
+  if (!P.go) return;
+  st.nt += 1;
+  const float dtchk = S.alfa * P.mdt;
+  st.min_dt = P.mdt;
+  st.dt = P.dt;
+  st.t = P.t;
+  if (S.nbnd > 0) {
+    st.itb0 = P.itb0;
+    st.itb1 = P.itb1;
+    st.tbfac = P.tbfac;
+    st.itbndlast = P.itbndlast;
   }
   st.min_dt_bits = __float_as_uint(S.dtmax);  // sfincs_momentum.f90:99
   if (dtchk < S.dtmin && st.nt > 1) {         // sfincs_lib.f90:634-648
@@ -251,9 +257,31 @@ __device__ __forceinline__ BndPre bnd_pre(const ScnDev& S, const StepState& st, 
   return r;
 }
 
+// Inputs of one boundary item that the previous kernel writes, read right
+// after the wait for it, before any of this thread's stores (a later item's
+// loads could otherwise not be issued ahead of an earlier item's stores).
+struct BndDyn {
+  float zsnmi;     // level of the interior cell (Neumann: of the source cell)
+  bool vol_dry;    // subgrid: the interior cell's volume is not positive
+  float zsmax;     // running maximum of the boundary cell
+};
+
+__device__ __forceinline__ BndDyn bnd_dyn(const ScnDev& S, int i, const BndPre& pre) {
+  BndDyn d{};
+  if (i < S.nkcuv2) {
+    d.zsnmi = S.zs[pre.b.nmi];
+    d.vol_dry = S.subgrid && S.zvol[pre.b.nmi] <= 0.0;
+    if (S.store_zsmax) d.zsmax = S.zsmax[pre.b.nmb];
+  } else if (i < S.nkcuv2 + S.nneu) {
+    d.zsnmi = S.zs[pre.nn.y];
+  }
+  return d;
+}
+
 // One water-level boundary face (i < nkcuv2) or Neumann cell: returns its FP64
 // inflow volume this step.
-__device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan& P, int i, BndPre pre) {
+__device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan& P, int i, BndPre pre,
+                                                const BndDyn& dyn) {
   double inflow = 0.0;
   if (i < S.nkcuv2) {
     const BndFace& b = pre.b;
@@ -262,8 +290,8 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan&
     const int p = P.parity;
     const float dt = P.dt;
     const double t = P.t;
-    const float zsnmi = S.zs[b.nmi];
-    const bool vol_dry = S.subgrid && S.zvol[b.nmi] <= 0.0;
+    const float zsnmi = dyn.zsnmi;
+    const bool vol_dry = dyn.vol_dry;
     // level of the boundary cell (sfincs_boundaries.f90:728-756, 800-876)
     float zsnmb, zs0nmb;
     if (b.info & 4) {
@@ -352,10 +380,10 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan&
       S.uvmean[i] = 0.0f;
     }
     S.zs[b.nmb] = zsb_v;
-    if (S.store_zsmax) S.zsmax[b.nmb] = fmaxf(S.zsmax[b.nmb], zsb_v);
+    if (S.store_zsmax) S.zsmax[b.nmb] = fmaxf(dyn.zsmax, zsb_v);
     inflow = (double)sgn * (double)qq * (double)b.len * (double)dt;
   } else if (i < S.nkcuv2 + S.nneu) {
-    S.zs[pre.nn.x] = S.zs[pre.nn.y];  // Neumann: zs(nmb) = zs(nmi) (sfincs_boundaries.f90:903-914)
+    S.zs[pre.nn.x] = dyn.zsnmi;  // Neumann: zs(nmb) = zs(nmi) (sfincs_boundaries.f90:903-914)
   }
   return inflow;
 }
@@ -376,11 +404,15 @@ __device__ __forceinline__ void add_inflow(StepState& st, double inflow) {
 
 // Step control and all boundary faces of one scenario in one CTA (ONE: the
 // single scenario's parameters by value).  This kernel's time is its chain of
-// dependent memory accesses, so the chain is kept short: the inputs of each
-// thread's first two boundary items that the previous kernel does not write
-// are read before the kernel waits for it; every thread derives the step plan
-// from the same loads of the step state; thread 0 commits the plan after the
-// barrier of the inflow sum, when no thread reads the step state any more.
+// dependent memory accesses, so the chain is kept short:
+// - the inputs of each thread's first two boundary items that the previous
+//   kernel does not write are read before the kernel waits for it, the others
+//   right after the wait, together with the step state;
+// - every thread derives the step plan from the same loads of the step state;
+// - the last thread, which has the fewest boundary items, then reads the
+//   forcing time series while the others finish theirs;
+// - thread 0 commits the plan after the barrier of the inflow sum, when no
+//   thread reads the step state any more.
 template <bool ONE>
 __global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ scns, const __grid_constant__ ScnDev one) {
   const ScnDev& S = ONE ? one : scns[blockIdx.x];
@@ -391,12 +423,18 @@ __global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ sc
   const BndPre pre1 = bnd_pre(S, st, i1);
   pdl_wait();  // the previous kernel of the step has completed
   pdl_trigger();
+  const BndDyn dyn0 = bnd_dyn(S, i0, pre0);
+  const BndDyn dyn1 = bnd_dyn(S, i1, pre1);
   const StepPlan P = plan_step(S, st);
   double inflow = 0.0;
   if (P.go) {
-    if (i0 < nitems) inflow += boundary_item(S, P, i0, pre0);
-    if (i1 < nitems) inflow += boundary_item(S, P, i1, pre1);
-    for (int i = i1 + (int)blockDim.x; i < nitems; i += blockDim.x) inflow += boundary_item(S, P, i, bnd_pre(S, st, i));
+    if (i0 < nitems) inflow += boundary_item(S, P, i0, pre0, dyn0);
+    if (i1 < nitems) inflow += boundary_item(S, P, i1, pre1, dyn1);
+    for (int i = i1 + (int)blockDim.x; i < nitems; i += blockDim.x) {
+      const BndPre pre = bnd_pre(S, st, i);
+      inflow += boundary_item(S, P, i, pre, bnd_dyn(S, i, pre));
+    }
+    if (threadIdx.x == blockDim.x - 1) step_forcing(S, st, P);
   }
   add_inflow(st, inflow);
   if (threadIdx.x == 0) commit_step(S, st, P);
