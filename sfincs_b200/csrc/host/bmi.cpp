@@ -44,6 +44,10 @@ struct ModelHandle {
   double* h_zs = nullptr;
   float* h_qext = nullptr;
   bool zs_exported = false, qext_exported = false;
+  // update(): the exported qext crosses PCIe on its own stream while the step's
+  // boundary and momentum kernels run; continuity waits for it.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t main_tail = nullptr, qext_ready = nullptr;
 
   ModelHandle(const std::string& dir, bool bmi) {
     host = load_model(dir, bmi);
@@ -56,10 +60,17 @@ struct ModelHandle {
     check_cuda(cudaMallocHost(&h_zs, np * sizeof(double)), "pinned zs");
     check_cuda(cudaMallocHost(&h_qext, np * sizeof(float)), "pinned qext");
     std::memset(h_qext, 0, np * sizeof(float));
+    check_cuda(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "copy stream");
+    check_cuda(cudaEventCreateWithFlags(&main_tail, cudaEventDisableTiming), "event");
+    check_cuda(cudaEventCreateWithFlags(&qext_ready, cudaEventDisableTiming), "event");
     refresh_zs();
   }
   ~ModelHandle() {
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
     runner.reset();
+    if (qext_ready) cudaEventDestroy(qext_ready);
+    if (main_tail) cudaEventDestroy(main_tail);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     dev.reset();
     if (d_stage) cudaFree(d_stage);
     if (d_part) cudaFree(d_part);
@@ -83,6 +94,22 @@ struct ModelHandle {
   }
   void before_update() {
     if (qext_exported) push_qext();
+  }
+  // One step with the exported qext pushed concurrently: the copy and the
+  // scatter into the model's qext start after everything queued before on the
+  // model's stream (the previous step's continuity reads qext), and only the
+  // step's continuity kernel waits for them.
+  void step_once() {
+    if (!(qext_exported && dev->dev().qext)) {
+      runner->step_once();
+      return;
+    }
+    check_cuda(cudaEventRecord(main_tail, s()), "record");
+    check_cuda(cudaStreamWaitEvent(copy_stream, main_tail, 0), "copy stream wait");
+    check_cuda(cudaMemcpyAsync(d_stage, h_qext, (size_t)np() * 4, cudaMemcpyHostToDevice, copy_stream), "qext to device");
+    launch_scatter_f32((const float*)d_stage, dev->d_cmp_off(), const_cast<float*>(dev->dev().qext), np(), copy_stream);
+    check_cuda(cudaEventRecord(qext_ready, copy_stream), "record");
+    runner->step_once(qext_ready);
   }
   void after_update() {
     if (zs_exported) refresh_zs();
@@ -311,8 +338,7 @@ int initialize(void) { return initialize_config("."); }
 int update(void) {
   return guarded([&] {
     sfg::require_bmi();
-    g_bmi->before_update();
-    g_bmi->runner->step_once();
+    g_bmi->step_once();
     g_bmi->after_update();
     g_bmi->runner->sync();  // the step is complete when update() returns, as in the reference
     return 0;

@@ -1127,7 +1127,7 @@ StepState Runner::read_state(int i) {
   return h_states_[i];
 }
 
-void Runner::step_once() {
+void Runner::step_once(cudaEvent_t continuity_after) {
   // run targets from pinned memory (no pageable round trip); the step is then
   // stream-ordered before whatever the caller queues next (e.g. the zs refresh)
   for (size_t i = 0; i < models_.size(); i++) {
@@ -1140,7 +1140,15 @@ void Runner::step_once() {
                                cudaMemcpyHostToDevice, stream_),
                "steps");
   }
-  issue(1);
+  if (continuity_after) {
+    launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_, one());
+    launch_momentum_any();
+    if (any_src_) launch_sources(d_scns_, nscn(), stream_);
+    check_cuda(cudaStreamWaitEvent(stream_, continuity_after, 0), "wait for the source terms");
+    launch_continuity_any();
+  } else {
+    issue(1);
+  }
   check_cuda(cudaGetLastError(), "step launch");
 }
 

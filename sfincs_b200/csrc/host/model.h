@@ -142,7 +142,9 @@ class Runner {
   void set_autotune(bool on) { autotune_ = on; }
   const std::vector<std::pair<int, float>>& tune_ms() const { return tune_ms_; }
   // One step exactly (reference update()); queued on the stream, not waited for.
-  void step_once();
+  // continuity_after: an event the continuity kernel of the step waits for (an
+  // update of its source terms still in flight on another stream), or null.
+  void step_once(cudaEvent_t continuity_after = nullptr);
   void sync();
   cudaStream_t stream() const { return stream_; }
   StepState read_state(int i);
