@@ -179,7 +179,7 @@ struct Model {
   int bndtype, iadvection, baro, storevelmax, storefluxmax, storetwet, storetzsmax;
   std::string inputtype, advstr, qtrfile, depfile, zsinifile, rstfile, mskfile, indexfile, sbgfile, manningfile,
       bndfile, bzsfile, bcafile, bzifile, srcfile, disfile, wndfile, prcpfile, qinffile, scsfile, sefffile,
-      psifile, f0file, infiltrationfile, inftype;
+      psifile, f0file, infiltrationfile, inftype, thdfile;
   bool coriolis, viscosity, friction2d, advection_mask, wiggle_suppression, h73table, spinup_meteo;
   float t0, t1, g, pi, fcorio, twet_threshold;
   bool crsgeo = false, advection, thetasmoothing, subgrid, store_maximum_waterlevel, store_maximum_velocity,
@@ -318,6 +318,7 @@ struct Model {
     bzifile = in.str("bzifile", "none");
     srcfile = in.str("srcfile", "none");
     disfile = in.str("disfile", "none");
+    thdfile = in.str("thdfile", "none");
     wndfile = in.str("wndfile", "none");
     prcpfile = in.str("prcfile", "none");
     if (prcpfile.substr(0, 4) == "none") prcpfile = in.str("precipfile", "none");
@@ -1353,6 +1354,111 @@ struct Model {
     }
   }
 
+  // read_thin_dams: sfincs_structures.f90:385-495.  Polylines of a .thd file
+  // (name line, "nrows ncols", nrows lines of x y); every uv point crossed by a
+  // polyline segment gets kcuv = 0.
+  void read_thin_dams() {
+    if (thdfile.substr(0, 4) == "none") return;
+    std::ifstream fin(path(thdfile));
+    if (!fin) throw std::runtime_error("oracle: cannot open " + thdfile);
+    std::vector<std::string> rec;  // list-directed input skips blank records
+    for (std::string l; std::getline(fin, l);) {
+      for (char& ch : l)
+        if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
+      if (l.find_first_not_of(' ') != std::string::npos) rec.push_back(l);
+    }
+    size_t ir = 0;
+    while (ir + 1 < rec.size()) {
+      ir++;  // cdummy
+      std::istringstream hs(rec[ir++]);
+      int nrows = 0, ncols = 0;
+      hs >> nrows >> ncols;
+      std::vector<float> xthd(nrows), ythd(nrows);
+      for (int i = 0; i < nrows; i++) {
+        if (ir >= rec.size()) throw std::runtime_error("oracle: truncated thin dam polyline");
+        std::istringstream ps(rec[ir++]);
+        ps >> xthd[i] >> ythd[i];
+      }
+      for (long ip : uv_points_crossed_by_polyline(xthd, ythd)) kcuv(ip) = 0;
+    }
+  }
+
+  // direction / cross: third_party_open/utils/geometry.f90:121-190 (real*4)
+  static int direction(float ax, float ay, float bx, float by, float cx, float cy) {
+    float val = (by - ay) * (cx - bx) - (bx - ax) * (cy - by);
+    if (val < -1.0e-6f) return -1;
+    if (val > 1.0e-6f) return 1;
+    return 0;
+  }
+  static bool cross(float x11, float y11, float x12, float y12, float x21, float y21, float x22, float y22) {
+    int dir1 = direction(x11, y11, x12, y12, x21, y21);
+    int dir2 = direction(x11, y11, x12, y12, x22, y22);
+    int dir3 = direction(x21, y21, x22, y22, x11, y11);
+    int dir4 = direction(x21, y21, x22, y22, x12, y12);
+    return dir1 != dir2 && dir3 != dir4;
+  }
+
+  // find_uv_points_intersected_by_polyline: sfincs_quadtree.F90:853-1010
+  // (the set of crossed uv points, ascending).
+  std::vector<long> uv_points_crossed_by_polyline(const std::vector<float>& xpol, const std::vector<float>& ypol) {
+    std::vector<int> ind((size_t)npuv + 1, 0);
+    const long npol = (long)xpol.size();
+    for (long ipol = 1; ipol <= npol - 1; ipol++) {
+      float xpa = xpol[ipol - 1], ypa = ypol[ipol - 1], xpb = xpol[ipol], ypb = ypol[ipol];
+      float xtmpa = qt_cosrot * (xpa - x0) + qt_sinrot * (ypa - y0);
+      float ytmpa = -qt_sinrot * (xpa - x0) + qt_cosrot * (ypa - y0);
+      float xtmpb = qt_cosrot * (xpb - x0) + qt_sinrot * (ypb - y0);
+      float ytmpb = -qt_sinrot * (xpb - x0) + qt_cosrot * (ypb - y0);
+      for (int iref = qt_nlev; iref >= 1; iref--) {
+        long na = (long)(ytmpa / qt_dyr(iref)) + 1, ma = (long)(xtmpa / qt_dxr(iref)) + 1;
+        long nb = (long)(ytmpb / qt_dyr(iref)) + 1, mb = (long)(xtmpb / qt_dxr(iref)) + 1;
+        long n0 = std::min(na, nb) - 1, n1 = std::max(na, nb) + 1, m0 = std::min(ma, mb) - 1, m1 = std::max(ma, mb) + 1;
+        for (long m = m0; m <= m1; m++) {
+          for (long n = n0; n <= n1; n++) {
+            long nm = find_qt_by_index_unchecked(n, m, iref);
+            if (nm == 0) continue;
+            nm = index_sfincs_in_quadtree(nm);
+            if (nm == 0) continue;
+            for (long ip : {(long)z_index_uv_mu1(nm), (long)z_index_uv_mu2(nm), (long)z_index_uv_nu1(nm),
+                            (long)z_index_uv_nu2(nm)}) {
+              if (ip <= 0) continue;
+              long nmu = uv_index_z_nmu(ip);
+              if (cross(xpa, ypa, xpb, ypb, z_xz(nm), z_yz(nm), z_xz(nmu), z_yz(nmu))) ind[(size_t)ip] = (int)ipol;
+            }
+          }
+        }
+      }
+    }
+    std::vector<long> out;
+    for (long ip = 1; ip <= npuv; ip++)
+      if (ind[(size_t)ip] > 0) out.push_back(ip);
+    return out;
+  }
+
+  // find_quadtree_cell_by_index as written (sfincs_quadtree.F90:822-850): no
+  // check of n against the level's row count, only nm > 0; a miss returns
+  // binary_search's 0 shifted by the level's first index minus one (0 on
+  // level 1, the only level of a regular grid).
+  long find_qt_by_index_unchecked(long n, long m, int iref) {
+    long nmx = (long)qt_nmax << (iref - 1);
+    long nm = (m - 1) * nmx + n;
+    if (nm <= 0) return 0;
+    long i1 = qt_first(iref), i2 = qt_last(iref);
+    long lo = 0, hi = i2 - i1 + 1, found = 0;  // binary_search(x(i1:i2), n, val): 1-based, middle 0 skipped
+    while (lo <= hi && !found) {
+      long mid = (lo + hi) / 2;
+      if (mid == 0)
+        lo = mid + 1;
+      else if (nm == qt_nm_indices(i1 + mid - 1))
+        found = mid;
+      else if (nm < qt_nm_indices(i1 + mid - 1))
+        hi = mid - 1;
+      else
+        lo = mid + 1;
+    }
+    return found + i1 - 1;
+  }
+
   // find_quadtree_cell_by_index + binary_search: sfincs_quadtree.F90:822-850
   long find_qt_by_index(long n, long m, int iref) {
     long nmx = (long)qt_nmax << (iref - 1);
@@ -1470,6 +1576,7 @@ struct Model {
     initialize_hydro();
     if (qt_nlev == 1) use_quadtree = false;  // sfincs_domain.f90:42-50
     set_advection_mask();
+    read_thin_dams();  // sfincs_lib.f90:156 read_structures, after initialize_domain
     read_boundary_data();
     find_boundary_indices();
     read_discharges();

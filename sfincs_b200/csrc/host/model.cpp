@@ -172,7 +172,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   std::string prcpfile = in.str("prcfile", "none");
   if (is_none(prcpfile)) prcpfile = in.str("precipfile", "none");
   // Inputs outside this core's path: refuse loudly instead of silently ignoring physics.
-  for (const char* k : {"bcafile", "bzifile", "bdrfile", "thdfile", "weirfile", "drnfile", "volfile", "spwfile",
+  for (const char* k : {"bcafile", "bzifile", "bdrfile", "weirfile", "drnfile", "volfile", "spwfile",
                         "amufile", "amvfile", "ampfile", "amprfile", "netbndbzsbzifile", "netsrcdisfile",
                         "netamuamvfile", "netamprfile", "netampfile", "netspwfile", "infiltration_file",
                         "scsfile", "sefffile", "psifile", "f0file", "wavemaker_wvmfile", "wvmfile"}) {
@@ -186,6 +186,8 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   if (inputtype != "bin") throw std::runtime_error("only inputformat = bin is supported");
   if (bndtype != 1) throw std::runtime_error("only bndtype = 1 is supported");
   const bool quadtree = !is_none(qtrfile);
+  const std::string thdfile = in.str("thdfile", "none");
+  if (quadtree && !is_none(thdfile)) throw std::runtime_error("input 'thdfile' is not supported on quadtree grids by this core");
   if (!quadtree && (nmax <= 0 || mmax <= 0)) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
 
   // ---- derived (sfincs_input.f90:347-745) ------------------------------------
@@ -230,8 +232,57 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   k.qinf_zmin = qinf_zmin; k.advection_mask = advection_mask; k.qtrfile = qtrfile; k.depfile = depfile;
   k.mskfile = mskfile; k.indexfile = indexfile; k.sbgfile = sbgfile; k.manningfile = manningfile;
   k.bndfile = bndfile; k.bzsfile = bzsfile; k.srcfile = srcfile; k.disfile = disfile; k.wndfile = wndfile;
-  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree;
+  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile;
   return k;
+}
+
+// ---- thin dams (sfincs_structures.f90:385-495) ----------------------------------
+// A .thd file holds polylines, each as a name line, an "nrows ncols" line and
+// nrows lines of x y (blank lines skipped, commas accepted as separators, as
+// list-directed input does).
+static std::vector<std::vector<std::pair<float, float>>> read_thin_dams(const std::string& file) {
+  FILE* fp = std::fopen(file.c_str(), "r");
+  if (!fp) throw std::runtime_error("cannot open thin dams file " + file);
+  std::vector<std::string> lines;
+  char buf[4096];
+  while (std::fgets(buf, sizeof buf, fp)) {
+    std::string l(buf);
+    for (char& ch : l)
+      if (ch == ',' || ch == '\t' || ch == '\r' || ch == '\n') ch = ' ';
+    if (l.find_first_not_of(' ') != std::string::npos) lines.push_back(l);
+  }
+  std::fclose(fp);
+  std::vector<std::vector<std::pair<float, float>>> out;
+  size_t i = 0;
+  while (i + 1 < lines.size()) {
+    i++;  // name line
+    int nrows = 0, ncols = 0;
+    if (std::sscanf(lines[i++].c_str(), "%d %d", &nrows, &ncols) != 2 || nrows < 0)
+      throw std::runtime_error("thin dams file " + file + ": bad block header");
+    std::vector<std::pair<float, float>> pl;
+    for (int r = 0; r < nrows; r++) {
+      float x = 0.0f, y = 0.0f;
+      if (i >= lines.size() || std::sscanf(lines[i++].c_str(), "%f %f", &x, &y) != 2)
+        throw std::runtime_error("thin dams file " + file + ": truncated polyline");
+      pl.push_back({x, y});
+    }
+    out.push_back(std::move(pl));
+  }
+  return out;
+}
+
+// Side of c relative to the line a -> b, with the 1e-6 dead band of the
+// reference's geometry helper (FP32 throughout, like the reference's real*4).
+static int side_of(float ax, float ay, float bx, float by, float cx, float cy) {
+  const float val = (by - ay) * (cx - bx) - (bx - ax) * (cy - by);
+  return val < -1.0e-6f ? -1 : (val > 1.0e-6f ? 1 : 0);
+}
+
+// Segments p1-p2 and q1-q2 cross when each separates the other's end points
+// (a touching or collinear end point counts as on neither side).
+static bool segments_cross(float p1x, float p1y, float p2x, float p2y, float q1x, float q1y, float q2x, float q2y) {
+  return side_of(p1x, p1y, p2x, p2y, q1x, q1y) != side_of(p1x, p1y, p2x, p2y, q2x, q2y) &&
+         side_of(q1x, q1y, q2x, q2y, p1x, p1y) != side_of(q1x, q1y, q2x, q2y, p2x, p2y);
 }
 
 std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
@@ -339,6 +390,42 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     }
   }
   h.npuv = (long long)face_off.size();
+  // Thin dams: a face whose segment between the two cell centres crosses a
+  // dam segment is no momentum face (kcuv = 0, sfincs_quadtree.F90:853-1010).
+  // Cells are searched in the dam segment's cell-index box widened by one,
+  // as the reference does.  The boundary lists and the advection mask are
+  // built from the faces as they were before (the reference applies the dams
+  // after initialize_domain); activity and the theta-smoothing neighbour rule
+  // see the dams (the reference tests kcuv there at run time).
+  std::vector<uint8_t> dam_u, dam_v;
+  if (!is_none(K.thdfile)) {
+    dam_u.assign(NA, 0);
+    dam_v.assign(NA, 0);
+    auto xz = [&](int n, int m) {
+      return x0 + cosrot * (1.0f * ((float)m - 0.5f)) * dx - sinrot * (1.0f * ((float)n - 0.5f)) * dy;
+    };
+    auto yz = [&](int n, int m) {
+      return y0 + sinrot * (1.0f * ((float)m - 0.5f)) * dx + cosrot * (1.0f * ((float)n - 0.5f)) * dy;
+    };
+    for (const auto& pl : read_thin_dams(path(K.thdfile))) {
+      for (size_t ipol = 0; ipol + 1 < pl.size(); ipol++) {
+        const float xpa = pl[ipol].first, ypa = pl[ipol].second, xpb = pl[ipol + 1].first, ypb = pl[ipol + 1].second;
+        const float xta = cosrot * (xpa - x0) + sinrot * (ypa - y0), yta = -sinrot * (xpa - x0) + cosrot * (ypa - y0);
+        const float xtb = cosrot * (xpb - x0) + sinrot * (ypb - y0), ytb = -sinrot * (xpb - x0) + cosrot * (ypb - y0);
+        const int na = (int)(yta / dy) + 1, ma = (int)(xta / dx) + 1, nb = (int)(ytb / dy) + 1, mb = (int)(xtb / dx) + 1;
+        for (int m = std::max(std::min(ma, mb) - 1, 1); m <= std::min(std::max(ma, mb) + 1, mmax); m++) {
+          for (int n = std::max(std::min(na, nb) - 1, 1); n <= std::min(std::max(na, nb) + 1, nmax); n++) {
+            if (!act(n, m)) continue;
+            const int64_t c = OFF(n, m);
+            if (act(n, m + 1) && segments_cross(xpa, ypa, xpb, ypb, xz(n, m), yz(n, m), xz(n, m + 1), yz(n, m + 1)))
+              dam_u[c] = 1;
+            if (act(n + 1, m) && segments_cross(xpa, ypa, xpb, ypb, xz(n, m), yz(n, m), xz(n + 1, m), yz(n + 1, m)))
+              dam_v[c] = 1;
+          }
+        }
+      }
+    }
+  }
 
   // ---- bathymetry (regular) or subgrid tables -----------------------------------
   std::vector<float> sg_level_raw;  // z_level as read, [np][levels]
@@ -608,6 +695,9 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   h.flags.assign(NA, 0);
   auto KU = [&](int n, int m) -> int { return (n >= 1 && n <= nmax && m >= 1 && m <= mmax) ? kcu[OFF(n, m)] : 0; };
   auto KV = [&](int n, int m) -> int { return (n >= 1 && n <= nmax && m >= 1 && m <= mmax) ? kcv[OFF(n, m)] : 0; };
+  // kcuv after the thin dams
+  auto KUd = [&](int n, int m) -> int { return KU(n, m) != 0 && !dam_u.empty() && dam_u[OFF(n, m)] ? 0 : KU(n, m); };
+  auto KVd = [&](int n, int m) -> int { return KV(n, m) != 0 && !dam_v.empty() && dam_v[OFF(n, m)] ? 0 : KV(n, m); };
   const bool do_mask = P.advection && advection_mask && nmax > 1;
   for (long long i = 0; i < h.np; i++) {
     const int n = h.z_n[i], m = h.z_m[i];
@@ -615,8 +705,8 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     uint16_t f = F_ACT;
     if (kcs[c] == 1) f |= F_KCS1;
     const int ku = kcu[c], kv = kcv[c];
-    if (ku == 1 || ku == 6) f |= F_UACT;
-    if (kv == 1 || kv == 6) f |= F_VACT;
+    if (KUd(n, m) == 1 || KUd(n, m) == 6) f |= F_UACT;
+    if (KVd(n, m) == 1 || KVd(n, m) == 6) f |= F_VACT;
     const bool cdn = act(n - 1, m), cup = act(n + 1, m), clf = act(n, m - 1), crt = act(n, m + 1);
     if (cdn) f |= F_CDN;
     if (cup) f |= F_CUP;
@@ -635,8 +725,8 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
       if (madv_u) f |= F_UADV;
       if (madv_v) f |= F_VADV;
     }
-    if (KU(n, m - 1) == 1 && KU(n, m + 1) == 1) f |= F_UTH;  // kcuv(u_nmd)==1 and kcuv(u_nmu)==1
-    if (KV(n - 1, m) == 1 && KV(n + 1, m) == 1) f |= F_VTH;
+    if (KUd(n, m - 1) == 1 && KUd(n, m + 1) == 1) f |= F_UTH;  // kcuv(u_nmd)==1 and kcuv(u_nmu)==1
+    if (KVd(n - 1, m) == 1 && KVd(n + 1, m) == 1) f |= F_VTH;
     h.flags[c] = f;
   }
   h.kcs_cmp.resize(h.np);

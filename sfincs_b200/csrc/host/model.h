@@ -75,6 +75,7 @@ struct Keys {
   float hmin_cfl = 0, dtmax = 0, uvmax = 0, nuviscdim = 0, manning = 0, manning_land = 0, manning_sea = 0,
         rghlevland = 0, qinf = 0, qinf_zmin = 0;
   bool viscosity = false, advection_mask = true, quadtree = false;
+  std::string thdfile;  // thin dams (regular grids)
   std::string qtrfile, depfile, mskfile, indexfile, sbgfile, manningfile, bndfile, bzsfile, srcfile, disfile,
       wndfile, qinffile, prcpfile;
 };

@@ -299,6 +299,7 @@ class RegularModel:
     qinf_field: Optional[np.ndarray] = None  # (nmax, mmax) mm/h for c2d infiltration
     src: Optional[np.ndarray] = None     # (nsrc, 2)
     dis: Optional[np.ndarray] = None     # (nt, 1+nsrc)
+    thd: Optional[List[np.ndarray]] = None  # thin dams: polylines, each (npoints, 2) x, y
 
     @property
     def nmax(self):
@@ -350,6 +351,14 @@ class RegularModel:
             np.savetxt(os.path.join(d, "sfincs.dis"), self.dis, fmt="%.6f")
             inp["srcfile"] = "sfincs.src"
             inp["disfile"] = "sfincs.dis"
+        if self.thd:
+            with open(os.path.join(d, "sfincs.thd"), "w") as f:
+                for i, pl in enumerate(self.thd):
+                    pl = np.asarray(pl, np.float64)
+                    f.write(f"THD{i + 1:02d}\n{pl.shape[0]} 2\n")
+                    for x, y in pl:
+                        f.write(f"{x:.4f} {y:.4f}\n")
+            inp["thdfile"] = "sfincs.thd"
         inp.update(self.params)
         with open(os.path.join(d, "sfincs.inp"), "w") as f:
             for k, v in inp.items():

@@ -4,7 +4,8 @@ The main parity tests (test_gpu_parity.py) run the default switches. Here each
 case turns on terms that those leave off: Coriolis, wind stress from a time
 series, theta smoothing, the "original" advection scheme, the slope limiter,
 friction2d off, viscosity and no wiggle suppression on a subgrid model, c2d
-infiltration, point sources, and Neumann and outflow boundary cells. For each
+infiltration, point sources, Neumann and outflow boundary cells, and thin dams
+(regular and subgrid). For each
 case the CUDA core is compared with the oracle in the core's own precision
 after 1, 2, 4, 10, 40 and 100 steps, on the default kernel path and on the
 per-thread-load path. The bars are those of the main stepwise test: time
@@ -80,9 +81,24 @@ def case_subgrid_infiltration_sources(tmp_path):
     return m
 
 
+def case_thin_dams_theta(tmp_path):
+    m = _plain(tmp_path, advection=1, theta=0.9)
+    # a dam across the domain between columns 15 and 16 with a gap, and a diagonal one
+    m.thd = [np.array([[6000.0, -200.0], [6000.0, 5000.0]]),
+             np.array([[2000.0, 2000.0], [4400.0, 7000.0], [9000.0, 8000.0]])]
+    return m
+
+
+def case_subgrid_thin_dams(tmp_path):
+    m = _subgrid(tmp_path, advection=1)
+    m.thd = [np.array([[5000.0, -100.0], [5000.0, 6500.0], [7000.0, 9000.0]])]
+    return m
+
+
 CASES = {f.__name__[5:]: f for f in (case_coriolis_wind_theta, case_original_advection_slopelim_nofric2d,
                                       case_boundary_kinds, case_plain_infiltration, case_subgrid_visc_nowiggle,
-                                      case_subgrid_infiltration_sources)}
+                                      case_subgrid_infiltration_sources, case_thin_dams_theta,
+                                      case_subgrid_thin_dams)}
 
 
 def _model(d, variant):

@@ -44,6 +44,13 @@ def _masks():
     tb = m.bzs[:, 0]
     m.bzs = np.stack([tb, np.sin(tb / 3000.0), 0.5 * np.cos(tb / 2000.0), 0.2 + 0 * tb], axis=1)
     out["three_bnd_points"] = m
+    m = plain(advection=1, theta=0.9)
+    # a straight dam between columns 8 and 9 across the whole grid, a diagonal
+    # one, and one along cell centres (touching points do not cut a face)
+    m.thd = [np.array([[2400.0, -100.0], [2400.0, 14 * 300.0 + 100.0]]),
+             np.array([[500.0, 500.0], [1700.0, 3100.0], [4100.0, 3500.0]]),
+             np.array([[150.0, 1650.0], [1350.0, 1650.0]])]
+    out["thin_dams"] = m
     return out
 
 
@@ -110,7 +117,24 @@ def test_subgrid_tables_and_volumes(tmp_path):
 
 def test_unsupported_inputs_are_refused(tmp_path):
     m = synth.plain_regular(nmax=6, mmax=7, dx=300.0, tstop=600.0, nbumps=1)
-    m.params["thdfile"] = "sfincs.thd"
+    m.params["weirfile"] = "sfincs.weir"
     d = m.write(str(tmp_path))
-    with pytest.raises(RuntimeError, match="thdfile"):
+    with pytest.raises(RuntimeError, match="weirfile"):
         B.layout(d, "counts", 10)
+
+
+def test_thin_dam_faces(tmp_path):
+    """The straight dam between columns 8 and 9 removes exactly the u faces of
+    column 8 (both sides active) and leaves every v face; the oracle's kcuv
+    agrees face by face with the layout (test_flags_match_oracle_index_arrays)."""
+    m = synth.plain_regular(nmax=14, mmax=17, dx=300.0, tstop=600.0, nbumps=5)
+    kcuv0 = _oracle(m.write(str(tmp_path / "open"))).get("kcuv")
+    m.thd = [np.array([[2400.0, -100.0], [2400.0, 14 * 300.0 + 100.0]])]
+    o = _oracle(m.write(str(tmp_path / "dam")))
+    kcuv = o.get("kcuv")
+    cell = o.get("uv_nm").astype(np.int64) - 1
+    dirn = o.get("uv_dir").astype(np.int64)
+    mcol = (np.flatnonzero(m.msk.ravel(order="F") > 0) // m.nmax + 1)[cell]  # 1-based column of each face's cell
+    dammed = (kcuv == 0) & (kcuv0 != 0)
+    assert np.array_equal(dammed & (dirn == 0), (dirn == 0) & (mcol == 8))
+    assert not np.any(dammed & (dirn == 1))

@@ -148,3 +148,22 @@ def test_symmetric_dam_break(tmp_path):
     # mirror symmetry across the channel axis (n -> 10 - n)
     np.testing.assert_allclose(grid, grid[::-1, :], rtol=0, atol=1e-12)
     assert grid[:, 12].max() > 0.0  # the front travelled east
+
+
+def test_thin_dam_holds_a_dam_break(tmp_path):
+    """A thin dam across the channel (sfincs_structures.f90:385-495): the front
+    of a dam break reaches it and nothing crosses; the water behind it keeps
+    its volume."""
+    m = _closed(synth.plain_regular(nmax=9, mmax=16, dx=100.0, tstop=3600.0, nbumps=0))
+    m.zb = np.full_like(m.zb, -1.0)
+    m.thd = [np.array([[1200.0, -50.0], [1200.0, 950.0]])]  # between columns 12 and 13
+    d = m.write(str(tmp_path))
+    o = _oracle(d)
+    mm = o.get("nm_m").astype(int)
+    o.set("zs", np.where(mm <= 6, 1.0, 0.0))
+    v0 = np.sum(o.get("zs") + 1.0)
+    o.update(-1000.0, 400)
+    z = o.get("zs")
+    assert np.all(z[mm >= 13] == 0.0)
+    assert z[mm == 12].max() > 0.05  # the front arrived at the dam
+    assert abs(np.sum(z + 1.0) - v0) <= 1e-10 * v0
