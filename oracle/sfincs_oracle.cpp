@@ -179,7 +179,7 @@ struct Model {
   int bndtype, iadvection, baro, storevelmax, storefluxmax, storetwet, storetzsmax;
   std::string inputtype, advstr, qtrfile, depfile, zsinifile, rstfile, mskfile, indexfile, sbgfile, manningfile,
       bndfile, bzsfile, bcafile, bzifile, srcfile, disfile, wndfile, prcpfile, qinffile, scsfile, sefffile,
-      psifile, f0file, infiltrationfile, inftype, thdfile;
+      psifile, f0file, infiltrationfile, inftype, thdfile, weirfile;
   bool coriolis, viscosity, friction2d, advection_mask, wiggle_suppression, h73table, spinup_meteo;
   float t0, t1, g, pi, fcorio, twet_threshold;
   bool crsgeo = false, advection, thetasmoothing, subgrid, store_maximum_waterlevel, store_maximum_velocity,
@@ -235,6 +235,13 @@ struct Model {
   F1<int32_t> nmindsrc;
   F1<float> tsrc, qtsrc;
   F2<float> qsrc;
+
+  // --- structures (sfincs_data.f90: structure_*)
+  long nrstructures = 0;
+  F1<int32_t> structure_uv_index;
+  F1<int8_t> structure_type;
+  F1<float> structure_length;
+  F2<float> structure_parameters;
 
   // --- hydro state
   F1<TZ> zs;
@@ -319,6 +326,7 @@ struct Model {
     srcfile = in.str("srcfile", "none");
     disfile = in.str("disfile", "none");
     thdfile = in.str("thdfile", "none");
+    weirfile = in.str("weirfile", "none");
     wndfile = in.str("wndfile", "none");
     prcpfile = in.str("prcfile", "none");
     if (prcpfile.substr(0, 4) == "none") prcpfile = in.str("precipfile", "none");
@@ -1379,7 +1387,7 @@ struct Model {
         std::istringstream ps(rec[ir++]);
         ps >> xthd[i] >> ythd[i];
       }
-      for (long ip : uv_points_crossed_by_polyline(xthd, ythd)) kcuv(ip) = 0;
+      for (const auto& e : uv_points_crossed_by_polyline(xthd, ythd)) kcuv(e.first) = 0;
     }
   }
 
@@ -1399,8 +1407,10 @@ struct Model {
   }
 
   // find_uv_points_intersected_by_polyline: sfincs_quadtree.F90:853-1010
-  // (the set of crossed uv points, ascending).
-  std::vector<long> uv_points_crossed_by_polyline(const std::vector<float>& xpol, const std::vector<float>& ypol) {
+  // (the crossed uv points, ascending, each with the last segment that
+  // crossed it, 1-based: uv_indices and vertices).
+  std::vector<std::pair<long, int>> uv_points_crossed_by_polyline(const std::vector<float>& xpol,
+                                                                   const std::vector<float>& ypol) {
     std::vector<int> ind((size_t)npuv + 1, 0);
     const long npol = (long)xpol.size();
     for (long ipol = 1; ipol <= npol - 1; ipol++) {
@@ -1429,10 +1439,193 @@ struct Model {
         }
       }
     }
-    std::vector<long> out;
+    std::vector<std::pair<long, int>> out;
     for (long ip = 1; ip <= npuv; ip++)
-      if (ind[(size_t)ip] > 0) out.push_back(ip);
+      if (ind[(size_t)ip] > 0) out.push_back({ip, ind[(size_t)ip]});
     return out;
+  }
+
+  // read_structures: sfincs_structures.f90:8-35 (thin dams, then weirs)
+  void read_structures() {
+    read_thin_dams();
+    nrstructures = 0;
+    if (weirfile.substr(0, 4) != "none") read_structure_file(weirfile, 1, 2);
+  }
+
+  // distance_between_points_projected_on_line_segment:
+  // third_party_open/utils/geometry.f90:215-297 (real*4)
+  static float projected_distance(float x0a, float y0a, float x0b, float y0b, float x1, float y1, float x2, float y2,
+                                  float mxdst) {
+    float b1, b2, c1, c2, aa, a1, a2, p1, p2;
+    b1 = std::fabs((x2 - x1) * (y1 - y0a) - (x1 - x0a) * (y2 - y1)) / (std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1)));
+    c1 = std::sqrt((x0a - x1) * (x0a - x1) + (y0a - y1) * (y0a - y1));
+    c2 = std::sqrt((x0a - x2) * (x0a - x2) + (y0a - y2) * (y0a - y2));
+    aa = std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+    a1 = std::sqrt(std::max(c1 * c1 - b1 * b1, 0.0f));
+    a2 = std::sqrt(std::max(c2 * c2 - b1 * b1, 0.0f));
+    if (a1 > aa || a2 > aa)
+      p1 = a1 < a2 ? 0.0f : 1.0f;
+    else
+      p1 = a1 / aa;
+    b2 = std::fabs((x2 - x1) * (y1 - y0b) - (x1 - x0b) * (y2 - y1)) / (std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1)));
+    c1 = std::sqrt((x0b - x1) * (x0b - x1) + (y0b - y1) * (y0b - y1));
+    c2 = std::sqrt((x0b - x2) * (x0b - x2) + (y0b - y2) * (y0b - y2));
+    aa = std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+    a1 = std::sqrt(std::max(c1 * c1 - b2 * b2, 0.0f));
+    a2 = std::sqrt(std::max(c2 * c2 - b2 * b2, 0.0f));
+    if (a1 > aa || a2 > aa)
+      p2 = a1 < a2 ? 0.0f : 1.0f;
+    else
+      p2 = a1 / aa;
+    return (b1 < mxdst && b2 < mxdst) ? aa * std::fabs(p2 - p1) : 0.0f;
+  }
+
+  // read_structure_file: sfincs_structures.f90:38-381 (projected grids)
+  void read_structure_file(const std::string& filename, int itype, int npars) {
+    std::ifstream fin(path(filename));
+    if (!fin) throw std::runtime_error("oracle: cannot open " + filename);
+    std::vector<std::string> rec;
+    for (std::string l; std::getline(fin, l);) {
+      for (char& ch : l)
+        if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
+      if (l.find_first_not_of(' ') != std::string::npos) rec.push_back(l);
+    }
+    F1<int8_t> istruc;
+    istruc.alloc(npuv);
+    F2<float> strucpars;
+    strucpars.alloc(npars, npuv);
+    for (long ip = 1; ip <= npuv; ip++) strucpars(1, ip) = -9999.0f;
+    F1<float> lngth;
+    lngth.alloc(npuv);
+    size_t ir = 0;
+    while (ir + 1 < rec.size()) {
+      ir++;  // cdummy
+      std::istringstream hs(rec[ir++]);
+      int nrows = 0, ncols = 0;
+      hs >> nrows >> ncols;
+      std::vector<float> xthd(nrows), ythd(nrows);
+      std::vector<std::vector<float>> pars(npars + 1, std::vector<float>(nrows + 1));
+      for (int irow = 1; irow <= nrows; irow++) {
+        if (ir >= rec.size()) throw std::runtime_error("oracle: truncated structure polyline");
+        std::istringstream ps(rec[ir++]);
+        ps >> xthd[irow - 1] >> ythd[irow - 1];
+        for (int ipar = 1; ipar <= npars; ipar++) ps >> pars[ipar][irow];
+      }
+      for (const auto& e : uv_points_crossed_by_polyline(xthd, ythd)) {
+        long indx = e.first;
+        int irow = e.second;
+        istruc(indx) = 1;
+        long nm = uv_index_z_nm(indx), nmu = uv_index_z_nmu(indx);
+        int iref = uv_flags_iref(indx), idir = uv_flags_dir(indx);
+        int irefnm = z_flags_iref(nm), irefnmu = z_flags_iref(nmu);
+        float dxs = idir == 0 ? dyrm(iref) : dxrm(iref);
+        float xuv, yuv, xuv1, yuv1, xuv2, yuv2;
+        if (irefnm >= irefnmu) {
+          if (idir == 0) {
+            xuv = z_xz(nm) + 0.5f * dxs * std::cos(rotation);
+            yuv = z_yz(nm) + 0.5f * dxs * std::sin(rotation);
+          } else {
+            xuv = z_xz(nm) + 0.5f * dxs * std::cos(rotation + 0.5f * pi);
+            yuv = z_yz(nm) + 0.5f * dxs * std::sin(rotation + 0.5f * pi);
+          }
+        } else {
+          if (idir == 0) {
+            xuv = z_xz(nmu) + 0.5f * dxs * std::cos(rotation - pi);
+            yuv = z_yz(nmu) + 0.5f * dxs * std::sin(rotation - pi);
+          } else {
+            xuv = z_xz(nmu) + 0.5f * dxs * std::cos(rotation - 0.5f * pi);
+            yuv = z_yz(nmu) + 0.5f * dxs * std::sin(rotation - 0.5f * pi);
+          }
+        }
+        if (idir == 0) {
+          xuv1 = xuv + 0.5f * dxs * std::cos(rotation - 0.5f * pi);
+          yuv1 = yuv + 0.5f * dxs * std::sin(rotation - 0.5f * pi);
+          xuv2 = xuv + 0.5f * dxs * std::cos(rotation + 0.5f * pi);
+          yuv2 = yuv + 0.5f * dxs * std::sin(rotation + 0.5f * pi);
+        } else {
+          xuv1 = xuv + 0.5f * dxs * std::cos(rotation - pi);
+          yuv1 = yuv + 0.5f * dxs * std::sin(rotation - pi);
+          xuv2 = xuv + 0.5f * dxs * std::cos(rotation);
+          yuv2 = yuv + 0.5f * dxs * std::sin(rotation);
+        }
+        float d = projected_distance(xuv1, yuv1, xuv2, yuv2, xthd[irow - 1], ythd[irow - 1], xthd[irow], ythd[irow],
+                                     999999.0f);
+        lngth(indx) = lngth(indx) + d;
+        float dst1 = std::sqrt((xuv - xthd[irow - 1]) * (xuv - xthd[irow - 1]) + (yuv - ythd[irow - 1]) * (yuv - ythd[irow - 1]));
+        float dst2 = std::sqrt((xuv - xthd[irow]) * (xuv - xthd[irow]) + (yuv - ythd[irow]) * (yuv - ythd[irow]));
+        float wfac = dst1 / (dst1 + dst2);
+        float height = pars[1][irow] * (1.0f - wfac) + pars[1][irow + 1] * wfac;
+        strucpars(1, indx) = std::max(strucpars(1, indx), height);
+        for (int ipar = 2; ipar <= npars; ipar++)
+          strucpars(ipar, indx) = pars[ipar][irow] * (1.0f - wfac) + pars[ipar][irow + 1] * wfac;
+      }
+    }
+    long nstruc = 0;
+    for (long ip = 1; ip <= npuv; ip++) {
+      bool okay = false;
+      if (istruc(ip) == 1) {
+        float height = strucpars(1, ip);
+        if (subgrid) {
+          if (height > sg_uv_zmin(ip)) okay = true;
+        } else {
+          if (height > zbuvmx(ip)) okay = true;
+        }
+      }
+      if (okay)
+        nstruc++;
+      else
+        istruc(ip) = 0;
+    }
+    structure_uv_index.alloc(nstruc);
+    structure_type.alloc(nstruc);
+    structure_length.alloc(nstruc);
+    structure_parameters.alloc(npars, nstruc);
+    nstruc = 0;
+    for (long ip = 1; ip <= npuv; ip++) {
+      if (istruc(ip) != 1) continue;
+      nstruc++;
+      structure_type(nstruc) = (int8_t)itype;
+      structure_uv_index(nstruc) = (int32_t)ip;
+      int iref = uv_flags_iref(ip), idir = uv_flags_dir(ip);
+      float dxs = idir == 0 ? dyrm(iref) : dxrm(iref);
+      structure_length(nstruc) = lngth(ip) / dxs;
+      for (int ipar = 1; ipar <= npars; ipar++) structure_parameters(ipar, nstruc) = strucpars(ipar, ip);
+      kcuv(ip) = 3;
+    }
+    nrstructures = nstruc;
+  }
+
+  // compute_fluxes_over_structures: sfincs_structures.f90:592-697
+  void compute_fluxes_over_structures() {
+    for (long istruc = 1; istruc <= nrstructures; istruc++) {
+      long ip = structure_uv_index(istruc);
+      q(ip) = (T)0;
+      uv(ip) = (T)0;
+      long nm = uv_index_z_nm(ip), nmu = uv_index_z_nmu(ip);
+      T zsnm = (T)zs(nm), zsnmu = (T)zs(nmu);
+      T height = (T)structure_parameters(1, istruc);
+      if (zsnm < height && zsnmu < height) continue;
+      T qstruc = (T)0;
+      int idir = 1;
+      if (structure_type(istruc) == 1) {
+        T cweir = (T)1.7049f, m = (T)0, Cd = (T)structure_parameters(2, istruc), h1, h2;
+        if (zsnm > zsnmu) {
+          idir = 1;
+          h1 = zsnm - height;
+          h2 = zsnmu - height;
+        } else {
+          idir = -1;
+          h1 = zsnmu - height;
+          h2 = zsnm - height;
+        }
+        if (h2 > (T)(2.0f / 3.0f) * h1)
+          qstruc = Cd * h2 * std::sqrt((T)2.0f * (T)9.81f * (h1 - h2) / ((T)1 - m));
+        else  // h1**1.5; the core's precision evaluates it as h1 * sqrt(h1), correctly rounded on CPU and GPU alike
+          qstruc = Cd * cweir * (std::is_same<TZ, float>::value ? h1 * std::sqrt(h1) : std::pow(h1, (T)1.5f));
+      }
+      qstruc = qstruc * (T)structure_length(istruc);
+      q(ip) = qstruc * (T)idir;
+    }
   }
 
   // find_quadtree_cell_by_index as written (sfincs_quadtree.F90:822-850): no
@@ -1576,7 +1769,7 @@ struct Model {
     initialize_hydro();
     if (qt_nlev == 1) use_quadtree = false;  // sfincs_domain.f90:42-50
     set_advection_mask();
-    read_thin_dams();  // sfincs_lib.f90:156 read_structures, after initialize_domain
+    read_structures();  // sfincs_lib.f90:156, after initialize_domain
     read_boundary_data();
     find_boundary_indices();
     read_discharges();
@@ -2132,6 +2325,7 @@ struct Model {
       }
       update_discharges(t);
       compute_fluxes(dt);
+      if (nrstructures > 0) compute_fluxes_over_structures();
       if (subgrid)
         compute_water_levels_subgrid(dt, t);
       else
@@ -2283,6 +2477,16 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "netprcp" && m.netprcp.allocated()) copy_out(m.netprcp, out, n);
     else if (s == "qext" && m.qext.allocated()) copy_out(m.qext, out, n);
     else if (s == "uvmean") copy_out(m.uvmean, out, n);
+    else if (s == "nrstructures") out[0] = (double)m.nrstructures;
+    else if (s == "struc") {
+      // per structure: uv point (1-based), crest level, Cd, relative length
+      for (long i = 1; i <= m.nrstructures && 4 * (i - 1) + 3 < n; i++) {
+        out[4 * (i - 1)] = m.structure_uv_index(i);
+        out[4 * (i - 1) + 1] = m.structure_parameters(1, i);
+        out[4 * (i - 1) + 2] = m.structure_parameters(2, i);
+        out[4 * (i - 1) + 3] = m.structure_length(i);
+      }
+    }
     else if (s == "kb_cell" || s == "kb_dir" || s == "kb_sign") {
       // water-level boundary faces (kcuv==2/6 list without lateral Neumann faces), reference order
       long k = 0;

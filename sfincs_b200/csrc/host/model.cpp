@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <type_traits>
 #include <stdexcept>
 
@@ -172,7 +173,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   std::string prcpfile = in.str("prcfile", "none");
   if (is_none(prcpfile)) prcpfile = in.str("precipfile", "none");
   // Inputs outside this core's path: refuse loudly instead of silently ignoring physics.
-  for (const char* k : {"bcafile", "bzifile", "bdrfile", "weirfile", "drnfile", "volfile", "spwfile",
+  for (const char* k : {"bcafile", "bzifile", "bdrfile", "drnfile", "volfile", "spwfile",
                         "amufile", "amvfile", "ampfile", "amprfile", "netbndbzsbzifile", "netsrcdisfile",
                         "netamuamvfile", "netamprfile", "netampfile", "netspwfile", "infiltration_file",
                         "scsfile", "sefffile", "psifile", "f0file", "wavemaker_wvmfile", "wvmfile"}) {
@@ -186,8 +187,9 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   if (inputtype != "bin") throw std::runtime_error("only inputformat = bin is supported");
   if (bndtype != 1) throw std::runtime_error("only bndtype = 1 is supported");
   const bool quadtree = !is_none(qtrfile);
-  const std::string thdfile = in.str("thdfile", "none");
+  const std::string thdfile = in.str("thdfile", "none"), weirfile = in.str("weirfile", "none");
   if (quadtree && !is_none(thdfile)) throw std::runtime_error("input 'thdfile' is not supported on quadtree grids by this core");
+  if (quadtree && !is_none(weirfile)) throw std::runtime_error("input 'weirfile' is not supported on quadtree grids by this core");
   if (!quadtree && (nmax <= 0 || mmax <= 0)) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
 
   // ---- derived (sfincs_input.f90:347-745) ------------------------------------
@@ -232,17 +234,20 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   k.qinf_zmin = qinf_zmin; k.advection_mask = advection_mask; k.qtrfile = qtrfile; k.depfile = depfile;
   k.mskfile = mskfile; k.indexfile = indexfile; k.sbgfile = sbgfile; k.manningfile = manningfile;
   k.bndfile = bndfile; k.bzsfile = bzsfile; k.srcfile = srcfile; k.disfile = disfile; k.wndfile = wndfile;
-  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile;
+  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile; k.weirfile = weirfile;
   return k;
 }
 
-// ---- thin dams (sfincs_structures.f90:385-495) ----------------------------------
-// A .thd file holds polylines, each as a name line, an "nrows ncols" line and
-// nrows lines of x y (blank lines skipped, commas accepted as separators, as
-// list-directed input does).
-static std::vector<std::vector<std::pair<float, float>>> read_thin_dams(const std::string& file) {
+// ---- thin dams and weirs (sfincs_structures.f90:38-495) --------------------------
+// A .thd / .weir file holds polylines, each as a name line, an "nrows ncols"
+// line and nrows lines of x y followed by npars values per point (blank lines
+// skipped, commas accepted as separators, as list-directed input does).
+struct PolyRow {
+  float x, y, p[2];
+};
+static std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars) {
   FILE* fp = std::fopen(file.c_str(), "r");
-  if (!fp) throw std::runtime_error("cannot open thin dams file " + file);
+  if (!fp) throw std::runtime_error("cannot open polyline file " + file);
   std::vector<std::string> lines;
   char buf[4096];
   while (std::fgets(buf, sizeof buf, fp)) {
@@ -252,23 +257,41 @@ static std::vector<std::vector<std::pair<float, float>>> read_thin_dams(const st
     if (l.find_first_not_of(' ') != std::string::npos) lines.push_back(l);
   }
   std::fclose(fp);
-  std::vector<std::vector<std::pair<float, float>>> out;
+  std::vector<std::vector<PolyRow>> out;
   size_t i = 0;
   while (i + 1 < lines.size()) {
     i++;  // name line
     int nrows = 0, ncols = 0;
     if (std::sscanf(lines[i++].c_str(), "%d %d", &nrows, &ncols) != 2 || nrows < 0)
-      throw std::runtime_error("thin dams file " + file + ": bad block header");
-    std::vector<std::pair<float, float>> pl;
+      throw std::runtime_error("polyline file " + file + ": bad block header");
+    std::vector<PolyRow> pl;
     for (int r = 0; r < nrows; r++) {
-      float x = 0.0f, y = 0.0f;
-      if (i >= lines.size() || std::sscanf(lines[i++].c_str(), "%f %f", &x, &y) != 2)
-        throw std::runtime_error("thin dams file " + file + ": truncated polyline");
-      pl.push_back({x, y});
+      PolyRow row{};
+      if (i >= lines.size() ||
+          std::sscanf(lines[i++].c_str(), "%f %f %f %f", &row.x, &row.y, &row.p[0], &row.p[1]) < 2 + npars)
+        throw std::runtime_error("polyline file " + file + ": truncated polyline");
+      pl.push_back(row);
     }
     out.push_back(std::move(pl));
   }
   return out;
+}
+
+// Length of the projection of the segment a-b onto the line segment 1-2,
+// each end clamped to the segment (third_party_open/utils/geometry.f90:215-297).
+static float projected_length(float x0a, float y0a, float x0b, float y0b, float x1, float y1, float x2, float y2) {
+  const float aa = std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+  auto along = [&](float px, float py, float& b) {
+    b = std::fabs((x2 - x1) * (y1 - py) - (x1 - px) * (y2 - y1)) / std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+    const float c1 = std::sqrt((px - x1) * (px - x1) + (py - y1) * (py - y1));
+    const float c2 = std::sqrt((px - x2) * (px - x2) + (py - y2) * (py - y2));
+    const float a1 = std::sqrt(std::max(c1 * c1 - b * b, 0.0f)), a2 = std::sqrt(std::max(c2 * c2 - b * b, 0.0f));
+    if (a1 > aa || a2 > aa) return a1 < a2 ? 0.0f : 1.0f;
+    return a1 / aa;
+  };
+  float b1 = 0.0f, b2 = 0.0f;
+  const float p1 = along(x0a, y0a, b1), p2 = along(x0b, y0b, b2);
+  return (b1 < 999999.0f && b2 < 999999.0f) ? aa * std::fabs(p2 - p1) : 0.0f;
 }
 
 // Side of c relative to the line a -> b, with the 1e-6 dead band of the
@@ -397,34 +420,40 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   // built from the faces as they were before (the reference applies the dams
   // after initialize_domain); activity and the theta-smoothing neighbour rule
   // see the dams (the reference tests kcuv there at run time).
+  auto xz = [&](int n, int m) {
+    return x0 + cosrot * (1.0f * ((float)m - 0.5f)) * dx - sinrot * (1.0f * ((float)n - 0.5f)) * dy;
+  };
+  auto yz = [&](int n, int m) {
+    return y0 + sinrot * (1.0f * ((float)m - 0.5f)) * dx + cosrot * (1.0f * ((float)n - 0.5f)) * dy;
+  };
+  // Faces crossed by one polyline: key (dense offset * 2 + 0 for u, 1 for v)
+  // -> the last crossing segment (0-based), as the reference records it.
+  auto crossed_faces = [&](const std::vector<PolyRow>& pl) {
+    std::map<int64_t, int> ind;
+    for (size_t ipol = 0; ipol + 1 < pl.size(); ipol++) {
+      const float xpa = pl[ipol].x, ypa = pl[ipol].y, xpb = pl[ipol + 1].x, ypb = pl[ipol + 1].y;
+      const float xta = cosrot * (xpa - x0) + sinrot * (ypa - y0), yta = -sinrot * (xpa - x0) + cosrot * (ypa - y0);
+      const float xtb = cosrot * (xpb - x0) + sinrot * (ypb - y0), ytb = -sinrot * (xpb - x0) + cosrot * (ypb - y0);
+      const int na = (int)(yta / dy) + 1, ma = (int)(xta / dx) + 1, nb = (int)(ytb / dy) + 1, mb = (int)(xtb / dx) + 1;
+      for (int m = std::max(std::min(ma, mb) - 1, 1); m <= std::min(std::max(ma, mb) + 1, mmax); m++) {
+        for (int n = std::max(std::min(na, nb) - 1, 1); n <= std::min(std::max(na, nb) + 1, nmax); n++) {
+          if (!act(n, m)) continue;
+          const int64_t c = OFF(n, m);
+          if (act(n, m + 1) && segments_cross(xpa, ypa, xpb, ypb, xz(n, m), yz(n, m), xz(n, m + 1), yz(n, m + 1)))
+            ind[c * 2] = (int)ipol;
+          if (act(n + 1, m) && segments_cross(xpa, ypa, xpb, ypb, xz(n, m), yz(n, m), xz(n + 1, m), yz(n + 1, m)))
+            ind[c * 2 + 1] = (int)ipol;
+        }
+      }
+    }
+    return ind;
+  };
   std::vector<uint8_t> dam_u, dam_v;
   if (!is_none(K.thdfile)) {
     dam_u.assign(NA, 0);
     dam_v.assign(NA, 0);
-    auto xz = [&](int n, int m) {
-      return x0 + cosrot * (1.0f * ((float)m - 0.5f)) * dx - sinrot * (1.0f * ((float)n - 0.5f)) * dy;
-    };
-    auto yz = [&](int n, int m) {
-      return y0 + sinrot * (1.0f * ((float)m - 0.5f)) * dx + cosrot * (1.0f * ((float)n - 0.5f)) * dy;
-    };
-    for (const auto& pl : read_thin_dams(path(K.thdfile))) {
-      for (size_t ipol = 0; ipol + 1 < pl.size(); ipol++) {
-        const float xpa = pl[ipol].first, ypa = pl[ipol].second, xpb = pl[ipol + 1].first, ypb = pl[ipol + 1].second;
-        const float xta = cosrot * (xpa - x0) + sinrot * (ypa - y0), yta = -sinrot * (xpa - x0) + cosrot * (ypa - y0);
-        const float xtb = cosrot * (xpb - x0) + sinrot * (ypb - y0), ytb = -sinrot * (xpb - x0) + cosrot * (ypb - y0);
-        const int na = (int)(yta / dy) + 1, ma = (int)(xta / dx) + 1, nb = (int)(ytb / dy) + 1, mb = (int)(xtb / dx) + 1;
-        for (int m = std::max(std::min(ma, mb) - 1, 1); m <= std::min(std::max(ma, mb) + 1, mmax); m++) {
-          for (int n = std::max(std::min(na, nb) - 1, 1); n <= std::min(std::max(na, nb) + 1, nmax); n++) {
-            if (!act(n, m)) continue;
-            const int64_t c = OFF(n, m);
-            if (act(n, m + 1) && segments_cross(xpa, ypa, xpb, ypb, xz(n, m), yz(n, m), xz(n, m + 1), yz(n, m + 1)))
-              dam_u[c] = 1;
-            if (act(n + 1, m) && segments_cross(xpa, ypa, xpb, ypb, xz(n, m), yz(n, m), xz(n + 1, m), yz(n + 1, m)))
-              dam_v[c] = 1;
-          }
-        }
-      }
-    }
+    for (const auto& pl : read_polylines(path(K.thdfile), 0))
+      for (const auto& e : crossed_faces(pl)) ((e.first & 1) ? dam_v : dam_u)[e.first >> 1] = 1;
   }
 
   // ---- bathymetry (regular) or subgrid tables -----------------------------------
@@ -691,13 +720,90 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     }
   }
 
+  // ---- weirs (sfincs_structures.f90:38-381) ----------------------------------------
+  // Every face a weir polyline crosses gets the crossed length (the face's
+  // corner-to-corner segment projected onto the weir segment), the larger
+  // crest level and the discharge coefficient interpolated at the face centre
+  // between the segment's end points.  Faces whose crest is above the face
+  // bed (zbuvmx, or the subgrid uv_zmin) become weir faces (kcuv = 3).  The
+  // face centre and corners use half the face width along both axes, as the
+  // reference does (exact for dx = dy).
+  std::vector<uint8_t> weir_u, weir_v;
+  if (!is_none(K.weirfile)) {
+    weir_u.assign(NA, 0);
+    weir_v.assign(NA, 0);
+    struct Acc {
+      float len = 0.0f, height = -9999.0f, cd = 0.0f;
+    };
+    std::map<int64_t, Acc> acc;
+    const float pi = P.pi;
+    for (const auto& pl : read_polylines(path(K.weirfile), 2)) {
+      for (const auto& e : crossed_faces(pl)) {
+        const int64_t c = e.first >> 1;
+        const int dir = (int)(e.first & 1), ipol = e.second;
+        const int m = (int)(c / ld), n = (int)(c % ld) - kGhostPad;
+        const float dxs = dir == 0 ? dy : dx;
+        float xuv, yuv, xuv1, yuv1, xuv2, yuv2;
+        if (dir == 0) {
+          xuv = xz(n, m) + 0.5f * dxs * std::cos(rotation);
+          yuv = yz(n, m) + 0.5f * dxs * std::sin(rotation);
+          xuv1 = xuv + 0.5f * dxs * std::cos(rotation - 0.5f * pi);
+          yuv1 = yuv + 0.5f * dxs * std::sin(rotation - 0.5f * pi);
+          xuv2 = xuv + 0.5f * dxs * std::cos(rotation + 0.5f * pi);
+          yuv2 = yuv + 0.5f * dxs * std::sin(rotation + 0.5f * pi);
+        } else {
+          xuv = xz(n, m) + 0.5f * dxs * std::cos(rotation + 0.5f * pi);
+          yuv = yz(n, m) + 0.5f * dxs * std::sin(rotation + 0.5f * pi);
+          xuv1 = xuv + 0.5f * dxs * std::cos(rotation - pi);
+          yuv1 = yuv + 0.5f * dxs * std::sin(rotation - pi);
+          xuv2 = xuv + 0.5f * dxs * std::cos(rotation);
+          yuv2 = yuv + 0.5f * dxs * std::sin(rotation);
+        }
+        const PolyRow &r0 = pl[(size_t)ipol], &r1 = pl[(size_t)ipol + 1];
+        Acc& a = acc[e.first];
+        a.len = a.len + projected_length(xuv1, yuv1, xuv2, yuv2, r0.x, r0.y, r1.x, r1.y);
+        const float dst1 = std::sqrt((xuv - r0.x) * (xuv - r0.x) + (yuv - r0.y) * (yuv - r0.y));
+        const float dst2 = std::sqrt((xuv - r1.x) * (xuv - r1.x) + (yuv - r1.y) * (yuv - r1.y));
+        const float wfac = dst1 / (dst1 + dst2);
+        a.height = std::max(a.height, r0.p[0] * (1.0f - wfac) + r1.p[0] * wfac);
+        a.cd = r0.p[1] * (1.0f - wfac) + r1.p[1] * wfac;
+      }
+    }
+    for (const auto& e : acc) {
+      const int64_t c = e.first >> 1;
+      const int dir = (int)(e.first & 1);
+      const float bed = P.subgrid ? (dir == 0 ? h.sgz_u : h.sgz_v)[c].x : (dir == 0 ? h.zbmx_u : h.zbmx_v)[c];
+      if (!(e.second.height > bed)) continue;
+      StrucFace w{};
+      w.face = (int)c;
+      w.nm = (int)c;
+      w.nmu = (int)(dir == 0 ? c + ld : c + 1);
+      w.dir = dir;
+      w.height = e.second.height;
+      w.cd = e.second.cd;
+      w.len = e.second.len / (dir == 0 ? dy : dx);
+      h.struc.push_back(w);
+      (dir == 0 ? weir_u : weir_v)[c] = 1;
+    }
+    // a weir on a water-level boundary face: no boundary flux there (sfincs_boundaries.f90:1009)
+    for (auto& b : h.bfaces)
+      if ((b.info & 1 ? weir_v : weir_u)[b.face]) b.info |= 16;
+  }
+  P.nstruc = (int)h.struc.size();
+
   // ---- flags, advection mask, theta smoothing -----------------------------------------------
   h.flags.assign(NA, 0);
   auto KU = [&](int n, int m) -> int { return (n >= 1 && n <= nmax && m >= 1 && m <= mmax) ? kcu[OFF(n, m)] : 0; };
   auto KV = [&](int n, int m) -> int { return (n >= 1 && n <= nmax && m >= 1 && m <= mmax) ? kcv[OFF(n, m)] : 0; };
-  // kcuv after the thin dams
-  auto KUd = [&](int n, int m) -> int { return KU(n, m) != 0 && !dam_u.empty() && dam_u[OFF(n, m)] ? 0 : KU(n, m); };
-  auto KVd = [&](int n, int m) -> int { return KV(n, m) != 0 && !dam_v.empty() && dam_v[OFF(n, m)] ? 0 : KV(n, m); };
+  // kcuv after the thin dams (0) and the weirs (3, applied after the dams)
+  auto after_structures = [&](int n, int m, int k, const std::vector<uint8_t>& weir, const std::vector<uint8_t>& dam) {
+    if (n < 1 || n > nmax || m < 1 || m > mmax) return k;
+    if (!weir.empty() && weir[OFF(n, m)]) return 3;
+    if (!dam.empty() && dam[OFF(n, m)]) return 0;
+    return k;
+  };
+  auto KUd = [&](int n, int m) -> int { return after_structures(n, m, KU(n, m), weir_u, dam_u); };
+  auto KVd = [&](int n, int m) -> int { return after_structures(n, m, KV(n, m), weir_v, dam_v); };
   const bool do_mask = P.advection && advection_mask && nmax > 1;
   for (long long i = 0; i < h.np; i++) {
     const int n = h.z_n[i], m = h.z_m[i];
@@ -983,6 +1089,7 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.qsrc, h.qsrc);
   zero(d.qtsrc, (size_t)std::max(h.p.nsrc, 1));
   up(d.src_cell, h.src_cell);
+  up(d.struc, h.struc);
   up(cmp, h.cmp_off);
   zero(d.st, 1);
 }
@@ -1045,6 +1152,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
     if (h.p.subgrid != subgrid_) throw std::runtime_error("an ensemble must be all-subgrid or all-regular");
     if (h.p.quadtree != qt_) throw std::runtime_error("an ensemble must be all-quadtree or all-regular-grid");
     if (h.p.nsrc > 0) any_src_ = 1;
+    if (h.p.nstruc > 0) any_struc_ = 1;
     bnd_blocks_ = std::max(bnd_blocks_, (h.p.nkcuv2 + h.p.nneu + 127) / 128);
     scns.push_back(models_[i]->dev());
     if (!qt_)
@@ -1140,6 +1248,7 @@ void Runner::launch_continuity_any() {
 void Runner::launch_one() {
   launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_, one());
   launch_momentum_any();
+  if (any_struc_) launch_structures(d_scns_, nscn(), stream_);
   if (any_src_) launch_sources(d_scns_, nscn(), stream_);
   launch_continuity_any();
 }
@@ -1192,6 +1301,7 @@ std::vector<double> Runner::time_kernels(int nsteps) {
     check_cuda(cudaEventRecord(ev[1], stream_), "record");
     launch_momentum_any();
     check_cuda(cudaEventRecord(ev[2], stream_), "record");
+    if (any_struc_) launch_structures(d_scns_, nscn(), stream_);
     if (any_src_) launch_sources(d_scns_, nscn(), stream_);
     check_cuda(cudaEventRecord(ev[3], stream_), "record");
     launch_continuity_any();
@@ -1233,6 +1343,7 @@ void Runner::step_once(cudaEvent_t continuity_after) {
   if (continuity_after) {
     launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_, one());
     launch_momentum_any();
+    if (any_struc_) launch_structures(d_scns_, nscn(), stream_);
     if (any_src_) launch_sources(d_scns_, nscn(), stream_);
     check_cuda(cudaStreamWaitEvent(stream_, continuity_after, 0), "wait for the source terms");
     launch_continuity_any();

@@ -51,6 +51,7 @@ struct HostModel {
   std::vector<float> tprcp, vprcp, twnd, wmag, wdir, cdval;
   std::vector<float> tsrc, qsrc;     // qsrc [ntsrc][nsrc]
   std::vector<int32_t> src_cell;
+  std::vector<StrucFace> struc;       // weir faces
   long long n_kcs1 = 0;
   double area_total_kcs1 = 0;
   std::vector<int2> tiles;  // (n0, m0) of every 32 x 8 tile holding an active cell
@@ -75,7 +76,7 @@ struct Keys {
   float hmin_cfl = 0, dtmax = 0, uvmax = 0, nuviscdim = 0, manning = 0, manning_land = 0, manning_sea = 0,
         rghlevland = 0, qinf = 0, qinf_zmin = 0;
   bool viscosity = false, advection_mask = true, quadtree = false;
-  std::string thdfile;  // thin dams (regular grids)
+  std::string thdfile, weirfile;  // thin dams and weirs (regular grids)
   std::string qtrfile, depfile, mskfile, indexfile, sbgfile, manningfile, bndfile, bzsfile, srcfile, disfile,
       wndfile, qinffile, prcpfile;
 };
@@ -178,7 +179,7 @@ class Runner {
   // Issue nsteps steps with CUDA events between the launches; returns the mean
   // duration (ms) of [step+boundary, momentum, sources, continuity] launches.
   std::vector<double> time_kernels(int nsteps);
-  int launches_per_step() const { return 3 + any_src_ + (qt_ && nqcuv_ > 0 ? 1 : 0); }
+  int launches_per_step() const { return 3 + any_src_ + any_struc_ + (qt_ && nqcuv_ > 0 ? 1 : 0); }
 
  private:
   void build_graph(int chunk);
@@ -196,7 +197,7 @@ class Runner {
   int subgrid_ = 0;
   int qt_ = 0;                       // quadtree models: face / combined-point / cell work lists in d_tiles_
   int nqf_ = 0, nqcuv_ = 0, nqc_ = 0;
-  int any_src_ = 0;
+  int any_src_ = 0, any_struc_ = 0;
   cudaStream_t stream_ = nullptr;
   bool own_stream_ = true;
   cudaGraphExec_t graph_ = nullptr;
@@ -217,6 +218,7 @@ void launch_step_bnd(const ScnDev* d_scns, int nscn, int bnd_blocks, cudaStream_
 void launch_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, int variant,
                      cudaStream_t s);
 void launch_sources(const ScnDev* d_scns, int nscn, cudaStream_t s);
+void launch_structures(const ScnDev* d_scns, int nscn, cudaStream_t s);
 void launch_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s);
 
 void check_cuda(cudaError_t e, const char* what);

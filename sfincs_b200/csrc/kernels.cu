@@ -349,7 +349,7 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan&
     zs0nmb = fmaxf(zs0nmb, b.floor);
     float qq = 0.0f, uu = 0.0f;
     float um = pre.um;
-    if (hnmb < S.huthresh + 1.0e-6f) {
+    if (hnmb < S.huthresh + 1.0e-6f || (b.info & 16)) {  // bit 4: a weir sits on this face (kcuv 3)
       um = 0.0f;
     } else {
       const float sq = sqrtf(S.g / hnmb);
@@ -613,6 +613,50 @@ __global__ void k_sources(const ScnDev* __restrict__ scns) {
 }
 
 // --------------------------------------------------------------------------
+// Weirs: fluxes over structure faces after the momentum faces
+// (sfincs_structures.f90:592-697), one CTA per scenario.  The flux goes into
+// the buffers this step's momentum wrote, which continuity reads.
+// --------------------------------------------------------------------------
+__global__ void k_structures(const ScnDev* __restrict__ scns) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
+  const ScnDev& S = scns[blockIdx.x];
+  const StepState& st = *S.st;
+  if (!st.run) return;
+  const int p1 = st.parity ^ 1;
+  for (int i = threadIdx.x; i < S.nstruc; i += blockDim.x) {
+    const StrucFace w = S.struc[i];
+    float* Q = w.dir == 0 ? S.qu[p1] : S.qv[p1];
+    float* U = w.dir == 0 ? S.uu[p1] : S.vv[p1];
+    const float zsnm = S.zs[w.nm], zsnmu = S.zs[w.nmu];
+    float q = 0.0f;
+    if (!(zsnm < w.height && zsnmu < w.height)) {
+      // broad-crested weir (type 1): submerged or free flow
+      const float cweir = 1.7049f, mlim = 0.0f;
+      float h1, h2, idir;
+      if (zsnm > zsnmu) {
+        idir = 1.0f;
+        h1 = zsnm - w.height;
+        h2 = zsnmu - w.height;
+      } else {
+        idir = -1.0f;
+        h1 = zsnmu - w.height;
+        h2 = zsnm - w.height;
+      }
+      float qstruc;
+      if (h2 > 2.0f / 3.0f * h1)
+        qstruc = w.cd * h2 * sqrtf(2.0f * 9.81f * (h1 - h2) / (1.0f - mlim));
+      else  // h1**1.5 as h1 * sqrt(h1): two correctly rounded operations, within 1.5 ulp of the power
+        qstruc = w.cd * cweir * (h1 * sqrtf(h1));
+      qstruc = qstruc * w.len;
+      q = qstruc * idir;
+    }
+    Q[w.face] = q;
+    U[w.face] = 0.0f;
+  }
+}
+
+// --------------------------------------------------------------------------
 // Continuity: one thread per cell.
 // --------------------------------------------------------------------------
 template <bool SG>
@@ -735,6 +779,10 @@ void launch_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int 
 
 void launch_sources(const ScnDev* d_scns, int nscn, cudaStream_t s) {
   launch_pdl(k_sources, dim3(nscn), dim3(32), 0, s, d_scns);
+}
+
+void launch_structures(const ScnDev* d_scns, int nscn, cudaStream_t s) {
+  launch_pdl(k_structures, dim3(nscn), dim3(128), 0, s, d_scns);
 }
 
 void launch_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {

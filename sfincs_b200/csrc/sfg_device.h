@@ -44,6 +44,20 @@ enum : uint16_t {
 // ping-pong buffers, so its (zero) writes are skipped.
 enum : uint8_t { KF_WET = 1u, KF_WET2 = 2u };
 
+// One weir face (kcuv = 3, sfincs_structures.f90:38-381): the uv face with
+// the dense offsets of its two cells, the crest level and discharge
+// coefficient interpolated along the weir polyline, and the crossed length
+// relative to the face width.
+struct alignas(16) StrucFace {
+  int face;      // dense offset of the face (the cell that owns it)
+  int nm, nmu;   // dense offsets of the cells on either side
+  int dir;       // 0: u face, 1: v face
+  float height;  // crest level
+  float cd;      // discharge coefficient
+  float len;     // crossed length / face width
+  int pad;
+};
+
 // One water-level boundary face (kcuv == 2), packed so one thread reads it in
 // three 16-byte loads.  The boundary cell's level is recomputed per face from
 // the two nearest boundary points (sfincs_boundaries.f90:806-876).
@@ -51,7 +65,8 @@ struct alignas(16) BndFace {
   int face;      // dense offset of the face
   int nmb;       // dense offset of the boundary cell
   int nmi;       // dense offset of the interior cell
-  int info;      // bit0: v face; bit1: ibuvdir = +1 (else -1); bit2: outflow cell (kcs 3); bit3: multiple bnd points
+  int info;      // bit0: v face; bit1: ibuvdir = +1 (else -1); bit2: outflow cell (kcs 3); bit3: multiple bnd points;
+                 // bit4: a weir on the face (kcuv 3: no boundary flux)
   int i1, i2;    // nearest boundary points (0-based)
   float fac;     // weight of i1
   float zbuv;    // zbuv of the face (regular grids; sfincs_domain.f90:1692)
@@ -189,6 +204,8 @@ struct ScnDev {
   const float* qsrc;     // [ntsrc][nsrc]
   float* qtsrc;          // [nsrc]
   const int* src_cell;   // [nsrc]
+  int nstruc;            // weir faces
+  const StrucFace* struc;  // [nstruc]
   float pi;
   StepState* st;
   // ---- quadtree (quadtree != 0; the regular-grid fields above that index

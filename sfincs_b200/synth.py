@@ -300,6 +300,7 @@ class RegularModel:
     src: Optional[np.ndarray] = None     # (nsrc, 2)
     dis: Optional[np.ndarray] = None     # (nt, 1+nsrc)
     thd: Optional[List[np.ndarray]] = None  # thin dams: polylines, each (npoints, 2) x, y
+    weir: Optional[List[np.ndarray]] = None  # weirs: polylines, each (npoints, 4) x, y, crest level, Cd
 
     @property
     def nmax(self):
@@ -359,6 +360,14 @@ class RegularModel:
                     for x, y in pl:
                         f.write(f"{x:.4f} {y:.4f}\n")
             inp["thdfile"] = "sfincs.thd"
+        if self.weir:
+            with open(os.path.join(d, "sfincs.weir"), "w") as f:
+                for i, pl in enumerate(self.weir):
+                    pl = np.asarray(pl, np.float64)
+                    f.write(f"WEIR{i + 1:02d}\n{pl.shape[0]} 4\n")
+                    for x, y, z, cd in pl:
+                        f.write(f"{x:.4f} {y:.4f} {z:.4f} {cd:.4f}\n")
+            inp["weirfile"] = "sfincs.weir"
         inp.update(self.params)
         with open(os.path.join(d, "sfincs.inp"), "w") as f:
             for k, v in inp.items():

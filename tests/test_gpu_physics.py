@@ -4,8 +4,8 @@ The main parity tests (test_gpu_parity.py) run the default switches. Here each
 case turns on terms that those leave off: Coriolis, wind stress from a time
 series, theta smoothing, the "original" advection scheme, the slope limiter,
 friction2d off, viscosity and no wiggle suppression on a subgrid model, c2d
-infiltration, point sources, Neumann and outflow boundary cells, and thin dams
-(regular and subgrid). For each
+infiltration, point sources, Neumann and outflow boundary cells, thin dams and
+weirs (regular and subgrid). For each
 case the CUDA core is compared with the oracle in the core's own precision
 after 1, 2, 4, 10, 40 and 100 steps, on the default kernel path and on the
 per-thread-load path. The bars are those of the main stepwise test: time
@@ -95,10 +95,26 @@ def case_subgrid_thin_dams(tmp_path):
     return m
 
 
+def case_weirs(tmp_path):
+    m = _plain(tmp_path, advection=1, theta=0.9)
+    # a weir across the channel with a varying crest, one over the boundary
+    # column, and a thin dam under the first weir (the weir wins)
+    m.weir = [np.array([[6000.0, -200.0, -1.0, 1.0], [6000.0, 5000.0, 0.5, 0.8], [7000.0, 9800.0, -2.0, 0.9]]),
+              np.array([[400.0, 2000.0, 1.5, 1.0], [400.0, 6000.0, 1.5, 1.0]])]
+    m.thd = [np.array([[5800.0, 3000.0], [6200.0, 3000.0]])]
+    return m
+
+
+def case_subgrid_weirs(tmp_path):
+    m = _subgrid(tmp_path, advection=1)
+    m.weir = [np.array([[5000.0, -100.0, 0.5, 1.0], [5000.0, 10100.0, 2.5, 1.0]])]
+    return m
+
+
 CASES = {f.__name__[5:]: f for f in (case_coriolis_wind_theta, case_original_advection_slopelim_nofric2d,
                                       case_boundary_kinds, case_plain_infiltration, case_subgrid_visc_nowiggle,
                                       case_subgrid_infiltration_sources, case_thin_dams_theta,
-                                      case_subgrid_thin_dams)}
+                                      case_subgrid_thin_dams, case_weirs, case_subgrid_weirs)}
 
 
 def _model(d, variant):

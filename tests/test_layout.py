@@ -117,9 +117,9 @@ def test_subgrid_tables_and_volumes(tmp_path):
 
 def test_unsupported_inputs_are_refused(tmp_path):
     m = synth.plain_regular(nmax=6, mmax=7, dx=300.0, tstop=600.0, nbumps=1)
-    m.params["weirfile"] = "sfincs.weir"
+    m.params["drnfile"] = "sfincs.drn"
     d = m.write(str(tmp_path))
-    with pytest.raises(RuntimeError, match="weirfile"):
+    with pytest.raises(RuntimeError, match="drnfile"):
         B.layout(d, "counts", 10)
 
 
@@ -138,3 +138,38 @@ def test_thin_dam_faces(tmp_path):
     dammed = (kcuv == 0) & (kcuv0 != 0)
     assert np.array_equal(dammed & (dirn == 0), (dirn == 0) & (mcol == 8))
     assert not np.any(dammed & (dirn == 1))
+
+
+def _weir_model():
+    m = synth.plain_regular(nmax=14, mmax=17, dx=300.0, tstop=600.0, nbumps=5)
+    m.params.update(advection=1, theta=0.9)
+    m.weir = [np.array([[3000.0, -100.0, 2.0, 1.0], [3000.0, 2000.0, 3.0, 0.8], [3300.0, 4300.0, 1.0, 0.9]]),
+              np.array([[700.0, 800.0, -20.0, 1.1], [2100.0, 3100.0, 5.0, 0.7]]),
+              np.array([[300.0, 1000.0, 4.0, 1.0], [300.0, 2500.0, 4.0, 1.0]])]  # over the boundary column
+    m.thd = [np.array([[2950.0, 500.0], [3050.0, 500.0]])]  # a dam under the weir: the weir wins
+    return m
+
+
+def test_weir_faces_match_oracle(tmp_path):
+    """Weir faces (sfincs_structures.f90:38-381): which faces, their crest
+    level, discharge coefficient and relative length, and the face activity
+    (kcuv = 3 is not a momentum face) agree with the oracle bit for bit."""
+    d = _weir_model().write(str(tmp_path))
+    o = _oracle(d, "f32")
+    n = int(o.get("nrstructures", 1)[0])
+    assert n > 10
+    assert int(B.layout(d, "nstruc", 1)[0]) == n
+    so = o.get("struc", 4 * n).reshape(n, 4)
+    sh = B.layout(d, "struc", 5 * n).reshape(n, 5)
+    uv_nm = o.get("uv_nm").astype(np.int64) - 1
+    uv_dir = o.get("uv_dir").astype(np.int64)
+    ip = so[:, 0].astype(np.int64) - 1
+    assert np.array_equal(uv_nm[ip], sh[:, 0].astype(np.int64))
+    assert np.array_equal(uv_dir[ip], sh[:, 1].astype(np.int64))
+    for k in range(3):
+        assert np.array_equal(so[:, 1 + k].astype(np.float32), sh[:, 2 + k].astype(np.float32)), k
+    flags = B.layout(d, "flags", int(o.scalars()["np"])).astype(np.int64)
+    kcuv = o.get("kcuv")
+    bit = np.where(uv_dir == 0, F_UACT, F_VACT)
+    assert np.array_equal((flags[uv_nm] & bit) > 0, np.isin(kcuv, (1, 6)))
+    assert np.count_nonzero(kcuv == 3) == n

@@ -167,3 +167,35 @@ def test_thin_dam_holds_a_dam_break(tmp_path):
     assert np.all(z[mm >= 13] == 0.0)
     assert z[mm == 12].max() > 0.05  # the front arrived at the dam
     assert abs(np.sum(z + 1.0) - v0) <= 1e-10 * v0
+
+
+def test_weir_free_and_submerged_flow(tmp_path):
+    """Broad-crested weir (sfincs_structures.f90:592-697) in a closed basin:
+    after one step the flux over every weir face is the free-flow discharge
+    Cd 1.7049 h1^1.5, or the submerged one Cd h2 sqrt(2 g (h1 - h2)), times
+    the crossed length, from the levels at the start of the step."""
+    m = _closed(synth.plain_regular(nmax=8, mmax=12, dx=100.0, tstop=3600.0, nbumps=0))
+    m.zb = np.full_like(m.zb, -2.0)
+    m.weir = [np.array([[600.0, -50.0, 0.0, 0.9], [600.0, 850.0, 0.0, 0.9]])]  # between columns 6 and 7
+    d = m.write(str(tmp_path))
+    o = _oracle(d)
+    assert int(o.get("nrstructures", 1)[0]) == 8
+    mm = o.get("nm_m").astype(int)
+    nn = o.get("nm_n").astype(int)
+    # rows 1-4: free flow (east below the crest); rows 5-8: submerged
+    zs = np.where(mm <= 6, 0.5, np.where(nn <= 4, -0.5, 0.45))
+    o.set("zs", zs)
+    o.update(-1000.0, 1)
+    q = o.get("q")
+    st = o.get("struc", 32).reshape(8, 4)
+    nmu = o.get("uv_nmu").astype(int) - 1
+    for ip, crest, cd, rel in st:
+        ip = int(ip) - 1
+        h1 = 0.5 - crest
+        h2 = zs[nmu[ip]] - crest  # the east neighbour, column 7
+        if h2 > 2.0 / 3.0 * h1:
+            want = cd * h2 * np.sqrt(2.0 * 9.81 * (h1 - h2))
+        else:
+            want = cd * 1.7049 * h1 ** 1.5
+        assert q[ip] == pytest.approx(want * rel, rel=1e-6)
+        assert rel == pytest.approx(1.0, abs=1e-6)
