@@ -179,7 +179,7 @@ struct Model {
   int bndtype, iadvection, baro, storevelmax, storefluxmax, storetwet, storetzsmax;
   std::string inputtype, advstr, qtrfile, depfile, zsinifile, rstfile, mskfile, indexfile, sbgfile, manningfile,
       bndfile, bzsfile, bcafile, bzifile, srcfile, disfile, wndfile, prcpfile, qinffile, scsfile, sefffile,
-      psifile, f0file, infiltrationfile, inftype, thdfile, weirfile;
+      psifile, f0file, infiltrationfile, inftype, thdfile, weirfile, drnfile;
   bool coriolis, viscosity, friction2d, advection_mask, wiggle_suppression, h73table, spinup_meteo;
   float t0, t1, g, pi, fcorio, twet_threshold;
   bool crsgeo = false, advection, thetasmoothing, subgrid, store_maximum_waterlevel, store_maximum_velocity,
@@ -231,7 +231,11 @@ struct Model {
   long ntwnd = 0, itwndlast = 1, ntprcp = 0, itprcplast = 1;
   F1<float> twnd, wndmag, wnddir, tprcpt, tprcpv, cdval;
   F1<float> tauwu, tauwv, prcp, netprcp, qext, qinffield, qinfmap, cumprcp, cuminf;
-  long nsrc = 0, ntsrc = 0, itsrclast = 1;
+  long nsrc = 0, ntsrc = 0, itsrclast = 1, ndrn = 0, nsrcdrn = 0;
+  float structure_relax = 10.0f;
+  F1<int8_t> drainage_type, drainage_status;
+  F2<float> drainage_params;  // (ndrn, 6)
+  F1<float> drainage_distance, drainage_fraction_open;
   F1<int32_t> nmindsrc;
   F1<float> tsrc, qtsrc;
   F2<float> qsrc;
@@ -327,6 +331,8 @@ struct Model {
     disfile = in.str("disfile", "none");
     thdfile = in.str("thdfile", "none");
     weirfile = in.str("weirfile", "none");
+    drnfile = in.str("drnfile", "none");
+    structure_relax = in.real("structure_relax", 10.0f);
     wndfile = in.str("wndfile", "none");
     prcpfile = in.str("prcfile", "none");
     if (prcpfile.substr(0, 4) == "none") prcpfile = in.str("precipfile", "none");
@@ -1718,27 +1724,77 @@ struct Model {
   }
 
   // read_discharges (src/dis branch): sfincs_discharges.f90:8-324
+  // read_discharges: sfincs_discharges.f90:8-320 (point sources, then drainage
+  // structures, whose intake and outfall follow the sources in nmindsrc/qtsrc)
   void read_discharges() {
     nsrc = 0;
     ntsrc = 0;
     itsrclast = 1;
-    if (srcfile.substr(0, 4) == "none") return;
-    auto xy = read_ascii_table(path(srcfile));
-    nsrc = (long)xy.size();
-    auto tb = read_ascii_table(path(disfile));
-    ntsrc = (long)tb.size();
-    nmindsrc.alloc(nsrc);
-    qtsrc.alloc(nsrc);
-    tsrc.alloc(ntsrc);
-    qsrc.alloc(nsrc, ntsrc);
-    for (long it = 1; it <= ntsrc; it++) {
-      tsrc(it) = (float)tb[it - 1][0];
-      for (long is = 1; is <= nsrc; is++) qsrc(is, it) = (float)tb[it - 1][is];
+    ndrn = 0;
+    std::vector<std::vector<double>> xy, tb;
+    std::vector<std::string> drn_lines;
+    if (srcfile.substr(0, 4) != "none") {
+      xy = read_ascii_table(path(srcfile));
+      nsrc = (long)xy.size();
+      tb = read_ascii_table(path(disfile));
+      ntsrc = (long)tb.size();
     }
-    for (long is = 1; is <= nsrc; is++) {
-      long nmq = find_quadtree_cell((float)xy[is - 1][0], (float)xy[is - 1][1]);
-      nmindsrc(is) = nmq > 0 ? index_sfincs_in_quadtree(nmq) : 0;
-      if (nmindsrc(is) == 0) throw std::runtime_error("oracle: source point outside the active mesh");
+    if (drnfile.substr(0, 4) != "none") {
+      std::ifstream fin(path(drnfile));
+      if (!fin) throw std::runtime_error("oracle: cannot open " + drnfile);
+      for (std::string l; std::getline(fin, l);) {
+        for (char& ch : l)
+          if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
+        if (l.find_first_not_of(' ') != std::string::npos) drn_lines.push_back(l);
+      }
+      ndrn = (long)drn_lines.size();
+    }
+    nsrcdrn = nsrc + 2 * ndrn;
+    if (nsrcdrn > 0) {
+      nmindsrc.alloc(nsrcdrn);
+      qtsrc.alloc(nsrcdrn);
+    }
+    if (nsrc > 0) {
+      tsrc.alloc(ntsrc);
+      qsrc.alloc(nsrc, ntsrc);
+      for (long it = 1; it <= ntsrc; it++) {
+        tsrc(it) = (float)tb[it - 1][0];
+        for (long is = 1; is <= nsrc; is++) qsrc(is, it) = (float)tb[it - 1][is];
+      }
+      for (long is = 1; is <= nsrc; is++) {
+        long nmq = find_quadtree_cell((float)xy[is - 1][0], (float)xy[is - 1][1]);
+        nmindsrc(is) = nmq > 0 ? index_sfincs_in_quadtree(nmq) : 0;
+        if (nmindsrc(is) == 0) throw std::runtime_error("oracle: source point outside the active mesh");
+      }
+    }
+    if (ndrn > 0) {
+      drainage_type.alloc(ndrn);
+      drainage_params.alloc(ndrn, 6);
+      drainage_status.alloc(ndrn, 1);             // open
+      drainage_distance.alloc(ndrn);
+      drainage_fraction_open.alloc(ndrn, 1.0f);  // fully open
+      for (long idrn = 1; idrn <= ndrn; idrn++) {
+        std::istringstream ls(drn_lines[idrn - 1]);
+        float xsnk, ysnk, xsrc, ysrc;
+        int type = 0;
+        ls >> xsnk >> ysnk >> xsrc >> ysrc >> type;
+        int npars = (type >= 1 && type <= 3) ? 1 : ((type == 4 || type == 5) ? 6 : 0);
+        if (npars == 0) throw std::runtime_error("oracle: drainage type not recognized");
+        drainage_type(idrn) = (int8_t)type;
+        for (int k = 1; k <= npars; k++)
+          if (!(ls >> drainage_params(idrn, k))) throw std::runtime_error("oracle: drainage parameters missing");
+        long j = nsrc + idrn * 2 - 1;
+        long nmq = find_quadtree_cell(xsnk, ysnk);
+        if (nmq > 0) nmindsrc(j) = index_sfincs_in_quadtree(nmq);
+        j = nsrc + idrn * 2;
+        nmq = find_quadtree_cell(xsrc, ysrc);
+        if (nmq > 0) nmindsrc(j) = index_sfincs_in_quadtree(nmq);
+        long a = nmindsrc(nsrc + idrn * 2 - 1), b = nmindsrc(nsrc + idrn * 2);
+        if (a == 0 || b == 0) throw std::runtime_error("oracle: drainage point outside the active mesh");
+        float xsnk_tmp = z_xz(a), ysnk_tmp = z_yz(a), xsrc_tmp = z_xz(b), ysrc_tmp = z_yz(b);
+        drainage_distance(idrn) =
+            std::sqrt((xsrc_tmp - xsnk_tmp) * (xsrc_tmp - xsnk_tmp) + (ysrc_tmp - ysnk_tmp) * (ysrc_tmp - ysnk_tmp));
+      }
     }
   }
 
@@ -1978,18 +2034,95 @@ struct Model {
   }
 
   // update_discharges (point sources): sfincs_discharges.f90:325-368
+  // update_discharges: sfincs_discharges.f90:325-659
   void update_discharges(double tt) {
-    if (nsrc <= 0) return;
-    for (long its = itsrclast; its <= ntsrc; its++) {
-      if ((double)tsrc(its) > tt) {
-        long i0 = std::max(its - 1, 1L);
-        for (long is = 1; is <= nsrc; is++)
-          qtsrc(is) = (float)((double)qsrc(is, i0) +
-                              (double)(qsrc(is, its) - qsrc(is, i0)) * (tt - (double)tsrc(i0)) /
-                                  (double)(tsrc(its) - tsrc(i0)));
-        itsrclast = its - 1 >= 1 ? its - 1 : 1;
-        break;
+    if (nsrc > 0) {
+      for (long its = itsrclast; its <= ntsrc; its++) {
+        if ((double)tsrc(its) > tt) {
+          long i0 = std::max(its - 1, 1L);
+          for (long is = 1; is <= nsrc; is++)
+            qtsrc(is) = (float)((double)qsrc(is, i0) +
+                                (double)(qsrc(is, its) - qsrc(is, i0)) * (tt - (double)tsrc(i0)) /
+                                    (double)(tsrc(its) - tsrc(i0)));
+          itsrclast = its - 1 >= 1 ? its - 1 : 1;
+          break;
+        }
       }
+    }
+    const bool core = std::is_same<TZ, float>::value;  // the core's precision: zs in FP32
+    for (long idrn = 1; idrn <= ndrn; idrn++) {
+      long jin = nsrc + idrn * 2 - 1, jout = nsrc + idrn * 2;
+      long nmin = nmindsrc(jin), nmout = nmindsrc(jout);
+      if (!(nmin > 0 && nmout > 0)) continue;
+      const double zin = (double)zs(nmin), zout = (double)zs(nmout);  // zs is real*8 in the reference
+      float qq = 0.0f;
+      int type = drainage_type(idrn);
+      if (type == 1) {  // pump
+        qq = drainage_params(idrn, 1);
+      } else if (type == 2 || type == 3) {  // culvert, check valve
+        if (zin > zout)
+          qq = (float)((double)drainage_params(idrn, 1) * std::sqrt(zin - zout));
+        else
+          qq = (float)((double)(-drainage_params(idrn, 1)) * std::sqrt(zout - zin));
+        if (type == 3) qq = std::max(qq, 0.0f);
+      } else {  // controlled gates (4: by level at the intake, 5: by time)
+        float wdt = drainage_params(idrn, 1), zsill = drainage_params(idrn, 2), mng = drainage_params(idrn, 3);
+        float tcls = drainage_params(idrn, 6);
+        float dzds = (float)((zout - zin) / (double)drainage_distance(idrn));
+        float frac = drainage_fraction_open(idrn);
+        float hgate = (float)std::max(std::max(zin, zout) - (double)zsill, 0.0);
+        float dfrac = dt / tcls;
+        float qq0 = -qtsrc(jin) / (wdt * std::max(frac, 0.001f));
+        int status = drainage_status(idrn);
+        if (type == 4) {
+          float zmin = drainage_params(idrn, 4), zmax = drainage_params(idrn, 5);
+          if (status == 0) {
+            if (zin > (double)zmin && zin < (double)zmax) status = 3;
+          } else if (status == 1) {
+            if (zin <= (double)zmin || zin >= (double)zmax) status = 2;
+          }
+        } else {
+          float tclose = drainage_params(idrn, 4), topen = drainage_params(idrn, 5);
+          if (status == 0) {
+            if (tt >= (double)topen) status = 3;
+          } else if (status == 1) {
+            if (tt >= (double)tclose && tt < (double)topen) status = 2;
+          }
+        }
+        if (status == 2) {
+          frac = frac - dfrac;
+          if (frac < 0.0f) {
+            frac = 0.0f;
+            status = 0;
+          }
+        } else if (status == 3) {
+          frac = frac + dfrac;
+          if (frac > 1.0f) {
+            frac = 1.0f;
+            status = 1;
+          }
+        }
+        drainage_fraction_open(idrn) = frac;
+        drainage_status(idrn) = (int8_t)status;
+        // hgate**(7.0/3.0); the core's precision evaluates it as hgate**2 * cbrt(hgate)
+        float h73 = core ? hgate * hgate * std::cbrt(hgate) : std::pow(hgate, 7.0f / 3.0f);
+        qq = (qq0 - g * hgate * dzds * dt) / (1.0f + g * (mng * mng) * dt * std::fabs(qq0) / h73);
+        qq = qq * wdt * frac;
+      }
+      qq = 1.0f / (structure_relax / dt) * qq + (1.0f - (1.0f / (structure_relax / dt))) * -qtsrc(jin);
+      if (subgrid) {
+        if (qq > 0.0f)
+          qq = (float)std::min((double)qq, std::max((double)z_volume(nmin), 0.0) / (double)dt);
+        else
+          qq = (float)std::max((double)qq, -std::max((double)z_volume(nmout), 0.0) / (double)dt);
+      } else {
+        if (qq > 0.0f)
+          qq = (float)std::min((double)qq, std::max((zin - (double)zb(nmin)) * (double)cell_area(z_flags_iref(nmin)), 0.0) / (double)dt);
+        else
+          qq = (float)std::max((double)qq, -std::max((zout - (double)zb(nmout)) * (double)cell_area(z_flags_iref(nmout)), 0.0) / (double)dt);
+      }
+      qtsrc(jin) = -qq;
+      qtsrc(jout) = qq;
     }
   }
 
@@ -2195,7 +2328,7 @@ struct Model {
 
   // compute_water_levels_regular: sfincs_continuity.f90:46-262
   void compute_water_levels_regular(float dtt, double tt) {
-    for (long is = 1; is <= nsrc; is++) {
+    for (long is = 1; is <= nsrcdrn; is++) {
       long nm = nmindsrc(is);
       zs(nm) = (TZ)std::max((double)(zs(nm) + (TZ)(qtsrc(is) * dtt / cell_area(z_flags_iref(nm)))), (double)zb(nm));
     }
@@ -2218,7 +2351,7 @@ struct Model {
 
   // compute_water_levels_subgrid: sfincs_continuity.f90:265-624
   void compute_water_levels_subgrid(float dtt, double tt) {
-    for (long is = 1; is <= nsrc; is++) {
+    for (long is = 1; is <= nsrcdrn; is++) {
       long nm = nmindsrc(is);
       if (z_volume(nm) >= 0.0 || (qtsrc(is) < 0.0f && z_volume(nm) >= 0.0))
         z_volume(nm) = z_volume(nm) + (TV)(qtsrc(is) * dtt);

@@ -173,7 +173,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   std::string prcpfile = in.str("prcfile", "none");
   if (is_none(prcpfile)) prcpfile = in.str("precipfile", "none");
   // Inputs outside this core's path: refuse loudly instead of silently ignoring physics.
-  for (const char* k : {"bcafile", "bzifile", "bdrfile", "drnfile", "volfile", "spwfile",
+  for (const char* k : {"bcafile", "bzifile", "bdrfile", "volfile", "spwfile",
                         "amufile", "amvfile", "ampfile", "amprfile", "netbndbzsbzifile", "netsrcdisfile",
                         "netamuamvfile", "netamprfile", "netampfile", "netspwfile", "infiltration_file",
                         "scsfile", "sefffile", "psifile", "f0file", "wavemaker_wvmfile", "wvmfile"}) {
@@ -187,7 +187,10 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   if (inputtype != "bin") throw std::runtime_error("only inputformat = bin is supported");
   if (bndtype != 1) throw std::runtime_error("only bndtype = 1 is supported");
   const bool quadtree = !is_none(qtrfile);
-  const std::string thdfile = in.str("thdfile", "none"), weirfile = in.str("weirfile", "none");
+  const std::string thdfile = in.str("thdfile", "none"), weirfile = in.str("weirfile", "none"),
+                    drnfile = in.str("drnfile", "none");
+  if (quadtree && !is_none(drnfile)) throw std::runtime_error("input 'drnfile' is not supported on quadtree grids by this core");
+  P.structure_relax = in.real("structure_relax", 10.0f);
   if (quadtree && !is_none(thdfile)) throw std::runtime_error("input 'thdfile' is not supported on quadtree grids by this core");
   if (quadtree && !is_none(weirfile)) throw std::runtime_error("input 'weirfile' is not supported on quadtree grids by this core");
   if (!quadtree && (nmax <= 0 || mmax <= 0)) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
@@ -234,7 +237,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   k.qinf_zmin = qinf_zmin; k.advection_mask = advection_mask; k.qtrfile = qtrfile; k.depfile = depfile;
   k.mskfile = mskfile; k.indexfile = indexfile; k.sbgfile = sbgfile; k.manningfile = manningfile;
   k.bndfile = bndfile; k.bzsfile = bzsfile; k.srcfile = srcfile; k.disfile = disfile; k.wndfile = wndfile;
-  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile; k.weirfile = weirfile;
+  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile; k.weirfile = weirfile; k.drnfile = drnfile;
   return k;
 }
 
@@ -904,6 +907,49 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     P.nsrc = nsrc;
     P.ntsrc = (int)h.tsrc.size();
   }
+  // drainage structures (sfincs_discharges.f90:70-320): one line each,
+  // "x_intake y_intake x_outfall y_outfall type params...", the intake and
+  // outfall cells appended after the point sources
+  if (!is_none(K.drnfile)) {
+    FILE* fp = std::fopen(path(K.drnfile).c_str(), "r");
+    if (!fp) throw std::runtime_error("cannot open drainage file " + K.drnfile);
+    char buf[4096];
+    auto cell_of = [&](float x, float y) -> int64_t {
+      const float xt = cosrot * (x - x0) + sinrot * (y - y0);
+      const float yt = -sinrot * (x - x0) + cosrot * (y - y0);
+      const int n = (int)(yt / dy) + 1, m = (int)(xt / dx) + 1;  // sfincs_quadtree.F90:788-790
+      if (!act(n, m)) throw std::runtime_error("drainage point outside the active mesh");
+      return OFF(n, m);
+    };
+    while (std::fgets(buf, sizeof buf, fp)) {
+      std::string l(buf);
+      for (char& ch : l)
+        if (ch == ',' || ch == '\t' || ch == '\r' || ch == '\n') ch = ' ';
+      if (l.find_first_not_of(' ') == std::string::npos) continue;
+      float xs, ys, xo, yo, p[6] = {0, 0, 0, 0, 0, 0};
+      int type = 0;
+      const int got = std::sscanf(l.c_str(), "%f %f %f %f %d %f %f %f %f %f %f", &xs, &ys, &xo, &yo, &type, &p[0], &p[1],
+                                  &p[2], &p[3], &p[4], &p[5]);
+      const int npars = (type >= 1 && type <= 3) ? 1 : ((type == 4 || type == 5) ? 6 : 0);
+      if (got < 5 || npars == 0) throw std::runtime_error("drainage type not recognized in " + K.drnfile);
+      if (got < 5 + npars) throw std::runtime_error("drainage type " + std::to_string(type) + " requires " +
+                                                    std::to_string(npars) + " parameters");
+      DrnDev d{};
+      d.type = type;
+      const int64_t ci = cell_of(xs, ys), co = cell_of(xo, yo);
+      d.cin = (int)ci;
+      d.cout = (int)co;
+      for (int k = 0; k < npars; k++) d.p[k] = p[k];
+      const int ni = (int)(ci % ld) - kGhostPad, mi = (int)(ci / ld), no = (int)(co % ld) - kGhostPad, mo = (int)(co / ld);
+      const float xsnk = xz(ni, mi), ysnk = yz(ni, mi), xsrc = xz(no, mo), ysrc = yz(no, mo);
+      d.distance = std::sqrt((xsrc - xsnk) * (xsrc - xsnk) + (ysrc - ysnk) * (ysrc - ysnk));
+      h.drn.push_back(d);
+      h.src_cell.push_back((int32_t)ci);
+      h.src_cell.push_back((int32_t)co);
+    }
+    std::fclose(fp);
+  }
+  P.ndrn = (int)h.drn.size();
   // 32 x 8 cell tiles that hold at least one active cell (the work list of the
   // cell kernels; a runner concatenates the lists of its models)
   for (int m0 = 1; m0 <= P.mmax; m0 += 8)
@@ -1087,9 +1133,12 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.cdval, h.cdval);
   up(d.tsrc, h.tsrc);
   up(d.qsrc, h.qsrc);
-  zero(d.qtsrc, (size_t)std::max(h.p.nsrc, 1));
+  zero(d.qtsrc, (size_t)std::max(h.p.nsrc + 2 * h.p.ndrn, 1));
   up(d.src_cell, h.src_cell);
   up(d.struc, h.struc);
+  up(d.drn, h.drn);
+  up(d.drn_status, std::vector<int>(h.drn.size(), 1));          // open
+  up(d.drn_frac, std::vector<float>(h.drn.size(), 1.0f));      // fully open
   up(cmp, h.cmp_off);
   zero(d.st, 1);
 }
@@ -1151,7 +1200,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
     const HostModel& h = models_[i]->host();
     if (h.p.subgrid != subgrid_) throw std::runtime_error("an ensemble must be all-subgrid or all-regular");
     if (h.p.quadtree != qt_) throw std::runtime_error("an ensemble must be all-quadtree or all-regular-grid");
-    if (h.p.nsrc > 0) any_src_ = 1;
+    if (h.p.nsrc > 0 || h.p.ndrn > 0) any_src_ = 1;
     if (h.p.nstruc > 0) any_struc_ = 1;
     bnd_blocks_ = std::max(bnd_blocks_, (h.p.nkcuv2 + h.p.nneu + 127) / 128);
     scns.push_back(models_[i]->dev());

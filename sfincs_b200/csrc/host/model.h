@@ -52,6 +52,7 @@ struct HostModel {
   std::vector<float> tsrc, qsrc;     // qsrc [ntsrc][nsrc]
   std::vector<int32_t> src_cell;
   std::vector<StrucFace> struc;       // weir faces
+  std::vector<DrnDev> drn;            // drainage structures
   long long n_kcs1 = 0;
   double area_total_kcs1 = 0;
   std::vector<int2> tiles;  // (n0, m0) of every 32 x 8 tile holding an active cell
@@ -76,7 +77,7 @@ struct Keys {
   float hmin_cfl = 0, dtmax = 0, uvmax = 0, nuviscdim = 0, manning = 0, manning_land = 0, manning_sea = 0,
         rghlevland = 0, qinf = 0, qinf_zmin = 0;
   bool viscosity = false, advection_mask = true, quadtree = false;
-  std::string thdfile, weirfile;  // thin dams and weirs (regular grids)
+  std::string thdfile, weirfile, drnfile;  // thin dams, weirs and drainage structures (regular grids)
   std::string qtrfile, depfile, mskfile, indexfile, sbgfile, manningfile, bndfile, bzsfile, srcfile, disfile,
       wndfile, qinffile, prcpfile;
 };

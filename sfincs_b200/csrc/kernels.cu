@@ -208,6 +208,86 @@ __device__ __forceinline__ void commit_step(const ScnDev& S, StepState& st, cons
   if (st.steps_left > 0) st.steps_left -= 1;
 }
 
+// Drainage structures (sfincs_discharges.f90:370-657), in order, after the
+// boundary conditions of the step: each sets the discharge of its intake
+// (qtsrc = -q) and outfall (+q), which the point-source kernel applies before
+// continuity.  Levels are the FP32 state widened to FP64, as the reference
+// evaluates them from its real*8 zs.
+__device__ __forceinline__ void update_drainage(const ScnDev& S, const StepPlan& P) {
+  const float dt = P.dt;
+  const double t = P.t;
+  for (int idrn = 0; idrn < S.ndrn; idrn++) {
+    const DrnDev d = S.drn[idrn];
+    const int jin = S.nsrc + 2 * idrn, jout = jin + 1;
+    const double zin = (double)S.zs[d.cin], zout = (double)S.zs[d.cout];
+    float qq = 0.0f;
+    if (d.type == 1) {  // pump
+      qq = d.p[0];
+    } else if (d.type == 2 || d.type == 3) {  // culvert; check valve (intake to outfall only)
+      if (zin > zout)
+        qq = (float)((double)d.p[0] * sqrt(zin - zout));
+      else
+        qq = (float)((double)(-d.p[0]) * sqrt(zout - zin));
+      if (d.type == 3) qq = fmaxf(qq, 0.0f);
+    } else {  // gates: 4 opened while the intake level is in (zmin, zmax), 5 closed in [tclose, topen)
+      const float wdt = d.p[0], zsill = d.p[1], mng = d.p[2], tcls = d.p[5];
+      const float dzds = (float)((zout - zin) / (double)d.distance);
+      float frac = S.drn_frac[idrn];
+      const float hgate = (float)fmax(fmax(zin, zout) - (double)zsill, 0.0);
+      const float dfrac = dt / tcls;
+      const float qq0 = -S.qtsrc[jin] / (wdt * fmaxf(frac, 0.001f));
+      int status = S.drn_status[idrn];
+      if (d.type == 4) {
+        if (status == 0) {
+          if (zin > (double)d.p[3] && zin < (double)d.p[4]) status = 3;
+        } else if (status == 1) {
+          if (zin <= (double)d.p[3] || zin >= (double)d.p[4]) status = 2;
+        }
+      } else {
+        if (status == 0) {
+          if (t >= (double)d.p[4]) status = 3;
+        } else if (status == 1) {
+          if (t >= (double)d.p[3] && t < (double)d.p[4]) status = 2;
+        }
+      }
+      if (status == 2) {
+        frac = frac - dfrac;
+        if (frac < 0.0f) {
+          frac = 0.0f;
+          status = 0;
+        }
+      } else if (status == 3) {
+        frac = frac + dfrac;
+        if (frac > 1.0f) {
+          frac = 1.0f;
+          status = 1;
+        }
+      }
+      S.drn_frac[idrn] = frac;
+      S.drn_status[idrn] = status;
+      // Bates et al. (2010) inertial flux; hgate**(7.0/3.0) as hgate**2 * cbrt(hgate)
+      const float h73 = hgate * hgate * cbrtf(hgate);
+      qq = (qq0 - S.g * hgate * dzds * dt) / (1.0f + S.g * (mng * mng) * dt * fabsf(qq0) / h73);
+      qq = qq * wdt * frac;
+    }
+    qq = 1.0f / (S.structure_relax / dt) * qq + (1.0f - (1.0f / (S.structure_relax / dt))) * -S.qtsrc[jin];
+    // no more than the volume the giving cell holds
+    if (S.subgrid) {
+      if (qq > 0.0f)
+        qq = (float)fmin((double)qq, fmax(S.zvol[d.cin], 0.0) / (double)dt);
+      else
+        qq = (float)fmax((double)qq, -fmax(S.zvol[d.cout], 0.0) / (double)dt);
+    } else {
+      if (qq > 0.0f)
+        qq = (float)fmin((double)qq, fmax((zin - (double)S.zb[d.cin]) * (double)S.area, 0.0) / (double)dt);
+      else
+        qq = (float)fmax((double)qq, -fmax((zout - (double)S.zb[d.cout]) * (double)S.area, 0.0) / (double)dt);
+    }
+    S.qtsrc[jin] = -qq;
+    S.qtsrc[jout] = qq;
+  }
+}
+
 // --------------------------------------------------------------------------
 // Boundary faces and Neumann cells.
 // --------------------------------------------------------------------------
@@ -412,7 +492,8 @@ __device__ __forceinline__ void add_inflow(StepState& st, double inflow) {
 // - the last thread, which has the fewest boundary items, then reads the
 //   forcing time series while the others finish theirs;
 // - thread 0 commits the plan after the barrier of the inflow sum, when no
-//   thread reads the step state any more.
+//   thread reads the step state any more, and then updates the drainage
+//   structures, which read the boundary cells' new levels.
 template <bool ONE>
 __global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ scns, const __grid_constant__ ScnDev one) {
   const ScnDev& S = ONE ? one : scns[blockIdx.x];
@@ -436,8 +517,11 @@ __global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ sc
     }
     if (threadIdx.x == blockDim.x - 1) step_forcing(S, st, P);
   }
-  add_inflow(st, inflow);
-  if (threadIdx.x == 0) commit_step(S, st, P);
+  add_inflow(st, inflow);  // also orders the boundary cells' levels before the drainage reads them
+  if (threadIdx.x == 0) {
+    commit_step(S, st, P);
+    if (P.go && S.ndrn > 0) update_drainage(S, P);
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -592,10 +676,10 @@ __global__ void k_sources(const ScnDev* __restrict__ scns) {
   pdl_trigger();
   const ScnDev& S = scns[blockIdx.x];
   StepState& st = *S.st;
-  if (!st.run || S.nsrc == 0 || threadIdx.x != 0) return;
+  if (!st.run || S.nsrc + S.ndrn == 0 || threadIdx.x != 0) return;
   const float dt = st.dt;
   double vol = 0.0;
-  for (int is = 0; is < S.nsrc; is++) {
+  for (int is = 0; is < S.nsrc + 2 * S.ndrn; is++) {
     const int c = S.src_cell[is];
     if (S.subgrid) {
       if (S.zvol[c] >= 0.0) {

@@ -58,6 +58,18 @@ struct alignas(16) StrucFace {
   int pad;
 };
 
+// One drainage structure (sfincs_discharges.f90:180-320): type 1 pump, 2
+// culvert, 3 check valve, 4 gate controlled by the intake level, 5 gate
+// controlled by time; the dense offsets of its intake and outfall cells.
+struct alignas(16) DrnDev {
+  int type;
+  int cin, cout;    // intake (sink) and outfall (source) cells
+  int pad;
+  float p[6];       // pump: q; culvert / valve: coefficient; gates: width, sill, n, zmin|tclose, zmax|topen, closing time
+  float distance;   // between the two cell centres
+  float pad2;
+};
+
 // One water-level boundary face (kcuv == 2), packed so one thread reads it in
 // three 16-byte loads.  The boundary cell's level is recomputed per face from
 // the two nearest boundary points (sfincs_boundaries.f90:806-876).
@@ -206,6 +218,11 @@ struct ScnDev {
   const int* src_cell;   // [nsrc]
   int nstruc;            // weir faces
   const StrucFace* struc;  // [nstruc]
+  int ndrn;              // drainage structures; qtsrc and src_cell hold nsrc + 2 ndrn entries (intake, outfall per structure)
+  const DrnDev* drn;     // [ndrn]
+  int* drn_status;       // [ndrn] gates: 0 closed, 1 open, 2 closing, 3 opening
+  float* drn_frac;       // [ndrn] gates: fraction open
+  float structure_relax; // seconds
   float pi;
   StepState* st;
   // ---- quadtree (quadtree != 0; the regular-grid fields above that index

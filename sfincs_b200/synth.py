@@ -301,6 +301,7 @@ class RegularModel:
     dis: Optional[np.ndarray] = None     # (nt, 1+nsrc)
     thd: Optional[List[np.ndarray]] = None  # thin dams: polylines, each (npoints, 2) x, y
     weir: Optional[List[np.ndarray]] = None  # weirs: polylines, each (npoints, 4) x, y, crest level, Cd
+    drn: Optional[List[Sequence[float]]] = None  # drainage: x_in, y_in, x_out, y_out, type, params...
 
     @property
     def nmax(self):
@@ -368,6 +369,11 @@ class RegularModel:
                     for x, y, z, cd in pl:
                         f.write(f"{x:.4f} {y:.4f} {z:.4f} {cd:.4f}\n")
             inp["weirfile"] = "sfincs.weir"
+        if self.drn:
+            with open(os.path.join(d, "sfincs.drn"), "w") as f:
+                for r in self.drn:
+                    f.write(" ".join(str(int(v)) if k == 4 else f"{v:.4f}" for k, v in enumerate(r)) + "\n")
+            inp["drnfile"] = "sfincs.drn"
         inp.update(self.params)
         with open(os.path.join(d, "sfincs.inp"), "w") as f:
             for k, v in inp.items():

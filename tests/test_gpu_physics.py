@@ -4,8 +4,8 @@ The main parity tests (test_gpu_parity.py) run the default switches. Here each
 case turns on terms that those leave off: Coriolis, wind stress from a time
 series, theta smoothing, the "original" advection scheme, the slope limiter,
 friction2d off, viscosity and no wiggle suppression on a subgrid model, c2d
-infiltration, point sources, Neumann and outflow boundary cells, thin dams and
-weirs (regular and subgrid). For each
+infiltration, point sources, Neumann and outflow boundary cells, thin dams,
+weirs and the five drainage structure types (regular and subgrid). For each
 case the CUDA core is compared with the oracle in the core's own precision
 after 1, 2, 4, 10, 40 and 100 steps, on the default kernel path and on the
 per-thread-load path. The bars are those of the main stepwise test: time
@@ -111,10 +111,30 @@ def case_subgrid_weirs(tmp_path):
     return m
 
 
+_DRAINAGE = [(1000.0, 1000.0, 3000.0, 3000.0, 1, 2.0),                  # pump
+             (2200.0, 5000.0, 4200.0, 7000.0, 2, 1.5),                  # culvert
+             (1400.0, 8200.0, 600.0, 4600.0, 3, 1.0),                   # check valve
+             (3400.0, 1800.0, 1800.0, 3400.0, 4, 3.0, -6.0, 0.02, -3.0, 4.0, 120.0),   # level-controlled gate
+             (2600.0, 2600.0, 600.0, 600.0, 5, 2.0, -8.0, 0.025, 900.0, 2400.0, 60.0)]  # time-controlled gate
+
+
+def case_drainage(tmp_path):
+    m = _plain(tmp_path)
+    m.drn = _DRAINAGE
+    return m
+
+
+def case_subgrid_drainage(tmp_path):
+    m = _subgrid(tmp_path, advection=1)
+    m.drn = _DRAINAGE
+    return m
+
+
 CASES = {f.__name__[5:]: f for f in (case_coriolis_wind_theta, case_original_advection_slopelim_nofric2d,
                                       case_boundary_kinds, case_plain_infiltration, case_subgrid_visc_nowiggle,
                                       case_subgrid_infiltration_sources, case_thin_dams_theta,
-                                      case_subgrid_thin_dams, case_weirs, case_subgrid_weirs)}
+                                      case_subgrid_thin_dams, case_weirs, case_subgrid_weirs, case_drainage,
+                                      case_subgrid_drainage)}
 
 
 def _model(d, variant):

@@ -117,9 +117,9 @@ def test_subgrid_tables_and_volumes(tmp_path):
 
 def test_unsupported_inputs_are_refused(tmp_path):
     m = synth.plain_regular(nmax=6, mmax=7, dx=300.0, tstop=600.0, nbumps=1)
-    m.params["drnfile"] = "sfincs.drn"
+    m.params["spwfile"] = "sfincs.spw"
     d = m.write(str(tmp_path))
-    with pytest.raises(RuntimeError, match="drnfile"):
+    with pytest.raises(RuntimeError, match="spwfile"):
         B.layout(d, "counts", 10)
 
 

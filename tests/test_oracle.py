@@ -199,3 +199,30 @@ def test_weir_free_and_submerged_flow(tmp_path):
             want = cd * 1.7049 * h1 ** 1.5
         assert q[ip] == pytest.approx(want * rel, rel=1e-6)
         assert rel == pytest.approx(1.0, abs=1e-6)
+
+
+def test_drainage_structures_move_water_and_conserve_volume(tmp_path):
+    """Drainage structures (sfincs_discharges.f90:370-657) in a closed basin: a
+    pump, a culvert, a check valve and two gates move water between cells;
+    the FP64 volume is unchanged, and the pump's intake loses water while its
+    outfall gains it."""
+    m = _closed(synth.plain_regular(nmax=10, mmax=14, dx=100.0, tstop=3600.0, nbumps=0))
+    m.zb = np.full_like(m.zb, -2.0)
+    m.drn = [(250.0, 250.0, 1150.0, 850.0, 1, 0.5),        # pump 0.5 m3/s
+             (550.0, 150.0, 550.0, 950.0, 2, 0.3),         # culvert
+             (950.0, 150.0, 150.0, 950.0, 3, 0.4),         # check valve
+             (1250.0, 350.0, 1250.0, 750.0, 4, 2.0, -1.0, 0.02, -0.5, 5.0, 60.0),   # level-controlled gate
+             (750.0, 550.0, 350.0, 550.0, 5, 1.5, -1.5, 0.025, 300.0, 900.0, 30.0)]  # time-controlled gate
+    d = m.write(str(tmp_path))
+    o = _oracle(d)
+    n = o.get("nm_n").astype(int)
+    mm = o.get("nm_m").astype(int)
+    zs = 0.1 * np.sin(n / 2.0) + 0.05 * np.cos(mm / 3.0)
+    o.set("zs", zs)
+    v0 = np.sum(o.get("zs") + 2.0)
+    o.update(-1000.0, 300)
+    z = o.get("zs")
+    assert abs(np.sum(z + 2.0) - v0) <= 1e-9 * v0
+    cell = lambda x, y: int(np.flatnonzero((n == int(y // 100) + 1) & (mm == int(x // 100) + 1))[0])
+    assert z[cell(250.0, 250.0)] < zs[cell(250.0, 250.0)]
+    assert z[cell(1150.0, 850.0)] > zs[cell(1150.0, 850.0)]
