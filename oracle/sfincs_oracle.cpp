@@ -1183,10 +1183,40 @@ struct Model {
     if (store_maximum_flux) qmax.alloc(np);
     if (store_twet) twet.alloc(np);
     if (store_t_zsmax) t_zsmax.alloc(np);
-    if (rstfile.substr(0, 4) != "none" || zsinifile.substr(0, 4) != "none")
-      throw std::runtime_error("oracle: restart/ini files are not part of this path");
+    if (zsinifile.substr(0, 4) != "none") throw std::runtime_error("oracle: ini files are not part of this path");
+    // set_initial_conditions / read_binary_restart_file: sfincs_initial_conditions.F90:14-268
+    std::vector<float> inizs4, iniq;
+    if (rstfile.substr(0, 4) != "none") {
+      std::ifstream fin(path(rstfile), std::ios::binary);
+      if (!fin) throw std::runtime_error("oracle: cannot open " + rstfile);
+      auto rd = [&](void* p, size_t n) {
+        fin.read((char*)p, (std::streamsize)n);
+        if (!fin) throw std::runtime_error("oracle: restart file too short");
+      };
+      float rdummy;
+      int32_t rsttype = 0;
+      rd(&rdummy, 4);
+      rd(&rsttype, 4);
+      rd(&rdummy, 4);
+      if (rsttype >= 1 && rsttype <= 6) {
+        if (rsttype >= 4) throw std::runtime_error("oracle: restart flavours 4-6 are not restated");
+        inizs4.resize((size_t)np);
+        rd(&rdummy, 4);
+        rd(inizs4.data(), 4 * (size_t)np);
+        rd(&rdummy, 4);
+        if (rsttype == 1 || rsttype == 2) {
+          iniq.resize((size_t)(npuv + ncuv + 1));
+          rd(&rdummy, 4);
+          rd(iniq.data(), 4 * iniq.size());
+          rd(&rdummy, 4);
+          rd(&rdummy, 4);
+          for (long ib = 1; ib <= nkcuv2; ib++) rd(&uvmean(ib), 4);
+          rd(&rdummy, 4);
+        }
+      }
+    }
     for (long nm = 1; nm <= np; nm++) {
-      double inizs = (double)zini;
+      double inizs = inizs4.empty() ? (double)zini : (double)inizs4[(size_t)nm - 1];
       if (subgrid)
         zs(nm) = (TZ)std::max((double)sg_z_zmin(nm), inizs);
       else
@@ -1203,6 +1233,30 @@ struct Model {
     if (store_twet) twet.fill((T)0.0f);
     if (store_t_zsmax) t_zsmax.fill(-999.0f);
     uv.fill((T)0);
+    if (!iniq.empty()) {  // fluxes from the restart file and the velocities they imply
+      for (long ip = 1; ip <= npuv; ip++) {
+        q(ip) = (T)iniq[(size_t)ip - 1];
+        long nm = uv_index_z_nm(ip), nmu = uv_index_z_nmu(ip);
+        float zsuv = (float)std::max(zs(nm), zs(nmu));
+        bool iok = subgrid ? zsuv > sg_uv_zmin(ip) + huthresh : zsuv > zbuvmx(ip);
+        if (!iok) continue;
+        float huv;
+        if (subgrid) {
+          if (zsuv > sg_uv_zmax(ip) - 1.0e-4f) {
+            huv = sg_uv_havg_zmax(ip) + zsuv;
+          } else {
+            float dzuv = (sg_uv_zmax(ip) - sg_uv_zmin(ip)) / (float)(subgrid_nlevels - 1);
+            long iuv = (long)((zsuv - sg_uv_zmin(ip)) / dzuv) + 1;
+            float facint = (zsuv - (sg_uv_zmin(ip) + (float)(iuv - 1) * dzuv)) / dzuv;
+            huv = sg_uv_havg(iuv, ip) + (sg_uv_havg(iuv + 1, ip) - sg_uv_havg(iuv, ip)) * facint;
+          }
+          huv = std::max(huv, huthresh);
+        } else {
+          huv = std::max(zsuv - zbuv(ip), huthresh);
+        }
+        uv(ip) = (T)std::max(std::min((float)q(ip) / huv, 4.0f), -4.0f);
+      }
+    }
     if (wind) {
       tauwu.alloc(np);
       tauwv.alloc(np);

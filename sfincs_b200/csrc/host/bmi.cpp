@@ -815,6 +815,18 @@ int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst
         out[i] = u[h.cmp_off[i]];
         out[h.np + i] = v[h.cmp_off[i]];
       }
+    } else if (nm == "uvmean0") {  // initial boundary mean fluxes, boundary-face order
+      out.assign(h.uvmean0.begin(), h.uvmean0.end());
+      out.resize(h.bfaces.size(), 0.0);
+    } else if (nm == "uv0" || nm == "q0") {  // initial u then v face values per cell (restart)
+      const auto& u = nm == "uv0" ? h.uv0u : h.q0u;
+      const auto& v = nm == "uv0" ? h.uv0v : h.q0v;
+      out.assign((size_t)h.np * 2, 0.0);
+      if (!u.empty())
+        for (long long i = 0; i < h.np; i++) {
+          out[i] = u[h.cmp_off[i]];
+          out[h.np + i] = v[h.cmp_off[i]];
+        }
     } else if (nm == "nstruc") {
       out = {(double)h.struc.size()};
     } else if (nm == "struc") {

@@ -182,7 +182,9 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   for (const char* k : {"snapwave", "nonh", "bathtub", "vegetation"})
     if (in.logical(k, false) || in.integer(k, 0) != 0)
       throw std::runtime_error(std::string("process '") + k + "' is not supported by this core");
-  if (!is_none(inifile) || !is_none(rstfile)) throw std::runtime_error("inifile/rstfile are not supported by this core yet");
+  if (!is_none(inifile)) throw std::runtime_error("inifile is not supported by this core yet");
+  if (!is_none(rstfile) && !is_none(in.str("qtrfile", "none")))
+    throw std::runtime_error("rstfile is not supported on quadtree grids by this core");
   if (igeo != 0) throw std::runtime_error("geographic grids (crsgeo=1) are not supported by this core");
   if (inputtype != "bin") throw std::runtime_error("only inputformat = bin is supported");
   if (bndtype != 1) throw std::runtime_error("only bndtype = 1 is supported");
@@ -237,7 +239,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   k.qinf_zmin = qinf_zmin; k.advection_mask = advection_mask; k.qtrfile = qtrfile; k.depfile = depfile;
   k.mskfile = mskfile; k.indexfile = indexfile; k.sbgfile = sbgfile; k.manningfile = manningfile;
   k.bndfile = bndfile; k.bzsfile = bzsfile; k.srcfile = srcfile; k.disfile = disfile; k.wndfile = wndfile;
-  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile; k.weirfile = weirfile; k.drnfile = drnfile;
+  k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile; k.weirfile = weirfile; k.drnfile = drnfile; k.rstfile = rstfile;
   return k;
 }
 
@@ -309,6 +311,51 @@ static int side_of(float ax, float ay, float bx, float by, float cx, float cy) {
 static bool segments_cross(float p1x, float p1y, float p2x, float p2y, float q1x, float q1y, float q2x, float q2y) {
   return side_of(p1x, p1y, p2x, p2y, q1x, q1y) != side_of(p1x, p1y, p2x, p2y, q2x, q2y) &&
          side_of(q1x, q1y, q2x, q2y, p1x, p1y) != side_of(q1x, q1y, q2x, q2y, p2x, p2y);
+}
+
+// ---- binary restart files (sfincs_initial_conditions.F90:183-268) -------------------
+// Fortran unformatted sequential records, each framed by its byte length:
+// the flavour (int32), zs (float32[np]), and for flavours 1, 2, 4-6 the fluxes
+// q (float32[npuv + ncuv + 1], reference face order) and the boundary mean
+// fluxes uvmean (float32[nkcuv2]).
+struct RestartData {
+  int type = 0;
+  std::vector<float> zs, q, uvmean;
+};
+static RestartData read_restart(const std::string& file) {
+  FILE* fp = std::fopen(file.c_str(), "rb");
+  if (!fp) throw std::runtime_error("cannot open restart file " + file);
+  std::vector<std::vector<char>> rec;
+  for (;;) {
+    int32_t len = 0, tail = 0;
+    if (std::fread(&len, 4, 1, fp) != 1) break;
+    if (len < 0) throw std::runtime_error("restart file " + file + ": bad record");
+    std::vector<char> r((size_t)len);
+    if ((len > 0 && std::fread(r.data(), 1, (size_t)len, fp) != (size_t)len) || std::fread(&tail, 4, 1, fp) != 1 ||
+        tail != len) {
+      std::fclose(fp);
+      throw std::runtime_error("restart file " + file + ": truncated record");
+    }
+    rec.push_back(std::move(r));
+  }
+  std::fclose(fp);
+  RestartData d;
+  if (rec.empty() || rec[0].size() != 4) throw std::runtime_error("restart file " + file + ": no flavour record");
+  std::memcpy(&d.type, rec[0].data(), 4);
+  auto floats = [&](size_t i) {
+    if (i >= rec.size() || rec[i].size() % 4) throw std::runtime_error("restart file " + file + ": missing record");
+    std::vector<float> v(rec[i].size() / 4);
+    std::memcpy(v.data(), rec[i].data(), rec[i].size());
+    return v;
+  };
+  if (d.type < 1 || d.type > 6) return d;  // the reference skips an unknown flavour with a warning
+  if (d.type >= 4) throw std::runtime_error("restart flavours 4-6 (cnb/gai/hor infiltration) are not supported by this core");
+  d.zs = floats(1);
+  if (d.type == 1 || d.type == 2) {
+    d.q = floats(2);
+    d.uvmean = floats(3);
+  }
+  return d;
 }
 
 std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
@@ -423,6 +470,15 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   // built from the faces as they were before (the reference applies the dams
   // after initialize_domain); activity and the theta-smoothing neighbour rule
   // see the dams (the reference tests kcuv there at run time).
+  RestartData rst;
+  if (!is_none(K.rstfile)) {
+    rst = read_restart(path(K.rstfile));
+    if (rst.type >= 1 && rst.type <= 6) {
+      if ((long long)rst.zs.size() != h.np) throw std::runtime_error("restart file: zs has the wrong length");
+      if (!rst.q.empty() && (long long)rst.q.size() != h.npuv + 1)
+        throw std::runtime_error("restart file: q has the wrong length");
+    }
+  }
   auto xz = [&](int n, int m) {
     return x0 + cosrot * (1.0f * ((float)m - 0.5f)) * dx - sinrot * (1.0f * ((float)n - 0.5f)) * dy;
   };
@@ -652,8 +708,15 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   }
   for (size_t ib = 0; ib < ngb; ib++)
     if (kcs[gb_cell[ib]] == 6 && gb_nmi[ib] >= 0) h.neu.push_back(make_int2(gb_cell[ib], gb_nmi[ib]));
-  for (auto& e : kb_all) {
+  if (!rst.uvmean.empty() && rst.uvmean.size() != kb_all.size())
+    throw std::runtime_error("restart file: uvmean has the wrong length");
+  for (size_t ib_ref = 0; ib_ref < kb_all.size(); ib_ref++) {
+    const auto& e = kb_all[ib_ref];
     if (kcs[e.nmb] == 6) continue;  // lateral Neumann faces are updated by the momentum kernel
+    if (!rst.uvmean.empty()) {
+      h.uvmean0.resize(h.bfaces.size() + 1, 0.0f);
+      h.uvmean0.back() = rst.uvmean[ib_ref];
+    }
     const int ib = gb_index[e.nmb];
     BndFace b{};
     b.face = (int)e.face;
@@ -852,9 +915,48 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   for (long long i = 0; i < h.np; i++) {
     const int64_t c = h.cmp_off[i];
     const float base = P.subgrid ? h.zz_min[c] : h.zb[c];
-    h.zs[c] = (float)std::max((double)base, (double)P.zini);
+    const double ini = rst.zs.empty() ? (double)P.zini : (double)rst.zs[i];  // inizs (real*8) from real*4
+    h.zs[c] = (float)std::max((double)base, ini);
   }
   h.zsmax.assign(NA, -999.0f);
+  // initial fluxes from a restart file, and the velocities they imply
+  // (sfincs_initial_conditions.F90:110-173), in both ping-pong buffers
+  if (!rst.q.empty()) {
+    h.q0u.assign(NA, 0.0f);
+    h.q0v.assign(NA, 0.0f);
+    h.uv0u.assign(NA, 0.0f);
+    h.uv0v.assign(NA, 0.0f);
+    h.kf0u.assign(NA, 0);
+    h.kf0v.assign(NA, 0);
+    for (size_t f = 0; f < face_off.size(); f++) {
+      const int64_t c = face_off[f];
+      const int dir = face_dir[f];
+      const int64_t cu = dir == 0 ? c + ld : c + 1;
+      const float q = rst.q[f];
+      (dir == 0 ? h.q0u : h.q0v)[c] = q;
+      if (q != 0.0f) (dir == 0 ? h.kf0u : h.kf0v)[c] = KF_STALE | KF_WET2;
+      const float zsuv = std::max(h.zs[c], h.zs[cu]);
+      float huv = 0.0f;
+      if (P.subgrid) {
+        const float2 zr = (dir == 0 ? h.sgz_u : h.sgz_v)[c];
+        if (!(zsuv > zr.x + P.huthresh)) continue;
+        if (zsuv > zr.y - 1.0e-4f) {
+          huv = (dir == 0 ? h.sgw_u : h.sgw_v)[c].x + zsuv;
+        } else {
+          const float dzuv = (zr.y - zr.x) / (float)(P.nlev - 1);
+          const int iuv = (int)((zsuv - zr.x) / dzuv) + 1;
+          const float facint = (zsuv - (zr.x + (float)(iuv - 1) * dzuv)) / dzuv;
+          const UvRec& r = (dir == 0 ? h.rec_u : h.rec_v)[(size_t)(iuv - 1) * NA + (size_t)c];
+          huv = r.havg + r.dhavg * facint;
+        }
+        huv = std::max(huv, P.huthresh);
+      } else {
+        if (!(zsuv > (dir == 0 ? h.zbmx_u : h.zbmx_v)[c])) continue;
+        huv = std::max(zsuv - 0.5f * (h.zb[c] + h.zb[cu]), P.huthresh);
+      }
+      (dir == 0 ? h.uv0u : h.uv0v)[c] = std::max(std::min(q / huv, 4.0f), -4.0f);
+    }
+  }
   if (P.wiggle) h.zs0 = h.zs;
   if (P.subgrid) {
     const int L = P.nlev;
@@ -1076,15 +1178,27 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     d.zs0 = nullptr;
     d.zsderv = nullptr;
   }
-  zero(d.kf[0], NA);
-  zero(d.kf[1], NA);
+  if (h.kf0u.empty()) {
+    zero(d.kf[0], NA);
+    zero(d.kf[1], NA);
+  } else {  // restart fluxes in both buffers: the first dry steps must clear them
+    up(d.kf[0], h.kf0u);
+    up(d.kf[1], h.kf0v);
+  }
   if (h.p.subgrid) up(d.vneg, h.vneg);
   else d.vneg = nullptr;
   for (int b = 0; b < 2; b++) {
-    zero(d.qu[b], NA);
-    zero(d.qv[b], NA);
-    zero(d.uu[b], NA);
-    zero(d.vv[b], NA);
+    if (h.q0u.empty()) {
+      zero(d.qu[b], NA);
+      zero(d.qv[b], NA);
+      zero(d.uu[b], NA);
+      zero(d.vv[b], NA);
+    } else {  // a restart file's fluxes
+      up(d.qu[b], h.q0u);
+      up(d.qv[b], h.q0v);
+      up(d.uu[b], h.uv0u);
+      up(d.vv[b], h.uv0v);
+    }
   }
   up(d.flags, h.flags);
   up(d.zb, h.zb);
@@ -1123,7 +1237,10 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.zs_bnd, h.zs_bnd);
   zero(d.zst_bnd, (size_t)std::max(h.p.nbnd, 1));
   up(d.bfaces, h.bfaces);
-  zero(d.uvmean, (size_t)std::max(h.p.nkcuv2, 1));
+  if (h.uvmean0.empty())
+    zero(d.uvmean, (size_t)std::max(h.p.nkcuv2, 1));
+  else
+    up(d.uvmean, h.uvmean0);
   up(d.neu, h.neu);
   up(d.tprcp, h.tprcp);
   up(d.vprcp, h.vprcp);

@@ -53,6 +53,8 @@ struct HostModel {
   std::vector<int32_t> src_cell;
   std::vector<StrucFace> struc;       // weir faces
   std::vector<DrnDev> drn;            // drainage structures
+  std::vector<float> q0u, q0v, uv0u, uv0v, uvmean0;  // initial fluxes from a restart file (else zero)
+  std::vector<uint8_t> kf0u, kf0v;                   // initial wet history with a restart file
   long long n_kcs1 = 0;
   double area_total_kcs1 = 0;
   std::vector<int2> tiles;  // (n0, m0) of every 32 x 8 tile holding an active cell
@@ -77,7 +79,7 @@ struct Keys {
   float hmin_cfl = 0, dtmax = 0, uvmax = 0, nuviscdim = 0, manning = 0, manning_land = 0, manning_sea = 0,
         rghlevland = 0, qinf = 0, qinf_zmin = 0;
   bool viscosity = false, advection_mask = true, quadtree = false;
-  std::string thdfile, weirfile, drnfile;  // thin dams, weirs and drainage structures (regular grids)
+  std::string thdfile, weirfile, drnfile, rstfile;  // thin dams, weirs, drainage structures, restart (regular grids)
   std::string qtrfile, depfile, mskfile, indexfile, sbgfile, manningfile, bndfile, bzsfile, srcfile, disfile,
       wndfile, qinffile, prcpfile;
 };

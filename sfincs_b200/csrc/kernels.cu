@@ -563,7 +563,7 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepVals& 
       Qn[c] = 0.0f;
       Un[c] = 0.0f;
     }
-    const uint8_t kfn = (uint8_t)((kf & KF_WET) ? KF_WET2 : 0);
+    const uint8_t kfn = (uint8_t)((kf & (KF_WET | KF_STALE)) ? KF_WET2 : 0);
     if (kfn != kf) kfp[c] = kfn;
     return FLT_MAX;
   }
@@ -633,7 +633,7 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepVals& 
   const float den = fmaxf(sqrtf(ghu), fabsf(uv)) * geo.dxuvinv;
   Qn[c] = q;
   Un[c] = uv;
-  const uint8_t kfn = (uint8_t)(KF_WET | ((kf & KF_WET) ? KF_WET2 : 0));
+  const uint8_t kfn = (uint8_t)(KF_WET | ((kf & (KF_WET | KF_STALE)) ? KF_WET2 : 0));
   if (kfn != kf) kfp[c] = kfn;
   return 1.0f / den;  // sfincs_momentum.f90:731
 }

@@ -393,8 +393,8 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
             S.qu[p ^ 1][c] = 0.0f;
             S.uu[p ^ 1][c] = 0.0f;
           }
-          const uint8_t kn = wet_u ? (uint8_t)(KF_WET | ((kfu & KF_WET) ? KF_WET2 : 0))
-                                   : (uint8_t)((kfu & KF_WET) ? KF_WET2 : 0);
+          const uint8_t kn = wet_u ? (uint8_t)(KF_WET | ((kfu & (KF_WET | KF_STALE)) ? KF_WET2 : 0))
+                                   : (uint8_t)((kfu & (KF_WET | KF_STALE)) ? KF_WET2 : 0);
           if (kn != kfu) S.kf[0][c] = kn;
         }
         // ---- v face
@@ -450,8 +450,8 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
             S.qv[p ^ 1][c] = 0.0f;
             S.vv[p ^ 1][c] = 0.0f;
           }
-          const uint8_t kn = wet_v ? (uint8_t)(KF_WET | ((kfv & KF_WET) ? KF_WET2 : 0))
-                                   : (uint8_t)((kfv & KF_WET) ? KF_WET2 : 0);
+          const uint8_t kn = wet_v ? (uint8_t)(KF_WET | ((kfv & (KF_WET | KF_STALE)) ? KF_WET2 : 0))
+                                   : (uint8_t)((kfv & (KF_WET | KF_STALE)) ? KF_WET2 : 0);
           if (kn != kfv) S.kf[1][c] = kn;
         }
       }

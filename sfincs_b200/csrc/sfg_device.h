@@ -42,7 +42,12 @@ enum : uint16_t {
 // bit 0 = wet after the previous step (the reference's kfuv), bit 1 = wet the
 // step before.  A face dry for two consecutive steps holds q = uv = 0 in both
 // ping-pong buffers, so its (zero) writes are skipped.
-enum : uint8_t { KF_WET = 1u, KF_WET2 = 2u };
+// Wet history of a face: KF_WET wet at the previous step, KF_WET2 wet the step
+// before (so the ping-pong buffer being written may hold a nonzero flux);
+// KF_STALE: both buffers hold fluxes from a restart file.  For the buffer
+// bookkeeping KF_STALE counts as wet at the previous step, for friction (the
+// newly-wet formula) it does not.
+enum : uint8_t { KF_WET = 1u, KF_WET2 = 2u, KF_STALE = 4u };
 
 // One weir face (kcuv = 3, sfincs_structures.f90:38-381): the uv face with
 // the dense offsets of its two cells, the crest level and discharge
