@@ -32,6 +32,36 @@ namespace {
 
 thread_local std::string g_err = "no error";
 
+// time_to_string (sfincs_date.f90:298-327): "yyyymmdd.HHMMSS" of tref + t
+// seconds, with the reference's real*4 arithmetic for the time of day.
+std::string restart_time_string(double t_sec, const std::string& tref) {
+  const int yyyy = std::atoi(tref.substr(0, 4).c_str()), mm = std::atoi(tref.substr(4, 2).c_str()),
+            dd = std::atoi(tref.substr(6, 2).c_str()), hh0 = std::atoi(tref.substr(9, 2).c_str()),
+            mn0 = std::atoi(tref.substr(11, 2).c_str()), ss0 = std::atoi(tref.substr(13, 2).c_str());
+  const float ref_fraction = (float)hh0 / 24.0f + (float)mn0 / 1440.0f + (float)ss0 / 86400.0f;
+  const float sec_add = (float)((double)(ref_fraction * 86400.0f) + t_sec);
+  const int ndays_add = (int)(sec_add / 86400.0f);
+  const float secs_time = sec_add - (float)ndays_add * 86400.0f;
+  // civil date of the reference day + ndays_add (proleptic Gregorian)
+  auto days_from_civil = [](long long y, long long m, long long d) {
+    y -= m <= 2;
+    const long long era = (y >= 0 ? y : y - 399) / 400, yoe = y - era * 400;
+    const long long doy = (153 * (m + (m > 2 ? -3 : 9)) + 2) / 5 + d - 1, doe = yoe * 365 + yoe / 4 - yoe / 100 + doy;
+    return era * 146097 + doe - 719468;
+  };
+  long long z = days_from_civil(yyyy, mm, dd) + ndays_add + 719468;
+  const long long era = (z >= 0 ? z : z - 146096) / 146097, doe = z - era * 146097;
+  const long long yoe = (doe - doe / 1460 + doe / 36524 - doe / 146096) / 365, doy = doe - (365 * yoe + yoe / 4 - yoe / 100);
+  const long long mp = (5 * doy + 2) / 153, d = doy - (153 * mp + 2) / 5 + 1, m = mp + (mp < 10 ? 3 : -9);
+  const long long y = yoe + era * 400 + (m <= 2);
+  const int hh = (int)(secs_time / 3600.0f);
+  const int mn = (int)((secs_time - (float)(hh * 3600)) / 60.0f);
+  const int ss = (int)(secs_time - (float)(hh * 3600) - (float)(mn * 60));
+  char buf[32];
+  std::snprintf(buf, sizeof buf, "%04lld%02lld%02lld.%02d%02d%02d", y, m, d, hh, mn, ss);
+  return buf;
+}
+
 // One model with its runner and data-interface staging buffers.
 struct ModelHandle {
   std::unique_ptr<HostModel> host;
@@ -114,7 +144,71 @@ struct ModelHandle {
   void after_update() {
     if (zs_exported) refresh_zs();
   }
-  void run(double tend, long long max_steps, int chunk) { runner->run({tend}, max_steps, chunk); }
+  // Runs to tend (or max_steps steps), stopping at every restart output time
+  // on the step that reaches it (t >= trstout after the step, as
+  // sfincs_lib.f90:447-463 checks), where it writes the restart file.
+  void run(double tend, long long max_steps, int chunk) {
+    if (host->trstout >= 1.0e9) {
+      runner->run({tend}, max_steps, chunk);
+      return;
+    }
+    long long left = max_steps;
+    for (;;) {
+      const StepState s0 = runner->read_state(0);
+      if (!(s0.t < tend) || left == 0) break;
+      if (host->trstout <= s0.t)
+        runner->run({tend}, 1, 1);  // the output falls on the next step
+      else
+        runner->run({std::min(tend, host->trstout)}, left, chunk);
+      const StepState s1 = runner->read_state(0);
+      if (left > 0) left = std::max(0LL, left - (long long)(s1.nt - s0.nt));
+      after_step_output();
+      if (s1.nt == s0.nt) break;  // stopped (instability or end of the run)
+    }
+  }
+  // sfincs_lib.f90:447-463 after a step
+  void after_step_output() {
+    if (host->trstout >= 1.0e9) return;
+    const StepState st = runner->read_state(0);
+    if (st.t >= host->trstout) {
+      write_restart(st.t);
+      host->trstout = host->dtrstout > 1.0e-6 ? host->trstout + host->dtrstout : 1.0e9;
+    }
+  }
+  // write_rst_file (sfincs_output.f90:657-733), flavour 1: zs, q, uvmean
+  void write_restart(double t) {
+    const HostModel& H = *host;
+    const ScnDev& D = dev->dev();
+    const StepState st = runner->read_state(0);
+    const int p = latest(st);
+    const size_t NA = (size_t)H.p.nalloc;
+    std::vector<float> zsd(NA), qu(NA), qv(NA), um((size_t)std::max(H.p.nkcuv2, 1));
+    check_cuda(cudaMemcpy(zsd.data(), D.zs, NA * 4, cudaMemcpyDeviceToHost), "restart zs");
+    check_cuda(cudaMemcpy(qu.data(), D.qu[p], NA * 4, cudaMemcpyDeviceToHost), "restart qu");
+    check_cuda(cudaMemcpy(qv.data(), D.qv[p], NA * 4, cudaMemcpyDeviceToHost), "restart qv");
+    if (H.p.nkcuv2 > 0)
+      check_cuda(cudaMemcpy(um.data(), D.uvmean, (size_t)H.p.nkcuv2 * 4, cudaMemcpyDeviceToHost), "restart uvmean");
+    std::vector<float> zs4((size_t)H.np), q((size_t)H.npuv + 1, 0.0f), uvm(H.kb_bface.size(), 0.0f);
+    for (long long i = 0; i < H.np; i++) zs4[(size_t)i] = zsd[(size_t)H.cmp_off[i]];
+    for (size_t f = 0; f < H.face_off.size(); f++) q[f] = (H.face_dir[f] == 0 ? qu : qv)[(size_t)H.face_off[f]];
+    for (size_t ib = 0; ib < H.kb_bface.size(); ib++)
+      if (H.kb_bface[ib] >= 0) uvm[ib] = um[(size_t)H.kb_bface[ib]];
+    const std::string name = H.dir + "/sfincs." + restart_time_string(1.0 * (double)(long long)t, H.tref) + ".rst";
+    FILE* fp = std::fopen(name.c_str(), "wb");
+    if (!fp) throw std::runtime_error("cannot write restart file " + name);
+    auto rec = [&](const void* data, size_t bytes) {
+      const int32_t n = (int32_t)bytes;
+      std::fwrite(&n, 4, 1, fp);
+      std::fwrite(data, 1, bytes, fp);
+      std::fwrite(&n, 4, 1, fp);
+    };
+    const int32_t type = 1;
+    rec(&type, 4);
+    rec(zs4.data(), zs4.size() * 4);
+    rec(q.data(), q.size() * 4);
+    rec(uvm.data(), uvm.size() * 4);
+    std::fclose(fp);
+  }
 
   void scalars(double* out) {
     StepState st = runner->read_state(0);
@@ -341,6 +435,7 @@ int update(void) {
     g_bmi->step_once();
     g_bmi->after_update();
     g_bmi->runner->sync();  // the step is complete when update() returns, as in the reference
+    g_bmi->after_step_output();
     return 0;
   });
 }

@@ -201,6 +201,15 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   if (is_none(tref)) tref = tstart;
   const float t0 = (float)(seconds_between(tref, tstart) * 1.0);
   const float t1 = (float)(seconds_between(tref, tstop) * 1.0);
+  {  // restart output times (sfincs_input.f90:61-66, 441-444; sfincs_output.f90:39-56)
+    float t0out = in.real("t0out", -999.0f);
+    const float dtrstout = in.real("dtrstout", 0.0f), trst = in.real("trstout", -999.0f);
+    if (t0out < -900.0f) t0out = t0;
+    t0out = std::max(t0out, t0);
+    h.tref = tref;
+    h.dtrstout = dtrstout;
+    h.trstout = dtrstout > 1.0e-6f ? (double)(t0out + dtrstout) : (trst > 1.0e-6f ? (double)trst : 1.0e9);
+  }
   tspinup = t0 + tspinup;
   P.g = 9.81f;
   P.pi = 3.14159f;
@@ -463,6 +472,8 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     }
   }
   h.npuv = (long long)face_off.size();
+  h.face_off = face_off;
+  h.face_dir = face_dir;
   // Thin dams: a face whose segment between the two cell centres crosses a
   // dam segment is no momentum face (kcuv = 0, sfincs_quadtree.F90:853-1010).
   // Cells are searched in the dam segment's cell-index box widened by one,
@@ -710,9 +721,11 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     if (kcs[gb_cell[ib]] == 6 && gb_nmi[ib] >= 0) h.neu.push_back(make_int2(gb_cell[ib], gb_nmi[ib]));
   if (!rst.uvmean.empty() && rst.uvmean.size() != kb_all.size())
     throw std::runtime_error("restart file: uvmean has the wrong length");
+  h.kb_bface.assign(kb_all.size(), -1);
   for (size_t ib_ref = 0; ib_ref < kb_all.size(); ib_ref++) {
     const auto& e = kb_all[ib_ref];
     if (kcs[e.nmb] == 6) continue;  // lateral Neumann faces are updated by the momentum kernel
+    h.kb_bface[ib_ref] = (int)h.bfaces.size();
     if (!rst.uvmean.empty()) {
       h.uvmean0.resize(h.bfaces.size() + 1, 0.0f);
       h.uvmean0.back() = rst.uvmean[ib_ref];

@@ -55,6 +55,13 @@ struct HostModel {
   std::vector<DrnDev> drn;            // drainage structures
   std::vector<float> q0u, q0v, uv0u, uv0v, uvmean0;  // initial fluxes from a restart file (else zero)
   std::vector<uint8_t> kf0u, kf0v;                   // initial wet history with a restart file
+  // restart output (sfincs_output.f90:8-58, 657-733): next time, interval, the
+  // reference face order and the reference boundary-face order (-1: lateral Neumann face)
+  std::string tref;
+  double trstout = 1.0e9, dtrstout = 0.0;
+  std::vector<int64_t> face_off;
+  std::vector<int8_t> face_dir;
+  std::vector<int> kb_bface;
   long long n_kcs1 = 0;
   double area_total_kcs1 = 0;
   std::vector<int2> tiles;  // (n0, m0) of every 32 x 8 tile holding an active cell

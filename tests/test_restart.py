@@ -100,3 +100,65 @@ def test_gpu_continues_from_restart_with_oracle(tmp_path, make):
         assert dzs <= 2e-5, f"zs differs by {dzs} after {done} steps"
         assert dq <= 2e-5, f"q differs by {dq} after {done} steps"
     g.close()
+
+
+def read_restart(path):
+    recs = []
+    with open(path, "rb") as f:
+        while True:
+            head = f.read(4)
+            if not head:
+                break
+            n = int(np.frombuffer(head, np.int32)[0])
+            recs.append(f.read(n))
+            assert int(np.frombuffer(f.read(4), np.int32)[0]) == n
+    return (int(np.frombuffer(recs[0], np.int32)[0]),) + tuple(np.frombuffer(r, np.float32) for r in recs[1:])
+
+
+@pytest.mark.gpu
+def test_gpu_writes_restart_files_at_output_times(tmp_path):
+    """dtrstout (sfincs_output.f90:657-733, sfincs_lib.f90:447-463): the step
+    that reaches each output time writes sfincs.<yyyymmdd.HHMMSS of int(t)>.rst
+    with that step's zs, q (reference face order) and uvmean; a model started
+    from the file holds the same state."""
+    import glob
+
+    from oracle.oracle import Oracle
+    from sfincs_b200.bmi import Model
+
+    d, _ = small_subgrid(tmp_path)
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        f.write(f"{'dtrstout':<20} = 600\n")
+    o = Oracle(d, "f32")
+    cell = o.get("uv_nm").astype(np.int64) - 1
+    dirn = o.get("uv_dir").astype(np.int64)
+    g = Model(d)
+    seen = set()
+    checked = 0
+    while g.scalars()["t"] < 1900.0:
+        g.step(1)
+        new = set(glob.glob(os.path.join(d, "sfincs.*.rst"))) - seen
+        if not new:
+            continue
+        assert len(new) == 1
+        path = new.pop()
+        seen.add(path)
+        t = g.scalars()["t"]
+        s = int(t)
+        assert os.path.basename(path) == f"sfincs.20000101.{s // 3600:02d}{s % 3600 // 60:02d}{s % 60:02d}.rst"
+        typ, zs, q, uvm = read_restart(path)
+        assert typ == 1
+        assert np.array_equal(zs, g.get("zs").astype(np.float32))
+        qx, qy = g.get("qx"), g.get("qy")
+        assert q.size == cell.size + 1 and q[-1] == 0.0
+        assert np.array_equal(q[:-1], np.where(dirn == 0, qx[cell], qy[cell]).astype(np.float32))
+        d2 = str(tmp_path / f"from{checked}")
+        shutil.copytree(d, d2)
+        with open(os.path.join(d2, "sfincs.inp"), "a") as f:
+            f.write(f"{'rstfile':<20} = {os.path.basename(path)}\n")
+        g2 = Model(d2)
+        assert np.array_equal(g2.get("zs"), g.get("zs"))
+        g2.close()
+        checked += 1
+    assert checked == 3  # 600, 1200 and 1800 s
+    g.close()
