@@ -110,7 +110,6 @@ void QtBuilder::mesh() {
   auto path = [&](const std::string& f) { return h.dir + "/" + f; };
   if (k.qtrfile.find(".nc") == std::string::npos)
     throw std::runtime_error("only netCDF quadtree files (qtrfile *.nc) are supported");
-  if (!none(k.srcfile)) throw std::runtime_error("point sources on quadtree meshes are not supported by this core");
   if (!none(k.manningfile)) throw std::runtime_error("manningfile on quadtree meshes is not supported by this core");
   if (!none(k.qinffile)) throw std::runtime_error("qinffile on quadtree meshes is not supported by this core");
   q = read_qtr(path(k.qtrfile));
@@ -773,6 +772,26 @@ void load_quadtree(HostModel& h, const Keys& k) {
   b.bed();
   b.boundaries();
   b.finish();
+  // point sources (sfincs_discharges.f90:95-178): the finest active cell at
+  // each point (find_quadtree_cell), compact indices
+  if (!none(k.srcfile)) {
+    auto path = [&](const std::string& f) { return h.dir + "/" + f; };
+    auto xy = read_table(path(k.srcfile));
+    auto tb = read_table(path(k.disfile));
+    const int nsrc = (int)xy.size();
+    for (auto& r : xy) {
+      const int nm = quadtree_cell_index(h, r.at(0), r.at(1));
+      if (nm <= 0) throw std::runtime_error("point source outside the active mesh");
+      h.src_cell.push_back((int32_t)(nm - 1));
+    }
+    for (auto& r : tb) {
+      if ((int)r.size() < nsrc + 1) throw std::runtime_error("dis file has fewer columns than src points");
+      h.tsrc.push_back((float)r[0]);
+      for (int is = 0; is < nsrc; is++) h.qsrc.push_back((float)r[is + 1]);
+    }
+    h.p.nsrc = nsrc;
+    h.p.ntsrc = (int)h.tsrc.size();
+  }
 }
 
 }  // namespace sfg

@@ -687,10 +687,11 @@ __global__ void k_sources(const ScnDev* __restrict__ scns) {
         vol += (double)(S.qtsrc[is] * dt);
       }
     } else {
+      const float area = S.quadtree ? S.lv_area[S.qlev[c]] : S.area;  // cell_area(z_flags_iref(nm))
       const float before = S.zs[c];
-      const float z = fmaxf(S.zs[c] + S.qtsrc[is] * dt / S.area, S.zb[c]);
+      const float z = fmaxf(S.zs[c] + S.qtsrc[is] * dt / area, S.zb[c]);
       S.zs[c] = z;
-      vol += ((double)z - (double)before) * (double)S.area;
+      vol += ((double)z - (double)before) * (double)area;
     }
   }
   st.src_vol += vol;

@@ -33,11 +33,25 @@ def _cell_q(o, n_cells, npq):
     return qx, qy
 
 
-@pytest.mark.parametrize("subgrid", [False, True])
-def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid):
+def _add_sources(d):
+    """Three point sources (x, y in metres) with a discharge series (m3/s)."""
+    import os
+
+    np.savetxt(os.path.join(d, "sfincs.src"), np.array([[1000.0, 1000.0], [2500.0, 1600.0], [3500.0, 2800.0]]),
+               fmt="%.4f")
+    np.savetxt(os.path.join(d, "sfincs.dis"), np.array([[0.0, 5.0, 0.0, 2.0], [900.0, 20.0, 3.0, 2.0],
+                                                        [2000.0, 0.0, 6.0, 2.0]]), fmt="%.6f")
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        f.write(f"{'srcfile':<20} = sfincs.src\n{'disfile':<20} = sfincs.dis\n")
+
+
+@pytest.mark.parametrize("subgrid,sources", [(False, False), (True, False), (False, True), (True, True)])
+def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, sources):
     from sfincs_b200 import bmi as B
 
     d, _ = _write(tmp_path, subgrid)
+    if sources:
+        _add_sources(d)
     qc = B.layout(d, "qt_counts", 4)
     npc, npuv, ncuv = int(qc[0]), int(qc[1]), int(qc[2])
     o = _oracle(d, "f32")
