@@ -193,7 +193,6 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
                     drnfile = in.str("drnfile", "none");
   if (quadtree && !is_none(drnfile)) throw std::runtime_error("input 'drnfile' is not supported on quadtree grids by this core");
   P.structure_relax = in.real("structure_relax", 10.0f);
-  if (quadtree && !is_none(thdfile)) throw std::runtime_error("input 'thdfile' is not supported on quadtree grids by this core");
   if (quadtree && !is_none(weirfile)) throw std::runtime_error("input 'weirfile' is not supported on quadtree grids by this core");
   if (!quadtree && (nmax <= 0 || mmax <= 0)) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
 
@@ -256,10 +255,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
 // A .thd / .weir file holds polylines, each as a name line, an "nrows ncols"
 // line and nrows lines of x y followed by npars values per point (blank lines
 // skipped, commas accepted as separators, as list-directed input does).
-struct PolyRow {
-  float x, y, p[2];
-};
-static std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars) {
+std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars) {
   FILE* fp = std::fopen(file.c_str(), "r");
   if (!fp) throw std::runtime_error("cannot open polyline file " + file);
   std::vector<std::string> lines;
@@ -317,7 +313,7 @@ static int side_of(float ax, float ay, float bx, float by, float cx, float cy) {
 
 // Segments p1-p2 and q1-q2 cross when each separates the other's end points
 // (a touching or collinear end point counts as on neither side).
-static bool segments_cross(float p1x, float p1y, float p2x, float p2y, float q1x, float q1y, float q2x, float q2y) {
+bool segments_cross(float p1x, float p1y, float p2x, float p2y, float q1x, float q1y, float q2x, float q2y) {
   return side_of(p1x, p1y, p2x, p2y, q1x, q1y) != side_of(p1x, p1y, p2x, p2y, q2x, q2y) &&
          side_of(q1x, q1y, q2x, q2y, p1x, p1y) != side_of(q1x, q1y, q2x, q2y, p2x, p2y);
 }

@@ -91,6 +91,13 @@ struct Keys {
       wndfile, qinffile, prcpfile;
 };
 Keys parse_keys(const InpFile& in, HostModel& h, bool bmi);
+// Polylines of a .thd / .weir file: x, y and npars values per point.
+struct PolyRow {
+  float x, y, p[2];
+};
+std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars);
+// The reference's segment crossing test (geometry.f90 cross / direction, FP32).
+bool segments_cross(float p1x, float p1y, float p2x, float p2y, float q1x, float q1y, float q2x, float q2y);
 void read_boundary_series(HostModel& h, const Keys& k, bool water_level_bnd, std::vector<float>& xb,
                           std::vector<float>& yb, int& nbnd);
 void read_meteo_series(HostModel& h, const Keys& k, float rotation);

@@ -637,6 +637,51 @@ void QtBuilder::finish() {
       kk = 1;
   }
   const bool do_mask = P.advection && k.advection_mask && (nref > 1 || q.nmax > 1);  // :2132-2178
+  // point lookup keys (find_quadtree_cell: sfincs_quadtree.F90:764-820)
+  {
+    std::vector<std::pair<int64_t, int32_t>> kv((size_t)np);
+    for (long nm = 1; nm <= np; nm++)
+      kv[nm - 1] = {qt_key(iref_of[nm], h.z_m[nm - 1], h.z_n[nm - 1]), (int32_t)(nm - 1)};
+    std::sort(kv.begin(), kv.end());
+    h.qt_key.resize(np);
+    h.qt_key_cell.resize(np);
+    for (long i = 0; i < np; i++) h.qt_key[i] = kv[i].first, h.qt_key_cell[i] = kv[i].second;
+  }
+  // Thin dams (sfincs_structures.f90:385-495, sfincs_quadtree.F90:853-1010):
+  // per dam segment and refinement level, the cells in the segment's cell
+  // index box widened by one; a right or upper uv point whose segment between
+  // the two cell centres crosses the dam gets kcuv 0.  Applied after the
+  // boundary lists, the combined points and the advection mask, as the
+  // reference applies them after initialize_domain.
+  std::vector<int8_t> kcuv_run = kcuv;
+  if (!none(k.thdfile)) {
+    auto path = [&](const std::string& f) { return h.dir + "/" + f; };
+    for (const auto& pl : read_polylines(path(k.thdfile), 0)) {
+      for (size_t ipol = 0; ipol + 1 < pl.size(); ipol++) {
+        const float xpa = pl[ipol].x, ypa = pl[ipol].y, xpb = pl[ipol + 1].x, ypb = pl[ipol + 1].y;
+        const float xta = cosrot * (xpa - q.x0) + sinrot * (ypa - q.y0), yta = -sinrot * (xpa - q.x0) + cosrot * (ypa - q.y0);
+        const float xtb = cosrot * (xpb - q.x0) + sinrot * (ypb - q.y0), ytb = -sinrot * (xpb - q.x0) + cosrot * (ypb - q.y0);
+        for (int iref = nref; iref >= 1; iref--) {
+          const int64_t na = (int64_t)(yta / dyr[iref]) + 1, ma = (int64_t)(xta / dxr[iref]) + 1;
+          const int64_t nb = (int64_t)(ytb / dyr[iref]) + 1, mb = (int64_t)(xtb / dxr[iref]) + 1;
+          for (int64_t m = std::max(std::min(ma, mb) - 1, (int64_t)1); m <= std::max(ma, mb) + 1; m++) {
+            for (int64_t n = std::max(std::min(na, nb) - 1, (int64_t)1); n <= std::max(na, nb) + 1; n++) {
+              const int64_t key = qt_key(iref, m, n);
+              auto it = std::lower_bound(h.qt_key.begin(), h.qt_key.end(), key);
+              if (it == h.qt_key.end() || *it != key) continue;  // no active cell of this level here
+              const long nm = h.qt_key_cell[it - h.qt_key.begin()] + 1;
+              for (int32_t ip : {zuv_mu1[nm], zuv_mu2[nm], zuv_nu1[nm], zuv_nu2[nm]}) {
+                if (ip <= 0) continue;
+                const long nmu = uv_nmu[ip];
+                if (segments_cross(xpa, ypa, xpb, ypb, h.z_xz[nm - 1], h.z_yz[nm - 1], h.z_xz[nmu - 1], h.z_yz[nmu - 1]))
+                  kcuv_run[ip] = 0;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
   // roughness of regular beds (sfincs_domain.f90:1960-2061)
   if (!P.subgrid) {
     h.gn2_q.assign(npuv, 9.81f * 0.02f * 0.02f);
@@ -655,13 +700,13 @@ void QtBuilder::finish() {
     f.u_nmd = u_nmd[ip] - 1, f.u_nmu = u_nmu[ip] - 1, f.u_ndm = u_ndm[ip] - 1, f.u_num = u_num[ip] - 1;
     f.v_ndm = v_ndm[ip] - 1, f.v_nm = v_nm[ip] - 1, f.v_ndmu = v_ndmu[ip] - 1, f.v_nmu = v_nmu[ip] - 1;
     uint32_t info = (uv_dir[ip] == 1 ? QF_DIR : 0u);
-    if (kcuv[ip] == 1 || kcuv[ip] == 6) info |= QF_ACT;
+    if (kcuv_run[ip] == 1 || kcuv_run[ip] == 6) info |= QF_ACT;
     bool adv = P.advection;
     if (do_mask && (kcuv[u_nmu[ip]] != 1 || kcuv[u_nmd[ip]] != 1 || kcuv[v_nm[ip]] != 1 || kcuv[v_nmu[ip]] != 1 ||
                     kcuv[v_ndm[ip]] != 1 || kcuv[v_ndmu[ip]] != 1 || kcuv[u_ndm[ip]] != 1 || kcuv[u_num[ip]] != 1))
       adv = false;
     if (adv) info |= QF_ADV;
-    if (kcuv[u_nmd[ip]] == 1 && kcuv[u_nmu[ip]] == 1) info |= QF_TH;
+    if (kcuv_run[u_nmd[ip]] == 1 && kcuv_run[u_nmu[ip]] == 1) info |= QF_TH;
     if (uv_type[ip] != 0) info |= QF_TRANS;
     info |= (uint32_t)(uv_iref[ip] - 1) << 8;
     f.info = info;
@@ -688,16 +733,6 @@ void QtBuilder::finish() {
       h.n_kcs1++;
       h.area_total_kcs1 += (double)h.cell_area[nm - 1];
     }
-  }
-  // point lookup keys (find_quadtree_cell: sfincs_quadtree.F90:764-820)
-  {
-    std::vector<std::pair<int64_t, int32_t>> kv((size_t)np);
-    for (long nm = 1; nm <= np; nm++)
-      kv[nm - 1] = {qt_key(iref_of[nm], h.z_m[nm - 1], h.z_n[nm - 1]), (int32_t)(nm - 1)};
-    std::sort(kv.begin(), kv.end());
-    h.qt_key.resize(np);
-    h.qt_key_cell.resize(np);
-    for (long i = 0; i < np; i++) h.qt_key[i] = kv[i].first, h.qt_key_cell[i] = kv[i].second;
   }
   h.qcuv.resize(ncuv);
   for (long ic = 1; ic <= ncuv; ic++) h.qcuv[ic - 1] = make_int2(cuv_uv1[ic] - 1, cuv_uv2[ic] - 1);

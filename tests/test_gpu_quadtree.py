@@ -45,13 +45,32 @@ def _add_sources(d):
         f.write(f"{'srcfile':<20} = sfincs.src\n{'disfile':<20} = sfincs.dis\n")
 
 
-@pytest.mark.parametrize("subgrid,sources", [(False, False), (True, False), (False, True), (True, True)])
-def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, sources):
+def _add_thin_dams(d):
+    """A dam across the domain and a bent one over several refinement levels."""
+    import os
+
+    with open(os.path.join(d, "sfincs.thd"), "w") as f:
+        f.write("D1\n2 2\n1900.0 -100.0\n2100.0 3300.0\nD2\n3 2\n300.0 2500.0\n1500.0 1500.0\n3900.0 2900.0\n")
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        f.write(f"{'thdfile':<20} = sfincs.thd\n")
+
+
+@pytest.mark.parametrize("subgrid,extra", [(False, None), (True, None), (False, "sources"), (True, "sources"),
+                                           (False, "dams"), (True, "dams")])
+def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, extra):
     from sfincs_b200 import bmi as B
 
     d, _ = _write(tmp_path, subgrid)
-    if sources:
+    if extra == "sources":
         _add_sources(d)
+    if extra == "dams":
+        _add_thin_dams(d)
+        qc = B.layout(d, "qt_counts", 4)
+        act = B.layout(d, "uv_act", int(qc[1]))
+        kc = _oracle(d, "f32").get("kcuv", int(qc[1]))
+        assert np.array_equal(act > 0, np.isin(kc, (1, 6)))  # face activity after the dams, face by face
+        d0, _ = _write(tmp_path, subgrid, name="open")
+        assert int((B.layout(d0, "uv_act", int(qc[1])) > 0).sum()) > int((act > 0).sum())  # the dams removed faces
     qc = B.layout(d, "qt_counts", 4)
     npc, npuv, ncuv = int(qc[0]), int(qc[1]), int(qc[2])
     o = _oracle(d, "f32")
