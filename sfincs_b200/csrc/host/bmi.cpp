@@ -925,9 +925,11 @@ int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst
     } else if (nm == "nstruc") {
       out = {(double)h.struc.size()};
     } else if (nm == "struc") {
-      // per weir face: compact cell (0-based), direction, crest level, Cd, relative length
+      // per weir face: compact cell (0-based; on a quadtree the uv point), direction, crest level, Cd,
+      // relative length
       for (auto& w : h.struc)
-        for (double v : {(double)h.dense2cmp[w.face], (double)w.dir, (double)w.height, (double)w.cd, (double)w.len})
+        for (double v : {h.p.quadtree ? (double)w.face : (double)h.dense2cmp[w.face], (double)w.dir, (double)w.height,
+                         (double)w.cd, (double)w.len})
           out.push_back(v);
     } else if (nm == "gb_cell") {
       for (auto c : h.gb_cmp) out.push_back((double)c);

@@ -193,7 +193,6 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
                     drnfile = in.str("drnfile", "none");
   if (quadtree && !is_none(drnfile)) throw std::runtime_error("input 'drnfile' is not supported on quadtree grids by this core");
   P.structure_relax = in.real("structure_relax", 10.0f);
-  if (quadtree && !is_none(weirfile)) throw std::runtime_error("input 'weirfile' is not supported on quadtree grids by this core");
   if (!quadtree && (nmax <= 0 || mmax <= 0)) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
 
   // ---- derived (sfincs_input.f90:347-745) ------------------------------------
@@ -289,7 +288,7 @@ std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int np
 
 // Length of the projection of the segment a-b onto the line segment 1-2,
 // each end clamped to the segment (third_party_open/utils/geometry.f90:215-297).
-static float projected_length(float x0a, float y0a, float x0b, float y0b, float x1, float y1, float x2, float y2) {
+float projected_length(float x0a, float y0a, float x0b, float y0b, float x1, float y1, float x2, float y2) {
   const float aa = std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
   auto along = [&](float px, float py, float& b) {
     b = std::fabs((x2 - x1) * (y1 - py) - (x1 - px) * (y2 - y1)) / std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -654,34 +655,101 @@ void QtBuilder::finish() {
   // boundary lists, the combined points and the advection mask, as the
   // reference applies them after initialize_domain.
   std::vector<int8_t> kcuv_run = kcuv;
-  if (!none(k.thdfile)) {
-    auto path = [&](const std::string& f) { return h.dir + "/" + f; };
-    for (const auto& pl : read_polylines(path(k.thdfile), 0)) {
-      for (size_t ipol = 0; ipol + 1 < pl.size(); ipol++) {
-        const float xpa = pl[ipol].x, ypa = pl[ipol].y, xpb = pl[ipol + 1].x, ypb = pl[ipol + 1].y;
-        const float xta = cosrot * (xpa - q.x0) + sinrot * (ypa - q.y0), yta = -sinrot * (xpa - q.x0) + cosrot * (ypa - q.y0);
-        const float xtb = cosrot * (xpb - q.x0) + sinrot * (ypb - q.y0), ytb = -sinrot * (xpb - q.x0) + cosrot * (ypb - q.y0);
-        for (int iref = nref; iref >= 1; iref--) {
-          const int64_t na = (int64_t)(yta / dyr[iref]) + 1, ma = (int64_t)(xta / dxr[iref]) + 1;
-          const int64_t nb = (int64_t)(ytb / dyr[iref]) + 1, mb = (int64_t)(xtb / dxr[iref]) + 1;
-          for (int64_t m = std::max(std::min(ma, mb) - 1, (int64_t)1); m <= std::max(ma, mb) + 1; m++) {
-            for (int64_t n = std::max(std::min(na, nb) - 1, (int64_t)1); n <= std::max(na, nb) + 1; n++) {
-              const int64_t key = qt_key(iref, m, n);
-              auto it = std::lower_bound(h.qt_key.begin(), h.qt_key.end(), key);
-              if (it == h.qt_key.end() || *it != key) continue;  // no active cell of this level here
-              const long nm = h.qt_key_cell[it - h.qt_key.begin()] + 1;
-              for (int32_t ip : {zuv_mu1[nm], zuv_mu2[nm], zuv_nu1[nm], zuv_nu2[nm]}) {
-                if (ip <= 0) continue;
-                const long nmu = uv_nmu[ip];
-                if (segments_cross(xpa, ypa, xpb, ypb, h.z_xz[nm - 1], h.z_yz[nm - 1], h.z_xz[nmu - 1], h.z_yz[nmu - 1]))
-                  kcuv_run[ip] = 0;
-              }
+  auto path = [&](const std::string& f) { return h.dir + "/" + f; };
+  // uv points crossed by one polyline -> the last segment crossing each
+  auto crossed = [&](const std::vector<PolyRow>& pl) {
+    std::map<long, int> ind;
+    for (size_t ipol = 0; ipol + 1 < pl.size(); ipol++) {
+      const float xpa = pl[ipol].x, ypa = pl[ipol].y, xpb = pl[ipol + 1].x, ypb = pl[ipol + 1].y;
+      const float xta = cosrot * (xpa - q.x0) + sinrot * (ypa - q.y0), yta = -sinrot * (xpa - q.x0) + cosrot * (ypa - q.y0);
+      const float xtb = cosrot * (xpb - q.x0) + sinrot * (ypb - q.y0), ytb = -sinrot * (xpb - q.x0) + cosrot * (ypb - q.y0);
+      for (int iref = nref; iref >= 1; iref--) {
+        const int64_t na = (int64_t)(yta / dyr[iref]) + 1, ma = (int64_t)(xta / dxr[iref]) + 1;
+        const int64_t nb = (int64_t)(ytb / dyr[iref]) + 1, mb = (int64_t)(xtb / dxr[iref]) + 1;
+        for (int64_t m = std::max(std::min(ma, mb) - 1, (int64_t)1); m <= std::max(ma, mb) + 1; m++) {
+          for (int64_t n = std::max(std::min(na, nb) - 1, (int64_t)1); n <= std::max(na, nb) + 1; n++) {
+            const int64_t key = qt_key(iref, m, n);
+            auto it = std::lower_bound(h.qt_key.begin(), h.qt_key.end(), key);
+            if (it == h.qt_key.end() || *it != key) continue;  // no active cell of this level here
+            const long nm = h.qt_key_cell[it - h.qt_key.begin()] + 1;
+            for (int32_t ip : {zuv_mu1[nm], zuv_mu2[nm], zuv_nu1[nm], zuv_nu2[nm]}) {
+              if (ip <= 0) continue;
+              const long nmu = uv_nmu[ip];
+              if (segments_cross(xpa, ypa, xpb, ypb, h.z_xz[nm - 1], h.z_yz[nm - 1], h.z_xz[nmu - 1], h.z_yz[nmu - 1]))
+                ind[ip] = (int)ipol;
             }
           }
         }
       }
     }
+    return ind;
+  };
+  if (!none(k.thdfile))
+    for (const auto& pl : read_polylines(path(k.thdfile), 0))
+      for (const auto& e : crossed(pl)) kcuv_run[e.first] = 0;
+  // Weirs (sfincs_structures.f90:38-381): crossed length, crest and Cd per uv
+  // point, kept where the crest is above the face bed (kcuv 3, after the dams)
+  if (!none(k.weirfile)) {
+    struct Acc {
+      float len = 0.0f, height = -9999.0f, cd = 0.0f;
+    };
+    std::map<long, Acc> acc;
+    const float pi = P.pi;
+    for (const auto& pl : read_polylines(path(k.weirfile), 2)) {
+      for (const auto& e : crossed(pl)) {
+        const long ip = e.first, nm = uv_nm[ip], nmu = uv_nmu[ip];
+        const int iref = uv_iref[ip], idir = uv_dir[ip];
+        const float dxs = idir == 0 ? dyr[iref] : dxr[iref];
+        float xuv, yuv, xuv1, yuv1, xuv2, yuv2;
+        if (iref_of[nm] >= iref_of[nmu]) {  // normal point or fine to coarse
+          xuv = h.z_xz[nm - 1] + 0.5f * dxs * std::cos(idir == 0 ? rotation : rotation + 0.5f * pi);
+          yuv = h.z_yz[nm - 1] + 0.5f * dxs * std::sin(idir == 0 ? rotation : rotation + 0.5f * pi);
+        } else {
+          xuv = h.z_xz[nmu - 1] + 0.5f * dxs * std::cos(idir == 0 ? rotation - pi : rotation - 0.5f * pi);
+          yuv = h.z_yz[nmu - 1] + 0.5f * dxs * std::sin(idir == 0 ? rotation - pi : rotation - 0.5f * pi);
+        }
+        if (idir == 0) {
+          xuv1 = xuv + 0.5f * dxs * std::cos(rotation - 0.5f * pi);
+          yuv1 = yuv + 0.5f * dxs * std::sin(rotation - 0.5f * pi);
+          xuv2 = xuv + 0.5f * dxs * std::cos(rotation + 0.5f * pi);
+          yuv2 = yuv + 0.5f * dxs * std::sin(rotation + 0.5f * pi);
+        } else {
+          xuv1 = xuv + 0.5f * dxs * std::cos(rotation - pi);
+          yuv1 = yuv + 0.5f * dxs * std::sin(rotation - pi);
+          xuv2 = xuv + 0.5f * dxs * std::cos(rotation);
+          yuv2 = yuv + 0.5f * dxs * std::sin(rotation);
+        }
+        const PolyRow &r0 = pl[(size_t)e.second], &r1 = pl[(size_t)e.second + 1];
+        Acc& a = acc[ip];
+        a.len = a.len + projected_length(xuv1, yuv1, xuv2, yuv2, r0.x, r0.y, r1.x, r1.y);
+        const float dst1 = std::sqrt((xuv - r0.x) * (xuv - r0.x) + (yuv - r0.y) * (yuv - r0.y));
+        const float dst2 = std::sqrt((xuv - r1.x) * (xuv - r1.x) + (yuv - r1.y) * (yuv - r1.y));
+        const float wfac = dst1 / (dst1 + dst2);
+        a.height = std::max(a.height, r0.p[0] * (1.0f - wfac) + r1.p[0] * wfac);
+        a.cd = r0.p[1] * (1.0f - wfac) + r1.p[1] * wfac;
+      }
+    }
+    std::vector<uint8_t> weir(npuv + 2, 0);
+    for (const auto& e : acc) {
+      const long ip = e.first;
+      const float bed = P.subgrid ? h.sgz_u[ip - 1].x : h.zbmx_q[ip - 1];
+      if (!(e.second.height > bed)) continue;
+      StrucFace w{};
+      w.face = (int)(ip - 1);
+      w.nm = (int)(uv_nm[ip] - 1);
+      w.nmu = (int)(uv_nmu[ip] - 1);
+      w.dir = uv_dir[ip];
+      w.height = e.second.height;
+      w.cd = e.second.cd;
+      w.len = e.second.len / (uv_dir[ip] == 0 ? dyr[uv_iref[ip]] : dxr[uv_iref[ip]]);
+      h.struc.push_back(w);
+      kcuv_run[ip] = 3;
+      weir[ip] = 1;
+    }
+    for (auto& b : h.bfaces)
+      if (weir[b.face + 1]) b.info |= 16;  // no boundary flux under a weir (sfincs_boundaries.f90:1009)
   }
+  P.nstruc = (int)h.struc.size();
   // roughness of regular beds (sfincs_domain.f90:1960-2061)
   if (!P.subgrid) {
     h.gn2_q.assign(npuv, 9.81f * 0.02f * 0.02f);
