@@ -191,7 +191,6 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   const bool quadtree = !is_none(qtrfile);
   const std::string thdfile = in.str("thdfile", "none"), weirfile = in.str("weirfile", "none"),
                     drnfile = in.str("drnfile", "none");
-  if (quadtree && !is_none(drnfile)) throw std::runtime_error("input 'drnfile' is not supported on quadtree grids by this core");
   P.structure_relax = in.real("structure_relax", 10.0f);
   if (!quadtree && (nmax <= 0 || mmax <= 0)) throw std::runtime_error("nmax/mmax missing in sfincs.inp");
 
@@ -283,6 +282,39 @@ std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int np
     }
     out.push_back(std::move(pl));
   }
+  return out;
+}
+
+// Drainage structures file (sfincs_discharges.f90:203-256): one line each,
+// "x_intake y_intake x_outfall y_outfall type params...", with 1 parameter for
+// types 1-3 and 6 for the gates (4, 5).
+std::vector<DrnLine> read_drainage(const std::string& file) {
+  FILE* fp = std::fopen(file.c_str(), "r");
+  if (!fp) throw std::runtime_error("cannot open drainage file " + file);
+  std::vector<DrnLine> out;
+  char buf[4096];
+  while (std::fgets(buf, sizeof buf, fp)) {
+    std::string l(buf);
+    for (char& ch : l)
+      if (ch == ',' || ch == '\t' || ch == '\r' || ch == '\n') ch = ' ';
+    if (l.find_first_not_of(' ') == std::string::npos) continue;
+    DrnLine d{};
+    const int got = std::sscanf(l.c_str(), "%f %f %f %f %d %f %f %f %f %f %f", &d.xs, &d.ys, &d.xo, &d.yo, &d.type,
+                                &d.p[0], &d.p[1], &d.p[2], &d.p[3], &d.p[4], &d.p[5]);
+    const int npars = (d.type >= 1 && d.type <= 3) ? 1 : ((d.type == 4 || d.type == 5) ? 6 : 0);
+    if (got < 5 || npars == 0) {
+      std::fclose(fp);
+      throw std::runtime_error("drainage type not recognized in " + file);
+    }
+    if (got < 5 + npars) {
+      std::fclose(fp);
+      throw std::runtime_error("drainage type " + std::to_string(d.type) + " requires " + std::to_string(npars) +
+                               " parameters");
+    }
+    for (int k = npars; k < 6; k++) d.p[k] = 0.0f;
+    out.push_back(d);
+  }
+  std::fclose(fp);
   return out;
 }
 
@@ -1021,9 +1053,6 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   // "x_intake y_intake x_outfall y_outfall type params...", the intake and
   // outfall cells appended after the point sources
   if (!is_none(K.drnfile)) {
-    FILE* fp = std::fopen(path(K.drnfile).c_str(), "r");
-    if (!fp) throw std::runtime_error("cannot open drainage file " + K.drnfile);
-    char buf[4096];
     auto cell_of = [&](float x, float y) -> int64_t {
       const float xt = cosrot * (x - x0) + sinrot * (y - y0);
       const float yt = -sinrot * (x - x0) + cosrot * (y - y0);
@@ -1031,25 +1060,13 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
       if (!act(n, m)) throw std::runtime_error("drainage point outside the active mesh");
       return OFF(n, m);
     };
-    while (std::fgets(buf, sizeof buf, fp)) {
-      std::string l(buf);
-      for (char& ch : l)
-        if (ch == ',' || ch == '\t' || ch == '\r' || ch == '\n') ch = ' ';
-      if (l.find_first_not_of(' ') == std::string::npos) continue;
-      float xs, ys, xo, yo, p[6] = {0, 0, 0, 0, 0, 0};
-      int type = 0;
-      const int got = std::sscanf(l.c_str(), "%f %f %f %f %d %f %f %f %f %f %f", &xs, &ys, &xo, &yo, &type, &p[0], &p[1],
-                                  &p[2], &p[3], &p[4], &p[5]);
-      const int npars = (type >= 1 && type <= 3) ? 1 : ((type == 4 || type == 5) ? 6 : 0);
-      if (got < 5 || npars == 0) throw std::runtime_error("drainage type not recognized in " + K.drnfile);
-      if (got < 5 + npars) throw std::runtime_error("drainage type " + std::to_string(type) + " requires " +
-                                                    std::to_string(npars) + " parameters");
+    for (const DrnLine& r : read_drainage(path(K.drnfile))) {
       DrnDev d{};
-      d.type = type;
-      const int64_t ci = cell_of(xs, ys), co = cell_of(xo, yo);
+      d.type = r.type;
+      const int64_t ci = cell_of(r.xs, r.ys), co = cell_of(r.xo, r.yo);
       d.cin = (int)ci;
       d.cout = (int)co;
-      for (int k = 0; k < npars; k++) d.p[k] = p[k];
+      for (int k = 0; k < 6; k++) d.p[k] = r.p[k];
       const int ni = (int)(ci % ld) - kGhostPad, mi = (int)(ci / ld), no = (int)(co % ld) - kGhostPad, mo = (int)(co / ld);
       const float xsnk = xz(ni, mi), ysnk = yz(ni, mi), xsrc = xz(no, mo), ysrc = yz(no, mo);
       d.distance = std::sqrt((xsrc - xsnk) * (xsrc - xsnk) + (ysrc - ysnk) * (ysrc - ysnk));
@@ -1057,7 +1074,6 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
       h.src_cell.push_back((int32_t)ci);
       h.src_cell.push_back((int32_t)co);
     }
-    std::fclose(fp);
   }
   P.ndrn = (int)h.drn.size();
   // 32 x 8 cell tiles that hold at least one active cell (the work list of the

@@ -98,6 +98,13 @@ struct PolyRow {
 std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars);
 // The reference's segment crossing test (geometry.f90 cross / direction, FP32).
 bool segments_cross(float p1x, float p1y, float p2x, float p2y, float q1x, float q1y, float q2x, float q2y);
+// One line of a drainage structures file: intake and outfall points, type, parameters.
+struct DrnLine {
+  float xs, ys, xo, yo;
+  int type;
+  float p[6];
+};
+std::vector<DrnLine> read_drainage(const std::string& file);
 // Projected length of segment a-b onto segment 1-2 (geometry.f90:215-297).
 float projected_length(float x0a, float y0a, float x0b, float y0b, float x1, float y1, float x2, float y2);
 void read_boundary_series(HostModel& h, const Keys& k, bool water_level_bnd, std::vector<float>& xb,

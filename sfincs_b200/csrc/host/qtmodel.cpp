@@ -895,6 +895,25 @@ void load_quadtree(HostModel& h, const Keys& k) {
     h.p.nsrc = nsrc;
     h.p.ntsrc = (int)h.tsrc.size();
   }
+  // drainage structures: intake and outfall cells after the point sources
+  if (!none(k.drnfile)) {
+    auto path = [&](const std::string& f) { return h.dir + "/" + f; };
+    for (const DrnLine& r : read_drainage(path(k.drnfile))) {
+      const int ni = quadtree_cell_index(h, r.xs, r.ys), no = quadtree_cell_index(h, r.xo, r.yo);
+      if (ni <= 0 || no <= 0) throw std::runtime_error("drainage point outside the active mesh");
+      DrnDev d{};
+      d.type = r.type;
+      d.cin = ni - 1;
+      d.cout = no - 1;
+      for (int j = 0; j < 6; j++) d.p[j] = r.p[j];
+      const float xsnk = h.z_xz[ni - 1], ysnk = h.z_yz[ni - 1], xsrc = h.z_xz[no - 1], ysrc = h.z_yz[no - 1];
+      d.distance = std::sqrt((xsrc - xsnk) * (xsrc - xsnk) + (ysrc - ysnk) * (ysrc - ysnk));
+      h.drn.push_back(d);
+      h.src_cell.push_back((int32_t)(ni - 1));
+      h.src_cell.push_back((int32_t)(no - 1));
+    }
+  }
+  h.p.ndrn = (int)h.drn.size();
 }
 
 }  // namespace sfg

@@ -278,10 +278,12 @@ __device__ __forceinline__ void update_drainage(const ScnDev& S, const StepPlan&
       else
         qq = (float)fmax((double)qq, -fmax(S.zvol[d.cout], 0.0) / (double)dt);
     } else {
+      const float ain = S.quadtree ? S.lv_area[S.qlev[d.cin]] : S.area;  // cell_area(z_flags_iref(nm))
+      const float aout = S.quadtree ? S.lv_area[S.qlev[d.cout]] : S.area;
       if (qq > 0.0f)
-        qq = (float)fmin((double)qq, fmax((zin - (double)S.zb[d.cin]) * (double)S.area, 0.0) / (double)dt);
+        qq = (float)fmin((double)qq, fmax((zin - (double)S.zb[d.cin]) * (double)ain, 0.0) / (double)dt);
       else
-        qq = (float)fmax((double)qq, -fmax((zout - (double)S.zb[d.cout]) * (double)S.area, 0.0) / (double)dt);
+        qq = (float)fmax((double)qq, -fmax((zout - (double)S.zb[d.cout]) * (double)aout, 0.0) / (double)dt);
     }
     S.qtsrc[jin] = -qq;
     S.qtsrc[jout] = qq;

@@ -66,14 +66,32 @@ def _add_weirs(d):
         f.write(f"{'weirfile':<20} = sfincs.weir\n")
 
 
+def _add_drainage(d):
+    """The five drainage structure types between cells of different levels."""
+    import os
+
+    rows = ["500.0 500.0 2500.0 2500.0 1 2.0",
+            "900.0 2100.0 3100.0 1700.0 2 1.5",
+            "1300.0 2900.0 700.0 1500.0 3 1.0",
+            "1700.0 700.0 300.0 2700.0 4 3.0 -6.0 0.02 -3.0 4.0 120.0",
+            "2100.0 1300.0 3700.0 300.0 5 2.0 -8.0 0.025 600.0 1500.0 60.0"]
+    with open(os.path.join(d, "sfincs.drn"), "w") as f:
+        f.write("\n".join(rows) + "\n")
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        f.write(f"{'drnfile':<20} = sfincs.drn\n")
+
+
 @pytest.mark.parametrize("subgrid,extra", [(False, None), (True, None), (False, "sources"), (True, "sources"),
-                                           (False, "dams"), (True, "dams"), (False, "weirs"), (True, "weirs")])
+                                           (False, "dams"), (True, "dams"), (False, "weirs"), (True, "weirs"),
+                                           (False, "drainage"), (True, "drainage")])
 def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, extra):
     from sfincs_b200 import bmi as B
 
     d, _ = _write(tmp_path, subgrid)
     if extra == "sources":
         _add_sources(d)
+    if extra == "drainage":
+        _add_drainage(d)
     if extra == "weirs":
         _add_weirs(d)
         n = int(_oracle(d, "f32").get("nrstructures", 1)[0])
