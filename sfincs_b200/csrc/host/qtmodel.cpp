@@ -112,7 +112,6 @@ void QtBuilder::mesh() {
   if (k.qtrfile.find(".nc") == std::string::npos)
     throw std::runtime_error("only netCDF quadtree files (qtrfile *.nc) are supported");
   if (!none(k.manningfile)) throw std::runtime_error("manningfile on quadtree meshes is not supported by this core");
-  if (!none(k.qinffile)) throw std::runtime_error("qinffile on quadtree meshes is not supported by this core");
   q = read_qtr(path(k.qtrfile));
   if (q.nlev > kMaxQtLevels) throw std::runtime_error("more than 8 quadtree refinement levels");
   P.quadtree = 1;
@@ -813,6 +812,11 @@ void QtBuilder::finish() {
       const float zz = P.subgrid ? h.zz_min[i] : h.zb[i];
       h.qinf[i] = zz > k.qinf_zmin ? k.qinf : 0.0f;
     }
+  } else if (P.precip && !none(k.qinffile)) {  // c2d: a binary field in cell order, mm/h
+    P.infiltration = 1;
+    const auto r = read_binary<float>(h.dir + "/" + k.qinffile, (size_t)np);
+    h.qinf.assign(np, 0.0f);
+    for (long i = 0; i < np; i++) h.qinf[i] = r[(size_t)i] / 3600.0f / 1000.0f;
   }
   // initial state (sfincs_initial_conditions.F90:98-106, sfincs_subgrid.F90:907-962)
   h.zs.assign(np, 0.0f);

@@ -81,7 +81,22 @@ def _add_drainage(d):
         f.write(f"{'drnfile':<20} = sfincs.drn\n")
 
 
-@pytest.mark.parametrize("subgrid,extra", [(False, None), (True, None), (False, "sources"), (True, "sources"),
+def _add_infiltration(d):
+    """A c2d infiltration field (mm/h per cell, cell order) under the rain."""
+    import os
+
+    from sfincs_b200 import bmi as B
+
+    n = int(B.layout(d, "qt_counts", 4)[0])
+    rng = np.random.default_rng(5)
+    rng.uniform(0.0, 20.0, n).astype(np.float32).tofile(os.path.join(d, "sfincs.qinf"))
+    np.savetxt(os.path.join(d, "sfincs.prcp"), np.array([[0.0, 30.0], [7200.0, 30.0]]), fmt="%.6f")
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        f.write(f"{'qinffile':<20} = sfincs.qinf\n{'prcfile':<20} = sfincs.prcp\n")
+
+
+@pytest.mark.parametrize("subgrid,extra", [(False, "infiltration"), (True, "infiltration"),
+                                           (False, None), (True, None), (False, "sources"), (True, "sources"),
                                            (False, "dams"), (True, "dams"), (False, "weirs"), (True, "weirs"),
                                            (False, "drainage"), (True, "drainage")])
 def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, extra):
@@ -92,6 +107,8 @@ def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, extra):
         _add_sources(d)
     if extra == "drainage":
         _add_drainage(d)
+    if extra == "infiltration":
+        _add_infiltration(d)
     if extra == "weirs":
         _add_weirs(d)
         n = int(_oracle(d, "f32").get("nrstructures", 1)[0])
