@@ -50,6 +50,39 @@ struct F1 {  // 1-based Fortran-style vector
   void fill(X x) { std::fill(v.begin() + (v.empty() ? 0 : 1), v.end(), x); }
 };
 
+// Cube root of the core-precision ("f32") instantiation, restating the CUDA
+// core's method with the same IEEE operations in the same order, so both give
+// the same bits: an estimate of x^(-1/3) from the float's bit pattern
+// (0x54a232a0 - bits / 3), two Newton steps r += r (1 - x r^3) / 3, y = x r^2
+// and one Newton correction of y; denormals are scaled by 2^72 first.  The
+// "ref" and "fp64" instantiations keep the reference's power x**(1.0/3.0).
+static float core_cube_root_pos(float x) {
+  float s = 1.0f;
+  if (x < 1.17549435e-38f) {
+    x = x * 4722366482869645213696.0f;
+    s = 5.9604644775390625e-08f;
+  }
+  uint32_t bits;
+  std::memcpy(&bits, &x, 4);
+  bits = 0x54a232a0u - bits / 3u;
+  float r;
+  std::memcpy(&r, &bits, 4);
+  for (int k = 0; k < 2; k++) {
+    const float r3 = (r * r) * r;
+    const float e = std::fma(-x, r3, 1.0f);
+    r = std::fma(r * 0.333333343f, e, r);
+  }
+  float y = (x * r) * r;
+  const float res = std::fma(-(y * y), y, x);
+  y = std::fma(res * 0.333333343f, r * r, y);
+  return y * s;
+}
+static float core_cube_root(float x) {
+  if (x > 0.0f && x < 3.40282347e+38f) return core_cube_root_pos(x);
+  if (x < 0.0f && x > -3.40282347e+38f) return -core_cube_root_pos(-x);
+  return x + x;
+}
+
 template <class X>
 struct F2 {  // (n1, n2) column-major, 1-based
   std::vector<X> v;
@@ -1877,6 +1910,7 @@ struct Model {
     initialize_roughness();
     initialize_infiltration();
     initialize_hydro();
+    fill_h73_tables();
     if (qt_nlev == 1) use_quadtree = false;  // sfincs_domain.f90:42-50
     set_advection_mask();
     read_structures();  // sfincs_lib.f90:156, after initialize_domain
@@ -1888,6 +1922,34 @@ struct Model {
     min_dt = 1.0e-6f;
     dtavg = 0.0f;
     nt = 0;
+  }
+
+  // fill_h73_tables: sfincs_data.f90:858-881.  x73(j, k) = hh**2 * hh**(1.0/3.0),
+  // hh = 0.001 * j * 10.0**(k - 6); stored 1-based at (k - 1) * 1000 + j.
+  void fill_h73_tables() {
+    if (!h73table) return;
+    x73.alloc(10000);
+    for (int k = 1; k <= 10; k++) {
+      T p10 = (T)1;
+      for (int i = 0; i < std::abs(k - 6); i++) p10 = p10 * (T)10;
+      if (k < 6) p10 = (T)1 / p10;
+      for (int j = 1; j <= 1000; j++) {
+        T hh = (T)0.001f * (T)j * p10;
+        x73((long)(k - 1) * 1000 + j) = hh * hh * std::pow(hh, (T)(1.0f / 3.0f));
+      }
+    }
+  }
+  // power7over3: sfincs_momentum.f90:787-820 (row clamped to 1..1000)
+  T power7over3(T hu) {
+    static const float lim[10] = {0.00001f, 0.0001f, 0.001f, 0.01f, 0.1f, 1.0f, 10.0f, 100.0f, 1000.0f, 10000.0f};
+    static const float scl[10] = {1e8f, 1e7f, 1e6f, 1e5f, 1e4f, 1e3f, 100.0f, 10.0f, 1.0f, 0.1f};
+    for (int k = 1; k <= 10; k++) {
+      if (hu < (T)lim[k - 1]) {
+        long j = std::min(std::max((long)((T)scl[k - 1] * hu), 1L), 1000L);
+        return x73((long)(k - 1) * 1000 + j);
+      }
+    }
+    return (T)std::pow((T)10000, (T)(7.0f / 3.0f));
   }
 
   // ============================================================ time step
@@ -2158,8 +2220,8 @@ struct Model {
         }
         drainage_fraction_open(idrn) = frac;
         drainage_status(idrn) = (int8_t)status;
-        // hgate**(7.0/3.0); the core's precision evaluates it as hgate**2 * cbrt(hgate)
-        float h73 = core ? hgate * hgate * std::cbrt(hgate) : std::pow(hgate, 7.0f / 3.0f);
+        // hgate**(7.0/3.0); the core's precision evaluates it as hgate**2 * cube root(hgate)
+        float h73 = core ? hgate * hgate * core_cube_root(hgate) : std::pow(hgate, 7.0f / 3.0f);
         qq = (qq0 - g * hgate * dzds * dt) / (1.0f + g * (mng * mng) * dt * std::fabs(qq0) / h73);
         qq = qq * wdt * frac;
       }
@@ -2190,6 +2252,11 @@ struct Model {
     const T expo = (T)(1.0f / 3.0f);
     const long L = subgrid_nlevels;
     float mdt = min_dt;
+    // The core-precision instantiation evaluates a few expressions as the CUDA
+    // core does (one division for the table interval and one for the flux
+    // update, fused multiply-adds, its own cube root); "ref" and "fp64" keep
+    // the reference's expressions.
+    constexpr bool CORE = std::is_same<TZ, float>::value;
 #pragma omp parallel for schedule(dynamic, 256) reduction(min : mdt)
     for (long ip = 1; ip <= npuv; ip++) {
       if (!(kcuv(ip) == 1 || kcuv(ip) == 6)) continue;
@@ -2247,10 +2314,23 @@ struct Model {
         T phi = 1;
         T hu, gnavg2;
         if (subgrid) {
-          if (zsu > zmax) {
+          if (zsu > zmax && CORE) {
+            hu = sg_uv_havg_zmax(ip) + zsu;
+            gnavg2 = sg_uv_navg_w(ip) -
+                     (sg_uv_navg_w(ip) - sg_uv_nrep_zmax(ip)) / std::fma(sg_uv_fnfit(ip), zsu - zmax, (T)1);
+          } else if (zsu > zmax) {
             hu = sg_uv_havg_zmax(ip) + zsu;
             gnavg2 = sg_uv_navg_w(ip) -
                      (sg_uv_navg_w(ip) - sg_uv_nrep_zmax(ip)) / (sg_uv_fnfit(ip) * (zsu - zmax) + (T)1);
+          } else if (CORE) {
+            // scaled level x = (zsu - zmin) (L - 1) / (zmax - zmin): interval int(x) + 1, weight x - (iuv - 1)
+            T rdz = (T)(L - 1) / (zmax - zmin);
+            T x = (zsu - zmin) * rdz;
+            long iuv = std::min(std::max((long)x + 1, 1L), L - 1);
+            T facint = x - (T)(iuv - 1);
+            hu = std::fma(sg_uv_havg(iuv + 1, ip) - sg_uv_havg(iuv, ip), facint, sg_uv_havg(iuv, ip));
+            gnavg2 = std::fma(sg_uv_nrep(iuv + 1, ip) - sg_uv_nrep(iuv, ip), facint, sg_uv_nrep(iuv, ip));
+            phi = std::fma(sg_uv_pwet(iuv + 1, ip) - sg_uv_pwet(iuv, ip), facint, sg_uv_pwet(iuv, ip));
           } else {
             T dzuv = (zmax - zmin) / (T)(L - 1);
             long iuv = std::min((long)((zsu - zmin) / dzuv) + 1, L - 1);
@@ -2329,13 +2409,19 @@ struct Model {
             frc = frc + tw * hu * (T)4;
         }
         T qfr;
+        const T cr = CORE ? (T)core_cube_root((float)hu) : (T)0;  // the core's hu**(1/3)
         if (kfuv(ip) == 0) {
-          qfr = std::sqrt(std::fabs(dzdx) / (std::max(gnavg2, (T)1.0e-5f) / (T)10)) * std::pow(hu, (T)(5.0f / 3.0f));
+          T h53 = CORE ? hu * (cr * cr) : (T)std::pow(hu, (T)(5.0f / 3.0f));
+          qfr = std::sqrt(std::fabs(dzdx) / (std::max(gnavg2, (T)1.0e-5f) / (T)10)) * h53;
         } else {
-          if (friction2d)
+          if (friction2d && CORE) {
+            T huvu = hu * vu;
+            qfr = std::sqrt(std::fma(qx_nm, qx_nm, huvu * huvu));
+          } else if (friction2d) {
             qfr = std::sqrt(qx_nm * qx_nm + (hu * vu) * (hu * vu));
-          else
+          } else {
             qfr = std::fabs(qx_nm);
+          }
         }
         T qsm = qx_nm;
         if (thetasmoothing) {
@@ -2344,12 +2430,22 @@ struct Model {
               qsm = (T)theta * qx_nm + (T)0.5f * ((T)1 - (T)theta) * (qx_nmu + qx_nmd);
           }
         }
-        if (h73table) throw std::runtime_error("oracle: h73table is off by default and not restated");
         // The CUDA core evaluates hu**(1.0/3.0) as a cube root (under one ulp from
-        // hu**0.333333343 for 1e-3 <= hu <= 1e3); the "f32" (core precision)
-        // instantiation does the same, "ref" and "fp64" keep the reference's pow.
-        T hu73 = hu * hu * (std::is_same<TZ, float>::value ? std::cbrt(hu) : std::pow(hu, expo));
-        T qn = (qsm + frc * (T)dtt) / ((T)1 + gnavg2 * (T)dtt * qfr / hu73);
+        // hu**0.333333343 for 1e-3 <= hu <= 1e3) and multiplies the flux update
+        // through by hu73 (one division); the "f32" (core precision)
+        // instantiation does the same, "ref" and "fp64" keep the reference's form.
+        T hu73, qn;
+        if (h73table) {
+          hu73 = power7over3(std::max(hu, (T)1.0e-6f));
+          qn = CORE ? (std::fma(frc, (T)dtt, qsm) * hu73) / std::fma(gnavg2 * (T)dtt, qfr, hu73)
+                    : (qsm + frc * (T)dtt) / ((T)1 + gnavg2 * (T)dtt * qfr / hu73);
+        } else if (CORE) {
+          hu73 = (hu * hu) * cr;
+          qn = (std::fma(frc, (T)dtt, qsm) * hu73) / std::fma(gnavg2 * (T)dtt, qfr, hu73);
+        } else {
+          hu73 = hu * hu * std::pow(hu, expo);
+          qn = (qsm + frc * (T)dtt) / ((T)1 + gnavg2 * (T)dtt * qfr / hu73);
+        }
         if (subgrid && wiggle_suppression) {
           T mdrv = std::fabs(zsderv(nm) - zsderv(nmu)) - (T)wiggle_threshold;
           if (mdrv > (T)0) qn = qn * (T)wiggle_threshold / ((T)wiggle_factor * mdrv + (T)wiggle_threshold);
@@ -2621,7 +2717,7 @@ void oracle_scalars(void* hv, double* out) {
 }
 
 // Copy a named array to a double buffer of length n (cells: np, faces: npuv).
-// Names: zs zsmax z_volume zs0 zsderv zb kcs nm_n nm_m q uv kfuv kcuv uv_nm uv_nmu uv_dir netprcp qext
+// Names: zs zsmax z_volume zs0 zsderv zb z_zmin kcs nm_n nm_m q uv kfuv kcuv uv_nm uv_nmu uv_dir netprcp qext
 int oracle_get(void* hv, const char* name, double* out, long n) {
   auto* h = static_cast<Handle*>(hv);
   std::string s(name);
@@ -2632,6 +2728,7 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "zs0" && m.zs0.allocated()) copy_out(m.zs0, out, n);
     else if (s == "zsderv" && m.zsderv.allocated()) copy_out(m.zsderv, out, n);
     else if (s == "zb" && m.zb.allocated()) copy_out(m.zb, out, n);
+    else if (s == "z_zmin" && m.sg_z_zmin.allocated()) copy_out(m.sg_z_zmin, out, n);
     else if (s == "kcs") copy_out(m.kcs, out, n);
     else if (s == "nm_n") copy_out(m.z_index_z_n, out, n);
     else if (s == "nm_m") copy_out(m.z_index_z_m, out, n);

@@ -140,11 +140,17 @@ double* g_scratch_ptr[kMaxDevices] = {};  // device address of g_volume_scratch,
 
 // The first call on a device looks the array's address up with
 // cudaGetSymbolAddress (with that device current); later calls reuse it.  Make
-// the first call for each device before any stream capture begins.
-int volume_scratch(double** out, const char** why) {
-  int dev = -1;
+// the first call for each device before any stream capture begins.  The
+// model's stream must belong to the current device: the address is only valid
+// there.
+int volume_scratch(cudaStream_t s, double** out, const char** why) {
+  int dev = -1, sdev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     *why = "no usable current CUDA device for the volume scratch array";
+    return 1;
+  }
+  if (cudaStreamGetDevice(s, &sdev) != cudaSuccess || sdev != dev) {
+    *why = "the model's stream is not on the current CUDA device; make the model's device current first";
     return 1;
   }
   std::lock_guard<std::mutex> lock(g_scratch_mu);
@@ -177,11 +183,20 @@ int volume_noalloc(const ScnDev* d_scn, const int32_t* cmp, long long n, cudaStr
     return 1;
   }
   double* scratch = nullptr;
-  if (volume_scratch(&scratch, why)) return 1;
+  if (volume_scratch(s, &scratch, why)) return 1;
+  // an error left by an earlier, unrelated call is reported as such, not as a launch failure here
+  if (cudaPeekAtLastError() != cudaSuccess) {
+    *why = "an earlier CUDA error is still pending on this thread";
+    return 1;
+  }
   k_volume_partial<<<g, 256, 0, s>>>(d_scn, cmp, n, scratch);
+  if (cudaGetLastError() != cudaSuccess) {
+    *why = "volume partial-sum kernel launch failed";
+    return 1;
+  }
   k_volume_final<<<1, 32, 0, s>>>(scratch, g, scratch + kNoAllocMaxParts);
   if (cudaGetLastError() != cudaSuccess) {
-    *why = "volume kernel launch failed";
+    *why = "volume final-sum kernel launch failed";
     return 1;
   }
   if (cudaMemcpyAsync(host_out, scratch + kNoAllocMaxParts, sizeof(double), cudaMemcpyDeviceToHost, s) !=

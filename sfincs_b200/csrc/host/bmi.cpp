@@ -57,7 +57,7 @@ std::string restart_time_string(double t_sec, const std::string& tref) {
   const int hh = (int)(secs_time / 3600.0f);
   const int mn = (int)((secs_time - (float)(hh * 3600)) / 60.0f);
   const int ss = (int)(secs_time - (float)(hh * 3600) - (float)(mn * 60));
-  char buf[32];
+  char buf[96];
   std::snprintf(buf, sizeof buf, "%04lld%02lld%02lld.%02d%02d%02d", y, m, d, hh, mn, ss);
   return buf;
 }

@@ -21,6 +21,23 @@ void check_cuda(cudaError_t e, const char* what) {
 
 static bool is_none(const std::string& s) { return s.size() >= 4 && s.compare(0, 4, "none") == 0; }
 
+// The hu**(7/3) lookup table of h73table (fill_h73_tables, sfincs_data.f90:
+// 858-881): x73(j, k) = hh**2 * hh**(1.0/3.0) at hh = 0.001 j 10**(k - 6),
+// j = 1..1000, k = 1..10, in real*4 (10.0**(k - 6) for k < 6 as the reciprocal
+// of the exact power), stored at (k - 1) * 1000 + j - 1.
+static void fill_h73_table(std::vector<float>& x73) {
+  x73.assign(10000, 0.0f);
+  for (int k = 1; k <= 10; k++) {
+    float p10 = 1.0f;
+    for (int i = 0; i < std::abs(k - 6); i++) p10 = p10 * 10.0f;
+    if (k < 6) p10 = 1.0f / p10;
+    for (int j = 1; j <= 1000; j++) {
+      const float hh = 0.001f * (float)j * p10;
+      x73[(size_t)(k - 1) * 1000 + (j - 1)] = hh * hh * std::pow(hh, 1.0f / 3.0f);
+    }
+  }
+}
+
 // ============================================================================
 // load_model
 // ============================================================================
@@ -162,7 +179,8 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   const bool friction2d = in.logical("friction2d", true);
   const bool advection_mask = in.logical("advection_mask", true);
   P.nuviscfac = in.real("nuviscfac", 100.0f);
-  if (in.logical("h73table", false)) throw std::runtime_error("h73table is not supported by this core");
+  P.h73table = in.logical("h73table", false) ? 1 : 0;
+  if (P.h73table) fill_h73_table(h.x73);
   const std::string qtrfile = in.str("qtrfile", "none"), depfile = in.str("depfile", "none"),
                     inifile = in.str("inifile", "none"), rstfile = in.str("rstfile", "none"),
                     mskfile = in.str("mskfile", "none"), indexfile = in.str("indexfile", "none"),
@@ -206,6 +224,8 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
     h.tref = tref;
     h.dtrstout = dtrstout;
     h.trstout = dtrstout > 1.0e-6f ? (double)(t0out + dtrstout) : (trst > 1.0e-6f ? (double)trst : 1.0e9);
+    if (quadtree && h.trstout < 1.0e9)
+      throw std::runtime_error("restart output (dtrstout / trstout) is not supported on quadtree grids by this core");
   }
   tspinup = t0 + tspinup;
   P.g = 9.81f;
@@ -1272,6 +1292,7 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.wmag, h.wmag);
   up(d.wdir, h.wdir);
   up(d.cdval, h.cdval);
+  up(d.x73, h.x73);
   up(d.tsrc, h.tsrc);
   up(d.qsrc, h.qsrc);
   zero(d.qtsrc, (size_t)std::max(h.p.nsrc + 2 * h.p.ndrn, 1));

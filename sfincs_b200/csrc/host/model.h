@@ -49,6 +49,7 @@ struct HostModel {
   // forcing series
   std::vector<float> t_bnd, zs_bnd;  // zs_bnd [ntbnd][nbnd]
   std::vector<float> tprcp, vprcp, twnd, wmag, wdir, cdval;
+  std::vector<float> x73;            // hu**(7/3) table when h73table is on (sfincs_data.f90:858-881)
   std::vector<float> tsrc, qsrc;     // qsrc [ntsrc][nsrc]
   std::vector<int32_t> src_cell;
   std::vector<StrucFace> struc;       // weir faces

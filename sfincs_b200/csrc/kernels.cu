@@ -265,8 +265,8 @@ __device__ __forceinline__ void update_drainage(const ScnDev& S, const StepPlan&
       }
       S.drn_frac[idrn] = frac;
       S.drn_status[idrn] = status;
-      // Bates et al. (2010) inertial flux; hgate**(7.0/3.0) as hgate**2 * cbrt(hgate)
-      const float h73 = hgate * hgate * cbrtf(hgate);
+      // Bates et al. (2010) inertial flux; hgate**(7.0/3.0) as hgate**2 * cube_root(hgate)
+      const float h73 = hgate * hgate * cube_root(hgate);
       qq = (qq0 - S.g * hgate * dzds * dt) / (1.0f + S.g * (mng * mng) * dt * fabsf(qq0) / h73);
       qq = qq * wdt * frac;
     }
@@ -593,15 +593,13 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepVals& 
     if (zsu > zmax) {  // sfincs_momentum.f90:347-366
       const float4 w = (DIR == 0 ? S.sgw_u : S.sgw_v)[c];
       hu = w.x + zsu;
-      gnavg2 = w.z - (w.z - w.y) / (w.w * (zsu - zmax) + 1.0f);
+      gnavg2 = sg_gnavg2_full(w.z, w.y, w.w, zsu - zmax);
     } else {  // sfincs_momentum.f90:372-378
-      const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
-      const int iuv = lev_index((zsu - zmin) / dzuv, S.nlev);
-      const float facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
-      const UvRec r = (DIR == 0 ? S.rec_u : S.rec_v)[(int64_t)(iuv - 1) * S.nalloc + c];
-      hu = r.havg + r.dhavg * facint;
-      gnavg2 = r.nrep + r.dnrep * facint;
-      phi = r.pwet + r.dpwet * facint;
+      const SgLevel lv = sg_level(zsu, zmin, zmax, S.nlev);
+      const UvRec r = (DIR == 0 ? S.rec_u : S.rec_v)[(int64_t)(lv.iuv - 1) * S.nalloc + c];
+      hu = fmaf(r.dhavg, lv.facint, r.havg);
+      gnavg2 = fmaf(r.dnrep, lv.facint, r.nrep);
+      phi = fmaf(r.dpwet, lv.facint, r.pwet);
     }
   } else {  // sfincs_momentum.f90:384-385
     dry_nm = zs_nm < S.zb[c];

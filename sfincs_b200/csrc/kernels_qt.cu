@@ -99,15 +99,13 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
           if (zsu > zmax) {
             const float4 w = S.sgw_u[i];
             hu = w.x + zsu;
-            gnavg2 = w.z - (w.z - w.y) / (w.w * (zsu - zmax) + 1.0f);
+            gnavg2 = sg_gnavg2_full(w.z, w.y, w.w, zsu - zmax);
           } else {
-            const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
-            const int iuv = lev_index((zsu - zmin) / dzuv, S.nlev);
-            const float facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
-            const UvRec r = S.rec_u[(int64_t)(iuv - 1) * S.nalloc + i];
-            hu = r.havg + r.dhavg * facint;
-            gnavg2 = r.nrep + r.dnrep * facint;
-            phi = r.pwet + r.dpwet * facint;
+            const SgLevel lv = sg_level(zsu, zmin, zmax, S.nlev);
+            const UvRec r = S.rec_u[(int64_t)(lv.iuv - 1) * S.nalloc + i];
+            hu = fmaf(r.dhavg, lv.facint, r.havg);
+            gnavg2 = fmaf(r.dnrep, lv.facint, r.nrep);
+            phi = fmaf(r.dpwet, lv.facint, r.pwet);
           }
           dry0 = S.vneg[f.nm] != 0;
           dry1 = S.vneg[f.nmu] != 0;

@@ -313,11 +313,10 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
             int code = kRecFull;
             const UvRec* r = nullptr;
             if (!L.full) {
-              const float dzuv = (zmax - zmin) / (float)(S.nlev - 1);
-              const int iuv = lev_index((zsu - zmin) / dzuv, S.nlev);
-              L.facint = (zsu - (zmin + (float)(iuv - 1) * dzuv)) / dzuv;
-              r = R + (int64_t)(iuv - 1) * S.nalloc + c;
-              code = iuv;
+              const SgLevel lv = sg_level(zsu, zmin, zmax, S.nlev);
+              L.facint = lv.facint;
+              r = R + (int64_t)(lv.iuv - 1) * S.nalloc + c;
+              code = lv.iuv;
             }
             if (code == (int)(sm + o_rl)[kc]) {
               L.v = make_float4(a.x, a.y, b.x, b.y);
@@ -371,11 +370,11 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               }
               if (lu.full) {
                 hu = lu.v.x + zsu_u;
-                gnavg2 = lu.v.z - (lu.v.z - lu.v.y) / (lu.v.w * (zsu_u - zmax_u) + 1.0f);
+                gnavg2 = sg_gnavg2_full(lu.v.z, lu.v.y, lu.v.w, zsu_u - zmax_u);
               } else {
-                hu = lu.v.x + lu.v.y * lu.facint;
-                gnavg2 = lu.v.z + lu.v.w * lu.facint;
-                phi = lu.v2.x + lu.v2.y * lu.facint;
+                hu = fmaf(lu.v.y, lu.facint, lu.v.x);
+                gnavg2 = fmaf(lu.v.w, lu.facint, lu.v.z);
+                phi = fmaf(lu.v2.y, lu.facint, lu.v2.x);
               }
             } else {
               const float* zb = (const float*)(sm + mom::O_ZB);
@@ -428,11 +427,11 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               }
               if (lv.full) {
                 hu = lv.v.x + zsu_v;
-                gnavg2 = lv.v.z - (lv.v.z - lv.v.y) / (lv.v.w * (zsu_v - zmax_v) + 1.0f);
+                gnavg2 = sg_gnavg2_full(lv.v.z, lv.v.y, lv.v.w, zsu_v - zmax_v);
               } else {
-                hu = lv.v.x + lv.v.y * lv.facint;
-                gnavg2 = lv.v.z + lv.v.w * lv.facint;
-                phi = lv.v2.x + lv.v2.y * lv.facint;
+                hu = fmaf(lv.v.y, lv.facint, lv.v.x);
+                gnavg2 = fmaf(lv.v.w, lv.facint, lv.v.z);
+                phi = fmaf(lv.v2.y, lv.facint, lv.v2.x);
               }
             } else {
               const float* zb = (const float*)(sm + mom::O_ZB);

@@ -229,6 +229,8 @@ struct ScnDev {
   float* drn_frac;       // [ndrn] gates: fraction open
   float structure_relax; // seconds
   float pi;
+  int h73table;          // hu**(7/3) from the lookup table (sfincs_momentum.f90:663-675)
+  const float* x73;      // [10][1000] the table x73(j, k) at (k - 1) * 1000 + j - 1 (sfincs_data.f90:858-881)
   StepState* st;
   // ---- quadtree (quadtree != 0; the regular-grid fields above that index
   // cells or faces then hold compact arrays: zs.. over npc cells, qu/qv and

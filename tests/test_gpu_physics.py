@@ -5,7 +5,8 @@ case turns on terms that those leave off: Coriolis, wind stress from a time
 series, theta smoothing, the "original" advection scheme, the slope limiter,
 friction2d off, viscosity and no wiggle suppression on a subgrid model, c2d
 infiltration, point sources, Neumann and outflow boundary cells, thin dams,
-weirs and the five drainage structure types (regular and subgrid). For each
+weirs, the five drainage structure types and the hu**(7/3) lookup table
+(regular and subgrid). For each
 case the CUDA core is compared with the oracle in the core's own precision
 after 1, 2, 4, 10, 40 and 100 steps, on the default kernel path and on the
 per-thread-load path. The bars are those of the main stepwise test: time
@@ -130,7 +131,15 @@ def case_subgrid_drainage(tmp_path):
     return m
 
 
-CASES = {f.__name__[5:]: f for f in (case_coriolis_wind_theta, case_original_advection_slopelim_nofric2d,
+def case_h73table(tmp_path):
+    return _plain(tmp_path, advection=1, h73table=1)
+
+
+def case_subgrid_h73table(tmp_path):
+    return _subgrid(tmp_path, advection=1, h73table=1)
+
+
+CASES = {f.__name__[5:]: f for f in (case_h73table, case_subgrid_h73table, case_coriolis_wind_theta, case_original_advection_slopelim_nofric2d,
                                       case_boundary_kinds, case_plain_infiltration, case_subgrid_visc_nowiggle,
                                       case_subgrid_infiltration_sources, case_thin_dams_theta,
                                       case_subgrid_thin_dams, case_weirs, case_subgrid_weirs, case_drainage,

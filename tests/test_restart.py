@@ -162,3 +162,18 @@ def test_gpu_writes_restart_files_at_output_times(tmp_path):
         checked += 1
     assert checked == 3  # 600, 1200 and 1800 s
     g.close()
+
+
+def test_quadtree_restart_output_is_refused(tmp_path):
+    """Restart files on quadtree meshes are not built: asking for restart
+    output there is an error at load, not a file with the fluxes missing."""
+    from sfincs_b200 import bmi as B
+    from sfincs_b200 import qtsynth
+
+    m = qtsynth.quadtree_coastal(nmax1=6, mmax1=8, dx1=400.0, nlev=2, bands=(600.0,), P=2, seed=4, tstop=600.0,
+                                 subgrid=False)
+    d = m.write(str(tmp_path))
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        f.write(f"{'dtrstout':<20} = 300\n")
+    with pytest.raises(RuntimeError, match="restart output"):
+        B.layout(d, "counts", 10)
