@@ -83,6 +83,36 @@ static float core_cube_root(float x) {
   return x + x;
 }
 
+// Exponential of the core-precision instantiation (Horton infiltration),
+// restating the CUDA core's method with the same IEEE operations: n =
+// rint(x log2 e), r = x - n ln2 with ln2 split in two parts (Cody and Waite),
+// e^r by its Taylor polynomial to degree 7 in Horner form with fused
+// multiply-adds, times 2^n in two factors.
+static float core_exp(float x) {
+  if (x != x) return x;
+  if (x > 88.8f) return INFINITY;
+  if (x < -104.0f) return 0.0f;
+  const float n = std::nearbyint(x * 1.44269502f);
+  float r = std::fma(-n, 0.693145752f, x);
+  r = std::fma(-n, 1.42860677e-06f, r);
+  float p = 1.98412701e-04f;  // 1/5040
+  p = std::fma(p, r, 1.38888892e-03f);  // 1/720
+  p = std::fma(p, r, 8.33333377e-03f);  // 1/120
+  p = std::fma(p, r, 4.16666679e-02f);  // 1/24
+  p = std::fma(p, r, 1.66666672e-01f);  // 1/6
+  p = std::fma(p, r, 0.5f);
+  p = std::fma(p, r, 1.0f);
+  p = std::fma(p, r, 1.0f);
+  const int ni = (int)n, n1 = ni / 2, n2 = ni - n1;
+  auto pow2 = [](int e) {
+    uint32_t b = (uint32_t)(e + 127) << 23;
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+  };
+  return (p * pow2(n1)) * pow2(n2);
+}
+
 template <class X>
 struct F2 {  // (n1, n2) column-major, 1-based
   std::vector<X> v;
@@ -258,12 +288,24 @@ struct Model {
   F1<int32_t> nmindbnd, index_kcuv2, nmbkcuv2, nmikcuv2, ibkcuv2, ind1_bnd_gbp, ind2_bnd_gbp, nmi_gbp;
   F1<int8_t> ibuvdir;
   F1<float> zsb, zsb0, uvmean, fac_bnd_gbp, x_bnd, y_bnd, t_bnd, zst_bnd;
+  // downstream river boundaries (sfincs_boundaries.f90:217-270, 596-613, 878-902)
+  long nbdr = 0;
+  F1<float> x_bdr, y_bdr, dzs_bdr;
+  F1<int32_t> index_zsi_bdr, index_bdr_gbp;
+  std::string bdrfile;
   F2<float> zs_bnd;
 
   // --- meteo, infiltration, sources
   long ntwnd = 0, itwndlast = 1, ntprcp = 0, itprcplast = 1;
   F1<float> twnd, wndmag, wnddir, tprcpt, tprcpv, cdval;
   F1<float> tauwu, tauwv, prcp, netprcp, qext, qinffield, qinfmap, cumprcp, cuminf;
+  // infiltration models with state (sfincs_infiltration.f90:8-600): curve number
+  // with recovery (scs_*), Green-Ampt (GA_*), Horton (horton_*), recovery clock
+  F1<float> scs_Se, scs_P1, scs_F1, scs_S1, ksfield, inf_kr, rain_T1, GA_head, GA_sigma, GA_sigma_max, GA_F, GA_Lu,
+      horton_fc, horton_f0, horton_kd;
+  F1<int> scs_rain;
+  float sfacinf = 0.2f, horton_kr_kd = 10.0f;
+  std::string smaxfile, sigmafile, ksfile, fcfile, kdfile;
   long nsrc = 0, ntsrc = 0, itsrclast = 1, ndrn = 0, nsrcdrn = 0;
   float structure_relax = 10.0f;
   F1<int8_t> drainage_type, drainage_status;
@@ -357,6 +399,7 @@ struct Model {
     sbgfile = in.str("sbgfile", "none");
     manningfile = in.str("manningfile", "none");
     bndfile = in.str("bndfile", "none");
+    bdrfile = in.str("bdrfile", "none");
     bzsfile = in.str("bzsfile", "none");
     bcafile = in.str("bcafile", "none");
     bzifile = in.str("bzifile", "none");
@@ -374,6 +417,14 @@ struct Model {
     sefffile = in.str("sefffile", "none");
     psifile = in.str("psifile", "none");
     f0file = in.str("f0file", "none");
+    smaxfile = in.str("smaxfile", "none");
+    sigmafile = in.str("sigmafile", "none");
+    ksfile = in.str("ksfile", "none");
+    fcfile = in.str("fcfile", "none");
+    kdfile = in.str("kdfile", "none");
+    sfacinf = in.real("sfacinf", 0.2f);
+    horton_kr_kd = in.real("horton_kr_kd", 10.0f);
+    store_cumulative_precipitation = in.integer("storecumprcp", 0) == 1;
     infiltrationfile = in.str("infiltration_file", "none");
     inftype = in.str("infiltration_type", "none");
     storevelmax = in.integer("storevelmax", 0);
@@ -1178,14 +1229,74 @@ struct Model {
     } else if (qinffile.substr(0, 4) != "none") {
       inftype = "c2d";
       infiltration = true;
-    } else if (scsfile != "none" || sefffile != "none" || psifile != "none" || f0file != "none" ||
-               infiltrationfile != "none") {
-      throw std::runtime_error("oracle: only con/c2d infiltration types are restated");
+    } else if (infiltrationfile != "none") {
+      throw std::runtime_error("oracle: netCDF infiltration files are not restated");
+    } else if (scsfile != "none") {
+      inftype = "cna";
+      infiltration = true;
+      store_cumulative_precipitation = true;
+    } else if (sefffile != "none") {
+      inftype = "cnb";
+      infiltration = true;
+      store_cumulative_precipitation = true;
+    } else if (psifile != "none") {
+      inftype = "gai";
+      infiltration = true;
+    } else if (f0file != "none") {
+      inftype = "hor";
+      infiltration = true;
     }
     cumprcp.alloc(np);
     cuminf.alloc(np);
     if (!infiltration) return;
     qinffield.alloc(np);
+    qinfmap.alloc(np);
+    auto rd = [&](const std::string& f) { return read_stream<float>(path(f), (size_t)np); };
+    if (inftype == "cna") {  // :249-279, S from inches to m
+      auto r = rd(scsfile);
+      for (long nm = 1; nm <= np; nm++) qinffield(nm) = r[nm - 1] * 0.0254f;
+      return;
+    }
+    if (inftype == "cnb") {  // :280-360
+      auto smax = rd(smaxfile), se = rd(sefffile), ks = rd(ksfile);
+      scs_Se.alloc(np); ksfield.alloc(np); inf_kr.alloc(np);
+      scs_P1.alloc(np); scs_F1.alloc(np); rain_T1.alloc(np); scs_S1.alloc(np); scs_rain.alloc(np);
+      for (long nm = 1; nm <= np; nm++) {
+        qinffield(nm) = smax[nm - 1];
+        scs_Se(nm) = se[nm - 1];
+        ksfield(nm) = ks[nm - 1];
+        inf_kr(nm) = std::sqrt(ksfield(nm) / 25.4f) / 75.0f;  // Equation 4-36 (ks in mm/h)
+      }
+      return;
+    }
+    if (inftype == "gai") {  // :361-505
+      auto psi = rd(psifile), sig = rd(sigmafile), ks = rd(ksfile);
+      GA_head.alloc(np); GA_sigma_max.alloc(np); ksfield.alloc(np); inf_kr.alloc(np); rain_T1.alloc(np);
+      GA_sigma.alloc(np); GA_F.alloc(np); GA_Lu.alloc(np);
+      for (long nm = 1; nm <= np; nm++) {
+        GA_head(nm) = psi[nm - 1];
+        GA_sigma_max(nm) = sig[nm - 1];
+        ksfield(nm) = ks[nm - 1];
+        inf_kr(nm) = std::sqrt(ksfield(nm) / 25.4f) / 75.0f;
+        GA_sigma(nm) = GA_sigma_max(nm);
+        GA_Lu(nm) = 4.0f * std::sqrt(25.4f) * std::sqrt(ksfield(nm));  // Equation 4-33
+        GA_head(nm) = GA_head(nm) / 1000.0f;
+        GA_Lu(nm) = GA_Lu(nm) / 1000.0f;
+        ksfield(nm) = ksfield(nm) / 1000.0f / 3600.0f;
+      }
+      return;
+    }
+    if (inftype == "hor") {  // :506-590
+      auto fc = rd(fcfile), f0 = rd(f0file), kd = rd(kdfile);
+      horton_fc.alloc(np); horton_f0.alloc(np); horton_kd.alloc(np); rain_T1.alloc(np);
+      for (long nm = 1; nm <= np; nm++) {
+        horton_fc(nm) = fc[nm - 1];
+        horton_f0(nm) = f0[nm - 1];
+        horton_kd(nm) = kd[nm - 1];
+        qinffield(nm) = horton_f0(nm) / 3600.0f / 1000.0f;
+      }
+      return;
+    }
     if (inftype == "con") {
       for (long nm = 1; nm <= np; nm++) {
         float zz = subgrid ? sg_z_zmin(nm) : zb(nm);
@@ -1195,7 +1306,6 @@ struct Model {
       auto r = read_stream<float>(path(qinffile), (size_t)np);
       for (long nm = 1; nm <= np; nm++) qinffield(nm) = r[nm - 1] / 3600.0f / 1000.0f;
     }
-    qinfmap.alloc(np);
   }
 
   // initialize_hydro + set_initial_conditions + compute_initial_subgrid_volumes:
@@ -1216,9 +1326,14 @@ struct Model {
     if (store_maximum_flux) qmax.alloc(np);
     if (store_twet) twet.alloc(np);
     if (store_t_zsmax) t_zsmax.alloc(np);
-    if (zsinifile.substr(0, 4) != "none") throw std::runtime_error("oracle: ini files are not part of this path");
     // set_initial_conditions / read_binary_restart_file: sfincs_initial_conditions.F90:14-268
     std::vector<float> inizs4, iniq;
+    if (rstfile.substr(0, 4) == "none" && zsinifile.substr(0, 4) != "none") {
+      // read_zsini_file (:270-288): np real*4 levels in cell order, widened to real*8
+      if (zsinifile.size() >= 2 && zsinifile.substr(zsinifile.size() - 2) == "nc")
+        throw std::runtime_error("oracle: netCDF ini files are not restated");
+      inizs4 = read_stream<float>(path(zsinifile), (size_t)np);
+    }
     if (rstfile.substr(0, 4) != "none") {
       std::ifstream fin(path(rstfile), std::ios::binary);
       if (!fin) throw std::runtime_error("oracle: cannot open " + rstfile);
@@ -1399,16 +1514,40 @@ struct Model {
       t_bnd(1) = t0;
       t_bnd(2) = t1;
     }
-    if (downstream_river_boundaries_in_mask)
-      throw std::runtime_error("oracle: downstream river boundaries are not restated");
+    // downstream river points: x, y, internal x, y, slope, distance per line (:217-270)
+    nbdr = 0;
+    if (downstream_river_boundaries_in_mask) {
+      if (bdrfile.substr(0, 4) == "none")
+        throw std::runtime_error("oracle: downstream river points in the mask without a bdrfile");
+      auto rows = read_ascii_table(path(bdrfile));
+      nbdr = (long)rows.size();
+      x_bdr.alloc(nbdr);
+      y_bdr.alloc(nbdr);
+      index_zsi_bdr.alloc(nbdr);
+      dzs_bdr.alloc(nbdr);
+      for (long i = 1; i <= nbdr; i++) {
+        const auto& r = rows[i - 1];
+        x_bdr(i) = (float)r.at(0);
+        y_bdr(i) = (float)r.at(1);
+        float xin = (float)r.at(2), yin = (float)r.at(3), slope = (float)r.at(4), dist = (float)r.at(5);
+        long nmq = find_quadtree_cell(xin, yin);
+        index_zsi_bdr(i) = nmq > 0 ? index_sfincs_in_quadtree(nmq) : 0;
+        if (index_zsi_bdr(i) == 0) throw std::runtime_error("oracle: river point outside the active mesh");
+        if (dist < 0.0f)
+          dzs_bdr(i) = -slope * std::sqrt((xin - x_bdr(i)) * (xin - x_bdr(i)) + (yin - y_bdr(i)) * (yin - y_bdr(i)));
+        else
+          dzs_bdr(i) = -slope * dist;
+      }
+    }
   }
 
   void find_boundary_indices() {
     if (ngbnd == 0) return;
-    if (nbnd == 0) return;
+    if (nbnd == 0 && nbdr == 0) return;
     ind1_bnd_gbp.alloc(ngbnd);
     ind2_bnd_gbp.alloc(ngbnd);
     fac_bnd_gbp.alloc(ngbnd);
+    if (downstream_river_boundaries_in_mask) index_bdr_gbp.alloc(ngbnd);
     if (neumann_boundaries_in_mask) nmi_gbp.alloc(ngbnd);
     for (long ib = 1; ib <= ngbnd; ib++) {
       long nm = nmindbnd(ib);
@@ -1438,6 +1577,18 @@ struct Model {
           ind2_bnd_gbp(ib) = 1;
           fac_bnd_gbp(ib) = 1.0f;
         }
+      } else if (kcs(nm) == 5) {  // nearest point of the bdr file (:596-613)
+        float dst1 = 1.0e10f;
+        long ib1 = 0;
+        for (long ibdr = 1; ibdr <= nbdr; ibdr++) {
+          float ddx = x_bdr(ibdr) - x, ddy = y_bdr(ibdr) - y;
+          float dst = std::sqrt(ddx * ddx + ddy * ddy);
+          if (dst < dst1) {
+            dst1 = dst;
+            ib1 = ibdr;
+          }
+        }
+        index_bdr_gbp(ib) = (int32_t)ib1;
       } else if (kcs(nm) == 6) {
         // regular grid: find_sfincs_cell(n, m+-1 / n+-1, iref) through the quadtree search arrays
         long n = z_index_z_n(nm), m = z_index_z_m(nm);
@@ -2001,14 +2152,106 @@ struct Model {
     }
   }
 
-  // update_infiltration_map (con/c2d): sfincs_infiltration.f90:609-676
+  // update_infiltration_map: sfincs_infiltration.f90:609-1039
   void update_infiltration_map(float dtt) {
+    constexpr bool CORE = std::is_same<TZ, float>::value;
+    // gai reads GA_head(np) * GA_sigma(np) for every cell (:858); in the
+    // reference's serial order every cell sees the last cell's value from
+    // before this update
+    const float ga_hs = inftype == "gai" ? GA_head(np) * GA_sigma(np) : 0.0f;
     for (long nm = 1; nm <= np; nm++) {
-      qinfmap(nm) = qinffield(nm);
-      if (subgrid) {
-        if (z_volume(nm) <= 0.0) qinfmap(nm) = 0.0f;
-      } else {
-        if (zs(nm) <= zb(nm)) qinfmap(nm) = 0.0f;
+      if (inftype == "con" || inftype == "c2d") {  // :632-676
+        qinfmap(nm) = qinffield(nm);
+        if (subgrid) {
+          if (z_volume(nm) <= 0.0) qinfmap(nm) = 0.0f;
+        } else {
+          if (zs(nm) <= zb(nm)) qinfmap(nm) = 0.0f;
+        }
+      } else if (inftype == "cna") {  // :678-723
+        if (cumprcp(nm) > sfacinf * qinffield(nm)) {
+          float a = cumprcp(nm) - sfacinf * qinffield(nm);
+          float Qq = a * a / (cumprcp(nm) + (1.0f - sfacinf) * qinffield(nm));
+          float I = cumprcp(nm) - Qq;
+          qinfmap(nm) = (I - cuminf(nm)) / dtt;
+        } else {
+          qinfmap(nm) = prcp(nm);
+        }
+      } else if (inftype == "cnb") {  // :724-829
+        if (prcp(nm) > 0.0f) {
+          if (scs_rain(nm) != 1) {
+            scs_P1(nm) = 0.0f;
+            scs_F1(nm) = 0.0f;
+            scs_S1(nm) = scs_Se(nm);
+            scs_rain(nm) = 1;
+          }
+          scs_P1(nm) = scs_P1(nm) + prcp(nm) * dtt;
+          if (scs_P1(nm) > sfacinf * scs_S1(nm)) {
+            float a = scs_P1(nm) - sfacinf * scs_S1(nm);
+            float Qq = a * a / (scs_P1(nm) + (1.0f - sfacinf) * scs_S1(nm));
+            float I = scs_P1(nm) - Qq;
+            qinfmap(nm) = (I - scs_F1(nm)) / dtt;
+            scs_F1(nm) = I;
+          } else {
+            scs_F1(nm) = scs_P1(nm);
+            qinfmap(nm) = prcp(nm);
+          }
+          scs_Se(nm) = std::max(scs_Se(nm) - qinfmap(nm) * dtt, 0.0f);
+          qinfmap(nm) = std::max(qinfmap(nm), 0.0f);
+        } else {
+          if (scs_rain(nm) == 1) {
+            scs_rain(nm) = 0;
+            qinfmap(nm) = 0.0f;
+            rain_T1(nm) = 0.0f;
+          }
+          rain_T1(nm) = rain_T1(nm) + dtt / 3600.0f;
+          if (rain_T1(nm) > 0.06f / inf_kr(nm)) {
+            scs_Se(nm) = scs_Se(nm) + inf_kr(nm) * qinffield(nm) * dtt / 3600.0f;
+            scs_Se(nm) = std::min(scs_Se(nm), qinffield(nm));
+          }
+        }
+      } else if (inftype == "gai") {  // :830-912; qinfmap keeps its last value while it does not rain
+        if (prcp(nm) > 0.0f) {
+          if (prcp(nm) < ksfield(nm)) {
+            qinfmap(nm) = prcp(nm);
+          } else {
+            qinfmap(nm) = ksfield(nm) * (1.0f + ga_hs / GA_F(nm));
+            qinfmap(nm) = std::fmax(std::fmin(qinfmap(nm), prcp(nm)), 0.0f);
+          }
+          GA_sigma(nm) = std::max(GA_sigma(nm) - qinfmap(nm) * dtt / GA_Lu(nm), 0.0f);
+          GA_F(nm) = GA_F(nm) + qinfmap(nm) * dtt;
+          rain_T1(nm) = 0.0f;
+        } else {
+          rain_T1(nm) = rain_T1(nm) + dtt / 3600.0f;
+          if (rain_T1(nm) > 0.06f / inf_kr(nm)) {
+            GA_sigma(nm) = GA_sigma(nm) + inf_kr(nm) * GA_sigma_max(nm) * dtt / 3600.0f;
+            GA_sigma(nm) = std::min(GA_sigma(nm), GA_sigma_max(nm));
+            GA_F(nm) = std::max(GA_F(nm) - inf_kr(nm) * GA_sigma_max(nm) * dtt / 3600.0f * GA_Lu(nm), 0.0f);
+          }
+        }
+      } else if (inftype == "hor") {  // :914-1033
+        float hh_local = subgrid ? (float)(z_volume(nm) / (double)cell_area(z_flags_iref(nm)))
+                                 : (float)((double)zs(nm) - (double)zb(nm));
+        if (hh_local > 0.0f || prcp(nm) > 0.0f) {
+          if (rain_T1(nm) > 0.0f)
+            rain_T1(nm) = 0.0f;
+          else
+            rain_T1(nm) = rain_T1(nm) - dtt;
+          float x = horton_kd(nm) * rain_T1(nm) / 3600.0f;
+          float I = CORE ? core_exp(x) : std::exp(x);
+          if (I < 0.01f) {
+            I = 0.0f;
+            rain_T1(nm) = rain_T1(nm) + dtt;
+            qinfmap(nm) = horton_fc(nm) / 3600.0f / 1000.0f;
+          } else {
+            qinfmap(nm) = (horton_fc(nm) + (horton_f0(nm) - horton_fc(nm)) * I) / 3600.0f / 1000.0f;
+          }
+          float Qq = hh_local > 0.0f ? prcp(nm) * dtt + hh_local : prcp(nm) * dtt;
+          I = qinfmap(nm) * dtt;
+          if (I > Qq) qinfmap(nm) = qinfmap(nm) * Qq / I;
+        } else {
+          rain_T1(nm) = rain_T1(nm) + dtt / horton_kr_kd;
+          qinfmap(nm) = 0.0f;
+        }
       }
       netprcp(nm) = netprcp(nm) - qinfmap(nm);
       if (store_cumulative_precipitation) cuminf(nm) = cuminf(nm) + qinfmap(nm) * dtt;
@@ -2073,6 +2316,12 @@ struct Model {
           zsb0(ib) = std::max(zsb0(ib), zb(nmb));
           zsb(ib) = std::max(zsb(ib), zb(nmb));
         }
+      } else if (kcs(nmb) == 5) {  // downstream river point (:878-902)
+        long ibdr = index_bdr_gbp(ib);
+        double zst = (double)zs(index_zsi_bdr(ibdr)) + (double)dzs_bdr(ibdr);
+        zst = std::max(zst, subgrid ? (double)sg_z_zmin(nmb) : (double)zb(nmb));
+        zsb(ib) = (float)zst;
+        zsb0(ib) = (float)zst;
       } else if (kcs(nmb) == 6) {
         zs(nmb) = zs(nmi_gbp(ib));
       }
@@ -2717,13 +2966,17 @@ void oracle_scalars(void* hv, double* out) {
 }
 
 // Copy a named array to a double buffer of length n (cells: np, faces: npuv).
-// Names: zs zsmax z_volume zs0 zsderv zb z_zmin kcs nm_n nm_m q uv kfuv kcuv uv_nm uv_nmu uv_dir netprcp qext
+// Names: zs zsmax vmax qmax twet tzsmax z_volume zs0 zsderv zb z_zmin kcs nm_n nm_m q uv kfuv kcuv uv_nm uv_nmu uv_dir netprcp qext
 int oracle_get(void* hv, const char* name, double* out, long n) {
   auto* h = static_cast<Handle*>(hv);
   std::string s(name);
   return dispatch(h, [&](auto& m) -> int {
     if (s == "zs") copy_out(m.zs, out, n);
     else if (s == "zsmax" && m.zsmax.allocated()) copy_out(m.zsmax, out, n);
+    else if (s == "vmax" && m.vmax.allocated()) copy_out(m.vmax, out, n);
+    else if (s == "qmax" && m.qmax.allocated()) copy_out(m.qmax, out, n);
+    else if (s == "twet" && m.twet.allocated()) copy_out(m.twet, out, n);
+    else if (s == "tzsmax" && m.t_zsmax.allocated()) copy_out(m.t_zsmax, out, n);
     else if (s == "z_volume" && m.z_volume.allocated()) copy_out(m.z_volume, out, n);
     else if (s == "zs0" && m.zs0.allocated()) copy_out(m.zs0, out, n);
     else if (s == "zsderv" && m.zsderv.allocated()) copy_out(m.zsderv, out, n);
@@ -2759,6 +3012,9 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "zbuvmx" && m.zbuvmx.allocated()) copy_out(m.zbuvmx, out, n);
     else if (s == "gn2uv" && m.gn2uv.allocated()) copy_out(m.gn2uv, out, n);
     else if (s == "netprcp" && m.netprcp.allocated()) copy_out(m.netprcp, out, n);
+    else if (s == "prcp" && m.prcp.allocated()) copy_out(m.prcp, out, n);
+    else if (s == "cumprcp" && m.cumprcp.allocated()) copy_out(m.cumprcp, out, n);
+    else if (s == "cuminf" && m.cuminf.allocated()) copy_out(m.cuminf, out, n);
     else if (s == "qext" && m.qext.allocated()) copy_out(m.qext, out, n);
     else if (s == "uvmean") copy_out(m.uvmean, out, n);
     else if (s == "nrstructures") out[0] = (double)m.nrstructures;

@@ -110,7 +110,7 @@ def _check(rc: int, what: str):
         raise RuntimeError(f"{what} failed ({rc}): {last_error()}")
 
 
-_F32_NAMES = {"zsmax", "qext", "qx", "qy", "uvx", "uvy", "zs0", "zsderv"}
+_F32_NAMES = {"zsmax", "qext", "qx", "qy", "uvx", "uvy", "zs0", "zsderv", "vmax", "qmax", "twet", "tzsmax", "cumprcp", "cuminf"}
 _F64_NAMES = {"zs", "z_volume"}
 
 

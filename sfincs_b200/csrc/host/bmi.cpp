@@ -264,6 +264,12 @@ struct ModelHandle {
       check_cuda(cudaMemcpyAsync(dst, d_stage, (size_t)n * 8, cudaMemcpyDeviceToHost, s()), "get");
     } else if (name == "zsmax") {
       f32(D.zsmax);
+    } else if (name == "vmax" || name == "qmax" || name == "twet" || name == "tzsmax" || name == "cumprcp" ||
+               name == "cuminf") {
+      const float* a = name == "vmax" ? D.vmax : name == "qmax" ? D.qmax : name == "twet" ? D.twet
+                       : name == "tzsmax" ? D.tzsmax : name == "cumprcp" ? D.cumprcp : D.cuminf;
+      if (!a) throw std::runtime_error("'" + name + "' is not stored by this model (store switch off)");
+      f32(a);
     } else if (name == "qext") {
       if (!D.qext) throw std::runtime_error("qext is not enabled for this model");
       f32(D.qext);
@@ -849,6 +855,10 @@ int sfg_ensemble_get(void* ev, int i, const char* name, void* dst, size_t bytes)
       const float* src = nullptr;
       const int32_t* map = d.d_cmp_off();
       if (nm == "zsmax") src = d.dev().zsmax;
+      else if (nm == "vmax" && d.dev().vmax) src = d.dev().vmax;
+      else if (nm == "qmax" && d.dev().qmax) src = d.dev().qmax;
+      else if (nm == "twet" && d.dev().twet) src = d.dev().twet;
+      else if (nm == "tzsmax" && d.dev().tzsmax) src = d.dev().tzsmax;
       else if (nm == "qx") src = d.dev().qu[p], map = d.face_map(0);
       else if (nm == "qy") src = d.dev().qv[p], map = d.face_map(1);
       else if (nm == "uvx") src = d.dev().uu[p], map = d.face_map(0);

@@ -21,6 +21,64 @@ void check_cuda(cudaError_t e, const char* what) {
 
 static bool is_none(const std::string& s) { return s.size() >= 4 && s.compare(0, 4, "none") == 0; }
 
+void load_infiltration_models(HostModel& h, const Keys& k, size_t nstore, const std::vector<int32_t>& store) {
+  ScnDev& P = h.p;
+  const size_t n = (size_t)h.np;
+  if (P.store_cumprcp && P.precip) {
+    h.cumprcp.assign(nstore, 0.0f);
+    h.cuminf.assign(nstore, 0.0f);
+  }
+  if (P.inftype < 2) return;
+  P.inf_last = store[n - 1];
+  auto rd = [&](const std::string& f, const char* what) {
+    if (is_none(f)) throw std::runtime_error(std::string("infiltration needs the ") + what + " file");
+    return read_binary<float>(h.dir + "/" + f, n);
+  };
+  auto field = [&](std::vector<float>& dst, const std::vector<float>& src) {
+    dst.assign(nstore, 0.0f);
+    for (size_t i = 0; i < n; i++) dst[(size_t)store[i]] = src[i];
+  };
+  auto state = [&](int j, float v) { h.inf_st[j].assign(nstore, v); };
+  if (P.inftype == 2) {  // cna: S in inches -> m (:249-279)
+    auto r = rd(k.scsfile, "scs");
+    for (auto& x : r) x = x * 0.0254f;
+    field(h.inf_par[0], r);
+  } else if (P.inftype == 3) {  // cnb: Smax, Se, recovery from ks in mm/h (:280-360, equation 4-36)
+    auto smax = rd(k.smaxfile, "smax"), se = rd(k.sefffile, "seff"), ks = rd(k.ksfile, "ks");
+    std::vector<float> kr(n);
+    for (size_t i = 0; i < n; i++) kr[i] = std::sqrt(ks[i] / 25.4f) / 75.0f;
+    field(h.inf_par[0], smax);
+    field(h.inf_par[1], kr);
+    field(h.inf_st[0], se);
+    for (int j = 1; j <= 4; j++) state(j, 0.0f);
+    h.inf_rain.assign(nstore, 0);
+  } else if (P.inftype == 4) {  // gai (:361-505, equations 4-33 and 4-36)
+    auto psi = rd(k.psifile, "psi"), sig = rd(k.sigmafile, "sigma"), ks = rd(k.ksfile, "ks");
+    std::vector<float> kr(n), lu(n), ksm(n), head(n);
+    for (size_t i = 0; i < n; i++) {
+      kr[i] = std::sqrt(ks[i] / 25.4f) / 75.0f;
+      lu[i] = 4.0f * std::sqrt(25.4f) * std::sqrt(ks[i]) / 1000.0f;
+      head[i] = psi[i] / 1000.0f;
+      ksm[i] = ks[i] / 1000.0f / 3600.0f;
+    }
+    field(h.inf_par[0], ksm);
+    field(h.inf_par[1], sig);
+    field(h.inf_par[2], lu);
+    field(h.inf_par[3], kr);
+    field(h.inf_par[4], head);
+    field(h.inf_st[0], sig);  // sigma starts at its maximum
+    state(1, 0.0f);
+    state(2, 0.0f);
+    state(3, 0.0f);
+  } else if (P.inftype == 5) {  // hor: fc, f0 (mm/h), kd (1/h) (:506-590)
+    auto fc = rd(k.fcfile, "fc"), f0 = rd(k.f0file, "f0"), kd = rd(k.kdfile, "kd");
+    field(h.inf_par[0], fc);
+    field(h.inf_par[1], f0);
+    field(h.inf_par[2], kd);
+    state(0, 0.0f);
+  }
+}
+
 // The hu**(7/3) lookup table of h73table (fill_h73_tables, sfincs_data.f90:
 // 858-881): x73(j, k) = hh**2 * hh**(1.0/3.0) at hh = 0.001 j 10**(k - 6),
 // j = 1..1000, k = 1..10, in real*4 (10.0**(k - 6) for k < 6 as the reciprocal
@@ -191,16 +249,19 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   std::string prcpfile = in.str("prcfile", "none");
   if (is_none(prcpfile)) prcpfile = in.str("precipfile", "none");
   // Inputs outside this core's path: refuse loudly instead of silently ignoring physics.
-  for (const char* k : {"bcafile", "bzifile", "bdrfile", "volfile", "spwfile",
+  for (const char* k : {"bcafile", "bzifile", "volfile", "spwfile",
                         "amufile", "amvfile", "ampfile", "amprfile", "netbndbzsbzifile", "netsrcdisfile",
                         "netamuamvfile", "netamprfile", "netampfile", "netspwfile", "infiltration_file",
-                        "scsfile", "sefffile", "psifile", "f0file", "wavemaker_wvmfile", "wvmfile"}) {
+                        "wavemaker_wvmfile", "wvmfile"}) {
     if (!is_none(in.str(k, "none"))) throw std::runtime_error(std::string("input '") + k + "' is not supported by this core");
   }
   for (const char* k : {"snapwave", "nonh", "bathtub", "vegetation"})
     if (in.logical(k, false) || in.integer(k, 0) != 0)
       throw std::runtime_error(std::string("process '") + k + "' is not supported by this core");
-  if (!is_none(inifile)) throw std::runtime_error("inifile is not supported by this core yet");
+  // A netCDF inifile goes through the reference's quadtree netCDF reader
+  // (sfincs_initial_conditions.F90:61-78); the binary form is read below.
+  if (!is_none(inifile) && inifile.size() >= 2 && inifile.compare(inifile.size() - 2, 2, "nc") == 0)
+    throw std::runtime_error("netCDF inifile is not supported by this core (use the binary real*4 form)");
   if (!is_none(rstfile) && !is_none(in.str("qtrfile", "none")))
     throw std::runtime_error("rstfile is not supported on quadtree grids by this core");
   if (igeo != 0) throw std::runtime_error("geographic grids (crsgeo=1) are not supported by this core");
@@ -240,6 +301,11 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   h.store_vmax = in.integer("storevelmax", 0) == 1 && dtmaxout > 0.0f;
   h.store_qmax = in.integer("storefluxmax", 0) == 1 && dtmaxout > 0.0f;
   h.store_twet = in.integer("storetwet", 0) == 1;
+  P.store_vmax = h.store_vmax;
+  P.store_qmax = h.store_qmax;
+  P.store_twet = h.store_twet;
+  P.store_tzsmax = in.integer("storetzsmax", 0) == 1 && P.store_zsmax;
+  P.twet_threshold = in.real("twet_threshold", 0.01f);
   P.subgrid = !is_none(sbgfile);
   P.advection = iadvection > 0;
   P.adv_scheme = 1;
@@ -266,6 +332,31 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   k.mskfile = mskfile; k.indexfile = indexfile; k.sbgfile = sbgfile; k.manningfile = manningfile;
   k.bndfile = bndfile; k.bzsfile = bzsfile; k.srcfile = srcfile; k.disfile = disfile; k.wndfile = wndfile;
   k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile; k.weirfile = weirfile; k.drnfile = drnfile; k.rstfile = rstfile;
+  k.inifile = inifile;
+  k.bdrfile = in.str("bdrfile", "none");
+  k.scsfile = in.str("scsfile", "none");
+  k.smaxfile = in.str("smaxfile", "none");
+  k.sefffile = in.str("sefffile", "none");
+  k.ksfile = in.str("ksfile", "none");
+  k.psifile = in.str("psifile", "none");
+  k.sigmafile = in.str("sigmafile", "none");
+  k.f0file = in.str("f0file", "none");
+  k.fcfile = in.str("fcfile", "none");
+  k.kdfile = in.str("kdfile", "none");
+  // infiltration type (sfincs_infiltration.f90:61-145): con / c2d first, then
+  // the models with state; all of it only with rain
+  P.sfacinf = in.real("sfacinf", 0.2f);
+  P.horton_kr_kd = in.real("horton_kr_kd", 10.0f);
+  P.store_cumprcp = in.integer("storecumprcp", 0) == 1;
+  P.inftype = 0;
+  if (P.precip) {
+    if (qinf > 0.0f || !is_none(qinffile)) P.inftype = 1;
+    else if (!is_none(k.scsfile)) P.inftype = 2;
+    else if (!is_none(k.sefffile)) P.inftype = 3;
+    else if (!is_none(k.psifile)) P.inftype = 4;
+    else if (!is_none(k.f0file)) P.inftype = 5;
+  }
+  if (P.inftype == 2 || P.inftype == 3) P.store_cumprcp = 1;  // the curve-number methods need the sums
   return k;
 }
 
@@ -466,7 +557,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   }
   h.np = (long long)h.cmp_off.size();
   for (int8_t k : kcs)
-    if (k == 4 || k == 5) throw std::runtime_error("msk values 4/5 (wave makers, downstream river) are not supported");
+    if (k == 4) throw std::runtime_error("msk value 4 (wave makers) is not supported");
   auto act = [&](int n, int m) { return n >= 1 && n <= nmax && m >= 1 && m <= mmax && kcs[OFF(n, m)] > 0; };
 
   // ---- geometry (sfincs_domain.f90:1369-1541, projected, one level) -----------
@@ -529,6 +620,8 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   // after initialize_domain); activity and the theta-smoothing neighbour rule
   // see the dams (the reference tests kcuv there at run time).
   RestartData rst;
+  std::vector<float> inizs;  // binary ini file (read_zsini_file, sfincs_initial_conditions.F90:270-288)
+  if (is_none(K.rstfile) && !is_none(K.inifile)) inizs = read_binary<float>(path(K.inifile), (size_t)h.np);
   if (!is_none(K.rstfile)) {
     rst = read_restart(path(K.rstfile));
     if (rst.type >= 1 && rst.type <= 6) {
@@ -721,8 +814,33 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   std::vector<float> xb, yb;
   read_boundary_series(h, K, water_level_bnd, xb, yb, nbnd);
 
+  // ---- downstream river points (sfincs_boundaries.f90:217-270): the cell of each
+  // point's internal point and the level drop slope * distance to it
+  bool river = false;
+  for (size_t ib = 0; ib < ngb; ib++) river = river || kcs[gb_cell[ib]] == 5;
+  std::vector<float> xr, yr, dzr;
+  std::vector<int32_t> zsir;
+  if (river) {
+    if (is_none(K.bdrfile)) throw std::runtime_error("downstream river points (msk 5) need a bdrfile");
+    for (const auto& r : read_table(path(K.bdrfile))) {
+      if (r.size() < 6) throw std::runtime_error("bdrfile: expected x y x_internal y_internal slope distance");
+      const float x = (float)r[0], y = (float)r[1], xin = (float)r[2], yin = (float)r[3];
+      const float slope = (float)r[4], dist = (float)r[5];
+      // the cell holding the internal point (find_quadtree_cell on the regular grid)
+      const float xt = cosrot * (xin - x0) + sinrot * (yin - y0), yt = -sinrot * (xin - x0) + cosrot * (yin - y0);
+      const int n = (int)(yt / dy) + 1, m = (int)(xt / dx) + 1;
+      if (!act(n, m)) throw std::runtime_error("bdrfile: internal point outside the active grid");
+      xr.push_back(x);
+      yr.push_back(y);
+      zsir.push_back((int32_t)OFF(n, m));
+      dzr.push_back(dist < 0.0f ? -slope * std::sqrt((xin - x) * (xin - x) + (yin - y) * (yin - y)) : -slope * dist);
+    }
+    if (xr.empty()) throw std::runtime_error("bdrfile holds no points");
+  }
+  std::vector<int> gb_bdr(ngb, -1);
+
   // ---- find_boundary_indices (sfincs_boundaries.f90:455-679) -------------------------
-  if (ngb > 0 && nbnd > 0) {
+  if (ngb > 0 && (nbnd > 0 || river)) {
     for (size_t ib = 0; ib < ngb; ib++) {
       const int64_t c = gb_cell[ib];
       const long long ic = cmp_of[c];
@@ -750,6 +868,16 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
           gb_fac[ib] = dst2 / std::max(dst1 + dst2, 1.0e-9f);
         } else {
           gb_fac[ib] = 1.0f;
+        }
+      } else if (kcs[c] == 5) {  // nearest point of the bdr file (:596-613)
+        float dst1 = 1.0e10f;
+        for (size_t j = 0; j < xr.size(); j++) {
+          const float ddx = xr[j] - x, ddy = yr[j] - y;
+          const float dst = std::sqrt(ddx * ddx + ddy * ddy);
+          if (dst < dst1) {
+            dst1 = dst;
+            gb_bdr[ib] = (int)j;
+          }
         }
       } else if (kcs[c] == 6) {
         const int n = h.z_n[ic], m = h.z_m[ic];
@@ -791,6 +919,14 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     b.zfix = gb_zfix[ib];
     b.len = e.dir == 1 ? dx : dy;
     if (kcs[e.nmb] == 2 && nbnd == 0) b.info |= 4, b.zfix = 0.0f;  // no boundary data: zsb stays 0
+    if (kcs[e.nmb] == 5) {  // downstream river cell: level from its internal point
+      const int j = gb_bdr[ib];
+      if (j < 0) throw std::runtime_error("downstream river cell without a bdr point");
+      b.info = (b.info & ~8) | 32;
+      b.zsi = zsir[(size_t)j];
+      b.zfix = dzr[(size_t)j];
+      b.i1 = b.i2 = 0;
+    }
     h.bfaces.push_back(b);
   }
   h.dense2cmp = cmp_of;
@@ -845,6 +981,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
       for (long long i = 0; i < h.np; i++) h.qinf[h.cmp_off[i]] = r[i] / 3600.0f / 1000.0f;
     }
   }
+  load_infiltration_models(h, K, NA, h.cmp_off);
 
   // ---- weirs (sfincs_structures.f90:38-381) ----------------------------------------
   // Every face a weir polyline crosses gets the crossed length (the face's
@@ -975,7 +1112,8 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   for (long long i = 0; i < h.np; i++) {
     const int64_t c = h.cmp_off[i];
     const float base = P.subgrid ? h.zz_min[c] : h.zb[c];
-    const double ini = rst.zs.empty() ? (double)P.zini : (double)rst.zs[i];  // inizs (real*8) from real*4
+    // inizs (real*8) from the real*4 restart or ini file, else zini
+    const double ini = !rst.zs.empty() ? (double)rst.zs[i] : (!inizs.empty() ? (double)inizs[i] : (double)P.zini);
     h.zs[c] = (float)std::max((double)base, ini);
   }
   h.zsmax.assign(NA, -999.0f);
@@ -1150,11 +1288,24 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     if (q) fill(q, nullptr, n * sizeof(X));
     dst = q;
   };
+  // store variables (sfincs_domain.f90:2296-2310): vmax and t_zsmax start at
+  // -999, twet at 0; qmax at 0 (the reference allocates it without a value)
+  auto place_store = [&](size_t n) {
+    auto filled = [&](float*& dst, bool on, float v) {
+      if (on) up(dst, std::vector<float>(n, v));
+      else dst = nullptr;
+    };
+    filled(d.vmax, h.p.store_vmax, -999.0f);
+    filled(d.qmax, h.p.store_qmax, 0.0f);
+    filled(d.twet, h.p.store_twet, 0.0f);
+    filled(d.tzsmax, h.p.store_tzsmax, -999.0f);
+  };
   if (h.p.quadtree) {
     // compact cells (npc), uv points (npuv) and q/uv arrays (npuv + ncuv + dummy)
     const size_t NC = (size_t)h.np, NF = (size_t)h.npuv, NQ = (size_t)(h.npuv + h.p.ncuv + 1);
     up(d.zs, h.zs);
     up(d.zsmax, h.zsmax);
+    place_store(NC);
     up(d.zvol, h.zvol);
     if (h.p.wiggle) {
       up(d.zs0, h.zs0);
@@ -1214,6 +1365,7 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     d.zl = nullptr;
   up(d.zs, h.zs);
   up(d.zsmax, h.zsmax);
+  place_store(NA);
   up(d.zvol, h.zvol);
   if (h.p.wiggle) {
     up(d.zs0, h.zs0);
@@ -1293,6 +1445,13 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.wdir, h.wdir);
   up(d.cdval, h.cdval);
   up(d.x73, h.x73);
+  for (int j = 0; j < 5; j++) {
+    up(d.inf_par[j], h.inf_par[j]);
+    up(d.inf_st[j], h.inf_st[j]);
+  }
+  up(d.inf_rain, h.inf_rain);
+  up(d.cumprcp, h.cumprcp);
+  up(d.cuminf, h.cuminf);
   up(d.tsrc, h.tsrc);
   up(d.qsrc, h.qsrc);
   zero(d.qtsrc, (size_t)std::max(h.p.nsrc + 2 * h.p.ndrn, 1));

@@ -50,6 +50,9 @@ struct HostModel {
   std::vector<float> t_bnd, zs_bnd;  // zs_bnd [ntbnd][nbnd]
   std::vector<float> tprcp, vprcp, twnd, wmag, wdir, cdval;
   std::vector<float> x73;            // hu**(7/3) table when h73table is on (sfincs_data.f90:858-881)
+  // infiltration models with state: parameters, state, event flag, cumulative sums (storage order)
+  std::vector<float> inf_par[5], inf_st[5], cumprcp, cuminf;
+  std::vector<uint8_t> inf_rain;
   std::vector<float> tsrc, qsrc;     // qsrc [ntsrc][nsrc]
   std::vector<int32_t> src_cell;
   std::vector<StrucFace> struc;       // weir faces
@@ -88,6 +91,10 @@ struct Keys {
         rghlevland = 0, qinf = 0, qinf_zmin = 0;
   bool viscosity = false, advection_mask = true, quadtree = false;
   std::string thdfile, weirfile, drnfile, rstfile;  // thin dams, weirs, drainage structures, restart (regular grids)
+  std::string inifile;                              // binary initial water levels (real*4, cell order)
+  std::string bdrfile;                              // downstream river points
+  // infiltration parameter files (binary real*4, cell order)
+  std::string scsfile, smaxfile, sefffile, ksfile, psifile, sigmafile, f0file, fcfile, kdfile;
   std::string qtrfile, depfile, mskfile, indexfile, sbgfile, manningfile, bndfile, bzsfile, srcfile, disfile,
       wndfile, qinffile, prcpfile;
 };
@@ -111,6 +118,11 @@ float projected_length(float x0a, float y0a, float x0b, float y0b, float x1, flo
 void read_boundary_series(HostModel& h, const Keys& k, bool water_level_bnd, std::vector<float>& xb,
                           std::vector<float>& yb, int& nbnd);
 void read_meteo_series(HostModel& h, const Keys& k, float rotation);
+// Infiltration models with state (cna, cnb, gai, hor; sfincs_infiltration.f90:
+// 8-600): per-cell parameters from the binary files, converted as the
+// reference does, laid out at storage index store[i] of compact cell i
+// (nstore entries); the cumulative sums when stored.  P.inftype must be set.
+void load_infiltration_models(HostModel& h, const Keys& k, size_t nstore, const std::vector<int32_t>& store);
 // Quadtree mesh (qtrfile): compact cells and uv points (host/qtmodel.cpp).
 void load_quadtree(HostModel& h, const Keys& k);
 // 1-based active cell of a quadtree mesh at point (x, y), 0 outside.

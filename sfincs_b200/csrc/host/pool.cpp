@@ -182,6 +182,9 @@ struct Pool {
       launch_gather_f64(D.zvol, s.dev->d_cmp_off(), (double*)d_stage, n, stream);
     } else if (name == "zsmax") {
       f32(D.zsmax);
+    } else if ((name == "vmax" && D.vmax) || (name == "qmax" && D.qmax) || (name == "twet" && D.twet) ||
+               (name == "tzsmax" && D.tzsmax)) {
+      f32(name == "vmax" ? D.vmax : name == "qmax" ? D.qmax : name == "twet" ? D.twet : D.tzsmax);
     } else if (name == "qx") {
       f32(D.qu[p], s.dev->face_map(0));
     } else if (name == "qy") {

@@ -818,11 +818,19 @@ void QtBuilder::finish() {
     h.qinf.assign(np, 0.0f);
     for (long i = 0; i < np; i++) h.qinf[i] = r[(size_t)i] / 3600.0f / 1000.0f;
   }
+  {  // infiltration models with state: parameters in cell order (compact storage)
+    std::vector<int32_t> ident((size_t)np);
+    for (long i = 0; i < np; i++) ident[(size_t)i] = (int32_t)i;
+    load_infiltration_models(h, k, (size_t)np, ident);
+  }
   // initial state (sfincs_initial_conditions.F90:98-106, sfincs_subgrid.F90:907-962)
+  // binary ini file: real*4 levels in cell order (read_zsini_file, sfincs_initial_conditions.F90:270-288)
+  std::vector<float> inizs;
+  if (!none(k.inifile)) inizs = read_binary<float>(h.dir + "/" + k.inifile, (size_t)np);
   h.zs.assign(np, 0.0f);
   for (long i = 0; i < np; i++) {
     const float base = P.subgrid ? h.zz_min[i] : h.zb[i];
-    h.zs[i] = (float)std::max((double)base, (double)P.zini);
+    h.zs[i] = (float)std::max((double)base, inizs.empty() ? (double)P.zini : (double)inizs[(size_t)i]);
   }
   h.zsmax.assign(np, -999.0f);
   if (P.wiggle) h.zs0 = h.zs;

@@ -322,7 +322,7 @@ __device__ __forceinline__ BndPre bnd_pre(const ScnDev& S, const StepState& st, 
     }
     r.um = S.uvmean[i];
     const int itb0 = st.itb0, itb1 = st.itb1;  // 0 before the first step
-    if (!(r.b.info & 4) && S.nbnd > 0 && itb0 >= 1 && itb0 <= S.ntbnd && itb1 >= 1 && itb1 <= S.ntbnd) {
+    if (!(r.b.info & (4 | 32)) && S.nbnd > 0 && itb0 >= 1 && itb0 <= S.ntbnd && itb1 >= 1 && itb1 <= S.ntbnd) {
       r.itb0 = itb0;
       r.itb1 = itb1;
       const int j1 = (r.b.info & 8) ? r.b.i1 : 0, j2 = (r.b.info & 8) ? r.b.i2 : 0;
@@ -378,6 +378,8 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan&
     float zsnmb, zs0nmb;
     if (b.info & 4) {
       zsnmb = zs0nmb = b.zfix;
+    } else if (b.info & 32) {  // downstream river: internal level plus the slope drop, not below the floor (:878-902)
+      zsnmb = zs0nmb = (float)fmax((double)S.zs[b.zsi] + (double)b.zfix, (double)b.floor);
     } else {
       if (S.nbnd > 0 && (pre.itb0 != P.itb0 || pre.itb1 != P.itb1)) {  // not read ahead, or another time record
         const int j1 = (b.info & 8) ? b.i1 : 0, j2 = (b.info & 8) ? b.i2 : 0;
@@ -462,7 +464,10 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan&
       S.uvmean[i] = 0.0f;
     }
     S.zs[b.nmb] = zsb_v;
-    if (S.store_zsmax) S.zsmax[b.nmb] = fmaxf(dyn.zsmax, zsb_v);
+    if (S.store_zsmax) {  // sfincs_boundaries.f90:1101-1113
+      if (S.store_tzsmax && zsb_v > dyn.zsmax) S.tzsmax[b.nmb] = (float)P.t;
+      S.zsmax[b.nmb] = fmaxf(dyn.zsmax, zsb_v);
+    }
     inflow = (double)sgn * (double)qq * (double)b.len * (double)dt;
   } else if (i < S.nkcuv2 + S.nneu) {
     S.zs[pre.nn.x] = dyn.zsnmi;  // Neumann: zs(nmb) = zs(nmi) (sfincs_boundaries.f90:903-914)
@@ -523,6 +528,9 @@ __global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ sc
   if (threadIdx.x == 0) {
     commit_step(S, st, P);
     if (P.go && S.ndrn > 0) update_drainage(S, P);
+    // Green-Ampt reads GA_head(np) * GA_sigma(np) for every cell
+    // (sfincs_infiltration.f90:858): the last cell's values before this step's update
+    if (P.go && S.inftype == 4) st.ga_hs = S.inf_par[4][S.inf_last] * S.inf_st[0][S.inf_last];
   }
 }
 
@@ -782,13 +790,24 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
   if (!(f & F_ACT)) return;
   const float dt = st.dt;
   float zsn = zs_old;
+  // infiltration with state (or cumulative rain) for every active cell, from the start-of-step state
+  const bool inf_cell = S.precip && (S.inftype >= 2 || S.store_cumprcp);
+  float qinf_cell = 0.0f;
+  if (inf_cell) {
+    if (SG) {
+      qinf_cell = cell_infiltration(S, c, st.ptmp, dt, v_old <= 0.0, (float)(v_old / (double)S.area), st.ga_hs);
+    } else {
+      const float zb0 = S.zb[c];
+      qinf_cell = cell_infiltration(S, c, st.ptmp, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
+    }
+  }
   if (f & F_KCS1) {
     if (SG) {  // sfincs_continuity.f90:341-577
       float dvol = ((q_md - q_mu) * S.dy + (q_nd - q_nu) * S.dx) * dt;
       if (S.precip || S.use_qext) {
         float dzsdt = 0.0f;
         if (S.precip) {
-          const float qinfmap = (S.infiltration && v_old > 0.0) ? qi : 0.0f;  // sfincs_infiltration.f90:639-670
+          const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && v_old > 0.0) ? qi : 0.0f);  // sfincs_infiltration.f90:639-670
           dzsdt = dzsdt + (st.ptmp - qinfmap);
         }
         if (S.use_qext) dzsdt = dzsdt + qx;
@@ -818,7 +837,7 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
     } else {  // sfincs_continuity.f90:112-153
       float z = zs_old;
       if (S.precip) {
-        const float qinfmap = (S.infiltration && !(z <= zbc)) ? qi : 0.0f;
+        const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && !(z <= zbc)) ? qi : 0.0f);
         z = z + (st.ptmp - qinfmap) * dt;
       }
       if (S.use_qext) z = z + qx * dt;
@@ -826,8 +845,22 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
       if (z != zs_old) S.zs[c] = z;
       zsn = z;
     }
+    if (S.store_vmax | S.store_qmax | S.store_twet) {
+      float u_md = 0.0f, u_mu = 0.0f, u_nd = 0.0f, u_nu = 0.0f;
+      if (S.store_vmax) {
+        u_md = S.uu[p1][c - ld];
+        u_mu = S.uu[p1][c];
+        u_nd = S.vv[p1][c - 1];
+        u_nu = S.vv[p1][c];
+      }
+      store_cell_variables(S, c, q_md, q_mu, q_nd, q_nu, u_md, u_mu, u_nd, u_nu, zsn,
+                           S.store_twet ? (SG ? S.zz_min[c] : S.zb[c]) : 0.0f, dt);
+    }
   }
-  if (S.store_zsmax && zsn > zm) S.zsmax[c] = zsn;
+  if (S.store_zsmax) {
+    if (S.store_tzsmax) store_tzsmax(S, c, zsn, zm, SG ? S.zz_min[c] : S.zb[c]);
+    if (zsn > zm) S.zsmax[c] = zsn;
+  }
 }
 
 // --------------------------------------------------------------------------

@@ -173,6 +173,19 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
   const float zs_old = S.zs[c];
   const float dt = st.dt;
   float zsn = zs_old;
+  // infiltration with state (or cumulative rain) for every active cell, from the start-of-step state
+  const bool inf_cell = S.precip && (S.inftype >= 2 || S.store_cumprcp);
+  float qinf_cell = 0.0f;
+  if (inf_cell) {
+    if (SG) {
+      const double v0 = S.zvol[c];
+      qinf_cell = cell_infiltration(S, c, st.ptmp, dt, v0 <= 0.0, (float)(v0 / (double)S.lv_area[S.qlev[c]]),
+                                    st.ga_hs);
+    } else {
+      const float zb0 = S.zb[c];
+      qinf_cell = cell_infiltration(S, c, st.ptmp, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
+    }
+  }
   if (fl & F_KCS1) {
     const int4 fc = S.qcell[c];
     const float q_md = q[fc.x], q_mu = q[fc.y], q_nd = q[fc.z], q_nu = q[fc.w];
@@ -188,7 +201,7 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
       if (S.precip || S.use_qext) {
         float dzsdt = 0.0f;
         if (S.precip) {
-          const float qinfmap = (S.infiltration && v_old > 0.0) ? qi : 0.0f;
+          const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && v_old > 0.0) ? qi : 0.0f);
           dzsdt = dzsdt + (st.ptmp - qinfmap);
         }
         if (S.use_qext) dzsdt = dzsdt + qx;
@@ -218,7 +231,7 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
       float z = zs_old;
       if (S.precip) {
         const float zbc = S.infiltration ? S.zb[c] : 0.0f;
-        const float qinfmap = (S.infiltration && !(z <= zbc)) ? qi : 0.0f;
+        const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && !(z <= zbc)) ? qi : 0.0f);
         z = z + (st.ptmp - qinfmap) * dt;
       }
       if (S.use_qext) z = z + qx * dt;
@@ -226,8 +239,24 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
       if (z != zs_old) S.zs[c] = z;
       zsn = z;
     }
+    if (S.store_vmax | S.store_qmax | S.store_twet) {
+      float u_md = 0.0f, u_mu = 0.0f, u_nd = 0.0f, u_nu = 0.0f;
+      if (S.store_vmax) {  // this step's velocities at the cell's uv points (combined points included)
+        const float* uv = S.uu[st.parity ^ 1];
+        u_md = uv[fc.x];
+        u_mu = uv[fc.y];
+        u_nd = uv[fc.z];
+        u_nu = uv[fc.w];
+      }
+      store_cell_variables(S, c, q_md, q_mu, q_nd, q_nu, u_md, u_mu, u_nd, u_nu, zsn,
+                           S.store_twet ? (SG ? S.zz_min[c] : S.zb[c]) : 0.0f, dt);
+    }
   }
-  if (S.store_zsmax && zsn > S.zsmax[c]) S.zsmax[c] = zsn;
+  if (S.store_zsmax) {
+    const float zm = S.zsmax[c];
+    if (S.store_tzsmax) store_tzsmax(S, c, zsn, zm, SG ? S.zz_min[c] : S.zb[c]);
+    if (zsn > zm) S.zsmax[c] = zsn;
+  }
 }
 
 void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {

@@ -567,6 +567,19 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
           const float zm = ((const float*)(sm + con::O_ZSMAX))[k];
           const float dt = sv.dt;
           float zsn = zs_old;
+          // infiltration with state (or cumulative rain) for every active cell, from the start-of-step state
+          const bool inf_cell = S.precip && (S.inftype >= 2 || S.store_cumprcp);
+          float qinf_cell = 0.0f;
+          if (inf_cell) {
+            if (SG) {
+              const double v0 = ((const double*)(sm + con::O_ZVOL))[k];
+              qinf_cell = cell_infiltration(S, c, sv.ptmp, dt, v0 <= 0.0, (float)(v0 / (double)S.area), S.st->ga_hs);
+            } else {
+              const float zbc = S.zb[c];
+              qinf_cell = cell_infiltration(S, c, sv.ptmp, dt, zs_old <= zbc, (float)((double)zs_old - (double)zbc),
+                                            S.st->ga_hs);
+            }
+          }
           if (f & F_KCS1) {
             const float qx = S.use_qext ? ((const float*)(sm + con::O_QEXT))[k] : 0.0f;
             const float qi = S.infiltration ? ((const float*)(sm + con::O_QINF))[k] : 0.0f;
@@ -579,7 +592,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
               if (S.precip || S.use_qext) {
                 float dzsdt = 0.0f;
                 if (S.precip) {
-                  const float qinfmap = (S.infiltration && v_old > 0.0) ? qi : 0.0f;
+                  const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && v_old > 0.0) ? qi : 0.0f);
                   dzsdt = dzsdt + (sv.ptmp - qinfmap);
                 }
                 if (S.use_qext) dzsdt = dzsdt + qx;
@@ -620,7 +633,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
               float z = zs_old;
               if (S.precip) {
                 const float zbc = S.infiltration ? ((const float*)(sm + con::O_ZB))[k] : 0.0f;
-                const float qinfmap = (S.infiltration && !(z <= zbc)) ? qi : 0.0f;
+                const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && !(z <= zbc)) ? qi : 0.0f);
                 z = z + (sv.ptmp - qinfmap) * dt;
               }
               if (S.use_qext) z = z + qx * dt;
@@ -628,8 +641,23 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
               if (z != zs_old) S.zs[c] = z;
               zsn = z;
             }
+            if (S.store_vmax | S.store_qmax | S.store_twet) {
+              float u_md = 0.0f, u_mu = 0.0f, u_nd = 0.0f, u_nu = 0.0f;
+              if (S.store_vmax) {
+                const int p1 = sv.parity ^ 1;  // this step's velocities
+                u_md = S.uu[p1][c - S.ld];
+                u_mu = S.uu[p1][c];
+                u_nd = S.vv[p1][c - 1];
+                u_nu = S.vv[p1][c];
+              }
+              store_cell_variables(S, c, q_md, q_mu, q_nd, q_nu, u_md, u_mu, u_nd, u_nu, zsn,
+                                   S.store_twet ? (SG ? S.zz_min[c] : S.zb[c]) : 0.0f, dt);
+            }
           }
-          if (S.store_zsmax && zsn > zm) S.zsmax[c] = zsn;
+          if (S.store_zsmax) {
+            if (S.store_tzsmax) store_tzsmax(S, c, zsn, zm, SG ? S.zz_min[c] : S.zb[c]);
+            if (zsn > zm) S.zsmax[c] = zsn;
+          }
         }
       }
     }

@@ -83,14 +83,15 @@ struct alignas(16) BndFace {
   int nmb;       // dense offset of the boundary cell
   int nmi;       // dense offset of the interior cell
   int info;      // bit0: v face; bit1: ibuvdir = +1 (else -1); bit2: outflow cell (kcs 3); bit3: multiple bnd points;
-                 // bit4: a weir on the face (kcuv 3: no boundary flux)
+                 // bit4: a weir on the face (kcuv 3: no boundary flux); bit5: downstream river cell (kcs 5)
   int i1, i2;    // nearest boundary points (0-based)
   float fac;     // weight of i1
   float zbuv;    // zbuv of the face (regular grids; sfincs_domain.f90:1692)
   float floor;   // zb or subgrid z_zmin of the boundary cell
-  float zfix;    // fixed level of an outflow (kcs 3) cell (sfincs_domain.f90:1937-1948)
+  float zfix;    // fixed level of an outflow (kcs 3) cell (sfincs_domain.f90:1937-1948); river (kcs 5): the level
+                 // difference dzs_bdr to the internal point (sfincs_boundaries.f90:250-263)
   float len;     // face length (m): dy for u faces, dx for v faces (per refinement level on a quadtree)
-  int pad1;
+  int zsi;       // river (kcs 5): dense offset of the cell holding the internal point
 };
 
 // ---- quadtree layout ---------------------------------------------------------
@@ -143,6 +144,7 @@ struct alignas(16) StepState {
   int steps_left;      // for single / bounded calls
   int itbndlast, itprcplast, itwndlast, itsrclast;
   int fault;           // nonzero: a bounded wait in a staged kernel gave up (its tile was skipped)
+  float ga_hs;         // Green-Ampt: GA_head * GA_sigma of the model's last cell at the start of the step
 };
 
 struct ScnDev {
@@ -229,6 +231,31 @@ struct ScnDev {
   float* drn_frac;       // [ndrn] gates: fraction open
   float structure_relax; // seconds
   float pi;
+  // store variables (compute_store_variables, sfincs_continuity.f90:626-720, and
+  // t_zsmax, :239-255): maximum cell velocity and flux, wet duration, time of
+  // the maximum level; dense per-cell arrays, null when off
+  int store_vmax, store_qmax, store_twet, store_tzsmax;
+  float twet_threshold;
+  float* vmax;
+  float* qmax;
+  float* twet;
+  float* tzsmax;
+  // Infiltration with state (update_infiltration_map, sfincs_infiltration.f90:
+  // 678-1033): inftype 2 curve number (cna), 3 curve number with recovery
+  // (cnb), 4 Green-Ampt (gai), 5 Horton (hor); con / c2d (inftype 1) use qinf.
+  // Per-cell parameters and state, dense like the other cell arrays:
+  //   cna: par 0 S (m)
+  //   cnb: par 0 Smax, 1 recovery rate kr; state 0 Se, 1 P1, 2 F1, 3 S1, 4 T1; rain flag
+  //   gai: par 0 ks (m/s), 1 sigma_max, 2 Lu (m), 3 kr, 4 suction head (m); state 0 sigma, 1 F, 2 T1, 3 qinfmap
+  //   hor: par 0 fc, 1 f0 (mm/h), 2 kd (1/h); state 0 T1
+  int inftype, store_cumprcp;
+  float sfacinf, horton_kr_kd;
+  int64_t inf_last;      // storage index of the model's last cell (gai reads its head and sigma)
+  const float* inf_par[5];
+  float* inf_st[5];
+  uint8_t* inf_rain;
+  float* cumprcp;        // cumulative rain and infiltration (m), when stored or needed (cna, cnb)
+  float* cuminf;
   int h73table;          // hu**(7/3) from the lookup table (sfincs_momentum.f90:663-675)
   const float* x73;      // [10][1000] the table x73(j, k) at (k - 1) * 1000 + j - 1 (sfincs_data.f90:858-881)
   StepState* st;
@@ -286,6 +313,169 @@ __device__ __forceinline__ StepVals step_vals(const StepState& st) {
 // after a model has gone unstable: the guards pass NaN to the interval branch,
 // and an f64 NaN converts to INT_MIN (an f32 NaN to 0), which would otherwise
 // index far outside the table.
+// Store variables of one kcs == 1 cell after its continuity update
+// (compute_store_variables, sfincs_continuity.f90:626-720): the cell-centre
+// velocity and flux magnitudes from the means of the cell's two u and two v
+// faces (this step's values), and the wet duration.  uv_* are read by the
+// caller only when vmax is stored; base is zb or the subgrid z_zmin.
+__device__ __forceinline__ void store_cell_variables(const ScnDev& S, int64_t c, float q_md, float q_mu, float q_nd,
+                                                     float q_nu, float uv_md, float uv_mu, float uv_nd, float uv_nu,
+                                                     float zsn, float base, float dt) {
+  if (S.store_vmax) {
+    const float quz = (uv_md + uv_mu) / 2.0f, qvz = (uv_nd + uv_nu) / 2.0f;
+    const float uvz = sqrtf(quz * quz + qvz * qvz);
+    S.vmax[c] = fmaxf(S.vmax[c], uvz);
+  }
+  if (S.store_qmax) {
+    const float quz = (q_md + q_mu) / 2.0f, qvz = (q_nd + q_nu) / 2.0f;
+    const float qz = sqrtf(quz * quz + qvz * qvz);
+    S.qmax[c] = fmaxf(S.qmax[c], qz);
+  }
+  if (S.store_twet && (double)zsn - (double)base > (double)S.twet_threshold) S.twet[c] = S.twet[c] + dt;
+}
+// Time of the maximum level (:239-255): set where the new level exceeds the
+// stored maximum and the cell is wet by more than huthresh; zm is the maximum
+// before this step's update.
+__device__ __forceinline__ void store_tzsmax(const ScnDev& S, int64_t c, float zsn, float zm, float base) {
+  if (zsn > zm && (double)zsn - (double)base > (double)S.huthresh) S.tzsmax[c] = (float)S.st->t;
+}
+
+// Exponential from IEEE operations only, so that the oracle reproduces it bit
+// for bit: n = rint(x log2 e), r = x - n ln2 with ln2 split in two parts
+// (Cody and Waite), e^r by its Taylor polynomial to degree 7 in Horner form,
+// times 2^n applied as two exact powers of two.  Within 0.94 ulp of e^x for
+// -87 <= x <= 88.7.
+__device__ __forceinline__ float exp_ieee(float x) {
+  if (x != x) return x;
+  if (x > 88.8f) return __int_as_float(0x7f800000);
+  if (x < -104.0f) return 0.0f;
+  const float n = rintf(x * 1.44269502f);
+  float r = fmaf(-n, 0.693145752f, x);
+  r = fmaf(-n, 1.42860677e-06f, r);
+  float p = 1.98412701e-04f;
+  p = fmaf(p, r, 1.38888892e-03f);
+  p = fmaf(p, r, 8.33333377e-03f);
+  p = fmaf(p, r, 4.16666679e-02f);
+  p = fmaf(p, r, 1.66666672e-01f);
+  p = fmaf(p, r, 0.5f);
+  p = fmaf(p, r, 1.0f);
+  p = fmaf(p, r, 1.0f);
+  const int ni = (int)n, n1 = ni / 2, n2 = ni - n1;
+  return (p * __int_as_float((n1 + 127) << 23)) * __int_as_float((n2 + 127) << 23);
+}
+
+// Infiltration of one active cell in this step (update_infiltration_map,
+// sfincs_infiltration.f90:609-1039, with the cumulative rain of
+// update_precipitation_from_timeseries, sfincs_meteo.f90:1545-1547); returns
+// qinfmap (m/s) and updates the cell's state.  dry: no water in the cell
+// (con / c2d), hh: the local depth estimate (Horton), ga_hs: the Green-Ampt
+// product GA_head(np) * GA_sigma(np) that the reference uses for every cell.
+__device__ __forceinline__ float cell_infiltration(const ScnDev& S, int64_t c, float prcp, float dt, bool dry,
+                                                   float hh, float ga_hs) {
+  if (S.store_cumprcp) S.cumprcp[c] = S.cumprcp[c] + prcp * dt;
+  float q = 0.0f;
+  if (S.inftype == 1) {  // con / c2d (:632-676)
+    q = dry ? 0.0f : S.qinf[c];
+  } else if (S.inftype == 2) {  // cna (:678-723)
+    const float cp = S.cumprcp[c], Sv = S.inf_par[0][c];
+    if (cp > S.sfacinf * Sv) {
+      const float a = cp - S.sfacinf * Sv;
+      const float Qq = a * a / (cp + (1.0f - S.sfacinf) * Sv);
+      q = ((cp - Qq) - S.cuminf[c]) / dt;
+    } else {
+      q = prcp;
+    }
+  } else if (S.inftype == 3) {  // cnb (:724-829)
+    float se = S.inf_st[0][c], t1 = S.inf_st[4][c];
+    if (prcp > 0.0f) {
+      float p1 = S.inf_st[1][c], f1 = S.inf_st[2][c], s1 = S.inf_st[3][c];
+      if (S.inf_rain[c] != 1) {  // a new rain event
+        p1 = 0.0f;
+        f1 = 0.0f;
+        s1 = se;
+        S.inf_rain[c] = 1;
+        S.inf_st[3][c] = s1;
+      }
+      p1 = p1 + prcp * dt;
+      if (p1 > S.sfacinf * s1) {
+        const float a = p1 - S.sfacinf * s1;
+        const float Qq = a * a / (p1 + (1.0f - S.sfacinf) * s1);
+        const float I = p1 - Qq;
+        q = (I - f1) / dt;
+        f1 = I;
+      } else {
+        f1 = p1;
+        q = prcp;
+      }
+      se = fmaxf(se - q * dt, 0.0f);
+      q = fmaxf(q, 0.0f);
+      S.inf_st[1][c] = p1;
+      S.inf_st[2][c] = f1;
+    } else {
+      if (S.inf_rain[c] == 1) {  // the event ended
+        S.inf_rain[c] = 0;
+        t1 = 0.0f;
+      }
+      t1 = t1 + dt / 3600.0f;
+      const float kr = S.inf_par[1][c], smax = S.inf_par[0][c];
+      if (t1 > 0.06f / kr) {  // recovery (SWMM equation 4-37)
+        se = se + kr * smax * dt / 3600.0f;
+        se = fminf(se, smax);
+      }
+    }
+    S.inf_st[0][c] = se;
+    S.inf_st[4][c] = t1;
+  } else if (S.inftype == 4) {  // gai (:830-912); the rate is kept while it does not rain
+    float sig = S.inf_st[0][c], F = S.inf_st[1][c], t1 = S.inf_st[2][c];
+    const float kr = S.inf_par[3][c], smax = S.inf_par[1][c], Lu = S.inf_par[2][c];
+    if (prcp > 0.0f) {
+      const float ks = S.inf_par[0][c];
+      if (prcp < ks) {
+        q = prcp;
+      } else {
+        q = ks * (1.0f + ga_hs / F);
+        q = fmaxf(fminf(q, prcp), 0.0f);
+      }
+      sig = fmaxf(sig - q * dt / Lu, 0.0f);
+      F = F + q * dt;
+      t1 = 0.0f;
+      S.inf_st[3][c] = q;
+    } else {
+      q = S.inf_st[3][c];
+      t1 = t1 + dt / 3600.0f;
+      if (t1 > 0.06f / kr) {
+        sig = sig + kr * smax * dt / 3600.0f;
+        sig = fminf(sig, smax);
+        F = fmaxf(F - kr * smax * dt / 3600.0f * Lu, 0.0f);
+      }
+    }
+    S.inf_st[0][c] = sig;
+    S.inf_st[1][c] = F;
+    S.inf_st[2][c] = t1;
+  } else if (S.inftype == 5) {  // hor (:914-1033)
+    float t1 = S.inf_st[0][c];
+    if (hh > 0.0f || prcp > 0.0f) {
+      t1 = t1 > 0.0f ? 0.0f : t1 - dt;
+      const float fc = S.inf_par[0][c];
+      float I = exp_ieee(S.inf_par[2][c] * t1 / 3600.0f);
+      if (I < 0.01f) {
+        t1 = t1 + dt;
+        q = fc / 3600.0f / 1000.0f;
+      } else {
+        q = (fc + (S.inf_par[1][c] - fc) * I) / 3600.0f / 1000.0f;
+      }
+      const float Qq = hh > 0.0f ? prcp * dt + hh : prcp * dt;
+      I = q * dt;
+      if (I > Qq) q = q * Qq / I;
+    } else {
+      t1 = t1 + dt / S.horton_kr_kd;
+    }
+    S.inf_st[0][c] = t1;
+  }
+  if (S.store_cumprcp && S.inftype >= 1) S.cuminf[c] = S.cuminf[c] + q * dt;
+  return q;
+}
+
 __device__ __forceinline__ int lev_index(float x, int nlev) { return min(max((int)x + 1, 1), nlev - 1); }
 __device__ __forceinline__ int lev_index(double x, int nlev) { return min(max((int)x + 1, 1), nlev - 1); }
 #endif

@@ -302,6 +302,8 @@ class RegularModel:
     thd: Optional[List[np.ndarray]] = None  # thin dams: polylines, each (npoints, 2) x, y
     weir: Optional[List[np.ndarray]] = None  # weirs: polylines, each (npoints, 4) x, y, crest level, Cd
     drn: Optional[List[Sequence[float]]] = None  # drainage: x_in, y_in, x_out, y_out, type, params...
+    zsini_field: Optional[np.ndarray] = None  # (nmax, mmax) initial water level: binary inifile (real*4)
+    cell_fields: Dict[str, np.ndarray] = field(default_factory=dict)  # keyword -> (nmax, mmax) binary real*4 file
 
     @property
     def nmax(self):
@@ -374,6 +376,12 @@ class RegularModel:
                 for r in self.drn:
                     f.write(" ".join(str(int(v)) if k == 4 else f"{v:.4f}" for k, v in enumerate(r)) + "\n")
             inp["drnfile"] = "sfincs.drn"
+        if self.zsini_field is not None:
+            self.compact(self.zsini_field).astype(np.float32).tofile(os.path.join(d, "sfincs.ini"))
+            inp["inifile"] = "sfincs.ini"
+        for key, arr in self.cell_fields.items():
+            self.compact(arr).astype(np.float32).tofile(os.path.join(d, f"sfincs.{key}"))
+            inp[key] = f"sfincs.{key}"
         inp.update(self.params)
         with open(os.path.join(d, "sfincs.inp"), "w") as f:
             for k, v in inp.items():

@@ -4,9 +4,10 @@ The main parity tests (test_gpu_parity.py) run the default switches. Here each
 case turns on terms that those leave off: Coriolis, wind stress from a time
 series, theta smoothing, the "original" advection scheme, the slope limiter,
 friction2d off, viscosity and no wiggle suppression on a subgrid model, c2d
-infiltration, point sources, Neumann and outflow boundary cells, thin dams,
-weirs, the five drainage structure types and the hu**(7/3) lookup table
-(regular and subgrid). For each
+infiltration and the infiltration models with state (curve number with and
+without recovery, Green-Ampt, Horton), point sources, Neumann and outflow boundary cells, thin dams,
+weirs, the five drainage structure types, the hu**(7/3) lookup table and
+initial levels from an inifile (regular and subgrid). For each
 case the CUDA core is compared with the oracle in the core's own precision
 after 1, 2, 4, 10, 40 and 100 steps, on the default kernel path and on the
 per-thread-load path. The bars are those of the main stepwise test: time
@@ -139,7 +140,70 @@ def case_subgrid_h73table(tmp_path):
     return _subgrid(tmp_path, advection=1, h73table=1)
 
 
-CASES = {f.__name__[5:]: f for f in (case_h73table, case_subgrid_h73table, case_coriolis_wind_theta, case_original_advection_slopelim_nofric2d,
+def _infiltration_fields(m, kind, seed=17):
+    """Per-cell parameter files of an infiltration model with state."""
+    rng = np.random.default_rng(seed)
+    shp = m.msk.shape
+    if kind == "cna":
+        m.cell_fields["scsfile"] = rng.uniform(0.05, 2.0, shp)
+    elif kind == "cnb":
+        m.cell_fields["smaxfile"] = rng.uniform(0.005, 0.05, shp)
+        m.cell_fields["sefffile"] = rng.uniform(0.002, 0.03, shp)
+        m.cell_fields["ksfile"] = rng.uniform(10.0, 20000.0, shp)
+    elif kind == "gai":
+        m.cell_fields["psifile"] = rng.uniform(50.0, 300.0, shp)
+        m.cell_fields["sigmafile"] = rng.uniform(0.1, 0.4, shp)
+        m.cell_fields["ksfile"] = rng.uniform(5.0, 20000.0, shp)
+    else:
+        m.cell_fields["fcfile"] = rng.uniform(5.0, 20.0, shp)
+        m.cell_fields["f0file"] = rng.uniform(50.0, 150.0, shp)
+        m.cell_fields["kdfile"] = rng.uniform(1.0, 5.0, shp)
+    # rain that stops early, so the recovery branches run too
+    m.prcp = np.array([[0.0, 40.0], [400.0, 40.0], [401.0, 0.0], [7200.0, 0.0]])
+    return m
+
+
+def case_infiltration_cna(tmp_path):
+    return _infiltration_fields(_plain(tmp_path, storecumprcp=1), "cna")
+
+
+def case_subgrid_infiltration_cnb(tmp_path):
+    return _infiltration_fields(_subgrid(tmp_path, advection=1), "cnb")
+
+
+def case_infiltration_gai(tmp_path):
+    return _infiltration_fields(_plain(tmp_path, advection=1), "gai")
+
+
+def case_subgrid_infiltration_gai(tmp_path):
+    return _infiltration_fields(_subgrid(tmp_path), "gai")
+
+
+def case_infiltration_hor(tmp_path):
+    return _infiltration_fields(_plain(tmp_path), "hor")
+
+
+def case_subgrid_infiltration_hor(tmp_path):
+    return _infiltration_fields(_subgrid(tmp_path, storecumprcp=1), "hor")
+
+
+def case_inifile(tmp_path):
+    m = _plain(tmp_path, advection=1)
+    ini = np.full(m.msk.shape, -1.0, np.float32)
+    ini[:, : m.mmax // 2] = 1.5  # initial levels from a file: a dam break across the middle
+    m.zsini_field = ini
+    return m
+
+
+def case_subgrid_inifile(tmp_path):
+    m = _subgrid(tmp_path, advection=1)
+    m.zsini_field = np.where(np.arange(m.mmax)[None, :] < m.mmax // 3, 2.0, 0.0).repeat(m.nmax, 0).astype(np.float32)
+    return m
+
+
+CASES = {f.__name__[5:]: f for f in (case_infiltration_cna, case_subgrid_infiltration_cnb, case_infiltration_gai,
+                                      case_subgrid_infiltration_gai, case_infiltration_hor,
+                                      case_subgrid_infiltration_hor, case_inifile, case_subgrid_inifile, case_h73table, case_subgrid_h73table, case_coriolis_wind_theta, case_original_advection_slopelim_nofric2d,
                                       case_boundary_kinds, case_plain_infiltration, case_subgrid_visc_nowiggle,
                                       case_subgrid_infiltration_sources, case_thin_dams_theta,
                                       case_subgrid_thin_dams, case_weirs, case_subgrid_weirs, case_drainage,
@@ -200,3 +264,53 @@ def test_physics_paths_agree_bitwise(tmp_path, kind):
             assert np.array_equal(runs[0].get(name), g.get(name)), f"{name}: variant {v} differs from 5"
     for g in runs:
         g.close()
+
+
+def _river(tmp_path, subgrid=False):
+    """A channel deepening to the east: tide on the west column, a downstream
+    river boundary (msk 5) on the east column whose level follows the water
+    two cells inside, lowered by the bed slope times the distance."""
+    import os
+
+    if subgrid:
+        m = _subgrid(tmp_path, advection=1)
+    else:
+        m = _plain(tmp_path, advection=1)
+        x = (np.arange(m.mmax) + 0.5) * m.dx
+        m.zb = (np.full(m.msk.shape, -3.0) - 0.0002 * x[None, :]).astype(np.float32)
+    m.msk[:, -1] = 5
+    d = m.write(str(tmp_path / ("river_sg" if subgrid else "river")))
+    xe = m.mmax * m.dx - 0.5 * m.dx
+    rows = []
+    for n in (2, m.nmax // 2, m.nmax - 3):
+        y = (n + 0.5) * m.dx
+        rows.append(f"{xe:.3f} {y:.3f} {xe - 2 * m.dx:.3f} {y:.3f} 0.0002 -1.0")
+    rows.append(f"{xe:.3f} {m.nmax * m.dx * 0.9:.3f} {xe - 3 * m.dx:.3f} {m.nmax * m.dx * 0.9:.3f} 0.0001 1000.0")
+    with open(os.path.join(d, "sfincs.bdr"), "w") as f:
+        f.write("\n".join(rows) + "\n")
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        f.write(f"{'bdrfile':<20} = sfincs.bdr\n")
+    return d
+
+
+@pytest.mark.parametrize("subgrid", [False, True])
+@pytest.mark.parametrize("variant", [2, 5])
+def test_downstream_river_boundary_matches_f32_oracle(tmp_path, subgrid, variant):
+    """Downstream river boundary cells (kcs 5, sfincs_boundaries.f90:878-902)."""
+    from oracle.oracle import Oracle
+
+    d = _river(tmp_path, subgrid)
+    o = Oracle(d, "f32")
+    g = _model(d, variant)
+    done = 0
+    for n in (1, 1, 2, 6, 30, 60):
+        o.update(-1000.0, n)
+        g.step(n)
+        done += n
+        dzs = float(np.abs(o.get("zs") - g.get("zs")).max())
+        qx_o, qy_o = oracle_faces_to_cells(o, o.get("q"))
+        dq = max(float(np.abs(qx_o - g.get("qx")).max()), float(np.abs(qy_o - g.get("qy")).max()))
+        print(f"river subgrid={subgrid} v{variant} step {done}: max|dzs| {dzs:.3g} max|dq| {dq:.3g}")
+        assert g.scalars()["nt"] == o.scalars()["nt"]
+        assert dzs <= 2e-5 and dq <= 2e-5, (done, dzs, dq)
+    g.close()

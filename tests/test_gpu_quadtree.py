@@ -95,7 +95,25 @@ def _add_infiltration(d):
         f.write(f"{'qinffile':<20} = sfincs.qinf\n{'prcfile':<20} = sfincs.prcp\n")
 
 
-@pytest.mark.parametrize("subgrid,extra", [(False, "infiltration"), (True, "infiltration"),
+def _add_green_ampt(d):
+    """Green-Ampt infiltration (suction head, moisture deficit, conductivity per cell) under rain that stops."""
+    import os
+
+    from sfincs_b200 import bmi as B
+
+    n = int(B.layout(d, "qt_counts", 4)[0])
+    rng = np.random.default_rng(6)
+    for name, lo, hi in (("psi", 50.0, 300.0), ("sigma", 0.1, 0.4), ("ks", 5.0, 20000.0)):
+        rng.uniform(lo, hi, n).astype(np.float32).tofile(os.path.join(d, f"sfincs.{name}"))
+    np.savetxt(os.path.join(d, "sfincs.prcp"), np.array([[0.0, 40.0], [400.0, 40.0], [401.0, 0.0], [7200.0, 0.0]]),
+               fmt="%.6f")
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        for key, name in (("psifile", "psi"), ("sigmafile", "sigma"), ("ksfile", "ks"), ("prcfile", "prcp")):
+            f.write(f"{key:<20} = sfincs.{name}\n")
+
+
+@pytest.mark.parametrize("subgrid,extra", [(False, "green_ampt"), (True, "green_ampt"),
+                                           (False, "infiltration"), (True, "infiltration"),
                                            (False, None), (True, None), (False, "sources"), (True, "sources"),
                                            (False, "dams"), (True, "dams"), (False, "weirs"), (True, "weirs"),
                                            (False, "drainage"), (True, "drainage")])
@@ -109,6 +127,8 @@ def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, extra):
         _add_drainage(d)
     if extra == "infiltration":
         _add_infiltration(d)
+    if extra == "green_ampt":
+        _add_green_ampt(d)
     if extra == "weirs":
         _add_weirs(d)
         n = int(_oracle(d, "f32").get("nrstructures", 1)[0])

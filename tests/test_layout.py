@@ -6,6 +6,8 @@ per-cell flag bits.  These CPU tests check, cell by cell, that the flags encode
 exactly the reference's face activity (kcuv), advection mask (mask_adv),
 regular-cell mask (kcs), initial state and boundary-face lists.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -173,3 +175,53 @@ def test_weir_faces_match_oracle(tmp_path):
     bit = np.where(uv_dir == 0, F_UACT, F_VACT)
     assert np.array_equal((flags[uv_nm] & bit) > 0, np.isin(kcuv, (1, 6)))
     assert np.count_nonzero(kcuv == 3) == n
+
+
+@pytest.mark.parametrize("sub", [False, True], ids=["plain", "subgrid"])
+def test_inifile_sets_initial_levels(tmp_path, sub):
+    """A binary inifile (real*4 levels in cell order) sets zs = max(bed, ini)
+    as set_initial_conditions does; levels below the bed are raised to it."""
+    if sub:
+        m = synth.subgrid_regular(nmax=12, mmax=14, dx=500.0, P=4, seed=5, tstop=600.0, coast_x=2000.0)
+    else:
+        m = synth.plain_regular(nmax=12, mmax=14, dx=300.0, tstop=600.0, nbumps=2)
+    rng = np.random.default_rng(3)
+    m.zsini_field = rng.uniform(-4.0, 3.0, size=m.msk.shape).astype(np.float32)
+    d = m.write(str(tmp_path))
+    o = _oracle(d, "f32")
+    n = int(o.scalars()["np"])
+    zs = B.layout(d, "zs", n)
+    assert np.array_equal(zs, o.get("zs"))
+    ini = m.compact(m.zsini_field).astype(np.float64)
+    assert np.any(zs == ini) and np.any(zs > ini)  # some cells take the file's level, some the bed
+
+
+def test_netcdf_inifile_is_refused(tmp_path):
+    m = synth.plain_regular(nmax=6, mmax=7, dx=300.0, tstop=600.0, nbumps=1)
+    m.params["inifile"] = "sfincs_ini.nc"
+    d = m.write(str(tmp_path))
+    with pytest.raises(RuntimeError, match="inifile"):
+        B.layout(d, "counts", 10)
+
+
+@pytest.mark.parametrize("sub", [False, True], ids=["plain", "subgrid"])
+def test_downstream_river_faces_match_oracle(tmp_path, sub):
+    """msk 5 cells become boundary faces in the reference's order (the east
+    column here), and the model starts like the oracle."""
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_gpu_physics import _river
+
+    d = _river(tmp_path, sub)
+    o = _oracle(d, "f32")
+    s = o.scalars()
+    nb = int(s["nkcuv2"])
+    n = int(s["np"])
+    cnt = B.layout(d, "counts", 10)
+    assert nb > 0
+    kb = B.layout(d, "kb_cell", nb)
+    assert np.array_equal(kb, o.get("kb_cell", nb))
+    assert np.array_equal(B.layout(d, "zs", n), o.get("zs"))
+    o.update(-1000.0, 20)
+    assert np.isfinite(o.get("zs")).all()

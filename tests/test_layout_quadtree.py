@@ -54,3 +54,20 @@ def test_quadtree_mesh_matches_oracle(tmp_path, subgrid, nlev, walk_km):
         assert np.array_equal(B.layout(d, "zbuvmx", npuv), o.get("zbuvmx", npuv))
         act = kcuv > 0
         assert np.array_equal(B.layout(d, "gn2uv", npuv)[act], o.get("gn2uv", npuv)[act])
+
+
+@pytest.mark.parametrize("subgrid", [False, True])
+def test_quadtree_inifile(tmp_path, subgrid):
+    """A binary inifile on a quadtree mesh: levels in sfincs cell order."""
+    import os
+
+    d, m = _model(tmp_path, subgrid)
+    npc = int(B.layout(d, "qt_counts", 4)[0])
+    rng = np.random.default_rng(9)
+    rng.uniform(-3.0, 2.0, npc).astype(np.float32).tofile(os.path.join(d, "sfincs.ini"))
+    with open(os.path.join(d, "sfincs.inp"), "a") as f:
+        f.write(f"{'inifile':<20} = sfincs.ini\n")
+    o = _oracle(d)
+    zs = B.layout(d, "zs", npc)
+    assert np.array_equal(zs, o.get("zs", npc))
+    assert np.any(zs != B.layout(_model(tmp_path / "plain", subgrid)[0], "zs", npc))
