@@ -503,25 +503,43 @@ def run_serve(args, rank: int, world: int, local: int):
     specs = []
     for i in range(args.requests):
         cells = float(np.clip(rng.lognormal(np.log(0.5e6), 1.0), 0.1e6, 10e6))
-        side = int(round(np.sqrt(cells)))
-        specs.append(dict(nmax=side, mmax=side, dx=100.0, P=8, seed=5000 + 100 * rank + i, tstop=86400.0,
-                          surge_peak=float(rng.uniform(1.0, 4.0)), rain_mmh=float(rng.uniform(0.0, 80.0)),
-                          rain_hours=3.0, coast_x=0.15 * side * 100.0, t_peak=43200.0, width_h=6.0))
+        seed = 5000 + 100 * rank + i
+        if i % 3 == 2:  # every third request a 3-level quadtree mesh (about 4.7 cells per level-1 cell)
+            n1 = max(40, int(round(np.sqrt(cells / 4.7))))
+            specs.append(dict(kind="quadtree", nmax1=n1, mmax1=n1, dx1=400.0, nlev=3, bands=(4000.0, 2000.0), P=4,
+                              seed=seed, tstop=86400.0, subgrid=True, walk_km=9000.0 * (n1 / 800.0) ** 2,
+                              tide_amp=float(rng.uniform(0.5, 2.0)), wind_speed=float(rng.uniform(0.0, 30.0))))
+        else:
+            side = int(round(np.sqrt(cells)))
+            specs.append(dict(nmax=side, mmax=side, dx=100.0, P=8, seed=seed, tstop=86400.0,
+                              surge_peak=float(rng.uniform(1.0, 4.0)), rain_mmh=float(rng.uniform(0.0, 80.0)),
+                              rain_hours=3.0, coast_x=0.15 * side * 100.0, t_peak=43200.0, width_h=6.0))
     dirs = ensemble.generate(specs, log=log)
-    # calibration: device throughput on a mid-size request -> service-time estimate
-    mid = int(np.argsort([s["nmax"] ** 2 for s in specs])[len(specs) // 2])
-    g = Model(dirs[mid])
-    g.step(64)
-    st = torch.cuda.ExternalStream(g.stream)
+    # calibration: device throughput and dt of a mid-size request of each kind -> service-time estimates
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    g.issue(128)
-    e1.record(st)
-    e1.synchronize()
-    rate = g.scalars()["np"] * 128 / (e0.elapsed_time(e1) / 1e3)
-    dt_est = g.scalars()["dt"]
-    g.close()
-    service = np.array([s["nmax"] * s["mmax"] * (86400.0 / dt_est) / rate for s in specs])
+    kinds = [s.get("kind", "subgrid") for s in specs]
+    cal = {}
+    for kind in sorted(set(kinds)):
+        idx = [i for i, k in enumerate(kinds) if k == kind]
+        sizes = [specs[i]["nmax"] * specs[i]["mmax"] if kind != "quadtree" else specs[i]["nmax1"] ** 2 for i in idx]
+        mid = idx[int(np.argsort(sizes)[len(idx) // 2])]
+        g = Model(dirs[mid])
+        g.step(64)
+        st = torch.cuda.ExternalStream(g.stream)
+        e0.record(st)
+        g.issue(128)
+        e1.record(st)
+        e1.synchronize()
+        cal[kind] = (g.scalars()["np"] * 128 / (e0.elapsed_time(e1) / 1e3), g.scalars()["dt"])
+        g.close()
+    cells_of = {}
+    for i, d in enumerate(dirs):
+        from sfincs_b200.serve import Prepared
+
+        pr = Prepared(d)
+        cells_of[i] = pr.cells
+        pr.release()
+    service = np.array([cells_of[i] * (86400.0 / cal[kinds[i]][1]) / cal[kinds[i]][0] for i in range(len(specs))])
     lam = 0.8 / service.mean()
     arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(specs)))
     arrivals -= arrivals[0]
@@ -531,6 +549,20 @@ def run_serve(args, rank: int, world: int, local: int):
     barrier(world)
     out = srv.serve(reqs, fetch=("zsmax",))
     srv.close()
+    torch.cuda.empty_cache()
+    # each request alone on the idle device, for the cost of sharing it
+    alone = {}
+    for r in reqs:
+        g = Model(r.model_dir)
+        st = torch.cuda.ExternalStream(g.stream)
+        e0.record(st)
+        g.run(g.scalars()["t1"])
+        e1.record(st)
+        e1.synchronize()
+        alone[r.rid] = e0.elapsed_time(e1) / 1e3
+        g.close()
+    served = {x.rid: x.latency_s for x in out["results"]}
+    slow = np.array([served[k] / alone[k] for k in alone])
     makespan = max_over_ranks(out["makespan_s"], world)
     value = world * len(reqs) / makespan * 3600.0
     cells = [r.cells for r in out["results"]]
@@ -540,16 +572,22 @@ def run_serve(args, rank: int, world: int, local: int):
         "steps": int(sum(r.steps for r in out["results"])), "warmup": 0, "ms_per_step": None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 time and volume)",
         "data": "synthetic",
-        "config": {"workload": "served forecast stream: subgrid regular grids, lognormal sizes (median 0.5M, "
-                               "clipped 0.1M..10M cells) at 100 m, P=8, surge U(1,4) m, rain U(0,80) mm/h 3 h, "
-                               "24 h simulated each; Poisson arrivals at ~80 % estimated load",
-                   "requests_per_rank": len(reqs), "cells_min": int(min(cells)), "cells_max": int(max(cells)),
+        "config": {"workload": "served forecast stream: lognormal sizes (median 0.5M, clipped 0.1M..10M cells); "
+                               "two of three requests subgrid regular grids at 100 m (P=8, surge U(1,4) m, rain "
+                               "U(0,80) mm/h 3 h), one of three 3-level quadtree meshes (400 m -> 100 m, 10-level "
+                               "subgrid tables, tide U(0.5,2) m, onshore wind U(0,30) m/s); 24 h simulated each; "
+                               "Poisson arrivals at ~80 % estimated load",
+                   "requests_per_rank": len(reqs), "quadtree_requests": int(sum(k == "quadtree" for k in kinds)),
+                   "cells_min": int(min(cells)), "cells_max": int(max(cells)),
                    "arrival_rate_per_s": lam, "service_estimate_s": float(service.mean()),
-                   "parallelism": f"replicas x{world} (one request stream per rank)",
-                   "quadtree_requests": "not served: quadtree meshes are not built in this core"},
+                   "parallelism": f"replicas x{world} (one request stream per rank)"},
         "gpu_launches": None,
         "latency_p50_s": out["latency_p50_s"], "latency_p99_s": out["latency_p99_s"],
         "latency_max_s": out["latency_max_s"], "makespan_s": makespan, "mean_running": out["mean_running"],
+        "alone_p50_s": float(np.percentile(list(alone.values()), 50)),
+        "alone_p99_s": float(np.percentile(list(alone.values()), 99)),
+        "served_over_alone_mean": float(slow.mean()), "served_over_alone_p99": float(np.percentile(slow, 99)),
+        "alone_sum_s": float(sum(alone.values())),
         "cell_updates_per_s": cu / out["makespan_s"],
         "errors": int(sum(1 for r in out["results"] if r.error)),
     }
@@ -564,7 +602,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="subgrid", choices=sorted(WORKLOADS) + ["ensemble", "serve"])
-    ap.add_argument("--requests", type=int, default=24, help="requests per rank (--workload serve)")
+    ap.add_argument("--requests", type=int, default=30, help="requests per rank (--workload serve)")
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--full-run", type=int, default=1, help="also time the whole simulated period (rank 0)")

@@ -93,7 +93,10 @@ SFG_API int get_last_bmi_error(char* msg);
 SFG_API int initialize_config(const char* model_dir);
 /* Copy-based access: "zs" (double[np]), "zsmax","qext" (float[np]),
  * "z_volume" (double[np], subgrid), "qx","qy","uvx","uvy" (float[np]: flux /
- * velocity of each cell's right (x) or upper (y) face, 0 where no face).
+ * velocity of each cell's right (x) or upper (y) face, 0 where no face);
+ * with their store switches on, "vmax","qmax","twet","tzsmax","cumprcp",
+ * "cuminf" (float[np]: maximum velocity and flux, wet duration, time of the
+ * maximum level, cumulative rain and infiltration).
  * bytes must equal the array size. */
 SFG_API int get_var(const char* name, void* dst, size_t bytes);
 SFG_API int set_var(const char* name, const void* src, size_t bytes);

@@ -200,6 +200,30 @@ static long time_difference(const std::string& a, const std::string& b) {
   return (j2 - j1) * 86400 + (y[3] * 3600 + y[4] * 60 + y[5]) - (x[3] * 3600 + x[4] * 60 + x[5]);
 }
 
+// compute_time_in_seconds: sfincs_spiderweb.f90:409-458.  "TIME = v unit since
+// yyyy-mm-dd HH:MM:SS": v times the unit, minus (tref - that date), truncated to
+// whole seconds, in the reference's real*4 / integer*8 steps.
+static float meteo_time_seconds(const std::string& line, const std::string& trefstr) {
+  const size_t j = line.find('='), jsince = line.find("since");
+  size_t junit = std::string::npos;
+  long ifac = 1;
+  const char* units[4] = {"seconds", "minutes", "hours", "days"};
+  const long facs[4] = {1, 60, 3600, 86400};
+  for (int u = 0; u < 4 && junit == std::string::npos; u++) {
+    junit = line.find(units[u]);
+    ifac = facs[u];
+  }
+  if (j == std::string::npos || jsince == std::string::npos || junit == std::string::npos)
+    throw std::runtime_error("oracle: bad TIME line in meteo file: " + line);
+  const float tim = std::strtof(line.substr(j + 1, junit - j - 1).c_str(), nullptr);
+  const std::string d = line.substr(jsince + 6, 19);  // yyyy-mm-dd HH:MM:SS
+  const std::string datespw = d.substr(0, 4) + d.substr(5, 2) + d.substr(8, 2) + " " + d.substr(11, 2) +
+                              d.substr(14, 2) + d.substr(17, 2);
+  const long dts = time_difference(datespw, trefstr);
+  const float v = tim * (float)ifac - (float)dts;
+  return (float)(long long)v;
+}
+
 static std::vector<std::vector<double>> read_ascii_table(const std::string& path) {
   std::ifstream f(path);
   if (!f) throw std::runtime_error("cannot open " + path);
@@ -299,6 +323,24 @@ struct Model {
   long ntwnd = 0, itwndlast = 1, ntprcp = 0, itprcplast = 1;
   F1<float> twnd, wndmag, wnddir, tprcpt, tprcpv, cdval;
   F1<float> tauwu, tauwv, prcp, netprcp, qext, qinffield, qinfmap, cumprcp, cuminf;
+  // gridded meteo on equidistant grids (ASCII amu/amv/amp/ampr, sfincs_meteo.f90:5-446, 802-1243):
+  // the raw fields, the two fields of the current update window on the cells,
+  // and the per-step values
+  struct AmGrid {
+    int nt = 0, nrows = 0, ncols = 0;
+    float x_ll = 0, y_ll = 0, dx = 0, dy = 0;
+    std::vector<float> times, v[2];  // v[q][((it - 1) * nrows + irow - 1) * ncols + icol - 1]
+    float at(int q, int it, int irow, int icol) const {
+      return v[q][((size_t)(it - 1) * nrows + (irow - 1)) * ncols + (icol - 1)];
+    }
+  };
+  AmGrid amuv, amp, ampr;
+  std::string amufile, amvfile, ampfile, amprfile;
+  bool meteo3d = false, ampr_block = true;
+
+  float dtwindupd = 1800.0f, twindupd = 0.0f, meteo_t0 = 0.0f, meteo_t1 = 0.0f, factor_wind = 1.0f,
+        factor_pres = 1.0f, factor_prcp = 1.0f;
+  F1<float> tauwu0, tauwu1, tauwv0, tauwv1, patm, patm0, patm1, prcp0, prcp1, patmb;
   // infiltration models with state (sfincs_infiltration.f90:8-600): curve number
   // with recovery (scs_*), Green-Ampt (GA_*), Horton (horton_*), recovery clock
   F1<float> scs_Se, scs_P1, scs_F1, scs_S1, ksfield, inf_kr, rain_T1, GA_head, GA_sigma, GA_sigma_max, GA_F, GA_Lu,
@@ -379,6 +421,17 @@ struct Model {
     nuviscdim = in.real("nuvisc", 0.01f);
     viscosity = in.logical("viscosity", false);
     spinup_meteo = in.integer("spinup_meteo", 0) != 0;
+    amufile = in.str("amufile", "none");
+    amvfile = in.str("amvfile", "none");
+    ampfile = in.str("ampfile", "none");
+    amprfile = in.str("amprfile", "none");
+    dtwindupd = in.real("dtwnd", 1800.0f);
+    ampr_block = in.integer("amprblock", 1) != 0;
+    factor_wind = in.real("factor_wind", 1.0f);
+    factor_pres = in.real("factor_pres", 1.0f);
+    factor_prcp = in.real("factor_prcp", 1.0f);
+    if (in.real("waveage", -999.0f) > 0.0f || in.integer("radstr", 0) == 1)
+      throw std::runtime_error("oracle: wave-age drag and radiation stresses are not restated");
     advstr = in.str("advection_scheme", "upw1");
     btrelax = in.real("btrelax", 3600.0f);
     wiggle_suppression = in.logical("wiggle_suppression", true);
@@ -465,9 +518,11 @@ struct Model {
   // initialize_processes: sfincs_domain.f90:59-140 (time-series meteo only)
   void initialize_processes() {
     use_quadtree = qtrfile.substr(0, 4) != "none";
-    wind = wndfile.substr(0, 4) != "none";
-    precip = prcpfile.substr(0, 4) != "none";
-    patmos = false;
+    auto has = [](const std::string& f) { return f.substr(0, 4) != "none"; };
+    wind = has(wndfile) || has(amufile);
+    patmos = has(ampfile) && baro == 1;
+    precip = has(prcpfile) || has(amprfile);
+    meteo3d = has(amufile) || has(amprfile) || has(ampfile);
   }
 
   // make_quadtree_from_indices: sfincs_quadtree.F90:445-669
@@ -1347,12 +1402,11 @@ struct Model {
       rd(&rsttype, 4);
       rd(&rdummy, 4);
       if (rsttype >= 1 && rsttype <= 6) {
-        if (rsttype >= 4) throw std::runtime_error("oracle: restart flavours 4-6 are not restated");
         inizs4.resize((size_t)np);
         rd(&rdummy, 4);
         rd(inizs4.data(), 4 * (size_t)np);
         rd(&rdummy, 4);
-        if (rsttype == 1 || rsttype == 2) {
+        if (rsttype != 3) {
           iniq.resize((size_t)(npuv + ncuv + 1));
           rd(&rdummy, 4);
           rd(iniq.data(), 4 * iniq.size());
@@ -1361,6 +1415,19 @@ struct Model {
           for (long ib = 1; ib <= nkcuv2; ib++) rd(&uvmean(ib), 4);
           rd(&rdummy, 4);
         }
+        // the infiltration state (:237-258); the arrays exist only with that method
+        auto state = [&](F1<float>& a, const char* what) {
+          if (!a.allocated()) throw std::runtime_error(std::string("oracle: restart file carries ") + what +
+                                                       " but the model does not use that infiltration method");
+          rd(&rdummy, 4);
+          rd(&a(1), 4 * (size_t)np);
+        };
+        if (rsttype == 4) state(scs_Se, "scs_Se");
+        if (rsttype == 5) {
+          state(GA_sigma, "GA_sigma");
+          state(GA_F, "GA_F");
+        }
+        if (rsttype == 6) state(rain_T1, "rain_T1");
       }
     }
     for (long nm = 1; nm <= np; nm++) {
@@ -1372,10 +1439,8 @@ struct Model {
     }
     if (wiggle_suppression)
       for (long nm = 1; nm <= np; nm++) zs0(nm) = (T)zs(nm);
-    for (long ic = 1; ic <= ncuv; ic++) {
-      q(cuv_index_uv(ic)) = (T)0.5f * (q(cuv_index_uv1(ic)) + q(cuv_index_uv2(ic)));
-      uv(cuv_index_uv(ic)) = (T)0.5f * (uv(cuv_index_uv1(ic)) + uv(cuv_index_uv2(ic)));
-    }
+    // combined uv points keep q = uv = 0 until the first momentum step (a
+    // restart sets the npuv regular points only, :110-113)
     if (store_maximum_waterlevel) zsmax.fill((T)-999.0f);
     if (store_maximum_velocity) vmax.fill((T)-999.0f);
     if (store_twet) twet.fill((T)0.0f);
@@ -1408,11 +1473,24 @@ struct Model {
     if (wind) {
       tauwu.alloc(np);
       tauwv.alloc(np);
+      tauwu0.alloc(np);
+      tauwu1.alloc(np);
+      tauwv0.alloc(np);
+      tauwv1.alloc(np);
     }
     if (precip) {
       prcp.alloc(np);
       netprcp.alloc(np);
+      prcp0.alloc(np);
+      prcp1.alloc(np);
     }
+    if (patmos) {  // sfincs_domain.f90:2354-2366
+      patm.alloc(np);
+      patm0.alloc(np);
+      patm1.alloc(np);
+      if (pavbnd > 0.0f) patmb.alloc(std::max(ngbnd, 1L), 101200.0f);
+    }
+    twindupd = t0;  // sfincs_lib.f90:290
     if (use_qext) qext.alloc(np);
     if (subgrid) {
       z_volume.alloc(np);
@@ -1916,7 +1994,151 @@ struct Model {
   }
 
   // read_meteo_data (time-series part) + Cd table: sfincs_meteo.f90:247-327
+  // read_amuv_dimensions + read_amuv_file: sfincs_spiderweb.f90:135-230, 320-403.
+  // Header keys up to the first line that starts with TIME, then per time a
+  // TIME line and nrows x ncols values (list-directed), rows from the top.
+  void read_am_file(const std::string& file, AmGrid& g, int q) {
+    std::ifstream fin(path(file));
+    if (!fin) throw std::runtime_error("oracle: cannot open " + file);
+    std::vector<std::string> lines;
+    for (std::string l; std::getline(fin, l);) {
+      if (!l.empty() && l.back() == '\r') l.pop_back();
+      lines.push_back(l);
+    }
+    size_t i = 0;
+    std::map<std::string, std::string> kv;
+    for (; i < lines.size() && lines[i].compare(0, 4, "TIME") != 0; i++) {
+      size_t e = lines[i].find('=');
+      if (e == std::string::npos) continue;
+      std::string k = lines[i].substr(0, e), v = lines[i].substr(e + 1);
+      k.erase(0, k.find_first_not_of(" \t"));
+      k.erase(k.find_last_not_of(" \t") + 1);
+      for (auto& ch : k) ch = (char)std::tolower(ch);
+      kv[k] = v;
+    }
+    auto num = [&](const char* k) {
+      auto it = kv.find(k);
+      return it == kv.end() ? 0.0 : std::strtod(it->second.c_str(), nullptr);
+    };
+    const int ncols = (int)num("n_cols"), nrows = (int)num("n_rows");
+    const float x_ll = (float)num("x_llcorner"), y_ll = (float)num("y_llcorner"), ddx = (float)num("dx"),
+                ddy = (float)num("dy");
+    if (ncols < 1 || nrows < 1) throw std::runtime_error("oracle: meteo file without n_cols / n_rows: " + file);
+    std::vector<float> times, vals;
+    while (i < lines.size()) {
+      if (lines[i].compare(0, 4, "TIME") != 0) {
+        i++;
+        continue;
+      }
+      times.push_back(meteo_time_seconds(lines[i], trefstr));
+      i++;
+      size_t need = (size_t)nrows * ncols, got = 0;
+      while (got < need && i < lines.size()) {
+        std::istringstream ls(lines[i++]);
+        double x;
+        while (got < need && ls >> x) {
+          vals.push_back((float)x);
+          got++;
+        }
+      }
+      if (got < need) throw std::runtime_error("oracle: truncated meteo file " + file);
+    }
+    if (q == 0) {
+      g.nt = (int)times.size();
+      g.nrows = nrows;
+      g.ncols = ncols;
+      g.x_ll = x_ll;
+      g.y_ll = y_ll;
+      g.dx = ddx;
+      g.dy = ddy;
+      g.times = times;
+    }
+    g.v[q] = vals;
+  }
+
+  // The window fields (update_amuv_data / update_amp_data / update_ampr_data,
+  // sfincs_meteo.f90:802-1243): for each end of the window the two records
+  // around it, blended in time on the meteo grid, then bilinear on each cell.
+  // kind 0: wind stress from amu/amv, 1: pressure, 2: rain.
+  void update_am_window(const AmGrid& g, int kind) {
+    for (int itw = 1; itw <= 2; itw++) {
+      float meteo_t = itw == 1 ? meteo_t0 : meteo_t1;
+      meteo_t = std::max(meteo_t, g.times[0]);
+      meteo_t = std::min(meteo_t, g.times[g.nt - 1]);
+      int itw0 = 1;
+      for (int it = 1; it <= g.nt; it++)
+        if (g.times[it - 1] <= meteo_t) itw0 = it;
+      const int itw1 = std::min(itw0 + 1, g.nt);
+      meteo_t = std::min(meteo_t, g.times[itw1 - 1]);
+      float twfac = (meteo_t - g.times[itw0 - 1]) / std::max(g.times[itw1 - 1] - g.times[itw0 - 1], 1.0e-6f);
+      if (kind == 2 && ampr_block) twfac = 0.0f;
+      auto v01 = [&](int q, int irow, int icol) {
+        return g.at(q, itw0, irow, icol) * (1.0f - twfac) + g.at(q, itw1, irow, icol) * twfac;
+      };
+      const float yul = g.y_ll + (float)(g.nrows - 1) * g.dy + 0.5f * g.dy;
+      const float xll = g.x_ll + 0.5f * g.dx;
+      for (long nm = 1; nm <= np; nm++) {
+        const float x = z_xz(nm), y = z_yz(nm);
+        const int iy = (int)((yul - y) / g.dy) + 1;
+        const int ind1[4] = {iy, iy, iy + 1, iy + 1};
+        const float dj1 = (yul - (float)(iy - 1) * g.dy - y) / g.dy;
+        const int ix = (int)((x - xll) / g.dx) + 1;
+        const int ind2[4] = {ix, ix + 1, ix + 1, ix};
+        const float di1 = (x - (xll + (float)(ix - 1) * g.dx)) / g.dx;
+        if (iy <= 1 || iy >= g.nrows || ix <= 0 || ix >= g.ncols) {  // outside the meteo grid
+          if (kind == 0) {
+            (itw == 1 ? tauwu0 : tauwu1)(nm) = 0.0f;
+            (itw == 1 ? tauwv0 : tauwv1)(nm) = 0.0f;
+          } else if (kind == 1) {
+            (itw == 1 ? patm0 : patm1)(nm) = gapres;
+          } else {
+            (itw == 1 ? prcp0 : prcp1)(nm) = 0.0f;
+          }
+          continue;
+        }
+        const float f[4] = {(1.0f - di1) * (1.0f - dj1), di1 * (1.0f - dj1), di1 * dj1, (1.0f - di1) * dj1};
+        if (kind == 0) {
+          float wup = 0.0f, wvp = 0.0f;
+          for (int ip = 0; ip < 4; ip++) {
+            wup = wup + f[ip] * v01(0, ind1[ip], ind2[ip]);
+            wvp = wvp + f[ip] * v01(1, ind1[ip], ind2[ip]);
+          }
+          const float vmag = std::sqrt(wup * wup + wvp * wvp);
+          const long icd = std::min(std::max((long)(vmag * 10.0f) + 1, 1L), 1000L);
+          const float cd = cdval(icd);
+          (itw == 1 ? tauwu0 : tauwu1)(nm) = vmag * (cosrot * wup + sinrot * wvp) * rhoa * cd / rhow;
+          (itw == 1 ? tauwv0 : tauwv1)(nm) = vmag * (-sinrot * wup + cosrot * wvp) * rhoa * cd / rhow;
+        } else {
+          float pr = 0.0f;
+          for (int ip = 0; ip < 4; ip++) pr = pr + f[ip] * v01(0, ind1[ip], ind2[ip]);
+          if (kind == 1)
+            (itw == 1 ? patm0 : patm1)(nm) = pr;
+          else
+            (itw == 1 ? prcp0 : prcp1)(nm) = pr / (float)(1000 * 3600);
+        }
+      }
+    }
+  }
+
   void read_meteo_data() {
+    // gridded fields (sfincs_meteo.f90:146-245) with the enhancement factors (:330-380)
+    if (amufile.substr(0, 4) != "none") {
+      read_am_file(amufile, amuv, 0);
+      read_am_file(amvfile, amuv, 1);
+      if (factor_wind != 1.0f)
+        for (int q = 0; q < 2; q++)
+          for (auto& x : amuv.v[q]) x = factor_wind * x;
+    }
+    if (amprfile.substr(0, 4) != "none") {
+      read_am_file(amprfile, ampr, 0);
+      if (factor_prcp != 1.0f)
+        for (auto& x : ampr.v[0]) x = factor_prcp * x;
+    }
+    if (ampfile.substr(0, 4) != "none") {
+      read_am_file(ampfile, amp, 0);
+      if (factor_pres != 1.0f)
+        for (auto& x : amp.v[0]) x = gapres - factor_pres * (gapres - x);
+    }
     if (wndfile.substr(0, 4) != "none") {
       auto tb = read_ascii_table(path(wndfile));
       ntwnd = (long)tb.size();
@@ -2105,8 +2327,53 @@ struct Model {
 
   // ============================================================ time step
   // update_meteo_forcing (time-series part): sfincs_meteo.f90:1246-1558
+  // update_meteo_fields: sfincs_meteo.f90:1561-1624 (ASCII gridded meteo)
+  void update_meteo_fields() {
+    if (amufile.substr(0, 4) != "none") update_am_window(amuv, 0);
+    if (ampfile.substr(0, 4) != "none" && patmos) update_am_window(amp, 1);
+    if (amprfile.substr(0, 4) != "none") update_am_window(ampr, 2);
+  }
+
   void update_meteo_forcing(double tt, float dtt) {
-    if (wind) {  // update_wind_forcing_from_timeseries :1445-1508
+    if (meteo3d) {  // :1264-1417
+      const float twfact = (float)((tt - (double)meteo_t0) / (double)(meteo_t1 - meteo_t0));
+      const float onemintwfact = 1.0f - twfact;
+      for (long nm = 1; nm <= np; nm++) {
+        if (wind) {
+          tauwu(nm) = tauwu0(nm) * onemintwfact + tauwu1(nm) * twfact;
+          tauwv(nm) = tauwv0(nm) * onemintwfact + tauwv1(nm) * twfact;
+        }
+        if (patmos) patm(nm) = patm0(nm) * onemintwfact + patm1(nm) * twfact;
+        if (precip) {
+          prcp(nm) = prcp0(nm) * onemintwfact + prcp1(nm) * twfact;
+          if (prcp(nm) < 0.0f) {  // no negative rain on a dry cell
+            if (subgrid ? z_volume(nm) <= 0.0 : (double)zs(nm) <= (double)zb(nm)) prcp(nm) = 0.0f;
+          }
+          netprcp(nm) = prcp(nm);
+          if (store_cumulative_precipitation) cumprcp(nm) = cumprcp(nm) + prcp(nm) * dtt;
+        }
+      }
+      if (tt < (double)(tspinup - 1.0e-3f) && spinup_meteo) {  // :1349-1398
+        const float smfac = (float)((tt - (double)t0) / (double)(tspinup - t0));
+        const float oneminsmfac = 1.0f - smfac;
+        for (long nm = 1; nm <= np; nm++) {
+          if (wind) {
+            tauwu(nm) = tauwu(nm) * smfac;
+            tauwv(nm) = tauwv(nm) * smfac;
+          }
+          if (patmos) patm(nm) = patm(nm) * smfac + gapres * oneminsmfac;
+          if (precip) {
+            netprcp(nm) = netprcp(nm) * smfac;
+            if (netprcp(nm) < 0.0f) {
+              if (subgrid ? z_volume(nm) <= 0.0 : (double)zs(nm) <= (double)zb(nm)) netprcp(nm) = 0.0f;
+            }
+          }
+        }
+      }
+      if (patmos && pavbnd > 0.0f)  // :1400-1417
+        for (long ib = 1; ib <= ngbnd; ib++) patmb(ib) = patm(nmindbnd(ib));
+    }
+    if (wind && wndfile.substr(0, 4) != "none") {  // update_wind_forcing_from_timeseries :1445-1508
       for (long itw = itwndlast; itw <= ntwnd; itw++) {
         if ((double)twnd(itw) > tt) {
           long i0 = std::max(itw - 1, 1L);  // out-of-range guard: series must cover t
@@ -2134,7 +2401,7 @@ struct Model {
         }
       }
     }
-    if (precip) {  // update_precipitation_from_timeseries :1510-1558
+    if (precip && prcpfile.substr(0, 4) != "none") {  // update_precipitation_from_timeseries :1510-1558
       long itp;
       for (itp = itprcplast; itp <= ntprcp; itp++)
         if ((double)tprcpt(itp) > tt) break;
@@ -2298,6 +2565,8 @@ struct Model {
                          zst_bnd(ind2_bnd_gbp(ib)) * (1.0f - fac_bnd_gbp(ib)));
         else
           zst = (double)zst_bnd(1);
+        if (patmos && pavbnd > 1.0f)  // barometric correction (sfincs_boundaries.f90:820-826)
+          zst = zst + (double)((pavbnd - patmb(ib)) / (rhow * 9.81f));
         float zsetup = 0.0f, zig = 0.0f;
         if (tt < (double)(tspinup - 1.0e-3f)) {
           float smfac = (float)(1.0 - (tt - (double)t0) / (double)(tspinup - t0));
@@ -2657,6 +2926,8 @@ struct Model {
           else
             frc = frc + tw * hu * (T)4;
         }
+        if (patmos)  // atmospheric pressure gradient (sfincs_momentum.f90:585-589)
+          frc = frc + hu * ((T)patm(nm) - (T)patm(nmu)) * dxuvinv / (T)rhow;
         T qfr;
         const T cr = CORE ? (T)core_cube_root((float)hu) : (T)0;  // the core's hu**(1/3)
         if (kfuv(ip) == 0) {
@@ -2846,7 +3117,15 @@ struct Model {
       float dtchk = alfa * min_dt;
       t = t + (double)dt;
       dtavg = dtavg + dt;
+      bool update_meteo = false;  // sfincs_lib.f90:493-503
+      if (meteo3d && t >= (double)twindupd) {
+        meteo_t0 = twindupd;
+        meteo_t1 = twindupd + dtwindupd;
+        twindupd = twindupd + dtwindupd;
+        update_meteo = true;
+      }
       if (wind || patmos || precip) {
+        if (meteo3d && update_meteo) update_meteo_fields();
         update_meteo_forcing(t, dt);
         if (infiltration) update_infiltration_map(dt);
       }

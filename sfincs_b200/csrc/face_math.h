@@ -85,6 +85,22 @@ __device__ __forceinline__ float power7over3(float hu, const float* __restrict__
   return __ldg(x73 + (k - 1) * 1000 + (j - 1));
 }
 
+// Wind stress and pressure difference of a face between storage cells c (nm)
+// and cu (nmu) this step: the uniform wind of a time series unless the wind
+// comes from a gridded field (then the value of cell nm), and patm(nm) -
+// patm(nmu) from the gridded pressure.
+__device__ __forceinline__ void face_meteo(const ScnDev& S, const StepVals& sv, int dir, int64_t c, int64_t cu,
+                                           float& tauw, float& dpatm) {
+  tauw = dir == 0 ? sv.twu : sv.twv;
+  dpatm = 0.0f;
+  if (S.wind_field | S.patmos) {
+    const StepState& st = *S.st;
+    const MeteoW w = meteo_weights(S, st.t, st.meteo_t0, st.meteo_t1);
+    if (S.wind_field) tauw = cell_tau(S, c, dir, w);
+    if (S.patmos) dpatm = cell_patm(S, c, w) - cell_patm(S, cu, w);
+  }
+}
+
 // Grid spacing of one face (sfincs_momentum.f90:205-313): across the face
 // (dxuv), along it (dyuv), their squared inverses for viscosity, and the
 // viscosity coefficient of the face's refinement level.
@@ -106,12 +122,15 @@ struct FaceV {
 // 1 / (max(sqrt(max g*hu), max |uv|) * dxuvinv) over faces of equal spacing,
 // bit for bit: callers fold g*hu and |uv| and take one square root and one
 // division per reduction instead of per face.
+// tauw: the wind stress of the face's cell nm in the face direction (uniform
+// from a time series, or the cell's value of the gridded field); dpatm:
+// patm(nm) - patm(nmu) when atmospheric pressure is on.
 template <bool SG>
 __device__ __forceinline__ float face_flux_geo(const ScnDev& S, const StepVals& st, int dir, bool adv_on,
                                                bool theta_on, const FaceGeo& geo, uint8_t kf, float zs_nm,
                                                float zs_nmu, float hu, float gnavg2, float phi, const FaceV& a,
-                                               bool dry_nm, bool dry_nmu, float zd_nm, float zd_nmu, float& q_out,
-                                               float& uv_out) {
+                                               bool dry_nm, bool dry_nmu, float zd_nm, float zd_nmu, float tauw,
+                                               float dpatm, float& q_out, float& uv_out) {
   const float dxuvinv = geo.dxuvinv, dyuvinv = geo.dyuvinv, dxuv2inv = geo.dxuv2inv, dyuv2inv = geo.dyuv2inv;
   float dzdx;
   if (S.slopelim < 9999.0f)
@@ -167,13 +186,13 @@ __device__ __forceinline__ float face_flux_geo(const ScnDev& S, const StepVals& 
       frc = frc - S.fcorio * hu * a.vu;
   }
   if (S.wind) {
-    const float tauw = dir == 0 ? st.twu : st.twv;
     const float hwet = hu / phi;
     if (hwet > 0.25f)
       frc = frc + phi * tauw;
     else
       frc = frc + tauw * hu * 4.0f;
   }
+  if (S.patmos) frc = frc + hu * dpatm * dxuvinv / S.rhow;  // atmospheric pressure (:585-589)
   // hu**(1.0/3.0) (:616, :673) as a cube root; the real*4 exponent 1.0/3.0 is
   // 0.333333343, so the two differ by a factor hu**(1e-8), under one ulp for
   // 1e-3 <= hu <= 1e3

@@ -181,18 +181,36 @@ struct ModelHandle {
     const ScnDev& D = dev->dev();
     const StepState st = runner->read_state(0);
     const int p = latest(st);
-    const size_t NA = (size_t)H.p.nalloc;
-    std::vector<float> zsd(NA), qu(NA), qv(NA), um((size_t)std::max(H.p.nkcuv2, 1));
-    check_cuda(cudaMemcpy(zsd.data(), D.zs, NA * 4, cudaMemcpyDeviceToHost), "restart zs");
-    check_cuda(cudaMemcpy(qu.data(), D.qu[p], NA * 4, cudaMemcpyDeviceToHost), "restart qu");
-    check_cuda(cudaMemcpy(qv.data(), D.qv[p], NA * 4, cudaMemcpyDeviceToHost), "restart qv");
-    if (H.p.nkcuv2 > 0)
-      check_cuda(cudaMemcpy(um.data(), D.uvmean, (size_t)H.p.nkcuv2 * 4, cudaMemcpyDeviceToHost), "restart uvmean");
-    std::vector<float> zs4((size_t)H.np), q((size_t)H.npuv + 1, 0.0f), uvm(H.kb_bface.size(), 0.0f);
-    for (long long i = 0; i < H.np; i++) zs4[(size_t)i] = zsd[(size_t)H.cmp_off[i]];
-    for (size_t f = 0; f < H.face_off.size(); f++) q[f] = (H.face_dir[f] == 0 ? qu : qv)[(size_t)H.face_off[f]];
-    for (size_t ib = 0; ib < H.kb_bface.size(); ib++)
-      if (H.kb_bface[ib] >= 0) uvm[ib] = um[(size_t)H.kb_bface[ib]];
+    const size_t NA = H.p.quadtree ? (size_t)H.np : (size_t)H.p.nalloc;  // storage length of a cell array
+    std::vector<float> zs4((size_t)H.np), q, uvm;
+    std::vector<int32_t> ident;  // quadtree: cells are stored in the reference's order
+    const std::vector<int32_t>* cells = &H.cmp_off;
+    if (H.p.quadtree) {
+      // zs, q of the uv points, combined points and dummy, uvmean: all in the reference's order already
+      const size_t NQ = (size_t)(H.npuv + H.p.ncuv + 1);
+      q.resize(NQ);
+      uvm.resize((size_t)H.p.nkcuv2);
+      check_cuda(cudaMemcpy(zs4.data(), D.zs, (size_t)H.np * 4, cudaMemcpyDeviceToHost), "restart zs");
+      check_cuda(cudaMemcpy(q.data(), D.qu[p], NQ * 4, cudaMemcpyDeviceToHost), "restart q");
+      if (H.p.nkcuv2 > 0)
+        check_cuda(cudaMemcpy(uvm.data(), D.uvmean, uvm.size() * 4, cudaMemcpyDeviceToHost), "restart uvmean");
+      ident.resize((size_t)H.np);
+      for (long long i = 0; i < H.np; i++) ident[(size_t)i] = (int32_t)i;
+      cells = &ident;
+    } else {
+      std::vector<float> zsd(NA), qu(NA), qv(NA), um((size_t)std::max(H.p.nkcuv2, 1));
+      check_cuda(cudaMemcpy(zsd.data(), D.zs, NA * 4, cudaMemcpyDeviceToHost), "restart zs");
+      check_cuda(cudaMemcpy(qu.data(), D.qu[p], NA * 4, cudaMemcpyDeviceToHost), "restart qu");
+      check_cuda(cudaMemcpy(qv.data(), D.qv[p], NA * 4, cudaMemcpyDeviceToHost), "restart qv");
+      if (H.p.nkcuv2 > 0)
+        check_cuda(cudaMemcpy(um.data(), D.uvmean, (size_t)H.p.nkcuv2 * 4, cudaMemcpyDeviceToHost), "restart uvmean");
+      q.assign((size_t)H.npuv + 1, 0.0f);
+      uvm.assign(H.kb_bface.size(), 0.0f);
+      for (long long i = 0; i < H.np; i++) zs4[(size_t)i] = zsd[(size_t)H.cmp_off[i]];
+      for (size_t f = 0; f < H.face_off.size(); f++) q[f] = (H.face_dir[f] == 0 ? qu : qv)[(size_t)H.face_off[f]];
+      for (size_t ib = 0; ib < H.kb_bface.size(); ib++)
+        if (H.kb_bface[ib] >= 0) uvm[ib] = um[(size_t)H.kb_bface[ib]];
+    }
     const std::string name = H.dir + "/sfincs." + restart_time_string(1.0 * (double)(long long)t, H.tref) + ".rst";
     FILE* fp = std::fopen(name.c_str(), "wb");
     if (!fp) throw std::runtime_error("cannot write restart file " + name);
@@ -202,11 +220,18 @@ struct ModelHandle {
       std::fwrite(data, 1, bytes, fp);
       std::fwrite(&n, 4, 1, fp);
     };
-    const int32_t type = 1;
+    // flavour 1, or 4 / 5 / 6 with the state of the cnb / gai / hor infiltration (sfincs_output.f90:690-722)
+    const int32_t type = H.p.inftype == 3 ? 4 : H.p.inftype == 4 ? 5 : H.p.inftype == 5 ? 6 : 1;
     rec(&type, 4);
     rec(zs4.data(), zs4.size() * 4);
     rec(q.data(), q.size() * 4);
     rec(uvm.data(), uvm.size() * 4);
+    for (int j = 0; j < (type == 5 ? 2 : (type == 1 ? 0 : 1)); j++) {
+      std::vector<float> sd(NA), s4((size_t)H.np);
+      check_cuda(cudaMemcpy(sd.data(), D.inf_st[j], NA * 4, cudaMemcpyDeviceToHost), "restart infiltration state");
+      for (long long i = 0; i < H.np; i++) s4[(size_t)i] = sd[(size_t)(*cells)[(size_t)i]];
+      rec(s4.data(), s4.size() * 4);
+    }
     std::fclose(fp);
   }
 

@@ -21,6 +21,17 @@ void check_cuda(cudaError_t e, const char* what) {
 
 static bool is_none(const std::string& s) { return s.size() >= 4 && s.compare(0, 4, "none") == 0; }
 
+void apply_restart_infiltration(HostModel& h, const RestartData& rst, const std::vector<int32_t>& store) {
+  if (rst.type < 4 || rst.type > 6) return;  // flavours 4 cnb, 5 gai, 6 hor: the state overwrites the inputs
+  if (h.p.inftype != rst.type - 1)
+    throw std::runtime_error("restart file flavour " + std::to_string(rst.type) +
+                             " carries the state of another infiltration method than the model's");
+  for (int j = 0; j < (rst.type == 5 ? 2 : 1); j++) {
+    if ((long long)rst.inf[j].size() != h.np) throw std::runtime_error("restart file: infiltration state has the wrong length");
+    for (long long i = 0; i < h.np; i++) h.inf_st[j][(size_t)store[(size_t)i]] = rst.inf[j][(size_t)i];
+  }
+}
+
 void load_infiltration_models(HostModel& h, const Keys& k, size_t nstore, const std::vector<int32_t>& store) {
   ScnDev& P = h.p;
   const size_t n = (size_t)h.np;
@@ -150,7 +161,27 @@ void read_boundary_series(HostModel& h, const Keys& k, bool water_level_bnd, std
 void read_meteo_series(HostModel& h, const Keys& k, float rotation) {
   ScnDev& P = h.p;
   auto path = [&](const std::string& f) { return h.dir + "/" + f; };
-  if (P.wind) {
+  // gridded meteo with the enhancement factors (sfincs_meteo.f90:146-245, 330-380)
+  if (!is_none(h.amufile)) {
+    read_meteo_grid(path(h.amufile), h.tref, h.mgh[0], 0);
+    read_meteo_grid(path(h.amvfile), h.tref, h.mgh[0], 1);
+    if (h.factor_wind != 1.0f)
+      for (int q = 0; q < 2; q++)
+        for (auto& x : h.mgh[0].v[q]) x = h.factor_wind * x;
+  }
+  if (!is_none(h.ampfile)) {
+    read_meteo_grid(path(h.ampfile), h.tref, h.mgh[1], 0);
+    if (h.factor_pres != 1.0f)
+      for (auto& x : h.mgh[1].v[0]) x = P.gapres - h.factor_pres * (P.gapres - x);
+  }
+  if (!is_none(h.amprfile)) {
+    read_meteo_grid(path(h.amprfile), h.tref, h.mgh[2], 0);
+    if (h.factor_prcp != 1.0f)
+      for (auto& x : h.mgh[2].v[0]) x = h.factor_prcp * x;
+  }
+  P.cosrot = std::cos(rotation);
+  P.sinrot = std::sin(rotation);
+  if (P.wind && !is_none(k.wndfile)) {
     auto tb = read_table(path(k.wndfile));
     for (auto& r : tb) {
       h.twnd.push_back((float)r.at(0));
@@ -160,7 +191,7 @@ void read_meteo_series(HostModel& h, const Keys& k, float rotation) {
     P.ntwnd = (int)h.twnd.size();
     if (P.ntwnd < 2) throw std::runtime_error("wind time series needs at least two records");
   }
-  if (P.precip) {
+  if (P.precip && !is_none(k.prcpfile)) {
     auto tb = read_table(path(k.prcpfile));
     for (auto& r : tb) {
       h.tprcp.push_back((float)r.at(0));
@@ -249,8 +280,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   std::string prcpfile = in.str("prcfile", "none");
   if (is_none(prcpfile)) prcpfile = in.str("precipfile", "none");
   // Inputs outside this core's path: refuse loudly instead of silently ignoring physics.
-  for (const char* k : {"bcafile", "bzifile", "volfile", "spwfile",
-                        "amufile", "amvfile", "ampfile", "amprfile", "netbndbzsbzifile", "netsrcdisfile",
+  for (const char* k : {"bcafile", "bzifile", "volfile", "spwfile", "netbndbzsbzifile", "netsrcdisfile",
                         "netamuamvfile", "netamprfile", "netampfile", "netspwfile", "infiltration_file",
                         "wavemaker_wvmfile", "wvmfile"}) {
     if (!is_none(in.str(k, "none"))) throw std::runtime_error(std::string("input '") + k + "' is not supported by this core");
@@ -262,8 +292,6 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   // (sfincs_initial_conditions.F90:61-78); the binary form is read below.
   if (!is_none(inifile) && inifile.size() >= 2 && inifile.compare(inifile.size() - 2, 2, "nc") == 0)
     throw std::runtime_error("netCDF inifile is not supported by this core (use the binary real*4 form)");
-  if (!is_none(rstfile) && !is_none(in.str("qtrfile", "none")))
-    throw std::runtime_error("rstfile is not supported on quadtree grids by this core");
   if (igeo != 0) throw std::runtime_error("geographic grids (crsgeo=1) are not supported by this core");
   if (inputtype != "bin") throw std::runtime_error("only inputformat = bin is supported");
   if (bndtype != 1) throw std::runtime_error("only bndtype = 1 is supported");
@@ -285,8 +313,6 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
     h.tref = tref;
     h.dtrstout = dtrstout;
     h.trstout = dtrstout > 1.0e-6f ? (double)(t0out + dtrstout) : (trst > 1.0e-6f ? (double)trst : 1.0e9);
-    if (quadtree && h.trstout < 1.0e9)
-      throw std::runtime_error("restart output (dtrstout / trstout) is not supported on quadtree grids by this core");
   }
   tspinup = t0 + tspinup;
   P.g = 9.81f;
@@ -314,8 +340,38 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   P.viscosity = viscosity;
   P.friction2d = friction2d;
   P.wiggle = wiggle;
-  P.wind = !is_none(wndfile);
-  P.precip = !is_none(prcpfile);
+  // meteo processes (sfincs_domain.f90:95-125): wind from a time series or
+  // the amu / amv grids, pressure from the amp grid, rain from a time series or
+  // the ampr grid; a quantity from both a grid and a time series is refused
+  // (the reference lets the series overwrite the field and counts the
+  // cumulative rain of both)
+  {
+    const std::string amu = in.str("amufile", "none"), amv = in.str("amvfile", "none"),
+                      amp = in.str("ampfile", "none"), ampr = in.str("amprfile", "none");
+    if (!is_none(amu) && is_none(amv)) throw std::runtime_error("amufile needs an amvfile");
+    if (!is_none(amu) && !is_none(wndfile)) throw std::runtime_error("wind from both amufile and wndfile");
+    if (!is_none(ampr) && !is_none(prcpfile)) throw std::runtime_error("rain from both amprfile and prcfile");
+    if (in.real("waveage", -999.0f) > 0.0f) throw std::runtime_error("waveage (wave-age wind drag) is not supported");
+    if (in.integer("radstr", 0) == 1) throw std::runtime_error("radstr is not supported");
+    P.wind = !is_none(wndfile) || !is_none(amu);
+    P.wind_field = !is_none(amu);
+    P.patmos = !is_none(amp) && in.integer("baro", 1) == 1;
+    P.precip = !is_none(prcpfile) || !is_none(ampr);
+    P.prcp_field = !is_none(ampr);
+    P.meteo3d = !is_none(amu) || !is_none(amp) || !is_none(ampr);
+    P.spinup_meteo = in.integer("spinup_meteo", 0) != 0;
+    P.ampr_block = in.integer("amprblock", 1) != 0;
+    P.dtwnd = in.real("dtwnd", 1800.0f);
+    P.gapres = in.real("gapres", 101200.0f);
+    P.pavbnd = in.real("pavbnd", 0.0f);
+    h.amufile = amu;
+    h.amvfile = amv;
+    h.ampfile = P.patmos ? amp : std::string("none");
+    h.amprfile = ampr;
+    h.factor_wind = in.real("factor_wind", 1.0f);
+    h.factor_pres = in.real("factor_pres", 1.0f);
+    h.factor_prcp = in.real("factor_prcp", 1.0f);
+  }
   P.use_qext = bmi;
   P.t0 = t0;
   P.t1 = t1;
@@ -465,11 +521,7 @@ bool segments_cross(float p1x, float p1y, float p2x, float p2y, float q1x, float
 // the flavour (int32), zs (float32[np]), and for flavours 1, 2, 4-6 the fluxes
 // q (float32[npuv + ncuv + 1], reference face order) and the boundary mean
 // fluxes uvmean (float32[nkcuv2]).
-struct RestartData {
-  int type = 0;
-  std::vector<float> zs, q, uvmean;
-};
-static RestartData read_restart(const std::string& file) {
+RestartData read_restart(const std::string& file) {
   FILE* fp = std::fopen(file.c_str(), "rb");
   if (!fp) throw std::runtime_error("cannot open restart file " + file);
   std::vector<std::vector<char>> rec;
@@ -496,11 +548,15 @@ static RestartData read_restart(const std::string& file) {
     return v;
   };
   if (d.type < 1 || d.type > 6) return d;  // the reference skips an unknown flavour with a warning
-  if (d.type >= 4) throw std::runtime_error("restart flavours 4-6 (cnb/gai/hor infiltration) are not supported by this core");
   d.zs = floats(1);
-  if (d.type == 1 || d.type == 2) {
+  if (d.type != 3) {  // q and uvmean in every flavour but 3 (sfincs_initial_conditions.F90:227-235)
     d.q = floats(2);
     d.uvmean = floats(3);
+  }
+  if (d.type == 4 || d.type == 6) d.inf[0] = floats(4);  // scs_Se / rain_T1 (:237-258)
+  if (d.type == 5) {                                    // GA_sigma, GA_F
+    d.inf[0] = floats(4);
+    d.inf[1] = floats(5);
   }
   return d;
 }
@@ -982,6 +1038,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     }
   }
   load_infiltration_models(h, K, NA, h.cmp_off);
+  apply_restart_infiltration(h, rst, h.cmp_off);
 
   // ---- weirs (sfincs_structures.f90:38-381) ----------------------------------------
   // Every face a weir polyline crosses gets the crossed length (the face's
@@ -1319,8 +1376,13 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     if (h.p.subgrid) up(d.vneg, h.vneg);
     else d.vneg = nullptr;
     for (int b = 0; b < 2; b++) {
-      zero(d.qu[b], NQ);
-      zero(d.uu[b], NQ);
+      if (h.q0u.empty()) {
+        zero(d.qu[b], NQ);
+        zero(d.uu[b], NQ);
+      } else {  // fluxes from a restart file in both buffers
+        up(d.qu[b], h.q0u);
+        up(d.uu[b], h.uv0u);
+      }
       d.qv[b] = d.qu[b];
       d.vv[b] = d.uu[b];
     }
@@ -1348,7 +1410,8 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     up(d.qlev, h.qlev);
     up(qmu, h.qmap_u);
     up(qmv, h.qmap_v);
-    d.rc_u = d.rc_v = nullptr;
+    d.rc4_u = d.rc4_v = nullptr;
+    d.rc2_u = d.rc2_v = nullptr;
     d.rl_u = d.rl_v = nullptr;
     d.zc = nullptr;
     d.zl = nullptr;
@@ -1359,7 +1422,8 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
     d.qlev = nullptr;
     d.zbmx = d.gn2 = nullptr;
     qmu = qmv = nullptr;
-    d.rc_u = d.rc_v = nullptr;  // set below for subgrid models
+    d.rc4_u = d.rc4_v = nullptr;
+    d.rc2_u = d.rc2_v = nullptr;  // set below for subgrid models
     d.rl_u = d.rl_v = nullptr;
     d.zc = nullptr;
     d.zl = nullptr;
@@ -1413,14 +1477,17 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.zz_volmax, h.zz_volmax);
   up(d.zlev, h.zlev);
   if (h.p.subgrid) {  // record cache, empty (all codes 0)
-    zero(d.rc_u, NA * 6);
-    zero(d.rc_v, NA * 6);
+    zero(d.rc4_u, NA);
+    zero(d.rc4_v, NA);
+    zero(d.rc2_u, NA);
+    zero(d.rc2_v, NA);
     zero(d.rl_u, NA);
     zero(d.rl_v, NA);
     zero(d.zc, NA);
     zero(d.zl, NA);
   } else {
-    d.rc_u = d.rc_v = nullptr;
+    d.rc4_u = d.rc4_v = nullptr;
+    d.rc2_u = d.rc2_v = nullptr;
     d.rl_u = d.rl_v = nullptr;
     d.zc = nullptr;
     d.zl = nullptr;
@@ -1445,6 +1512,44 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.wdir, h.wdir);
   up(d.cdval, h.cdval);
   up(d.x73, h.x73);
+  {  // gridded meteo: the raw grids, the cell centres, the window fields
+    const size_t ncell = h.p.quadtree ? (size_t)h.np : NA;
+    for (int kq = 0; kq < 3; kq++) {
+      const MeteoGridHost& g = h.mgh[kq];
+      MeteoGrid& m = d.mg[kq];
+      m = MeteoGrid{};
+      m.nt = g.nt;
+      m.nrows = g.nrows;
+      m.ncols = g.ncols;
+      m.x_ll = g.x_ll;
+      m.y_ll = g.y_ll;
+      m.dx = g.dx;
+      m.dy = g.dy;
+      up(m.times, g.times);
+      up(m.v0, g.v[0]);
+      up(m.v1, g.v[1]);
+    }
+    d.nmeteo = (int)h.np;
+    if (h.p.meteo3d) {
+      up(d.xz, h.z_xz);
+      up(d.yz, h.z_yz);
+    } else {
+      d.xz = d.yz = nullptr;
+    }
+    auto field = [&](float*& dst, bool on, float v) {
+      if (on) up(dst, std::vector<float>(ncell, v));
+      else dst = nullptr;
+    };
+    const bool wf = h.p.wind_field, pf = h.p.patmos, rf = h.p.prcp_field;
+    field(d.tauwu0, wf, 0.0f);
+    field(d.tauwu1, wf, 0.0f);
+    field(d.tauwv0, wf, 0.0f);
+    field(d.tauwv1, wf, 0.0f);
+    field(d.patm0, pf, 0.0f);
+    field(d.patm1, pf, 0.0f);
+    field(d.prcp0, rf, 0.0f);
+    field(d.prcp1, rf, 0.0f);
+  }
   for (int j = 0; j < 5; j++) {
     up(d.inf_par[j], h.inf_par[j]);
     up(d.inf_st[j], h.inf_st[j]);
@@ -1461,6 +1566,7 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(d.drn_status, std::vector<int>(h.drn.size(), 1));          // open
   up(d.drn_frac, std::vector<float>(h.drn.size(), 1.0f));      // fully open
   up(cmp, h.cmp_off);
+  d.cmp = h.p.quadtree ? nullptr : cmp;  // compact cell -> storage offset for the meteo fields
   zero(d.st, 1);
 }
 
@@ -1491,6 +1597,7 @@ DeviceModel::DeviceModel(const HostModel& h) : h_(&h) {
     s.min_dt = 1.0e-6f;
     s.dt = 1.0e-6f;
     s.itbndlast = s.itprcplast = s.itwndlast = s.itsrclast = 1;
+    s.twindupd = (float)h.t0;  // sfincs_lib.f90:290
     s.steps_left = 0;
     float one_e_minus6 = 1.0e-6f;
     std::memcpy(&s.min_dt_bits, &one_e_minus6, 4);
@@ -1523,6 +1630,14 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
     if (h.p.quadtree != qt_) throw std::runtime_error("an ensemble must be all-quadtree or all-regular-grid");
     if (h.p.nsrc > 0 || h.p.ndrn > 0) any_src_ = 1;
     if (h.p.nstruc > 0) any_struc_ = 1;
+    if (h.p.wind_field || h.p.patmos) met_ = 1;
+    if (h.p.inftype >= 2 || h.p.store_cumprcp || h.p.prcp_field || h.p.store_vmax || h.p.store_qmax ||
+        h.p.store_twet || h.p.store_tzsmax)
+      ext_ = 1;
+    if (h.p.meteo3d) {
+      any_meteo_ = 1;
+      meteo_cells_ = std::max(meteo_cells_, (int)h.np);
+    }
     bnd_blocks_ = std::max(bnd_blocks_, (h.p.nkcuv2 + h.p.nneu + 127) / 128);
     scns.push_back(models_[i]->dev());
     if (!qt_)
@@ -1574,12 +1689,12 @@ void Runner::configure_grids() {
   int dev = 0, nsm = 0, nb_m = 0, nb_c = 0;
   check_cuda(cudaGetDevice(&dev), "device");
   check_cuda(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "sm count");
-  const void* mfn = momentum_tma_fn(subgrid_, variant_, one() != nullptr);
+  const void* mfn = momentum_tma_fn(subgrid_, variant_ + (met_ ? 10 : 0), one() != nullptr);
   check_cuda(cudaFuncSetAttribute(mfn, cudaFuncAttributeMaxDynamicSharedMemorySize, momentum_tma_smem(variant_, subgrid_)),
              "momentum shared memory");
   check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_m, mfn, 256, momentum_tma_smem(variant_, subgrid_)), "occupancy");
   check_cuda(
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_c, continuity_tma_fn(subgrid_, one() != nullptr), 256, continuity_tma_smem()),
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_c, continuity_tma_fn(subgrid_, one() != nullptr, ext_ != 0), 256, continuity_tma_smem()),
       "occupancy");
   mom_grid_ = std::max(1, std::min(ntiles_, std::max(nb_m, 1) * nsm));
   con_grid_ = std::max(1, std::min(ntiles_, std::max(nb_c, 1) * nsm));
@@ -1597,10 +1712,11 @@ Runner::~Runner() {
 
 void Runner::launch_momentum_any() {
   if (qt_) {
-    launch_qt_momentum(d_scns_, d_tiles_, nqf_, subgrid_, stream_);
+    launch_qt_momentum(d_scns_, d_tiles_, nqf_, subgrid_, met_ != 0, stream_);
     launch_qt_cuv(d_scns_, d_tiles_ + nqf_, nqcuv_, stream_);
   } else if (tma()) {
-    launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, variant_, mom_grid_, stream_, one());
+    launch_momentum_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, variant_ + (met_ ? 10 : 0), mom_grid_, stream_,
+                        one());
   } else {
     launch_momentum(d_scns_, d_tiles_, ntiles_, subgrid_, variant_, stream_);
   }
@@ -1608,14 +1724,15 @@ void Runner::launch_momentum_any() {
 
 void Runner::launch_continuity_any() {
   if (qt_)
-    launch_qt_continuity(d_scns_, d_tiles_ + nqf_ + nqcuv_, nqc_, subgrid_, stream_);
+    launch_qt_continuity(d_scns_, d_tiles_ + nqf_ + nqcuv_, nqc_, subgrid_, ext_ != 0, stream_);
   else if (tma())
-    launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_, one());
+    launch_continuity_tma(d_scns_, d_maps_, d_tiles_, ntiles_, subgrid_, con_grid_, stream_, one(), ext_ != 0);
   else
     launch_continuity(d_scns_, d_tiles_, ntiles_, subgrid_, stream_);
 }
 
 void Runner::launch_one() {
+  if (any_meteo_) launch_meteo_window(d_scns_, nscn(), meteo_cells_, stream_);
   launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_, one());
   launch_momentum_any();
   if (any_struc_) launch_structures(d_scns_, nscn(), stream_);
@@ -1667,6 +1784,7 @@ std::vector<double> Runner::time_kernels(int nsteps) {
   std::vector<double> acc(4, 0.0);
   for (int i = 0; i < nsteps; i++) {
     check_cuda(cudaEventRecord(ev[0], stream_), "record");
+    if (any_meteo_) launch_meteo_window(d_scns_, nscn(), meteo_cells_, stream_);
     launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_, one());
     check_cuda(cudaEventRecord(ev[1], stream_), "record");
     launch_momentum_any();
@@ -1711,6 +1829,7 @@ void Runner::step_once(cudaEvent_t continuity_after) {
                "steps");
   }
   if (continuity_after) {
+    if (any_meteo_) launch_meteo_window(d_scns_, nscn(), meteo_cells_, stream_);
     launch_step_bnd(d_scns_, nscn(), bnd_blocks_, stream_, one());
     launch_momentum_any();
     if (any_struc_) launch_structures(d_scns_, nscn(), stream_);

@@ -14,6 +14,16 @@
 
 namespace sfg {
 
+// One gridded meteo quantity as read from its ASCII file(s): nt records of
+// nrows x ncols values, first row at the top; v[1] is the second wind component.
+struct MeteoGridHost {
+  int nt = 0, nrows = 0, ncols = 0;
+  float x_ll = 0, y_ll = 0, dx = 0, dy = 0;
+  std::vector<float> times, v[2];
+};
+// Reads an amu / amv / amp / ampr file into g (q: 0 first quantity, 1 second wind component).
+void read_meteo_grid(const std::string& file, const std::string& tref, MeteoGridHost& g, int q);
+
 // Everything read from a model directory and laid out densely on the host.
 struct HostModel {
   std::string dir;
@@ -50,6 +60,9 @@ struct HostModel {
   std::vector<float> t_bnd, zs_bnd;  // zs_bnd [ntbnd][nbnd]
   std::vector<float> tprcp, vprcp, twnd, wmag, wdir, cdval;
   std::vector<float> x73;            // hu**(7/3) table when h73table is on (sfincs_data.f90:858-881)
+  MeteoGridHost mgh[3];              // gridded meteo: 0 wind (amu, amv), 1 pressure (amp), 2 rain (ampr)
+  std::string amufile = "none", amvfile = "none", ampfile = "none", amprfile = "none";  // their files
+  float factor_wind = 1, factor_pres = 1, factor_prcp = 1;
   // infiltration models with state: parameters, state, event flag, cumulative sums (storage order)
   std::vector<float> inf_par[5], inf_st[5], cumprcp, cuminf;
   std::vector<uint8_t> inf_rain;
@@ -123,6 +136,17 @@ void read_meteo_series(HostModel& h, const Keys& k, float rotation);
 // reference does, laid out at storage index store[i] of compact cell i
 // (nstore entries); the cumulative sums when stored.  P.inftype must be set.
 void load_infiltration_models(HostModel& h, const Keys& k, size_t nstore, const std::vector<int32_t>& store);
+// A binary restart file (sfincs_initial_conditions.F90:183-268): flavour, zs,
+// q (npuv + ncuv + 1, reference order) and uvmean, and the infiltration state
+// of flavours 4-6 (cnb: scs_Se; gai: GA_sigma, GA_F; hor: rain_T1).
+struct RestartData {
+  int type = 0;
+  std::vector<float> zs, q, uvmean;
+  std::vector<float> inf[2];
+};
+RestartData read_restart(const std::string& file);
+// The infiltration state of a flavour 4-6 restart into the model's state arrays.
+void apply_restart_infiltration(HostModel& h, const RestartData& rst, const std::vector<int32_t>& store);
 // Quadtree mesh (qtrfile): compact cells and uv points (host/qtmodel.cpp).
 void load_quadtree(HostModel& h, const Keys& k);
 // 1-based active cell of a quadtree mesh at point (x, y), 0 outside.
@@ -218,7 +242,7 @@ class Runner {
   // Issue nsteps steps with CUDA events between the launches; returns the mean
   // duration (ms) of [step+boundary, momentum, sources, continuity] launches.
   std::vector<double> time_kernels(int nsteps);
-  int launches_per_step() const { return 3 + any_src_ + any_struc_ + (qt_ && nqcuv_ > 0 ? 1 : 0); }
+  int launches_per_step() const { return 3 + any_src_ + any_struc_ + any_meteo_ + (qt_ && nqcuv_ > 0 ? 1 : 0); }
 
  private:
   void build_graph(int chunk);
@@ -237,6 +261,9 @@ class Runner {
   int qt_ = 0;                       // quadtree models: face / combined-point / cell work lists in d_tiles_
   int nqf_ = 0, nqcuv_ = 0, nqc_ = 0;
   int any_src_ = 0, any_struc_ = 0;
+  int any_meteo_ = 0, meteo_cells_ = 0;  // gridded meteo: the window kernel runs before each step kernel
+  int met_ = 0;  // gridded wind or pressure: momentum runs its meteo instance (variant + 10)
+  int ext_ = 0;  // continuity runs its extended instance (infiltration with state, sums, gridded rain, store variables)
   cudaStream_t stream_ = nullptr;
   bool own_stream_ = true;
   cudaGraphExec_t graph_ = nullptr;
@@ -254,6 +281,7 @@ class Runner {
 void launch_step(const ScnDev* d_scns, int nscn, int bnd_blocks, const Tile* d_tiles, int ntiles, int subgrid,
                  int any_src, int variant, cudaStream_t s);
 void launch_step_bnd(const ScnDev* d_scns, int nscn, int bnd_blocks, cudaStream_t s, const ScnDev* one);
+void launch_meteo_window(const ScnDev* d_scns, int nscn, int max_cells, cudaStream_t s);
 void launch_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, int variant,
                      cudaStream_t s);
 void launch_sources(const ScnDev* d_scns, int nscn, cudaStream_t s);
@@ -266,13 +294,14 @@ MapSet build_map_set(const ScnDev& d);
 int momentum_tma_smem(int form, int subgrid);
 int continuity_tma_smem();
 const void* momentum_tma_fn(int subgrid, int form, bool one);
-const void* continuity_tma_fn(int subgrid, bool one);
+const void* continuity_tma_fn(int subgrid, bool one, bool ext);
 void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
                          int form, int grid, cudaStream_t s, const ScnDev* one);
 void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
-                           int grid, cudaStream_t s, const ScnDev* one);
-void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s);
+                           int grid, cudaStream_t s, const ScnDev* one, bool ext);
+void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, bool met, cudaStream_t s);
 void launch_qt_cuv(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, cudaStream_t s);
-void launch_qt_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s);
+void launch_qt_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, bool ext,
+                          cudaStream_t s);
 
 }  // namespace sfg

@@ -10,7 +10,9 @@
 // has read their results and releases the slot.  Membership changes take
 // effect between chunks of steps: the runner (scenario table, tiles, tensor
 // maps, CUDA graph) is rebuilt over the current members; the models' states
-// live in their own device memory and are untouched by a rebuild.
+// live in their own device memory and are untouched by a rebuild.  Regular
+// grids and quadtree meshes run in two runners on two streams, so the two
+// kinds of request overlap on the device too.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,25 +50,34 @@ struct Pool {
   int max_slots;
   size_t budget, used_bytes = 0;
   std::vector<Slot> slots;
-  std::vector<int> members;  // slot of each runner scenario
-  std::unique_ptr<Runner> runner;
+  std::vector<int> members[2];  // slot of each runner scenario: regular grids, quadtree meshes
+  std::unique_ptr<Runner> runner[2];
   bool dirty = false;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;   // regular-grid runner, uploads and reads
+  cudaStream_t stream_qt = nullptr;  // quadtree runner
   void* d_stage = nullptr;
   size_t stage_bytes = 0;
   StepState* h_states = nullptr;
 
   Pool(int n, size_t b) : max_slots(n), budget(b), slots((size_t)n) {
     check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "pool stream");
+    check_cuda(cudaStreamCreateWithFlags(&stream_qt, cudaStreamNonBlocking), "pool stream");
     check_cuda(cudaMallocHost(&h_states, (size_t)n * sizeof(StepState)), "pinned states");
+  }
+  void sync_all() {
+    check_cuda(cudaStreamSynchronize(stream), "pool sync");
+    check_cuda(cudaStreamSynchronize(stream_qt), "pool sync");
   }
   ~Pool() {
     if (stream) cudaStreamSynchronize(stream);
-    runner.reset();
+    if (stream_qt) cudaStreamSynchronize(stream_qt);
+    runner[0].reset();
+    runner[1].reset();
     for (auto& s : slots) s.dev.reset();
     if (d_stage) cudaFree(d_stage);
     if (h_states) cudaFreeHost(h_states);
     if (stream) cudaStreamDestroy(stream);
+    if (stream_qt) cudaStreamDestroy(stream_qt);
   }
 
   int admit(Prepared* pr, double t_end) {
@@ -97,40 +108,51 @@ struct Pool {
   }
 
   void rebuild() {
-    check_cuda(cudaStreamSynchronize(stream), "pool sync");
-    runner.reset();
-    members.clear();
-    std::vector<DeviceModel*> devs;
-    for (int i = 0; i < max_slots; i++)
-      if (slots[i].used && !slots[i].finished) {
-        members.push_back(i);
-        devs.push_back(slots[i].dev.get());
-      }
-    if (!devs.empty()) runner = std::make_unique<Runner>(devs, 8, stream);
+    sync_all();
+    for (int k = 0; k < 2; k++) {
+      runner[k].reset();
+      members[k].clear();
+      std::vector<DeviceModel*> devs;
+      for (int i = 0; i < max_slots; i++)
+        if (slots[i].used && !slots[i].finished && (slots[i].host->p.quadtree != 0) == (k == 1)) {
+          members[k].push_back(i);
+          devs.push_back(slots[i].dev.get());
+        }
+      if (!devs.empty()) runner[k] = std::make_unique<Runner>(devs, 8, k == 0 ? stream : stream_qt);
+    }
     dirty = false;
   }
 
   // Advance the running members by up to nsteps steps; returns how many are
-  // still running afterwards.
+  // still running afterwards.  Both runners are queued before either is
+  // waited for.
   int advance(int nsteps) {
     if (dirty) rebuild();
-    if (!runner) return 0;
-    runner->issue(nsteps);
-    for (size_t j = 0; j < members.size(); j++)
-      check_cuda(cudaMemcpyAsync(&h_states[j], slots[members[j]].dev->state(), sizeof(StepState),
-                                 cudaMemcpyDeviceToHost, stream),
-                 "read state");
-    check_cuda(cudaStreamSynchronize(stream), "pool sync");
+    if (!runner[0] && !runner[1]) return 0;
+    size_t j = 0;
+    for (int k = 0; k < 2; k++) {
+      if (!runner[k]) continue;
+      runner[k]->issue(nsteps);
+      for (int slot : members[k])
+        check_cuda(cudaMemcpyAsync(&h_states[j++], slots[slot].dev->state(), sizeof(StepState),
+                                   cudaMemcpyDeviceToHost, k == 0 ? stream : stream_qt),
+                   "read state");
+    }
+    sync_all();
     int running = 0;
-    for (size_t j = 0; j < members.size(); j++) {
-      Slot& s = slots[members[j]];
-      s.last = h_states[j];
-      const StepState& st = h_states[j];
-      if (st.stop_pending || !(st.t < st.tend) || st.error || st.fault) {
-        s.finished = true;
-        dirty = true;
-      } else {
-        running++;
+    j = 0;
+    for (int k = 0; k < 2; k++) {
+      if (!runner[k]) continue;
+      for (int slot : members[k]) {
+        Slot& s = slots[slot];
+        s.last = h_states[j];
+        const StepState& st = h_states[j++];
+        if (st.stop_pending || !(st.t < st.tend) || st.error || st.fault) {
+          s.finished = true;
+          dirty = true;
+        } else {
+          running++;
+        }
       }
     }
     return running;
@@ -143,8 +165,9 @@ struct Pool {
 
   void release(int k) {
     Slot& s = at(k);
-    check_cuda(cudaStreamSynchronize(stream), "pool sync");
-    runner.reset();  // it may still reference the model; rebuilt on the next advance
+    sync_all();
+    runner[0].reset();  // they may still reference the model; rebuilt on the next advance
+    runner[1].reset();
     dirty = true;
     used_bytes -= s.dev->bytes();
     s.dev.reset();
@@ -157,6 +180,7 @@ struct Pool {
     Slot& s = at(k);
     const long long n = s.host->np;
     ScnDev& D = s.dev->dev();
+    sync_all();
     check_cuda(cudaMemcpyAsync(&s.last, s.dev->state(), sizeof(StepState), cudaMemcpyDeviceToHost, stream), "state");
     check_cuda(cudaStreamSynchronize(stream), "pool sync");
     const int p = s.last.run ? (s.last.parity ^ 1) : s.last.parity;
@@ -202,6 +226,7 @@ struct Pool {
 
   void scalars(int k, double* out) {
     Slot& s = at(k);
+    sync_all();
     check_cuda(cudaMemcpyAsync(&s.last, s.dev->state(), sizeof(StepState), cudaMemcpyDeviceToHost, stream), "state");
     check_cuda(cudaStreamSynchronize(stream), "pool sync");
     const HostModel& h = *s.host;

@@ -818,20 +818,68 @@ void QtBuilder::finish() {
     h.qinf.assign(np, 0.0f);
     for (long i = 0; i < np; i++) h.qinf[i] = r[(size_t)i] / 3600.0f / 1000.0f;
   }
+  // restart file (sfincs_initial_conditions.F90:183-268): zs, q in the
+  // reference's uv order (which is this mesh's), uvmean in boundary-face order
+  RestartData rst;
+  if (!none(k.rstfile)) {
+    rst = read_restart(h.dir + "/" + k.rstfile);
+    if (rst.type >= 1 && rst.type <= 6) {
+      if ((long)rst.zs.size() != np) throw std::runtime_error("restart file: zs has the wrong length");
+      if (!rst.q.empty() && (long)rst.q.size() != npuv + ncuv + 1)
+        throw std::runtime_error("restart file: q has the wrong length");
+      if (!rst.uvmean.empty() && (long)rst.uvmean.size() != (long)h.bfaces.size())
+        throw std::runtime_error("restart file: uvmean has the wrong length");
+    }
+  }
   {  // infiltration models with state: parameters in cell order (compact storage)
     std::vector<int32_t> ident((size_t)np);
     for (long i = 0; i < np; i++) ident[(size_t)i] = (int32_t)i;
     load_infiltration_models(h, k, (size_t)np, ident);
+    apply_restart_infiltration(h, rst, ident);
   }
   // initial state (sfincs_initial_conditions.F90:98-106, sfincs_subgrid.F90:907-962)
   // binary ini file: real*4 levels in cell order (read_zsini_file, sfincs_initial_conditions.F90:270-288)
   std::vector<float> inizs;
-  if (!none(k.inifile)) inizs = read_binary<float>(h.dir + "/" + k.inifile, (size_t)np);
+  if (!rst.zs.empty()) inizs = rst.zs;
+  else if (!none(k.inifile)) inizs = read_binary<float>(h.dir + "/" + k.inifile, (size_t)np);
   h.zs.assign(np, 0.0f);
   for (long i = 0; i < np; i++) {
     const float base = P.subgrid ? h.zz_min[i] : h.zb[i];
     h.zs[i] = (float)std::max((double)base, inizs.empty() ? (double)P.zini : (double)inizs[(size_t)i]);
   }
+  // fluxes of the uv points from the restart and the velocities they imply
+  // (:110-173); combined points start at zero as in the reference
+  if (!rst.q.empty()) {
+    const size_t NQ = (size_t)(npuv + ncuv + 1);
+    h.q0u.assign(NQ, 0.0f);
+    h.uv0u.assign(NQ, 0.0f);
+    const int L = P.nlev;
+    for (long ip = 1; ip <= npuv; ip++) {
+      const float q = rst.q[(size_t)ip - 1];
+      h.q0u[(size_t)ip - 1] = q;
+      const float zsuv = std::max(h.zs[uv_nm[ip] - 1], h.zs[uv_nmu[ip] - 1]);
+      float huv;
+      if (P.subgrid) {
+        const float2 zr = h.sgz_u[(size_t)ip - 1];
+        if (!(zsuv > zr.x + P.huthresh)) continue;
+        if (zsuv > zr.y - 1.0e-4f) {
+          huv = h.sgw_u[(size_t)ip - 1].x + zsuv;
+        } else {
+          const float dzuv = (zr.y - zr.x) / (float)(L - 1);
+          const int iuv = std::min(std::max((int)((zsuv - zr.x) / dzuv) + 1, 1), L - 1);
+          const float facint = (zsuv - (zr.x + (float)(iuv - 1) * dzuv)) / dzuv;
+          const UvRec& r = h.rec_u[(size_t)(iuv - 1) * npuv + (size_t)ip - 1];
+          huv = r.havg + r.dhavg * facint;
+        }
+        huv = std::max(huv, P.huthresh);
+      } else {
+        if (!(zsuv > h.zbmx_q[(size_t)ip - 1])) continue;
+        huv = std::max(zsuv - zbuv[ip], P.huthresh);
+      }
+      h.uv0u[(size_t)ip - 1] = std::max(std::min(q / huv, 4.0f), -4.0f);
+    }
+  }
+  if (!rst.uvmean.empty()) h.uvmean0 = rst.uvmean;
   h.zsmax.assign(np, -999.0f);
   if (P.wiggle) h.zs0 = h.zs;
   if (P.subgrid) {

@@ -69,6 +69,8 @@ struct StepPlan {
   int itb0, itb1;  // boundary time records (1-based)
   int itbndlast;   // cached boundary time record for the next search
   float tbfac;     // boundary time-interpolation factor
+  int meteo_upd;   // the gridded meteo window advances this step
+  float mt0, mt1;  // the gridded meteo window of this step
 };
 
 __device__ __forceinline__ StepPlan plan_step(const ScnDev& S, const StepState& st) {
@@ -83,6 +85,10 @@ __device__ __forceinline__ StepPlan plan_step(const ScnDev& S, const StepState& 
   P.itb0 = st.itb0;
   P.itb1 = st.itb1;
   P.tbfac = st.tbfac;
+  // ---- gridded meteo window (sfincs_lib.f90:493-503): t >= twindupd opens [twindupd, twindupd + dtwnd]
+  P.meteo_upd = P.go && S.meteo3d && P.t >= (double)st.twindupd;
+  P.mt0 = P.meteo_upd ? st.twindupd : st.meteo_t0;
+  P.mt1 = P.meteo_upd ? st.twindupd + S.dtwnd : st.meteo_t1;
   // ---- boundary time interpolation (sfincs_boundaries.f90:696-726)
   if (P.go && S.nbnd > 0) {
     const double t = P.t;
@@ -119,7 +125,7 @@ __device__ __forceinline__ void step_forcing(const ScnDev& S, StepState& st, con
   const float dt = P.dt;
   const double t = P.t;
   // ---- uniform wind from time series (sfincs_meteo.f90:1445-1508)
-  if (S.wind) {
+  if (S.wind && S.ntwnd > 0) {
     for (int itw = st.itwndlast; itw <= S.ntwnd; itw++) {
       if ((double)S.twnd[itw - 1] > t) {
         const int i0 = itw - 1 >= 1 ? itw - 1 : 1;
@@ -146,7 +152,7 @@ __device__ __forceinline__ void step_forcing(const ScnDev& S, StepState& st, con
     }
   }
   // ---- uniform rain from time series (sfincs_meteo.f90:1510-1558)
-  if (S.precip) {
+  if (S.precip && S.ntprcp > 0) {
     int itp;
     for (itp = st.itprcplast; itp <= S.ntprcp; itp++)
       if ((double)S.tprcp[itp - 1] > t) break;
@@ -198,6 +204,11 @@ __device__ __forceinline__ void commit_step(const ScnDev& S, StepState& st, cons
     st.itb1 = P.itb1;
     st.tbfac = P.tbfac;
     st.itbndlast = P.itbndlast;
+  }
+  if (P.meteo_upd) {  // the gridded meteo window this step opened (the fields were made before this kernel)
+    st.meteo_t0 = P.mt0;
+    st.meteo_t1 = P.mt1;
+    st.twindupd = st.twindupd + S.dtwnd;
   }
   st.min_dt_bits = __float_as_uint(S.dtmax);  // sfincs_momentum.f90:99
   if (dtchk < S.dtmin && st.nt > 1) {         // sfincs_lib.f90:634-648
@@ -398,6 +409,8 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan&
         zst = (double)(zp1 * b.fac + zp2 * (1.0f - b.fac));
       else
         zst = (double)zp1;
+      if (S.patmos && S.pavbnd > 1.0f)  // barometric correction with the boundary cell's pressure (:820-826)
+        zst = zst + (double)((S.pavbnd - cell_patm(S, b.nmb, meteo_weights(S, t, P.mt0, P.mt1))) / (S.rhow * 9.81f));
       float zb0;
       if (t < (double)(S.tspinup - 1.0e-3f)) {
         const float smfac = (float)(1.0 - (t - (double)S.t0) / (double)(S.tspinup - S.t0));
@@ -535,6 +548,112 @@ __global__ void __launch_bounds__(1024) k_step_bnd(const ScnDev* __restrict__ sc
 }
 
 // --------------------------------------------------------------------------
+// Gridded meteo: the two fields of an update window on the cells.
+// --------------------------------------------------------------------------
+// The records around one end of the window (update_amuv_data and its
+// pressure / rain twins, sfincs_meteo.f90:823-845, 998-1020, 1128-1155).
+struct MeteoRec {
+  int i0, i1;  // 0-based records
+  float twfac;
+};
+__device__ __forceinline__ MeteoRec meteo_rec(const MeteoGrid& g, float meteo_t, bool block) {
+  meteo_t = fmaxf(meteo_t, g.times[0]);
+  meteo_t = fminf(meteo_t, g.times[g.nt - 1]);
+  int itw0 = 1;
+  for (int it = 1; it <= g.nt; it++)
+    if (g.times[it - 1] <= meteo_t) itw0 = it;
+  const int itw1 = min(itw0 + 1, g.nt);
+  meteo_t = fminf(meteo_t, g.times[itw1 - 1]);
+  MeteoRec r;
+  r.i0 = itw0 - 1;
+  r.i1 = itw1 - 1;
+  r.twfac = block ? 0.0f : (meteo_t - g.times[itw0 - 1]) / fmaxf(g.times[itw1 - 1] - g.times[itw0 - 1], 1.0e-6f);
+  return r;
+}
+
+// Bilinear interpolation of quantity v (records blended by r) at (x, y), in
+// the reference's index arithmetic (:851-898); false outside the grid (the
+// reference treats the first row band and the edges as outside too).
+__device__ __forceinline__ bool meteo_at(const MeteoGrid& g, const float* v, const float* v2, const MeteoRec& r,
+                                         float x, float y, float& out, float& out2) {
+  const float yul = g.y_ll + (float)(g.nrows - 1) * g.dy + 0.5f * g.dy;
+  const float xll = g.x_ll + 0.5f * g.dx;
+  const int iy = (int)((yul - y) / g.dy) + 1;
+  const float dj1 = (yul - (float)(iy - 1) * g.dy - y) / g.dy;
+  const int ix = (int)((x - xll) / g.dx) + 1;
+  const float di1 = (x - (xll + (float)(ix - 1) * g.dx)) / g.dx;
+  if (iy <= 1 || iy >= g.nrows || ix <= 0 || ix >= g.ncols) return false;
+  const int ind1[4] = {iy, iy, iy + 1, iy + 1}, ind2[4] = {ix, ix + 1, ix + 1, ix};
+  const float f[4] = {(1.0f - di1) * (1.0f - dj1), di1 * (1.0f - dj1), di1 * dj1, (1.0f - di1) * dj1};
+  const size_t rec = (size_t)g.nrows * g.ncols;
+  float a = 0.0f, b = 0.0f;
+  for (int ip = 0; ip < 4; ip++) {
+    const size_t o = (size_t)(ind1[ip] - 1) * g.ncols + (ind2[ip] - 1);
+    a = a + f[ip] * (v[r.i0 * rec + o] * (1.0f - r.twfac) + v[r.i1 * rec + o] * r.twfac);
+    if (v2) b = b + f[ip] * (v2[r.i0 * rec + o] * (1.0f - r.twfac) + v2[r.i1 * rec + o] * r.twfac);
+  }
+  out = a;
+  out2 = b;
+  return true;
+}
+
+// Runs before the step kernel: when the step about to run opens a new window
+// (the same decision the step kernel commits), every cell gets the window's
+// wind stress, pressure and rain at both ends (update_meteo_fields,
+// sfincs_meteo.f90:1561-1624); otherwise every CTA returns at once.
+__global__ void __launch_bounds__(256) k_meteo_window(const ScnDev* __restrict__ scns) {
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
+  const ScnDev& S = scns[blockIdx.y];
+  if (!S.meteo3d) return;
+  const StepState& st = *S.st;
+  const StepPlan P = plan_step(S, st);
+  if (!P.meteo_upd) return;
+  __shared__ MeteoRec recs[3][2];
+  if (threadIdx.x < 6) {
+    const int kind = threadIdx.x >> 1, itw = threadIdx.x & 1;
+    const MeteoGrid& g = S.mg[kind];
+    if (g.nt > 0) recs[kind][itw] = meteo_rec(g, itw == 0 ? P.mt0 : P.mt1, kind == 2 && S.ampr_block);
+  }
+  __syncthreads();
+  const float cosrot = S.cosrot, sinrot = S.sinrot;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S.nmeteo; i += gridDim.x * blockDim.x) {
+    const int64_t c = S.cmp ? (int64_t)S.cmp[i] : (int64_t)i;
+    const float x = S.xz[i], y = S.yz[i];
+    for (int itw = 0; itw < 2; itw++) {
+      if (S.mg[0].nt > 0) {  // wind stress (:862-936)
+        float wup, wvp, tu = 0.0f, tv = 0.0f;
+        if (meteo_at(S.mg[0], S.mg[0].v0, S.mg[0].v1, recs[0][itw], x, y, wup, wvp)) {
+          const float vmag = sqrtf(wup * wup + wvp * wvp);
+          const int icd = min(max((int)(vmag * 10.0f) + 1, 1), 1000);
+          const float cd = S.cdval[icd - 1];
+          tu = vmag * (cosrot * wup + sinrot * wvp) * S.rhoa * cd / S.rhow;
+          tv = vmag * (-sinrot * wup + cosrot * wvp) * S.rhoa * cd / S.rhow;
+        }
+        (itw == 0 ? S.tauwu0 : S.tauwu1)[c] = tu;
+        (itw == 0 ? S.tauwv0 : S.tauwv1)[c] = tv;
+      }
+      if (S.mg[1].nt > 0 && S.patmos) {  // pressure (:1035-1080), outside the grid gapres
+        float p, unused;
+        if (!meteo_at(S.mg[1], S.mg[1].v0, nullptr, recs[1][itw], x, y, p, unused)) p = S.gapres;
+        (itw == 0 ? S.patm0 : S.patm1)[c] = p;
+      }
+      if (S.mg[2].nt > 0) {  // rain in mm/h to m/s (:1160-1232), outside the grid 0
+        float pr, unused;
+        if (!meteo_at(S.mg[2], S.mg[2].v0, nullptr, recs[2][itw], x, y, pr, unused)) pr = 0.0f;
+        else pr = pr / (float)(1000 * 3600);
+        (itw == 0 ? S.prcp0 : S.prcp1)[c] = pr;
+      }
+    }
+  }
+}
+
+void launch_meteo_window(const ScnDev* d_scns, int nscn, int max_cells, cudaStream_t s) {
+  const int blocks = max(1, min((max_cells + 255) / 256, 1184));
+  launch_pdl(k_meteo_window, dim3(blocks, nscn), dim3(256), 0, s, d_scns);
+}
+
+// --------------------------------------------------------------------------
 // k_momentum: one thread per uv face.
 // --------------------------------------------------------------------------
 template <bool SG, int DIR>
@@ -635,9 +754,10 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepVals& 
   a.uu_ndm = uu_ndm;
   a.uu_num = uu_num;
   a.vu = (v0 + v1 + v2 + v3) / 4.0f;
-  float q, uv;
+  float q, uv, tauw, dpatm;
+  face_meteo(S, sv, DIR, c, c + du, tauw, dpatm);
   const float ghu = face_flux_geo<SG>(S, sv, DIR, (f & ADV) != 0, (f & TH) != 0, geo, kf, zs_nm, zs_nmu, hu, gnavg2,
-                                      phi, a, dry_nm, dry_nmu, zd_nm, zd_nmu, q, uv);
+                                      phi, a, dry_nm, dry_nmu, zd_nm, zd_nmu, tauw, dpatm, q, uv);
   const float den = fmaxf(sqrtf(ghu), fabsf(uv)) * geo.dxuvinv;
   Qn[c] = q;
   Un[c] = uv;
@@ -793,12 +913,17 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
   // infiltration with state (or cumulative rain) for every active cell, from the start-of-step state
   const bool inf_cell = S.precip && (S.inftype >= 2 || S.store_cumprcp);
   float qinf_cell = 0.0f;
+  // rain of the cell: uniform from a time series, or from the gridded field
+  float prc = st.ptmp, netr = st.ptmp;
+  if (S.prcp_field)
+    prc = cell_rain(S, c, meteo_weights(S, st.t, st.meteo_t0, st.meteo_t1), SG ? v_old <= 0.0 : zs_old <= S.zb[c],
+                    netr);
   if (inf_cell) {
     if (SG) {
-      qinf_cell = cell_infiltration(S, c, st.ptmp, dt, v_old <= 0.0, (float)(v_old / (double)S.area), st.ga_hs);
+      qinf_cell = cell_infiltration(S, c, prc, dt, v_old <= 0.0, (float)(v_old / (double)S.area), st.ga_hs);
     } else {
       const float zb0 = S.zb[c];
-      qinf_cell = cell_infiltration(S, c, st.ptmp, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
+      qinf_cell = cell_infiltration(S, c, prc, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
     }
   }
   if (f & F_KCS1) {
@@ -808,7 +933,7 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
         float dzsdt = 0.0f;
         if (S.precip) {
           const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && v_old > 0.0) ? qi : 0.0f);  // sfincs_infiltration.f90:639-670
-          dzsdt = dzsdt + (st.ptmp - qinfmap);
+          dzsdt = dzsdt + (netr - qinfmap);
         }
         if (S.use_qext) dzsdt = dzsdt + qx;
         dvol = dvol + dzsdt * S.area * dt;
@@ -838,7 +963,7 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
       float z = zs_old;
       if (S.precip) {
         const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && !(z <= zbc)) ? qi : 0.0f);
-        z = z + (st.ptmp - qinfmap) * dt;
+        z = z + (netr - qinfmap) * dt;
       }
       if (S.use_qext) z = z + qx * dt;
       z = z + ((q_md - q_mu) * S.dxinv + (q_nd - q_nu) * S.dyinv) * dt;

@@ -28,7 +28,9 @@ __device__ __forceinline__ float qt_warp_max(float v) {
 // Momentum of one uv point per thread (sfincs_momentum.f90:157-752, quadtree
 // branches).  Dry points get q = uv = 0; points that are not momentum points
 // (kcuv 0, boundary faces) are left alone.
-template <bool SG>
+// MET: gridded wind or pressure fields (a separate instance, so that the
+// plain path keeps its register allocation)
+template <bool SG, bool MET>
 __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
   pdl_wait();  // the previous kernel of the step has completed
   pdl_trigger();
@@ -119,9 +121,11 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
           dry0 = zs_nm < S.zb[f.nm];
           dry1 = zs_nmu < S.zb[f.nmu];
         }
-        float qn, un;
+        float qn, un, tauw = dir == 0 ? sv.twu : sv.twv, dpatm = 0.0f;
+        if (MET) face_meteo(S, sv, dir, f.nm, f.nmu, tauw, dpatm);
         const float ghu = face_flux_geo<SG>(S, sv, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kfuv[i],
-                                            zs_nm, zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, qn, un);
+                                            zs_nm, zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, tauw, dpatm, qn,
+                                            un);
         den = fmaxf(sqrtf(ghu), fabsf(un)) * geo.dxuvinv;  // the face's own spacing (refinement level)
         q1[i] = qn;
         uv1[i] = un;
@@ -157,7 +161,8 @@ __global__ void __launch_bounds__(256) k_qt_cuv(const ScnDev* __restrict__ scns,
 
 // Continuity of one cell per thread (sfincs_continuity.f90:46-262 and
 // 265-624, quadtree spacing per refinement level).
-template <bool SG>
+// EXT: infiltration with state, cumulative sums, gridded rain, store variables
+template <bool SG, bool EXT>
 __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict__ scns,
                                                         const Tile* __restrict__ tiles) {
   pdl_wait();  // the previous kernel of the step has completed
@@ -174,16 +179,20 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
   const float dt = st.dt;
   float zsn = zs_old;
   // infiltration with state (or cumulative rain) for every active cell, from the start-of-step state
-  const bool inf_cell = S.precip && (S.inftype >= 2 || S.store_cumprcp);
+  const bool inf_cell = EXT && S.precip && (S.inftype >= 2 || S.store_cumprcp);
   float qinf_cell = 0.0f;
+  // rain of the cell: uniform from a time series, or from the gridded field
+  float prc = st.ptmp, netr = st.ptmp;
+  if (EXT && S.prcp_field)
+    prc = cell_rain(S, c, meteo_weights(S, st.t, st.meteo_t0, st.meteo_t1), SG ? S.zvol[c] <= 0.0 : zs_old <= S.zb[c],
+                    netr);
   if (inf_cell) {
     if (SG) {
       const double v0 = S.zvol[c];
-      qinf_cell = cell_infiltration(S, c, st.ptmp, dt, v0 <= 0.0, (float)(v0 / (double)S.lv_area[S.qlev[c]]),
-                                    st.ga_hs);
+      qinf_cell = cell_infiltration(S, c, prc, dt, v0 <= 0.0, (float)(v0 / (double)S.lv_area[S.qlev[c]]), st.ga_hs);
     } else {
       const float zb0 = S.zb[c];
-      qinf_cell = cell_infiltration(S, c, st.ptmp, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
+      qinf_cell = cell_infiltration(S, c, prc, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
     }
   }
   if (fl & F_KCS1) {
@@ -202,7 +211,7 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
         float dzsdt = 0.0f;
         if (S.precip) {
           const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && v_old > 0.0) ? qi : 0.0f);
-          dzsdt = dzsdt + (st.ptmp - qinfmap);
+          dzsdt = dzsdt + (netr - qinfmap);
         }
         if (S.use_qext) dzsdt = dzsdt + qx;
         dvol = dvol + dzsdt * area * dt;
@@ -232,14 +241,14 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
       if (S.precip) {
         const float zbc = S.infiltration ? S.zb[c] : 0.0f;
         const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && !(z <= zbc)) ? qi : 0.0f);
-        z = z + (st.ptmp - qinfmap) * dt;
+        z = z + (netr - qinfmap) * dt;
       }
       if (S.use_qext) z = z + qx * dt;
       z = z + ((q_md - q_mu) * S.lv_dxrinv[L] + (q_nd - q_nu) * S.lv_dyrinv[L]) * dt;
       if (z != zs_old) S.zs[c] = z;
       zsn = z;
     }
-    if (S.store_vmax | S.store_qmax | S.store_twet) {
+    if (EXT && (S.store_vmax | S.store_qmax | S.store_twet)) {
       float u_md = 0.0f, u_mu = 0.0f, u_nd = 0.0f, u_nu = 0.0f;
       if (S.store_vmax) {  // this step's velocities at the cell's uv points (combined points included)
         const float* uv = S.uu[st.parity ^ 1];
@@ -254,27 +263,26 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
   }
   if (S.store_zsmax) {
     const float zm = S.zsmax[c];
-    if (S.store_tzsmax) store_tzsmax(S, c, zsn, zm, SG ? S.zz_min[c] : S.zb[c]);
+    if (EXT && S.store_tzsmax) store_tzsmax(S, c, zsn, zm, SG ? S.zz_min[c] : S.zb[c]);
     if (zsn > zm) S.zsmax[c] = zsn;
   }
 }
 
-void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {
+void launch_qt_momentum(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, bool met, cudaStream_t s) {
   if (ntiles <= 0) return;
-  if (subgrid)
-    launch_pdl(k_qt_momentum<true>, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
-  else
-    launch_pdl(k_qt_momentum<false>, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
+  auto k = subgrid ? (met ? k_qt_momentum<true, true> : k_qt_momentum<true, false>)
+                   : (met ? k_qt_momentum<false, true> : k_qt_momentum<false, false>);
+  launch_pdl(k, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
 }
 void launch_qt_cuv(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, cudaStream_t s) {
   if (ntiles > 0) launch_pdl(k_qt_cuv, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
 }
-void launch_qt_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, cudaStream_t s) {
+void launch_qt_continuity(const ScnDev* d_scns, const Tile* d_tiles, int ntiles, int subgrid, bool ext,
+                          cudaStream_t s) {
   if (ntiles <= 0) return;
-  if (subgrid)
-    launch_pdl(k_qt_continuity<true>, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
-  else
-    launch_pdl(k_qt_continuity<false>, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
+  auto k = subgrid ? (ext ? k_qt_continuity<true, true> : k_qt_continuity<true, false>)
+                   : (ext ? k_qt_continuity<false, true> : k_qt_continuity<false, false>);
+  launch_pdl(k, dim3(ntiles), dim3(256), 0, s, d_scns, d_tiles);
 }
 
 }  // namespace sfg

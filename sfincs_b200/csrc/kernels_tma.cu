@@ -95,7 +95,7 @@ constexpr int W_ZS = 36, W_QU = 36, W_QV = 40, W_UV = 40;
 constexpr int O_ZS = 0, O_QU = 1408, O_QV = 2944, O_UU = 4480, O_VV = 6144, O_FLAGS = 7808, O_KFU = 8320,
               O_KFV = 8576;
 constexpr int O_VNEG = 8832, O_ZSD = 9344, O_SGZU = 10752, O_SGZV = 12800;       // subgrid
-// subgrid record-cache codes: one byte per face (the 24-byte entries are read per thread)
+// subgrid record-cache codes: one byte per face (the 16 + 8-byte entries are read per thread)
 constexpr int O_RLU = 14848, O_RLV = 15104;
 constexpr int O_ZB = 8832, O_ZBMXU = 10240, O_ZBMXV = 11264, O_GN2U = 12288, O_GN2V = 13312;  // regular
 constexpr int STAGE = 14848, STAGE_SG = 15360;
@@ -166,11 +166,11 @@ __device__ __forceinline__ bool issue_momentum(const ScnDev& S, const MapSet* ma
 
 // Regular-grid face of direction DIR: spacing and switches from the scenario
 // and the cell's flag bits.
-template <bool SG, int DIR>
+template <bool SG, int DIR, bool MET>
 __device__ __forceinline__ float face_flux(const ScnDev& S, const StepVals& st, uint16_t f, uint8_t kf, float zs_nm,
                                            float zs_nmu, float hu, float gnavg2, float phi, const FaceV& a,
-                                           bool dry_nm, bool dry_nmu, float zd_nm, float zd_nmu, float& q_out,
-                                           float& uv_out) {
+                                           bool dry_nm, bool dry_nmu, float zd_nm, float zd_nmu, int64_t c,
+                                           float& q_out, float& uv_out) {
   constexpr uint16_t ADV = DIR == 0 ? F_UADV : F_VADV;
   constexpr uint16_t TH = DIR == 0 ? F_UTH : F_VTH;
   FaceGeo geo;
@@ -179,8 +179,12 @@ __device__ __forceinline__ float face_flux(const ScnDev& S, const StepVals& st, 
   geo.dxuv2inv = DIR == 0 ? S.dx2inv : S.dy2inv;
   geo.dyuv2inv = DIR == 0 ? S.dy2inv : S.dx2inv;
   geo.nuvisc = S.nuvisc;
+  // MET: a gridded wind or pressure field is present (a separate kernel
+  // instance, so that the plain path keeps its register allocation)
+  float tauw = DIR == 0 ? st.twu : st.twv, dpatm = 0.0f;
+  if (MET) face_meteo(S, st, DIR, c, DIR == 0 ? c + S.ld : c + 1, tauw, dpatm);
   return face_flux_geo<SG>(S, st, DIR, (f & ADV) != 0, (f & TH) != 0, geo, kf, zs_nm, zs_nmu, hu, gnavg2, phi, a,
-                           dry_nm, dry_nmu, zd_nm, zd_nmu, q_out, uv_out);
+                           dry_nm, dry_nmu, zd_nm, zd_nmu, tauw, dpatm, q_out, uv_out);
 }
 
 // Subgrid depth / roughness / wet fraction at the face level zsu (sfincs_momentum.f90:345-380).
@@ -197,7 +201,7 @@ struct SgLook {
 // it on through shared memory; the step scalars are read once per scenario.
 // NST stages: the loads of a tile are issued NST - 1 tiles before its update
 // (one CTA barrier per tile orders the reuse of a stage).
-template <bool SG, int MINB, bool ONE, int NST>
+template <bool SG, int MINB, bool ONE, int NST, bool MET>
 __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __restrict__ scns,
                                                             const MapSet* __restrict__ maps,
                                                             const Tile* __restrict__ tiles, int ntiles,
@@ -305,10 +309,10 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
           // table's, bit for bit.
           const int kc = ty * 32 + tx;
           auto look = [&](bool wet, float zsu, float zmin, float zmax, const float4* W, const UvRec* R, int o_rl,
-                          float* rc, uint8_t* rl, SgLook& L) {
+                          float4* rc4, float2* rc2, uint8_t* rl, SgLook& L) {
             if (!wet) return;
-            const float2* eg = reinterpret_cast<const float2*>(rc + 6 * c);
-            const float2 a = eg[0], b = eg[1], d = eg[2];
+            const float4 a = rc4[c];
+            const float2 d = rc2[c];
             L.full = zsu > zmax;
             int code = kRecFull;
             const UvRec* r = nullptr;
@@ -319,7 +323,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               code = lv.iuv;
             }
             if (code == (int)(sm + o_rl)[kc]) {
-              L.v = make_float4(a.x, a.y, b.x, b.y);
+              L.v = a;
               L.v2 = d;
             } else {
               if (L.full) {
@@ -329,15 +333,13 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
                 L.v = *reinterpret_cast<const float4*>(r);
                 L.v2 = *reinterpret_cast<const float2*>(&r->pwet);
               }
-              float2* e = reinterpret_cast<float2*>(rc + 6 * c);
-              e[0] = make_float2(L.v.x, L.v.y);
-              e[1] = make_float2(L.v.z, L.v.w);
-              e[2] = L.v2;
+              rc4[c] = L.v;
+              rc2[c] = L.v2;
               rl[c] = (uint8_t)code;
             }
           };
-          look(wet_u, zsu_u, zmin_u, zmax_u, S.sgw_u, S.rec_u, mom::O_RLU, S.rc_u, S.rl_u, lu);
-          look(wet_v, zsu_v, zmin_v, zmax_v, S.sgw_v, S.rec_v, mom::O_RLV, S.rc_v, S.rl_v, lv);
+          look(wet_u, zsu_u, zmin_u, zmax_u, S.sgw_u, S.rec_u, mom::O_RLU, S.rc4_u, S.rc2_u, S.rl_u, lu);
+          look(wet_v, zsu_v, zmin_v, zmax_v, S.sgw_v, S.rec_v, mom::O_RLV, S.rc4_v, S.rc2_v, S.rl_v, lv);
         }
         // ---- u face
         if (act_u) {
@@ -383,8 +385,8 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               hu = fmaxf(zsu_u - zmin_u, S.huthresh);
               gnavg2 = ((const float*)(sm + mom::O_GN2U))[ty * 32 + tx];
             }
-            cfl.ghu_u = fmaxf(cfl.ghu_u, face_flux<SG, 0>(S, sv, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1,
-                                                          zd0, zd1, qn, un));
+            cfl.ghu_u = fmaxf(cfl.ghu_u, face_flux<SG, 0, MET>(S, sv, f, kfu, zs_c, zs_u, hu, gnavg2, phi, a, dry0, dry1,
+                                                          zd0, zd1, c, qn, un));
             cfl.uv_u = fmaxf(cfl.uv_u, fabsf(un));
             S.qu[p ^ 1][c] = qn;
             S.uu[p ^ 1][c] = un;
@@ -440,8 +442,8 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
               hu = fmaxf(zsu_v - zmin_v, S.huthresh);
               gnavg2 = ((const float*)(sm + mom::O_GN2V))[ty * 32 + tx];
             }
-            cfl.ghu_v = fmaxf(cfl.ghu_v, face_flux<SG, 1>(S, sv, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1,
-                                                          zd0, zd1, qn, un));
+            cfl.ghu_v = fmaxf(cfl.ghu_v, face_flux<SG, 1, MET>(S, sv, f, kfv, zs_c, zs_v, hu, gnavg2, phi, a, dry0, dry1,
+                                                          zd0, zd1, c, qn, un));
             cfl.uv_v = fmaxf(cfl.uv_v, fabsf(un));
             S.qv[p ^ 1][c] = qn;
             S.vv[p ^ 1][c] = un;
@@ -500,7 +502,10 @@ __device__ __forceinline__ bool issue_continuity(const ScnDev& S, const MapSet* 
   return true;
 }
 
-template <bool SG, bool ONE>
+// EXT: the instance with the extended per-cell work (infiltration with
+// state, cumulative sums, gridded rain, store variables); the plain instance
+// keeps the register allocation of the common path.
+template <bool SG, bool ONE, bool EXT>
 __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restrict__ scns, const MapSet* __restrict__ maps,
                                                         const Tile* __restrict__ tiles, int ntiles,
                                                         const __grid_constant__ ScnDev one) {
@@ -568,15 +573,22 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
           const float dt = sv.dt;
           float zsn = zs_old;
           // infiltration with state (or cumulative rain) for every active cell, from the start-of-step state
-          const bool inf_cell = S.precip && (S.inftype >= 2 || S.store_cumprcp);
+          const bool inf_cell = EXT && S.precip && (S.inftype >= 2 || S.store_cumprcp);
           float qinf_cell = 0.0f;
+          // rain of the cell: uniform from a time series, or from the gridded field
+          float prc = sv.ptmp, netr = sv.ptmp;
+          if (EXT && S.prcp_field) {
+            const StepState& st0 = *S.st;
+            const bool dry = SG ? ((const double*)(sm + con::O_ZVOL))[k] <= 0.0 : zs_old <= S.zb[c];
+            prc = cell_rain(S, c, meteo_weights(S, st0.t, st0.meteo_t0, st0.meteo_t1), dry, netr);
+          }
           if (inf_cell) {
             if (SG) {
               const double v0 = ((const double*)(sm + con::O_ZVOL))[k];
-              qinf_cell = cell_infiltration(S, c, sv.ptmp, dt, v0 <= 0.0, (float)(v0 / (double)S.area), S.st->ga_hs);
+              qinf_cell = cell_infiltration(S, c, prc, dt, v0 <= 0.0, (float)(v0 / (double)S.area), S.st->ga_hs);
             } else {
               const float zbc = S.zb[c];
-              qinf_cell = cell_infiltration(S, c, sv.ptmp, dt, zs_old <= zbc, (float)((double)zs_old - (double)zbc),
+              qinf_cell = cell_infiltration(S, c, prc, dt, zs_old <= zbc, (float)((double)zs_old - (double)zbc),
                                             S.st->ga_hs);
             }
           }
@@ -593,7 +605,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
                 float dzsdt = 0.0f;
                 if (S.precip) {
                   const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && v_old > 0.0) ? qi : 0.0f);
-                  dzsdt = dzsdt + (sv.ptmp - qinfmap);
+                  dzsdt = dzsdt + (netr - qinfmap);
                 }
                 if (S.use_qext) dzsdt = dzsdt + qx;
                 dvol = dvol + dzsdt * S.area * dt;
@@ -634,14 +646,14 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
               if (S.precip) {
                 const float zbc = S.infiltration ? ((const float*)(sm + con::O_ZB))[k] : 0.0f;
                 const float qinfmap = inf_cell ? qinf_cell : ((S.infiltration && !(z <= zbc)) ? qi : 0.0f);
-                z = z + (sv.ptmp - qinfmap) * dt;
+                z = z + (netr - qinfmap) * dt;
               }
               if (S.use_qext) z = z + qx * dt;
               z = z + ((q_md - q_mu) * S.dxinv + (q_nd - q_nu) * S.dyinv) * dt;
               if (z != zs_old) S.zs[c] = z;
               zsn = z;
             }
-            if (S.store_vmax | S.store_qmax | S.store_twet) {
+            if (EXT && (S.store_vmax | S.store_qmax | S.store_twet)) {
               float u_md = 0.0f, u_mu = 0.0f, u_nd = 0.0f, u_nu = 0.0f;
               if (S.store_vmax) {
                 const int p1 = sv.parity ^ 1;  // this step's velocities
@@ -655,7 +667,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
             }
           }
           if (S.store_zsmax) {
-            if (S.store_tzsmax) store_tzsmax(S, c, zsn, zm, SG ? S.zz_min[c] : S.zb[c]);
+            if (EXT && S.store_tzsmax) store_tzsmax(S, c, zsn, zm, SG ? S.zz_min[c] : S.zb[c]);
             if (zsn > zm) S.zsmax[c] = zsn;
           }
         }
@@ -677,17 +689,28 @@ int continuity_tma_smem() { return 2 * con::STAGE; }
 // or null for an ensemble table.
 int momentum_tma_smem(int form, int subgrid) { return 2 * (subgrid ? mom::STAGE_SG : mom::STAGE); }
 
-template <bool SG, bool ONE>
+template <bool SG, bool ONE, bool MET>
 static const void* momentum_fn(int form) {
-  return form == 5 ? (const void*)k_momentum_tma<SG, 4, ONE, 2> : (const void*)k_momentum_tma<SG, 3, ONE, 2>;
+  return form == 5 ? (const void*)k_momentum_tma<SG, 4, ONE, 2, MET> : (const void*)k_momentum_tma<SG, 3, ONE, 2, MET>;
 }
+// form + 10: the instance with gridded wind / pressure fields
 const void* momentum_tma_fn(int subgrid, int form, bool one) {
-  if (one) return subgrid ? momentum_fn<true, true>(form) : momentum_fn<false, true>(form);
-  return subgrid ? momentum_fn<true, false>(form) : momentum_fn<false, false>(form);
+  const bool met = form >= 10;
+  form = form % 10;
+  if (met) {
+    if (one) return subgrid ? momentum_fn<true, true, true>(form) : momentum_fn<false, true, true>(form);
+    return subgrid ? momentum_fn<true, false, true>(form) : momentum_fn<false, false, true>(form);
+  }
+  if (one) return subgrid ? momentum_fn<true, true, false>(form) : momentum_fn<false, true, false>(form);
+  return subgrid ? momentum_fn<true, false, false>(form) : momentum_fn<false, false, false>(form);
 }
-const void* continuity_tma_fn(int subgrid, bool one) {
-  if (one) return subgrid ? (const void*)k_continuity_tma<true, true> : (const void*)k_continuity_tma<false, true>;
-  return subgrid ? (const void*)k_continuity_tma<true, false> : (const void*)k_continuity_tma<false, false>;
+template <bool EXT>
+static const void* continuity_fn(int subgrid, bool one) {
+  if (one) return subgrid ? (const void*)k_continuity_tma<true, true, EXT> : (const void*)k_continuity_tma<false, true, EXT>;
+  return subgrid ? (const void*)k_continuity_tma<true, false, EXT> : (const void*)k_continuity_tma<false, false, EXT>;
+}
+const void* continuity_tma_fn(int subgrid, bool one, bool ext) {
+  return ext ? continuity_fn<true>(subgrid, one) : continuity_fn<false>(subgrid, one);
 }
 
 void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
@@ -702,22 +725,12 @@ void launch_momentum_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile*
 }
 
 void launch_continuity_tma(const ScnDev* d_scns, const MapSet* d_maps, const Tile* d_tiles, int ntiles, int subgrid,
-                           int grid, cudaStream_t s, const ScnDev* one) {
+                           int grid, cudaStream_t s, const ScnDev* one, bool ext) {
   if (ntiles <= 0) return;
   static const ScnDev none{};
-  const ScnDev& o = one ? *one : none;
-  const dim3 blk(32, 8);
-  if (one) {
-    if (subgrid)
-      launch_pdl(k_continuity_tma<true, true>, dim3(grid), dim3(blk), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, o);
-    else
-      launch_pdl(k_continuity_tma<false, true>, dim3(grid), dim3(blk), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, o);
-  } else {
-    if (subgrid)
-      launch_pdl(k_continuity_tma<true, false>, dim3(grid), dim3(blk), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, o);
-    else
-      launch_pdl(k_continuity_tma<false, false>, dim3(grid), dim3(blk), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, o);
-  }
+  using Kernel = void (*)(const ScnDev*, const MapSet*, const Tile*, int, ScnDev);
+  const Kernel k = reinterpret_cast<Kernel>(const_cast<void*>(continuity_tma_fn(subgrid, one != nullptr, ext)));
+  launch_pdl(k, dim3(grid), dim3(32, 8), 2 * con::STAGE, s, d_scns, d_maps, d_tiles, ntiles, one ? *one : none);
 }
 
 }  // namespace sfg

@@ -145,6 +145,21 @@ struct alignas(16) StepState {
   int itbndlast, itprcplast, itwndlast, itsrclast;
   int fault;           // nonzero: a bounded wait in a staged kernel gave up (its tile was skipped)
   float ga_hs;         // Green-Ampt: GA_head * GA_sigma of the model's last cell at the start of the step
+  // gridded meteo update window (sfincs_lib.f90:493-503), real*4 like the reference
+  float twindupd;      // next window start
+  float meteo_t0, meteo_t1;
+  int pad_m;
+};
+
+// One gridded meteo quantity on an equidistant grid (ASCII amu/amv, amp,
+// ampr; sfincs_spiderweb.f90:135-230): nt records of nrows x ncols values,
+// the first row at the top, as the file holds them.
+struct MeteoGrid {
+  int nt, nrows, ncols, pad;
+  float x_ll, y_ll, dx, dy;
+  const float* times;  // [nt] seconds after tref
+  const float* v0;     // [nt][nrows][ncols]: amu, amp or ampr
+  const float* v1;     // amv (wind only)
 };
 
 struct ScnDev {
@@ -187,13 +202,17 @@ struct ScnDev {
   const float* zz_max;
   const float* zz_volmax;
   const float2* zlev;    // [level][cell]: (dep_k, dep_k+1 - dep_k)
-  // Per-face record cache (regular subgrid grids, TMA kernels).  rc: 6 floats
-  // per face, the table values the face used last step (UvRec fields havg ..
-  // dpwet for level k, or the full-branch coefficients sgw); rl: what rc
-  // holds, 0 = nothing, k + 1 = level k, kRecFull = the full branch.  Both
-  // depend on (face, level) only, so an entry never goes stale.
-  float* rc_u;
-  float* rc_v;
+  // Per-face record cache (regular subgrid grids, TMA kernels): the table
+  // values the face used last step, in two arrays so that a warp reads whole
+  // lines with one 16-byte and one 8-byte load per face: rc4 = (havg, dhavg,
+  // nrep, dnrep) of level k or the full-branch coefficients sgw, rc2 = (pwet,
+  // dpwet); rl: what they hold, 0 = nothing, k + 1 = level k, kRecFull = the
+  // full branch.  Both depend on (face, level) only, so an entry never goes
+  // stale.
+  float4* rc4_u;
+  float4* rc4_v;
+  float2* rc2_u;
+  float2* rc2_v;
   uint8_t* rl_u;
   uint8_t* rl_v;
   // The same for the volume-to-level inversion: zc holds the z_level pair of
@@ -256,6 +275,25 @@ struct ScnDev {
   uint8_t* inf_rain;
   float* cumprcp;        // cumulative rain and infiltration (m), when stored or needed (cna, cnb)
   float* cuminf;
+  // gridded meteo (sfincs_meteo.f90:802-1442): the raw grids (0 wind, 1
+  // pressure, 2 rain), the cell centres they are interpolated to (compact
+  // order, cmp: compact cell -> storage offset, null when they coincide), the
+  // two fields of the current update window per cell, and the switches
+  int meteo3d, patmos, wind_field, prcp_field, spinup_meteo, ampr_block;
+  int nmeteo;            // cells the fields cover (compact count)
+  float dtwnd, gapres, pavbnd, cosrot, sinrot;
+  MeteoGrid mg[3];
+  const float* xz;
+  const float* yz;
+  const int32_t* cmp;
+  float* tauwu0;
+  float* tauwu1;
+  float* tauwv0;
+  float* tauwv1;
+  float* patm0;
+  float* patm1;
+  float* prcp0;
+  float* prcp1;
   int h73table;          // hu**(7/3) from the lookup table (sfincs_momentum.f90:663-675)
   const float* x73;      // [10][1000] the table x73(j, k) at (k - 1) * 1000 + j - 1 (sfincs_data.f90:858-881)
   StepState* st;
@@ -338,6 +376,47 @@ __device__ __forceinline__ void store_cell_variables(const ScnDev& S, int64_t c,
 // before this step's update.
 __device__ __forceinline__ void store_tzsmax(const ScnDev& S, int64_t c, float zsn, float zm, float base) {
   if (zsn > zm && (double)zsn - (double)base > (double)S.huthresh) S.tzsmax[c] = (float)S.st->t;
+}
+
+// Time weights of the gridded meteo fields at model time t
+// (update_meteo_forcing, sfincs_meteo.f90:1272-1274, 1349-1352): the window
+// weight and, while the meteo spins up, the spin-up factor.
+struct MeteoW {
+  float twf, smf;
+  bool spin;
+};
+__device__ __forceinline__ MeteoW meteo_weights(const ScnDev& S, double t, float mt0, float mt1) {
+  MeteoW w;
+  w.twf = (float)((t - (double)mt0) / (double)(mt1 - mt0));
+  w.spin = S.spinup_meteo && t < (double)(S.tspinup - 1.0e-3f);
+  w.smf = w.spin ? (float)((t - (double)S.t0) / (double)(S.tspinup - S.t0)) : 1.0f;
+  return w;
+}
+// Pressure of storage cell c this step (:1302-1304, 1364-1366).
+__device__ __forceinline__ float cell_patm(const ScnDev& S, int64_t c, const MeteoW& w) {
+  float p = S.patm0[c] * (1.0f - w.twf) + S.patm1[c] * w.twf;
+  if (w.spin) p = p * w.smf + S.gapres * (1.0f - w.smf);
+  return p;
+}
+// Wind stress of storage cell c in direction dir this step (:1282-1288, 1357-1360).
+__device__ __forceinline__ float cell_tau(const ScnDev& S, int64_t c, int dir, const MeteoW& w) {
+  const float* a = dir == 0 ? S.tauwu0 : S.tauwv0;
+  const float* b = dir == 0 ? S.tauwu1 : S.tauwv1;
+  float tw = a[c] * (1.0f - w.twf) + b[c] * w.twf;
+  if (w.spin) tw = tw * w.smf;
+  return tw;
+}
+// Rain of storage cell c this step (:1306-1330, 1368-1394): prcp, and the net
+// rain before infiltration; negative rain is dropped on a dry cell.
+__device__ __forceinline__ float cell_rain(const ScnDev& S, int64_t c, const MeteoW& w, bool dry, float& net) {
+  float pr = S.prcp0[c] * (1.0f - w.twf) + S.prcp1[c] * w.twf;
+  if (pr < 0.0f && dry) pr = 0.0f;
+  net = pr;
+  if (w.spin) {
+    net = net * w.smf;
+    if (net < 0.0f && dry) net = 0.0f;
+  }
+  return pr;
 }
 
 // Exponential from IEEE operations only, so that the oracle reproduces it bit

@@ -2,7 +2,8 @@
 
 An ensemble member is a subgrid regular-grid model (the generator of
 ``synth.subgrid_regular``) with its own size, DEM seed, surge peak and rain
-rate.  The batched form advances all members with the same launches
+rate; a spec with ``kind="quadtree"`` is a quadtree mesh of
+``qtsynth.quadtree_coastal`` instead.  The batched form advances all members with the same launches
 (``bmi.Ensemble``); the plain form solves them one after another
 (``bmi.Model``).
 """
@@ -55,7 +56,13 @@ def generate(specs: List[Dict], root: str = None, device: str = None, log=None) 
         if not os.path.exists(os.path.join(d, "READY")):
             tmp = d + f".tmp{os.getpid()}"
             shutil.rmtree(tmp, ignore_errors=True)
-            m = synth.subgrid_regular(device=device, **spec)
+            kw = dict(spec)
+            if kw.pop("kind", "subgrid") == "quadtree":
+                from . import qtsynth
+
+                m = qtsynth.quadtree_coastal(device=device, **kw)
+            else:
+                m = synth.subgrid_regular(device=device, **kw)
             m.write(tmp)
             open(os.path.join(tmp, "READY"), "w").write("ok\n")
             shutil.rmtree(d, ignore_errors=True)

@@ -278,6 +278,27 @@ def write_sbg(path: str, tables: Dict[str, np.ndarray]) -> None:
     )
 
 
+def write_meteo_grid(path: str, quantity: str, unit: str, x_ll: float, y_ll: float, dx: float, dy: float,
+                     times_s, fields, ref: str = "2000-01-01 00:00:00") -> None:
+    """Write a gridded meteo series in the ASCII equidistant-grid format the
+    reference reads (amu / amv / amp / ampr files): header keys, then per time
+    a ``TIME = <hours> hours since <ref>`` line and the field, top row first.
+    ``fields`` is (nt, nrows, ncols) with row 0 at the bottom (y_ll)."""
+    fields = np.asarray(fields, np.float64)
+    nt, nrows, ncols = fields.shape
+    with open(path, "w") as f:
+        f.write("FileVersion      = 1.03\nfiletype         = meteo_on_equidistant_grid\n"
+                f"NODATA_value     = -999.000\nn_cols           = {ncols}\nn_rows           = {nrows}\n"
+                "grid_unit        = m\n"
+                f"x_llcorner       = {x_ll:.4f}\ny_llcorner       = {y_ll:.4f}\ndx               = {dx:.4f}\n"
+                f"dy               = {dy:.4f}\nn_quantity       = 1\nquantity1        = {quantity}\n"
+                f"unit1            = {unit}\n")
+        for it in range(nt):
+            f.write(f"TIME = {times_s[it] / 3600.0:.6f} hours since {ref} +00:00\n")
+            for row in fields[it][::-1]:
+                f.write(" ".join(f"{v:.4f}" for v in row) + "\n")
+
+
 # ------------------------------------------------------------------ model files
 @dataclass
 class RegularModel:

@@ -73,3 +73,31 @@ def test_served_results_equal_alone(tmp_path):
         assert r.latency_s >= 0 and r.done_s >= r.admitted_s >= r.arrival_s - 1e-9
     assert out["latency_p99_s"] >= out["latency_p50_s"] > 0
     assert out["mean_running"] > 1.0  # requests really overlapped on the device
+
+
+def test_served_mix_of_regular_and_quadtree_equals_alone(tmp_path):
+    """Regular grids and quadtree meshes in one stream: the pool advances them
+    in two runners on two streams, and every result is bitwise the result of
+    the same request alone."""
+    from sfincs_b200 import qtsynth
+
+    dirs = _dirs(tmp_path, 3)
+    for i in range(2):
+        m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=3, bands=(1000.0, 500.0), P=4, seed=40 + i,
+                                     tstop=1500.0 + 600.0 * i, subgrid=i == 1, wind_speed=20.0, tide_period=1800.0)
+        d = tmp_path / f"q{i}"
+        d.mkdir()
+        dirs.append(m.write(str(d)))
+    alone = [_alone(d) for d in dirs]
+    srv = Server(max_slots=4, chunk=8, prep_threads=2)
+    arr = [0.0, 0.0, 0.03, 0.0, 0.02]
+    reqs = [Request(arrival_s=a, model_dir=d, rid=i) for i, (a, d) in enumerate(zip(arr, dirs))]
+    out = srv.serve(reqs, fetch=("zs", "zsmax", "qx", "qy"))
+    srv.close()
+    assert len(out["results"]) == 5
+    for r in out["results"]:
+        a = alone[r.rid]
+        assert r.steps == a["nt"], (r.rid, r.steps, a["nt"])
+        for k in ("zs", "zsmax", "qx", "qy"):
+            assert np.array_equal(r.fields[k], a[k]), (r.rid, k)
+    assert out["mean_running"] > 1.0

@@ -164,16 +164,118 @@ def test_gpu_writes_restart_files_at_output_times(tmp_path):
     g.close()
 
 
-def test_quadtree_restart_output_is_refused(tmp_path):
-    """Restart files on quadtree meshes are not built: asking for restart
-    output there is an error at load, not a file with the fluxes missing."""
+def _qt_restart_dirs(tmp_path, subgrid, steps=40):
+    """A 3-level quadtree model, its oracle state after `steps` steps written
+    as a restart file, and a copy of the model that starts from it."""
+    from oracle.oracle import Oracle
     from sfincs_b200 import bmi as B
     from sfincs_b200 import qtsynth
 
-    m = qtsynth.quadtree_coastal(nmax1=6, mmax1=8, dx1=400.0, nlev=2, bands=(600.0,), P=2, seed=4, tstop=600.0,
-                                 subgrid=False)
-    d = m.write(str(tmp_path))
+    m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=3, bands=(1000.0, 500.0), P=4, seed=21,
+                                 tstop=1800.0, subgrid=subgrid, wind_speed=30.0, tide_period=1800.0)
+    d = m.write(str(tmp_path / "a"))
+    qc = B.layout(d, "qt_counts", 4)
+    npc, npuv, ncuv = int(qc[0]), int(qc[1]), int(qc[2])
+    o = Oracle(d, "f32")
+    o.update(-1000.0, steps)
+    zs, q, uvm = o.get("zs", npc), o.get("q", npuv + ncuv + 1), o.get("uvmean")
+    d2 = str(tmp_path / "b")
+    shutil.copytree(d, d2)
+    write_restart(os.path.join(d2, "sfincs.rst"), zs, q, uvm)
+    with open(os.path.join(d2, "sfincs.inp"), "a") as f:
+        f.write(f"{'rstfile':<20} = sfincs.rst\n")
+    return d, d2, zs, q, npc, npuv, ncuv
+
+
+@pytest.mark.parametrize("subgrid", [False, True])
+def test_quadtree_restart_is_read(tmp_path, subgrid):
+    """Quadtree restart files: zs per cell and q per uv point in the
+    reference's order; the oracle and the core's layout start from them."""
+    from oracle.oracle import Oracle
+    from sfincs_b200 import bmi as B
+
+    d, d2, zs, q, npc, npuv, ncuv = _qt_restart_dirs(tmp_path, subgrid)
+    o = Oracle(d2, "f32")
+    assert np.array_equal(o.get("zs", npc), zs)
+    assert np.array_equal(o.get("q", npuv), q[:npuv])
+    assert np.array_equal(B.layout(d2, "zs", npc), zs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("subgrid", [False, True])
+def test_gpu_quadtree_restart_round_trip(tmp_path, subgrid):
+    """The core started from a quadtree restart file follows the oracle started
+    from it, and the file the core writes (dtrstout) holds its own state in the
+    reference's order and length."""
+    import glob
+
+    from oracle.oracle import Oracle
+    from sfincs_b200.bmi import Model
+
+    d, d2, zs, q, npc, npuv, ncuv = _qt_restart_dirs(tmp_path, subgrid)
+    o = Oracle(d2, "f32")
+    g = Model(d2)
+    assert np.array_equal(g.get("zs").astype(np.float64), zs)
+    done = 0
+    for n in (1, 1, 2, 6, 30):
+        o.update(-1000.0, n)
+        g.step(n)
+        done += n
+        dzs = float(np.abs(o.get("zs", npc) - g.get("zs")).max())
+        assert g.scalars()["nt"] == o.scalars()["nt"]
+        assert dzs <= 2e-5, (done, dzs)
+    g.close()
     with open(os.path.join(d, "sfincs.inp"), "a") as f:
-        f.write(f"{'dtrstout':<20} = 300\n")
-    with pytest.raises(RuntimeError, match="restart output"):
-        B.layout(d, "counts", 10)
+        f.write(f"{'dtrstout':<20} = 600\n")
+    g = Model(d)
+    files = []
+    while not files and g.scalars()["t"] < 900.0:
+        g.step(1)
+        files = sorted(glob.glob(os.path.join(d, "sfincs.*.rst")))
+    zs_now = g.get("zs").astype(np.float32)
+    g.close()
+    assert files
+    typ, zs_f, q_f, uvm_f = read_restart(files[0])
+    assert typ == 1 and zs_f.size == npc and q_f.size == npuv + ncuv + 1
+    assert np.array_equal(zs_f, zs_now)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,flavour", [("cnb", 4), ("gai", 5), ("hor", 6)])
+def test_gpu_restart_flavours_with_infiltration_state(tmp_path, kind, flavour):
+    """With a curve-number-with-recovery, Green-Ampt or Horton model the
+    restart file is flavour 4, 5 or 6 and carries that method's state
+    (sfincs_output.f90:690-722); the core and the oracle started from it stay
+    together step by step."""
+    import glob
+
+    from oracle.oracle import Oracle
+    from sfincs_b200.bmi import Model
+    from test_gpu_physics import _infiltration_fields, _plain, _subgrid
+
+    m = (_subgrid if kind == "hor" else _plain)(tmp_path, dtrstout=600)
+    d = _infiltration_fields(m, kind).write(str(tmp_path / "a"))
+    g = Model(d)
+    g.run(650.0)
+    g.close()
+    files = sorted(glob.glob(os.path.join(d, "sfincs.*.rst")))
+    assert files, "no restart file written"
+    recs = read_restart(files[0])
+    assert recs[0] == flavour
+    n = recs[1].size
+    assert len(recs) == (6 if flavour == 5 else 5) and all(r.size == n for r in recs[4:])
+    d2 = str(tmp_path / "b")
+    shutil.copytree(d, d2)
+    with open(os.path.join(d2, "sfincs.inp"), "a") as f:
+        f.write(f"{'rstfile':<20} = {os.path.basename(files[0])}\n")
+    o = Oracle(d2, "f32")
+    g = Model(d2)
+    done = 0
+    for k in (1, 5, 30, 60):
+        o.update(-1000.0, k)
+        g.step(k)
+        done += k
+        dzs = float(np.abs(o.get("zs") - g.get("zs")).max())
+        assert g.scalars()["nt"] == o.scalars()["nt"]
+        assert dzs <= 2e-5, (done, dzs)
+    g.close()
