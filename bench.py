@@ -448,6 +448,7 @@ def run_ensemble(args, rank: int, world: int, local: int):
     torch.cuda.empty_cache()
     # ---- plain: one model at a time
     ms_p = 0.0
+    ms_each = []
     same = True
     for i, d in enumerate(dirs):
         g = Model(d)
@@ -457,10 +458,16 @@ def run_ensemble(args, rank: int, world: int, local: int):
         g.run(g.scalars()["t1"])
         e1.record(sp)
         e1.synchronize()
-        ms_p += e0.elapsed_time(e1)
+        ms_each.append(e0.elapsed_time(e1))
+        ms_p += ms_each[-1]
         same = same and np.array_equal(g.get("zs"), zs_b[i])
         g.close()
     ms_p = max_over_ranks(ms_p, world)
+    # Where batching stands: the members' step counts differ (per-member dt);
+    # a batched run cannot finish before its longest member alone, so
+    # plain_sum / longest_alone bounds batched_over_plain for any batching.
+    longest = int(np.argmax(ms_each))
+    bound = ms_p / ms_each[longest]
     n_all = len(specs)
     value = n_all / (ms_b / 1e3) * 3600.0
     plain = n_all / (ms_p / 1e3) * 3600.0
@@ -480,6 +487,11 @@ def run_ensemble(args, rank: int, world: int, local: int):
         "plain": {"seconds": ms_p / 1e3, "scenarios_per_h": plain},
         "batched_over_plain": value / plain,
         "alone_equals_mix_bitwise": bool(same),
+        "members": {"cells": [int(c) for c in ncell], "steps": steps_b, "plain_ms": [round(x, 3) for x in ms_each]},
+        "longest_member": {"cells": int(ncell[longest]), "steps": int(steps_b[longest]),
+                           "alone_s": ms_each[longest] / 1e3,
+                           "share_of_batched_time": ms_each[longest] / ms_b},
+        "batched_over_plain_bound": bound,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

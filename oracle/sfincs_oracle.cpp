@@ -83,6 +83,30 @@ static float core_cube_root(float x) {
   return x + x;
 }
 
+// Four-quadrant arctangent in IEEE operations (the core's own: argument
+// reduction by atan(a) = pi/6 + atan((sqrt3 a - 1)/(sqrt3 + a)) above
+// tan(pi/12), then the Taylor series to degree 15).
+static float core_atan2(float y, float x) {
+  const float ax = std::fabs(x), ay = std::fabs(y);
+  const float mx = std::max(ax, ay), mn = std::min(ax, ay);
+  if (mx == 0.0f) return 0.0f;
+  const float a = mn / mx;
+  float t = a, off = 0.0f;
+  if (a > 0.267949194f) {
+    t = (1.73205081f * a - 1.0f) / (1.73205081f + a);
+    off = 0.523598776f;
+  }
+  const float t2 = t * t;
+  const float c[6] = {1.0f / 13.0f, -1.0f / 11.0f, 1.0f / 9.0f, -1.0f / 7.0f, 1.0f / 5.0f, -1.0f / 3.0f};
+  float p = -1.0f / 15.0f;
+  for (int k = 0; k < 6; k++) p = std::fma(p, t2, c[k]);
+  float r = off + std::fma(t * t2, p, t);
+  if (ay > ax) r = 1.57079633f - r;
+  if (x < 0.0f) r = 3.14159265f - r;
+  return y < 0.0f ? -r : r;
+}
+
+
 // Exponential of the core-precision instantiation (Horton infiltration),
 // restating the CUDA core's method with the same IEEE operations: n =
 // rint(x log2 e), r = x - n ln2 with ln2 split in two parts (Cody and Waite),
@@ -336,6 +360,19 @@ struct Model {
   };
   AmGrid amuv, amp, ampr;
   std::string amufile, amvfile, ampfile, amprfile;
+  // spiderweb (sfincs_data.f90:686-762): polar records around the eye track
+  struct SpwData {
+    int nt = 0, nrows = 0, ncols = 0, nquant = 0;
+    float radius = 0, drad = 0, dphi = 0;
+    std::vector<float> times, xe, ye, wu, wv, pabs, prcp;  // [(it-1)*nrows*ncols + (irow-1)*ncols + icol-1]
+    size_t at(int it, int irow, int icol) const {
+      return ((size_t)(it - 1) * nrows + (irow - 1)) * ncols + (icol - 1);
+    }
+  };
+  SpwData spw;
+  std::string spwfile = "none", utmzone = "nil", z0lfile = "none";
+  bool use_spw_precip = true, spw_precip = false;
+  float spw_merge_frac = 0.5f, factor_spw_size = 1.0f;
   bool meteo3d = false, ampr_block = true;
 
   float dtwindupd = 1800.0f, twindupd = 0.0f, meteo_t0 = 0.0f, meteo_t1 = 0.0f, factor_wind = 1.0f,
@@ -425,6 +462,14 @@ struct Model {
     amvfile = in.str("amvfile", "none");
     ampfile = in.str("ampfile", "none");
     amprfile = in.str("amprfile", "none");
+    spwfile = in.str("spwfile", "none");  // sfincs_input.f90:95-108, 203, 236, 247, 601-604
+    utmzone = in.str("utmzone", "nil");
+    z0lfile = in.str("z0lfile", "none");
+    spw_merge_frac = in.real("spwmergefrac", 0.5f);
+    use_spw_precip = in.integer("usespwprecip", 1) != 0;
+    factor_spw_size = in.real("factor_spw_size", 1.0f);
+    if (spwfile.substr(0, 4) != "none" && (utmzone != "nil" || z0lfile.substr(0, 4) != "none"))
+      throw std::runtime_error("oracle: spiderweb reprojection and wind reduction are not restated");
     dtwindupd = in.real("dtwnd", 1800.0f);
     ampr_block = in.integer("amprblock", 1) != 0;
     factor_wind = in.real("factor_wind", 1.0f);
@@ -519,10 +564,10 @@ struct Model {
   void initialize_processes() {
     use_quadtree = qtrfile.substr(0, 4) != "none";
     auto has = [](const std::string& f) { return f.substr(0, 4) != "none"; };
-    wind = has(wndfile) || has(amufile);
-    patmos = has(ampfile) && baro == 1;
-    precip = has(prcpfile) || has(amprfile);
-    meteo3d = has(amufile) || has(amprfile) || has(ampfile);
+    wind = has(wndfile) || has(amufile) || has(spwfile);
+    patmos = (has(ampfile) || has(spwfile)) && baro == 1;
+    precip = has(prcpfile) || has(amprfile) || spw_precip;
+    meteo3d = has(amufile) || has(amprfile) || has(ampfile) || has(spwfile);
   }
 
   // make_quadtree_from_indices: sfincs_quadtree.F90:445-669
@@ -2120,7 +2165,165 @@ struct Model {
     }
   }
 
+  // read_spw_dimensions + read_spw_file: sfincs_spiderweb.f90:8-134, 231-316.
+  // The header keys, the first TIME line within 30 lines (else 16 / 18 header
+  // lines), then per record the TIME line, the eye x and y (twelve characters
+  // after '='), a skipped line, and nrows rows of ncols values per quantity.
+  void read_spw(const std::string& file) {
+    std::ifstream fin(path(file));
+    if (!fin) throw std::runtime_error("oracle: cannot open " + file);
+    std::vector<std::string> lines;
+    for (std::string l; std::getline(fin, l);) {
+      if (!l.empty() && l.back() == '\r') l.pop_back();
+      lines.push_back(l);
+    }
+    auto key = [&](const char* name) {
+      for (const auto& l : lines) {
+        size_t e = l.find('=');
+        if (e == std::string::npos) continue;
+        std::string k = l.substr(0, e);
+        k.erase(0, k.find_first_not_of(" \t"));
+        k.erase(k.find_last_not_of(" \t") + 1);
+        if (k == name) return std::strtod(l.substr(e + 1).c_str(), nullptr);
+      }
+      return 0.0;
+    };
+    SpwData& w = spw;
+    w.ncols = (int)key("n_cols");
+    w.nrows = (int)key("n_rows");
+    w.nquant = (int)key("n_quantity");
+    w.radius = (float)key("spw_radius");
+    long nheader = 0;
+    for (long ip = 1; ip <= 30 && ip <= (long)lines.size(); ip++)
+      if (lines[ip - 1].find("TIME") == 0) {
+        nheader = ip - 1;
+        break;
+      }
+    if (nheader == 0) nheader = w.nquant == 4 ? 18 : 16;
+    const long blk = 4 + (long)w.nrows * w.nquant;
+    w.nt = (int)(((long)lines.size() - nheader) / blk);
+    const size_t rec = (size_t)w.nrows * w.ncols;
+    std::vector<float> vmag(rec * w.nt, 0.0f), vdir(rec * w.nt, 0.0f), pdrp(rec * w.nt, 0.0f);
+    w.prcp.assign(rec * w.nt, 0.0f);
+    long i = nheader;
+    auto eye = [&](const std::string& l) { return std::strtof(l.substr(l.find('=') + 1, 12).c_str(), nullptr); };
+    for (int it = 1; it <= w.nt; it++) {
+      w.times.push_back(meteo_time_seconds(lines[i], trefstr));
+      w.xe.push_back(eye(lines[i + 1]));
+      w.ye.push_back(eye(lines[i + 2]));
+      i += 4;
+      std::vector<float>* qs[4] = {&vmag, &vdir, &pdrp, &w.prcp};
+      for (int q = 0; q < w.nquant; q++)
+        for (int n = 1; n <= w.nrows; n++) {
+          std::istringstream ls(lines[i++]);
+          for (int m = 1; m <= w.ncols; m++) ls >> (*qs[q])[w.at(it, n, m)];
+        }
+    }
+    // sfincs_meteo.f90:65-93: absolute pressure, ring and sector widths, wind components
+    w.pabs.resize(pdrp.size());
+    for (size_t k = 0; k < pdrp.size(); k++) w.pabs[k] = gapres - pdrp[k];
+    w.drad = w.radius / (float)w.nrows;
+    w.dphi = 2.0f * pi / (float)w.ncols;
+    w.wu.resize(vmag.size());
+    w.wv.resize(vmag.size());
+    for (size_t k = 0; k < vmag.size(); k++) {
+      w.wu[k] = vmag[k] * std::cos(pi * (270.0f - vdir[k]) / 180.0f);
+      w.wv[k] = vmag[k] * std::sin(pi * (270.0f - vdir[k]) / 180.0f);
+    }
+    spw_precip = w.nquant == 4 && use_spw_precip;
+  }
+
+  // update_spiderweb_data: sfincs_meteo.f90:450-800 (projected grids, no wave
+  // age, no wind reduction). core: the core's arctangent instead of libm's.
+  void update_spiderweb_data(bool core) {
+    const SpwData& w = spw;
+    for (int itw = 1; itw <= 2; itw++) {
+      const float meteo_t = itw == 1 ? meteo_t0 : meteo_t1;
+      int itw0 = 1, itw1 = 1;
+      float twfac = 1.0f, tspinup_fac = 1.0f;
+      if (meteo_t < w.times[0]) {
+        tspinup_fac = std::max(1.0f - (w.times[0] - meteo_t) / 21600.0f, 0.0f);
+      } else if (meteo_t > w.times[w.nt - 1]) {
+        itw0 = itw1 = w.nt;
+        tspinup_fac = std::max(1.0f - (meteo_t - w.times[w.nt - 1]) / 21600.0f, 0.0f);
+      } else {
+        for (int it = 1; it <= w.nt; it++)
+          if (w.times[it - 1] <= meteo_t) itw0 = it;
+        itw1 = std::min(itw0 + 1, w.nt);
+        twfac = (meteo_t - w.times[itw0 - 1]) / std::max(w.times[itw1 - 1] - w.times[itw0 - 1], 1.0e-6f);
+      }
+      const float xe01 = w.xe[itw0 - 1] * (1.0f - twfac) + w.xe[itw1 - 1] * twfac;
+      const float ye01 = w.ye[itw0 - 1] * (1.0f - twfac) + w.ye[itw1 - 1] * twfac;
+      auto v01 = [&](const std::vector<float>& v, int irow, int icol) {
+        return v[w.at(itw0, irow, icol)] * (1.0f - twfac) + v[w.at(itw1, irow, icol)] * twfac;
+      };
+      F1<float>& tu = itw == 1 ? tauwu0 : tauwu1;
+      F1<float>& tv = itw == 1 ? tauwv0 : tauwv1;
+      F1<float>& pa = itw == 1 ? patm0 : patm1;
+      F1<float>& pr = itw == 1 ? prcp0 : prcp1;
+      for (long nm = 1; nm <= np; nm++) {
+        const float x = z_xz(nm), y = z_yz(nm);
+        const float dxe = x - xe01, dye = y - ye01;
+        const float dstspw = std::sqrt(dxe * dxe + dye * dye);
+        if (amufile.substr(0, 4) == "none") {
+          tu(nm) = 0.0f;
+          tv(nm) = 0.0f;
+        }
+        if (patmos && ampfile.substr(0, 4) == "none") pa(nm) = gapres;
+        if (precip && spw_precip && amprfile.substr(0, 4) == "none") pr(nm) = 0.0f;
+        if (dstspw > w.radius) continue;
+        int idstspw = std::max((int)(dstspw / w.drad), 1);
+        const int ind1[4] = {idstspw, idstspw, idstspw + 1, idstspw + 1};
+        if (ind1[2] > w.nrows) continue;
+        const float dj1 = std::max((dstspw - w.drad * (float)idstspw) / w.drad, 0.0f);
+        float phispw = 0.5f * pi - (core ? core_atan2(dye, dxe) : std::atan2(dye, dxe));
+        const float tp = 2.0f * pi;
+        phispw = phispw - std::floor(phispw / tp) * tp;  // modulo(phispw, 2 pi)
+        const int iphispw = std::min((int)(phispw / w.dphi) + 1, w.ncols);
+        int ind2[4] = {iphispw, iphispw + 1, iphispw + 1, iphispw};
+        if (ind2[1] > w.ncols) ind2[1] = 1;
+        if (ind2[2] > w.ncols) ind2[2] = 1;
+        const float di1 = (phispw - w.dphi * (float)(iphispw - 1)) / w.dphi;
+        const float f[4] = {(1.0f - di1) * (1.0f - dj1), di1 * (1.0f - dj1), di1 * dj1, (1.0f - di1) * dj1};
+        float wup = 0.0f, wvp = 0.0f, prp = 0.0f, pcp = 0.0f;
+        for (int ip = 0; ip < 4; ip++) {
+          wup = wup + f[ip] * v01(w.wu, ind1[ip], ind2[ip]);
+          wvp = wvp + f[ip] * v01(w.wv, ind1[ip], ind2[ip]);
+          if (patmos) pcp = pcp + f[ip] * v01(w.pabs, ind1[ip], ind2[ip]);
+          if (precip && spw_precip) prp = prp + f[ip] * v01(w.prcp, ind1[ip], ind2[ip]);
+        }
+        const float vmag = std::sqrt(wup * wup + wvp * wvp);
+        const float cd = cdval(std::min(std::max((long)(vmag * 10.0f) + 1, 1L), 1000L));
+        float merge_frac = 1.0f;
+        if (dstspw > spw_merge_frac * w.radius)
+          merge_frac = (1.0f / (1.0f - std::min(spw_merge_frac, 0.999f))) * (w.radius - dstspw) / w.radius;
+        merge_frac = merge_frac * tspinup_fac;
+        tu(nm) = (1.0f - merge_frac) * tu(nm) + merge_frac * vmag * (cosrot * wup + sinrot * wvp) * rhoa * cd / rhow;
+        tv(nm) = (1.0f - merge_frac) * tv(nm) + merge_frac * vmag * (-sinrot * wup + cosrot * wvp) * rhoa * cd / rhow;
+        if (patmos) pa(nm) = (1.0f - merge_frac) * pa(nm) + merge_frac * pcp;
+        if (precip && spw_precip) pr(nm) = (1.0f - merge_frac) * pr(nm) + merge_frac * prp / (float)(1000 * 3600);
+      }
+    }
+  }
+
   void read_meteo_data() {
+    // spiderweb first (sfincs_meteo.f90:35-98), factors below (:330-412)
+    if (spwfile.substr(0, 4) != "none") {
+      read_spw(spwfile);
+      if (factor_wind != 1.0f)
+        for (size_t k = 0; k < spw.wu.size(); k++) {
+          spw.wu[k] = factor_wind * spw.wu[k];
+          spw.wv[k] = factor_wind * spw.wv[k];
+        }
+      if (factor_pres != 1.0f)
+        for (auto& x : spw.pabs) x = gapres - factor_pres * (gapres - x);
+      if (spw_precip && factor_prcp != 1.0f)
+        for (auto& x : spw.prcp) x = factor_prcp * x;
+      if (factor_spw_size != 1.0f) {
+        spw.radius = factor_spw_size * spw.radius;
+        spw.drad = spw.radius / (float)spw.nrows;
+      }
+    }
     // gridded fields (sfincs_meteo.f90:146-245) with the enhancement factors (:330-380)
     if (amufile.substr(0, 4) != "none") {
       read_am_file(amufile, amuv, 0);
@@ -2332,6 +2535,7 @@ struct Model {
     if (amufile.substr(0, 4) != "none") update_am_window(amuv, 0);
     if (ampfile.substr(0, 4) != "none" && patmos) update_am_window(amp, 1);
     if (amprfile.substr(0, 4) != "none") update_am_window(ampr, 2);
+    if (spwfile.substr(0, 4) != "none") update_spiderweb_data(std::is_same<TZ, float>::value);
   }
 
   void update_meteo_forcing(double tt, float dtt) {
@@ -3212,6 +3416,9 @@ void* oracle_create(const char* dir, const char* precision, int bmi) {
 
 const char* oracle_last_error() { return g_last_error.c_str(); }
 
+// The core's arctangent (IEEE operations only), for its accuracy test.
+float oracle_core_atan2(float y, float x) { return core_atan2(y, x); }
+
 void oracle_destroy(void* hv) {
   auto* h = static_cast<Handle*>(hv);
   if (!h) return;
@@ -3296,6 +3503,14 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "cuminf" && m.cuminf.allocated()) copy_out(m.cuminf, out, n);
     else if (s == "qext" && m.qext.allocated()) copy_out(m.qext, out, n);
     else if (s == "uvmean") copy_out(m.uvmean, out, n);
+    else if (s == "tauwu0" && m.tauwu0.allocated()) copy_out(m.tauwu0, out, n);
+    else if (s == "tauwv0" && m.tauwv0.allocated()) copy_out(m.tauwv0, out, n);
+    else if (s == "tauwu1" && m.tauwu1.allocated()) copy_out(m.tauwu1, out, n);
+    else if (s == "tauwv1" && m.tauwv1.allocated()) copy_out(m.tauwv1, out, n);
+    else if (s == "patm0" && m.patm0.allocated()) copy_out(m.patm0, out, n);
+    else if (s == "patm1" && m.patm1.allocated()) copy_out(m.patm1, out, n);
+    else if (s == "prcp0" && m.prcp0.allocated()) copy_out(m.prcp0, out, n);
+    else if (s == "prcp1" && m.prcp1.allocated()) copy_out(m.prcp1, out, n);
     else if (s == "nrstructures") out[0] = (double)m.nrstructures;
     else if (s == "struc") {
       // per structure: uv point (1-based), crest level, Cd, relative length

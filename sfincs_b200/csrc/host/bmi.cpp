@@ -150,6 +150,7 @@ struct ModelHandle {
   void run(double tend, long long max_steps, int chunk) {
     if (host->trstout >= 1.0e9) {
       runner->run({tend}, max_steps, chunk);
+      check_fault();
       return;
     }
     long long left = max_steps;
@@ -162,9 +163,17 @@ struct ModelHandle {
         runner->run({std::min(tend, host->trstout)}, left, chunk);
       const StepState s1 = runner->read_state(0);
       if (left > 0) left = std::max(0LL, left - (long long)(s1.nt - s0.nt));
+      check_fault();
       after_step_output();
       if (s1.nt == s0.nt) break;  // stopped (instability or end of the run)
     }
+  }
+  // A staged kernel whose bounded wait for its tile data gave up skipped that
+  // tile and set the fault flag: the run is reported as failed.
+  void check_fault() {
+    if (runner->read_state(0).fault)
+      throw std::runtime_error("a staged kernel gave up waiting for its tile data (fault flag set); the state of "
+                               "this model is incomplete");
   }
   // sfincs_lib.f90:447-463 after a step
   void after_step_output() {
@@ -466,6 +475,7 @@ int update(void) {
     g_bmi->step_once();
     g_bmi->after_update();
     g_bmi->runner->sync();  // the step is complete when update() returns, as in the reference
+    g_bmi->check_fault();
     g_bmi->after_step_output();
     return 0;
   });
@@ -711,6 +721,7 @@ int sfg_model_issue(void* m, int nsteps) {
 int sfg_model_sync(void* m) {
   return guarded([&] {
     static_cast<sfg::ModelHandle*>(m)->runner->sync();
+    static_cast<sfg::ModelHandle*>(m)->check_fault();
     return 0;
   });
 }
@@ -806,6 +817,10 @@ int sfg_ensemble_run(void* ev, const double* t_end, long long max_steps, int chu
     auto* e = static_cast<sfg::EnsembleHandle*>(ev);
     std::vector<double> te(t_end, t_end + e->devs.size());
     e->runner->run(te, max_steps, chunk > 0 ? chunk : 32);
+    for (int i = 0; i < (int)e->devs.size(); i++)
+      if (e->runner->read_state(i).fault)
+        throw std::runtime_error("ensemble member " + std::to_string(i) +
+                                 ": a staged kernel gave up waiting for its tile data (fault flag set)");
     return 0;
   });
 }

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <map>
 #include <type_traits>
 #include <stdexcept>
@@ -179,6 +180,29 @@ void read_meteo_series(HostModel& h, const Keys& k, float rotation) {
     if (h.factor_prcp != 1.0f)
       for (auto& x : h.mgh[2].v[0]) x = h.factor_prcp * x;
   }
+  if (!is_none(h.spwfile)) {  // spiderweb (sfincs_meteo.f90:35-98) with its factors (:330-412)
+    SpwHost& w = h.spw;
+    read_spw_file(path(h.spwfile), h.tref, h.use_spw_precip, w);
+    h.spw_pabs.resize(w.pdrp.size());
+    for (size_t i = 0; i < w.pdrp.size(); i++) h.spw_pabs[i] = P.gapres - w.pdrp[i];
+    if (h.factor_wind != 1.0f) {
+      for (auto& x : w.wu) x = h.factor_wind * x;
+      for (auto& x : w.wv) x = h.factor_wind * x;
+    }
+    if (h.factor_pres != 1.0f)
+      for (auto& x : h.spw_pabs) x = P.gapres - h.factor_pres * (P.gapres - x);
+    if (w.precip && h.factor_prcp != 1.0f)
+      for (auto& x : w.prcp) x = h.factor_prcp * x;
+    if (h.factor_spw_size != 1.0f) w.radius = h.factor_spw_size * w.radius;
+    P.spw.nt = w.nt;
+    P.spw.nrows = w.nrows;
+    P.spw.ncols = w.ncols;
+    P.spw.precip = w.precip;
+    P.spw.radius = w.radius;
+    P.spw.drad = w.radius / (float)w.nrows;
+    P.spw.dphi = 2.0f * P.pi / (float)w.ncols;
+    P.spw.merge_frac = h.spw_merge_frac;
+  }
   P.cosrot = std::cos(rotation);
   P.sinrot = std::sin(rotation);
   if (P.wind && !is_none(k.wndfile)) {
@@ -280,7 +304,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   std::string prcpfile = in.str("prcfile", "none");
   if (is_none(prcpfile)) prcpfile = in.str("precipfile", "none");
   // Inputs outside this core's path: refuse loudly instead of silently ignoring physics.
-  for (const char* k : {"bcafile", "bzifile", "volfile", "spwfile", "netbndbzsbzifile", "netsrcdisfile",
+  for (const char* k : {"bcafile", "bzifile", "volfile", "netbndbzsbzifile", "netsrcdisfile",
                         "netamuamvfile", "netamprfile", "netampfile", "netspwfile", "infiltration_file",
                         "wavemaker_wvmfile", "wvmfile"}) {
     if (!is_none(in.str(k, "none"))) throw std::runtime_error(std::string("input '") + k + "' is not supported by this core");
@@ -353,12 +377,39 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
     if (!is_none(ampr) && !is_none(prcpfile)) throw std::runtime_error("rain from both amprfile and prcfile");
     if (in.real("waveage", -999.0f) > 0.0f) throw std::runtime_error("waveage (wave-age wind drag) is not supported");
     if (in.integer("radstr", 0) == 1) throw std::runtime_error("radstr is not supported");
-    P.wind = !is_none(wndfile) || !is_none(amu);
-    P.wind_field = !is_none(amu);
-    P.patmos = !is_none(amp) && in.integer("baro", 1) == 1;
-    P.precip = !is_none(prcpfile) || !is_none(ampr);
-    P.prcp_field = !is_none(ampr);
-    P.meteo3d = !is_none(amu) || !is_none(amp) || !is_none(ampr);
+    // spiderweb: a cyclone's polar wind / pressure / rain merged over the grids
+    // (sfincs_meteo.f90:35-98, 450-800); its options that need tables or
+    // projections outside this core are refused
+    const std::string spw = in.str("spwfile", "none");
+    const bool use_spw_precip = in.integer("usespwprecip", 1) != 0;
+    bool spw_precip = false;
+    if (!is_none(spw)) {
+      if (!is_none(wndfile)) throw std::runtime_error("wind from both spwfile and wndfile");
+      if (in.str("utmzone", "nil") != "nil") throw std::runtime_error("utmzone (spiderweb reprojection) is not supported");
+      if (!is_none(in.str("z0lfile", "none")))
+        throw std::runtime_error("z0lfile (wind reduction over land) is not supported");
+      // n_quantity decides whether the web brings rain (read_meteo_data, :83-93)
+      std::ifstream fs(h.dir + "/" + spw);
+      for (std::string l; std::getline(fs, l) && l.compare(0, 4, "TIME") != 0;) {
+        const size_t e = l.find('=');
+        if (e == std::string::npos) continue;
+        std::string k = l.substr(0, e);
+        k.erase(0, k.find_first_not_of(" \t"));
+        k.erase(k.find_last_not_of(" \t") + 1);
+        if (k == "n_quantity" || k == "N_quantity") spw_precip = std::atoi(l.substr(e + 1).c_str()) == 4 && use_spw_precip;
+      }
+      if (spw_precip && !is_none(prcpfile)) throw std::runtime_error("rain from both spwfile and prcfile");
+    }
+    P.wind = !is_none(wndfile) || !is_none(amu) || !is_none(spw);
+    P.wind_field = !is_none(amu) || !is_none(spw);
+    P.patmos = (!is_none(amp) || !is_none(spw)) && in.integer("baro", 1) == 1;
+    P.precip = !is_none(prcpfile) || !is_none(ampr) || spw_precip;
+    P.prcp_field = !is_none(ampr) || spw_precip;
+    P.meteo3d = !is_none(amu) || !is_none(amp) || !is_none(ampr) || !is_none(spw);
+    h.spwfile = spw;
+    h.use_spw_precip = use_spw_precip;
+    h.spw_merge_frac = in.real("spwmergefrac", 0.5f);
+    h.factor_spw_size = in.real("factor_spw_size", 1.0f);
     P.spinup_meteo = in.integer("spinup_meteo", 0) != 0;
     P.ampr_block = in.integer("amprblock", 1) != 0;
     P.dtwnd = in.real("dtwnd", 1800.0f);
@@ -569,6 +620,10 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   auto path = [&](const std::string& f) { return dir + "/" + f; };
   InpFile in(path("sfincs.inp"));
   const Keys K = parse_keys(in, h, bmi);
+  // bounded wait of the staged kernels; SFG_TEST_WAIT_ROUNDS lowers it so a
+  // test can make the wait give up (the fault path) without a fault on the GPU
+  P.wait_limit = 1 << 22;
+  if (const char* w = std::getenv("SFG_TEST_WAIT_ROUNDS")) P.wait_limit = std::max(0, std::atoi(w));
   if (K.quadtree) {
     load_quadtree(h, K);
     return H;
@@ -1529,6 +1584,16 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
       up(m.v0, g.v[0]);
       up(m.v1, g.v[1]);
     }
+    {  // the spiderweb's records (scalars came with h.p)
+      const SpwHost& w = h.spw;
+      up(d.spw.times, w.times);
+      up(d.spw.xe, w.xe);
+      up(d.spw.ye, w.ye);
+      up(d.spw.wu, w.wu);
+      up(d.spw.wv, w.wv);
+      up(d.spw.pabs, h.spw_pabs);
+      up(d.spw.prcp, w.precip ? w.prcp : std::vector<float>());
+    }
     d.nmeteo = (int)h.np;
     if (h.p.meteo3d) {
       up(d.xz, h.z_xz);
@@ -1892,7 +1957,7 @@ void Runner::run(const std::vector<double>& tend, long long max_steps, int chunk
   auto all_done = [&]() {
     for (int i = 0; i < nscn(); i++) {
       const StepState& s = h_states_[i];
-      if (!(s.stop_pending || !(s.t < s.tend) || s.steps_left == 0)) return false;
+      if (!(s.stop_pending || !(s.t < s.tend) || s.steps_left == 0 || s.fault)) return false;
     }
     return true;
   };

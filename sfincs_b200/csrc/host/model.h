@@ -23,6 +23,19 @@ struct MeteoGridHost {
 };
 // Reads an amu / amv / amp / ampr file into g (q: 0 first quantity, 1 second wind component).
 void read_meteo_grid(const std::string& file, const std::string& tref, MeteoGridHost& g, int q);
+// Seconds after tref of a meteo file's "TIME = <v> <unit> since <date>" line.
+float meteo_time(const std::string& line, const std::string& tref);
+// A spiderweb file as read: nt records of nrows x ncols polar values, the
+// wind already in components, the pressure drop, the rain (zeros without a
+// fourth quantity), the eye track.
+struct SpwHost {
+  int nt = 0, nrows = 0, ncols = 0, nquant = 0;
+  bool precip = false;
+  float radius = 0;
+  std::vector<float> times, xe, ye, wu, wv, pdrp, prcp;
+};
+// Reads an ASCII spiderweb file (use_precip: usespwprecip).
+void read_spw_file(const std::string& file, const std::string& tref, bool use_precip, SpwHost& s);
 
 // Everything read from a model directory and laid out densely on the host.
 struct HostModel {
@@ -62,6 +75,11 @@ struct HostModel {
   std::vector<float> x73;            // hu**(7/3) table when h73table is on (sfincs_data.f90:858-881)
   MeteoGridHost mgh[3];              // gridded meteo: 0 wind (amu, amv), 1 pressure (amp), 2 rain (ampr)
   std::string amufile = "none", amvfile = "none", ampfile = "none", amprfile = "none";  // their files
+  SpwHost spw;                       // spiderweb (nt == 0: none)
+  std::string spwfile = "none";
+  bool use_spw_precip = true;
+  float spw_merge_frac = 0.5f, factor_spw_size = 1.0f;
+  std::vector<float> spw_pabs;       // absolute pressure of the web
   float factor_wind = 1, factor_pres = 1, factor_prcp = 1;
   // infiltration models with state: parameters, state, event flag, cumulative sums (storage order)
   std::vector<float> inf_par[5], inf_st[5], cumprcp, cuminf;

@@ -597,10 +597,87 @@ __device__ __forceinline__ bool meteo_at(const MeteoGrid& g, const float* v, con
   return true;
 }
 
+// The records around one end of the window in a spiderweb and its eye
+// (update_spiderweb_data, sfincs_meteo.f90:485-531): before the first record
+// and after the last the nearest record, faded in / out over 6 h.
+struct SpwRec {
+  int i0, i1;  // 0-based records
+  float twfac, spin, xe, ye;
+};
+__device__ __forceinline__ SpwRec spw_rec(const SpwGrid& g, float meteo_t) {
+  SpwRec r;
+  int itw0 = 1, itw1 = 1;
+  r.twfac = 1.0f;
+  r.spin = 1.0f;
+  if (meteo_t < g.times[0]) {
+    r.spin = fmaxf(1.0f - (g.times[0] - meteo_t) / 21600.0f, 0.0f);
+  } else if (meteo_t > g.times[g.nt - 1]) {
+    itw0 = itw1 = g.nt;
+    r.spin = fmaxf(1.0f - (meteo_t - g.times[g.nt - 1]) / 21600.0f, 0.0f);
+  } else {
+    for (int it = 1; it <= g.nt; it++)
+      if (g.times[it - 1] <= meteo_t) itw0 = it;
+    itw1 = min(itw0 + 1, g.nt);
+    r.twfac = (meteo_t - g.times[itw0 - 1]) / fmaxf(g.times[itw1 - 1] - g.times[itw0 - 1], 1.0e-6f);
+  }
+  r.i0 = itw0 - 1;
+  r.i1 = itw1 - 1;
+  r.xe = g.xe[r.i0] * (1.0f - r.twfac) + g.xe[r.i1] * r.twfac;
+  r.ye = g.ye[r.i0] * (1.0f - r.twfac) + g.ye[r.i1] * r.twfac;
+  return r;
+}
+
+// Merges the spiderweb into one cell's window values at one end (the
+// per-cell loop of update_spiderweb_data, sfincs_meteo.f90:589-790): the
+// polar bilinear weights around the eye, the drag of the interpolated wind,
+// and the blend with the background fields towards the web's rim.
+__device__ __forceinline__ void spw_merge(const ScnDev& S, const SpwRec& r, float x, float y, float& tu, float& tv,
+                                          float& p, float& pr) {
+  const SpwGrid& g = S.spw;
+  const float dxe = x - r.xe, dye = y - r.ye;
+  const float dst = sqrtf(dxe * dxe + dye * dye);
+  if (dst > g.radius) return;  // outside the web
+  const int idst = max((int)(dst / g.drad), 1);
+  if (idst + 1 > g.nrows) return;
+  const float dj1 = fmaxf((dst - g.drad * (float)idst) / g.drad, 0.0f);
+  float phi = 0.5f * S.pi - atan2_ieee(dye, dxe);  // clockwise from north
+  if (phi < 0.0f) phi = phi + 2.0f * S.pi;          // modulo 2 pi (phi > -pi here)
+  const int iphi = min((int)(phi / g.dphi) + 1, g.ncols);
+  const int ind1[4] = {idst, idst, idst + 1, idst + 1};
+  int ind2[4] = {iphi, iphi + 1, iphi + 1, iphi};
+  if (ind2[1] > g.ncols) ind2[1] = 1;
+  if (ind2[2] > g.ncols) ind2[2] = 1;
+  const float di1 = (phi - g.dphi * (float)(iphi - 1)) / g.dphi;
+  const float f[4] = {(1.0f - di1) * (1.0f - dj1), di1 * (1.0f - dj1), di1 * dj1, (1.0f - di1) * dj1};
+  const size_t rec = (size_t)g.nrows * g.ncols;
+  const float a = 1.0f - r.twfac, b = r.twfac;
+  float wup = 0.0f, wvp = 0.0f, pcp = 0.0f, prp = 0.0f;
+  for (int ip = 0; ip < 4; ip++) {
+    const size_t o = (size_t)(ind1[ip] - 1) * g.ncols + (ind2[ip] - 1);
+    const size_t o0 = r.i0 * rec + o, o1 = r.i1 * rec + o;
+    wup = wup + f[ip] * (g.wu[o0] * a + g.wu[o1] * b);
+    wvp = wvp + f[ip] * (g.wv[o0] * a + g.wv[o1] * b);
+    if (S.patmos) pcp = pcp + f[ip] * (g.pabs[o0] * a + g.pabs[o1] * b);
+    if (g.precip) prp = prp + f[ip] * (g.prcp[o0] * a + g.prcp[o1] * b);
+  }
+  const float vmag = sqrtf(wup * wup + wvp * wvp);
+  const int icd = min(max((int)(vmag * 10.0f) + 1, 1), 1000);
+  const float cd = S.cdval[icd - 1];
+  float merge = 1.0f;
+  if (dst > g.merge_frac * g.radius)
+    merge = (1.0f / (1.0f - fminf(g.merge_frac, 0.999f))) * (g.radius - dst) / g.radius;
+  merge = merge * r.spin;
+  tu = (1.0f - merge) * tu + merge * vmag * (S.cosrot * wup + S.sinrot * wvp) * S.rhoa * cd / S.rhow;
+  tv = (1.0f - merge) * tv + merge * vmag * (-S.sinrot * wup + S.cosrot * wvp) * S.rhoa * cd / S.rhow;
+  if (S.patmos) p = (1.0f - merge) * p + merge * pcp;
+  if (g.precip) pr = (1.0f - merge) * pr + merge * prp / (float)(1000 * 3600);
+}
+
 // Runs before the step kernel: when the step about to run opens a new window
 // (the same decision the step kernel commits), every cell gets the window's
 // wind stress, pressure and rain at both ends (update_meteo_fields,
-// sfincs_meteo.f90:1561-1624); otherwise every CTA returns at once.
+// sfincs_meteo.f90:1561-1624: the equidistant grids, then the spiderweb
+// merged over them); otherwise every CTA returns at once.
 __global__ void __launch_bounds__(256) k_meteo_window(const ScnDev* __restrict__ scns) {
   pdl_wait();  // the previous kernel of the step has completed
   pdl_trigger();
@@ -610,19 +687,24 @@ __global__ void __launch_bounds__(256) k_meteo_window(const ScnDev* __restrict__
   const StepPlan P = plan_step(S, st);
   if (!P.meteo_upd) return;
   __shared__ MeteoRec recs[3][2];
+  __shared__ SpwRec srecs[2];
   if (threadIdx.x < 6) {
     const int kind = threadIdx.x >> 1, itw = threadIdx.x & 1;
     const MeteoGrid& g = S.mg[kind];
     if (g.nt > 0) recs[kind][itw] = meteo_rec(g, itw == 0 ? P.mt0 : P.mt1, kind == 2 && S.ampr_block);
+  } else if (threadIdx.x < 8 && S.spw.nt > 0) {
+    srecs[threadIdx.x - 6] = spw_rec(S.spw, threadIdx.x == 6 ? P.mt0 : P.mt1);
   }
   __syncthreads();
   const float cosrot = S.cosrot, sinrot = S.sinrot;
+  const bool wf = S.wind_field, pf = S.patmos, rf = S.prcp_field;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S.nmeteo; i += gridDim.x * blockDim.x) {
     const int64_t c = S.cmp ? (int64_t)S.cmp[i] : (int64_t)i;
     const float x = S.xz[i], y = S.yz[i];
     for (int itw = 0; itw < 2; itw++) {
-      if (S.mg[0].nt > 0) {  // wind stress (:862-936)
-        float wup, wvp, tu = 0.0f, tv = 0.0f;
+      float tu = 0.0f, tv = 0.0f, p = S.gapres, pr = 0.0f;
+      if (S.mg[0].nt > 0) {  // wind stress (:862-936), outside the grid 0
+        float wup, wvp;
         if (meteo_at(S.mg[0], S.mg[0].v0, S.mg[0].v1, recs[0][itw], x, y, wup, wvp)) {
           const float vmag = sqrtf(wup * wup + wvp * wvp);
           const int icd = min(max((int)(vmag * 10.0f) + 1, 1), 1000);
@@ -630,20 +712,22 @@ __global__ void __launch_bounds__(256) k_meteo_window(const ScnDev* __restrict__
           tu = vmag * (cosrot * wup + sinrot * wvp) * S.rhoa * cd / S.rhow;
           tv = vmag * (-sinrot * wup + cosrot * wvp) * S.rhoa * cd / S.rhow;
         }
+      }
+      if (S.mg[1].nt > 0 && pf) {  // pressure (:1035-1080), outside the grid gapres
+        float v, unused;
+        if (meteo_at(S.mg[1], S.mg[1].v0, nullptr, recs[1][itw], x, y, v, unused)) p = v;
+      }
+      if (S.mg[2].nt > 0) {  // rain in mm/h to m/s (:1160-1232), outside the grid 0
+        float v, unused;
+        if (meteo_at(S.mg[2], S.mg[2].v0, nullptr, recs[2][itw], x, y, v, unused)) pr = v / (float)(1000 * 3600);
+      }
+      if (S.spw.nt > 0) spw_merge(S, srecs[itw], x, y, tu, tv, p, pr);
+      if (wf) {
         (itw == 0 ? S.tauwu0 : S.tauwu1)[c] = tu;
         (itw == 0 ? S.tauwv0 : S.tauwv1)[c] = tv;
       }
-      if (S.mg[1].nt > 0 && S.patmos) {  // pressure (:1035-1080), outside the grid gapres
-        float p, unused;
-        if (!meteo_at(S.mg[1], S.mg[1].v0, nullptr, recs[1][itw], x, y, p, unused)) p = S.gapres;
-        (itw == 0 ? S.patm0 : S.patm1)[c] = p;
-      }
-      if (S.mg[2].nt > 0) {  // rain in mm/h to m/s (:1160-1232), outside the grid 0
-        float pr, unused;
-        if (!meteo_at(S.mg[2], S.mg[2].v0, nullptr, recs[2][itw], x, y, pr, unused)) pr = 0.0f;
-        else pr = pr / (float)(1000 * 3600);
-        (itw == 0 ? S.prcp0 : S.prcp1)[c] = pr;
-      }
+      if (pf) (itw == 0 ? S.patm0 : S.patm1)[c] = p;
+      if (rf) (itw == 0 ? S.prcp0 : S.prcp1)[c] = pr;
     }
   }
 }

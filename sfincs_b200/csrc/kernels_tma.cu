@@ -51,11 +51,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: ~2^22 try_wait rounds (each already suspends for a while) before giving up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (int i = 0; i < (1 << 22); i++)
+// Bounded wait: `limit` try_wait rounds (each already suspends for a while)
+// before giving up; the scenario's wait_limit is 2^22 unless a test lowers it.
+constexpr int kDrainRounds = 1 << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; i++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
+}
+// A stage whose wait gave up may still have copies in flight: before the
+// stage is refilled, and before the CTA exits, thread 0 waits (bounded) for
+// that phase to complete.  pend: bit s = a wait on stage s gave up; the phase
+// still outstanding on stage s has the parity opposite to its next one.
+__device__ __forceinline__ void drain_stage(uint64_t* bar, int s, uint32_t phase, uint32_t& pend) {
+  if (!(pend & (1u << s))) return;
+  (void)mbar_wait_bounded(&bar[s], ((phase >> s) & 1u) ^ 1u, kDrainRounds);
+  pend &= ~(1u << s);
 }
 __device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, int y, uint64_t* bar) {
   asm volatile(
@@ -212,6 +223,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
   __shared__ __align__(8) uint64_t bar[NST];
   __shared__ int s_issued[NST];
   __shared__ Tile s_tile[NST];
+  __shared__ uint32_t s_pend;  // stages whose wait gave up (drained by thread 0 before reuse)
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + 32 * ty;
   const int G = gridDim.x;
@@ -229,6 +241,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
   if (tid == 0) {
     for (int k = 0; k < NST; k++) mbar_init(&bar[k], 1);
     fence_barrier_init();
+    s_pend = 0u;
     for (int k = 0; k < NST - 1; k++) issue(tile + k * G, k);
   }
   uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
@@ -242,6 +255,9 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
     const int sl = s == 0 ? NST - 1 : s - 1;  // stage of the previous tile, refilled now
     __syncthreads();  // s_issued[s] and s_tile[s] visible; stage sl no longer read
     if (tid == 0) {
+      uint32_t pend = s_pend;
+      drain_stage(bar, sl, phase, pend);
+      s_pend = pend;
       fence_proxy_async();
       issue(tile + (NST - 1) * G, sl);
     }
@@ -257,11 +273,12 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
         cfl_dyinv = S.dyinv;
         sv = step_vals(st);
       }
-      const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u);
+      const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u, S.wait_limit);
       phase ^= 1u << s;
       const int n = tl.n0 + tx, m = tl.m0 + ty;
       if (!ok) {
         st.fault = 1;
+        atomicOr(&s_pend, 1u << s);
       } else if (n <= S.nmax && m <= S.mmax) {
         const unsigned char* sm = smem + s * mom::stage_bytes<SG>();
         const float* zs = (const float*)(sm + mom::O_ZS);
@@ -460,7 +477,13 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
     s = s + 1 == NST ? 0 : s + 1;
   }
   flush_cfl(cfl_st, cfl, cfl_dxinv, cfl_dyinv, tx);
-  // drain: every issued stage has been waited for in the loop; nothing in flight here
+  // every issued stage has been waited for in the loop; a stage whose wait gave
+  // up is drained here, so that no copy is in flight when the CTA exits
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t pend = s_pend;
+    for (int k = 0; k < NST; k++) drain_stage(bar, k, phase, pend);
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -515,6 +538,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_issued[2];
   __shared__ Tile s_tile[2];
+  __shared__ uint32_t s_pend;  // stages whose wait gave up (drained by thread 0 before reuse)
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + 32 * ty;
   int tile = blockIdx.x;
@@ -532,6 +556,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     fence_barrier_init();
+    s_pend = 0u;
     issue(tile, 0);
   }
   uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
@@ -542,6 +567,9 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
     const int next = tile + gridDim.x;
     __syncthreads();  // s_issued[s] and s_tile[s] visible; stage s^1 no longer read
     if (tid == 0) {
+      uint32_t pend = s_pend;
+      drain_stage(bar, s ^ 1, phase, pend);
+      s_pend = pend;
       fence_proxy_async();
       issue(next, s ^ 1);
     }
@@ -553,11 +581,12 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
         sv_st = &st;
         sv = step_vals(st);
       }
-      const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u);
+      const bool ok = mbar_wait_bounded(&bar[s], (phase >> s) & 1u, S.wait_limit);
       phase ^= 1u << s;
       const int n = tl.n0 + tx, m = tl.m0 + ty;
       if (!ok) {
         st.fault = 1;
+        atomicOr(&s_pend, 1u << s);
       } else if (n <= S.nmax && m <= S.mmax) {
         const unsigned char* sm = smem + s * con::STAGE;
         const int k = ty * 32 + tx;
@@ -674,6 +703,13 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
       }
     }
     tile = next;
+  }
+  // a stage whose wait gave up is drained, so that no copy is in flight when the CTA exits
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t pend = s_pend;
+    drain_stage(bar, 0, phase, pend);
+    drain_stage(bar, 1, phase, pend);
   }
 }
 

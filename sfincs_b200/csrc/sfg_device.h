@@ -162,6 +162,21 @@ struct MeteoGrid {
   const float* v1;     // amv (wind only)
 };
 
+// A spiderweb: wind, pressure and rain on a polar grid around a moving
+// cyclone eye (ASCII spw file, sfincs_spiderweb.f90:8-134, with the
+// conversions of read_meteo_data, sfincs_meteo.f90:35-98, 330-412).
+struct SpwGrid {
+  int nt, nrows, ncols, precip;  // precip: the fourth quantity is used as rain
+  float radius, drad, dphi, merge_frac;
+  const float* times;  // [nt] seconds after tref
+  const float* xe;     // [nt] eye position
+  const float* ye;
+  const float* wu;     // [nt][nrows][ncols] wind components (m/s), rows outward, columns clockwise from north
+  const float* wv;
+  const float* pabs;   // absolute pressure (Pa)
+  const float* prcp;   // rain (mm/h), when precip
+};
+
 struct ScnDev {
   // ---- grid
   int nmax, mmax, ld, subgrid;
@@ -283,6 +298,7 @@ struct ScnDev {
   int nmeteo;            // cells the fields cover (compact count)
   float dtwnd, gapres, pavbnd, cosrot, sinrot;
   MeteoGrid mg[3];
+  SpwGrid spw;           // nt == 0: none
   const float* xz;
   const float* yz;
   const int32_t* cmp;
@@ -294,6 +310,7 @@ struct ScnDev {
   float* patm1;
   float* prcp0;
   float* prcp1;
+  int wait_limit;        // try_wait rounds of a staged kernel's bounded wait for its tile data (2^22)
   int h73table;          // hu**(7/3) from the lookup table (sfincs_momentum.f90:663-675)
   const float* x73;      // [10][1000] the table x73(j, k) at (k - 1) * 1000 + j - 1 (sfincs_data.f90:858-881)
   StepState* st;
@@ -417,6 +434,37 @@ __device__ __forceinline__ float cell_rain(const ScnDev& S, int64_t c, const Met
     if (net < 0.0f && dry) net = 0.0f;
   }
   return pr;
+}
+
+// Four-quadrant arctangent from IEEE operations only, so that the oracle
+// reproduces it bit for bit: a = min(|x|,|y|) / max(|x|,|y|) in [0, 1]; above
+// tan(pi/12) the addition formula atan(a) = pi/6 + atan((sqrt3 a - 1) / (sqrt3 + a))
+// brings the argument into [-tan(pi/12), tan(pi/12)], where the Taylor series
+// of atan to degree 15 (Horner form) leaves a truncation error below 1e-11;
+// the octant and the quadrant follow from the signs and from |y| > |x|.
+// atan2(0, 0) is 0.
+__device__ __forceinline__ float atan2_ieee(float y, float x) {
+  const float ax = fabsf(x), ay = fabsf(y);
+  const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+  if (mx == 0.0f) return 0.0f;
+  const float a = mn / mx;
+  float t = a, off = 0.0f;
+  if (a > 0.267949194f) {
+    t = (1.73205081f * a - 1.0f) / (1.73205081f + a);
+    off = 0.523598776f;
+  }
+  const float t2 = t * t;
+  float p = -1.0f / 15.0f;
+  p = fmaf(p, t2, 1.0f / 13.0f);
+  p = fmaf(p, t2, -1.0f / 11.0f);
+  p = fmaf(p, t2, 1.0f / 9.0f);
+  p = fmaf(p, t2, -1.0f / 7.0f);
+  p = fmaf(p, t2, 1.0f / 5.0f);
+  p = fmaf(p, t2, -1.0f / 3.0f);
+  float r = off + fmaf(t * t2, p, t);
+  if (ay > ax) r = 1.57079633f - r;
+  if (x < 0.0f) r = 3.14159265f - r;
+  return y < 0.0f ? -r : r;
 }
 
 // Exponential from IEEE operations only, so that the oracle reproduces it bit

@@ -299,6 +299,54 @@ def write_meteo_grid(path: str, quantity: str, unit: str, x_ll: float, y_ll: flo
                 f.write(" ".join(f"{v:.4f}" for v in row) + "\n")
 
 
+def write_spiderweb(path: str, times_s, xe, ye, radius: float, vmag, vdir, pdrop, prcp=None,
+                    ref: str = "2000-01-01 00:00:00") -> None:
+    """Write a cyclone in the ASCII spiderweb format the reference reads
+    (sfincs_spiderweb.f90:8-134): header keys, then per record a TIME line,
+    the eye position, the eye pressure drop and ``nrows`` lines per quantity
+    (wind speed, nautical from-direction, pressure drop, optionally rain in
+    mm/h).  The quantity arrays are (nt, nrows, ncols): row i at radius
+    i * radius / nrows, column j clockwise from north."""
+    vmag = np.asarray(vmag, np.float64)
+    nt, nrows, ncols = vmag.shape
+    quants = [("wind_speed", "m s-1", vmag), ("wind_from_direction", "degree", vdir), ("p_drop", "Pa", pdrop)]
+    if prcp is not None:
+        quants.append(("precipitation", "mm/h", prcp))
+    with open(path, "w") as f:
+        f.write("FileVersion      = 1.03\nfiletype         = meteo_on_spiderweb_grid\n"
+                f"NODATA_value     = -999.000\nn_cols           = {ncols}\nn_rows           = {nrows}\n"
+                f"grid_unit        = m\nspw_radius       = {radius:.1f}\nspw_rad_unit     = m\n"
+                f"n_quantity       = {len(quants)}\n")
+        for k, (q, u, _) in enumerate(quants):
+            f.write(f"quantity{k + 1}        = {q}\n")
+        for k, (q, u, _) in enumerate(quants):
+            f.write(f"unit{k + 1}            = {u}\n")
+        for it in range(nt):
+            f.write(f"TIME             = {times_s[it] / 3600.0:.6f} hours since {ref} +00:00\n")
+            f.write(f"x_spw_eye        = {xe[it]:.2f}\ny_spw_eye        = {ye[it]:.2f}\n")
+            f.write(f"p_drop_spw_eye   = {float(np.max(pdrop[it])):.1f}\n")
+            for _, _, v in quants:
+                for row in np.asarray(v, np.float64)[it]:
+                    f.write(" ".join(f"{x:.3f}" for x in row) + "\n")
+
+
+def cyclone(rng, nt: int, nrows: int, ncols: int, vmax: float = 45.0, rmax_frac: float = 0.2, dp: float = 4000.0,
+            rain: float = 0.0):
+    """Seeded polar fields of a synthetic cyclone (Rankine-like speed profile
+    with noise, counter-clockwise from-directions with a 20 degree inflow,
+    exponential pressure drop, rain peaking near the eye wall)."""
+    r = (np.arange(1, nrows + 1) / nrows)[None, :, None]
+    phi = (np.arange(ncols) * 360.0 / ncols)[None, None, :]
+    prof = np.where(r < rmax_frac, r / rmax_frac, (rmax_frac / r) ** 0.6)
+    vmag = vmax * prof * (1.0 + 0.1 * rng.standard_normal((nt, nrows, ncols)))
+    vdir = np.mod(phi + 90.0 + 20.0 + 5.0 * rng.standard_normal((nt, nrows, ncols)), 360.0)
+    pdrop = dp * np.exp(-r / (2 * rmax_frac)) * np.ones((nt, 1, ncols))
+    out = dict(vmag=np.abs(vmag), vdir=vdir, pdrop=pdrop)
+    if rain > 0:
+        out["prcp"] = rain * np.exp(-((r - rmax_frac) / 0.2) ** 2) * (1 + 0.2 * np.abs(rng.standard_normal((nt, nrows, ncols))))
+    return out
+
+
 # ------------------------------------------------------------------ model files
 @dataclass
 class RegularModel:

@@ -100,3 +100,53 @@ def test_quadtree_gridded_meteo_matches_f32_oracle(tmp_path, subgrid):
     znu = o.get("z_uv_nu", npc).astype(np.int64) - 1
     o.close()
     _stepwise(d, None, cells=(npc, npq, zmu, znu))
+
+
+def _spw_regular(tmp_path, subgrid, background):
+    from meteo_cases import add_spiderweb
+    from sfincs_b200 import synth
+
+    if subgrid:
+        m = synth.subgrid_regular(nmax=20, mmax=24, dx=500.0, P=8, seed=5, tstop=3600.0, rain_mmh=40.0,
+                                  rain_hours=0.5, coast_x=24 * 500.0 * 0.3, t_peak=1800.0, width_h=0.5,
+                                  surge_peak=1.5)
+        m.prcp = None  # rain comes from the web (and the grid)
+    else:
+        m = synth.plain_regular(nmax=24, mmax=30, dx=400.0, tstop=3600.0, seed=3, nbumps=6)
+    m.params.update(advection=1)
+    d = m.write(str(tmp_path))
+    if background:
+        add_meteo(d, m.mmax * m.dx, m.nmax * m.dy)
+    add_spiderweb(d, m.mmax * m.dx, m.nmax * m.dy, extra={"spwmergefrac": 0.6})
+    return d
+
+
+@pytest.mark.parametrize("variant", [2, 5])
+def test_spiderweb_matches_f32_oracle(tmp_path, variant):
+    """A cyclone's polar wind, pressure and rain alone (faded in and out)."""
+    _stepwise(_spw_regular(tmp_path, False, False), variant)
+
+
+def test_spiderweb_over_gridded_meteo_matches_f32_oracle(tmp_path):
+    """A cyclone merged over amu/amv/amp/ampr background fields on a subgrid model."""
+    _stepwise(_spw_regular(tmp_path, True, True), 5)
+
+
+def test_quadtree_spiderweb_matches_f32_oracle(tmp_path):
+    from meteo_cases import add_spiderweb
+    from oracle.oracle import Oracle
+    from sfincs_b200 import bmi as B
+    from sfincs_b200 import qtsynth
+
+    m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=3, bands=(1000.0, 500.0), P=4, seed=21,
+                                 tstop=3600.0, subgrid=True, wind_speed=0.0, tide_period=1800.0)
+    m.wnd = None
+    d = m.write(str(tmp_path))
+    add_spiderweb(d, 10 * 400.0, 8 * 400.0)
+    qc = B.layout(d, "qt_counts", 4)
+    npc, npq = int(qc[0]), int(qc[1]) + int(qc[2]) + 1
+    o = Oracle(d, "f32")
+    zmu = o.get("z_uv_mu", npc).astype(np.int64) - 1
+    znu = o.get("z_uv_nu", npc).astype(np.int64) - 1
+    o.close()
+    _stepwise(d, None, cells=(npc, npq, zmu, znu))

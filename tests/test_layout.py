@@ -119,9 +119,9 @@ def test_subgrid_tables_and_volumes(tmp_path):
 
 def test_unsupported_inputs_are_refused(tmp_path):
     m = synth.plain_regular(nmax=6, mmax=7, dx=300.0, tstop=600.0, nbumps=1)
-    m.params["spwfile"] = "sfincs.spw"
+    m.params["netspwfile"] = "sfincs_spw.nc"
     d = m.write(str(tmp_path))
-    with pytest.raises(RuntimeError, match="spwfile"):
+    with pytest.raises(RuntimeError, match="netspwfile"):
         B.layout(d, "counts", 10)
 
 
@@ -225,3 +225,19 @@ def test_downstream_river_faces_match_oracle(tmp_path, sub):
     assert np.array_equal(B.layout(d, "zs", n), o.get("zs"))
     o.update(-1000.0, 20)
     assert np.isfinite(o.get("zs")).all()
+
+
+def test_spiderweb_options_outside_the_core_are_refused(tmp_path):
+    """Spiderweb reprojection (utmzone) and wind reduction over land (z0lfile)
+    need tables and projections this core does not carry: refused at load."""
+    from meteo_cases import add_spiderweb
+    from sfincs_b200 import bmi as B
+
+    for extra in ({"utmzone": "17N"}, {"z0lfile": "sfincs.z0l"}):
+        d = tmp_path / list(extra)[0]
+        d.mkdir()
+        m = synth.plain_regular(nmax=10, mmax=12, dx=300.0, tstop=600.0, seed=1, nbumps=2)
+        m.write(str(d))
+        add_spiderweb(str(d), 3600.0, 3000.0, extra=extra)
+        with pytest.raises(RuntimeError, match=list(extra)[0]):
+            B.layout(str(d), "flags", 1)
