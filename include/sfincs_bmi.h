@@ -107,6 +107,11 @@ SFG_API int set_var(const char* name, const void* src, size_t bytes);
  * the message is then in err[errlen]. */
 SFG_API void* sfg_model_create(const char* model_dir, int bmi, char* err, int errlen);
 SFG_API void sfg_model_destroy(void* model);
+/* finalize_output (sfincs_output.f90:260-296): the last max-output interval,
+ * the run's scalars, the map / his files closed.  finalize() does this for the
+ * BMI model; sfg_model_destroy does it when it was not called, without an
+ * error report. */
+SFG_API int sfg_model_finalize(void* model);
 /* sfincs_update semantics: run while t < t_end, at most max_steps steps when
  * max_steps >= 0; steps are issued as CUDA graphs of `chunk` steps. */
 SFG_API int sfg_model_run(void* model, double t_end, long long max_steps, int chunk);

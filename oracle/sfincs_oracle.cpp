@@ -286,7 +286,13 @@ struct Model {
   std::string trefstr, tstartstr, tstopstr;
   float tspinup, alfa, theta, hmin_cfl, manning, manning_land, manning_sea, rghlevland, zini, qinf, dtmax,
       huthresh, huvmin, rhoa, rhow, latitude, pavbnd, gapres, advlim, slopelim, qinf_zmin, btfilter, btrelax,
-      nuviscdim, wiggle_factor, wiggle_threshold, uvlim, uvmax, nuviscfac, dtmaxout;
+      nuviscdim, wiggle_factor, wiggle_threshold, uvlim, uvmax, nuviscfac, dtmaxout, t0out = -999.0f;
+  // max output (sfincs_lib.f90:430-445, sfincs_output.f90:197-230): the next
+  // time, the count, and the fields as they were when last written
+  double tmaxout = 1.0e9;
+  long ntmaxout = 0;
+  F1<T> zsmax_out, vmax_out, qmax_out, twet_out;
+  F1<float> tzsmax_out;
   int bndtype, iadvection, baro, storevelmax, storefluxmax, storetwet, storetzsmax;
   std::string inputtype, advstr, qtrfile, depfile, zsinifile, rstfile, mskfile, indexfile, sbgfile, manningfile,
       bndfile, bzsfile, bcafile, bzifile, srcfile, disfile, wndfile, prcpfile, qinffile, scsfile, sefffile,
@@ -429,6 +435,7 @@ struct Model {
     tstopstr = in.str("tstop", "20000101 000000");
     tspinup = in.real("tspinup", 0.0f);
     dtmaxout = in.real("dtmaxout", 9999999.0f);
+    t0out = in.real("t0out", -999.0f);
     alfa = in.real("alpha", 0.50f);
     theta = in.real("theta", 1.0f);
     hmin_cfl = in.real("hmin_cfl", 0.1f);
@@ -546,6 +553,8 @@ struct Model {
     crsgeo = false;
     fcorio = 2.0f * 7.2921e-05f * std::sin(latitude * pi / 180.0f);
     if (latitude < 0.01f && latitude > -0.01f) coriolis = false;
+    if (t0out < -900.0f) t0out = t0;  // sfincs_input.f90:441-444
+    t0out = std::max(t0out, t0);
     store_maximum_waterlevel = dtmaxout > 0.0f;
     store_maximum_velocity = storevelmax == 1 && dtmaxout > 0.0f;
     store_maximum_flux = storefluxmax == 1 && dtmaxout > 0.0f;
@@ -1487,6 +1496,7 @@ struct Model {
     // combined uv points keep q = uv = 0 until the first momentum step (a
     // restart sets the npuv regular points only, :110-113)
     if (store_maximum_waterlevel) zsmax.fill((T)-999.0f);
+    tmaxout = dtmaxout > 1.0e-6f ? (double)t0out + (double)dtmaxout : 1.0e9;  // sfincs_output.f90:30-38
     if (store_maximum_velocity) vmax.fill((T)-999.0f);
     if (store_twet) twet.fill((T)0.0f);
     if (store_t_zsmax) t_zsmax.fill(-999.0f);
@@ -3321,6 +3331,12 @@ struct Model {
       float dtchk = alfa * min_dt;
       t = t + (double)dt;
       dtavg = dtavg + dt;
+      bool write_max = false;  // sfincs_lib.f90:430-445
+      if (t >= tmaxout) {
+        write_max = true;
+        ntmaxout++;
+        if (t < (double)t1) tmaxout = tmaxout + (double)dtmaxout;
+      }
       bool update_meteo = false;  // sfincs_lib.f90:493-503
       if (meteo3d && t >= (double)twindupd) {
         meteo_t0 = twindupd;
@@ -3346,6 +3362,28 @@ struct Model {
       else
         compute_water_levels_regular(dt, t);
       if (store_maximum_velocity || store_maximum_flux || store_twet) compute_store_variables(dt);
+      if (write_max) {  // write_output: the max fields as written, then reset (sfincs_output.f90:158-230)
+        if (store_maximum_waterlevel) {
+          zsmax_out = zsmax;
+          zsmax.fill((T)-999.0f);
+        }
+        if (store_maximum_velocity) {
+          vmax_out = vmax;
+          vmax.fill((T)-999.0f);
+        }
+        if (store_maximum_flux) {
+          qmax_out = qmax;
+          qmax.fill((T)-999.0f);
+        }
+        if (store_twet) {
+          twet_out = twet;
+          twet.fill((T)0.0f);
+        }
+        if (store_t_zsmax) {
+          tzsmax_out = t_zsmax;
+          t_zsmax.fill(-999.0f);
+        }
+      }
       if (dtchk < dtmin && nt > 1) {
         error = 1;
         t = (double)t1 + 1.0;
@@ -3503,6 +3541,12 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "cuminf" && m.cuminf.allocated()) copy_out(m.cuminf, out, n);
     else if (s == "qext" && m.qext.allocated()) copy_out(m.qext, out, n);
     else if (s == "uvmean") copy_out(m.uvmean, out, n);
+    else if (s == "zsmax_out" && m.zsmax_out.allocated()) copy_out(m.zsmax_out, out, n);
+    else if (s == "vmax_out" && m.vmax_out.allocated()) copy_out(m.vmax_out, out, n);
+    else if (s == "qmax_out" && m.qmax_out.allocated()) copy_out(m.qmax_out, out, n);
+    else if (s == "twet_out" && m.twet_out.allocated()) copy_out(m.twet_out, out, n);
+    else if (s == "tzsmax_out" && m.tzsmax_out.allocated()) copy_out(m.tzsmax_out, out, n);
+    else if (s == "ntmaxout") out[0] = (double)m.ntmaxout;
     else if (s == "tauwu0" && m.tauwu0.allocated()) copy_out(m.tauwu0, out, n);
     else if (s == "tauwv0" && m.tauwv0.allocated()) copy_out(m.tauwv0, out, n);
     else if (s == "tauwu1" && m.tauwu1.allocated()) copy_out(m.tauwu1, out, n);

@@ -66,6 +66,7 @@ def lib(build_if_missing: bool = True):
     L.sfg_model_create.restype = ctypes.c_void_p
     L.sfg_model_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
     L.sfg_model_destroy.argtypes = [ctypes.c_void_p]
+    L.sfg_model_finalize.argtypes = [ctypes.c_void_p]
     L.sfg_model_run.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_longlong, ctypes.c_int]
     L.sfg_model_issue.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.sfg_model_sync.argtypes = [ctypes.c_void_p]
@@ -240,6 +241,10 @@ class Model:
         if not self._h:
             raise RuntimeError("sfg_model_create: " + err.value.decode())
         self.np = int(self.scalars()["np"])
+
+    def finalize(self):
+        """finalize_output: the last max interval, the run's scalars, the output files closed."""
+        _check(self.L.sfg_model_finalize(self._h), "sfg_model_finalize")
 
     def close(self):
         if getattr(self, "_h", None):

@@ -32,6 +32,10 @@ __global__ void k_gather_u8(const uint8_t* __restrict__ ku, const uint8_t* __res
     out[n + i] = (float)(kv[cmp[i]] & 1);
   }
 }
+__global__ void k_fill_f32(float* __restrict__ a, float v, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    a[i] = v;
+}
 __global__ void k_or_u8(uint8_t* __restrict__ a, uint8_t mask, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     a[i] |= mask;
@@ -95,6 +99,9 @@ void launch_gather_f64(const double* src, const int32_t* cmp, double* out, long 
 void launch_gather_u8(const uint8_t* ku, const uint8_t* kv, const int32_t* cmp, float* out, long long n,
                       cudaStream_t s) {
   if (n > 0) k_gather_u8<<<grid_for(n), 256, 0, s>>>(ku, kv, cmp, out, n);
+}
+void launch_fill_f32(float* a, float v, long long n, cudaStream_t s) {
+  if (n > 0) k_fill_f32<<<grid_for(n), 256, 0, s>>>(a, v, n);
 }
 void launch_or_u8(uint8_t* a, uint8_t mask, long long n, cudaStream_t s) {
   if (n > 0) k_or_u8<<<grid_for(n), 256, 0, s>>>(a, mask, n);

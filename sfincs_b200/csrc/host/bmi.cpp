@@ -13,6 +13,7 @@
 
 #include "../../../include/sfincs_bmi.h"
 #include "model.h"
+#include "output.h"
 
 namespace sfg {
 void launch_gather_f32_f64(const float* src, const int32_t* cmp, double* out, long long n, cudaStream_t s);
@@ -78,6 +79,9 @@ struct ModelHandle {
   // boundary and momentum kernels run; continuity waits for it.
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t main_tail = nullptr, qext_ready = nullptr;
+  // map / his / max output (off the step's critical path)
+  std::unique_ptr<OutputWriter> out;
+  bool finalized = false;
 
   ModelHandle(const std::string& dir, bool bmi) {
     host = load_model(dir, bmi);
@@ -94,8 +98,14 @@ struct ModelHandle {
     check_cuda(cudaEventCreateWithFlags(&main_tail, cudaEventDisableTiming), "event");
     check_cuda(cudaEventCreateWithFlags(&qext_ready, cudaEventDisableTiming), "event");
     refresh_zs();
+    out = std::make_unique<OutputWriter>(*host, *dev, s());
   }
   ~ModelHandle() {
+    try {
+      finalize_output();
+    } catch (...) {
+    }
+    out.reset();
     if (copy_stream) cudaStreamSynchronize(copy_stream);
     runner.reset();
     if (qext_ready) cudaEventDestroy(qext_ready);
@@ -144,11 +154,14 @@ struct ModelHandle {
   void after_update() {
     if (zs_exported) refresh_zs();
   }
-  // Runs to tend (or max_steps steps), stopping at every restart output time
-  // on the step that reaches it (t >= trstout after the step, as
-  // sfincs_lib.f90:447-463 checks), where it writes the restart file.
+  double next_output() const {
+    return std::min({host->trstout, out->tmapout, out->tmaxout, out->thisout});
+  }
+  // Runs to tend (or max_steps steps), stopping at every output time on the
+  // step that reaches it (t >= tout after the step, as sfincs_lib.f90:419-476
+  // checks), where it writes the map / max / his output and the restart file.
   void run(double tend, long long max_steps, int chunk) {
-    if (host->trstout >= 1.0e9) {
+    if (next_output() >= 1.0e9) {
       runner->run({tend}, max_steps, chunk);
       check_fault();
       return;
@@ -157,10 +170,11 @@ struct ModelHandle {
     for (;;) {
       const StepState s0 = runner->read_state(0);
       if (!(s0.t < tend) || left == 0) break;
-      if (host->trstout <= s0.t)
+      const double tnext = next_output();
+      if (tnext <= s0.t)
         runner->run({tend}, 1, 1);  // the output falls on the next step
       else
-        runner->run({std::min(tend, host->trstout)}, left, chunk);
+        runner->run({std::min(tend, tnext)}, left, chunk);
       const StepState s1 = runner->read_state(0);
       if (left > 0) left = std::max(0LL, left - (long long)(s1.nt - s0.nt));
       check_fault();
@@ -175,14 +189,49 @@ struct ModelHandle {
       throw std::runtime_error("a staged kernel gave up waiting for its tile data (fault flag set); the state of "
                                "this model is incomplete");
   }
-  // sfincs_lib.f90:447-463 after a step
+  // The output checks after a step (sfincs_lib.f90:419-476), in the
+  // reference's order: each due output sets the output time, the last one
+  // set is the time every file of this step is written with.
   void after_step_output() {
-    if (host->trstout >= 1.0e9) return;
+    if (next_output() >= 1.0e9) return;
     const StepState st = runner->read_state(0);
-    if (st.t >= host->trstout) {
-      write_restart(st.t);
+    const double t = st.t, dt = (double)st.dt;
+    const OutputSpec& o = host->out;
+    bool wmap = false, wmax = false, wrst = false, whis = false;
+    double tout = t;
+    if (t >= out->tmapout) {
+      wmap = true;
+      out->ntmapout++;
+      tout = std::max(out->tmapout, t - dt);
+      out->tmapout += o.dtmapout;
+    }
+    if (t >= out->tmaxout) {
+      wmax = true;
+      out->ntmaxout++;
+      tout = std::max(out->tmaxout, t - dt);
+      if (t < (double)(float)host->t1) out->tmaxout += o.dtmaxout;
+    }
+    if (t >= host->trstout) {
+      wrst = true;
+      tout = host->trstout;
       host->trstout = host->dtrstout > 1.0e-6 ? host->trstout + host->dtrstout : 1.0e9;
     }
+    if (t >= out->thisout) {
+      whis = true;
+      out->nthisout++;
+      tout = std::max(out->thisout, t - dt);
+      out->thisout += o.dthisout;
+    }
+    if (wmap || wmax || whis) out->write(wmap, wmax, whis, tout, latest(st));
+    if (wrst) write_restart(tout);
+  }
+  // finalize_output (sfincs_output.f90:260-296): once, at finalize
+  void finalize_output() {
+    if (finalized || !out) return;
+    finalized = true;
+    const StepState st = runner->read_state(0);
+    const float avg = st.nt > 0 ? (float)((st.t - host->t0) / (double)st.nt) : 0.0f;
+    out->finalize(st.t, (double)(float)host->t1, latest(st), avg, st.error);
   }
   // write_rst_file (sfincs_output.f90:657-733), flavour 1: zs, q, uvmean
   void write_restart(double t) {
@@ -376,17 +425,7 @@ struct ModelHandle {
   }
 
   // find_quadtree_cell on a single-level grid (sfincs_quadtree.F90:764-820)
-  int cell_index(double xd, double yd) const {
-    const HostModel& h = *host;
-    if (h.p.quadtree) return quadtree_cell_index(h, xd, yd);
-    const float x = (float)xd, y = (float)yd;
-    const float xt = h.cosrot * (x - h.x0) + h.sinrot * (y - h.y0);
-    const float yt = -h.sinrot * (x - h.x0) + h.cosrot * (y - h.y0);
-    const int n = (int)(yt / h.p.dy) + 1, m = (int)(xt / h.p.dx) + 1;
-    if (n < 1 || n > h.p.nmax || m < 1 || m > h.p.mmax) return 0;
-    const int32_t ic = h.dense2cmp[(size_t)m * h.p.ld + kGhostPad + n];
-    return ic < 0 ? 0 : ic + 1;
-  }
+  int cell_index(double xd, double yd) const { return sfg::cell_index(*host, xd, yd); }
 
   void update_zbuv() {
     HostModel& h = *host;
@@ -498,6 +537,7 @@ int finalize(void) {
     double s[19];
     g_bmi->scalars(s);
     err = (int)s[4];
+    g_bmi->finalize_output();
     delete g_bmi;
     g_bmi = nullptr;
     return 0;
@@ -684,6 +724,12 @@ void* sfg_model_create(const char* model_dir, int bmi, char* err, int errlen) {
   }
 }
 void sfg_model_destroy(void* m) { delete static_cast<sfg::ModelHandle*>(m); }
+int sfg_model_finalize(void* m) {
+  return guarded([&] {
+    static_cast<sfg::ModelHandle*>(m)->finalize_output();
+    return 0;
+  });
+}
 int sfg_model_run(void* m, double t_end, long long max_steps, int chunk) {
   return guarded([&] {
     auto* h = static_cast<sfg::ModelHandle*>(m);

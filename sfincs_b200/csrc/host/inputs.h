@@ -20,6 +20,7 @@ class InpFile {
   int integer(const std::string& key, int def) const;
   std::string str(const std::string& key, const std::string& def) const;
   bool logical(const std::string& key, bool def) const;
+  const std::map<std::string, std::string>& all() const { return kv_; }
 
  private:
   std::map<std::string, std::string> kv_;

@@ -337,6 +337,37 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
     h.tref = tref;
     h.dtrstout = dtrstout;
     h.trstout = dtrstout > 1.0e-6f ? (double)(t0out + dtrstout) : (trst > 1.0e-6f ? (double)trst : 1.0e9);
+    // map / his / max output (sfincs_input.f90:61-87, 274-294, 341-343, 441-447, 532-535)
+    OutputSpec& o = h.out;
+    float t1out = in.real("t1out", -999.0f);
+    if (t1out < -900.0f) t1out = t1;
+    o.t0out = t0out;
+    o.t1out = t1out;
+    float dtmapout = in.real("dtout", 0.0f);
+    if (dtmapout == 0.0f) dtmapout = in.real("dtmapout", 0.0f);
+    o.dtmapout = dtmapout;
+    o.dtmaxout = dtmaxout;
+    o.dthisout = in.real("dthisout", 600.0f);
+    const std::string otype = in.str("outputformat", "net");
+    o.map_type = in.str("outputtype_map", "nil");
+    o.his_type = in.str("outputtype_his", "nil");
+    if (o.map_type == "nil" || o.his_type == "nil") o.map_type = o.his_type = otype;
+    if (o.map_type != "net" && o.map_type != "bin" && o.map_type != "asc")
+      throw std::runtime_error("outputformat '" + o.map_type + "' is not supported (net, bin or asc)");
+    if (o.map_type == "asc" && dtmapout > 1.0e-6f)
+      throw std::runtime_error("ASCII map output (outputformat = asc) is not supported; use net or bin");
+    o.store_velocity = in.integer("storevel", 0) == 1;
+    o.store_hsubgrid = in.integer("storehsubgrid", 0) == 1;
+    o.store_zvolume = in.integer("storezvolume", 0) == 1;
+    o.epsg = in.integer("epsg", 0);
+    o.epsg_code = in.str("epsg_code", std::to_string(o.epsg));
+    if (in.logical("storehmean", false)) throw std::runtime_error("storehmean (subgrid mean depth output) is not supported");
+    if (in.integer("storemeteo", 0) == 1) throw std::runtime_error("storemeteo (meteo map output) is not supported");
+    if (in.logical("debug", false)) throw std::runtime_error("debug output (every step) is not supported");
+    for (const char* f : {"crsfile", "rugfile"})
+      if (!is_none(in.str(f, "none")))
+        throw std::runtime_error(std::string("input '") + f + "' (cross-section / run-up output) is not supported");
+    for (const auto& kv : in.all()) o.inp.push_back(kv);
   }
   tspinup = t0 + tspinup;
   P.g = 9.81f;
@@ -626,6 +657,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
   if (const char* w = std::getenv("SFG_TEST_WAIT_ROUNDS")) P.wait_limit = std::max(0, std::atoi(w));
   if (K.quadtree) {
     load_quadtree(h, K);
+    read_obs_points(h);
     return H;
   }
   const int mmax = K.mmax, nmax = K.nmax;
@@ -1359,6 +1391,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
           }
       if (any) h.tiles.push_back(int2{n0, m0});
     }
+  read_obs_points(h);
   return H;
 }
 
@@ -1621,6 +1654,10 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   }
   up(d.inf_rain, h.inf_rain);
   up(d.cumprcp, h.cumprcp);
+  if (h.need_qinfmap)
+    zero(d.qinfmap, h.p.quadtree ? (size_t)h.np : NA);
+  else
+    d.qinfmap = nullptr;
   up(d.cuminf, h.cuminf);
   up(d.tsrc, h.tsrc);
   up(d.qsrc, h.qsrc);
@@ -1633,6 +1670,17 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   up(cmp, h.cmp_off);
   d.cmp = h.p.quadtree ? nullptr : cmp;  // compact cell -> storage offset for the meteo fields
   zero(d.st, 1);
+}
+
+int cell_index(const HostModel& h, double xd, double yd) {
+  if (h.p.quadtree) return quadtree_cell_index(h, xd, yd);
+  const float x = (float)xd, y = (float)yd;
+  const float xt = h.cosrot * (x - h.x0) + h.sinrot * (y - h.y0);
+  const float yt = -h.sinrot * (x - h.x0) + h.cosrot * (y - h.y0);
+  const int n = (int)(yt / h.p.dy) + 1, m = (int)(xt / h.p.dx) + 1;
+  if (n < 1 || n > h.p.nmax || m < 1 || m > h.p.mmax) return 0;
+  const int32_t ic = h.dense2cmp[(size_t)m * h.p.ld + kGhostPad + n];
+  return ic < 0 ? 0 : ic + 1;
 }
 
 size_t device_bytes_needed(const HostModel& h) {
@@ -1697,7 +1745,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
     if (h.p.nstruc > 0) any_struc_ = 1;
     if (h.p.wind_field || h.p.patmos) met_ = 1;
     if (h.p.inftype >= 2 || h.p.store_cumprcp || h.p.prcp_field || h.p.store_vmax || h.p.store_qmax ||
-        h.p.store_twet || h.p.store_tzsmax)
+        h.p.store_twet || h.p.store_tzsmax || h.need_qinfmap)
       ext_ = 1;
     if (h.p.meteo3d) {
       any_meteo_ = 1;

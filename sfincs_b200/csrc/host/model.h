@@ -37,6 +37,25 @@ struct SpwHost {
 // Reads an ASCII spiderweb file (use_precip: usespwprecip).
 void read_spw_file(const std::string& file, const std::string& tref, bool use_precip, SpwHost& s);
 
+// An observation point of the obsfile (sfincs_obspoints.f90:4-140): its
+// name and position, and the cell it falls in (1-based, 0 outside) with that
+// cell's centre and bed level (-999 outside).
+struct ObsPoint {
+  std::string name;
+  float x = 0, y = 0, xg = -999.0f, yg = -999.0f, zb = -999.0f;
+  int nm = 0;
+};
+// Output settings (sfincs_input.f90:61-87, 274-294, 441-540), times in seconds after tref.
+struct OutputSpec {
+  double t0out = 0, t1out = 0, dtmapout = 0, dthisout = 600, dtmaxout = 9999999;
+  std::string map_type = "net", his_type = "net";  // net: netCDF; bin: Fortran records; his asc/bin: text
+  bool store_velocity = false, store_hsubgrid = false, store_zvolume = false;
+  int epsg = 0;
+  std::string epsg_code;
+  std::vector<ObsPoint> obs;
+  std::vector<std::pair<std::string, std::string>> inp;  // the sfincs.inp keys, for the files' 'inp' attributes
+};
+
 // Everything read from a model directory and laid out densely on the host.
 struct HostModel {
   std::string dir;
@@ -110,6 +129,13 @@ struct HostModel {
   std::vector<float> cell_area;         // [np] m2
   std::vector<int64_t> qt_key;          // sorted keys (level, m, n) of the active cells, for point lookup
   std::vector<int32_t> qt_key_cell;     // compact cell of each key
+  // every point of the quadtree file (active or not), for the map file's mesh
+  std::vector<int32_t> qt_n, qt_m, qt_nm;  // qt_nm: 1-based active cell, 0 inactive
+  std::vector<uint8_t> qt_lev;
+  std::vector<float> qt_dxr, qt_dyr;       // cell size per level
+  // output
+  OutputSpec out;
+  bool need_qinfmap = false;               // an output reads the step's infiltration rate per cell
 };
 
 class InpFile;
@@ -169,6 +195,10 @@ void apply_restart_infiltration(HostModel& h, const RestartData& rst, const std:
 void load_quadtree(HostModel& h, const Keys& k);
 // 1-based active cell of a quadtree mesh at point (x, y), 0 outside.
 int quadtree_cell_index(const HostModel& h, double x, double y);
+// 1-based active cell of either mesh at point (x, y), 0 outside (find_quadtree_cell).
+int cell_index(const HostModel& h, double x, double y);
+// The obsfile's points with their cells (sfincs_obspoints.f90:4-140), into h.out.obs.
+void read_obs_points(HostModel& h);
 
 // Reads <dir>/sfincs.inp and the files it names.  bmi mirrors the reference's
 // BMI initialize() (use_qext on).  Throws std::runtime_error on bad input.

@@ -136,6 +136,10 @@ void QtBuilder::mesh() {
     }
   np = (long)q_of_sf.size() - 1;
   h.np = np;
+  h.qt_n = q.n;
+  h.qt_m = q.m;
+  h.qt_lev.assign(q.level.begin(), q.level.end());
+  h.qt_nm.assign(sf_of_q.begin() + 1, sf_of_q.end());
   if (np == 0) throw std::runtime_error("quadtree mask has no active cells");
   for (auto* v : {&kcs, &iref_of, &fmd, &fmu, &fnd, &fnu}) v->assign(np + 1, 0);
   for (auto* v : {&md1, &md2, &mu1, &mu2, &nd1, &nd2, &nu1, &nu2}) v->assign(np + 1, 0);
@@ -373,6 +377,8 @@ void QtBuilder::geometry() {
   P.dy2inv = P.lv_dyr2inv[0];
   P.area = P.lv_area[0];
   P.nuvisc = P.lv_nuvisc[0];
+  h.qt_dxr.assign(dxr.begin() + 1, dxr.end());
+  h.qt_dyr.assign(dyr.begin() + 1, dyr.end());
   h.z_xz.resize(np);
   h.z_yz.resize(np);
   h.cell_area.resize(np);

@@ -1010,6 +1010,7 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
       qinf_cell = cell_infiltration(S, c, prc, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
     }
   }
+  if (S.qinfmap) store_qinfmap(S, c, inf_cell, qinf_cell, SG ? v_old > 0.0 : !(zs_old <= S.zb[c]));
   if (f & F_KCS1) {
     if (SG) {  // sfincs_continuity.f90:341-577
       float dvol = ((q_md - q_mu) * S.dy + (q_nd - q_nu) * S.dx) * dt;

@@ -195,6 +195,7 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
       qinf_cell = cell_infiltration(S, c, prc, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
     }
   }
+  if (EXT && S.qinfmap) store_qinfmap(S, c, inf_cell, qinf_cell, SG ? S.zvol[c] > 0.0 : !(zs_old <= S.zb[c]));
   if (fl & F_KCS1) {
     const int4 fc = S.qcell[c];
     const float q_md = q[fc.x], q_mu = q[fc.y], q_nd = q[fc.z], q_nu = q[fc.w];

@@ -621,6 +621,9 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
                                             S.st->ga_hs);
             }
           }
+          if (EXT && S.qinfmap)
+            store_qinfmap(S, c, inf_cell, qinf_cell,
+                          SG ? ((const double*)(sm + con::O_ZVOL))[k] > 0.0 : !(zs_old <= S.zb[c]));
           if (f & F_KCS1) {
             const float qx = S.use_qext ? ((const float*)(sm + con::O_QEXT))[k] : 0.0f;
             const float qi = S.infiltration ? ((const float*)(sm + con::O_QINF))[k] : 0.0f;

@@ -288,6 +288,7 @@ struct ScnDev {
   const float* inf_par[5];
   float* inf_st[5];
   uint8_t* inf_rain;
+  float* qinfmap;        // infiltration rate of the step (m/s) per cell, when an output needs it (else null)
   float* cumprcp;        // cumulative rain and infiltration (m), when stored or needed (cna, cnb)
   float* cuminf;
   // gridded meteo (sfincs_meteo.f90:802-1442): the raw grids (0 wind, 1
@@ -434,6 +435,13 @@ __device__ __forceinline__ float cell_rain(const ScnDev& S, int64_t c, const Met
     if (net < 0.0f && dry) net = 0.0f;
   }
   return pr;
+}
+
+// The step's infiltration rate of an active cell (qinfmap,
+// sfincs_infiltration.f90:632-1033), kept when an output needs it: the rate
+// of the model with state, else the constant / c2d rate on a wet cell.
+__device__ __forceinline__ void store_qinfmap(const ScnDev& S, int64_t c, bool inf_cell, float qinf_cell, bool wet) {
+  S.qinfmap[c] = inf_cell ? qinf_cell : ((S.infiltration && wet) ? S.qinf[c] : 0.0f);
 }
 
 // Four-quadrant arctangent from IEEE operations only, so that the oracle
