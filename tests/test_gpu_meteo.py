@@ -45,7 +45,7 @@ def _regular(tmp_path, subgrid, **params):
     return d
 
 
-def _stepwise(d, variant, cells=None):
+def _stepwise(d, variant, cells=None, t_min=1200.0):
     from oracle.oracle import Oracle
 
     o = Oracle(d, "f32")
@@ -68,7 +68,7 @@ def _stepwise(d, variant, cells=None):
         assert sg["nt"] == so["nt"]
         assert abs(sg["t"] - so["t"]) <= 1e-6 * max(1.0, abs(so["t"]))
         assert dzs <= 2e-5 and dq <= 2e-5, (done, dzs, dq)
-    assert so["t"] > 1200.0  # two update windows of 600 s passed
+    assert so["t"] > t_min  # at least two update windows passed
     g.close()
 
 
@@ -92,14 +92,14 @@ def test_quadtree_gridded_meteo_matches_f32_oracle(tmp_path, subgrid):
                                  tstop=3600.0, subgrid=subgrid, wind_speed=0.0, tide_period=1800.0)
     m.wnd = None
     d = m.write(str(tmp_path))
-    add_meteo(d, 10 * 400.0, 8 * 400.0)
+    add_meteo(d, 10 * 400.0, 8 * 400.0, dt_rec=300.0, dtwnd=150.0)  # the fine levels take short steps
     qc = B.layout(d, "qt_counts", 4)
     npc, npq = int(qc[0]), int(qc[1]) + int(qc[2]) + 1
     o = Oracle(d, "f32")
     zmu = o.get("z_uv_mu", npc).astype(np.int64) - 1
     znu = o.get("z_uv_nu", npc).astype(np.int64) - 1
     o.close()
-    _stepwise(d, None, cells=(npc, npq, zmu, znu))
+    _stepwise(d, None, cells=(npc, npq, zmu, znu), t_min=300.0)
 
 
 def _spw_regular(tmp_path, subgrid, background):
@@ -142,11 +142,11 @@ def test_quadtree_spiderweb_matches_f32_oracle(tmp_path):
                                  tstop=3600.0, subgrid=True, wind_speed=0.0, tide_period=1800.0)
     m.wnd = None
     d = m.write(str(tmp_path))
-    add_spiderweb(d, 10 * 400.0, 8 * 400.0)
+    add_spiderweb(d, 10 * 400.0, 8 * 400.0, t_first=100.0, dt_rec=150.0, dtwnd=100.0)
     qc = B.layout(d, "qt_counts", 4)
     npc, npq = int(qc[0]), int(qc[1]) + int(qc[2]) + 1
     o = Oracle(d, "f32")
     zmu = o.get("z_uv_mu", npc).astype(np.int64) - 1
     znu = o.get("z_uv_nu", npc).astype(np.int64) - 1
     o.close()
-    _stepwise(d, None, cells=(npc, npq, zmu, znu))
+    _stepwise(d, None, cells=(npc, npq, zmu, znu), t_min=200.0)

@@ -46,9 +46,10 @@ class Expected:
     """The oracle stepped one step at a time, with the reference's output
     schedule (sfincs_lib.f90:419-476): per output, its time and the state."""
 
-    def __init__(self, d, dtmap, dthis, dtmax, obs_xy):
+    def __init__(self, d, dtmap, dthis, dtmax, stored=("vmax_out", "twet_out")):
         from oracle.oracle import Oracle
 
+        self.stored = stored
         self.o = o = Oracle(d, "f32")
         s = o.scalars()
         self.np = n = int(s["np"])
@@ -76,7 +77,7 @@ class Expected:
                 whis, tout = True, max(this, t - dt)
                 this += dthis
             zs = o.get("zs").astype(np.float32)
-            uv = np.append(0.0, o.get("uv"))  # 1-based, 0 = no face
+            uv = np.concatenate([[0.0], o.get("uv"), [0.0]])  # 1-based; 0 and npuv + 1 (the dummy) hold 0
             u = (0.5 * uv[md] + 0.5 * uv[mu]).astype(np.float32)
             v = (0.5 * uv[nd] + 0.5 * uv[nu]).astype(np.float32)
             if wmap:
@@ -86,7 +87,8 @@ class Expected:
             if wmax:
                 assert int(o.get("ntmaxout", 1)[0]) == nmax_before + 1
                 nmax_before += 1
-                self.max.append((np.float32(tout), o.get("zsmax_out"), o.get("vmax_out"), o.get("twet_out")))
+                opt = lambda k: o.get(k) if k in self.stored else None  # noqa: E731
+                self.max.append((np.float32(tout), o.get("zsmax_out"), opt("vmax_out"), opt("twet_out")))
         self.t_end = o.scalars()["t"]
 
 
@@ -100,7 +102,7 @@ def test_netcdf_map_his_and_max_match_the_oracle(tmp_path, subgrid):
     s = g.scalars()
     g.run(s["t1"])
     g.finalize()
-    e = Expected(d, 600.0, 300.0, 1200.0, None)
+    e = Expected(d, 600.0, 300.0, 1200.0)
     g.close()
     n = e.np
     # map file: cells on the (n, m) grid
@@ -110,7 +112,7 @@ def test_netcdf_map_his_and_max_match_the_oracle(tmp_path, subgrid):
     mi, ni = np.nonzero(m.msk.T > 0)  # compact order: n fastest
     zs_f = f.variables["zs"][:]
     assert zs_f.shape[0] == len(e.map) >= 6
-    huthresh = 0.0 if subgrid else 0.05
+    huthresh = 0.0 if subgrid else float(m.params.get("huthresh", 0.05))  # netCDF subgrid tables force 0
     for k, (t, zs, u, v) in enumerate(e.map):
         assert f.variables["time"][k] == t
         got = zs_f[k][ni, mi]
@@ -175,7 +177,7 @@ def test_binary_map_max_and_text_his(tmp_path):
     g.run(g.scalars()["t1"])
     g.finalize()
     g.close()
-    e = Expected(d, 900.0, 600.0, 1800.0, None)
+    e = Expected(d, 900.0, 600.0, 1800.0, stored=())
     n = e.np
     raw = np.fromfile(os.path.join(d, "zs.dat"), np.uint8)
     rec = 4 + 8 * n + 4
@@ -190,7 +192,7 @@ def test_binary_map_max_and_text_his(tmp_path):
     assert raw.size == rec * len(e.max)
     for k, (t, zsmax, vmax, twet) in enumerate(e.max):
         got = np.frombuffer(raw[k * rec + 4:(k + 1) * rec - 4].tobytes(), np.float32)
-        want = np.where(zsmax < e.zb + 0.05, -999.0, zsmax)
+        want = np.where(zsmax < e.zb + float(m.params.get("huthresh", 0.05)), -999.0, zsmax)
         assert np.allclose(got, want, atol=2e-5)
     lines = open(os.path.join(d, "zst.txt")).read().splitlines()
     assert len(lines) == len(e.his)

@@ -31,7 +31,7 @@ def _compare(d, npc, steps=120):
 
 @pytest.mark.parametrize("make", [small_plain, small_subgrid], ids=["plain", "subgrid"])
 def test_store_variables_match_oracle(tmp_path, make):
-    d, _ = make(tmp_path, advection=1, **STORE)
+    d, _ = make(tmp_path, advection=1, tstop=7200.0, **STORE)  # 120 steps end before tstop
     from oracle.oracle import Oracle
 
     _compare(d, int(Oracle(d, "f32").scalars()["np"]))
