@@ -59,14 +59,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
-// A stage whose wait gave up may still have copies in flight: before the
-// stage is refilled, and before the CTA exits, thread 0 waits (bounded) for
-// that phase to complete.  pend: bit s = a wait on stage s gave up; the phase
-// still outstanding on stage s has the parity opposite to its next one.
-__device__ __forceinline__ void drain_stage(uint64_t* bar, int s, uint32_t phase, uint32_t& pend) {
-  if (!(pend & (1u << s))) return;
-  (void)mbar_wait_bounded(&bar[s], ((phase >> s) & 1u) ^ 1u, kDrainRounds);
-  pend &= ~(1u << s);
+// A wait that gave up leaves its stage's copies in flight.  The CTA then
+// issues no further loads (every tile it still visits is skipped), and
+// before it exits thread 0 waits (bounded) for the last phase of every
+// stage: each issued phase has been waited for in the loop, so when those
+// waits succeeded each of these returns at the first try_wait (a stage never
+// loaded has completed its phase of parity 1).
+__device__ __noinline__ void drain_stages(uint64_t* bar, int nst, uint32_t phase) {
+  for (int k = 0; k < nst; k++) (void)mbar_wait_bounded(&bar[k], ((phase >> k) & 1u) ^ 1u, kDrainRounds);
 }
 __device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, int y, uint64_t* bar) {
   asm volatile(
@@ -190,6 +190,7 @@ __device__ __forceinline__ float face_flux(const ScnDev& S, const StepVals& st, 
   geo.dxuv2inv = DIR == 0 ? S.dx2inv : S.dy2inv;
   geo.dyuv2inv = DIR == 0 ? S.dy2inv : S.dx2inv;
   geo.nuvisc = S.nuvisc;
+  geo.fcorio = S.fcorio;
   // MET: a gridded wind or pressure field is present (a separate kernel
   // instance, so that the plain path keeps its register allocation)
   float tauw = DIR == 0 ? st.twu : st.twv, dpatm = 0.0f;
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
   __shared__ __align__(8) uint64_t bar[NST];
   __shared__ int s_issued[NST];
   __shared__ Tile s_tile[NST];
-  __shared__ uint32_t s_pend;  // stages whose wait gave up (drained by thread 0 before reuse)
+  __shared__ int s_stop;  // a wait of this CTA ran out
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + 32 * ty;
   const int G = gridDim.x;
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
   if (tid == 0) {
     for (int k = 0; k < NST; k++) mbar_init(&bar[k], 1);
     fence_barrier_init();
-    s_pend = 0u;
+    s_stop = 0;
     for (int k = 0; k < NST - 1; k++) issue(tile + k * G, k);
   }
   uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
@@ -255,11 +256,12 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
     const int sl = s == 0 ? NST - 1 : s - 1;  // stage of the previous tile, refilled now
     __syncthreads();  // s_issued[s] and s_tile[s] visible; stage sl no longer read
     if (tid == 0) {
-      uint32_t pend = s_pend;
-      drain_stage(bar, sl, phase, pend);
-      s_pend = pend;
-      fence_proxy_async();
-      issue(tile + (NST - 1) * G, sl);
+      if (s_stop) {  // a wait of this CTA ran out: no further loads
+        s_issued[sl] = 0;
+      } else {
+        fence_proxy_async();
+        issue(tile + (NST - 1) * G, sl);
+      }
     }
     if (s_issued[s]) {
       const Tile tl = s_tile[s];
@@ -278,7 +280,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
       const int n = tl.n0 + tx, m = tl.m0 + ty;
       if (!ok) {
         st.fault = 1;
-        atomicOr(&s_pend, 1u << s);
+        s_stop = 1;
       } else if (n <= S.nmax && m <= S.mmax) {
         const unsigned char* sm = smem + s * mom::stage_bytes<SG>();
         const float* zs = (const float*)(sm + mom::O_ZS);
@@ -477,13 +479,7 @@ __global__ void __launch_bounds__(256, MINB) k_momentum_tma(const ScnDev* __rest
     s = s + 1 == NST ? 0 : s + 1;
   }
   flush_cfl(cfl_st, cfl, cfl_dxinv, cfl_dyinv, tx);
-  // every issued stage has been waited for in the loop; a stage whose wait gave
-  // up is drained here, so that no copy is in flight when the CTA exits
-  __syncthreads();
-  if (tid == 0) {
-    uint32_t pend = s_pend;
-    for (int k = 0; k < NST; k++) drain_stage(bar, k, phase, pend);
-  }
+  if (tid == 0 && s_stop) drain_stages(bar, NST, phase);  // no copy in flight at exit
 }
 
 // --------------------------------------------------------------------------
@@ -538,7 +534,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_issued[2];
   __shared__ Tile s_tile[2];
-  __shared__ uint32_t s_pend;  // stages whose wait gave up (drained by thread 0 before reuse)
+  __shared__ int s_stop;  // a wait of this CTA ran out
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + 32 * ty;
   int tile = blockIdx.x;
@@ -556,7 +552,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     fence_barrier_init();
-    s_pend = 0u;
+    s_stop = 0;
     issue(tile, 0);
   }
   uint32_t phase = 0u;  // bit s: parity of the next completion of stage s's barrier (a register, not a local array)
@@ -567,11 +563,12 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
     const int next = tile + gridDim.x;
     __syncthreads();  // s_issued[s] and s_tile[s] visible; stage s^1 no longer read
     if (tid == 0) {
-      uint32_t pend = s_pend;
-      drain_stage(bar, s ^ 1, phase, pend);
-      s_pend = pend;
-      fence_proxy_async();
-      issue(next, s ^ 1);
+      if (s_stop) {  // a wait of this CTA ran out: no further loads
+        s_issued[s ^ 1] = 0;
+      } else {
+        fence_proxy_async();
+        issue(next, s ^ 1);
+      }
     }
     if (s_issued[s]) {
       const Tile tl = s_tile[s];
@@ -586,7 +583,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
       const int n = tl.n0 + tx, m = tl.m0 + ty;
       if (!ok) {
         st.fault = 1;
-        atomicOr(&s_pend, 1u << s);
+        s_stop = 1;
       } else if (n <= S.nmax && m <= S.mmax) {
         const unsigned char* sm = smem + s * con::STAGE;
         const int k = ty * 32 + tx;
@@ -707,13 +704,7 @@ __global__ void __launch_bounds__(256, 6) k_continuity_tma(const ScnDev* __restr
     }
     tile = next;
   }
-  // a stage whose wait gave up is drained, so that no copy is in flight when the CTA exits
-  __syncthreads();
-  if (tid == 0) {
-    uint32_t pend = s_pend;
-    drain_stage(bar, 0, phase, pend);
-    drain_stage(bar, 1, phase, pend);
-  }
+  if (tid == 0 && s_stop) drain_stages(bar, 2, phase);  // no copy in flight at exit
 }
 
 // --------------------------------------------------------------------------
