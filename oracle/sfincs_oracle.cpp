@@ -326,7 +326,11 @@ struct Model {
       uv_index_v_ndmu, uv_index_v_nmu, cuv_index_uv, cuv_index_uv1, cuv_index_uv2;
   F1<float> dxr, dyr, dxyr, z_xz, z_yz, dxrm, dxrinv, dxr2inv, dxrinvc, dyrm, dyrinv, dyr2inv, dyrinvc, cell_area,
       nuvisc;
-  float dtmin, cosrot, sinrot;
+  // geographic grids (sfincs_domain.f90:1403-1473): per uv point the inverse
+  // width across it, per cell the width, area and Coriolis parameter
+  F1<float> dxminv, dxm2inv, dxm, cell_area_m2, fcorio2d;
+  float dtmin = 0.0f, cosrot, sinrot;
+  float area_of(long nm) const { return crsgeo ? cell_area_m2(nm) : cell_area(z_flags_iref(nm)); }
 
   // --- bathymetry / subgrid
   F1<float> zb, zbuv, zbuvmx, gn2uv;
@@ -549,10 +553,14 @@ struct Model {
     cosrot = std::cos(rotation);
     sinrot = std::sin(rotation);
     fcorio = 0.0f;
-    if (igeo != 0) throw std::runtime_error("oracle: geographic grids are not part of this path");
-    crsgeo = false;
-    fcorio = 2.0f * 7.2921e-05f * std::sin(latitude * pi / 180.0f);
-    if (latitude < 0.01f && latitude > -0.01f) coriolis = false;
+    crsgeo = igeo != 0;  // sfincs_input.f90:399-421
+    if (crsgeo && (weirfile.substr(0, 4) != "none" || drnfile.substr(0, 4) != "none" ||
+                   spwfile.substr(0, 4) != "none"))
+      throw std::runtime_error("oracle: weirs, drainage and spiderwebs on geographic grids are not restated");
+    if (!crsgeo) {  // projected: Coriolis from the latitude, off near the equator
+      fcorio = 2.0f * 7.2921e-05f * std::sin(latitude * pi / 180.0f);
+      if (latitude < 0.01f && latitude > -0.01f) coriolis = false;
+    }  // geographic: Coriolis per cell (fcorio2d), on unless the input turns it off
     if (t0out < -900.0f) t0out = t0;  // sfincs_input.f90:441-444
     t0out = std::max(t0out, t0);
     store_maximum_waterlevel = dtmaxout > 0.0f;
@@ -1086,6 +1094,36 @@ struct Model {
     dxrm.alloc(nref); dxrinv.alloc(nref); dxr2inv.alloc(nref); dxrinvc.alloc(nref);
     dyrm.alloc(nref); dyrinv.alloc(nref); dyr2inv.alloc(nref); dyrinvc.alloc(nref);
     cell_area.alloc(nref);
+    if (crsgeo) {  // dxr, dyr in degrees (:1403-1473); no dtmax limit from the spacing, no dtmin
+      dxminv.alloc(npuv);
+      dxm2inv.alloc(npuv);
+      dxm.alloc(np);
+      cell_area_m2.alloc(np);
+      fcorio2d.alloc(np);
+      for (long ip = 1; ip <= npuv; ip++) {
+        const int iref = use_quadtree ? uv_flags_iref(ip) : 1;
+        const long nm = uv_index_z_nm(ip);
+        dxminv(ip) = 1.0f / (dxr(iref) * 111111.1f * std::cos(z_yz(nm) * pi / 180.0f));
+        dxm2inv(ip) = dxminv(ip) * dxminv(ip);
+      }
+      for (int iref = 1; iref <= nref; iref++) {
+        dyrm(iref) = 111111.1f * dyr(iref);
+        dyrinv(iref) = 1.0f / dyrm(iref);
+        dyr2inv(iref) = dyrinv(iref) * dyrinv(iref);
+        if (iref > 1) dyrinvc(iref) = 1.0f / (3.0f * dyrm(iref) / 2.0f);
+      }
+      for (long nm = 1; nm <= np; nm++) {
+        const int iref = z_flags_iref(nm);
+        dxm(nm) = dxr(iref) * 111111.1f * std::cos(z_yz(nm) * pi / 180.0f);
+        cell_area_m2(nm) = dxm(nm) * dyrm(iref);
+      }
+      if (coriolis)
+        for (long nm = 1; nm <= np; nm++) fcorio2d(nm) = 2.0f * 7.2921e-05f * std::sin(z_yz(nm) * pi / 180.0f);
+      nuvisc.alloc(nref);
+      if (viscosity)  // :1549-1559
+        for (int iref = 1; iref <= nref; iref++) nuvisc(iref) = std::max(nuviscdim * dxyr(iref) / 0.00001f, 0.0f);
+      return;
+    }
     for (int iref = 1; iref <= nref; iref++) {
       dxrm(iref) = dxr(iref);
       dxrinv(iref) = 1.0f / dxrm(iref);
@@ -1552,7 +1590,7 @@ struct Model {
       long L = subgrid_nlevels;
       for (long nm = 1; nm <= np; nm++) {
         if (zs(nm) >= sg_z_zmax(nm)) {
-          z_volume(nm) = (TV)((double)sg_z_volmax(nm) + (double)cell_area(z_flags_iref(nm)) *
+          z_volume(nm) = (TV)((double)sg_z_volmax(nm) + (double)area_of(nm) *
                                                          ((double)zs(nm) - (double)std::max(sg_z_zmax(nm), -20.0f)));
         } else {
           long ivol = 1;
@@ -2710,7 +2748,7 @@ struct Model {
           }
         }
       } else if (inftype == "hor") {  // :914-1033
-        float hh_local = subgrid ? (float)(z_volume(nm) / (double)cell_area(z_flags_iref(nm)))
+        float hh_local = subgrid ? (float)(z_volume(nm) / (double)area_of(nm))
                                  : (float)((double)zs(nm) - (double)zb(nm));
         if (hh_local > 0.0f || prcp(nm) > 0.0f) {
           if (rain_T1(nm) > 0.0f)
@@ -3011,7 +3049,23 @@ struct Model {
         }
         int idir = uv_flags_dir(ip);
         T dxuvinv, dyuvinv, dxuv2inv, dyuv2inv;
-        if (itype == 0) {
+        if (crsgeo) {  // sfincs_momentum.f90:205-234
+          if (itype == 0) {
+            if (idir == 0) {
+              dxuvinv = dxminv(ip); dyuvinv = dyrinv(iref); dxuv2inv = dxm2inv(ip); dyuv2inv = dyr2inv(iref);
+            } else {
+              dxuvinv = dyrinv(iref); dyuvinv = dxminv(ip); dxuv2inv = dyr2inv(iref); dyuv2inv = dxm2inv(ip);
+            }
+          } else {
+            if (idir == 0) {
+              dxuvinv = (T)(1.0f / (3.0f * (1.0f / dxminv(ip)) / 2.0f)); dyuvinv = dyrinv(iref); dxuv2inv = 0;
+              dyuv2inv = dyr2inv(iref);
+            } else {
+              dxuvinv = (T)(1.0f / (3.0f * (1.0f / dyrinv(iref)) / 2.0f)); dyuvinv = dxminv(ip); dxuv2inv = 0;
+              dyuv2inv = dxm2inv(ip);
+            }
+          }
+        } else if (itype == 0) {
           if (idir == 0) {
             dxuvinv = dxrinv(iref); dyuvinv = dyrinv(iref); dxuv2inv = dxr2inv(iref); dyuv2inv = dyr2inv(iref);
           } else {
@@ -3024,7 +3078,7 @@ struct Model {
             dxuvinv = dyrinvc(iref); dyuvinv = dxrinv(iref); dxuv2inv = 0; dyuv2inv = dxr2inv(iref);
           }
         }
-        T fcoriouv = (T)fcorio;
+        T fcoriouv = crsgeo ? (T)fcorio2d(nm) : (T)fcorio;
         T qx_nm = q0(ip);
         T qx_nmd = 0, qx_nmu = 0, qy_nm = 0, qy_nmu = 0, qy_ndm = 0, qy_ndmu = 0;
         T uu_nm = 0, uu_nmd = 0, uu_nmu = 0, uu_ndm = 0, uu_num = 0, vu = 0;
@@ -3214,7 +3268,7 @@ struct Model {
   void compute_water_levels_regular(float dtt, double tt) {
     for (long is = 1; is <= nsrcdrn; is++) {
       long nm = nmindsrc(is);
-      zs(nm) = (TZ)std::max((double)(zs(nm) + (TZ)(qtsrc(is) * dtt / cell_area(z_flags_iref(nm)))), (double)zb(nm));
+      zs(nm) = (TZ)std::max((double)(zs(nm) + (TZ)(qtsrc(is) * dtt / area_of(nm))), (double)zb(nm));
     }
 #pragma omp parallel for schedule(dynamic, 256)
     for (long nm = 1; nm <= np; nm++) {
@@ -3223,7 +3277,8 @@ struct Model {
         if (use_qext) zs(nm) = zs(nm) + (TZ)((T)qext(nm) * (T)dtt);
         long nmd = z_index_uv_md(nm), nmu = z_index_uv_mu(nm), ndm = z_index_uv_nd(nm), num = z_index_uv_nu(nm);
         int ir = z_flags_iref(nm);
-        T dz = ((q(nmd) - q(nmu)) * (T)dxrinv(ir) + (q(ndm) - q(num)) * (T)dyrinv(ir)) * (T)dtt;
+        T dz = crsgeo ? ((q(nmd) - q(nmu)) / (T)dxm(nm) + (q(ndm) - q(num)) * (T)dyrinv(ir)) * (T)dtt  // :135-147
+                      : ((q(nmd) - q(nmu)) * (T)dxrinv(ir) + (q(ndm) - q(num)) * (T)dyrinv(ir)) * (T)dtt;
         zs(nm) = zs(nm) + (TZ)dz;
       }
       if (store_maximum_waterlevel) {
@@ -3246,7 +3301,10 @@ struct Model {
       T dvol = 0;
       if (kcs(nm) == 1) {
         long nmd = z_index_uv_md(nm), nmu = z_index_uv_mu(nm), ndm = z_index_uv_nd(nm), num = z_index_uv_nu(nm);
-        if (use_quadtree) {
+        if (crsgeo) {  // :350-361
+          int ir = z_flags_iref(nm);
+          dvol = dvol + ((q(nmd) - q(nmu)) * (T)dyrm(ir) + (q(ndm) - q(num)) * (T)dxm(nm)) * (T)dtt;
+        } else if (use_quadtree) {
           int ir = z_flags_iref(nm);
           dvol = dvol + ((q(nmd) - q(nmu)) * (T)dyrm(ir) + (q(ndm) - q(num)) * (T)dxrm(ir)) * (T)dtt;
         } else {
@@ -3254,7 +3312,7 @@ struct Model {
         }
       }
       if (kcs(nm) == 1 || kcs(nm) == 4) {
-        T a = cell_area(z_flags_iref(nm));
+        T a = area_of(nm);  // :458-470
         if (precip || use_qext) {
           T dzsdt = 0;
           if (precip) dzsdt = dzsdt + (T)netprcp(nm);
@@ -3541,6 +3599,8 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "cuminf" && m.cuminf.allocated()) copy_out(m.cuminf, out, n);
     else if (s == "qext" && m.qext.allocated()) copy_out(m.qext, out, n);
     else if (s == "uvmean") copy_out(m.uvmean, out, n);
+    else if (s == "cell_area_m2" && m.cell_area_m2.allocated()) copy_out(m.cell_area_m2, out, n);
+    else if (s == "dxm" && m.dxm.allocated()) copy_out(m.dxm, out, n);
     else if (s == "zsmax_out" && m.zsmax_out.allocated()) copy_out(m.zsmax_out, out, n);
     else if (s == "vmax_out" && m.vmax_out.allocated()) copy_out(m.vmax_out, out, n);
     else if (s == "qmax_out" && m.qmax_out.allocated()) copy_out(m.qmax_out, out, n);

@@ -61,7 +61,7 @@ __global__ void k_volume_partial(const ScnDev* __restrict__ scn, const int32_t* 
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int32_t c = cmp[i];
     if (!(S.flags[c] & F_KCS1)) continue;
-    const float area = S.quadtree ? S.lv_area[S.qlev[c]] : S.area;
+    const float area = S.geo ? S.geo_area[c] : S.quadtree ? S.lv_area[S.qlev[c]] : S.area;
     acc += S.subgrid ? S.zvol[c] : ((double)S.zs[c] - (double)S.zb[c]) * (double)area;
   }
   __shared__ double s[32];

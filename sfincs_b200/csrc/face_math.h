@@ -106,6 +106,7 @@ __device__ __forceinline__ void face_meteo(const ScnDev& S, const StepVals& sv, 
 // viscosity coefficient of the face's refinement level.
 struct FaceGeo {
   float dxuvinv, dyuvinv, dxuv2inv, dyuv2inv, nuvisc;
+  float fcorio;  // Coriolis parameter at the face (per cell on geographic grids)
 };
 
 // Gathered inputs of one face (sfincs_momentum.f90:317-335 naming).
@@ -181,9 +182,9 @@ __device__ __forceinline__ float face_flux_geo(const ScnDev& S, const StepVals& 
   }
   if (S.coriolis) {
     if (dir == 0)
-      frc = frc + S.fcorio * hu * a.vu;
+      frc = frc + geo.fcorio * hu * a.vu;
     else
-      frc = frc - S.fcorio * hu * a.vu;
+      frc = frc - geo.fcorio * hu * a.vu;
   }
   if (S.wind) {
     const float hwet = hu / phi;

@@ -687,7 +687,13 @@ int get_sfincs_cell_area(const int* index, double* area) {
   return guarded([&] {
     sfg::require_bmi();
     if (*index < 1 || *index > g_bmi->np()) throw std::runtime_error("cell index out of range");
-    *area = (double)g_bmi->host->p.area;
+    const sfg::HostModel& h = *g_bmi->host;
+    if (h.p.geo)  // cell_area_m2 (sfincs_bmi.f90:359-362)
+      *area = (double)h.geo_area[(size_t)h.cmp_off[(size_t)*index - 1]];
+    else if (h.p.quadtree)
+      *area = (double)h.cell_area[(size_t)*index - 1];
+    else
+      *area = (double)h.p.area;
     return 0;
   });
 }

@@ -316,7 +316,15 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   // (sfincs_initial_conditions.F90:61-78); the binary form is read below.
   if (!is_none(inifile) && inifile.size() >= 2 && inifile.compare(inifile.size() - 2, 2, "nc") == 0)
     throw std::runtime_error("netCDF inifile is not supported by this core (use the binary real*4 form)");
-  if (igeo != 0) throw std::runtime_error("geographic grids (crsgeo=1) are not supported by this core");
+  // geographic grids (crsgeo, sfincs_input.f90:399-421): regular grids; the
+  // options whose geographic arithmetic this core does not carry are refused
+  if (igeo != 0) {
+    if (!is_none(qtrfile)) throw std::runtime_error("geographic quadtree meshes (crsgeo=1 with qtrfile) are not supported");
+    for (const char* k : {"spwfile", "weirfile", "drnfile"})
+      if (!is_none(in.str(k, "none")))
+        throw std::runtime_error(std::string("input '") + k + "' on a geographic grid (crsgeo=1) is not supported");
+  }
+  P.geo = igeo != 0 ? 1 : 0;
   if (inputtype != "bin") throw std::runtime_error("only inputformat = bin is supported");
   if (bndtype != 1) throw std::runtime_error("only bndtype = 1 is supported");
   const bool quadtree = !is_none(qtrfile);
@@ -375,8 +383,10 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   qinf = qinf / (float)(3600 * 1000);
   rotation = rotation * P.pi / 180.0f;
   const float cosrot = std::cos(rotation), sinrot = std::sin(rotation);
-  P.fcorio = 2.0f * 7.2921e-05f * std::sin(latitude * P.pi / 180.0f);
-  if (latitude < 0.01f && latitude > -0.01f) coriolis = false;
+  if (!P.geo) {  // projected: Coriolis from the latitude, off near the equator (geographic: per cell)
+    P.fcorio = 2.0f * 7.2921e-05f * std::sin(latitude * P.pi / 180.0f);
+    if (latitude < 0.01f && latitude > -0.01f) coriolis = false;
+  }
   P.coriolis = coriolis;
   P.store_zsmax = dtmaxout > 0.0f;
   h.store_vmax = in.integer("storevelmax", 0) == 1 && dtmaxout > 0.0f;
@@ -723,6 +733,26 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     h.z_xz[i] = x0 + cosrot * (1.0f * (m - 0.5f)) * dx - sinrot * (1.0f * (n - 0.5f)) * dy;
     h.z_yz[i] = y0 + sinrot * (1.0f * (m - 0.5f)) * dx + cosrot * (1.0f * (n - 0.5f)) * dy;
   }
+  if (P.geo) {  // geographic: dx, dy in degrees (sfincs_domain.f90:1403-1473, 1549-1559)
+    P.geo_dyrm = 111111.1f * dy;
+    P.dyinv = 1.0f / P.geo_dyrm;
+    P.dy2inv = P.dyinv * P.dyinv;
+    P.dtmax = dtmax;  // no limit from the spacing, and no dtmin, on geographic grids
+    P.dtmin = 0.0f;
+    P.nuvisc = viscosity ? std::max(nuviscdim * std::min(dx, dy) / 0.00001f, 0.0f) : 0.0f;
+    h.geo_dxm.assign(NA, 0.0f);
+    h.geo_dxminv.assign(NA, 0.0f);
+    h.geo_area.assign(NA, 0.0f);
+    if (P.coriolis) h.geo_fcor.assign(NA, 0.0f);
+    for (long long i = 0; i < h.np; i++) {
+      const int64_t c = h.cmp_off[i];
+      const float cl = std::cos(h.z_yz[i] * P.pi / 180.0f);
+      h.geo_dxm[c] = dx * 111111.1f * cl;
+      h.geo_dxminv[c] = 1.0f / (dx * 111111.1f * cl);
+      h.geo_area[c] = h.geo_dxm[c] * P.geo_dyrm;
+      if (P.coriolis) h.geo_fcor[c] = 2.0f * 7.2921e-05f * std::sin(h.z_yz[i] * P.pi / 180.0f);
+    }
+  }
 
   // ---- faces and their reference order (sfincs_domain.f90:727-1003) ----------
   // kcu/kcv: kcuv of the u/v face owned by each dense cell (0 where no face).
@@ -1060,7 +1090,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     b.zbuv = P.subgrid ? 0.0f : 0.5f * (h.zb[e.face] + h.zb[e.dir == 0 ? e.face + ld : e.face + 1]);
     b.floor = P.subgrid ? h.zz_min[e.nmb] : h.zb[e.nmb];
     b.zfix = gb_zfix[ib];
-    b.len = e.dir == 1 ? dx : dy;
+    b.len = P.geo ? (e.dir == 1 ? h.geo_dxm[b.nmi] : P.geo_dyrm) : (e.dir == 1 ? dx : dy);
     if (kcs[e.nmb] == 2 && nbnd == 0) b.info |= 4, b.zfix = 0.0f;  // no boundary data: zsb stays 0
     if (kcs[e.nmb] == 5) {  // downstream river cell: level from its internal point
       const int j = gb_bdr[ib];
@@ -1247,7 +1277,7 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     h.kcs_cmp[i] = kcs[h.cmp_off[i]];
     if (kcs[h.cmp_off[i]] == 1) {
       h.n_kcs1++;
-      h.area_total_kcs1 += (double)P.area;
+      h.area_total_kcs1 += (double)(P.geo ? h.geo_area[h.cmp_off[i]] : P.area);
     }
   }
 
@@ -1308,7 +1338,8 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
       const int64_t c = h.cmp_off[i];
       const double zs = h.zs[c];
       if (zs >= (double)h.zz_max[c]) {
-        h.zvol[c] = (double)h.zz_volmax[c] + (double)P.area * (zs - (double)std::max(h.zz_max[c], -20.0f));
+        h.zvol[c] = (double)h.zz_volmax[c] + (double)(P.geo ? h.geo_area[c] : P.area) *
+                                                 (zs - (double)std::max(h.zz_max[c], -20.0f));
       } else {
         const float* dep = &sg_level_raw[(size_t)i * L];  // z_level of this cell, levels 1..L
         int ivol = 1;
@@ -1654,6 +1685,10 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   }
   up(d.inf_rain, h.inf_rain);
   up(d.cumprcp, h.cumprcp);
+  up(d.geo_dxm, h.geo_dxm);
+  up(d.geo_dxminv, h.geo_dxminv);
+  up(d.geo_area, h.geo_area);
+  up(d.geo_fcor, h.geo_fcor);
   if (h.need_qinfmap)
     zero(d.qinfmap, h.p.quadtree ? (size_t)h.np : NA);
   else
@@ -1744,6 +1779,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
     if (h.p.nsrc > 0 || h.p.ndrn > 0) any_src_ = 1;
     if (h.p.nstruc > 0) any_struc_ = 1;
     if (h.p.wind_field || h.p.patmos) met_ = 1;
+    if (h.p.geo) geo_ = 1;
     if (h.p.inftype >= 2 || h.p.store_cumprcp || h.p.prcp_field || h.p.store_vmax || h.p.store_qmax ||
         h.p.store_twet || h.p.store_tzsmax || h.need_qinfmap)
       ext_ = 1;
@@ -1783,6 +1819,7 @@ Runner::Runner(std::vector<DeviceModel*> models, int tile_m, cudaStream_t stream
     const int x = std::atoi(v);
     variant_ = (x >= 2 && x <= 5) ? x : 5;
   }
+  if (geo_ && variant_ >= 4) variant_ = 2;  // the staged tile kernels assume one spacing per scenario
   if (!qt_) {
     // TMA tensor maps (one set per model) and persistent grid sizes
     std::vector<MapSet> maps;
@@ -1961,7 +1998,7 @@ void Runner::step_once(cudaEvent_t continuity_after) {
 // result, and the tuning steps are part of the run.  Only meaningful while
 // the models still have steps to take; returns the chosen variant.
 int Runner::autotune(int chunk) {
-  if (qt_) return variant_;  // one quadtree kernel path
+  if (qt_ || geo_) return variant_;  // one quadtree kernel path; geographic grids on the per-thread kernels
   static const int kCandidates[] = {5, 4, 2};
   cudaEvent_t e0, e1;
   check_cuda(cudaEventCreate(&e0), "event");

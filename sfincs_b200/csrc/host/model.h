@@ -136,6 +136,7 @@ struct HostModel {
   // output
   OutputSpec out;
   bool need_qinfmap = false;               // an output reads the step's infiltration rate per cell
+  std::vector<float> geo_dxm, geo_dxminv, geo_area, geo_fcor;  // geographic grids: per dense cell
 };
 
 class InpFile;
@@ -268,7 +269,7 @@ class Runner {
   int bnd_blocks() const { return bnd_blocks_; }
   // kernel variant (momentum occupancy target); SFG_MOMENTUM_VARIANT overrides the default
   void set_variant(int v) {
-    variant_ = v;
+    variant_ = (geo_ && v >= 4) ? 2 : v;  // geographic grids run the per-thread kernels
     if (graph_) {
       cudaGraphExecDestroy(graph_);
       graph_ = nullptr;
@@ -312,6 +313,7 @@ class Runner {
   int any_meteo_ = 0, meteo_cells_ = 0;  // gridded meteo: the window kernel runs before each step kernel
   int met_ = 0;  // gridded wind or pressure: momentum runs its meteo instance (variant + 10)
   int ext_ = 0;  // continuity runs its extended instance (infiltration with state, sums, gridded rain, store variables)
+  int geo_ = 0;  // a geographic grid: per-cell spacing, on the per-thread kernels (variants 2 and 3)
   cudaStream_t stream_ = nullptr;
   bool own_stream_ = true;
   cudaGraphExec_t graph_ = nullptr;

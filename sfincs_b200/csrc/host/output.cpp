@@ -401,8 +401,9 @@ void OutputWriter::open_map() {
     auto axis = [&](const char* name, bool x, std::vector<int> dims, const char* long_name) {
       const int v = nc.def_var(name, NcWriter::FLOAT, dims);
       nc.att_float(v, "_FillValue", kFill);
-      nc.att_text(v, "units", "m");
-      nc.att_text(v, "standard_name", x ? "projection_x_coordinate" : "projection_y_coordinate");
+      nc.att_text(v, "units", P.geo ? "degrees" : "m");  // def_grid_axis_coord
+      nc.att_text(v, "standard_name", P.geo ? (x ? "longitude" : "latitude")
+                                            : (x ? "projection_x_coordinate" : "projection_y_coordinate"));
       nc.att_text(v, "long_name", long_name);
       nc.att_text(v, "grid_mapping", "crs");
       nc.att_text(v, "grid", "sfincsgrid");
@@ -603,8 +604,9 @@ void OutputWriter::open_his() {
   nc.att_text(v_name, "cf_role", "timeseries_id");
   auto coord = [&](const char* name, bool x, const char* long_name) {
     const int v = nc.def_var(name, NcWriter::FLOAT, {d_st});
-    nc.att_text(v, "units", "m");
-    nc.att_text(v, "standard_name", x ? "projection_x_coordinate" : "projection_y_coordinate");
+    nc.att_text(v, "units", P.geo ? "degrees" : "m");  // def_his_point_coord
+    nc.att_text(v, "standard_name", P.geo ? (x ? "longitude" : "latitude")
+                                          : (x ? "projection_x_coordinate" : "projection_y_coordinate"));
     nc.att_text(v, "long_name", long_name);
     nc.att_text(v, "grid_mapping", "crs");
     return v;

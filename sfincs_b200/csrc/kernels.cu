@@ -819,10 +819,20 @@ __device__ __forceinline__ float momentum_face(const ScnDev& S, const StepVals& 
     gnavg2 = (DIR == 0 ? S.gn2_u : S.gn2_v)[c];
   }
   FaceGeo geo;
-  geo.dxuvinv = DIR == 0 ? S.dxinv : S.dyinv;
-  geo.dyuvinv = DIR == 0 ? S.dyinv : S.dxinv;
-  geo.dxuv2inv = DIR == 0 ? S.dx2inv : S.dy2inv;
-  geo.dyuv2inv = DIR == 0 ? S.dy2inv : S.dx2inv;
+  if (S.geo) {  // geographic: the cell's width across x, in metres (sfincs_momentum.f90:205-217)
+    const float dxm_inv = S.geo_dxminv[c];
+    geo.dxuvinv = DIR == 0 ? dxm_inv : S.dyinv;
+    geo.dyuvinv = DIR == 0 ? S.dyinv : dxm_inv;
+    geo.dxuv2inv = DIR == 0 ? dxm_inv * dxm_inv : S.dy2inv;
+    geo.dyuv2inv = DIR == 0 ? S.dy2inv : dxm_inv * dxm_inv;
+    geo.fcorio = S.geo_fcor ? S.geo_fcor[c] : 0.0f;
+  } else {
+    geo.dxuvinv = DIR == 0 ? S.dxinv : S.dyinv;
+    geo.dyuvinv = DIR == 0 ? S.dyinv : S.dxinv;
+    geo.dxuv2inv = DIR == 0 ? S.dx2inv : S.dy2inv;
+    geo.dyuv2inv = DIR == 0 ? S.dy2inv : S.dx2inv;
+    geo.fcorio = S.fcorio;
+  }
   geo.nuvisc = S.nuvisc;
   FaceV a;
   a.qx_nm = qx_nm;
@@ -899,7 +909,7 @@ __global__ void k_sources(const ScnDev* __restrict__ scns) {
         vol += (double)(S.qtsrc[is] * dt);
       }
     } else {
-      const float area = S.quadtree ? S.lv_area[S.qlev[c]] : S.area;  // cell_area(z_flags_iref(nm))
+      const float area = S.geo ? S.geo_area[c] : S.quadtree ? S.lv_area[S.qlev[c]] : S.area;  // cell_area(_m2)
       const float before = S.zs[c];
       const float z = fmaxf(S.zs[c] + S.qtsrc[is] * dt / area, S.zb[c]);
       S.zs[c] = z;
@@ -994,6 +1004,7 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
   if (!(f & F_ACT)) return;
   const float dt = st.dt;
   float zsn = zs_old;
+  const float area = S.geo ? S.geo_area[c] : S.area;  // cell_area_m2 on geographic grids (:458-470)
   // infiltration with state (or cumulative rain) for every active cell, from the start-of-step state
   const bool inf_cell = S.precip && (S.inftype >= 2 || S.store_cumprcp);
   float qinf_cell = 0.0f;
@@ -1004,7 +1015,7 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
                     netr);
   if (inf_cell) {
     if (SG) {
-      qinf_cell = cell_infiltration(S, c, prc, dt, v_old <= 0.0, (float)(v_old / (double)S.area), st.ga_hs);
+      qinf_cell = cell_infiltration(S, c, prc, dt, v_old <= 0.0, (float)(v_old / (double)area), st.ga_hs);
     } else {
       const float zb0 = S.zb[c];
       qinf_cell = cell_infiltration(S, c, prc, dt, zs_old <= zb0, (float)((double)zs_old - (double)zb0), st.ga_hs);
@@ -1013,7 +1024,9 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
   if (S.qinfmap) store_qinfmap(S, c, inf_cell, qinf_cell, SG ? v_old > 0.0 : !(zs_old <= S.zb[c]));
   if (f & F_KCS1) {
     if (SG) {  // sfincs_continuity.f90:341-577
-      float dvol = ((q_md - q_mu) * S.dy + (q_nd - q_nu) * S.dx) * dt;
+      // geographic: the face lengths are dyrm and the cell's width dxm (:350-361)
+      float dvol = S.geo ? ((q_md - q_mu) * S.geo_dyrm + (q_nd - q_nu) * S.geo_dxm[c]) * dt
+                         : ((q_md - q_mu) * S.dy + (q_nd - q_nu) * S.dx) * dt;
       if (S.precip || S.use_qext) {
         float dzsdt = 0.0f;
         if (S.precip) {
@@ -1021,13 +1034,13 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
           dzsdt = dzsdt + (netr - qinfmap);
         }
         if (S.use_qext) dzsdt = dzsdt + qx;
-        dvol = dvol + dzsdt * S.area * dt;
+        dvol = dvol + dzsdt * area * dt;
       }
       const double v = v_old + (double)dvol;
       if (v != v_old) S.zvol[c] = v;
       const float zs11 = zs_old;
       if (v >= (double)(volmax * 0.999f)) {
-        zsn = (float)((double)fmaxf(S.zz_max[c], -20.0f) + (v - (double)volmax) / (double)S.area);
+        zsn = (float)((double)fmaxf(S.zz_max[c], -20.0f) + (v - (double)volmax) / (double)area);
       } else if (v <= (double)1.0e-6f) {
         zsn = fmaxf(S.zz_min[c], -20.0f);
       } else {
@@ -1051,7 +1064,10 @@ __global__ void __launch_bounds__(256) k_continuity(const ScnDev* __restrict__ s
         z = z + (netr - qinfmap) * dt;
       }
       if (S.use_qext) z = z + qx * dt;
-      z = z + ((q_md - q_mu) * S.dxinv + (q_nd - q_nu) * S.dyinv) * dt;
+      if (S.geo)  // the cell's width, divided as the reference divides (:135-147)
+        z = z + ((q_md - q_mu) / S.geo_dxm[c] + (q_nd - q_nu) * S.dyinv) * dt;
+      else
+        z = z + ((q_md - q_mu) * S.dxinv + (q_nd - q_nu) * S.dyinv) * dt;
       if (z != zs_old) S.zs[c] = z;
       zsn = z;
     }

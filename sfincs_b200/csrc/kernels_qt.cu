@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
           geo.dyuv2inv = dir == 0 ? S.lv_dyr2inv[L] : S.lv_dxr2inv[L];
           geo.nuvisc = S.lv_nuvisc_t[L];
         }
+        geo.fcorio = S.fcorio;
         FaceV a{};
         a.qx_nm = q0[i];
         if (S.advection || S.coriolis || S.viscosity || S.friction2d || S.thetasmooth) {

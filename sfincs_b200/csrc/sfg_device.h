@@ -288,6 +288,15 @@ struct ScnDev {
   const float* inf_par[5];
   float* inf_st[5];
   uint8_t* inf_rain;
+  // geographic grids (crsgeo, sfincs_domain.f90:1403-1473; null on projected
+  // grids): per cell its width dxm (m), 1/dxm (the inverse spacing of both of
+  // its faces across x), its area (m2) and its Coriolis parameter
+  int geo;
+  float geo_dyrm;        // 111111.1 dy (m): the length of the u faces
+  const float* geo_dxm;
+  const float* geo_dxminv;
+  const float* geo_area;
+  const float* geo_fcor;
   float* qinfmap;        // infiltration rate of the step (m/s) per cell, when an output needs it (else null)
   float* cumprcp;        // cumulative rain and infiltration (m), when stored or needed (cna, cnb)
   float* cuminf;

@@ -405,7 +405,7 @@ class RegularModel:
             write_sbg(os.path.join(d, "sfincs.sbg"), self.sbg)
             inp["sbgfile"] = "sfincs.sbg"
         if self.bnd is not None:
-            np.savetxt(os.path.join(d, "sfincs.bnd"), self.bnd, fmt="%.4f")
+            np.savetxt(os.path.join(d, "sfincs.bnd"), self.bnd, fmt="%.8f" if self.params.get("crsgeo") else "%.4f")
             inp["bndfile"] = "sfincs.bnd"
         if self.bzs is not None:
             np.savetxt(os.path.join(d, "sfincs.bzs"), self.bzs, fmt="%.6f")

@@ -241,3 +241,23 @@ def test_spiderweb_options_outside_the_core_are_refused(tmp_path):
         add_spiderweb(str(d), 3600.0, 3000.0, extra=extra)
         with pytest.raises(RuntimeError, match=list(extra)[0]):
             B.layout(str(d), "flags", 1)
+
+
+def test_geographic_grids_load_and_refuse_what_they_do_not_carry(tmp_path):
+    """crsgeo = 1 loads on regular grids; spiderwebs, weirs and drainage on a
+    geographic grid are refused, naming the keyword."""
+    from geo_cases import geographic
+
+    m = synth.plain_regular(nmax=8, mmax=10, dx=300.0, tstop=600.0, seed=1, nbumps=2)
+    geographic(m)
+    d = m.write(str(tmp_path / "ok"))
+    cnt = B.layout(d, "counts", 10)
+    assert int(cnt[0]) == 80
+    assert cnt[6] == 60.0 and cnt[7] == 0.0  # dtmax not limited by the spacing, no dtmin (sfincs_domain.f90:1403-1475)
+    for key in ("spwfile", "weirfile", "drnfile"):
+        m2 = synth.plain_regular(nmax=8, mmax=10, dx=300.0, tstop=600.0, seed=1, nbumps=2)
+        geographic(m2)
+        m2.params[key] = "x.dat"
+        d2 = m2.write(str(tmp_path / key))
+        with pytest.raises(RuntimeError, match=key):
+            B.layout(d2, "counts", 10)
