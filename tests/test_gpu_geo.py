@@ -34,7 +34,7 @@ def test_geographic_matches_f32_oracle(tmp_path, subgrid):
     d, m = _write(tmp_path, subgrid)
     o = Oracle(d, "f32")
     g = Model(d)
-    assert g.variant() == 2  # geographic grids run the per-thread kernels
+    assert g.variant == 2  # geographic grids run the per-thread kernels
     done = 0
     for n in (1, 1, 2, 6, 30, 60, 100):
         o.update(-1000.0, n)
