@@ -1092,6 +1092,9 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     b.zfix = gb_zfix[ib];
     b.len = P.geo ? (e.dir == 1 ? h.geo_dxm[b.nmi] : P.geo_dyrm) : (e.dir == 1 ? dx : dy);
     if (kcs[e.nmb] == 2 && nbnd == 0) b.info |= 4, b.zfix = 0.0f;  // no boundary data: zsb stays 0
+    // an isolated Neumann cell reset to inactive keeps its lateral face in the
+    // boundary list, where its level zsb stays at its initial 0 (sfincs_boundaries.f90:661-672, 800-921)
+    if (kcs[e.nmb] == 0) b.info |= 4, b.zfix = 0.0f;
     if (kcs[e.nmb] == 5) {  // downstream river cell: level from its internal point
       const int j = gb_bdr[ib];
       if (j < 0) throw std::runtime_error("downstream river cell without a bdr point");

@@ -147,7 +147,7 @@ void QtBuilder::mesh() {
   for (long nm = 1; nm <= np; nm++) {
     const long iq = q_of_sf[nm];
     kcs[nm] = q.mask[iq - 1];
-    if (kcs[nm] == 4 || kcs[nm] == 5) throw std::runtime_error("msk values 4/5 are not supported");
+    if (kcs[nm] == 4) throw std::runtime_error("msk value 4 (wave makers) is not supported");
     iref_of[nm] = q.level[iq - 1];
     fmd[nm] = q.md[iq - 1], fmu[nm] = q.mu[iq - 1], fnd[nm] = q.nd[iq - 1], fnu[nm] = q.nu[iq - 1];
     md1[nm] = sf(q.md1[iq - 1]), md2[nm] = sf(q.md2[iq - 1]);
@@ -536,8 +536,22 @@ void QtBuilder::bed() {
 void QtBuilder::boundaries() {
   ScnDev& P = h.p;
   auto path = [&](const std::string& f) { return h.dir + "/" + f; };
-  for (long nm = 1; nm <= np; nm++)
-    if (kcs[nm] == 6) throw std::runtime_error("Neumann boundaries (msk 6) on quadtree meshes are not supported by this core");
+  // point lookup keys (find_quadtree_cell: sfincs_quadtree.F90:764-820)
+  {
+    std::vector<std::pair<int64_t, int32_t>> kv((size_t)np);
+    for (long nm = 1; nm <= np; nm++)
+      kv[nm - 1] = {qt_key(iref_of[nm], h.z_m[nm - 1], h.z_n[nm - 1]), (int32_t)(nm - 1)};
+    std::sort(kv.begin(), kv.end());
+    h.qt_key.resize(np);
+    h.qt_key_cell.resize(np);
+    for (long i = 0; i < np; i++) h.qt_key[i] = kv[i].first, h.qt_key_cell[i] = kv[i].second;
+  }
+  // the active cell of level iref at (n, m), 0 if none (find_sfincs_cell)
+  auto cell_at = [&](long n, long m, int iref) -> long {
+    const int64_t key = qt_key(iref, m, n);
+    auto it = std::lower_bound(h.qt_key.begin(), h.qt_key.end(), key);
+    return (it != h.qt_key.end() && *it == key) ? (long)h.qt_key_cell[it - h.qt_key.begin()] + 1 : 0;
+  };
   kcuv.assign(npuv + ncuv + 2, 0);
   auto kcuv_of = [](int a, int b) -> int8_t {
     if (a > 1 && b > 1) return 0;
@@ -549,11 +563,11 @@ void QtBuilder::boundaries() {
     return 1;
   };
   for (long ip = 1; ip <= npuv; ip++) kcuv[ip] = kcuv_of(kcs[uv_nm[ip]], kcs[uv_nmu[ip]]);
-  // boundary cells and their forcing
+  // boundary cells (water level, outflow, downstream river, Neumann; sfincs_domain.f90:1786-1830) and their forcing
   std::vector<int32_t> gb_cell, gb_index(np + 1, -1);
   bool water_level_bnd = false;
   for (long nm = 1; nm <= np; nm++)
-    if (kcs[nm] == 2 || kcs[nm] == 3) {
+    if (kcs[nm] == 2 || kcs[nm] == 3 || kcs[nm] == 5 || kcs[nm] == 6) {
       gb_index[nm] = (int32_t)gb_cell.size();
       gb_cell.push_back((int32_t)nm);
       h.gb_cmp.push_back((int32_t)(nm - 1));
@@ -563,6 +577,56 @@ void QtBuilder::boundaries() {
   std::vector<float> xb, yb;
   int nbnd = 0;
   read_boundary_series(h, k, water_level_bnd, xb, yb, nbnd);
+  // downstream river points (sfincs_boundaries.f90:217-270): the cell of each
+  // point's internal point and the level drop slope * distance to it
+  std::vector<float> xr, yr, dzr;
+  std::vector<int32_t> zsir;
+  bool river = false;
+  for (long nm : gb_cell) river = river || kcs[nm] == 5;
+  if (river) {
+    if (none(k.bdrfile)) throw std::runtime_error("downstream river points (msk 5) need a bdrfile");
+    for (const auto& r : read_table(path(k.bdrfile))) {
+      if (r.size() < 6) throw std::runtime_error("bdrfile: expected x y x_internal y_internal slope distance");
+      const float x = (float)r[0], y = (float)r[1], xin = (float)r[2], yin = (float)r[3];
+      const float slope = (float)r[4], dist = (float)r[5];
+      const int ci = quadtree_cell_index(h, xin, yin);
+      if (ci <= 0) throw std::runtime_error("bdrfile: internal point outside the active mesh");
+      xr.push_back(x);
+      yr.push_back(y);
+      zsir.push_back(ci - 1);
+      dzr.push_back(dist < 0.0f ? -slope * std::sqrt((xin - x) * (xin - x) + (yin - y) * (yin - y)) : -slope * dist);
+    }
+    if (xr.empty()) throw std::runtime_error("bdrfile holds no points");
+  }
+  std::vector<int> gb_bdr(ngb, -1);
+  for (size_t ib = 0; ib < ngb; ib++) {
+    const long nm = gb_cell[ib];
+    if (kcs[nm] == 5) {  // nearest point of the bdr file (:596-613)
+      const float x = h.z_xz[nm - 1], y = h.z_yz[nm - 1];
+      float dst1 = 1.0e10f;
+      for (size_t j = 0; j < xr.size(); j++) {
+        const float ddx = xr[j] - x, ddy = yr[j] - y;
+        const float dst = std::sqrt(ddx * ddx + ddy * ddy);
+        if (dst < dst1) {
+          dst1 = dst;
+          gb_bdr[ib] = (int)j;
+        }
+      }
+    } else if (kcs[nm] == 6) {  // Neumann: the last regular neighbour of the same level found (:615-672)
+      const long n = h.z_n[nm - 1], m = h.z_m[nm - 1];
+      const int iref = iref_of[nm];
+      const long cand[4][2] = {{n, m + 1}, {n + 1, m}, {n, m - 1}, {n - 1, m}};
+      long nmi = 0;
+      for (auto& c : cand) {
+        const long ci = cell_at(c[0], c[1], iref);
+        if (ci > 0 && kcs[ci] == 1) nmi = ci;
+      }
+      if (nmi == 0)
+        kcs[nm] = 0;  // isolated Neumann cell reset to inactive
+      else
+        h.neu.push_back(make_int2((int)(nm - 1), (int)(nmi - 1)));
+    }
+  }
   std::vector<int> gb_i1(ngb, 0), gb_i2(ngb, 0);
   std::vector<float> gb_fac(ngb, 0.0f);
   if (nbnd > 0)
@@ -594,11 +658,16 @@ void QtBuilder::boundaries() {
         gb_fac[ib] = 1.0f;
       }
     }
+  // the reference's boundary-face list holds the faces with kcuv 2 or 6; those
+  // of Neumann cells are left to the momentum kernel, but a Neumann cell reset
+  // to inactive keeps its faces in the list with its level zsb at its initial
+  // 0 (sfincs_boundaries.f90:661-672, 800-921, 947-960)
   for (long ip = 1; ip <= npuv; ip++) {
-    if (kcuv[ip] != 2) continue;
+    if (kcuv[ip] != 2 && kcuv[ip] != 6) continue;
     const long a = uv_nm[ip], b = uv_nmu[ip];
     const bool a_int = kcs[a] == 1;
     const long nmb = a_int ? b : a, nmi = a_int ? a : b;
+    if (kcuv[ip] == 6 && kcs[nmb] != 0) continue;
     BndFace f{};
     f.face = (int)(ip - 1);
     f.nmb = (int)(nmb - 1);
@@ -613,11 +682,20 @@ void QtBuilder::boundaries() {
     f.zfix = kcs[nmb] == 3 ? f.floor : 0.0f;
     f.len = uv_dir[ip] == 1 ? dxr[uv_iref[ip]] : dyr[uv_iref[ip]];
     if (kcs[nmb] == 2 && nbnd == 0) f.info |= 4, f.zfix = 0.0f;  // no boundary data: zsb stays 0
+    if (kcs[nmb] == 0) f.info |= 4, f.zfix = 0.0f;                 // reset Neumann cell: zsb stays 0
+    if (kcs[nmb] == 5) {  // downstream river cell: level from its internal point
+      const int j = gb_bdr[ib];
+      if (j < 0) throw std::runtime_error("downstream river cell without a bdr point");
+      f.info = (f.info & ~8) | 32;
+      f.zsi = zsir[(size_t)j];
+      f.zfix = dzr[(size_t)j];
+      f.i1 = f.i2 = 0;
+    }
     h.bfaces.push_back(f);
   }
   P.ngbnd = (int)ngb;
   P.nkcuv2 = (int)h.bfaces.size();
-  P.nneu = 0;
+  P.nneu = (int)h.neu.size();
 }
 
 // Device records of the uv points and cells, advection mask, roughness,
@@ -643,16 +721,6 @@ void QtBuilder::finish() {
       kk = 1;
   }
   const bool do_mask = P.advection && k.advection_mask && (nref > 1 || q.nmax > 1);  // :2132-2178
-  // point lookup keys (find_quadtree_cell: sfincs_quadtree.F90:764-820)
-  {
-    std::vector<std::pair<int64_t, int32_t>> kv((size_t)np);
-    for (long nm = 1; nm <= np; nm++)
-      kv[nm - 1] = {qt_key(iref_of[nm], h.z_m[nm - 1], h.z_n[nm - 1]), (int32_t)(nm - 1)};
-    std::sort(kv.begin(), kv.end());
-    h.qt_key.resize(np);
-    h.qt_key_cell.resize(np);
-    for (long i = 0; i < np; i++) h.qt_key[i] = kv[i].first, h.qt_key_cell[i] = kv[i].second;
-  }
   // Thin dams (sfincs_structures.f90:385-495, sfincs_quadtree.F90:853-1010):
   // per dam segment and refinement level, the cells in the segment's cell
   // index box widened by one; a right or upper uv point whose segment between
@@ -827,6 +895,9 @@ void QtBuilder::finish() {
   // restart file (sfincs_initial_conditions.F90:183-268): zs, q in the
   // reference's uv order (which is this mesh's), uvmean in boundary-face order
   RestartData rst;
+  // the reference's uvmean also holds the lateral (Neumann) faces of its boundary list
+  if (!h.neu.empty() && (!none(k.rstfile) || h.trstout < 1.0e9))
+    throw std::runtime_error("restart files on quadtree meshes with Neumann cells (msk 6) are not supported");
   if (!none(k.rstfile)) {
     rst = read_restart(h.dir + "/" + k.rstfile);
     if (rst.type >= 1 && rst.type <= 6) {

@@ -17,12 +17,26 @@ def _oracle(d, prec):
     return Oracle(d, prec)
 
 
-def _write(tmp_path, subgrid, seed=21, wind=30.0, tstop=1800.0, name="m"):
+def _write(tmp_path, subgrid, seed=21, wind=30.0, tstop=1800.0, name="m", edges=False):
     m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=3, bands=(1000.0, 500.0), P=4, seed=seed,
                                  tstop=tstop, subgrid=subgrid, wind_speed=wind, tide_period=1800.0)
+    if edges:  # lateral Neumann edges (msk 6) north and south, a downstream river edge (msk 5) east
+        lev, n, mm = m.mesh.level, m.mesh.n, m.mesh.m
+        nmax_l, mmax_l = 8 * 2 ** (lev - 1), 10 * 2 ** (lev - 1)
+        lateral = ((n == 1) | (n == nmax_l)) & (m.mask != 2)
+        m.mask[lateral] = 6
+        m.mask[(mm == mmax_l) & ~lateral] = 5
     d = tmp_path / name
     d.mkdir()
-    return m.write(str(d)), m
+    out = m.write(str(d))
+    if edges:
+        import os
+
+        with open(os.path.join(out, "sfincs.bdr"), "w") as f:  # x y x_internal y_internal slope distance
+            f.write("3950.0 1600.0 2950.0 1600.0 0.0005 -1.0\n3950.0 500.0 3450.0 700.0 0.0002 600.0\n")
+        with open(os.path.join(out, "sfincs.inp"), "a") as f:
+            f.write(f"{'bdrfile':<20} = sfincs.bdr\n")
+    return out, m
 
 
 def _cell_q(o, n_cells, npq):
@@ -116,11 +130,12 @@ def _add_green_ampt(d):
                                            (False, "infiltration"), (True, "infiltration"),
                                            (False, None), (True, None), (False, "sources"), (True, "sources"),
                                            (False, "dams"), (True, "dams"), (False, "weirs"), (True, "weirs"),
-                                           (False, "drainage"), (True, "drainage")])
+                                           (False, "drainage"), (True, "drainage"), (False, "edges"),
+                                           (True, "edges")])
 def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, extra):
     from sfincs_b200 import bmi as B
 
-    d, _ = _write(tmp_path, subgrid)
+    d, _ = _write(tmp_path, subgrid, edges=extra == "edges")
     if extra == "sources":
         _add_sources(d)
     if extra == "drainage":

@@ -71,3 +71,31 @@ def test_quadtree_inifile(tmp_path, subgrid):
     zs = B.layout(d, "zs", npc)
     assert np.array_equal(zs, o.get("zs", npc))
     assert np.any(zs != B.layout(_model(tmp_path / "plain", subgrid)[0], "zs", npc))
+
+
+@pytest.mark.parametrize("subgrid", [False, True])
+def test_quadtree_neumann_and_river_edges_match_oracle(tmp_path, subgrid):
+    """Lateral Neumann edges (msk 6) and a downstream river edge (msk 5) on a
+    3-level mesh: face activity and the water-level boundary faces (river
+    faces included, lateral faces left to the momentum kernel) face by face."""
+    import sys
+
+    sys.path.insert(0, str(__import__("pathlib").Path(__file__).parent))
+    from test_gpu_quadtree import _write
+
+    d, m = _write(tmp_path, subgrid, edges=True)
+    assert (m.mask == 6).sum() > 10 and (m.mask == 5).sum() > 5
+    o = _oracle(d)
+    qc = B.layout(d, "qt_counts", 4)
+    npc, npuv = int(qc[0]), int(qc[1])
+    kcuv = o.get("kcuv", npuv)
+    assert (kcuv == 6).sum() > 10
+    assert np.array_equal(B.layout(d, "uv_act", npuv), ((kcuv == 1) | (kcuv == 6)).astype(float))
+    nkb = int(B.layout(d, "counts", 10)[3])
+    # the oracle's list holds kcuv 2 and 6 faces; those of Neumann cells that
+    # found a regular neighbour belong to the momentum kernel, isolated ones
+    # (reset to inactive) stay in the list with their level at 0; the oracle's
+    # getter returns exactly the kept faces and refuses any other length
+    assert nkb > int((kcuv == 2).sum())
+    for name in ("kb_cell", "kb_dir", "kb_sign"):
+        assert np.array_equal(B.layout(d, name, nkb), o.get(name, nkb)), name
