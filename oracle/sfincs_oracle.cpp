@@ -137,6 +137,221 @@ static float core_exp(float x) {
   return (p * pow2(n1)) * pow2(n2);
 }
 
+// Cosine in FP64 of the core-precision instantiation (astronomic boundary
+// constituents), restating the CUDA core's method with the same IEEE
+// operations: n = rint(x 2/pi), r = x - n pi/2 with pi/2 split in three
+// doubles, each product fused with its subtraction (Cody and Waite), then the
+// Taylor series of sin (degree 17) or cos (degree 18) of r in Horner form with
+// fused multiply-adds, by the quadrant n mod 4.  The "ref" and "fp64"
+// instantiations call the library cosine, as the reference does.
+static double core_cos(double x) {
+  const double n = std::nearbyint(x * 0.6366197723675814);
+  double r = std::fma(-n, 1.5707963267948966, x);
+  r = std::fma(-n, 6.123233995736766e-17, r);
+  r = std::fma(-n, -1.4973849048591698e-33, r);
+  const double r2 = r * r;
+  const int q = (int)((long long)n & 3);
+  if (q & 1) {
+    const double c[8] = {2.8114572543455206e-15, -7.647163731819816e-13, 1.6059043836821613e-10,
+                         -2.505210838544172e-08,  2.7557319223985893e-06, -0.0001984126984126984,
+                         0.008333333333333333,    -0.16666666666666666};
+    double p = c[0];
+    for (int k = 1; k < 8; k++) p = std::fma(p, r2, c[k]);
+    const double sn = std::fma(r * r2, p, r);
+    return q == 1 ? -sn : sn;
+  }
+  const double c[9] = {-1.5619206968586225e-16, 4.779477332387385e-14, -1.1470745597729725e-11,
+                       2.08767569878681e-09,    -2.755731922398589e-07, 2.48015873015873e-05,
+                       -0.001388888888888889,   0.041666666666666664,   -0.5};
+  double p = c[0];
+  for (int k = 1; k < 9; k++) p = std::fma(p, r2, c[k]);
+  const double cs = std::fma(r2, p, 1.0);
+  return q == 0 ? cs : -cs;
+}
+
+// ------------------------------------------------------- astronomic constituents
+// The nodal factors of the tidal package the reference vendors (Delft3D
+// astro.f90): `update_nodal_factors` :5-96, `asc` :98-189, `hulpgr`
+// :482-643, `datumi` :646-748, `bewvuf` :750-910.  Per constituent: the
+// multipliers of v(1..7) (T, s, p, h, p1, xi, nu), the phase in quarter turns
+// (field 8), two extra u terms (+-index into v) and three (exponent, index
+// into f) nodal factor terms, for the constituents of `kompbs` :192-479 this
+// oracle carries.
+struct AstroRow {
+  const char* name;
+  int j[16];
+};
+static const AstroRow kAstro[] = {
+    {"SA", {0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"SSA", {0, 0, 0, 2, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"MSM", {0, 1, 1, -2, 0, 0, 0, 0, 0, 0, 1, 1, 0, 0, 0, 0}},
+    {"MM", {0, 1, -1, 0, 0, 0, 0, 0, 0, 0, 1, 1, 0, 0, 0, 0}},
+    {"MSF", {0, 2, 0, -2, 0, 0, 0, 0, 0, 0, 1, 1, 0, 0, 0, 0}},
+    {"MF", {0, 2, 0, 0, 0, -2, 0, 0, 0, 0, 1, 2, 0, 0, 0, 0}},
+    {"MFM", {0, 3, -1, 0, 0, -2, 0, 0, 0, 0, 1, 2, 0, 0, 0, 0}},
+    {"MSQM", {0, 4, 0, -2, 0, -2, 0, 0, 0, 0, 1, 2, 0, 0, 0, 0}},
+    {"MQM", {0, 4, -2, 0, 0, -2, 0, 0, 0, 0, 1, 2, 0, 0, 0, 0}},
+    {"2Q1", {1, -4, 2, 1, 0, 2, -1, 1, 0, 0, 1, 3, 0, 0, 0, 0}},
+    {"SIGMA1", {1, -4, 0, 3, 0, 2, -1, 1, 0, 0, 1, 3, 0, 0, 0, 0}},
+    {"Q1", {1, -3, 1, 1, 0, 2, -1, 1, 0, 0, 1, 3, 0, 0, 0, 0}},
+    {"RO1", {1, -3, -1, 3, 0, 2, -1, 1, 0, 0, 1, 3, 0, 0, 0, 0}},
+    {"O1", {1, -2, 0, 1, 0, 2, -1, 1, 0, 0, 1, 3, 0, 0, 0, 0}},
+    {"M1", {1, -1, 1, 1, 0, 0, -1, -1, -12, 0, 1, 21, 0, 0, 0, 0}},
+    {"NO1", {1, -1, 1, 1, 0, 0, -1, -1, 0, 0, 1, 3, 1, 6, 0, 0}},
+    {"PI1", {1, 0, 0, -2, 1, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"P1", {1, 0, 0, -1, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"S1", {1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"K1", {1, 0, 0, 1, 0, 0, 0, -1, -10, 0, 1, 19, 0, 0, 0, 0}},
+    {"PSI1", {1, 0, 0, 2, -1, 0, 0, -1, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"FI1", {1, 0, 0, 3, 0, 0, 0, -1, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"THETA1", {1, 1, 1, -1, 0, 0, -1, -1, 0, 0, 1, 4, 0, 0, 0, 0}},
+    {"J1", {1, 1, -1, 1, 0, 0, -1, -1, 0, 0, 1, 4, 0, 0, 0, 0}},
+    {"OO1", {1, 2, 0, 1, 0, -2, -1, -1, 0, 0, 1, 5, 0, 0, 0, 0}},
+    {"EPSILON2", {2, -5, 1, 4, 0, 2, -2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"2N2", {2, -4, 2, 2, 0, 2, -2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"MU2", {2, -4, 0, 4, 0, 2, -2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"N2", {2, -3, 1, 2, 0, 2, -2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"NU2", {2, -3, -1, 4, 0, 2, -2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"M2", {2, -2, 0, 2, 0, 2, -2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"MKS2", {2, -2, 0, 4, 0, 2, -2, 0, -11, 0, 1, 6, 1, 20, 0, 0}},
+    {"LABDA2", {2, -1, 1, 0, 0, 2, -2, 2, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"L2", {2, -1, -1, 2, 0, 2, -2, 2, -13, 0, 1, 22, 0, 0, 0, 0}},
+    {"T2", {2, 0, 0, -1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"S2", {2, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"R2", {2, 0, 0, 1, -1, 0, 0, 2, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"K2", {2, 0, 0, 2, 0, 0, 0, 0, -11, 0, 1, 20, 0, 0, 0, 0}},
+    {"MSN2", {2, 1, -1, 0, 0, 0, 0, 0, 0, 0, 2, 6, 0, 0, 0, 0}},
+    {"ETA2", {2, 1, -1, 2, 0, 0, -2, 0, 0, 0, 1, 7, 0, 0, 0, 0}},
+    {"2SM2", {2, 2, 0, -2, 0, -2, 2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"MO3", {3, -4, 0, 3, 0, 4, -3, 1, 0, 0, 1, 3, 1, 6, 0, 0}},
+    {"2MK3", {3, -4, 0, 3, 0, 4, -4, 1, 10, 0, 2, 6, 1, 19, 0, 0}},
+    {"M3", {3, -3, 0, 3, 0, 3, -3, 0, 0, 0, 1, 17, 0, 0, 0, 0}},
+    {"MK3", {3, -2, 0, 3, 0, 2, -2, -1, -10, 0, 1, 6, 1, 19, 0, 0}},
+    {"SK3", {3, 0, 0, 1, 0, 0, 0, -1, -10, 0, 1, 19, 0, 0, 0, 0}},
+    {"3MS4", {4, -6, 0, 6, 0, 6, -6, 0, 0, 0, 3, 6, 0, 0, 0, 0}},
+    {"MN4", {4, -5, 1, 4, 0, 4, -4, 0, 0, 0, 2, 6, 0, 0, 0, 0}},
+    {"M4", {4, -4, 0, 4, 0, 4, -4, 0, 0, 0, 2, 6, 0, 0, 0, 0}},
+    {"SN4", {4, -3, 1, 2, 0, 2, -2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"MS4", {4, -2, 0, 2, 0, 2, -2, 0, 0, 0, 1, 6, 0, 0, 0, 0}},
+    {"MK4", {4, -2, 0, 4, 0, 2, -2, 0, -11, 0, 1, 6, 1, 20, 0, 0}},
+    {"S4", {4, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {"SK4", {4, 0, 0, 2, 0, 0, 0, 0, -11, 0, 1, 20, 0, 0, 0, 0}},
+    {"2MN6", {6, -7, 1, 6, 0, 6, -6, 0, 0, 0, 3, 6, 0, 0, 0, 0}},
+    {"M6", {6, -6, 0, 6, 0, 6, -6, 0, 0, 0, 3, 6, 0, 0, 0, 0}},
+    {"2MS6", {6, -4, 0, 4, 0, 4, -4, 0, 0, 0, 2, 6, 0, 0, 0, 0}},
+    {"MSK6", {6, -2, 0, 4, 0, 2, -2, 0, -11, 0, 1, 6, 1, 20, 0, 0}},
+    {"M8", {8, -8, 0, 8, 0, 8, -8, 0, 0, 0, 4, 6, 0, 0, 0, 0}},
+};
+
+// Fortran SIGN(0.5d0, v) (negative zero counts as negative) and MOD for reals.
+static double fsign_half(double v) { return std::signbit(v) ? -0.5 : 0.5; }
+static double fpowi(double x, int n) {  // real**integer by binary powering (the Fortran runtime)
+  double r = 1.0;
+  for (unsigned u = (unsigned)n;;) {
+    if (u & 1u) r *= x;
+    u >>= 1;
+    if (u) x *= x;
+    else break;
+  }
+  return r;
+}
+
+// hulpgr (astro.f90:482-643): v(1..15), f(1..22) for year jaar and tm1 hours into it.
+static void astro_hulpgr(int jaar, double tm1, double* v, double* f) {
+  const double pix2 = 8.0 * std::atan(1.0), dhalf = 0.5, rad = pix2 / 360.0;
+  const double rjaar = (double)(float)(jaar - 1900);
+  const int ischrk = (int)((rjaar - 0.99) / 4.0) - (int)((rjaar - 0.99) / 100.0) + (int)((rjaar + 300.0 - 0.99) / 400.0);
+  const double tm3 = (double)(float)ischrk + tm1 / 24.0;
+  v[1] = (180.000 + 360.0000000 * tm3) * rad;
+  v[2] = (277.026 + 129.3848200 * rjaar + 13.176396800000 * tm3) * rad;
+  v[3] = (334.384 + 40.6624700 * rjaar + 0.111404000000 * tm3) * rad;
+  v[4] = (280.190 - 0.2387136 * rjaar + 0.985647360000 * tm3) * rad;
+  v[5] = (281.221 + 0.0171800 * rjaar + 0.000047064943 * tm3) * rad;
+  v[8] = (259.156 + 340.6718100 * rjaar - 0.052953945000 * tm3) * rad;
+  double z = 0.009415;
+  double p = std::atan(z * std::sin(v[8]) / (1.0 + z * (1.0 - std::cos(v[8]))));
+  z = -0.17794;
+  const double q = std::atan(z * std::sin(v[8]) / (1.0 + z * (1.0 - std::cos(v[8]))));
+  v[6] = -p - q;
+  v[7] = p - q;
+  double rk = 0.9137 - 0.03569 * std::cos(v[8]);
+  const double ri = std::atan(std::sqrt(1.0 - rk * rk) / rk);
+  v[9] = ri;
+  p = std::fmod(v[3], pix2) - pix2 * (fsign_half(v[3]) - dhalf);
+  rk = v[6];
+  const double rn1 = v[7];
+  const double s2ri = std::sin(2.0 * ri), sri = std::sin(ri), si = std::sin(0.5 * ri), cri = std::cos(ri),
+               ci = std::cos(0.5 * ri);
+  v[10] = std::atan(s2ri * std::sin(rn1) / (s2ri * std::cos(rn1) + 0.3347));
+  v[11] = std::atan(sri * sri * std::sin(2.0 * rn1) / (sri * sri * std::cos(2.0 * rn1) + 0.0727));
+  v[12] = std::atan(std::sin(2.0 * (p - rk)) / (3.0 * cri / (ci * ci) + std::cos(2.0 * (p - rk))));
+  v[13] = std::atan(std::sin(2.0 * (p - rk)) / (ci * ci / (si * si * 6.0) - std::cos(2.0 * (p - rk))));
+  v[14] = 3.0 * v[10];
+  v[15] = 0.0;
+  for (int j = 1; j <= 15; j++) v[j] = std::fmod(v[j], pix2) - pix2 * (fsign_half(v[j]) - dhalf);
+  const double ci4 = ci * ci * ci * ci, si4 = si * si * si * si, sri3 = sri * sri * sri;
+  f[1] = (2.0 / 3.0 - sri * sri) / 0.5021;
+  f[2] = sri * sri / 0.1578;
+  f[3] = sri * ci * ci / 0.38;
+  f[4] = s2ri / 0.7214;
+  f[5] = sri * si * si / 0.0164;
+  f[6] = ci4 / 0.9154;
+  f[7] = sri * sri / 0.1565;
+  f[8] = si4 / 0.0017;
+  f[9] = (sri - 1.25 * sri3) / 0.3192;
+  f[10] = sri3 / 0.063;
+  f[11] = sri * sri * ci * ci / 0.1518;
+  f[12] = (1.0 - 10.0 * si * si + 15.0 * si4) * ci * ci / 0.5873;
+  f[13] = (1.0 - 10.0 * ci * ci + 15.0 * ci4) * si * si / 0.2147;
+  f[14] = sri * ci4 / 0.3658;
+  f[15] = (ci * ci - 2.0 / 3.0) * sri * ci * ci / 0.1114;
+  f[16] = (ci * ci - 1.0 / 3.0) * sri * si * si / 0.0103;
+  f[17] = ci4 * ci * ci / 0.8758;
+  f[18] = ci4 * si * si / 0.038;
+  f[19] = std::sqrt(0.8965 * s2ri * s2ri + 0.6001 * s2ri * std::cos(rn1) + 0.1006);
+  f[20] = std::sqrt(19.0444 * sri3 * sri + 2.7702 * sri * sri * std::cos(2.0 * rn1) + 0.0981);
+  f[21] = 6.0 * cri * std::cos(2.0 * (p - rk)) / (ci * ci) + 9.0 * cri * cri / (ci4);
+  f[21] = 2.6316 * sri * ci * ci * 0.5 * std::sqrt(1.0 + f[21]);
+  f[22] = 36.0 * si4 / (ci4) - 12.0 * si * si / (ci * ci) * std::cos(2.0 * (p - rk));
+  f[22] = 1.0924 * ci4 * std::sqrt(1.0 + f[22]);
+}
+
+// bewvuf (astro.f90:750-910) for one constituent: w (rad/h), v0u (rad), fr.
+static bool astro_bewvuf(const std::string& name, const double* v, const double* f, double& w, double& v0u,
+                         double& fr) {
+  const double pix2 = 8.0 * std::atan(1.0), dhalf = 0.5;
+  for (const auto& row : kAstro) {
+    if (name != row.name) continue;
+    const int* jn = row.j;
+    w = (double)jn[0] * 15.0 + (double)jn[1] * 0.54901653 + (double)jn[2] * 0.0046418333 +
+        (double)jn[3] * 0.04106864 + (double)jn[4] * 0.0000019610393;
+    w = (w * pix2) / 360.0;
+    v0u = ((double)jn[7] * pix2) / 4.0;
+    for (int kw = 1; kw <= 7; kw++) v0u = v0u + v[kw] * (double)jn[kw - 1];
+    const int ie1 = jn[8];
+    if (ie1 != 0) {
+      const int ia1 = std::abs(ie1);
+      v0u = v0u + (double)(float)(ie1 / ia1) * v[ia1];
+      const int ie2 = jn[9];
+      if (ie2 != 0) {
+        const int ia2 = std::abs(ie2);
+        v0u = v0u + (double)(float)(ie2 / ia2) * v[ia2];
+      }
+    }
+    v0u = std::fmod(v0u, pix2) - pix2 * (fsign_half(v0u) - dhalf);
+    fr = 1.0;
+    if (jn[10] != 0) {
+      fr = fpowi(f[jn[11]], jn[10]);
+      if (jn[12] != 0) {
+        fr = fr * fpowi(f[jn[13]], jn[12]);
+        if (jn[14] != 0) fr = fr * fpowi(f[jn[15]], jn[14]);
+      }
+    }
+    return true;
+  }
+  return false;
+}
+
 template <class X>
 struct F2 {  // (n1, n2) column-major, 1-based
   std::vector<X> v;
@@ -352,6 +567,12 @@ struct Model {
   F1<int32_t> index_zsi_bdr, index_bdr_gbp;
   std::string bdrfile;
   F2<float> zs_bnd;
+  // astronomic constituents (sfincs_boundaries.f90:289-450; sfincs_data.f90:672-674)
+  bool use_bcafile = true;
+  long nr_tidal_components = 0;
+  std::vector<double> tidal_component_frequency;      // [ic-1], rad/s
+  std::vector<double> tidal_amp, tidal_phase;         // [(ib-1) * nc + ic-1]
+  std::vector<std::string> tidal_component_names;
 
   // --- meteo, infiltration, sources
   long ntwnd = 0, itwndlast = 1, ntprcp = 0, itprcplast = 1;
@@ -511,6 +732,7 @@ struct Model {
     bdrfile = in.str("bdrfile", "none");
     bzsfile = in.str("bzsfile", "none");
     bcafile = in.str("bcafile", "none");
+    use_bcafile = in.logical("use_bcafile", true);
     bzifile = in.str("bzifile", "none");
     srcfile = in.str("srcfile", "none");
     disfile = in.str("disfile", "none");
@@ -1685,6 +1907,8 @@ struct Model {
       t_bnd(1) = t0;
       t_bnd(2) = t1;
     }
+    nr_tidal_components = 0;
+    if (bcafile.substr(0, 4) != "none" && nbnd > 0 && use_bcafile) read_bca();
     // downstream river points: x, y, internal x, y, slope, distance per line (:217-270)
     nbdr = 0;
     if (downstream_river_boundaries_in_mask) {
@@ -2777,6 +3001,127 @@ struct Model {
     }
   }
 
+  // The bca file (sfincs_boundaries.f90:289-450): two passes over the lines,
+  // cleaned as clean_line (:1242-1252) does; then update_nodal_factors at the
+  // date of tref (astro.f90:5-96, time_to_vector sfincs_date.f90:329-364,
+  // datumi astro.f90:646-748).  Inputs the reference would index outside its
+  // arrays with are refused.
+  void read_bca() {
+    std::ifstream in(path(bcafile));
+    if (!in) throw std::runtime_error("oracle: cannot open " + bcafile);
+    std::vector<std::string> lines;
+    for (std::string l; std::getline(in, l);) {
+      const size_t cr = l.find('\r');
+      if (cr != std::string::npos) l = l.substr(0, cr);
+      const size_t a = l.find_first_not_of(' ');
+      l = a == std::string::npos ? std::string() : l.substr(a);
+      while (!l.empty() && (l.back() == ' ' || l.back() == '\t')) l.pop_back();
+      lines.push_back(l);
+    }
+    auto meta = [](const std::string& l) {
+      for (const char* k : {"Quantity", "Unit", "Name", "Function", "quantity", "unit", "name", "function"})
+        if (l.find(k) != std::string::npos) return true;
+      return false;
+    };
+    auto data = [](const std::string& l, std::string& cname, float& a, float& p) {
+      std::string t = l;
+      for (char& c : t)
+        if (c == ',' || c == '\t') c = ' ';
+      std::istringstream is(t);
+      std::string sa, sp;
+      if (!(is >> cname >> sa >> sp)) return false;
+      char* e;
+      a = std::strtof(sa.c_str(), &e);
+      if (e == sa.c_str() || *e) return false;
+      p = std::strtof(sp.c_str(), &e);
+      if (e == sp.c_str() || *e) return false;
+      return true;
+    };
+    long n_sets = 0, n_components = 0;
+    bool has_a0 = false;
+    for (const auto& l : lines) {
+      std::string cname;
+      float a, p;
+      if (l == "[forcing]" || l == "[Forcing]") n_sets++;
+      else if (meta(l)) continue;
+      else if (data(l, cname, a, p)) {
+        if (n_sets == 0) throw std::runtime_error("oracle: bca data before the first [forcing]");
+        if (n_sets == 1) {
+          n_components++;
+          if (n_components == 1 && (cname.compare(0, 2, "a0") == 0 || cname.compare(0, 2, "A0") == 0)) has_a0 = true;
+        }
+      }
+    }
+    if (n_sets != nbnd) throw std::runtime_error("oracle: bca sets do not match the bnd points");
+    if (!has_a0) n_components++;
+    const long nc = n_components;
+    nr_tidal_components = nc;
+    tidal_component_names.assign(nc, "");
+    tidal_amp.assign((size_t)nc * nbnd, 0.0);
+    tidal_phase.assign((size_t)nc * nbnd, 0.0);
+    long current_set = 0, current_component = 0;
+    for (const auto& l : lines) {
+      std::string cname;
+      float a, p;
+      if (l == "[forcing]" || l == "[Forcing]") {
+        current_set++;
+        current_component = 0;
+        if (!has_a0) {
+          current_component = 1;
+          tidal_component_names[0] = "A0";
+        }
+      } else if (meta(l)) {
+        continue;
+      } else if (data(l, cname, a, p)) {
+        current_component++;
+        if (current_component > nc) throw std::runtime_error("oracle: bca set longer than the first");
+        tidal_component_names[current_component - 1] = cname;
+        tidal_amp[(size_t)(current_set - 1) * nc + current_component - 1] = (double)a;
+        tidal_phase[(size_t)(current_set - 1) * nc + current_component - 1] = (double)p;
+      }
+    }
+    // time_to_vector(0, tref): the time of day through real*4 fractions
+    const int yyyy = std::atoi(trefstr.substr(0, 4).c_str()), mm = std::atoi(trefstr.substr(4, 2).c_str()),
+              dd = std::atoi(trefstr.substr(6, 2).c_str()), hh = std::atoi(trefstr.substr(9, 2).c_str()),
+              mn = std::atoi(trefstr.substr(11, 2).c_str()), ss = std::atoi(trefstr.substr(13, 2).c_str());
+    const float ref_fraction = (float)hh / 24 + (float)mn / 1440 + (float)ss / 86400;
+    const float sec_add = (float)((double)(ref_fraction * 86400) + 0.0);
+    const int ndays_add = (int)(sec_add / 86400);
+    if (ndays_add != 0) throw std::runtime_error("oracle: tref time of day out of range");
+    const float secs_time = sec_add - (float)ndays_add * 86400.0f;
+    const int h = (int)(secs_time / 3600);
+    const int mi = (int)((secs_time - (float)(h * 3600)) / 60);
+    const int se = (int)(secs_time - (float)(h * 3600) - (float)(mi * 60));
+    // datumi: hours into the year
+    double rmd[13] = {0, 0, 31, 59, 90, 120, 151, 181, 212, 243, 273, 304, 334};
+    if (yyyy % 4 == 0 && (yyyy % 100 != 0 || yyyy % 400 == 0))
+      for (int i = 3; i <= 12; i++) rmd[i] += 1.0;
+    const double thours = rmd[mm] * 24.0 + (double)(float)(dd - 1) * 24.0 + (double)(float)h +
+                          (double)(float)mi / 60.0 + (double)(float)se / 3600.0;
+    double v[16] = {0}, f[26] = {0};
+    astro_hulpgr(yyyy, thours, v, f);
+    const double pi = (double)(4.0f * std::atan(1.0f));  // 4 * atan(1.0): single precision
+    tidal_component_frequency.assign(nc, 0.0);         // A0: left unset by the reference, 0 here
+    for (long k = 2; k <= nc; k++) {
+      std::string nm = tidal_component_names[k - 1];
+      if (nm == "EPS2") nm = "EPSILON2";
+      if (nm == "LA2") nm = "LABDA2";
+      if (nm == "MTM") nm = "MFM";
+      double w, v0u, fr;
+      if (!astro_bewvuf(nm, v, f, w, v0u, fr)) throw std::runtime_error("oracle: constituent " + nm + " not carried");
+      tidal_component_frequency[k - 1] = w / 3600;
+      for (long n = 1; n <= nbnd; n++) {
+        double& A = tidal_amp[(size_t)(n - 1) * nc + k - 1];
+        double& P = tidal_phase[(size_t)(n - 1) * nc + k - 1];
+        A = A * fr;
+        P = (pi / 180) * P - v0u;
+        double r = std::fmod(P, 2 * pi);  // MODULO(P, 2 pi)
+        if (r != 0.0 && r < 0.0) r = r + 2 * pi;
+        P = r;
+      }
+    }
+  }
+
   // update_boundary_points: sfincs_boundaries.f90:682-758
   void update_boundary_points(double tt) {
     if (nbnd == 0) return;
@@ -2802,8 +3147,16 @@ struct Model {
       }
     }
     float tbfac = (tb - t_bnd(itb0)) / std::max(t_bnd(itb1) - t_bnd(itb0), 1.0e-6f);
-    for (long ib = 1; ib <= nbnd; ib++)
-      zst_bnd(ib) = zs_bnd(ib, itb0) + (zs_bnd(ib, itb1) - zs_bnd(ib, itb0)) * tbfac;
+    const bool core = std::is_same<TZ, float>::value;
+    for (long ib = 1; ib <= nbnd; ib++) {
+      float zstb = zs_bnd(ib, itb0) + (zs_bnd(ib, itb1) - zs_bnd(ib, itb0)) * tbfac;
+      const long nc = nr_tidal_components;
+      for (long ic = 1; ic <= nc; ic++) {  // astronomic tides (:736-744)
+        const double arg = tidal_component_frequency[ic - 1] * tt - tidal_phase[(size_t)(ib - 1) * nc + ic - 1];
+        zstb = (float)((double)zstb + tidal_amp[(size_t)(ib - 1) * nc + ic - 1] * (core ? core_cos(arg) : std::cos(arg)));
+      }
+      zst_bnd(ib) = zstb;
+    }
   }
 
   // update_boundary_conditions: sfincs_boundaries.f90:761-921
@@ -3514,6 +3867,7 @@ const char* oracle_last_error() { return g_last_error.c_str(); }
 
 // The core's arctangent (IEEE operations only), for its accuracy test.
 float oracle_core_atan2(float y, float x) { return core_atan2(y, x); }
+double oracle_core_cos(double x) { return core_cos(x); }
 
 void oracle_destroy(void* hv) {
   auto* h = static_cast<Handle*>(hv);
@@ -3624,6 +3978,13 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
         out[4 * (i - 1) + 2] = m.structure_parameters(2, i);
         out[4 * (i - 1) + 3] = m.structure_length(i);
       }
+    }
+    else if (s == "tide_omega" || s == "tide_amp" || s == "tide_phase") {
+      // astronomic constituents after the nodal correction: per constituent, or per point and constituent
+      const std::vector<double>& src =
+          s == "tide_omega" ? m.tidal_component_frequency : (s == "tide_amp" ? m.tidal_amp : m.tidal_phase);
+      if ((long)src.size() != n) return -1;
+      for (long i = 0; i < n; i++) out[i] = src[(size_t)i];
     }
     else if (s == "kb_cell" || s == "kb_dir" || s == "kb_sign") {
       // water-level boundary faces (kcuv==2/6 list without lateral Neumann faces), reference order

@@ -1033,6 +1033,12 @@ int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst
         for (double v : {h.p.quadtree ? (double)w.face : (double)h.dense2cmp[w.face], (double)w.dir, (double)w.height,
                          (double)w.cd, (double)w.len})
           out.push_back(v);
+    } else if (nm == "tide_omega") {
+      out.assign(h.tide.omega.begin(), h.tide.omega.end());
+    } else if (nm == "tide_amp") {
+      out.assign(h.tide.amp.begin(), h.tide.amp.end());
+    } else if (nm == "tide_phase") {
+      out.assign(h.tide.phase.begin(), h.tide.phase.end());
     } else if (nm == "gb_cell") {
       for (auto c : h.gb_cmp) out.push_back((double)c);
     } else if (nm == "kb_cell") {

@@ -156,6 +156,10 @@ void read_boundary_series(HostModel& h, const Keys& k, bool water_level_bnd, std
   }
   P.nbnd = nbnd;
   P.ntbnd = ntbnd;
+  // astronomic constituents of the boundary points, nodal-corrected at tref (sfincs_boundaries.f90:289-450)
+  h.tide = TideHost{};
+  if (!is_none(k.bcafile) && nbnd > 0) read_bca_file(path(k.bcafile), h.tref, nbnd, h.tide);
+  P.ntide = h.tide.ncomp;
 }
 
 // Uniform wind and rain time series and the wind drag table (sfincs_meteo.f90:247-327).
@@ -304,7 +308,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   std::string prcpfile = in.str("prcfile", "none");
   if (is_none(prcpfile)) prcpfile = in.str("precipfile", "none");
   // Inputs outside this core's path: refuse loudly instead of silently ignoring physics.
-  for (const char* k : {"bcafile", "bzifile", "volfile", "netbndbzsbzifile", "netsrcdisfile",
+  for (const char* k : {"bzifile", "volfile", "netbndbzsbzifile", "netsrcdisfile",
                         "netamuamvfile", "netamprfile", "netampfile", "netspwfile", "infiltration_file",
                         "wavemaker_wvmfile", "wvmfile"}) {
     if (!is_none(in.str(k, "none"))) throw std::runtime_error(std::string("input '") + k + "' is not supported by this core");
@@ -482,6 +486,8 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   k.qinffile = qinffile; k.prcpfile = prcpfile; k.quadtree = quadtree; k.thdfile = thdfile; k.weirfile = weirfile; k.drnfile = drnfile; k.rstfile = rstfile;
   k.inifile = inifile;
   k.bdrfile = in.str("bdrfile", "none");
+  // astronomic constituents apply when use_bcafile (default on) and a bca file is given (sfincs_input.f90:199, 231)
+  k.bcafile = in.logical("use_bcafile", true) ? in.str("bcafile", "none") : std::string("none");
   k.scsfile = in.str("scsfile", "none");
   k.smaxfile = in.str("smaxfile", "none");
   k.sefffile = in.str("sefffile", "none");
@@ -1620,6 +1626,9 @@ static void place_model(const HostModel& h, ScnDev& d, int32_t*& cmp, int32_t*& 
   }
   up(d.t_bnd, h.t_bnd);
   up(d.zs_bnd, h.zs_bnd);
+  up(d.tide_w, h.tide.omega);
+  up(d.tide_amp, h.tide.amp);
+  up(d.tide_pha, h.tide.phase);
   zero(d.zst_bnd, (size_t)std::max(h.p.nbnd, 1));
   up(d.bfaces, h.bfaces);
   if (h.uvmean0.empty())

@@ -57,6 +57,18 @@ struct OutputSpec {
 };
 
 // Everything read from a model directory and laid out densely on the host.
+// Astronomic boundary constituents after the nodal correction at tref: per
+// constituent its frequency (rad/s), per point and constituent the amplitude
+// times the nodal factor and the phase less V0+u (rad, in [0, 2 pi)); the first
+// constituent is A0 (frequency 0).
+struct TideHost {
+  int ncomp = 0;
+  std::vector<std::string> names;
+  std::vector<double> omega;       // [ncomp]
+  std::vector<double> amp, phase;  // [nbnd][ncomp]
+};
+void read_bca_file(const std::string& file, const std::string& tref, int nbnd, TideHost& out);
+
 struct HostModel {
   std::string dir;
   ScnDev p{};  // scalar parameters (pointer fields unused on the host copy)
@@ -90,6 +102,7 @@ struct HostModel {
   std::vector<int32_t> gb_cmp;         // compact index of every boundary cell (diagnostics)
   // forcing series
   std::vector<float> t_bnd, zs_bnd;  // zs_bnd [ntbnd][nbnd]
+  TideHost tide;                     // astronomic constituents of the boundary points (bca file)
   std::vector<float> tprcp, vprcp, twnd, wmag, wdir, cdval;
   std::vector<float> x73;            // hu**(7/3) table when h73table is on (sfincs_data.f90:858-881)
   MeteoGridHost mgh[3];              // gridded meteo: 0 wind (amu, amv), 1 pressure (amp), 2 rain (ampr)
@@ -151,6 +164,7 @@ struct Keys {
   std::string thdfile, weirfile, drnfile, rstfile;  // thin dams, weirs, drainage structures, restart (regular grids)
   std::string inifile;                              // binary initial water levels (real*4, cell order)
   std::string bdrfile;                              // downstream river points
+  std::string bcafile;                              // astronomic boundary constituents (when use_bcafile)
   // infiltration parameter files (binary real*4, cell order)
   std::string scsfile, smaxfile, sefffile, ksfile, psifile, sigmafile, f0file, fcfile, kdfile;
   std::string qtrfile, depfile, mskfile, indexfile, sbgfile, manningfile, bndfile, bzsfile, srcfile, disfile,

@@ -402,8 +402,12 @@ __device__ __forceinline__ double boundary_item(const ScnDev& S, const StepPlan&
         pre.z01[3] = z1[j2];
       }
       // levels at the two boundary points (:728-756), then the face's weighted level
-      const float zp1 = pre.z01[0] + (pre.z01[1] - pre.z01[0]) * P.tbfac;
-      const float zp2 = pre.z01[2] + (pre.z01[3] - pre.z01[2]) * P.tbfac;
+      float zp1 = pre.z01[0] + (pre.z01[1] - pre.z01[0]) * P.tbfac;
+      float zp2 = pre.z01[2] + (pre.z01[3] - pre.z01[2]) * P.tbfac;
+      if (S.ntide > 0) {  // astronomic constituents (:736-744)
+        zp1 = tide_level(S, (b.info & 8) ? b.i1 : 0, t, zp1);
+        if (b.info & 8) zp2 = tide_level(S, b.i2, t, zp2);
+      }
       double zst;
       if (b.info & 8)
         zst = (double)(zp1 * b.fac + zp2 * (1.0f - b.fac));

@@ -242,6 +242,10 @@ struct ScnDev {
   const float* t_bnd;    // [ntbnd]
   const float* zs_bnd;   // [ntbnd][nbnd]
   float* zst_bnd;        // [nbnd] levels at the boundary points for the current step
+  int ntide;             // astronomic constituents per boundary point (0: none; the first is A0)
+  const double* tide_w;  // [ntide] frequency (rad/s)
+  const double* tide_amp;  // [nbnd][ntide] amplitude times nodal factor
+  const double* tide_pha;  // [nbnd][ntide] phase less V0+u (rad)
   const BndFace* bfaces; // [nkcuv2]
   float* uvmean;         // [nkcuv2]
   const int2* neu;       // [nneu] Neumann (kcs 6) cell and its interior cell (dense offsets)
@@ -451,6 +455,56 @@ __device__ __forceinline__ float cell_rain(const ScnDev& S, int64_t c, const Met
 // of the model with state, else the constant / c2d rate on a wet cell.
 __device__ __forceinline__ void store_qinfmap(const ScnDev& S, int64_t c, bool inf_cell, float qinf_cell, bool wet) {
   S.qinfmap[c] = inf_cell ? qinf_cell : ((S.infiltration && wet) ? S.qinf[c] : 0.0f);
+}
+
+// Cosine in FP64 from IEEE operations only, so that the oracle reproduces it
+// bit for bit: n = rint(x 2/pi); r = x - n pi/2 with pi/2 split in three
+// doubles (Cody and Waite, each product fused with its subtraction), so r is
+// within an ulp for |n| far beyond any tidal argument; then the Taylor series
+// of sin (to degree 17) or cos (to degree 18) of r in [-pi/4, pi/4], in Horner
+// form, by the quadrant n mod 4.  Truncation stays below 1e-19.
+__device__ __forceinline__ double cos_ieee(double x) {
+  const double n = rint(__dmul_rn(x, 0.6366197723675814));
+  double r = __fma_rn(-n, 1.5707963267948966, x);
+  r = __fma_rn(-n, 6.123233995736766e-17, r);
+  r = __fma_rn(-n, -1.4973849048591698e-33, r);
+  const double r2 = __dmul_rn(r, r);
+  const int q = (int)((long long)n & 3);
+  if (q & 1) {  // +-sin(r)
+    double p = 2.8114572543455206e-15;
+    p = __fma_rn(p, r2, -7.647163731819816e-13);
+    p = __fma_rn(p, r2, 1.6059043836821613e-10);
+    p = __fma_rn(p, r2, -2.505210838544172e-08);
+    p = __fma_rn(p, r2, 2.7557319223985893e-06);
+    p = __fma_rn(p, r2, -0.0001984126984126984);
+    p = __fma_rn(p, r2, 0.008333333333333333);
+    p = __fma_rn(p, r2, -0.16666666666666666);
+    const double sn = __fma_rn(__dmul_rn(r, r2), p, r);
+    return q == 1 ? -sn : sn;
+  }
+  double p = -1.5619206968586225e-16;
+  p = __fma_rn(p, r2, 4.779477332387385e-14);
+  p = __fma_rn(p, r2, -1.1470745597729725e-11);
+  p = __fma_rn(p, r2, 2.08767569878681e-09);
+  p = __fma_rn(p, r2, -2.755731922398589e-07);
+  p = __fma_rn(p, r2, 2.48015873015873e-05);
+  p = __fma_rn(p, r2, -0.001388888888888889);
+  p = __fma_rn(p, r2, 0.041666666666666664);
+  p = __fma_rn(p, r2, -0.5);
+  const double cs = __fma_rn(r2, p, 1.0);
+  return q == 0 ? cs : -cs;
+}
+
+// Level of boundary point ib with its astronomic constituents added one by one
+// in FP64, each sum rounded to the point's real*4 level (sfincs_boundaries.f90:736-744).
+__device__ __forceinline__ float tide_level(const ScnDev& S, int ib, double t, float z) {
+  const double* a = S.tide_amp + (size_t)ib * S.ntide;
+  const double* ph = S.tide_pha + (size_t)ib * S.ntide;
+  for (int c = 0; c < S.ntide; c++) {
+    const double arg = __dsub_rn(__dmul_rn(S.tide_w[c], t), ph[c]);
+    z = (float)__dadd_rn((double)z, __dmul_rn(a[c], cos_ieee(arg)));
+  }
+  return z;
 }
 
 // Four-quadrant arctangent from IEEE operations only, so that the oracle
