@@ -181,6 +181,30 @@ def test_quadtree_stepwise_matches_f32_oracle(tmp_path, subgrid, extra):
         assert abs(sg["t"] - so["t"]) <= 1e-6 * max(1.0, abs(so["t"]))
 
 
+@pytest.mark.parametrize("subgrid", [False, True])
+def test_quadtree_weirs_long_run(tmp_path, subgrid):
+    """Past the free/submerged switches: over 600 steps the weir faces keep
+    the FP64 volume balance, and the levels stay with the oracle's within a
+    bar that a dropped or doubled weir flux would exceed."""
+    d, _ = _write(tmp_path, subgrid, tstop=7200.0)
+    _add_weirs(d)
+    o = _oracle(d, "f32")
+    g = Model(d)
+    v0 = g.volume()
+    for n in (200, 200, 200):
+        o.update(-1000.0, n)
+        g.step(n)
+        s = g.scalars()
+        dz = np.abs(g.get("zs") - o.get("zs"))
+        print(f"weirs subgrid={subgrid} nt {s['nt']:.0f}: mean|dzs| {dz.mean():.3g} max|dzs| {dz.max():.3g}")
+        assert s["nt"] == o.scalars()["nt"]
+        assert float(dz.mean()) <= 2e-3 and float(dz.max()) <= 0.1
+    v1 = g.volume()
+    src = s["bflux_vol"] + s["rain_vol"] + s["src_vol"]
+    assert abs((v1 - v0) - src) / max(abs(v1), 1.0) <= 1e-6, (v1 - v0, src)
+    g.close()
+
+
 def test_quadtree_lake_at_rest(tmp_path):
     m = qtsynth.quadtree_coastal(nmax1=8, mmax1=10, dx1=400.0, nlev=3, bands=(1000.0, 500.0), P=4, seed=21,
                                  tstop=1800.0, subgrid=False, wind_speed=0.0)
