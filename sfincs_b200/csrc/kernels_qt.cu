@@ -31,11 +31,32 @@ __device__ __forceinline__ float qt_warp_max(float v) {
 // MET: gridded wind or pressure fields (a separate instance, so that the
 // plain path keeps its register allocation)
 template <bool SG, bool MET>
-__global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
-  pdl_wait();  // the previous kernel of the step has completed
-  pdl_trigger();
+__global__ void __launch_bounds__(256, 4) k_qt_momentum(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
+  // The point's static inputs (its record, its table bounds) are read before
+  // the wait for the previous kernel; after it, every load that depends only
+  // on the record (both cell levels, the neighbours' fluxes and velocities,
+  // the dry flags) is issued before the wet test, so that a wet point waits
+  // for two rounds of loads (these, then its table record) instead of four.
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
+  const int i = tl.n0 + (int)threadIdx.x;
+  const bool mine = (int)threadIdx.x < tl.m0;
+  FaceQ f{};
+  float2 zr = make_float2(0.0f, 0.0f);
+  float4 wz = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float zbmx = 0.0f, gn2 = 0.0f;
+  if (mine) {
+    f = S.qface[i];
+    if (SG) {
+      zr = S.sgz_u[i];
+      wz = S.sgw_u[i];
+    } else {
+      zbmx = S.zbmx[i];
+      gn2 = S.gn2[i];
+    }
+  }
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
   StepState& st = *S.st;
   if (!st.run) return;
   const StepVals sv = step_vals(st);
@@ -45,97 +66,88 @@ __global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ 
   float* q1 = S.qu[p ^ 1];
   float* uv1 = S.uu[p ^ 1];
   float den = 0.0f;
-  const int i = tl.n0 + (int)threadIdx.x;
-  if ((int)threadIdx.x < tl.m0) {
-    const FaceQ f = S.qface[i];
-    if (f.info & QF_ACT) {
-      const float zs_nm = S.zs[f.nm], zs_nmu = S.zs[f.nmu];
-      const float zsu = fmaxf(zs_nm, zs_nmu);
-      float zmin = 0.0f, zmax = 0.0f;
-      bool wet;
+  if (mine && (f.info & QF_ACT)) {
+    uint8_t* kfuv = S.kf[0];
+    const float zs_nm = S.zs[f.nm], zs_nmu = S.zs[f.nmu];
+    const uint8_t kf = kfuv[i];
+    FaceV a{};
+    a.qx_nm = q0[i];
+    if (S.advection || S.coriolis || S.viscosity || S.friction2d || S.thetasmooth) {
+      a.qx_nmd = q0[f.u_nmd];
+      a.qx_nmu = q0[f.u_nmu];
+      a.qy_nm = q0[f.v_nm];
+      a.qy_nmu = q0[f.v_nmu];
+      a.qy_ndm = q0[f.v_ndm];
+      a.qy_ndmu = q0[f.v_ndmu];
+      a.uu_nm = uv0[i];
+      a.uu_nmd = uv0[f.u_nmd];
+      a.uu_nmu = uv0[f.u_nmu];
+      a.uu_ndm = uv0[f.u_ndm];
+      a.uu_num = uv0[f.u_num];
+      a.vu = (uv0[f.v_ndm] + uv0[f.v_ndmu] + uv0[f.v_nm] + uv0[f.v_nmu]) / 4.0f;
+    }
+    bool dry0, dry1;
+    float zd0 = 0.0f, zd1 = 0.0f;
+    if (SG) {
+      dry0 = S.vneg[f.nm] != 0;
+      dry1 = S.vneg[f.nmu] != 0;
+      if (S.wiggle) {
+        zd0 = S.zsderv[f.nm];
+        zd1 = S.zsderv[f.nmu];
+      }
+    } else {
+      dry0 = zs_nm < S.zb[f.nm];
+      dry1 = zs_nmu < S.zb[f.nmu];
+    }
+    const float zsu = fmaxf(zs_nm, zs_nmu);
+    const bool wet = SG ? zsu > zr.x + S.huthresh : zsu > zbmx;
+    if (wet) {
+      const int L = (int)((f.info >> 8) & 15u);
+      const int dir = (f.info & QF_DIR) ? 1 : 0;
+      FaceGeo geo;
+      if (!(f.info & QF_TRANS)) {
+        geo.dxuvinv = dir == 0 ? S.lv_dxrinv[L] : S.lv_dyrinv[L];
+        geo.dyuvinv = dir == 0 ? S.lv_dyrinv[L] : S.lv_dxrinv[L];
+        geo.dxuv2inv = dir == 0 ? S.lv_dxr2inv[L] : S.lv_dyr2inv[L];
+        geo.dyuv2inv = dir == 0 ? S.lv_dyr2inv[L] : S.lv_dxr2inv[L];
+        geo.nuvisc = S.lv_nuvisc[L];
+      } else {  // refinement transition: 1.5 cell spacing, no viscosity across (dxuv2inv = 0)
+        geo.dxuvinv = dir == 0 ? S.lv_dxrinvc[L] : S.lv_dyrinvc[L];
+        geo.dyuvinv = dir == 0 ? S.lv_dyrinv[L] : S.lv_dxrinv[L];
+        geo.dxuv2inv = 0.0f;
+        geo.dyuv2inv = dir == 0 ? S.lv_dyr2inv[L] : S.lv_dxr2inv[L];
+        geo.nuvisc = S.lv_nuvisc_t[L];
+      }
+      geo.fcorio = S.fcorio;
+      float hu, gnavg2, phi = 1.0f;
       if (SG) {
-        const float2 z = S.sgz_u[i];
-        zmin = z.x;
-        zmax = z.y;
-        wet = zsu > zmin + S.huthresh;
-      } else {
-        wet = zsu > S.zbmx[i];
-      }
-      uint8_t* kfuv = S.kf[0];
-      if (wet) {
-        const int L = (int)((f.info >> 8) & 15u);
-        const int dir = (f.info & QF_DIR) ? 1 : 0;
-        FaceGeo geo;
-        if (!(f.info & QF_TRANS)) {
-          geo.dxuvinv = dir == 0 ? S.lv_dxrinv[L] : S.lv_dyrinv[L];
-          geo.dyuvinv = dir == 0 ? S.lv_dyrinv[L] : S.lv_dxrinv[L];
-          geo.dxuv2inv = dir == 0 ? S.lv_dxr2inv[L] : S.lv_dyr2inv[L];
-          geo.dyuv2inv = dir == 0 ? S.lv_dyr2inv[L] : S.lv_dxr2inv[L];
-          geo.nuvisc = S.lv_nuvisc[L];
-        } else {  // refinement transition: 1.5 cell spacing, no viscosity across (dxuv2inv = 0)
-          geo.dxuvinv = dir == 0 ? S.lv_dxrinvc[L] : S.lv_dyrinvc[L];
-          geo.dyuvinv = dir == 0 ? S.lv_dyrinv[L] : S.lv_dxrinv[L];
-          geo.dxuv2inv = 0.0f;
-          geo.dyuv2inv = dir == 0 ? S.lv_dyr2inv[L] : S.lv_dxr2inv[L];
-          geo.nuvisc = S.lv_nuvisc_t[L];
-        }
-        geo.fcorio = S.fcorio;
-        FaceV a{};
-        a.qx_nm = q0[i];
-        if (S.advection || S.coriolis || S.viscosity || S.friction2d || S.thetasmooth) {
-          a.qx_nmd = q0[f.u_nmd];
-          a.qx_nmu = q0[f.u_nmu];
-          a.qy_nm = q0[f.v_nm];
-          a.qy_nmu = q0[f.v_nmu];
-          a.qy_ndm = q0[f.v_ndm];
-          a.qy_ndmu = q0[f.v_ndmu];
-          a.uu_nm = uv0[i];
-          a.uu_nmd = uv0[f.u_nmd];
-          a.uu_nmu = uv0[f.u_nmu];
-          a.uu_ndm = uv0[f.u_ndm];
-          a.uu_num = uv0[f.u_num];
-          a.vu = (uv0[f.v_ndm] + uv0[f.v_ndmu] + uv0[f.v_nm] + uv0[f.v_nmu]) / 4.0f;
-        }
-        float hu, gnavg2, phi = 1.0f, zd0 = 0.0f, zd1 = 0.0f;
-        bool dry0, dry1;
-        if (SG) {
-          if (zsu > zmax) {
-            const float4 w = S.sgw_u[i];
-            hu = w.x + zsu;
-            gnavg2 = sg_gnavg2_full(w.z, w.y, w.w, zsu - zmax);
-          } else {
-            const SgLevel lv = sg_level(zsu, zmin, zmax, S.nlev);
-            const UvRec r = S.rec_u[(int64_t)(lv.iuv - 1) * S.nalloc + i];
-            hu = fmaf(r.dhavg, lv.facint, r.havg);
-            gnavg2 = fmaf(r.dnrep, lv.facint, r.nrep);
-            phi = fmaf(r.dpwet, lv.facint, r.pwet);
-          }
-          dry0 = S.vneg[f.nm] != 0;
-          dry1 = S.vneg[f.nmu] != 0;
-          if (S.wiggle) {
-            zd0 = S.zsderv[f.nm];
-            zd1 = S.zsderv[f.nmu];
-          }
+        const float zmin = zr.x, zmax = zr.y;
+        if (zsu > zmax) {
+          hu = wz.x + zsu;
+          gnavg2 = sg_gnavg2_full(wz.z, wz.y, wz.w, zsu - zmax);
         } else {
-          hu = fmaxf(zsu - S.zbmx[i], S.huthresh);
-          gnavg2 = S.gn2[i];
-          dry0 = zs_nm < S.zb[f.nm];
-          dry1 = zs_nmu < S.zb[f.nmu];
+          const SgLevel lv = sg_level(zsu, zmin, zmax, S.nlev);
+          const UvRec r = S.rec_u[(int64_t)(lv.iuv - 1) * S.nalloc + i];
+          hu = fmaf(r.dhavg, lv.facint, r.havg);
+          gnavg2 = fmaf(r.dnrep, lv.facint, r.nrep);
+          phi = fmaf(r.dpwet, lv.facint, r.pwet);
         }
-        float qn, un, tauw = dir == 0 ? sv.twu : sv.twv, dpatm = 0.0f;
-        if (MET) face_meteo(S, sv, dir, f.nm, f.nmu, tauw, dpatm);
-        const float ghu = face_flux_geo<SG>(S, sv, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kfuv[i],
-                                            zs_nm, zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, tauw, dpatm, qn,
-                                            un);
-        den = fmaxf(sqrtf(ghu), fabsf(un)) * geo.dxuvinv;  // the face's own spacing (refinement level)
-        q1[i] = qn;
-        uv1[i] = un;
-        kfuv[i] = KF_WET;
       } else {
-        q1[i] = 0.0f;
-        uv1[i] = 0.0f;
-        kfuv[i] = 0;
+        hu = fmaxf(zsu - zbmx, S.huthresh);
+        gnavg2 = gn2;
       }
+      float qn, un, tauw = dir == 0 ? sv.twu : sv.twv, dpatm = 0.0f;
+      if (MET) face_meteo(S, sv, dir, f.nm, f.nmu, tauw, dpatm);
+      const float ghu = face_flux_geo<SG>(S, sv, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kf, zs_nm,
+                                          zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, tauw, dpatm, qn, un);
+      den = fmaxf(sqrtf(ghu), fabsf(un)) * geo.dxuvinv;  // the face's own spacing (refinement level)
+      q1[i] = qn;
+      uv1[i] = un;
+      kfuv[i] = KF_WET;
+    } else {
+      q1[i] = 0.0f;
+      uv1[i] = 0.0f;
+      kfuv[i] = 0;
     }
   }
   // CFL: largest denominator of the warp, one division and one atomicMin per warp
@@ -166,14 +178,26 @@ __global__ void __launch_bounds__(256) k_qt_cuv(const ScnDev* __restrict__ scns,
 template <bool SG, bool EXT>
 __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict__ scns,
                                                         const Tile* __restrict__ tiles) {
-  pdl_wait();  // the previous kernel of the step has completed
-  pdl_trigger();
+  // the cell's static inputs (flags, uv points, level, volume bound) are read
+  // before the wait for the previous kernel
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
-  const StepState& st = *S.st;
-  if (!st.run || (int)threadIdx.x >= tl.m0) return;
   const int c = tl.n0 + (int)threadIdx.x;
-  const uint16_t fl = S.flags[c];
+  const bool mine = (int)threadIdx.x < tl.m0;
+  uint16_t fl = 0;
+  int4 fc = make_int4(0, 0, 0, 0);
+  int L = 0;
+  float volmax = 0.0f;
+  if (mine) {
+    fl = S.flags[c];
+    fc = S.qcell[c];
+    L = S.qlev[c];
+    if (SG) volmax = S.zz_volmax[c];
+  }
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
+  const StepState& st = *S.st;
+  if (!st.run || !mine) return;
   if (!(fl & F_ACT)) return;
   const float* q = S.qu[st.parity ^ 1];
   const float zs_old = S.zs[c];
@@ -198,14 +222,11 @@ __global__ void __launch_bounds__(256) k_qt_continuity(const ScnDev* __restrict_
   }
   if (EXT && S.qinfmap) store_qinfmap(S, c, inf_cell, qinf_cell, SG ? S.zvol[c] > 0.0 : !(zs_old <= S.zb[c]));
   if (fl & F_KCS1) {
-    const int4 fc = S.qcell[c];
     const float q_md = q[fc.x], q_mu = q[fc.y], q_nd = q[fc.z], q_nu = q[fc.w];
-    const int L = S.qlev[c];
     const float qx = S.use_qext ? S.qext[c] : 0.0f;
     const float qi = S.infiltration ? S.qinf[c] : 0.0f;
     if (SG) {
       const double v_old = S.zvol[c];
-      const float volmax = S.zz_volmax[c];
       const float area = S.lv_area[L];
       const float zs00 = S.wiggle ? S.zs0[c] : 0.0f;
       float dvol = ((q_md - q_mu) * S.lv_dyrm[L] + (q_nd - q_nu) * S.lv_dxrm[L]) * dt;
