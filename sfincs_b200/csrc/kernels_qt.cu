@@ -31,29 +31,28 @@ __device__ __forceinline__ float qt_warp_max(float v) {
 // MET: gridded wind or pressure fields (a separate instance, so that the
 // plain path keeps its register allocation)
 template <bool SG, bool MET>
-__global__ void __launch_bounds__(256, 4) k_qt_momentum(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
-  // The point's static inputs (its record, its table bounds) are read before
-  // the wait for the previous kernel; after it, every load that depends only
-  // on the record (both cell levels, the neighbours' fluxes and velocities,
-  // the dry flags) is issued before the wet test, so that a wet point waits
-  // for two rounds of loads (these, then its table record) instead of four.
+__global__ void __launch_bounds__(256) k_qt_momentum(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
+  // The point's two cells, flags and table bounds are static: they are read
+  // before the wait for the previous kernel, so the first round of loads after
+  // it is the cell levels.  The rest of the record (the neighbour indices, in
+  // the same cache lines) and the neighbours' fluxes and velocities are read
+  // only for wet points: holding the whole record across the wait, or reading
+  // the neighbours of every point, cost more than the round trip it saved.
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
   const int i = tl.n0 + (int)threadIdx.x;
   const bool mine = (int)threadIdx.x < tl.m0;
-  FaceQ f{};
+  int2 cells = make_int2(0, 0);
+  uint32_t info = 0;
   float2 zr = make_float2(0.0f, 0.0f);
-  float4 wz = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  float zbmx = 0.0f, gn2 = 0.0f;
+  float zbmx = 0.0f;
   if (mine) {
-    f = S.qface[i];
-    if (SG) {
+    cells = *reinterpret_cast<const int2*>(&S.qface[i].nm);
+    info = S.qface[i].info;
+    if (SG)
       zr = S.sgz_u[i];
-      wz = S.sgw_u[i];
-    } else {
+    else
       zbmx = S.zbmx[i];
-      gn2 = S.gn2[i];
-    }
   }
   pdl_wait();  // the previous kernel of the step has completed
   pdl_trigger();
@@ -66,42 +65,13 @@ __global__ void __launch_bounds__(256, 4) k_qt_momentum(const ScnDev* __restrict
   float* q1 = S.qu[p ^ 1];
   float* uv1 = S.uu[p ^ 1];
   float den = 0.0f;
-  if (mine && (f.info & QF_ACT)) {
-    uint8_t* kfuv = S.kf[0];
-    const float zs_nm = S.zs[f.nm], zs_nmu = S.zs[f.nmu];
-    const uint8_t kf = kfuv[i];
-    FaceV a{};
-    a.qx_nm = q0[i];
-    if (S.advection || S.coriolis || S.viscosity || S.friction2d || S.thetasmooth) {
-      a.qx_nmd = q0[f.u_nmd];
-      a.qx_nmu = q0[f.u_nmu];
-      a.qy_nm = q0[f.v_nm];
-      a.qy_nmu = q0[f.v_nmu];
-      a.qy_ndm = q0[f.v_ndm];
-      a.qy_ndmu = q0[f.v_ndmu];
-      a.uu_nm = uv0[i];
-      a.uu_nmd = uv0[f.u_nmd];
-      a.uu_nmu = uv0[f.u_nmu];
-      a.uu_ndm = uv0[f.u_ndm];
-      a.uu_num = uv0[f.u_num];
-      a.vu = (uv0[f.v_ndm] + uv0[f.v_ndmu] + uv0[f.v_nm] + uv0[f.v_nmu]) / 4.0f;
-    }
-    bool dry0, dry1;
-    float zd0 = 0.0f, zd1 = 0.0f;
-    if (SG) {
-      dry0 = S.vneg[f.nm] != 0;
-      dry1 = S.vneg[f.nmu] != 0;
-      if (S.wiggle) {
-        zd0 = S.zsderv[f.nm];
-        zd1 = S.zsderv[f.nmu];
-      }
-    } else {
-      dry0 = zs_nm < S.zb[f.nm];
-      dry1 = zs_nmu < S.zb[f.nmu];
-    }
+  if (mine && (info & QF_ACT)) {
+    const float zs_nm = S.zs[cells.x], zs_nmu = S.zs[cells.y];
     const float zsu = fmaxf(zs_nm, zs_nmu);
     const bool wet = SG ? zsu > zr.x + S.huthresh : zsu > zbmx;
+    uint8_t* kfuv = S.kf[0];
     if (wet) {
+      const FaceQ f = S.qface[i];
       const int L = (int)((f.info >> 8) & 15u);
       const int dir = (f.info & QF_DIR) ? 1 : 0;
       FaceGeo geo;
@@ -119,12 +89,30 @@ __global__ void __launch_bounds__(256, 4) k_qt_momentum(const ScnDev* __restrict
         geo.nuvisc = S.lv_nuvisc_t[L];
       }
       geo.fcorio = S.fcorio;
-      float hu, gnavg2, phi = 1.0f;
+      FaceV a{};
+      a.qx_nm = q0[i];
+      if (S.advection || S.coriolis || S.viscosity || S.friction2d || S.thetasmooth) {
+        a.qx_nmd = q0[f.u_nmd];
+        a.qx_nmu = q0[f.u_nmu];
+        a.qy_nm = q0[f.v_nm];
+        a.qy_nmu = q0[f.v_nmu];
+        a.qy_ndm = q0[f.v_ndm];
+        a.qy_ndmu = q0[f.v_ndmu];
+        a.uu_nm = uv0[i];
+        a.uu_nmd = uv0[f.u_nmd];
+        a.uu_nmu = uv0[f.u_nmu];
+        a.uu_ndm = uv0[f.u_ndm];
+        a.uu_num = uv0[f.u_num];
+        a.vu = (uv0[f.v_ndm] + uv0[f.v_ndmu] + uv0[f.v_nm] + uv0[f.v_nmu]) / 4.0f;
+      }
+      float hu, gnavg2, phi = 1.0f, zd0 = 0.0f, zd1 = 0.0f;
+      bool dry0, dry1;
       if (SG) {
         const float zmin = zr.x, zmax = zr.y;
         if (zsu > zmax) {
-          hu = wz.x + zsu;
-          gnavg2 = sg_gnavg2_full(wz.z, wz.y, wz.w, zsu - zmax);
+          const float4 w = S.sgw_u[i];
+          hu = w.x + zsu;
+          gnavg2 = sg_gnavg2_full(w.z, w.y, w.w, zsu - zmax);
         } else {
           const SgLevel lv = sg_level(zsu, zmin, zmax, S.nlev);
           const UvRec r = S.rec_u[(int64_t)(lv.iuv - 1) * S.nalloc + i];
@@ -132,14 +120,23 @@ __global__ void __launch_bounds__(256, 4) k_qt_momentum(const ScnDev* __restrict
           gnavg2 = fmaf(r.dnrep, lv.facint, r.nrep);
           phi = fmaf(r.dpwet, lv.facint, r.pwet);
         }
+        dry0 = S.vneg[f.nm] != 0;
+        dry1 = S.vneg[f.nmu] != 0;
+        if (S.wiggle) {
+          zd0 = S.zsderv[f.nm];
+          zd1 = S.zsderv[f.nmu];
+        }
       } else {
         hu = fmaxf(zsu - zbmx, S.huthresh);
-        gnavg2 = gn2;
+        gnavg2 = S.gn2[i];
+        dry0 = zs_nm < S.zb[f.nm];
+        dry1 = zs_nmu < S.zb[f.nmu];
       }
       float qn, un, tauw = dir == 0 ? sv.twu : sv.twv, dpatm = 0.0f;
       if (MET) face_meteo(S, sv, dir, f.nm, f.nmu, tauw, dpatm);
-      const float ghu = face_flux_geo<SG>(S, sv, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kf, zs_nm,
-                                          zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, tauw, dpatm, qn, un);
+      const float ghu = face_flux_geo<SG>(S, sv, dir, (f.info & QF_ADV) != 0, (f.info & QF_TH) != 0, geo, kfuv[i],
+                                          zs_nm, zs_nmu, hu, gnavg2, phi, a, dry0, dry1, zd0, zd1, tauw, dpatm, qn,
+                                          un);
       den = fmaxf(sqrtf(ghu), fabsf(un)) * geo.dxuvinv;  // the face's own spacing (refinement level)
       q1[i] = qn;
       uv1[i] = un;
@@ -157,17 +154,18 @@ __global__ void __launch_bounds__(256, 4) k_qt_momentum(const ScnDev* __restrict
 
 // Combined uv points: mean of the two fine faces (sfincs_momentum.f90:757-779).
 __global__ void __launch_bounds__(256) k_qt_cuv(const ScnDev* __restrict__ scns, const Tile* __restrict__ tiles) {
-  pdl_wait();  // the previous kernel of the step has completed
-  pdl_trigger();
   const Tile tl = tiles[blockIdx.x];
   const ScnDev& S = scns[tl.scn];
-  const StepState& st = *S.st;
-  if (!st.run || (int)threadIdx.x >= tl.m0) return;
   const int ic = tl.n0 + (int)threadIdx.x;
+  const bool mine = (int)threadIdx.x < tl.m0;
+  const int2 c = mine ? S.qcuv[ic] : make_int2(0, 0);  // static: read before the wait
+  pdl_wait();  // the previous kernel of the step has completed
+  pdl_trigger();
+  const StepState& st = *S.st;
+  if (!st.run || !mine) return;
   const int p1 = st.parity ^ 1;
   float* q1 = S.qu[p1];
   float* uv1 = S.uu[p1];
-  const int2 c = S.qcuv[ic];
   q1[S.npuv + ic] = (q1[c.x] + q1[c.y]) / 2.0f;
   uv1[S.npuv + ic] = (uv1[c.x] + uv1[c.y]) / 2.0f;
 }

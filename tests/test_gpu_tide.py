@@ -114,3 +114,33 @@ def test_quadtree_matches_f32_oracle(tmp_path):
     znu = o.get("z_uv_nu", npc).astype(np.int64) - 1
     o.close()
     _stepwise(d, None, cells=(npc, npq, zmu, znu))
+
+
+def test_members_with_constituents_alone_equal_in_mix(tmp_path):
+    """Two members with different constituents, dates and grids advanced by
+    the same launches end bitwise where each ends alone."""
+    from sfincs_b200 import synth
+    from sfincs_b200.bmi import Ensemble, Model
+
+    dirs = []
+    for k, (tref, sets) in enumerate([("20210315 061530", SETS_A0),
+                                      ("20180704 000000", [[("M2", 0.8, 10.0), ("K1", 0.2, 40.0)]])]):
+        m = synth.plain_regular(nmax=20 + 4 * k, mmax=24 + 6 * k, dx=400.0, tstop=1800.0 + 600.0 * k, seed=3 + k,
+                                nbumps=4)
+        if len(sets) == 2:
+            m.bnd = np.array([[0.0, 1200.0], [0.0, 6000.0]])
+            m.bzs = np.stack([m.bzs[:, 0], 0.3 * m.bzs[:, 1], 0.2 * m.bzs[:, 1]], axis=1)
+        d = m.write(str(tmp_path / f"m{k}"))
+        set_tref(d, tref)
+        add_bca(d, sets)
+        dirs.append(d)
+    e = Ensemble(dirs)
+    e.run([e.scalars(i)["t1"] for i in range(len(dirs))])
+    for i, d in enumerate(dirs):
+        g = Model(d)
+        g.run(g.scalars()["t1"])
+        assert e.scalars(i)["nt"] == g.scalars()["nt"]
+        for name in ("zs", "qx", "qy"):
+            assert np.array_equal(e.get(i, name), g.get(name)), (i, name)
+        g.close()
+    e.close()
