@@ -732,6 +732,7 @@ struct Model {
     bdrfile = in.str("bdrfile", "none");
     bzsfile = in.str("bzsfile", "none");
     bcafile = in.str("bcafile", "none");
+    crsfile = in.str("crsfile", "none");
     use_bcafile = in.logical("use_bcafile", true);
     bzifile = in.str("bzifile", "none");
     srcfile = in.str("srcfile", "none");
@@ -2084,6 +2085,69 @@ struct Model {
     return out;
   }
 
+  // read_crs_file: sfincs_crosssections.f90:8-127.  Polylines of the crs
+  // file; per polyline the uv points it crosses and the sign of each crossing
+  // from the angle between the uv point's direction and the segment.
+  std::string crsfile = "none";
+  std::vector<std::string> namecrs;
+  std::vector<std::vector<long>> crs_uv_index;
+  std::vector<std::vector<int>> crs_idir;
+  void read_crs_file() {
+    if (crsfile.substr(0, 4) == "none") return;
+    std::ifstream fin(path(crsfile));
+    if (!fin) throw std::runtime_error("oracle: cannot open " + crsfile);
+    std::vector<std::string> rec;
+    for (std::string l; std::getline(fin, l);) {
+      for (char& ch : l)
+        if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
+      if (l.find_first_not_of(' ') != std::string::npos) rec.push_back(l);
+    }
+    size_t ir = 0;
+    while (ir + 1 < rec.size()) {
+      std::string cdummy;
+      std::istringstream(rec[ir++]) >> cdummy;
+      if (cdummy.size() >= 2 && (cdummy.front() == '\'' || cdummy.front() == '"') && cdummy.back() == cdummy.front())
+        cdummy = cdummy.substr(1, cdummy.size() - 2);
+      std::istringstream hs(rec[ir++]);
+      int nrows = 0, ncols = 0;
+      hs >> nrows >> ncols;
+      std::vector<float> xcrs(nrows), ycrs(nrows);
+      for (int i = 0; i < nrows; i++) {
+        if (ir >= rec.size()) throw std::runtime_error("oracle: truncated cross-section polyline");
+        std::istringstream ps(rec[ir++]);
+        ps >> xcrs[i] >> ycrs[i];
+      }
+      namecrs.push_back(cdummy);
+      std::vector<long> idx;
+      std::vector<int> idir;
+      for (const auto& e : uv_points_crossed_by_polyline(xcrs, ycrs)) {
+        const long indx = e.first, irow = e.second;
+        const long nm = uv_index_z_nm(indx), nmu = uv_index_z_nmu(indx);
+        const float phiuv = std::atan2(z_yz(nmu) - z_yz(nm), z_xz(nmu) - z_xz(nm));
+        const float phic = std::atan2(ycrs[irow] - ycrs[irow - 1], xcrs[irow] - xcrs[irow - 1]);
+        float dphi = phiuv - phic;
+        if (dphi < 0.0f) dphi = dphi + 2 * pi;
+        if (dphi > 2 * pi) dphi = dphi - 2 * pi;
+        idx.push_back(indx);
+        idir.push_back(dphi <= pi ? 1 : -1);
+      }
+      crs_uv_index.push_back(idx);
+      crs_idir.push_back(idir);
+    }
+  }
+
+  // get_discharges_through_crosssections: sfincs_crosssections.f90:130-176
+  float crs_discharge(size_t icrs) {
+    float qq = 0.0f;
+    for (size_t ip = 0; ip < crs_uv_index[icrs].size(); ip++) {
+      const long indx = crs_uv_index[icrs][ip];
+      const int iref = uv_flags_iref(indx), iuv = uv_flags_dir(indx);
+      const float dxycrs = iuv == 0 ? dyrm(iref) : dxrm(iref);
+      qq = qq + (float)q(indx) * (float)crs_idir[icrs][ip] * dxycrs;
+    }
+    return qq;
+  }
+
   // read_structures: sfincs_structures.f90:8-35 (thin dams, then weirs)
   void read_structures() {
     read_thin_dams();
@@ -2762,6 +2826,7 @@ struct Model {
     if (qt_nlev == 1) use_quadtree = false;  // sfincs_domain.f90:42-50
     set_advection_mask();
     read_structures();  // sfincs_lib.f90:156, after initialize_domain
+    read_crs_file();
     read_boundary_data();
     find_boundary_indices();
     read_discharges();
@@ -3978,6 +4043,24 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
         out[4 * (i - 1) + 2] = m.structure_parameters(2, i);
         out[4 * (i - 1) + 3] = m.structure_length(i);
       }
+    }
+    else if (s == "crs_faces") {  // per crossed uv point: cross-section, cell nm (0-based), direction, sign
+      long k = 0;
+      for (size_t c = 0; c < m.crs_uv_index.size(); c++)
+        for (size_t j = 0; j < m.crs_uv_index[c].size(); j++) {
+          if (4 * k + 3 >= n) return -1;
+          const long ip = m.crs_uv_index[c][j];
+          out[4 * k] = (double)c;
+          out[4 * k + 1] = (double)(m.uv_index_z_nm(ip) - 1);
+          out[4 * k + 2] = (double)m.uv_flags_dir(ip);
+          out[4 * k + 3] = (double)m.crs_idir[c][j];
+          k++;
+        }
+      if (4 * k != n) return -1;
+    }
+    else if (s == "crs_discharge") {  // discharge through every cross-section from the current q
+      if ((long)m.namecrs.size() != n) return -1;
+      for (long i = 0; i < n; i++) out[i] = (double)m.crs_discharge((size_t)i);
     }
     else if (s == "tide_omega" || s == "tide_amp" || s == "tide_phase") {
       // astronomic constituents after the nodal correction: per constituent, or per point and constituent

@@ -1033,6 +1033,12 @@ int sfg_layout_get(const char* model_dir, int bmi, const char* name, double* dst
         for (double v : {h.p.quadtree ? (double)w.face : (double)h.dense2cmp[w.face], (double)w.dir, (double)w.height,
                          (double)w.cd, (double)w.len})
           out.push_back(v);
+    } else if (nm == "crs_faces") {  // per crossed face: cross-section, cell (0-based compact), direction, sign
+      for (size_t c = 0; c < h.out.crs.size(); c++)
+        for (const auto& f : h.out.crs[c].faces) {
+          const double cell = h.p.quadtree ? (double)h.qface[(size_t)f.face].nm : (double)h.dense2cmp[(size_t)f.face];
+          for (double v : {(double)c, cell, (double)f.dir, (double)f.idir}) out.push_back(v);
+        }
     } else if (nm == "tide_omega") {
       out.assign(h.tide.omega.begin(), h.tide.omega.end());
     } else if (nm == "tide_amp") {

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <sstream>
 #include <type_traits>
 #include <stdexcept>
 
@@ -324,7 +325,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
   // options whose geographic arithmetic this core does not carry are refused
   if (igeo != 0) {
     if (!is_none(qtrfile)) throw std::runtime_error("geographic quadtree meshes (crsgeo=1 with qtrfile) are not supported");
-    for (const char* k : {"spwfile", "weirfile", "drnfile"})
+    for (const char* k : {"spwfile", "weirfile", "drnfile", "crsfile"})
       if (!is_none(in.str(k, "none")))
         throw std::runtime_error(std::string("input '") + k + "' on a geographic grid (crsgeo=1) is not supported");
   }
@@ -376,9 +377,9 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
     if (in.logical("storehmean", false)) throw std::runtime_error("storehmean (subgrid mean depth output) is not supported");
     if (in.integer("storemeteo", 0) == 1) throw std::runtime_error("storemeteo (meteo map output) is not supported");
     if (in.logical("debug", false)) throw std::runtime_error("debug output (every step) is not supported");
-    for (const char* f : {"crsfile", "rugfile"})
-      if (!is_none(in.str(f, "none")))
-        throw std::runtime_error(std::string("input '") + f + "' (cross-section / run-up output) is not supported");
+    o.crsfile = in.str("crsfile", "none");
+    if (!is_none(in.str("rugfile", "none")))
+      throw std::runtime_error("input 'rugfile' (run-up gauge output) is not supported");
     for (const auto& kv : in.all()) o.inp.push_back(kv);
   }
   tspinup = t0 + tspinup;
@@ -518,7 +519,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
 // A .thd / .weir file holds polylines, each as a name line, an "nrows ncols"
 // line and nrows lines of x y followed by npars values per point (blank lines
 // skipped, commas accepted as separators, as list-directed input does).
-std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars) {
+std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars, std::vector<std::string>* names) {
   FILE* fp = std::fopen(file.c_str(), "r");
   if (!fp) throw std::runtime_error("cannot open polyline file " + file);
   std::vector<std::string> lines;
@@ -533,6 +534,13 @@ std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int np
   std::vector<std::vector<PolyRow>> out;
   size_t i = 0;
   while (i + 1 < lines.size()) {
+    if (names) {  // the name: the line's first item, quotes removed (list-directed read)
+      std::string nm;
+      std::istringstream(lines[i]) >> nm;
+      if (nm.size() >= 2 && (nm.front() == '\'' || nm.front() == '"') && nm.back() == nm.front())
+        nm = nm.substr(1, nm.size() - 2);
+      names->push_back(nm);
+    }
     i++;  // name line
     int nrows = 0, ncols = 0;
     if (std::sscanf(lines[i++].c_str(), "%d %d", &nrows, &ncols) != 2 || nrows < 0)
@@ -548,6 +556,15 @@ std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int np
     out.push_back(std::move(pl));
   }
   return out;
+}
+
+float crossing_sign(float xnm, float ynm, float xnmu, float ynmu, float xa, float ya, float xb, float yb, float pi) {
+  const float phiuv = std::atan2(ynmu - ynm, xnmu - xnm);
+  const float phic = std::atan2(yb - ya, xb - xa);
+  float dphi = phiuv - phic;
+  if (dphi < 0.0f) dphi = dphi + 2.0f * pi;
+  if (dphi > 2.0f * pi) dphi = dphi - 2.0f * pi;
+  return dphi <= pi ? 1.0f : -1.0f;
 }
 
 // Drainage structures file (sfincs_discharges.f90:203-256): one line each,
@@ -843,6 +860,27 @@ std::unique_ptr<HostModel> load_model(const std::string& dir, bool bmi) {
     dam_v.assign(NA, 0);
     for (const auto& pl : read_polylines(path(K.thdfile), 0))
       for (const auto& e : crossed_faces(pl)) ((e.first & 1) ? dam_v : dam_u)[e.first >> 1] = 1;
+  }
+  // cross-sections (sfincs_crosssections.f90:8-127): the crossed uv points in
+  // uv-point order, the sign from the last segment crossing each
+  if (!is_none(h.out.crsfile)) {
+    std::vector<std::string> names;
+    const auto pls = read_polylines(path(h.out.crsfile), 0, &names);
+    for (size_t k = 0; k < pls.size(); k++) {
+      CrossSection cs;
+      cs.name = names[k];
+      for (const auto& e : crossed_faces(pls[k])) {
+        const int64_t c = e.first >> 1;
+        const int dir = (int)(e.first & 1);
+        const int n = (int)(c % ld) - kGhostPad, m = (int)(c / ld);
+        const int n2 = dir == 0 ? n : n + 1, m2 = dir == 0 ? m + 1 : m;
+        const auto& a = pls[k][(size_t)e.second];
+        const auto& b = pls[k][(size_t)e.second + 1];
+        cs.faces.push_back(CrsFace{c, dir, crossing_sign(xz(n, m), yz(n, m), xz(n2, m2), yz(n2, m2), a.x, a.y, b.x, b.y, P.pi),
+                                   dir == 0 ? dy : dx});
+      }
+      h.out.crs.push_back(std::move(cs));
+    }
   }
 
   // ---- bathymetry (regular) or subgrid tables -----------------------------------

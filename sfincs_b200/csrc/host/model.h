@@ -46,6 +46,21 @@ struct ObsPoint {
   int nm = 0;
 };
 // Output settings (sfincs_input.f90:61-87, 274-294, 441-540), times in seconds after tref.
+// One cross-section (sfincs_crosssections.f90:8-127): the uv points its
+// polyline crosses, in uv-point order, each with the sign of the crossing
+// and the face width; face is the dense offset of the u or v face (regular
+// grids) or the uv point (quadtree meshes).
+struct CrsFace {
+  int64_t face;
+  int dir;       // 0: u face, 1: v face
+  float idir;    // +1 or -1
+  float width;   // dyrm of a u face, dxrm of a v face (m)
+};
+struct CrossSection {
+  std::string name;
+  std::vector<CrsFace> faces;
+};
+
 struct OutputSpec {
   double t0out = 0, t1out = 0, dtmapout = 0, dthisout = 600, dtmaxout = 9999999;
   std::string map_type = "net", his_type = "net";  // net: netCDF; bin: Fortran records; his asc/bin: text
@@ -53,10 +68,11 @@ struct OutputSpec {
   int epsg = 0;
   std::string epsg_code;
   std::vector<ObsPoint> obs;
+  std::string crsfile = "none";
+  std::vector<CrossSection> crs;
   std::vector<std::pair<std::string, std::string>> inp;  // the sfincs.inp keys, for the files' 'inp' attributes
 };
 
-// Everything read from a model directory and laid out densely on the host.
 // Astronomic boundary constituents after the nodal correction at tref: per
 // constituent its frequency (rad/s), per point and constituent the amplitude
 // times the nodal factor and the phase less V0+u (rad, in [0, 2 pi)); the first
@@ -69,6 +85,7 @@ struct TideHost {
 };
 void read_bca_file(const std::string& file, const std::string& tref, int nbnd, TideHost& out);
 
+// Everything read from a model directory and laid out densely on the host.
 struct HostModel {
   std::string dir;
   ScnDev p{};  // scalar parameters (pointer fields unused on the host copy)
@@ -175,7 +192,11 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi);
 struct PolyRow {
   float x, y, p[2];
 };
-std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars);
+std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int npars,
+                                                  std::vector<std::string>* names = nullptr);
+// The sign of a crossing: +1 when the uv point's direction (cell nm to nmu)
+// lies within pi counter-clockwise of the polyline segment (sfincs_crosssections.f90:92-107).
+float crossing_sign(float xnm, float ynm, float xnmu, float ynmu, float xa, float ya, float xb, float yb, float pi);
 // The reference's segment crossing test (geometry.f90 cross / direction, FP32).
 bool segments_cross(float p1x, float p1y, float p2x, float p2y, float q1x, float q1y, float q2x, float q2y);
 // One line of a drainage structures file: intake and outfall points, type, parameters.

@@ -50,6 +50,7 @@ enum {
   S_ZS, S_UMD, S_UMU, S_VND, S_VNU, S_INF, S_ZVOL,                    // map
   S_ZSMAX, S_VMAX, S_QMAX, S_TWET, S_TZSMAX, S_CUMP, S_CUMI,          // max
   H_ZS, H_UMD, H_UMU, H_VND, H_VNU, H_QINF, H_S,                      // his (obs points)
+  H_CRSU, H_CRSV,                                                     // his (cross-section faces: u, v fluxes)
   NSLOT
 };
 
@@ -112,6 +113,8 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
   const ScnDev& P = h.p;
   np_ = (size_t)h.np;
   nobs_ = o.obs.size();
+  ncrs_ = o.crs.size();
+  for (const auto& cs : o.crs) ncrs_faces_ += cs.faces.size();
   // which files (sfincs_output.f90:8-58)
   if (o.dtmapout > 1.0e-6) {
     tmapout = o.t0out;
@@ -123,7 +126,7 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
     // netCDF: into the map file, which exists only with map output; binary: files of their own
     max_on_ = o.map_type == "net" ? map_net_ : true;
   }
-  if (o.dthisout > 1.0e-6 && nobs_ > 0) {
+  if (o.dthisout > 1.0e-6 && (nobs_ > 0 || ncrs_ > 0)) {
     thisout = (double)h.t0;
     his_net_ = o.his_type == "net";
     his_txt_ = !his_net_;
@@ -137,7 +140,7 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
   // gather maps: per cell the storage index of its md, nd, mu, nu uv points
   // (regular grids: the cell's own faces and those of its left / lower
   // neighbours), then per observation point its cell and faces
-  std::vector<int32_t> maps(4 * np_ + 5 * std::max<size_t>(nobs_, 1), 0);
+  std::vector<int32_t> maps(4 * np_ + 5 * std::max<size_t>(nobs_, 1) + std::max<size_t>(ncrs_faces_, 1), 0);
   for (size_t i = 0; i < np_; i++) {
     if (P.quadtree) {
       const int4 c = h.qcell[i];
@@ -152,6 +155,11 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
     if (nm <= 0) continue;
     for (int j = 0; j < 4; j++) maps[4 * np_ + j * nobs_ + k] = maps[(size_t)j * np_ + (size_t)nm - 1];
     maps[4 * np_ + 4 * nobs_ + k] = h.cmp_off[(size_t)nm - 1];
+  }
+  {  // then per cross-section face its flux storage (dense face offset, or quadtree uv point)
+    size_t j = 4 * np_ + 5 * std::max<size_t>(nobs_, 1);
+    for (const auto& cs : o.crs)
+      for (const auto& f : cs.faces) maps[j++] = (int32_t)f.face;
   }
   check(cudaMalloc(&d_maps_, maps.size() * 4), "maps");
   check(cudaMemcpy(d_maps_, maps.data(), maps.size() * 4, cudaMemcpyHostToDevice), "maps");
@@ -184,6 +192,10 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
       for (int k : {H_UMD, H_UMU, H_VND, H_VNU}) want(k, nobs_, 4);
     if (his_net_ && P.infiltration && d.dev().qinfmap) want(H_QINF, nobs_, 4);
     if (his_net_ && (P.inftype == 3 || P.inftype == 4)) want(H_S, nobs_, 4);
+    if (ncrs_faces_ > 0) {
+      want(H_CRSU, ncrs_faces_, 4);
+      if (!P.quadtree) want(H_CRSV, ncrs_faces_, 4);
+    }
   }
   // file layout of the cell fields: (n, m) rows of the regular grid, or every point of the quadtree file
   file_idx_.resize(np_);
@@ -207,6 +219,7 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
   if (his_txt_) {  // open_his_output: fresh text files
     std::remove((h.dir + "/zst.txt").c_str());
     if (P.precip) std::remove((h.dir + "/prcp.txt").c_str());
+    if (ncrs_ > 0) std::remove((h.dir + "/qt.txt").c_str());
   }
   worker_ = std::thread([this] { run_worker(); });
 }
@@ -590,7 +603,8 @@ void OutputWriter::open_his() {
   his_nc_ = std::make_unique<NcWriter>();
   NcWriter& nc = *his_nc_;
   const int d_time = nc.def_dim("time", NcWriter::UNLIMITED);
-  const int d_st = nc.def_dim("stations", (long long)nobs_);
+  const int d_st = nc.def_dim("stations", (long long)std::max<size_t>(nobs_, 1));  // 1 without points, as the reference
+  const int d_crs = ncrs_ > 0 ? nc.def_dim("crosssections", (long long)ncrs_) : -1;
   const int d_len = nc.def_dim("pointnamelength", 256);
   const int d_run = nc.def_dim("runtime", 1);
   nc.att_text(NcWriter::GLOBAL, "Conventions", "CF-1.8");
@@ -602,6 +616,7 @@ void OutputWriter::open_his() {
   const int v_id = nc.def_var("station_id", NcWriter::FLOAT, {d_st});
   const int v_name = nc.def_var("station_name", NcWriter::CHAR, {d_st, d_len});
   nc.att_text(v_name, "cf_role", "timeseries_id");
+  const int v_crsname = ncrs_ > 0 ? nc.def_var("crosssection_name", NcWriter::CHAR, {d_crs, d_len}) : -1;
   auto coord = [&](const char* name, bool x, const char* long_name) {
     const int v = nc.def_var(name, NcWriter::FLOAT, {d_st});
     nc.att_text(v, "units", P.geo ? "degrees" : "m");  // def_his_point_coord
@@ -633,7 +648,7 @@ void OutputWriter::open_his() {
   nc.att_text(v_time, "units", "seconds since " + iso8601(h.tref));
   nc.att_text(v_time, "standard_name", "time");
   nc.att_text(v_time, "long_name", "time_in_seconds_since_" + iso8601(h.tref));
-  his_ids_.assign(9, -1);
+  his_ids_.assign(10, -1);
   his_ids_[0] = v_time;
   his_ids_[1] = pvar("point_zs", {d_time, d_st}, "m", "Water level", "sea_surface_height_above_reference_level");
   if (!P.subgrid || o.store_hsubgrid) his_ids_[2] = pvar("point_h", {d_time, d_st}, "m", "Water depth", "depth");
@@ -647,6 +662,10 @@ void OutputWriter::open_his() {
   if (slot(H_QINF).dev) his_ids_[7] = pvar("point_qinf", {d_time, d_st}, "mm hr-1", "Infiltration rate", nullptr);
   if (P.inftype == 3) his_ids_[8] = pvar("point_S", {d_time, d_st}, "m", "current moisture storage (Se) capacity", nullptr);
   if (P.inftype == 4) his_ids_[8] = pvar("point_S", {d_time, d_st}, "m", "maximum soil moisture deficit", nullptr);
+  if (ncrs_ > 0) {  // ncoutput_his_init (sfincs_ncoutput.F90:1033-1036)
+    his_ids_[9] = pvar("crosssection_discharge", {d_time, d_crs}, "m3 s-1", "discharge", nullptr);
+    nc.att_text(his_ids_[9], "coordinates", "crosssection_name");
+  }
   pvar("total_runtime", {d_run}, "s", "Total model runtime (s)", nullptr);
   pvar("average_dt", {d_run}, "s", "Average model time step (s)", nullptr);
   pvar("status", {d_run}, "-", "status of SFINCS simulation - 0 is no error", nullptr);
@@ -666,6 +685,12 @@ void OutputWriter::open_his() {
   nc.put(v_px, px.data(), nobs_);
   nc.put(v_py, py.data(), nobs_);
   nc.put(v_zb, zb.data(), nobs_);
+  if (ncrs_ > 0) {
+    std::vector<char> cn(ncrs_ * 256, ' ');
+    for (size_t k = 0; k < ncrs_; k++)
+      std::memcpy(&cn[k * 256], o.crs[k].name.data(), std::min<size_t>(o.crs[k].name.size(), 256));
+    nc.put(v_crsname, cn.data(), cn.size());
+  }
   const int32_t epsg = o.epsg;
   nc.put(v_crs, &epsg, 1);
   nc.sync();
@@ -753,6 +778,9 @@ void OutputWriter::write(bool map, bool max, bool his, double tout, int p) {
     g(H_VNU, uvv, om + 3 * nobs_);
     g(H_QINF, D.qinfmap, om + 4 * nobs_);
     g(H_S, D.inf_st[0], om + 4 * nobs_);
+    const int32_t* oc = d_maps_ + 4 * np_ + 5 * std::max<size_t>(nobs_, 1);
+    g(H_CRSU, D.qu[p], oc);
+    g(H_CRSV, D.quadtree ? nullptr : D.qv[p], oc);
   }
   check(cudaGetLastError(), "gather launch");
   check(cudaEventRecord(gathered_, main_), "record");
@@ -875,6 +903,23 @@ void OutputWriter::write_max_files(double tout, int rec) {
 }
 
 // ncoutput_update_his (sfincs_ncoutput.F90:1275-1436) / write_his_output (sfincs_output.f90:577-620)
+// get_discharges_through_crosssections (sfincs_crosssections.f90:130-176):
+// per cross-section, in uv-point order, q times the crossing sign times the
+// face width, summed in real*4.
+std::vector<float> OutputWriter::crs_discharges() {
+  const float* qu = (const float*)slot(H_CRSU).host;
+  const float* qv = (const float*)slot(H_CRSV).host;
+  std::vector<float> qq(ncrs_, 0.0f);
+  size_t j = 0;
+  for (size_t k = 0; k < ncrs_; k++)
+    for (const auto& f : h_.out.crs[k].faces) {
+      const float q = (f.dir == 0 || !qv) ? qu[j] : qv[j];
+      qq[k] = qq[k] + q * f.idir * f.width;
+      j++;
+    }
+  return qq;
+}
+
 void OutputWriter::write_his_files(double tout, int rec) {
   const HostModel& h = h_;
   const ScnDev& P = h.p;
@@ -887,6 +932,15 @@ void OutputWriter::write_his_files(double tout, int rec) {
     for (size_t k = 0; k < nobs_; k++) std::fprintf(f, "%9.3f", o.obs[k].nm > 0 ? zs[k] : -999.0f);
     std::fprintf(f, "\n");
     std::fclose(f);
+    if (ncrs_ > 0) {  // qt.txt: f12.1 then f12.3 per cross-section
+      const std::vector<float> qq = crs_discharges();
+      FILE* fq = std::fopen((h.dir + "/qt.txt").c_str(), "a");
+      if (!fq) throw std::runtime_error("cannot append to qt.txt");
+      std::fprintf(fq, "%12.1f", tout);
+      for (float v : qq) std::fprintf(fq, "%12.3f", v);
+      std::fprintf(fq, "\n");
+      std::fclose(fq);
+    }
     return;
   }
   NcWriter& nc = *his_nc_;
@@ -930,6 +984,10 @@ void OutputWriter::write_his_files(double tout, int rec) {
   };
   point(his_ids_[7], H_QINF, 3600000.0f);
   point(his_ids_[8], H_S, 1.0f);
+  if (his_ids_[9] >= 0) {
+    const std::vector<float> qq = crs_discharges();
+    nc.put_record(his_ids_[9], rec, qq.data(), ncrs_);
+  }
   nc.sync();
 }
 

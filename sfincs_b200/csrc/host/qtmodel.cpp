@@ -757,6 +757,28 @@ void QtBuilder::finish() {
     }
     return ind;
   };
+  // cross-sections (sfincs_crosssections.f90:8-127): the crossed uv points in
+  // uv-point order, the sign from the last segment crossing each, the width
+  // of the point's refinement level
+  if (!none(h.out.crsfile)) {
+    std::vector<std::string> names;
+    const auto pls = read_polylines(path(h.out.crsfile), 0, &names);
+    for (size_t kp = 0; kp < pls.size(); kp++) {
+      CrossSection cs;
+      cs.name = names[kp];
+      for (const auto& e : crossed(pls[kp])) {
+        const long ip = e.first, nm = uv_nm[ip], nmu = uv_nmu[ip];
+        const int dir = uv_dir[ip];
+        const auto& a = pls[kp][(size_t)e.second];
+        const auto& b = pls[kp][(size_t)e.second + 1];
+        cs.faces.push_back(CrsFace{ip - 1, dir,
+                                   crossing_sign(h.z_xz[nm - 1], h.z_yz[nm - 1], h.z_xz[nmu - 1], h.z_yz[nmu - 1], a.x,
+                                                 a.y, b.x, b.y, h.p.pi),
+                                   dir == 0 ? dyr[uv_iref[ip]] : dxr[uv_iref[ip]]});
+      }
+      h.out.crs.push_back(std::move(cs));
+    }
+  }
   if (!none(k.thdfile))
     for (const auto& pl : read_polylines(path(k.thdfile), 0))
       for (const auto& e : crossed(pl)) kcuv_run[e.first] = 0;

@@ -19,7 +19,8 @@ def _nc(path):
     return f
 
 
-def _model(tmp_path, extra, quadtree=False, subgrid=False):
+def _model(tmp_path, extra, quadtree=False, subgrid=False, crs=True):
+    from crs_cases import add_crs
     from sfincs_b200 import qtsynth, synth
 
     if quadtree:
@@ -39,6 +40,8 @@ def _model(tmp_path, extra, quadtree=False, subgrid=False):
     with open(os.path.join(d, "sfincs.inp"), "a") as f:
         for k, v in keys.items():
             f.write(f"{k:<20} = {v}\n")
+    if crs:  # three cross-sections (the quadtree mesh spans 4 km x 3.2 km)
+        add_crs(d, scale=1.0 / 3.0 if quadtree else 1.0)
     return d, m
 
 
@@ -46,7 +49,7 @@ class Expected:
     """The oracle stepped one step at a time, with the reference's output
     schedule (sfincs_lib.f90:419-476): per output, its time and the state."""
 
-    def __init__(self, d, dtmap, dthis, dtmax, stored=("vmax_out", "twet_out")):
+    def __init__(self, d, dtmap, dthis, dtmax, stored=("vmax_out", "twet_out"), ncrs=3):
         from oracle.oracle import Oracle
 
         self.stored = stored
@@ -57,7 +60,7 @@ class Expected:
         self.zb = o.get("z_zmin") if s["subgrid"] else o.get("zb")
         md, mu = o.get("z_uv_md", n).astype(np.int64), o.get("z_uv_mu", n).astype(np.int64)
         nd, nu = o.get("z_uv_nd", n).astype(np.int64), o.get("z_uv_nu", n).astype(np.int64)
-        self.map, self.his, self.max = [], [], []
+        self.map, self.his, self.max, self.crs = [], [], [], []
         tmap, this, tmax = t0, t0, t0 + dtmax
         nmax_before = 0
         while o.scalars()["t"] < t1:
@@ -84,6 +87,8 @@ class Expected:
                 self.map.append((np.float32(tout), zs, u, v))
             if whis:
                 self.his.append((np.float32(tout), zs.copy()))
+                if ncrs:
+                    self.crs.append(o.get("crs_discharge", ncrs))
             if wmax:
                 assert int(o.get("ntmaxout", 1)[0]) == nmax_before + 1
                 nmax_before += 1
@@ -152,6 +157,15 @@ def test_netcdf_map_his_and_max_match_the_oracle(tmp_path, subgrid):
         assert np.allclose(pz[k, :2], zs[cells[:2]], atol=2e-5)
         assert pz[k, 2] == FILL
     assert np.allclose(h.variables["point_zb"][:2], e.zb[cells[:2]].astype(np.float32))
+    # cross-sections: names and discharges at every his time (sfincs_crosssections.f90:130-176)
+    from crs_cases import NAMES
+
+    assert [b"".join(r).decode().strip() for r in h.variables["crosssection_name"][:]] == NAMES
+    qd = h.variables["crosssection_discharge"][:]
+    assert qd.shape == (len(e.his), 3)
+    want = np.array(e.crs)
+    assert np.abs(want).max() > 1.0
+    assert np.allclose(qd, want, rtol=1e-4, atol=0.2), np.abs(qd - want).max()
     h.close()
 
 
@@ -196,6 +210,11 @@ def test_binary_map_max_and_text_his(tmp_path):
         assert np.allclose(got, want, atol=2e-5)
     lines = open(os.path.join(d, "zst.txt")).read().splitlines()
     assert len(lines) == len(e.his)
+    qt = open(os.path.join(d, "qt.txt")).read().splitlines()
+    assert len(qt) == len(e.his)
+    for line, want in zip(qt, e.crs):
+        assert len(line) == 12 + 12 * 3
+        assert np.allclose([float(line[12 + 12 * k:24 + 12 * k]) for k in range(3)], want, rtol=1e-4, atol=0.2)
     for line, (t, zs) in zip(lines, e.his):
         assert len(line) == 12 + 9 * 3
         assert float(line[:12]) == pytest.approx(float(t), abs=0.05)
@@ -205,7 +224,7 @@ def test_binary_map_max_and_text_his(tmp_path):
 def test_quadtree_map_file_is_a_ugrid_mesh(tmp_path):
     from sfincs_b200.bmi import Model
 
-    d, m = _model(tmp_path, dict(dtout=1200, dtmaxout=3600, dthisout=0), quadtree=True, subgrid=True)
+    d, m = _model(tmp_path, dict(dtout=1200, dtmaxout=3600, dthisout=600), quadtree=True, subgrid=True)
     g = Model(d)
     g.run(g.scalars()["t1"])
     zs_end = g.get("zs")
@@ -228,3 +247,7 @@ def test_quadtree_map_file_is_a_ugrid_mesh(tmp_path):
     assert np.allclose(fx, nx.mean(axis=1), atol=1e-3)
     assert f.variables["zsmax"][:].shape == (1, nq)
     f.close()
+    h = _nc(os.path.join(d, "sfincs_his.nc"))
+    qd = h.variables["crosssection_discharge"][:]
+    assert qd.shape == (7, 3) and np.all(np.isfinite(qd)) and np.abs(qd).max() > 0.0  # t = 0, 600, ..., 3600
+    h.close()
