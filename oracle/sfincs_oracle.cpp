@@ -2104,10 +2104,17 @@ struct Model {
     }
     size_t ir = 0;
     while (ir + 1 < rec.size()) {
-      std::string cdummy;
-      std::istringstream(rec[ir++]) >> cdummy;
-      if (cdummy.size() >= 2 && (cdummy.front() == '\'' || cdummy.front() == '"') && cdummy.back() == cdummy.front())
-        cdummy = cdummy.substr(1, cdummy.size() - 2);
+      std::string cdummy;  // list-directed: the first item, a quoted string whole
+      {
+        const std::string& l = rec[ir++];
+        const size_t a = l.find_first_not_of(' ');
+        if (l[a] == '\'' || l[a] == '"') {
+          const size_t b = l.find(l[a], a + 1);
+          cdummy = l.substr(a + 1, (b == std::string::npos ? l.size() : b) - a - 1);
+        } else {
+          std::istringstream(l) >> cdummy;
+        }
+      }
       std::istringstream hs(rec[ir++]);
       int nrows = 0, ncols = 0;
       hs >> nrows >> ncols;
@@ -4057,6 +4064,10 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
           k++;
         }
       if (4 * k != n) return -1;
+    }
+    else if (s == "q_drain") {  // per drainage structure the rate of its intake entry (sfincs_ncoutput.F90:1410-1421)
+      if (m.ndrn != n) return -1;
+      for (long i = 1; i <= n; i++) out[i - 1] = (double)m.qtsrc(m.nsrc + 2 * i - 1);
     }
     else if (s == "crs_discharge") {  // discharge through every cross-section from the current q
       if ((long)m.namecrs.size() != n) return -1;

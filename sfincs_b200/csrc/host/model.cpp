@@ -534,11 +534,16 @@ std::vector<std::vector<PolyRow>> read_polylines(const std::string& file, int np
   std::vector<std::vector<PolyRow>> out;
   size_t i = 0;
   while (i + 1 < lines.size()) {
-    if (names) {  // the name: the line's first item, quotes removed (list-directed read)
+    if (names) {  // the name: the line's first item, a quoted string whole (list-directed read)
+      const std::string& l = lines[i];
+      const size_t a = l.find_first_not_of(' ');
       std::string nm;
-      std::istringstream(lines[i]) >> nm;
-      if (nm.size() >= 2 && (nm.front() == '\'' || nm.front() == '"') && nm.back() == nm.front())
-        nm = nm.substr(1, nm.size() - 2);
+      if (l[a] == '\'' || l[a] == '"') {
+        const size_t b = l.find(l[a], a + 1);
+        nm = l.substr(a + 1, (b == std::string::npos ? l.size() : b) - a - 1);
+      } else {
+        std::istringstream(l) >> nm;
+      }
       names->push_back(nm);
     }
     i++;  // name line

@@ -51,6 +51,7 @@ enum {
   S_ZSMAX, S_VMAX, S_QMAX, S_TWET, S_TZSMAX, S_CUMP, S_CUMI,          // max
   H_ZS, H_UMD, H_UMU, H_VND, H_VNU, H_QINF, H_S,                      // his (obs points)
   H_CRSU, H_CRSV,                                                     // his (cross-section faces: u, v fluxes)
+  H_QDRN,                                                             // his (drainage structures)
   NSLOT
 };
 
@@ -140,7 +141,8 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
   // gather maps: per cell the storage index of its md, nd, mu, nu uv points
   // (regular grids: the cell's own faces and those of its left / lower
   // neighbours), then per observation point its cell and faces
-  std::vector<int32_t> maps(4 * np_ + 5 * std::max<size_t>(nobs_, 1) + std::max<size_t>(ncrs_faces_, 1), 0);
+  ndrn_ = (size_t)P.ndrn;
+  std::vector<int32_t> maps(4 * np_ + 5 * std::max<size_t>(nobs_, 1) + std::max<size_t>(ncrs_faces_, 1) + ndrn_, 0);
   for (size_t i = 0; i < np_; i++) {
     if (P.quadtree) {
       const int4 c = h.qcell[i];
@@ -160,6 +162,9 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
     size_t j = 4 * np_ + 5 * std::max<size_t>(nobs_, 1);
     for (const auto& cs : o.crs)
       for (const auto& f : cs.faces) maps[j++] = (int32_t)f.face;
+    // then per drainage structure its intake entry of the source rates
+    j = 4 * np_ + 5 * std::max<size_t>(nobs_, 1) + std::max<size_t>(ncrs_faces_, 1);
+    for (size_t k = 0; k < ndrn_; k++) maps[j++] = (int32_t)(P.nsrc + 2 * k);
   }
   check(cudaMalloc(&d_maps_, maps.size() * 4), "maps");
   check(cudaMemcpy(d_maps_, maps.data(), maps.size() * 4, cudaMemcpyHostToDevice), "maps");
@@ -192,6 +197,7 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
       for (int k : {H_UMD, H_UMU, H_VND, H_VNU}) want(k, nobs_, 4);
     if (his_net_ && P.infiltration && d.dev().qinfmap) want(H_QINF, nobs_, 4);
     if (his_net_ && (P.inftype == 3 || P.inftype == 4)) want(H_S, nobs_, 4);
+    if (his_net_ && ndrn_ > 0) want(H_QDRN, ndrn_, 4);
     if (ncrs_faces_ > 0) {
       want(H_CRSU, ncrs_faces_, 4);
       if (!P.quadtree) want(H_CRSV, ncrs_faces_, 4);
@@ -605,6 +611,7 @@ void OutputWriter::open_his() {
   const int d_time = nc.def_dim("time", NcWriter::UNLIMITED);
   const int d_st = nc.def_dim("stations", (long long)std::max<size_t>(nobs_, 1));  // 1 without points, as the reference
   const int d_crs = ncrs_ > 0 ? nc.def_dim("crosssections", (long long)ncrs_) : -1;
+  const int d_drn = ndrn_ > 0 ? nc.def_dim("drainage", (long long)ndrn_) : -1;
   const int d_len = nc.def_dim("pointnamelength", 256);
   const int d_run = nc.def_dim("runtime", 1);
   nc.att_text(NcWriter::GLOBAL, "Conventions", "CF-1.8");
@@ -648,7 +655,7 @@ void OutputWriter::open_his() {
   nc.att_text(v_time, "units", "seconds since " + iso8601(h.tref));
   nc.att_text(v_time, "standard_name", "time");
   nc.att_text(v_time, "long_name", "time_in_seconds_since_" + iso8601(h.tref));
-  his_ids_.assign(10, -1);
+  his_ids_.assign(11, -1);
   his_ids_[0] = v_time;
   his_ids_[1] = pvar("point_zs", {d_time, d_st}, "m", "Water level", "sea_surface_height_above_reference_level");
   if (!P.subgrid || o.store_hsubgrid) his_ids_[2] = pvar("point_h", {d_time, d_st}, "m", "Water depth", "depth");
@@ -666,6 +673,8 @@ void OutputWriter::open_his() {
     his_ids_[9] = pvar("crosssection_discharge", {d_time, d_crs}, "m3 s-1", "discharge", nullptr);
     nc.att_text(his_ids_[9], "coordinates", "crosssection_name");
   }
+  if (ndrn_ > 0)  // (:1038-1041)
+    his_ids_[10] = pvar("drainage_discharge", {d_time, d_drn}, "m3 s-1", "discharge through drainage structure", nullptr);
   pvar("total_runtime", {d_run}, "s", "Total model runtime (s)", nullptr);
   pvar("average_dt", {d_run}, "s", "Average model time step (s)", nullptr);
   pvar("status", {d_run}, "-", "status of SFINCS simulation - 0 is no error", nullptr);
@@ -781,6 +790,7 @@ void OutputWriter::write(bool map, bool max, bool his, double tout, int p) {
     const int32_t* oc = d_maps_ + 4 * np_ + 5 * std::max<size_t>(nobs_, 1);
     g(H_CRSU, D.qu[p], oc);
     g(H_CRSV, D.quadtree ? nullptr : D.qv[p], oc);
+    g(H_QDRN, D.qtsrc, oc + std::max<size_t>(ncrs_faces_, 1));
   }
   check(cudaGetLastError(), "gather launch");
   check(cudaEventRecord(gathered_, main_), "record");
@@ -988,6 +998,8 @@ void OutputWriter::write_his_files(double tout, int rec) {
     const std::vector<float> qq = crs_discharges();
     nc.put_record(his_ids_[9], rec, qq.data(), ncrs_);
   }
+  if (his_ids_[10] >= 0 && slot(H_QDRN).host)  // qtsrc of each structure's intake (sfincs_ncoutput.F90:1410-1421)
+    nc.put_record(his_ids_[10], rec, (const float*)slot(H_QDRN).host, ndrn_);
   nc.sync();
 }
 

@@ -19,7 +19,7 @@ def _nc(path):
     return f
 
 
-def _model(tmp_path, extra, quadtree=False, subgrid=False, crs=True):
+def _model(tmp_path, extra, quadtree=False, subgrid=False, crs=True, drn=False):
     from crs_cases import add_crs
     from sfincs_b200 import qtsynth, synth
 
@@ -32,6 +32,10 @@ def _model(tmp_path, extra, quadtree=False, subgrid=False, crs=True):
                                   surge_peak=1.5)
     else:
         m = synth.plain_regular(nmax=24, mmax=30, dx=400.0, tstop=3600.0, seed=3, nbumps=6)
+    if drn:  # the five drainage structure types
+        from test_gpu_physics import _DRAINAGE
+
+        m.drn = _DRAINAGE
     d = m.write(str(tmp_path))
     with open(os.path.join(d, "sfincs.obs"), "w") as f:
         f.write("1000.0 1000.0 'harbour'\n2600.0 1800.0\n-500.0 -500.0 \"outside\"\n")
@@ -49,7 +53,7 @@ class Expected:
     """The oracle stepped one step at a time, with the reference's output
     schedule (sfincs_lib.f90:419-476): per output, its time and the state."""
 
-    def __init__(self, d, dtmap, dthis, dtmax, stored=("vmax_out", "twet_out"), ncrs=3):
+    def __init__(self, d, dtmap, dthis, dtmax, stored=("vmax_out", "twet_out"), ncrs=3, ndrn=0):
         from oracle.oracle import Oracle
 
         self.stored = stored
@@ -60,7 +64,7 @@ class Expected:
         self.zb = o.get("z_zmin") if s["subgrid"] else o.get("zb")
         md, mu = o.get("z_uv_md", n).astype(np.int64), o.get("z_uv_mu", n).astype(np.int64)
         nd, nu = o.get("z_uv_nd", n).astype(np.int64), o.get("z_uv_nu", n).astype(np.int64)
-        self.map, self.his, self.max, self.crs = [], [], [], []
+        self.map, self.his, self.max, self.crs, self.drn = [], [], [], [], []
         tmap, this, tmax = t0, t0, t0 + dtmax
         nmax_before = 0
         while o.scalars()["t"] < t1:
@@ -89,6 +93,8 @@ class Expected:
                 self.his.append((np.float32(tout), zs.copy()))
                 if ncrs:
                     self.crs.append(o.get("crs_discharge", ncrs))
+                if ndrn:
+                    self.drn.append(o.get("q_drain", ndrn))
             if wmax:
                 assert int(o.get("ntmaxout", 1)[0]) == nmax_before + 1
                 nmax_before += 1
@@ -102,12 +108,12 @@ def test_netcdf_map_his_and_max_match_the_oracle(tmp_path, subgrid):
     from sfincs_b200.bmi import Model
 
     extra = dict(dtout=600, dtmaxout=1200, dthisout=300, storevel=1, storevelmax=1, storetwet=1)
-    d, m = _model(tmp_path, extra, subgrid=subgrid)
+    d, m = _model(tmp_path, extra, subgrid=subgrid, drn=True)
     g = Model(d)
     s = g.scalars()
     g.run(s["t1"])
     g.finalize()
-    e = Expected(d, 600.0, 300.0, 1200.0)
+    e = Expected(d, 600.0, 300.0, 1200.0, ndrn=5)
     g.close()
     n = e.np
     # map file: cells on the (n, m) grid
@@ -166,6 +172,11 @@ def test_netcdf_map_his_and_max_match_the_oracle(tmp_path, subgrid):
     want = np.array(e.crs)
     assert np.abs(want).max() > 1.0
     assert np.allclose(qd, want, rtol=1e-4, atol=0.2), np.abs(qd - want).max()
+    # drainage structures: the rate of each intake at every his time (sfincs_ncoutput.F90:1410-1421)
+    qdr = h.variables["drainage_discharge"][:]
+    assert qdr.shape == (len(e.his), 5)
+    assert np.abs(np.array(e.drn)).max() > 0.1
+    assert np.allclose(qdr, np.array(e.drn), rtol=1e-3, atol=1e-3), np.abs(qdr - np.array(e.drn)).max()
     h.close()
 
 
