@@ -733,6 +733,8 @@ struct Model {
     bzsfile = in.str("bzsfile", "none");
     bcafile = in.str("bcafile", "none");
     crsfile = in.str("crsfile", "none");
+    rugfile = in.str("rugfile", "none");
+    runup_gauge_depth = in.real("rugdepth", 0.05f);
     use_bcafile = in.logical("use_bcafile", true);
     bzifile = in.str("bzifile", "none");
     srcfile = in.str("srcfile", "none");
@@ -2143,6 +2145,58 @@ struct Model {
     }
   }
 
+  // read_rug_file: sfincs_runup_gauges.f90:3-115 (two points per gauge, a
+  // point every 0.2 finest cell widths, its cell by find_quadtree_cell)
+  std::string rugfile = "none";
+  float runup_gauge_depth = 0.05f;
+  std::vector<std::vector<long>> runup_gauge_nm;
+  void read_rug_file() {
+    if (rugfile.substr(0, 4) == "none") return;
+    std::ifstream fin(path(rugfile));
+    if (!fin) throw std::runtime_error("oracle: cannot open " + rugfile);
+    std::vector<std::string> rec;
+    for (std::string l; std::getline(fin, l);) {
+      for (char& ch : l)
+        if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
+      if (l.find_first_not_of(' ') != std::string::npos) rec.push_back(l);
+    }
+    const float dxstep = 0.2f * dxyr(nref);
+    size_t ir = 0;
+    while (ir + 3 < rec.size() + 1 && ir + 1 < rec.size()) {
+      ir++;  // name
+      std::istringstream hs(rec[ir++]);
+      int nrows = 0, ncols = 0;
+      hs >> nrows >> ncols;
+      if (nrows != 2 || ir + 2 > rec.size()) throw std::runtime_error("oracle: run-up gauge needs two points");
+      float xru0, yru0, xru1, yru1;
+      std::istringstream(rec[ir++]) >> xru0 >> yru0;
+      std::istringstream(rec[ir++]) >> xru1 >> yru1;
+      const float rdx = xru1 - xru0, rdy = yru1 - yru0;
+      const float rlen = std::sqrt(rdx * rdx + rdy * rdy);
+      const long nrp = (long)(rlen / dxstep) + 1;
+      std::vector<long> nms;
+      for (long ip = 1; ip <= nrp; ip++) {
+        const float x = xru0 + (float)(ip - 1) * dxstep * rdx / rlen;
+        const float y = yru0 + (float)(ip - 1) * dxstep * rdy / rlen;
+        const long nmq = find_quadtree_cell(x, y);
+        const long nm = nmq > 0 ? index_sfincs_in_quadtree(nmq) : 0;
+        if (nm <= 0) throw std::runtime_error("oracle: run-up gauge point outside the mesh");
+        nms.push_back(nm);
+      }
+      runup_gauge_nm.push_back(nms);
+    }
+  }
+
+  // get_runup_levels: sfincs_runup_gauges.f90:117-150
+  float runup_level(size_t irug) {
+    float zru = -999.0f;
+    for (long nm : runup_gauge_nm[irug]) {
+      const float zbt = subgrid ? (float)sg_z_zmin(nm) : (float)zb(nm);
+      if ((double)zs(nm) > (double)(zbt + runup_gauge_depth)) zru = (float)zs(nm);
+    }
+    return zru;
+  }
+
   // get_discharges_through_crosssections: sfincs_crosssections.f90:130-176
   float crs_discharge(size_t icrs) {
     float qq = 0.0f;
@@ -2834,6 +2888,7 @@ struct Model {
     set_advection_mask();
     read_structures();  // sfincs_lib.f90:156, after initialize_domain
     read_crs_file();
+    read_rug_file();
     read_boundary_data();
     find_boundary_indices();
     read_discharges();
@@ -4068,6 +4123,10 @@ int oracle_get(void* hv, const char* name, double* out, long n) {
     else if (s == "q_drain") {  // per drainage structure the rate of its intake entry (sfincs_ncoutput.F90:1410-1421)
       if (m.ndrn != n) return -1;
       for (long i = 1; i <= n; i++) out[i - 1] = (double)m.qtsrc(m.nsrc + 2 * i - 1);
+    }
+    else if (s == "runup_zs") {  // run-up level of every gauge from the current zs
+      if ((long)m.runup_gauge_nm.size() != n) return -1;
+      for (long i = 0; i < n; i++) out[i] = (double)m.runup_level((size_t)i);
     }
     else if (s == "crs_discharge") {  // discharge through every cross-section from the current q
       if ((long)m.namecrs.size() != n) return -1;

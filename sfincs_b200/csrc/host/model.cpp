@@ -378,8 +378,7 @@ Keys parse_keys(const InpFile& in, HostModel& h, bool bmi) {
     if (in.integer("storemeteo", 0) == 1) throw std::runtime_error("storemeteo (meteo map output) is not supported");
     if (in.logical("debug", false)) throw std::runtime_error("debug output (every step) is not supported");
     o.crsfile = in.str("crsfile", "none");
-    if (!is_none(in.str("rugfile", "none")))
-      throw std::runtime_error("input 'rugfile' (run-up gauge output) is not supported");
+    o.rugdepth = in.real("rugdepth", 0.05f);
     for (const auto& kv : in.all()) o.inp.push_back(kv);
   }
   tspinup = t0 + tspinup;

@@ -61,6 +61,13 @@ struct CrossSection {
   std::vector<CrsFace> faces;
 };
 
+// One run-up gauge (sfincs_runup_gauges.f90:3-150): the cells (1-based) of
+// the points every 0.2 finest cell widths along its segment.
+struct RunupGauge {
+  std::string name;
+  std::vector<int32_t> cells;
+};
+
 struct OutputSpec {
   double t0out = 0, t1out = 0, dtmapout = 0, dthisout = 600, dtmaxout = 9999999;
   std::string map_type = "net", his_type = "net";  // net: netCDF; bin: Fortran records; his asc/bin: text
@@ -70,6 +77,8 @@ struct OutputSpec {
   std::vector<ObsPoint> obs;
   std::string crsfile = "none";
   std::vector<CrossSection> crs;
+  float rugdepth = 0.05f;
+  std::vector<RunupGauge> rug;
   std::vector<std::pair<std::string, std::string>> inp;  // the sfincs.inp keys, for the files' 'inp' attributes
 };
 

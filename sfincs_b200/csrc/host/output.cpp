@@ -52,18 +52,53 @@ enum {
   H_ZS, H_UMD, H_UMU, H_VND, H_VNU, H_QINF, H_S,                      // his (obs points)
   H_CRSU, H_CRSV,                                                     // his (cross-section faces: u, v fluxes)
   H_QDRN,                                                             // his (drainage structures)
+  H_RUG,                                                              // his (run-up gauge points: zs)
   NSLOT
 };
 
 }  // namespace
 
 // read_obs_points: sfincs_obspoints.f90:4-140
+// read_rug_file: sfincs_runup_gauges.f90:3-115.  Per gauge (name line,
+// "nrows ncols", its begin and end points) the cells of the points every
+// 0.2 finest cell widths from the begin point; a point outside the mesh is
+// refused (the reference would read level 0 there).
+static void read_runup_gauges(HostModel& h, const std::string& file) {
+  h.out.rug.clear();
+  if (file.compare(0, 4, "none") == 0) return;
+  std::vector<std::string> names;
+  const auto pls = read_polylines(h.dir + "/" + file, 0, &names);
+  const float dxyr = h.p.quadtree ? std::min(h.qt_dxr.back(), h.qt_dyr.back()) : std::min(h.p.dx, h.p.dy);
+  const float dxstep = 0.2f * dxyr;
+  for (size_t k = 0; k < pls.size(); k++) {
+    if (pls[k].size() != 2) throw std::runtime_error("run-up gauge '" + names[k] + "' must have exactly two points");
+    const float x0 = pls[k][0].x, y0 = pls[k][0].y, rdx = pls[k][1].x - x0, rdy = pls[k][1].y - y0;
+    const float rlen = std::sqrt(rdx * rdx + rdy * rdy);
+    const int nrp = (int)(rlen / dxstep) + 1;
+    RunupGauge g;
+    g.name = names[k];
+    for (int ip = 1; ip <= nrp; ip++) {
+      const float x = x0 + (float)(ip - 1) * dxstep * rdx / rlen;
+      const float y = y0 + (float)(ip - 1) * dxstep * rdy / rlen;
+      const int nm = cell_index(h, (double)x, (double)y);
+      if (nm <= 0) throw std::runtime_error("run-up gauge '" + names[k] + "' leaves the active mesh");
+      g.cells.push_back(nm);
+    }
+    h.out.rug.push_back(std::move(g));
+  }
+}
+
 void read_obs_points(HostModel& h) {
   const std::string file = [&] {
     for (const auto& kv : h.out.inp)
       if (kv.first == "obsfile") return kv.second;
     return std::string("none");
   }();
+  read_runup_gauges(h, [&] {
+    for (const auto& kv : h.out.inp)
+      if (kv.first == "rugfile") return kv.second;
+    return std::string("none");
+  }());
   h.out.obs.clear();
   h.need_qinfmap = h.p.infiltration && h.p.inftype == 5 && h.out.dtmapout > 1.0e-6 && h.out.map_type == "net";
   if (file.compare(0, 4, "none") == 0) return;
@@ -115,6 +150,8 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
   np_ = (size_t)h.np;
   nobs_ = o.obs.size();
   ncrs_ = o.crs.size();
+  nrug_ = o.rug.size();
+  for (const auto& g : o.rug) nrug_pts_ += g.cells.size();
   for (const auto& cs : o.crs) ncrs_faces_ += cs.faces.size();
   // which files (sfincs_output.f90:8-58)
   if (o.dtmapout > 1.0e-6) {
@@ -127,7 +164,7 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
     // netCDF: into the map file, which exists only with map output; binary: files of their own
     max_on_ = o.map_type == "net" ? map_net_ : true;
   }
-  if (o.dthisout > 1.0e-6 && (nobs_ > 0 || ncrs_ > 0)) {
+  if (o.dthisout > 1.0e-6 && (nobs_ > 0 || ncrs_ > 0 || nrug_ > 0)) {
     thisout = (double)h.t0;
     his_net_ = o.his_type == "net";
     his_txt_ = !his_net_;
@@ -142,7 +179,8 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
   // (regular grids: the cell's own faces and those of its left / lower
   // neighbours), then per observation point its cell and faces
   ndrn_ = (size_t)P.ndrn;
-  std::vector<int32_t> maps(4 * np_ + 5 * std::max<size_t>(nobs_, 1) + std::max<size_t>(ncrs_faces_, 1) + ndrn_, 0);
+  std::vector<int32_t> maps(4 * np_ + 5 * std::max<size_t>(nobs_, 1) + std::max<size_t>(ncrs_faces_, 1) + ndrn_ + nrug_pts_,
+                            0);
   for (size_t i = 0; i < np_; i++) {
     if (P.quadtree) {
       const int4 c = h.qcell[i];
@@ -165,6 +203,9 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
     // then per drainage structure its intake entry of the source rates
     j = 4 * np_ + 5 * std::max<size_t>(nobs_, 1) + std::max<size_t>(ncrs_faces_, 1);
     for (size_t k = 0; k < ndrn_; k++) maps[j++] = (int32_t)(P.nsrc + 2 * k);
+    // then the cell of every run-up gauge point
+    for (const auto& g : o.rug)
+      for (int32_t nm : g.cells) maps[j++] = h.cmp_off[(size_t)nm - 1];
   }
   check(cudaMalloc(&d_maps_, maps.size() * 4), "maps");
   check(cudaMemcpy(d_maps_, maps.data(), maps.size() * 4, cudaMemcpyHostToDevice), "maps");
@@ -198,6 +239,7 @@ OutputWriter::OutputWriter(const HostModel& h, DeviceModel& d, cudaStream_t main
     if (his_net_ && P.infiltration && d.dev().qinfmap) want(H_QINF, nobs_, 4);
     if (his_net_ && (P.inftype == 3 || P.inftype == 4)) want(H_S, nobs_, 4);
     if (his_net_ && ndrn_ > 0) want(H_QDRN, ndrn_, 4);
+    if (his_net_ && nrug_pts_ > 0) want(H_RUG, nrug_pts_, 4);
     if (ncrs_faces_ > 0) {
       want(H_CRSU, ncrs_faces_, 4);
       if (!P.quadtree) want(H_CRSV, ncrs_faces_, 4);
@@ -612,6 +654,7 @@ void OutputWriter::open_his() {
   const int d_st = nc.def_dim("stations", (long long)std::max<size_t>(nobs_, 1));  // 1 without points, as the reference
   const int d_crs = ncrs_ > 0 ? nc.def_dim("crosssections", (long long)ncrs_) : -1;
   const int d_drn = ndrn_ > 0 ? nc.def_dim("drainage", (long long)ndrn_) : -1;
+  const int d_rug = nrug_ > 0 ? nc.def_dim("runup_gauges", (long long)nrug_) : -1;
   const int d_len = nc.def_dim("pointnamelength", 256);
   const int d_run = nc.def_dim("runtime", 1);
   nc.att_text(NcWriter::GLOBAL, "Conventions", "CF-1.8");
@@ -624,6 +667,7 @@ void OutputWriter::open_his() {
   const int v_name = nc.def_var("station_name", NcWriter::CHAR, {d_st, d_len});
   nc.att_text(v_name, "cf_role", "timeseries_id");
   const int v_crsname = ncrs_ > 0 ? nc.def_var("crosssection_name", NcWriter::CHAR, {d_crs, d_len}) : -1;
+  const int v_rugname = nrug_ > 0 ? nc.def_var("runup_gauge_name", NcWriter::CHAR, {d_rug, d_len}) : -1;
   auto coord = [&](const char* name, bool x, const char* long_name) {
     const int v = nc.def_var(name, NcWriter::FLOAT, {d_st});
     nc.att_text(v, "units", P.geo ? "degrees" : "m");  // def_his_point_coord
@@ -655,7 +699,7 @@ void OutputWriter::open_his() {
   nc.att_text(v_time, "units", "seconds since " + iso8601(h.tref));
   nc.att_text(v_time, "standard_name", "time");
   nc.att_text(v_time, "long_name", "time_in_seconds_since_" + iso8601(h.tref));
-  his_ids_.assign(11, -1);
+  his_ids_.assign(12, -1);
   his_ids_[0] = v_time;
   his_ids_[1] = pvar("point_zs", {d_time, d_st}, "m", "Water level", "sea_surface_height_above_reference_level");
   if (!P.subgrid || o.store_hsubgrid) his_ids_[2] = pvar("point_h", {d_time, d_st}, "m", "Water depth", "depth");
@@ -672,6 +716,10 @@ void OutputWriter::open_his() {
   if (ncrs_ > 0) {  // ncoutput_his_init (sfincs_ncoutput.F90:1033-1036)
     his_ids_[9] = pvar("crosssection_discharge", {d_time, d_crs}, "m3 s-1", "discharge", nullptr);
     nc.att_text(his_ids_[9], "coordinates", "crosssection_name");
+  }
+  if (nrug_ > 0) {  // (:1043-1046)
+    his_ids_[11] = pvar("runup_gauge_zs", {d_time, d_rug}, "m", "run-up elevation", nullptr);
+    nc.att_text(his_ids_[11], "coordinates", "runup_gauge_name");
   }
   if (ndrn_ > 0)  // (:1038-1041)
     his_ids_[10] = pvar("drainage_discharge", {d_time, d_drn}, "m3 s-1", "discharge through drainage structure", nullptr);
@@ -699,6 +747,12 @@ void OutputWriter::open_his() {
     for (size_t k = 0; k < ncrs_; k++)
       std::memcpy(&cn[k * 256], o.crs[k].name.data(), std::min<size_t>(o.crs[k].name.size(), 256));
     nc.put(v_crsname, cn.data(), cn.size());
+  }
+  if (nrug_ > 0) {
+    std::vector<char> rn(nrug_ * 256, ' ');
+    for (size_t k = 0; k < nrug_; k++)
+      std::memcpy(&rn[k * 256], o.rug[k].name.data(), std::min<size_t>(o.rug[k].name.size(), 256));
+    nc.put(v_rugname, rn.data(), rn.size());
   }
   const int32_t epsg = o.epsg;
   nc.put(v_crs, &epsg, 1);
@@ -791,6 +845,7 @@ void OutputWriter::write(bool map, bool max, bool his, double tout, int p) {
     g(H_CRSU, D.qu[p], oc);
     g(H_CRSV, D.quadtree ? nullptr : D.qv[p], oc);
     g(H_QDRN, D.qtsrc, oc + std::max<size_t>(ncrs_faces_, 1));
+    g(H_RUG, D.zs, oc + std::max<size_t>(ncrs_faces_, 1) + ndrn_);
   }
   check(cudaGetLastError(), "gather launch");
   check(cudaEventRecord(gathered_, main_), "record");
@@ -997,6 +1052,18 @@ void OutputWriter::write_his_files(double tout, int rec) {
   if (his_ids_[9] >= 0) {
     const std::vector<float> qq = crs_discharges();
     nc.put_record(his_ids_[9], rec, qq.data(), ncrs_);
+  }
+  if (his_ids_[11] >= 0) {  // get_runup_levels (sfincs_runup_gauges.f90:117-150): the last point wetter than rugdepth
+    const float* z = (const float*)slot(H_RUG).host;
+    std::vector<float> zru(nrug_, -999.0f);
+    size_t j = 0;
+    for (size_t k = 0; k < nrug_; k++)
+      for (int32_t nm : o.rug[k].cells) {
+        const float zbt = P.subgrid ? h.zmin_cmp[(size_t)nm - 1] : h.zb_cmp[(size_t)nm - 1];
+        if (z[j] > zbt + o.rugdepth) zru[k] = z[j];
+        j++;
+      }
+    nc.put_record(his_ids_[11], rec, zru.data(), nrug_);
   }
   if (his_ids_[10] >= 0 && slot(H_QDRN).host)  // qtsrc of each structure's intake (sfincs_ncoutput.F90:1410-1421)
     nc.put_record(his_ids_[10], rec, (const float*)slot(H_QDRN).host, ndrn_);

@@ -54,7 +54,7 @@ class OutputWriter {
   cudaStream_t main_ = nullptr, copy_ = nullptr;
   cudaEvent_t gathered_ = nullptr, copied_ = nullptr;
   int32_t* d_maps_ = nullptr;  // device gather maps: md, nd, mu, nu uv points of every cell; obs cells
-  size_t np_ = 0, nobs_ = 0, ncrs_ = 0, ncrs_faces_ = 0, ndrn_ = 0;
+  size_t np_ = 0, nobs_ = 0, ncrs_ = 0, ncrs_faces_ = 0, ndrn_ = 0, nrug_ = 0, nrug_pts_ = 0;
   bool map_net_ = false, map_bin_ = false, his_net_ = false, his_txt_ = false, max_on_ = false;
   int infstate_ = 0;  // map state of the infiltration: 3 Seff, 4 sigma, 5 f
   std::unique_ptr<NcWriter> map_nc_, his_nc_;
@@ -65,7 +65,8 @@ class OutputWriter {
   std::vector<int> max_vars_;  // netCDF ids: timemax, zsmax, cumprcp, tmax, t_zsmax, hmax, vmax, qmax, cuminf (-1: off)
   std::vector<int> rec_ids_;   // netCDF ids: time, zs, h, u, v, subgrid_volume, infiltration state (-1: off)
   std::vector<int> his_ids_;   // netCDF ids: time, point_zs, point_h, point_u, point_v, point_uvmag, point_uvdir,
-                               // point_qinf, point_S, crosssection_discharge, drainage_discharge
+                               // point_qinf, point_S, crosssection_discharge, drainage_discharge,
+                               // runup_gauge_zs
   std::vector<size_t> file_idx_;  // file position (n, m) or quadtree point of every compact cell
   size_t ncells_file_ = 0;
   float huthresh_ = 0;

@@ -46,6 +46,11 @@ def _model(tmp_path, extra, quadtree=False, subgrid=False, crs=True, drn=False):
             f.write(f"{k:<20} = {v}\n")
     if crs:  # three cross-sections (the quadtree mesh spans 4 km x 3.2 km)
         add_crs(d, scale=1.0 / 3.0 if quadtree else 1.0)
+    if drn:  # two run-up gauges from the sea onto the beach
+        with open(os.path.join(d, "sfincs.rug"), "w") as f:
+            f.write("rug_south\n2 2\n500.0 3000.0\n11000.0 3000.0\nrug_north\n2 2\n500.0 7000.0\n11000.0 7000.0\n")
+        with open(os.path.join(d, "sfincs.inp"), "a") as f:
+            f.write(f"{'rugfile':<20} = sfincs.rug\n{'rugdepth':<20} = 0.05\n")
     return d, m
 
 
@@ -53,7 +58,7 @@ class Expected:
     """The oracle stepped one step at a time, with the reference's output
     schedule (sfincs_lib.f90:419-476): per output, its time and the state."""
 
-    def __init__(self, d, dtmap, dthis, dtmax, stored=("vmax_out", "twet_out"), ncrs=3, ndrn=0):
+    def __init__(self, d, dtmap, dthis, dtmax, stored=("vmax_out", "twet_out"), ncrs=3, ndrn=0, nrug=0):
         from oracle.oracle import Oracle
 
         self.stored = stored
@@ -64,7 +69,7 @@ class Expected:
         self.zb = o.get("z_zmin") if s["subgrid"] else o.get("zb")
         md, mu = o.get("z_uv_md", n).astype(np.int64), o.get("z_uv_mu", n).astype(np.int64)
         nd, nu = o.get("z_uv_nd", n).astype(np.int64), o.get("z_uv_nu", n).astype(np.int64)
-        self.map, self.his, self.max, self.crs, self.drn = [], [], [], [], []
+        self.map, self.his, self.max, self.crs, self.drn, self.rug = [], [], [], [], [], []
         tmap, this, tmax = t0, t0, t0 + dtmax
         nmax_before = 0
         while o.scalars()["t"] < t1:
@@ -95,6 +100,8 @@ class Expected:
                     self.crs.append(o.get("crs_discharge", ncrs))
                 if ndrn:
                     self.drn.append(o.get("q_drain", ndrn))
+                if nrug:
+                    self.rug.append(o.get("runup_zs", nrug))
             if wmax:
                 assert int(o.get("ntmaxout", 1)[0]) == nmax_before + 1
                 nmax_before += 1
@@ -113,7 +120,7 @@ def test_netcdf_map_his_and_max_match_the_oracle(tmp_path, subgrid):
     s = g.scalars()
     g.run(s["t1"])
     g.finalize()
-    e = Expected(d, 600.0, 300.0, 1200.0, ndrn=5)
+    e = Expected(d, 600.0, 300.0, 1200.0, ndrn=5, nrug=2)
     g.close()
     n = e.np
     # map file: cells on the (n, m) grid
@@ -177,6 +184,12 @@ def test_netcdf_map_his_and_max_match_the_oracle(tmp_path, subgrid):
     assert qdr.shape == (len(e.his), 5)
     assert np.abs(np.array(e.drn)).max() > 0.1
     assert np.allclose(qdr, np.array(e.drn), rtol=1e-3, atol=1e-3), np.abs(qdr - np.array(e.drn)).max()
+    # run-up gauges: the level of the last point wetter than rugdepth (sfincs_runup_gauges.f90:117-150)
+    assert [b"".join(r).decode().strip() for r in h.variables["runup_gauge_name"][:]] == ["rug_south", "rug_north"]
+    zru, want = h.variables["runup_gauge_zs"][:], np.array(e.rug)
+    assert zru.shape == (len(e.his), 2) and np.all(want > -999.0)
+    assert np.allclose(zru, want, atol=0.05), np.abs(zru - want).max()
+    assert np.mean(np.abs(zru - want) <= 2e-5) >= 0.8
     h.close()
 
 
